@@ -1,0 +1,168 @@
+/*
+ * profit_b200: B200-native (sm_100a) model images and likelihoods for the
+ * ProFit / libprofit galaxy-profile path, behind a plain C ABI.
+ *
+ * The entry points mirror libprofit 1.9.3's C++ Model/Profile/Convolver API
+ * (src/libprofit/src/profit/model.h, profile.h, convolve.h) and the R glue
+ * R_profit_make_model (src/r_profit.cpp:549-680) so that ProFit's
+ * profitMakeModel (R/profitMakeModel.R:283) and profitLikeModel
+ * (R/profitLikeModel.R:225-379) can call this library instead of libprofit.
+ *
+ * Conventions
+ *  - Every function returns PF_OK (0) or a negative PF_E* status; the message
+ *    of the last failure on the calling thread is pf_last_error().  No C++
+ *    exception crosses this boundary.
+ *  - Images are row-major doubles with x fastest: pixel (x, y) of a W x H
+ *    image is at [x + y*W].  This is libprofit's Image layout
+ *    (image.h:262-267) and R's column-major matrix with nrow = W
+ *    (r_profit.cpp:26-27).
+ *  - Host pointers are caller-owned and only read/written during the call.
+ *  - A pf_model owns one CUDA stream and its device buffers.  It is not
+ *    re-entrant: use one handle per host thread.
+ *  - The library needs a CUDA device of compute capability 10.0 (B200).
+ *    There is no CPU fallback: without one, pf_model_create fails with
+ *    PF_E_CUDA.
+ */
+#ifndef PROFIT_B200_H
+#define PROFIT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  libprofit throws profit::invalid_parameter /
+ * unknown_parameter (exceptions.h:41-100); those map to PF_E_INVALID and
+ * PF_E_UNKNOWN_PARAM here. */
+#define PF_OK 0
+#define PF_E_INVALID -1          /* invalid parameter value or model setup */
+#define PF_E_UNKNOWN_PARAM -2    /* profile has no parameter of that name/type */
+#define PF_E_CUDA -3             /* CUDA runtime error (message has details) */
+#define PF_E_CAPACITY -4         /* a device work queue could not grow enough */
+#define PF_E_BUFFER -5           /* caller's output buffer too small */
+#define PF_E_STATE -6            /* call out of order (e.g. likelihood without data) */
+
+/* Arithmetic of the pixel path.
+ *  PF_FP64: the plain form.  Same subsampling decisions as libprofit, pixel
+ *           for pixel; images within 1e-12 relative of the reference.
+ *  PF_FP32: per-pixel rendering and convolution in FP32; FP64 for the
+ *           per-profile scalars (Sersic b_n, normalisation), sub-pixel
+ *           coordinates, and the likelihood sum.  Required for gradients. */
+#define PF_FP64 0
+#define PF_FP32 1
+
+typedef struct pf_model pf_model;
+
+/* Last error message of the calling thread ("" if none). */
+const char *pf_last_error(void);
+
+/* Library version string, e.g. "profit_b200 0.1 (libprofit 1.9.3 API)". */
+const char *pf_version(void);
+
+/* ---- Model life cycle -------------------------------------------------
+ * Replaces profit::Model::Model(width, height) (model.h:88-100). */
+int pf_model_create(unsigned width, unsigned height, pf_model **out);
+int pf_model_destroy(pf_model *m);
+
+/* ---- Profiles ---------------------------------------------------------
+ * pf_model_add_profile replaces Model::add_profile (model.cpp:103-135):
+ * names "sersic", "moffat", "ferrer"/"ferrers", "coresersic", "king",
+ * "brokenexp", "sky", "psf", "null".  *index receives the profile's index.
+ * Parameters keep libprofit's names and types (profile.h:150-177):
+ *   double: xcen ycen mag ang axrat box acc rscale_switch rscale_max
+ *           re nser fwhm con rout a b rb rc rt h1 h2 bg
+ *   uint:   resolution max_recursions
+ *   bool:   convolve rough adjust force_cpu rescale_flux
+ * Setting a name the profile lacks, or with the wrong type, returns
+ * PF_E_UNKNOWN_PARAM like Profile::parameter (profile.cpp:81-93). */
+int pf_model_add_profile(pf_model *m, const char *name, int *index);
+int pf_profile_set_double(pf_model *m, int index, const char *name, double value);
+int pf_profile_set_uint(pf_model *m, int index, const char *name, unsigned value);
+int pf_profile_set_bool(pf_model *m, int index, const char *name, int value);
+/* "name = value", like Profile::parameter(const std::string&) (profile.cpp:136-158). */
+int pf_profile_set(pf_model *m, int index, const char *spec);
+int pf_profile_get_double(pf_model *m, int index, const char *name, double *value);
+int pf_model_profile_count(pf_model *m, int *count);
+/* Removes all profiles (R rebuilds the Model on every call; handles can be reused). */
+int pf_model_clear_profiles(pf_model *m);
+
+/* ---- Model settings (model.h:142-343) --------------------------------- */
+/* PSF is copied and normalised to unit sum, like Model::set_psf (model.h:160-170). */
+int pf_model_set_psf(pf_model *m, const double *psf, unsigned width, unsigned height);
+int pf_model_set_magzero(pf_model *m, double magzero);
+int pf_model_set_image_pixel_scale(pf_model *m, double scale_x, double scale_y);
+int pf_model_set_psf_pixel_scale(pf_model *m, double scale_x, double scale_y);
+int pf_model_set_finesampling(pf_model *m, unsigned finesampling);
+int pf_model_set_return_finesampled(pf_model *m, int value);
+/* Only crop = true is supported (ProFit's returncrop default). */
+int pf_model_set_crop(pf_model *m, int value);
+/* "brute" (default, like Model::ensure_convolver, model.cpp:144-150),
+ * "brute-old", "fft" or "null" (create_convolver, convolve.cpp:526-594). */
+int pf_model_set_convolver(pf_model *m, const char *type);
+int pf_model_set_precision(pf_model *m, int precision);
+
+/* Dimensions the profiles are drawn on before convolution and crop
+ * (Model::get_drawing_dimensions, model.cpp:152-219). */
+int pf_model_drawing_dims(pf_model *m, unsigned *width, unsigned *height);
+
+/* ---- Evaluation ---------------------------------------------------------
+ * Replaces Model::evaluate(Image&, Point&) (model.cpp:271-338).  `image`
+ * receives the cropped (and, with finesampling and !return_finesampled,
+ * downsampled) model of out_w x out_h pixels; `capacity` is its length in
+ * doubles.  offset_x/y receive the offset Model::evaluate reports.  Any of
+ * the out pointers may be NULL. */
+int pf_model_evaluate(pf_model *m, double *image, size_t capacity,
+                      unsigned *out_w, unsigned *out_h, int *offset_x, int *offset_y);
+
+/* ---- Likelihood (R/profitLikeModel.R:244-276, like.func = "norm") ------
+ * Data image and sigma map of the model's output size; region (optional,
+ * 1 = use pixel, like Data$region_which) may be NULL.  Copied to the device
+ * once, as profitSetupData prepares Data once per fit. */
+int pf_model_set_data(pf_model *m, const double *image, const double *sigma,
+                      const uint8_t *region, unsigned width, unsigned height);
+
+/* logL = sum over region of log dnorm((image - model)/sigma), the value of
+ * profitLikeModel's LL for like.func = "norm". */
+int pf_model_loglike(pf_model *m, double *loglike);
+
+/* Parameters the gradient is taken with respect to.  Each entry names a
+ * profile index and one of its double parameters ("xcen", "ycen", "mag",
+ * "ang", "axrat", "box", "re", "nser", "fwhm", "con", ...). */
+typedef struct {
+	int profile;
+	const char *name;
+} pf_param_ref;
+
+/* logL and d(logL)/d(parameter) for every entry of `params`, by the
+ * hand-written adjoint (precision PF_FP32).  The reference has no gradient;
+ * this is new.  Subsampling decisions are held fixed, as the derivative of
+ * the chosen quadrature. */
+int pf_model_loglike_grad(pf_model *m, const pf_param_ref *params, int n_params,
+                          double *loglike, double *grad);
+
+/* Same quantities by central finite differences of the plain form (FP64),
+ * 2*n_params + 1 evaluations with relative step `rel_step` (absolute step
+ * rel_step*max(|p|, 1)); the baseline that pf_model_loglike_grad replaces. */
+int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_params,
+                             double rel_step, double *loglike, double *grad);
+
+/* ---- Instrumentation ---------------------------------------------------
+ * With debug on, evaluations record for each radial profile the number of
+ * subsample_pixel calls per drawing pixel (-1 = beyond rscale_max, 0 =
+ * evaluated directly) and per recursion level, like libprofit's PROFIT_DEBUG
+ * counters (radial.cpp:70-78). */
+int pf_model_set_debug(pf_model *m, int value);
+int pf_model_decisions(pf_model *m, int profile, int32_t *out, size_t capacity);
+int pf_model_level_counts(pf_model *m, int profile, int64_t *out, int max_levels, int *n_levels);
+
+/* Device time (ms, CUDA events) of the last evaluation's phases:
+ * [0] total, [1] render, [2] convolution, [3] likelihood/adjoint. */
+int pf_model_last_timings(pf_model *m, float *ms, int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PROFIT_B200_H */

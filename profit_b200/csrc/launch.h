@@ -1,0 +1,49 @@
+// Host-side launch wrappers of the kernels (one translation unit each, so the
+// FP64 parity kernels can be compiled without FMA contraction).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace pf {
+
+// render64.cu
+cudaError_t launch_pixels64(const DevProfile *profiles, int n_profiles, unsigned width, unsigned height, double sx,
+                            double sy, double *img_conv, double *img_plain, const QueueSet &q, cudaStream_t s);
+cudaError_t launch_levels64(const DevProfile *profiles, int n_levels, double *img_conv, double *img_plain,
+                            const QueueSet &q, cudaStream_t s);
+cudaError_t launch_count_decisions(const QueueSet &q, int n_levels, size_t npix, cudaStream_t s);
+cudaError_t launch_psf_stamp64(const DevProfile *profiles, int p, const double *psf, unsigned psf_w, unsigned psf_h,
+                               double psf_sx, double psf_sy, double scale_x, double scale_y, double offx, double offy,
+                               unsigned width, unsigned height, double *img_conv, double *img_plain, cudaStream_t s);
+cudaError_t launch_conv64(const double *src, int sw, int sh, int ox, int oy, const double *K, int kw, int kh,
+                          double *out, int ow, int oh, const double *add, int add_stride, int add_ox, int add_oy,
+                          cudaStream_t s);
+cudaError_t launch_loglike64(const double *model, const double *data, const double *sigma, const uint8_t *region,
+                             int n, double2 *partials, int nparts, double *out, cudaStream_t s);
+cudaError_t launch_crop64(const double *src, unsigned sw, unsigned ox, unsigned oy, double *out, unsigned ow,
+                          unsigned oh, const double *add, cudaStream_t s);
+cudaError_t launch_downsample64(const double *src, unsigned sw, unsigned sh, unsigned fs, double *out, unsigned ow,
+                                unsigned oh, cudaStream_t s);
+
+// render32.cu
+cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
+                            unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
+                            const QueueSet &q, cudaStream_t s);
+cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
+                            float *jac, const QueueSet &q, cudaStream_t s);
+cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
+                              const int *prof_batch, int n_profiles, unsigned npix, double *out, cudaStream_t s);
+cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
+                              unsigned dh, int batch, float *g_plain, cudaStream_t s);
+cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
+                          float *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
+                          int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s);
+cudaError_t launch_loglike32(const float *model, const double *data, const double *sigma, const uint8_t *region,
+                             int n, int batch, int data_batch_stride, double2 *partials, int nparts, double *out,
+                             float *wseed, cudaStream_t s);
+cudaError_t launch_crop32(const float *src, unsigned sw, unsigned ox, unsigned oy, float *out, unsigned ow,
+                          unsigned oh, const float *add, int batch, unsigned src_stride, cudaStream_t s);
+
+}  // namespace pf

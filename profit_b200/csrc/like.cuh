@@ -1,0 +1,114 @@
+// ProFit's "norm" log-likelihood (R/profitLikeModel.R:263-276):
+//   cutsig = (image - model) / sigma,  LL = sum(dnorm(cutsig, log = TRUE))
+// with dnorm(x, 0, 1, log) = -(log(sqrt(2 pi)) + x^2/2).
+//
+// The sum runs in FP64 with Neumaier compensation per thread, a shuffle
+// reduction of (sum, compensation) pairs per warp and block, one partial per
+// block, and a one-block final pass: deterministic for a fixed grid.  The
+// same pass can write the adjoint seed dLL/dmodel = (image - model)/sigma^2.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace pf {
+
+struct Neumaier {
+	double s, c;
+};
+
+__device__ __forceinline__ void neumaier_add(Neumaier &a, double x)
+{
+	double t = a.s + x;
+	if (fabs(a.s) >= fabs(x)) a.c += (a.s - t) + x;
+	else a.c += (x - t) + a.s;
+	a.s = t;
+}
+
+__device__ __forceinline__ Neumaier neumaier_merge(Neumaier a, Neumaier b)
+{
+	Neumaier r;
+	r.c = a.c + b.c;
+	r.s = a.s;
+	neumaier_add(r, b.s);
+	return r;
+}
+
+__device__ __forceinline__ Neumaier neumaier_warp(Neumaier v)
+{
+	for (int o = 16; o > 0; o >>= 1) {
+		Neumaier other;
+		other.s = __shfl_xor_sync(0xffffffffu, v.s, o);
+		other.c = __shfl_xor_sync(0xffffffffu, v.c, o);
+		v = neumaier_merge(v, other);
+	}
+	return v;
+}
+
+__device__ __forceinline__ Neumaier neumaier_block(Neumaier v)
+{
+	__shared__ double s_s[32], s_c[32];
+	int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	v = neumaier_warp(v);
+	if (lane == 0) {
+		s_s[wid] = v.s;
+		s_c[wid] = v.c;
+	}
+	__syncthreads();
+	int nw = (blockDim.x + 31) >> 5;
+	if (wid == 0) {
+		Neumaier u{0.0, 0.0};
+		if (lane < nw) {
+			u.s = s_s[lane];
+			u.c = s_c[lane];
+		}
+		v = neumaier_warp(u);
+	}
+	return v;
+}
+
+constexpr double LN_SQRT_2PI = 0.918938533204672741780329736406;
+
+// n pixels per image, `batch` images laid out back to back; one partial
+// (s, c) per block in partials[batch][gridDim.x].
+template <class T>
+__global__ void k_loglike_partial(const T *__restrict__ model, const double *__restrict__ data,
+                                  const double *__restrict__ sigma, const uint8_t *__restrict__ region, int n,
+                                  double2 *__restrict__ partials, float *__restrict__ wseed,
+                                  int data_batch_stride)
+{
+	const int b = blockIdx.y;
+	model += (size_t)b * n;
+	data += (size_t)b * data_batch_stride;
+	sigma += (size_t)b * data_batch_stride;
+	if (region) region += (size_t)b * data_batch_stride;
+	if (wseed) wseed += (size_t)b * n;
+	Neumaier acc{0.0, 0.0};
+	for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+		bool use = !region || region[k];
+		double m = (double)model[k];
+		double s = sigma[k];
+		double diff = data[k] - m;
+		if (use) {
+			double x = diff / s;
+			neumaier_add(acc, -(LN_SQRT_2PI + 0.5 * x * x));
+		}
+		if (wseed) wseed[k] = use ? (float)(diff / (s * s)) : 0.0f;
+	}
+	acc = neumaier_block(acc);
+	if (threadIdx.x == 0) partials[(size_t)b * gridDim.x + blockIdx.x] = make_double2(acc.s, acc.c);
+}
+
+static __global__ void k_loglike_final(const double2 *__restrict__ partials, int nparts, double *__restrict__ out)
+{
+	const int b = blockIdx.x;
+	Neumaier acc{0.0, 0.0};
+	for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
+		double2 p = partials[(size_t)b * nparts + k];
+		acc = neumaier_merge(acc, Neumaier{p.x, p.y});
+	}
+	acc = neumaier_block(acc);
+	if (threadIdx.x == 0) out[b] = acc.s + acc.c;
+}
+
+}  // namespace pf

@@ -1,0 +1,1141 @@
+// Host side of the library: the Model/Profile API of libprofit 1.9.3
+// (model.h:55-421, profile.h:79-261, convolve.h:68-209) over device buffers,
+// and the C ABI declared in include/profit_b200.h.
+//
+// Evaluation mirrors Model::evaluate (model.cpp:271-338) and
+// Model::produce_image (model.cpp:340-380): profiles marked `convolve` are
+// drawn into one padded image, the others into a second one; the first is
+// convolved with the normalised PSF, the PSF padding is cropped, the second
+// is added, and finesampled images are summed back down when requested.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "launch.h"
+#include "profit_b200.h"
+
+using namespace pf;
+
+namespace {
+
+thread_local std::string g_error;
+
+int set_error(int code, const std::string &msg)
+{
+	g_error = msg;
+	return code;
+}
+
+#define PF_CUDA(expr)                                                                          \
+	do {                                                                                       \
+		cudaError_t e_ = (expr);                                                               \
+		if (e_ != cudaSuccess)                                                                 \
+			return set_error(PF_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+	} while (0)
+
+#define PF_TRY(expr)          \
+	do {                      \
+		int st_ = (expr);     \
+		if (st_ != PF_OK)     \
+			return st_;       \
+	} while (0)
+
+struct DevBuf {
+	void *p = nullptr;
+	size_t bytes = 0;
+	~DevBuf()
+	{
+		if (p) cudaFree(p);
+	}
+	template <class T>
+	T *as() const
+	{
+		return static_cast<T *>(p);
+	}
+};
+
+struct HostBuf {
+	void *p = nullptr;
+	size_t bytes = 0;
+	~HostBuf()
+	{
+		if (p) cudaFreeHost(p);
+	}
+	template <class T>
+	T *as() const
+	{
+		return static_cast<T *>(p);
+	}
+};
+
+cudaError_t ensure(DevBuf &b, size_t bytes)
+{
+	if (bytes <= b.bytes && b.p) return cudaSuccess;
+	if (b.p) cudaFree(b.p);
+	b.p = nullptr;
+	b.bytes = 0;
+	size_t want = std::max<size_t>(bytes + bytes / 4, 256);
+	cudaError_t e = cudaMalloc(&b.p, want);
+	if (e == cudaSuccess) b.bytes = want;
+	return e;
+}
+
+cudaError_t ensure(HostBuf &b, size_t bytes)
+{
+	if (bytes <= b.bytes && b.p) return cudaSuccess;
+	if (b.p) cudaFreeHost(b.p);
+	b.p = nullptr;
+	b.bytes = 0;
+	size_t want = std::max<size_t>(bytes + bytes / 4, 256);
+	cudaError_t e = cudaMallocHost(&b.p, want);
+	if (e == cudaSuccess) b.bytes = want;
+	return e;
+}
+
+// Parameter registry: libprofit's register_parameter calls per profile.
+enum PType { T_DOUBLE, T_UINT, T_BOOL };
+struct ParamDesc {
+	const char *name;
+	PType type;
+	size_t off;
+};
+#define PDD(n) {#n, T_DOUBLE, offsetof(ProfileParams, n)}
+#define PDU(n) {#n, T_UINT, offsetof(ProfileParams, n)}
+#define PDB(n) {#n, T_BOOL, offsetof(ProfileParams, n)}
+const ParamDesc kRadial[] = {PDD(xcen), PDD(ycen), PDD(mag), PDD(ang), PDD(axrat), PDD(box), PDB(rough), PDB(adjust),
+                             PDB(force_cpu), PDD(acc), PDD(rscale_switch), PDD(rscale_max), PDU(max_recursions),
+                             PDU(resolution), PDB(convolve), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kSersic[] = {PDD(re), PDD(nser), PDB(rescale_flux), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kMoffat[] = {PDD(fwhm), PDD(con), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kFerrer[] = {PDD(rout), PDD(a), PDD(b), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kCoreSersic[] = {PDD(re), PDD(rb), PDD(nser), PDD(a), PDD(b), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kKing[] = {PDD(rc), PDD(rt), PDD(a), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kBrokenExp[] = {PDD(h1), PDD(h2), PDD(rb), PDD(a), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kSky[] = {PDD(bg), PDB(convolve), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kPsf[] = {PDD(xcen), PDD(ycen), PDD(mag), PDB(convolve), {nullptr, T_DOUBLE, 0}};
+const ParamDesc kNull[] = {PDB(convolve), {nullptr, T_DOUBLE, 0}};
+
+const char *kind_name(int k)
+{
+	static const char *names[] = {"sersic", "moffat", "ferrer", "coresersic", "king", "brokenexp", "sky", "psf", "null"};
+	return (k >= 0 && k <= 8) ? names[k] : "?";
+}
+
+const ParamDesc *find_param(int kind, const char *name)
+{
+	const ParamDesc *lists[2] = {nullptr, nullptr};
+	switch (kind) {
+	case PK_SERSIC: lists[0] = kRadial; lists[1] = kSersic; break;
+	case PK_MOFFAT: lists[0] = kRadial; lists[1] = kMoffat; break;
+	case PK_FERRER: lists[0] = kRadial; lists[1] = kFerrer; break;
+	case PK_CORESERSIC: lists[0] = kRadial; lists[1] = kCoreSersic; break;
+	case PK_KING: lists[0] = kRadial; lists[1] = kKing; break;
+	case PK_BROKENEXP: lists[0] = kRadial; lists[1] = kBrokenExp; break;
+	case PK_SKY: lists[0] = kSky; break;
+	case PK_PSF: lists[0] = kPsf; break;
+	default: lists[0] = kNull; break;
+	}
+	for (auto *l : lists) {
+		if (!l) continue;
+		for (const ParamDesc *d = l; d->name; d++)
+			if (std::strcmp(d->name, name) == 0) return d;
+	}
+	return nullptr;
+}
+
+ProfileParams default_params(int kind)
+{
+	ProfileParams p;
+	std::memset(&p, 0, sizeof(p));
+	p.kind = kind;
+	// radial.cpp:724-752
+	p.mag = 15;
+	p.axrat = 1;
+	p.acc = 0.1;
+	p.rscale_switch = 1;
+	p.resolution = 9;
+	p.max_recursions = 2;
+	p.adjust = 1;
+	switch (kind) {
+	case PK_SERSIC: p.re = 1; p.nser = 1; break;                              // sersic.cpp:350-359
+	case PK_MOFFAT: p.fwhm = 3; p.con = 2; break;                             // moffat.cpp:102-108
+	case PK_FERRER: p.rout = 3; p.a = 1; p.b = 1; p.acc = 1; break;           // ferrer.cpp:115-126
+	case PK_CORESERSIC: p.re = 1; p.rb = 1; p.nser = 4; p.a = 1; p.b = 1; break;  // coresersic.cpp:131-140
+	case PK_KING: p.rc = 1; p.rt = 3; p.a = 2; break;                         // king.cpp:111-119
+	case PK_BROKENEXP: p.h1 = 1; p.h2 = 1; p.rb = 1; p.a = 1; break;          // brokenexponential.cpp:141-150
+	case PK_PSF: p.mag = 0; break;                                            // psf.cpp:147-156
+	default: break;
+	}
+	return p;
+}
+
+int kind_from_name(const char *name)
+{
+	// model.cpp:103-135
+	if (!std::strcmp(name, "null")) return PK_NULL;
+	if (!std::strcmp(name, "sky")) return PK_SKY;
+	if (!std::strcmp(name, "sersic")) return PK_SERSIC;
+	if (!std::strcmp(name, "moffat")) return PK_MOFFAT;
+	if (!std::strcmp(name, "ferrer") || !std::strcmp(name, "ferrers")) return PK_FERRER;
+	if (!std::strcmp(name, "coresersic")) return PK_CORESERSIC;
+	if (!std::strcmp(name, "king")) return PK_KING;
+	if (!std::strcmp(name, "brokenexp")) return PK_BROKENEXP;
+	if (!std::strcmp(name, "psf")) return PK_PSF;
+	return -1;
+}
+
+enum ConvKind { CONV_BRUTE = 0, CONV_FFT = 1, CONV_NULL = 2 };
+
+struct Analysis {
+	bool conv;
+	unsigned padx, pady, dw, dh;  // drawing dims
+	unsigned cw, ch;              // cropped dims (finesampled)
+	unsigned ow, oh;              // output dims
+	int levels;
+	int n_profiles;
+};
+
+// Per-evaluation device results: [0] logL, [1..] tangent reductions.
+struct ResultLayout {
+	static constexpr int LL = 0;
+	static constexpr int T0 = 8;
+};
+
+}  // namespace
+
+struct pf_model {
+	unsigned width, height;
+	std::vector<ProfileParams> profiles;
+	std::vector<double> psf;  // normalised
+	unsigned psf_w = 0, psf_h = 0;
+	bool psf_dirty = true;
+	double magzero = 0, sx = 1, sy = 1, psf_sx = 1, psf_sy = 1;
+	unsigned fs = 1;
+	bool return_fine = true, crop = true, debug = false;
+	int conv_kind = CONV_BRUTE;
+	int precision = PF_FP64;
+	int device = 0;
+	cudaStream_t stream = nullptr;
+	cudaEvent_t ev[5] = {};
+	float timings[4] = {0, 0, 0, 0};
+
+	// device buffers
+	DevBuf d_prof, d_fprof, d_prof_begin, d_prof_batch;
+	DevBuf d_conv64, d_plain64, d_model64;
+	DevBuf d_conv32, d_plain32, d_model32, d_jac, d_gconv, d_gplain, d_wseed;
+	DevBuf d_psf64, d_psfrev64, d_psf32, d_psfrev32;
+	DevBuf d_items, d_ctrl, d_partials, d_results;
+	DevBuf d_decisions, d_level_counts;
+	DevBuf d_data, d_sigma, d_region;
+	HostBuf h_prof, h_fprof, h_results, h_ctrl;
+	std::vector<uint32_t> caps;
+	bool has_data = false, has_region = false;
+	unsigned data_w = 0, data_h = 0;
+
+	// debug output of the last evaluation
+	std::vector<int32_t> decisions;
+	std::vector<unsigned long long> level_counts;
+	unsigned dec_npix = 0;
+	int dec_levels = 0;
+};
+
+namespace {
+
+constexpr int NPARTS = 296;  // likelihood partial sums (2 per SM)
+constexpr size_t CTRL_WORDS = 64;  // counts[16], overflow, ...
+
+int analyze(pf_model *m, Analysis &a)
+{
+	if (m->width == 0 || m->height == 0) return set_error(PF_E_INVALID, "Model's requested dimensions are 0");
+	if (m->sx <= 0) return set_error(PF_E_INVALID, "Model's scale_x cannot be negative or zero");
+	if (m->sy <= 0) return set_error(PF_E_INVALID, "Model's scale_y cannot be negative or zero");
+	if (m->profiles.empty()) return set_error(PF_E_INVALID, "No profiles provided in the model");
+	a.conv = false;
+	for (auto &p : m->profiles)
+		if (p.convolve) a.conv = true;
+	if (a.conv && m->psf.empty()) return set_error(PF_E_INVALID, "No psf provided but profile(s) requested convolution");
+	a.levels = 1;
+	for (auto &p : m->profiles) {
+		const char *err = validate_profile(p, !m->psf.empty());
+		if (err) return set_error(PF_E_INVALID, err);
+		if (is_radial_kind(p.kind)) {
+			// With adjust the resolution is derived in [4, 16] (radial.cpp:169-172);
+			// otherwise the user's value is used as is.
+			if (!p.adjust && !p.rough && (p.resolution == 0 || p.resolution > 16))
+				return set_error(PF_E_INVALID, "resolution must be in [1, 16] when adjust is false");
+			unsigned mr = p.max_recursions;
+			if (p.kind == PK_SERSIC && p.adjust && p.nser > 1) mr = std::max(mr, 10u);
+			if (mr + 1 > (unsigned)MAX_LEVELS)
+				return set_error(PF_E_INVALID, "max_recursions above 15 is not supported");
+			a.levels = std::max(a.levels, (int)mr + 1);
+		}
+	}
+	if (m->profiles.size() > 65535) return set_error(PF_E_INVALID, "too many profiles");
+	a.padx = a.conv ? m->psf_w / 2 : 0;
+	a.pady = a.conv ? m->psf_h / 2 : 0;
+	a.cw = m->width * m->fs;
+	a.ch = m->height * m->fs;
+	a.dw = a.cw + 2 * a.padx;
+	a.dh = a.ch + 2 * a.pady;
+	if ((size_t)a.dw * a.dh >= (1ull << 31)) return set_error(PF_E_INVALID, "image too large");
+	if (m->fs > 1 && !m->return_fine) {
+		a.ow = (a.cw + m->fs - 1) / m->fs;
+		a.oh = (a.ch + m->fs - 1) / m->fs;
+	}
+	else {
+		a.ow = a.cw;
+		a.oh = a.ch;
+	}
+	a.n_profiles = (int)m->profiles.size();
+	return PF_OK;
+}
+
+ModelGeom geometry(const pf_model *m, const Analysis &a)
+{
+	ModelGeom g;
+	g.magzero = m->magzero;
+	g.sx = m->sx / m->fs;
+	g.sy = m->sy / m->fs;
+	g.img_sx = m->sx;
+	g.img_sy = m->sy;
+	g.offx = a.padx;
+	g.offy = a.pady;
+	g.finesampling = m->fs;
+	return g;
+}
+
+FProfile to_fprofile(const DevProfile &d, const ProfileParams &p)
+{
+	FProfile f;
+	std::memset(&f, 0, sizeof(f));
+	f.kind = d.kind;
+	f.target = d.target;
+	f.rough = d.rough;
+	f.centre_override = d.centre_override;
+	f.resolution = d.resolution;
+	f.max_rec = d.max_rec;
+	f.cos_ang = (float)d.cos_ang;
+	f.sin_ang = (float)d.sin_ang;
+	f.cos_q = (float)d.cos_q;
+	f.sin_q = (float)d.sin_q;
+	f.r_switch = (float)d.r_switch;
+	f.r_max = (float)d.r_max;
+	f.acc = (float)d.acc;
+	f.re = (float)d.re;
+	f.nser = (float)d.nser;
+	f.bn = (float)d.bn;
+	f.B = (float)(p.box + 2);
+	f.inv_nB = (float)(1.0 / (p.nser * (p.box + 2)));
+	f.dbn_dn = (float)d.dbn_dn;
+	f.rscale = (float)d.rscale;
+	f.con = (float)d.con;
+	f.a = (float)d.a;
+	f.b = (float)d.b;
+	f.rb = (float)d.rb;
+	f.rc = (float)d.rc;
+	f.rt = (float)d.rt;
+	f.h1 = (float)d.h1;
+	f.h2 = (float)d.h2;
+	f.king_t = (float)d.king_t;
+	f.flux_scale = (float)d.flux_scale;
+	f.flux_scale64 = d.flux_scale;
+	f.cx = d.cx;
+	f.cy = d.cy;
+	f.img_sx = d.img_sx;
+	f.img_sy = d.img_sy;
+	if (d.kind == PK_SKY) f.flux_scale = (float)d.bg;
+	if (d.kind == PK_MOFFAT) {
+		double c = p.con, t = std::pow(2.0, 1.0 / c);
+		f.a = (float)(1.0 / p.fwhm);
+		f.b = (float)(0.5 * t * std::log(2.0) / (c * c * (t - 1.0)));
+	}
+	return f;
+}
+
+int upload_psf(pf_model *m)
+{
+	if (!m->psf_dirty) return PF_OK;
+	size_t n = m->psf.size();
+	if (n == 0) {
+		m->psf_dirty = false;
+		return PF_OK;
+	}
+	std::vector<double> rev(m->psf.rbegin(), m->psf.rend());
+	std::vector<float> f32(m->psf.begin(), m->psf.end()), r32(rev.begin(), rev.end());
+	PF_CUDA(ensure(m->d_psf64, n * 8));
+	PF_CUDA(ensure(m->d_psfrev64, n * 8));
+	PF_CUDA(ensure(m->d_psf32, n * 4));
+	PF_CUDA(ensure(m->d_psfrev32, n * 4));
+	PF_CUDA(cudaMemcpy(m->d_psf64.p, m->psf.data(), n * 8, cudaMemcpyHostToDevice));
+	PF_CUDA(cudaMemcpy(m->d_psfrev64.p, rev.data(), n * 8, cudaMemcpyHostToDevice));
+	PF_CUDA(cudaMemcpy(m->d_psf32.p, f32.data(), n * 4, cudaMemcpyHostToDevice));
+	PF_CUDA(cudaMemcpy(m->d_psfrev32.p, r32.data(), n * 4, cudaMemcpyHostToDevice));
+	m->psf_dirty = false;
+	return PF_OK;
+}
+
+// Queue segments per level; capacities start from a pixel-count estimate and
+// grow after an overflow.
+int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q, int32_t *decisions,
+                  unsigned long long *level_counts)
+{
+	if (m->caps.size() != (size_t)MAX_LEVELS) {
+		m->caps.assign(MAX_LEVELS, 0);
+	}
+	uint32_t base0 = (uint32_t)std::min<size_t>(std::max<size_t>(npix_total / 4, 4096), 1u << 24);
+	for (int l = 0; l < MAX_LEVELS; l++) {
+		uint32_t want = l == 0 ? base0 : (l < 3 ? base0 / 2 : 4096);
+		if (m->caps[l] < want) m->caps[l] = want;
+	}
+	size_t total = 0;
+	for (int l = 0; l < a.levels; l++) {
+		q.off[l] = (uint32_t)total;
+		q.cap[l] = m->caps[l];
+		total += m->caps[l];
+	}
+	for (int l = a.levels; l < MAX_LEVELS; l++) {
+		q.off[l] = 0;
+		q.cap[l] = 0;
+	}
+	if (total >= (1ull << 32)) return set_error(PF_E_CAPACITY, "subsampling work queue exceeds 2^32 items");
+	PF_CUDA(ensure(m->d_items, total * sizeof(SubItem)));
+	PF_CUDA(ensure(m->d_ctrl, CTRL_WORDS * 4));
+	q.items = m->d_items.as<SubItem>();
+	q.counts = m->d_ctrl.as<uint32_t>();
+	q.overflow = m->d_ctrl.as<uint32_t>() + MAX_LEVELS;
+	q.levels = (uint32_t)a.levels;
+	q.decisions = decisions;
+	q.level_counts = level_counts;
+	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, m->stream));
+	return PF_OK;
+}
+
+// Reads counts back (after the stream is synchronised) and grows the
+// capacities of overflowing levels.  Returns 1 if a retry is needed.
+int check_overflow(pf_model *m, const Analysis &a, const uint32_t *ctrl, int &retry)
+{
+	retry = 0;
+	for (int l = 0; l < a.levels; l++) {
+		if (ctrl[l] > m->caps[l]) {
+			uint64_t want = (uint64_t)ctrl[l] + ctrl[l] / 2 + 1024;
+			if (want > (1ull << 30)) return set_error(PF_E_CAPACITY, "subsampling work queue overflow");
+			m->caps[l] = (uint32_t)want;
+			retry = 1;
+		}
+	}
+	if (ctrl[MAX_LEVELS] & 2u) return set_error(PF_E_CAPACITY, "recursion deeper than the configured levels");
+	return PF_OK;
+}
+
+int ensure_stream(pf_model *m)
+{
+	PF_CUDA(cudaSetDevice(m->device));
+	return PF_OK;
+}
+
+// Upload the derived profile scalars of one parameter set into slot `slot`
+// of the device profile array (FP64 form, plus FP32 form when asked).
+int derive_and_upload(pf_model *m, const Analysis &a, const std::vector<ProfileParams> &params, int slot,
+                      int n_slots, bool fp32)
+{
+	ModelGeom g = geometry(m, a);
+	size_t n = params.size();
+	PF_CUDA(ensure(m->h_prof, n * n_slots * sizeof(DevProfile)));
+	PF_CUDA(ensure(m->d_prof, n * n_slots * sizeof(DevProfile)));
+	DevProfile *hp = m->h_prof.as<DevProfile>() + n * slot;
+	for (size_t i = 0; i < n; i++) derive_profile(params[i], g, hp[i]);
+	PF_CUDA(cudaMemcpyAsync(m->d_prof.as<DevProfile>() + n * slot, hp, n * sizeof(DevProfile), cudaMemcpyHostToDevice,
+	                        m->stream));
+	if (fp32) {
+		PF_CUDA(ensure(m->h_fprof, n * n_slots * sizeof(FProfile)));
+		PF_CUDA(ensure(m->d_fprof, n * n_slots * sizeof(FProfile)));
+		FProfile *hf = m->h_fprof.as<FProfile>() + n * slot;
+		for (size_t i = 0; i < n; i++) hf[i] = to_fprofile(hp[i], params[i]);
+		PF_CUDA(cudaMemcpyAsync(m->d_fprof.as<FProfile>() + n * slot, hf, n * sizeof(FProfile),
+		                        cudaMemcpyHostToDevice, m->stream));
+	}
+	return PF_OK;
+}
+
+// FP64 model image into d_model64 (out dims), queue-overflow checked by caller.
+int run_plain64(pf_model *m, const Analysis &a, const DevProfile *dprof, QueueSet &q)
+{
+	size_t npix = (size_t)a.dw * a.dh;
+	PF_CUDA(ensure(m->d_conv64, npix * 8));
+	PF_CUDA(ensure(m->d_plain64, npix * 8));
+	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
+	double *conv = m->d_conv64.as<double>(), *plain = m->d_plain64.as<double>();
+	PF_CUDA(launch_pixels64(dprof, a.n_profiles, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain, q, m->stream));
+	for (int p = 0; p < a.n_profiles; p++) {
+		if (m->profiles[p].kind == PK_PSF) {
+			PF_CUDA(launch_psf_stamp64(dprof, p, m->d_psf64.as<double>(), m->psf_w, m->psf_h, m->psf_sx, m->psf_sy,
+			                           m->sx / m->fs, m->sy / m->fs, a.padx, a.pady, a.dw, a.dh, conv, plain,
+			                           m->stream));
+		}
+	}
+	PF_CUDA(launch_levels64(dprof, a.levels, conv, plain, q, m->stream));
+	if (q.decisions) PF_CUDA(launch_count_decisions(q, a.levels, npix, m->stream));
+	PF_CUDA(cudaEventRecord(m->ev[1], m->stream));
+
+	double *model = m->d_model64.as<double>();
+	if (a.conv && m->conv_kind != CONV_NULL) {
+		PF_CUDA(launch_conv64(conv, a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w, m->psf_h, model, a.cw,
+		                      a.ch, plain, a.dw, a.padx, a.pady, m->stream));
+	}
+	else {
+		PF_CUDA(launch_crop64(conv, a.dw, a.padx, a.pady, model, a.cw, a.ch, plain, m->stream));
+	}
+	if (a.ow != a.cw || a.oh != a.ch) {
+		// finesampled output summed down (model.cpp:326-329); reuse conv as scratch
+		PF_CUDA(cudaMemcpyAsync(conv, model, (size_t)a.cw * a.ch * 8, cudaMemcpyDeviceToDevice, m->stream));
+		PF_CUDA(launch_downsample64(conv, a.cw, a.ch, m->fs, model, a.ow, a.oh, m->stream));
+	}
+	PF_CUDA(cudaEventRecord(m->ev[2], m->stream));
+	return PF_OK;
+}
+
+int fetch_debug(pf_model *m, const Analysis &a)
+{
+	size_t npix = (size_t)a.dw * a.dh;
+	m->decisions.resize(npix * a.n_profiles);
+	m->level_counts.resize((size_t)MAX_LEVELS * a.n_profiles);
+	PF_CUDA(cudaMemcpyAsync(m->decisions.data(), m->d_decisions.p, npix * a.n_profiles * 4, cudaMemcpyDeviceToHost,
+	                        m->stream));
+	PF_CUDA(cudaMemcpyAsync(m->level_counts.data(), m->d_level_counts.p, (size_t)MAX_LEVELS * a.n_profiles * 8,
+	                        cudaMemcpyDeviceToHost, m->stream));
+	PF_CUDA(cudaStreamSynchronize(m->stream));
+	m->dec_npix = (unsigned)npix;
+	m->dec_levels = a.levels;
+	return PF_OK;
+}
+
+// Full FP64 evaluation into d_model64 with retries on queue overflow.
+int evaluate64(pf_model *m, Analysis &a)
+{
+	PF_TRY(ensure_stream(m));
+	PF_TRY(analyze(m, a));
+	PF_TRY(upload_psf(m));
+	PF_CUDA(cudaEventRecord(m->ev[0], m->stream));
+	PF_TRY(derive_and_upload(m, a, m->profiles, 0, 1, false));
+	size_t npix = (size_t)a.dw * a.dh;
+	PF_CUDA(ensure(m->h_ctrl, CTRL_WORDS * 4));
+	for (int attempt = 0; attempt < 8; attempt++) {
+		int32_t *dec = nullptr;
+		unsigned long long *lc = nullptr;
+		if (m->debug) {
+			PF_CUDA(ensure(m->d_decisions, npix * a.n_profiles * 4));
+			PF_CUDA(ensure(m->d_level_counts, (size_t)MAX_LEVELS * a.n_profiles * 8));
+			PF_CUDA(cudaMemsetAsync(m->d_decisions.p, 0, npix * a.n_profiles * 4, m->stream));
+			PF_CUDA(cudaMemsetAsync(m->d_level_counts.p, 0, (size_t)MAX_LEVELS * a.n_profiles * 8, m->stream));
+			dec = m->d_decisions.as<int32_t>();
+			lc = m->d_level_counts.as<unsigned long long>();
+		}
+		QueueSet q;
+		PF_TRY(prepare_queue(m, a, npix * a.n_profiles, q, dec, lc));
+		PF_TRY(run_plain64(m, a, m->d_prof.as<DevProfile>(), q));
+		PF_CUDA(cudaMemcpyAsync(m->h_ctrl.p, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, m->stream));
+		PF_CUDA(cudaStreamSynchronize(m->stream));
+		int retry = 0;
+		PF_TRY(check_overflow(m, a, m->h_ctrl.as<uint32_t>(), retry));
+		if (!retry) {
+			if (m->debug) PF_TRY(fetch_debug(m, a));
+			float t = 0;
+			cudaEventElapsedTime(&t, m->ev[0], m->ev[2]);
+			m->timings[0] = t;
+			cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
+			cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
+			return PF_OK;
+		}
+	}
+	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+}
+
+// ---------------------------------------------------------------------------
+// FP32 path with forward tangents and the adjoint reduction
+// ---------------------------------------------------------------------------
+
+int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q, bool want_grad, double *d_out)
+{
+	size_t npix = (size_t)a.dw * a.dh;
+	size_t nout = (size_t)a.ow * a.oh;
+	int nprof = a.n_profiles;
+	PF_CUDA(ensure(m->d_conv32, npix * 4));
+	PF_CUDA(ensure(m->d_plain32, npix * 4));
+	PF_CUDA(ensure(m->d_model32, (size_t)a.cw * a.ch * 4 + 4));
+	float *jac = nullptr;
+	if (want_grad) {
+		PF_CUDA(ensure(m->d_jac, npix * NTAN * nprof * 4));
+		jac = m->d_jac.as<float>();
+	}
+	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *model = m->d_model32.as<float>();
+	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), 1, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain,
+	                        jac, q, m->stream));
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, m->stream));
+	PF_CUDA(cudaEventRecord(m->ev[1], m->stream));
+	if (a.conv && m->conv_kind != CONV_NULL) {
+		PF_CUDA(launch_conv32(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model, a.cw, a.ch,
+		                      plain, a.dw, a.padx, a.pady, 1, 0, 0, m->stream));
+	}
+	else {
+		PF_CUDA(launch_crop32(conv, a.dw, a.padx, a.pady, model, a.cw, a.ch, plain, 1, 0, m->stream));
+	}
+	PF_CUDA(cudaEventRecord(m->ev[2], m->stream));
+	if (!m->has_data) return PF_OK;
+	PF_CUDA(ensure(m->d_partials, NPARTS * sizeof(double2)));
+	float *wseed = nullptr;
+	if (want_grad) {
+		PF_CUDA(ensure(m->d_wseed, nout * 4));
+		wseed = m->d_wseed.as<float>();
+	}
+	PF_CUDA(launch_loglike32(model, m->d_data.as<double>(), m->d_sigma.as<double>(),
+	                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout, 1, 0,
+	                         m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
+	if (want_grad) {
+		PF_CUDA(ensure(m->d_gconv, npix * 4));
+		PF_CUDA(ensure(m->d_gplain, npix * 4));
+		float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>();
+		PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, 1, gplain, m->stream));
+		if (a.conv && m->conv_kind != CONV_NULL) {
+			PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(),
+			                      m->psf_w, m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, 1, 0, 0, m->stream));
+		}
+		else {
+			gconv = gplain;
+		}
+		PF_CUDA(cudaMemsetAsync(d_out + ResultLayout::T0, 0, (size_t)nprof * NTAN * 8, m->stream));
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix,
+		                          d_out + ResultLayout::T0, m->stream));
+	}
+	PF_CUDA(cudaEventRecord(m->ev[3], m->stream));
+	return PF_OK;
+}
+
+int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *results)
+{
+	PF_TRY(ensure_stream(m));
+	PF_TRY(analyze(m, a));
+	if (m->fs != 1) return set_error(PF_E_INVALID, "the FP32 path does not support finesampling yet");
+	for (auto &p : m->profiles)
+		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
+	if (m->has_data && (m->data_w != a.ow || m->data_h != a.oh))
+		return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
+	PF_TRY(upload_psf(m));
+	PF_CUDA(cudaEventRecord(m->ev[0], m->stream));
+	PF_TRY(derive_and_upload(m, a, m->profiles, 0, 1, true));
+	int nprof = a.n_profiles;
+	{
+		std::vector<int> begin = {0, nprof};
+		std::vector<int> batch(nprof, 0);
+		PF_CUDA(ensure(m->d_prof_begin, 2 * 4));
+		PF_CUDA(ensure(m->d_prof_batch, nprof * 4));
+		PF_CUDA(cudaMemcpyAsync(m->d_prof_begin.p, begin.data(), 8, cudaMemcpyHostToDevice, m->stream));
+		PF_CUDA(cudaMemcpyAsync(m->d_prof_batch.p, batch.data(), nprof * 4, cudaMemcpyHostToDevice, m->stream));
+	}
+	size_t nres = ResultLayout::T0 + (size_t)nprof * NTAN;
+	PF_CUDA(ensure(m->d_results, nres * 8));
+	PF_CUDA(ensure(m->h_results, nres * 8 + CTRL_WORDS * 4));
+	size_t npix = (size_t)a.dw * a.dh;
+	for (int attempt = 0; attempt < 8; attempt++) {
+		QueueSet q;
+		PF_TRY(prepare_queue(m, a, npix * nprof, q, nullptr, nullptr));
+		PF_TRY(run_fp32(m, a, m->d_fprof.as<FProfile>(), q, want_grad, m->d_results.as<double>()));
+		char *hr = m->h_results.as<char>();
+		PF_CUDA(cudaMemcpyAsync(hr, m->d_results.p, nres * 8, cudaMemcpyDeviceToHost, m->stream));
+		PF_CUDA(cudaMemcpyAsync(hr + nres * 8, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, m->stream));
+		PF_CUDA(cudaStreamSynchronize(m->stream));
+		int retry = 0;
+		PF_TRY(check_overflow(m, a, reinterpret_cast<uint32_t *>(hr + nres * 8), retry));
+		if (!retry) {
+			if (results) results->assign(reinterpret_cast<double *>(hr), reinterpret_cast<double *>(hr) + nres);
+			cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
+			cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
+			if (m->has_data) {
+				cudaEventElapsedTime(&m->timings[3], m->ev[2], m->ev[3]);
+				cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[3]);
+			}
+			else {
+				cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[2]);
+			}
+			return PF_OK;
+		}
+	}
+	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+}
+
+// d logL / d parameter from the tangent reductions T[0..8] of one profile.
+int combine_gradient(const ProfileParams &p, const DevProfile &d, const double *T, const char *name, double &g)
+{
+	const double F = d.flux_scale, q = p.axrat, c = d.cos_ang, s = d.sin_ang;
+	const double deg = M_PI / 180.0;
+	if (!is_radial_kind(p.kind))
+		return set_error(PF_E_INVALID, std::string("no gradient for parameters of ") + kind_name(p.kind) + " profiles");
+	if (p.kind != PK_SERSIC && p.kind != PK_MOFFAT)
+		return set_error(PF_E_INVALID, std::string("gradients of ") + kind_name(p.kind) + " profiles are not available yet");
+	if (p.kind == PK_SERSIC && p.rescale_flux)
+		return set_error(PF_E_INVALID, "gradients with rescale_flux are not available");
+	if (!std::strcmp(name, "xcen")) g = F * (-c * T[1] + (s / q) * T[2]);
+	else if (!std::strcmp(name, "ycen")) g = F * (-s * T[1] - (c / q) * T[2]);
+	else if (!std::strcmp(name, "mag")) g = F * d.dlnI_dmag * T[0];
+	else if (!std::strcmp(name, "ang")) g = F * deg * (q * T[3] - T[4] / q);
+	else if (!std::strcmp(name, "axrat")) g = F * (-T[5] / q + d.dlnI_dq * T[0]);
+	else if (!std::strcmp(name, "box")) g = F * (T[8] + d.dlnI_dbox * T[0]);
+	else if ((p.kind == PK_SERSIC && !std::strcmp(name, "re")) || (p.kind == PK_MOFFAT && !std::strcmp(name, "fwhm")))
+		g = F * (T[6] + d.dlnI_dp1 * T[0]);
+	else if ((p.kind == PK_SERSIC && !std::strcmp(name, "nser")) || (p.kind == PK_MOFFAT && !std::strcmp(name, "con")))
+		g = F * (T[7] + d.dlnI_dp2 * T[0]);
+	else
+		return set_error(PF_E_INVALID, std::string("no gradient with respect to ") + name);
+	return PF_OK;
+}
+
+int check_profile(pf_model *m, int index)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (index < 0 || index >= (int)m->profiles.size()) return set_error(PF_E_INVALID, "profile index out of range");
+	return PF_OK;
+}
+
+int set_param(pf_model *m, int index, const char *name, PType type, double dv, unsigned uv, int bv)
+{
+	PF_TRY(check_profile(m, index));
+	ProfileParams &p = m->profiles[index];
+	const ParamDesc *d = find_param(p.kind, name);
+	if (!d || d->type != type) {
+		const char *tn = type == T_DOUBLE ? "double" : type == T_UINT ? "unsigned int" : "bool";
+		return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown ") + tn + " parameter in profile " +
+		                                         kind_name(p.kind) + ": " + name);
+	}
+	char *base = reinterpret_cast<char *>(&p) + d->off;
+	if (type == T_DOUBLE) *reinterpret_cast<double *>(base) = dv;
+	else if (type == T_UINT) *reinterpret_cast<uint32_t *>(base) = uv;
+	else *reinterpret_cast<int32_t *>(base) = bv != 0;
+	return PF_OK;
+}
+
+std::string trim(const std::string &s)
+{
+	size_t b = s.find_first_not_of(" \t\n"), e = s.find_last_not_of(" \t\n");
+	return b == std::string::npos ? std::string() : s.substr(b, e - b + 1);
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char *pf_last_error(void) { return g_error.c_str(); }
+
+const char *pf_version(void) { return "profit_b200 0.1 (libprofit 1.9.3 API)"; }
+
+int pf_model_create(unsigned width, unsigned height, pf_model **out)
+{
+	if (!out) return set_error(PF_E_INVALID, "null output pointer");
+	int dev = 0;
+	PF_CUDA(cudaGetDevice(&dev));
+	cudaDeviceProp prop;
+	PF_CUDA(cudaGetDeviceProperties(&prop, dev));
+	if (prop.major != 10)
+		return set_error(PF_E_CUDA, std::string("profit_b200 needs an sm_100 (B200) device, found ") + prop.name);
+	pf_model *m = new pf_model();
+	m->width = width;
+	m->height = height;
+	m->device = dev;
+	cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+	for (int i = 0; i < 5 && e == cudaSuccess; i++) e = cudaEventCreate(&m->ev[i]);
+	if (e != cudaSuccess) {
+		delete m;
+		return set_error(PF_E_CUDA, std::string("stream/event creation: ") + cudaGetErrorString(e));
+	}
+	*out = m;
+	return PF_OK;
+}
+
+int pf_model_destroy(pf_model *m)
+{
+	if (!m) return PF_OK;
+	cudaSetDevice(m->device);
+	if (m->stream) cudaStreamSynchronize(m->stream);
+	for (auto &e : m->ev)
+		if (e) cudaEventDestroy(e);
+	if (m->stream) cudaStreamDestroy(m->stream);
+	delete m;
+	return PF_OK;
+}
+
+int pf_model_add_profile(pf_model *m, const char *name, int *index)
+{
+	if (!m || !name) return set_error(PF_E_INVALID, "null argument");
+	int k = kind_from_name(name);
+	if (k < 0) return set_error(PF_E_INVALID, std::string("Unknown profile name: ") + name);
+	m->profiles.push_back(default_params(k));
+	if (index) *index = (int)m->profiles.size() - 1;
+	return PF_OK;
+}
+
+int pf_profile_set_double(pf_model *m, int index, const char *name, double value)
+{
+	return set_param(m, index, name, T_DOUBLE, value, 0, 0);
+}
+
+int pf_profile_set_uint(pf_model *m, int index, const char *name, unsigned value)
+{
+	return set_param(m, index, name, T_UINT, 0, value, 0);
+}
+
+int pf_profile_set_bool(pf_model *m, int index, const char *name, int value)
+{
+	return set_param(m, index, name, T_BOOL, 0, 0, value);
+}
+
+int pf_profile_set(pf_model *m, int index, const char *spec)
+{
+	PF_TRY(check_profile(m, index));
+	std::string s(spec ? spec : "");
+	size_t eq = s.find('=');
+	if (eq == std::string::npos || s.find('=', eq + 1) != std::string::npos)
+		return set_error(PF_E_INVALID, "missing = in parameter: " + s);
+	std::string name = trim(s.substr(0, eq)), val = trim(s.substr(eq + 1));
+	const ParamDesc *d = find_param(m->profiles[index].kind, name.c_str());
+	if (!d)
+		return set_error(PF_E_UNKNOWN_PARAM, std::string("Profile ") + kind_name(m->profiles[index].kind) +
+		                                         " doesn't support parameter " + name +
+		                                         ", or parameter has invalid value: " + val);
+	char *end = nullptr;
+	if (d->type == T_DOUBLE) {
+		double v = std::strtod(val.c_str(), &end);
+		if (end == val.c_str()) return set_error(PF_E_INVALID, "Parameter " + name + " cannot be parsed as double: " + val);
+		return set_param(m, index, name.c_str(), T_DOUBLE, v, 0, 0);
+	}
+	unsigned long v = std::strtoul(val.c_str(), &end, 10);
+	if (end == val.c_str()) return set_error(PF_E_INVALID, "Parameter " + name + " cannot be parsed: " + val);
+	return set_param(m, index, name.c_str(), d->type, 0, (unsigned)v, (int)v);
+}
+
+int pf_profile_get_double(pf_model *m, int index, const char *name, double *value)
+{
+	PF_TRY(check_profile(m, index));
+	const ParamDesc *d = find_param(m->profiles[index].kind, name);
+	if (!d || d->type != T_DOUBLE)
+		return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown double parameter: ") + name);
+	*value = *reinterpret_cast<const double *>(reinterpret_cast<const char *>(&m->profiles[index]) + d->off);
+	return PF_OK;
+}
+
+int pf_model_profile_count(pf_model *m, int *count)
+{
+	if (!m || !count) return set_error(PF_E_INVALID, "null argument");
+	*count = (int)m->profiles.size();
+	return PF_OK;
+}
+
+int pf_model_clear_profiles(pf_model *m)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->profiles.clear();
+	return PF_OK;
+}
+
+int pf_model_set_psf(pf_model *m, const double *psf, unsigned width, unsigned height)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (!psf || width == 0 || height == 0) {
+		m->psf.clear();
+		m->psf_w = m->psf_h = 0;
+		m->psf_dirty = true;
+		return PF_OK;
+	}
+	size_t n = (size_t)width * height;
+	m->psf.assign(psf, psf + n);
+	// Image::normalize (image.cpp:231-237): divide by the sum when positive
+	double sum = 0;
+	for (double v : m->psf) sum += v;
+	if (sum > 0)
+		for (double &v : m->psf) v /= sum;
+	m->psf_w = width;
+	m->psf_h = height;
+	m->psf_dirty = true;
+	return PF_OK;
+}
+
+int pf_model_set_magzero(pf_model *m, double magzero)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->magzero = magzero;
+	return PF_OK;
+}
+
+int pf_model_set_image_pixel_scale(pf_model *m, double sx, double sy)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->sx = sx;
+	m->sy = sy;
+	return PF_OK;
+}
+
+int pf_model_set_psf_pixel_scale(pf_model *m, double sx, double sy)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->psf_sx = sx;
+	m->psf_sy = sy;
+	return PF_OK;
+}
+
+int pf_model_set_finesampling(pf_model *m, unsigned fs)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (fs == 0) return set_error(PF_E_INVALID, "finesampling must be > 0");
+	m->fs = fs;
+	return PF_OK;
+}
+
+int pf_model_set_return_finesampled(pf_model *m, int value)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->return_fine = value != 0;
+	return PF_OK;
+}
+
+int pf_model_set_crop(pf_model *m, int value)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (!value) return set_error(PF_E_INVALID, "crop = false is not supported");
+	m->crop = true;
+	return PF_OK;
+}
+
+int pf_model_set_convolver(pf_model *m, const char *type)
+{
+	if (!m || !type) return set_error(PF_E_INVALID, "null argument");
+	if (!std::strcmp(type, "brute") || !std::strcmp(type, "brute-old")) m->conv_kind = CONV_BRUTE;
+	else if (!std::strcmp(type, "fft")) m->conv_kind = CONV_FFT;
+	else if (!std::strcmp(type, "null")) m->conv_kind = CONV_NULL;
+	else return set_error(PF_E_INVALID, std::string("Unknown convolver type: ") + type);
+	return PF_OK;
+}
+
+int pf_model_set_precision(pf_model *m, int precision)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (precision != PF_FP64 && precision != PF_FP32) return set_error(PF_E_INVALID, "unknown precision");
+	m->precision = precision;
+	return PF_OK;
+}
+
+int pf_model_drawing_dims(pf_model *m, unsigned *w, unsigned *h)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	Analysis a;
+	PF_TRY(analyze(m, a));
+	if (w) *w = a.dw;
+	if (h) *h = a.dh;
+	return PF_OK;
+}
+
+int pf_model_evaluate(pf_model *m, double *image, size_t capacity, unsigned *out_w, unsigned *out_h, int *offset_x,
+                      int *offset_y)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	Analysis a;
+	if (m->precision == PF_FP64) {
+		PF_TRY(evaluate64(m, a));
+		size_t n = (size_t)a.ow * a.oh;
+		if (image) {
+			if (capacity < n) return set_error(PF_E_BUFFER, "output buffer too small");
+			PF_CUDA(cudaMemcpy(image, m->d_model64.p, n * 8, cudaMemcpyDeviceToHost));
+		}
+	}
+	else {
+		PF_TRY(evaluate32(m, a, false, nullptr));
+		size_t n = (size_t)a.ow * a.oh;
+		if (image) {
+			if (capacity < n) return set_error(PF_E_BUFFER, "output buffer too small");
+			std::vector<float> tmp(n);
+			PF_CUDA(cudaMemcpy(tmp.data(), m->d_model32.p, n * 4, cudaMemcpyDeviceToHost));
+			for (size_t i = 0; i < n; i++) image[i] = tmp[i];
+		}
+	}
+	if (out_w) *out_w = a.ow;
+	if (out_h) *out_h = a.oh;
+	if (offset_x) *offset_x = 0;
+	if (offset_y) *offset_y = 0;
+	return PF_OK;
+}
+
+int pf_model_set_data(pf_model *m, const double *image, const double *sigma, const uint8_t *region, unsigned width,
+                      unsigned height)
+{
+	if (!m || !image || !sigma) return set_error(PF_E_INVALID, "null argument");
+	PF_TRY(ensure_stream(m));
+	size_t n = (size_t)width * height;
+	PF_CUDA(ensure(m->d_data, n * 8));
+	PF_CUDA(ensure(m->d_sigma, n * 8));
+	PF_CUDA(cudaMemcpy(m->d_data.p, image, n * 8, cudaMemcpyHostToDevice));
+	PF_CUDA(cudaMemcpy(m->d_sigma.p, sigma, n * 8, cudaMemcpyHostToDevice));
+	m->has_region = region != nullptr;
+	if (region) {
+		PF_CUDA(ensure(m->d_region, n));
+		PF_CUDA(cudaMemcpy(m->d_region.p, region, n, cudaMemcpyHostToDevice));
+	}
+	m->data_w = width;
+	m->data_h = height;
+	m->has_data = true;
+	return PF_OK;
+}
+
+int pf_model_loglike(pf_model *m, double *loglike)
+{
+	if (!m || !loglike) return set_error(PF_E_INVALID, "null argument");
+	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
+	Analysis a;
+	if (m->precision == PF_FP64) {
+		PF_TRY(evaluate64(m, a));
+		if (m->data_w != a.ow || m->data_h != a.oh)
+			return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
+		PF_CUDA(ensure(m->d_partials, NPARTS * sizeof(double2)));
+		PF_CUDA(ensure(m->d_results, 64));
+		PF_CUDA(launch_loglike64(m->d_model64.as<double>(), m->d_data.as<double>(), m->d_sigma.as<double>(),
+		                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)(a.ow * a.oh),
+		                         m->d_partials.as<double2>(), NPARTS, m->d_results.as<double>(), m->stream));
+		PF_CUDA(cudaMemcpyAsync(loglike, m->d_results.p, 8, cudaMemcpyDeviceToHost, m->stream));
+		PF_CUDA(cudaStreamSynchronize(m->stream));
+		return PF_OK;
+	}
+	std::vector<double> res;
+	PF_TRY(evaluate32(m, a, false, &res));
+	*loglike = res[ResultLayout::LL];
+	return PF_OK;
+}
+
+int pf_model_loglike_grad(pf_model *m, const pf_param_ref *params, int n_params, double *loglike, double *grad)
+{
+	if (!m || (n_params > 0 && (!params || !grad))) return set_error(PF_E_INVALID, "null argument");
+	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
+	for (int i = 0; i < n_params; i++) PF_TRY(check_profile(m, params[i].profile));
+	Analysis a;
+	std::vector<double> res;
+	PF_TRY(evaluate32(m, a, true, &res));
+	if (loglike) *loglike = res[ResultLayout::LL];
+	const DevProfile *hp = m->h_prof.as<DevProfile>();
+	for (int i = 0; i < n_params; i++) {
+		int pi = params[i].profile;
+		PF_TRY(combine_gradient(m->profiles[pi], hp[pi], &res[ResultLayout::T0 + (size_t)pi * NTAN], params[i].name,
+		                        grad[i]));
+	}
+	return PF_OK;
+}
+
+int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_params, double rel_step, double *loglike,
+                             double *grad)
+{
+	if (!m || (n_params > 0 && (!params || !grad))) return set_error(PF_E_INVALID, "null argument");
+	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
+	if (!(rel_step > 0)) return set_error(PF_E_INVALID, "rel_step must be positive");
+	PF_TRY(ensure_stream(m));
+	Analysis a;
+	PF_TRY(analyze(m, a));
+	if (m->data_w != a.ow || m->data_h != a.oh)
+		return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
+	PF_TRY(upload_psf(m));
+	const int n_eval = 2 * n_params + 1;
+	std::vector<double> steps(n_params);
+	// parameter sets: base, then (+h, -h) per parameter
+	std::vector<std::vector<ProfileParams>> sets(n_eval, m->profiles);
+	for (int i = 0; i < n_params; i++) {
+		PF_TRY(check_profile(m, params[i].profile));
+		const ParamDesc *d = find_param(m->profiles[params[i].profile].kind, params[i].name);
+		if (!d || d->type != T_DOUBLE)
+			return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown double parameter: ") + params[i].name);
+		double v = *reinterpret_cast<const double *>(reinterpret_cast<const char *>(&m->profiles[params[i].profile]) +
+		                                             d->off);
+		double h = rel_step * std::max(std::fabs(v), 1.0);
+		steps[i] = h;
+		for (int sgn = 0; sgn < 2; sgn++) {
+			auto &ps = sets[1 + 2 * i + sgn][params[i].profile];
+			*reinterpret_cast<double *>(reinterpret_cast<char *>(&ps) + d->off) = sgn == 0 ? v + h : v - h;
+			if (const char *err = validate_profile(ps, !m->psf.empty()))
+				return set_error(PF_E_INVALID, std::string("finite-difference step leaves the valid range: ") + err);
+		}
+	}
+	size_t npix = (size_t)a.dw * a.dh;
+	PF_CUDA(ensure(m->d_partials, NPARTS * sizeof(double2)));
+	PF_CUDA(ensure(m->d_results, (size_t)n_eval * 8));
+	PF_CUDA(ensure(m->h_results, (size_t)n_eval * 8 + CTRL_WORDS * 4 * n_eval));
+	for (int attempt = 0; attempt < 8; attempt++) {
+		PF_CUDA(cudaEventRecord(m->ev[0], m->stream));
+		for (int e = 0; e < n_eval; e++) PF_TRY(derive_and_upload(m, a, sets[e], e, n_eval, false));
+		uint32_t *hctrl = reinterpret_cast<uint32_t *>(m->h_results.as<char>() + (size_t)n_eval * 8);
+		for (int e = 0; e < n_eval; e++) {
+			QueueSet q;
+			PF_TRY(prepare_queue(m, a, npix * a.n_profiles, q, nullptr, nullptr));
+			PF_TRY(run_plain64(m, a, m->d_prof.as<DevProfile>() + (size_t)e * a.n_profiles, q));
+			PF_CUDA(launch_loglike64(m->d_model64.as<double>(), m->d_data.as<double>(), m->d_sigma.as<double>(),
+			                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)(a.ow * a.oh),
+			                         m->d_partials.as<double2>(), NPARTS, m->d_results.as<double>() + e, m->stream));
+			PF_CUDA(cudaMemcpyAsync(hctrl + (size_t)e * CTRL_WORDS, m->d_ctrl.p, CTRL_WORDS * 4,
+			                        cudaMemcpyDeviceToHost, m->stream));
+		}
+		PF_CUDA(cudaMemcpyAsync(m->h_results.p, m->d_results.p, (size_t)n_eval * 8, cudaMemcpyDeviceToHost,
+		                        m->stream));
+		PF_CUDA(cudaEventRecord(m->ev[3], m->stream));
+		PF_CUDA(cudaStreamSynchronize(m->stream));
+		int retry = 0;
+		for (int e = 0; e < n_eval; e++) {
+			int r = 0;
+			PF_TRY(check_overflow(m, a, hctrl + (size_t)e * CTRL_WORDS, r));
+			retry |= r;
+		}
+		if (retry) continue;
+		const double *ll = m->h_results.as<double>();
+		if (loglike) *loglike = ll[0];
+		for (int i = 0; i < n_params; i++) grad[i] = (ll[1 + 2 * i] - ll[2 + 2 * i]) / (2 * steps[i]);
+		cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[3]);
+		return PF_OK;
+	}
+	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+}
+
+int pf_model_set_debug(pf_model *m, int value)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->debug = value != 0;
+	return PF_OK;
+}
+
+int pf_model_decisions(pf_model *m, int profile, int32_t *out, size_t capacity)
+{
+	PF_TRY(check_profile(m, profile));
+	if (m->decisions.empty()) return set_error(PF_E_STATE, "no decisions recorded: enable debug and evaluate");
+	if (capacity < m->dec_npix) return set_error(PF_E_BUFFER, "output buffer too small");
+	std::memcpy(out, m->decisions.data() + (size_t)profile * m->dec_npix, (size_t)m->dec_npix * 4);
+	return PF_OK;
+}
+
+int pf_model_level_counts(pf_model *m, int profile, int64_t *out, int max_levels, int *n_levels)
+{
+	PF_TRY(check_profile(m, profile));
+	if (m->level_counts.empty()) return set_error(PF_E_STATE, "no counters recorded: enable debug and evaluate");
+	int n = 0;
+	for (int l = 0; l < MAX_LEVELS; l++) {
+		unsigned long long c = m->level_counts[(size_t)profile * MAX_LEVELS + l];
+		if (l < max_levels) out[l] = (int64_t)c;
+		if (c) n = l + 1;
+	}
+	if (n_levels) *n_levels = n;
+	return PF_OK;
+}
+
+int pf_model_last_timings(pf_model *m, float *ms, int n)
+{
+	if (!m || !ms) return set_error(PF_E_INVALID, "null argument");
+	for (int i = 0; i < n && i < 4; i++) ms[i] = m->timings[i];
+	return PF_OK;
+}
+
+}  // extern "C"

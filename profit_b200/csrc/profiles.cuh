@@ -1,0 +1,442 @@
+// Profile parameters, the per-profile scalar prologue and the FP64 profile
+// evaluators of the plain form.
+//
+// The FP64 evaluators keep libprofit's operation order (and Sersic's
+// pow-avoiding specialisations) so that, with sm_100a FP64 arithmetic
+// compiled without FMA contraction, the subsampling tests
+// |f(|x'|,|y'|+|dy'|) - f(x',y')| > acc * f(x',y') take the same branches as
+// the reference.  Sources: radial.cpp:46-199, radial.h:93-102,
+// sersic.cpp:78-347, moffat.cpp:52-100, ferrer.cpp:50-113,
+// coresersic.cpp:51-125, king.cpp:51-109, brokenexponential.cpp:38-139.
+#pragma once
+
+#include <cstdint>
+
+#include "specfun.cuh"
+
+namespace pf {
+
+enum ProfileKind : int32_t {
+	PK_SERSIC = 0,
+	PK_MOFFAT = 1,
+	PK_FERRER = 2,
+	PK_CORESERSIC = 3,
+	PK_KING = 4,
+	PK_BROKENEXP = 5,
+	PK_SKY = 6,
+	PK_PSF = 7,
+	PK_NULL = 8
+};
+
+PF_HD inline bool is_radial_kind(int k) { return k >= PK_SERSIC && k <= PK_BROKENEXP; }
+
+// Sersic r_factor forms of sersic.cpp:78-189
+enum SersicForm : int32_t { SF_GENERAL = 0, SF_HALF, SF_ONE, SF_TWO, SF_THREE, SF_FOUR, SF_EIGHT, SF_SIXTEEN };
+
+// User-facing parameters of one profile, with libprofit's defaults
+// (radial.cpp:724-752 and each profile's constructor).
+struct ProfileParams {
+	int32_t kind;
+	int32_t convolve, rough, adjust, force_cpu, rescale_flux;
+	uint32_t resolution, max_recursions;
+	double xcen, ycen, mag, ang, axrat, box;
+	double acc, rscale_switch, rscale_max;
+	double re, nser, fwhm, con, rout, a, b, rb, rc, rt, h1, h2, bg;
+};
+
+// Everything a pixel kernel needs for one profile.
+struct DevProfile {
+	int32_t kind, form, boxy, rough;
+	int32_t target;          // 0: image to convolve, 1: unconvolved image
+	int32_t centre_override; // Sersic nser > 1 with adjust (sersic.cpp:339-345)
+	uint32_t resolution, max_rec;
+	double cx, cy;                     // centre in drawing-pixel coordinates
+	double cos_ang, sin_ang, cos_q, sin_q;
+	double rscale, r_switch, r_max;    // r_switch = rscale_switch*rscale, r_max = rscale_max*rscale (0 = none)
+	double acc, flux_scale, bn;
+	double re, nser, box, invexp;
+	double con, a, b, rb, rc, rt, h1, h2, king_t;
+	double img_sx, img_sy;             // image pixel scale (centre-pixel test)
+	double bg;                         // sky value per drawing pixel
+	double psf_flux, px, py;           // psf point source: 10^(-0.4(mag-magzero)), centre
+	// derivatives of log(flux_scale) w.r.t. parameters (FP32+adjoint path)
+	double dlnI_dmag, dlnI_dq, dlnI_dbox, dlnI_dp1, dlnI_dp2;
+	double dbn_dn;
+};
+
+struct ModelGeom {
+	double magzero;
+	double sx, sy;          // profile pixel scale (image scale / finesampling)
+	double img_sx, img_sy;  // image pixel scale
+	double offx, offy;      // PSF padding in drawing pixels
+	unsigned finesampling;
+};
+
+PF_HD inline bool almost_eq(double x, double y) { return fabs(x - y) < 1e-10; }
+
+// ---- radial functions (values), reference operation order ---------------
+
+PF_HD inline double boxy_r(const DevProfile &p, double x, double y)
+{
+	if (p.box == 0) return sqrt(x * x + y * y);
+	double bp2 = p.box + 2.;
+	return pow(pow(fabs(x), bp2) + pow(fabs(y), bp2), 1. / bp2);
+}
+
+PF_HD inline double coresersic_r(double r, double rb, double a, double b, double re, double nser, double bn)
+{
+	return pow(1 + pow(r / rb, -a), b / a) * exp(-bn * pow((pow(r, a) + pow(rb, a)) / pow(re, a), 1 / (nser * a)));
+}
+
+PF_HD inline double king_r(double r, double rc, double rt, double a)
+{
+	if (r < rt) return pow(1 / pow(1 + pow(r / rc, 2), 1 / a) - 1 / pow(1 + pow(rt / rc, 2), 1 / a), a);
+	return 0;
+}
+
+PF_HD inline double brokenexp_r(double r, double h1, double h2, double rb, double a)
+{
+	double base = r - rb;
+	double expo = 1 / h1 - 1 / h2;
+	if (a * base < 40) base = log(1 + exp(a * base)) / a;
+	return exp(-r / h1 + expo * base);
+}
+
+PF_HD inline double sersic64(const DevProfile &p, double x, double y)
+{
+	double base, rf;
+	if (p.boxy) {
+		double B = p.box + 2;
+		base = pow(fabs(x / p.re), B) + pow(fabs(y / p.re), B);
+		switch (p.form) {
+		case SF_HALF: rf = base * base; break;
+		case SF_ONE: rf = base; break;
+		case SF_TWO: rf = sqrt(base); break;
+		case SF_THREE: rf = cbrt(base); break;
+		case SF_FOUR: rf = sqrt(sqrt(base)); break;
+		case SF_EIGHT: rf = sqrt(sqrt(sqrt(base))); break;
+		case SF_SIXTEEN: rf = sqrt(sqrt(sqrt(sqrt(base)))); break;
+		default: rf = pow(base, 1 / p.invexp); break;
+		}
+	}
+	else {
+		base = (x * x + y * y) / (p.re * p.re);
+		switch (p.form) {
+		case SF_HALF: rf = base; break;
+		case SF_ONE: rf = sqrt(base); break;
+		case SF_TWO: rf = sqrt(sqrt(base)); break;
+		case SF_THREE: rf = cbrt(sqrt(base)); break;
+		case SF_FOUR: rf = sqrt(sqrt(sqrt(base))); break;
+		case SF_EIGHT: rf = sqrt(sqrt(sqrt(sqrt(base)))); break;
+		case SF_SIXTEEN: rf = sqrt(sqrt(sqrt(sqrt(sqrt(base))))); break;
+		default: rf = pow(sqrt(base), 1 / p.invexp); break;
+		}
+	}
+	return exp(-p.bn * (rf - 1));
+}
+
+PF_HD inline double eval64(const DevProfile &p, double x, double y)
+{
+	switch (p.kind) {
+	case PK_SERSIC: return sersic64(p, x, y);
+	case PK_MOFFAT: {
+		double r = boxy_r(p, x, y);
+		double rf = r / p.rscale;
+		return pow(1 + rf * rf, -p.con);
+	}
+	case PK_FERRER: {
+		double r = boxy_r(p, x, y);
+		double rf = r / p.rscale;
+		if (rf < 1) return pow(1 - pow(rf, 2 - p.b), p.a);
+		return 0;
+	}
+	case PK_CORESERSIC: return coresersic_r(boxy_r(p, x, y), p.rb, p.a, p.b, p.re, p.nser, p.bn);
+	case PK_KING: return king_r(boxy_r(p, x, y), p.rc, p.rt, p.a);
+	case PK_BROKENEXP: return brokenexp_r(boxy_r(p, x, y), p.h1, p.h2, p.rb, p.a);
+	default: return 0;
+	}
+}
+
+// image -> profile coordinates (radial.cpp:46-52)
+PF_HD inline void to_profile64(const DevProfile &p, double x, double y, double &xp, double &yp)
+{
+	x -= p.cx;
+	y -= p.cy;
+	xp = x * p.cos_ang + y * p.sin_ang;
+	yp = -x * p.sin_q + y * p.cos_q;
+}
+
+// ---- validation (radial.cpp:204-214 and each profile's validate) --------
+
+// Returns nullptr if valid, else libprofit's message.
+inline const char *validate_profile(const ProfileParams &p, bool have_psf)
+{
+	if (p.kind == PK_PSF) return have_psf ? nullptr : "No psf present in the model, cannot produce a psf profile";
+	if (!is_radial_kind(p.kind)) return nullptr;
+	if (p.axrat <= 0) return "axrat <= 0, must have axrat > 0";
+	if (p.axrat > 1) return "axrat > 1, must have axrat <= 1";
+	if (p.box <= -2) return "box <= -2, must have box > -2";
+	switch (p.kind) {
+	case PK_SERSIC:
+		if (p.re <= 0) return "re <= 0, must have re > 0";
+		if (p.nser <= 0) return "nser <= 0, must have nser > 0";
+		break;
+	case PK_MOFFAT:
+		if (p.fwhm <= 0) return "fwhm <= 0, must have fwhm > 0";
+		if (p.con < 0) return "con < 0, must have con >= 0";
+		break;
+	case PK_FERRER:
+		if (p.rout <= 0) return "rout <= 0, must have rout >= 0";
+		if (p.a < 0) return "a < 0, must have a >= 0";
+		if (p.b > 2) return "b > 2, must have b <= 2";
+		break;
+	case PK_CORESERSIC:
+		if (p.re <= 0) return "re <= 0, must have re > 0";
+		if (p.rb <= 0) return "rb <= 0, must have rb > 0";
+		if (p.nser <= 0) return "nser <= 0, must have nser > 0";
+		if (p.a <= 0) return "a <= 0, must have a > 0";
+		if (p.b > 1.999) return "b > 1.999, must have b < 1.999";
+		break;
+	case PK_KING:
+		if (p.rc <= 0) return "rc <= 0, must have rc > 0";
+		if (p.rt <= 0) return "rt <= 0, must have rt > 0";
+		if (p.a < 0) return "a < 0, must have a >=0";
+		break;
+	case PK_BROKENEXP:
+		if (p.h1 <= 0) return "h1 <= 0, must have h1 > 0";
+		if (p.h2 <= 0) return "h2 <= 0, must have h2 > 0";
+		if (p.rb <= 0) return "rb <= 0, must have rb > 0";
+		break;
+	}
+	return nullptr;
+}
+
+// ---- per-profile prologue ------------------------------------------------
+
+struct CoreSersicIntegrand {
+	double rb, a, b, re, nser, bn;
+	PF_HD double operator()(double r) const { return r * coresersic_r(r, rb, a, b, re, nser, bn); }
+};
+struct KingIntegrand {
+	double rc, rt, a;
+	PF_HD double operator()(double r) const { return r * king_r(r, rc, rt, a); }
+};
+struct BrokenExpIntegrand {
+	double h1, h2, rb, a;
+	PF_HD double operator()(double r) const { return r * brokenexp_r(r, h1, h2, rb, a); }
+};
+
+// Fills the derived scalars of `d` from the user parameters `p`
+// (RadialProfile::initial_calculations and the profile overrides).  Values
+// libprofit writes back into the profile (acc, rscale_switch, resolution,
+// rscale_max) are derived here without touching `p`, which is what a fresh
+// profit::Model per evaluation (R_profit_make_model) observes.
+PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, DevProfile &d)
+{
+	d.kind = p.kind;
+	d.target = p.convolve ? 0 : 1;
+	d.rough = p.rough;
+	d.form = SF_GENERAL;
+	d.boxy = 0;
+	d.img_sx = g.img_sx;
+	d.img_sy = g.img_sy;
+	d.dlnI_dmag = -0.4 * 2.302585092994045684;
+	d.dlnI_dq = d.dlnI_dbox = d.dlnI_dp1 = d.dlnI_dp2 = d.dbn_dn = 0;
+	d.centre_override = 0;
+	d.bn = 0;
+
+	if (p.kind == PK_SKY) {
+		d.bg = p.bg / (g.finesampling * g.finesampling);
+		return;
+	}
+	if (p.kind == PK_PSF) {
+		d.psf_flux = pow(10, -0.4 * (p.mag - g.magzero));
+		d.px = p.xcen;
+		d.py = p.ycen;
+		return;
+	}
+	if (!is_radial_kind(p.kind)) return;
+
+	d.re = p.re;
+	d.nser = p.nser;
+	d.box = p.box;
+	d.con = p.con;
+	d.a = p.a;
+	d.b = p.b;
+	d.rb = p.rb;
+	d.rc = p.rc;
+	d.rt = p.rt;
+	d.h1 = p.h1;
+	d.h2 = p.h2;
+
+	if (p.kind == PK_SERSIC) {
+		double inv_exponent = p.nser;
+		d.boxy = p.box != 0;
+		if (d.boxy) inv_exponent *= (p.box + 2);
+		d.invexp = inv_exponent;
+		if (almost_eq(inv_exponent, 0.5)) d.form = SF_HALF;
+		else if (almost_eq(inv_exponent, 1)) d.form = SF_ONE;
+		else if (almost_eq(inv_exponent, 2)) d.form = SF_TWO;
+		else if (almost_eq(inv_exponent, 3)) d.form = SF_THREE;
+		else if (almost_eq(inv_exponent, 4)) d.form = SF_FOUR;
+		else if (almost_eq(inv_exponent, 8)) d.form = SF_EIGHT;
+		else if (almost_eq(inv_exponent, 16)) d.form = SF_SIXTEEN;
+		else d.form = SF_GENERAL;
+		// the specialised forms recompute 1/invexp with the same operands
+		d.invexp = d.boxy ? p.nser * (p.box + 2) : p.nser;
+	}
+	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) d.bn = qgamma(0.5, 2 * p.nser);
+
+	// rscale (get_rscale overrides)
+	double rscale;
+	switch (p.kind) {
+	case PK_MOFFAT: rscale = p.fwhm / (2 * sqrt(pow(2, (1 / p.con)) - 1)); break;
+	case PK_FERRER: rscale = p.rout; break;
+	case PK_KING: rscale = p.rt; break;
+	case PK_BROKENEXP: rscale = p.h1 * 4; break;
+	default: rscale = p.re; break;
+	}
+	d.rscale = rscale;
+
+	// lumtot (get_lumtot overrides)
+	double lum;
+	switch (p.kind) {
+	case PK_SERSIC: {
+		double g_factor = gamma_fn(2 * p.nser);
+		lum = pow(p.re, 2) * 2 * M_PI * p.nser * g_factor * exp(d.bn) / pow(d.bn, 2 * p.nser);
+		break;
+	}
+	case PK_MOFFAT: lum = pow(rscale, 2) * M_PI / (p.con - 1); break;
+	case PK_FERRER: {
+		double g_factor = p.a * beta_fn(p.a, 1 + 2 / (2 - p.b));
+		lum = pow(p.rout, 2) * M_PI * g_factor;
+		break;
+	}
+	case PK_CORESERSIC: {
+		CoreSersicIntegrand f{p.rb, p.a, p.b, p.re, p.nser, d.bn};
+		lum = 2 * M_PI * integrate_qagi(f, 0.0);
+		break;
+	}
+	case PK_KING: {
+		KingIntegrand f{p.rc, p.rt, p.a};
+		lum = 2 * M_PI * integrate_qags(f, 0.0, p.rt);
+		break;
+	}
+	default: {
+		BrokenExpIntegrand f{p.h1, p.h2, p.rb, p.a};
+		lum = 2 * M_PI * integrate_qagi(f, 0.0);
+		break;
+	}
+	}
+
+	double b2 = p.box + 2;
+	double r_box = M_PI * b2 / (2 * beta_fn(1 / b2, 1 / b2));
+	double lumtot = lum * p.axrat / r_box;
+	double ie = pow(10, -0.4 * (p.mag - g.magzero)) / lumtot;
+
+	double acc = p.acc, rscale_switch = p.rscale_switch, rscale_max = p.rscale_max;
+	unsigned resolution = p.resolution;
+	if (p.adjust) {
+		switch (p.kind) {
+		case PK_SERSIC: {
+			double fr = p.re * pow(qgamma(1. - p.nser * p.nser / 2e3, 2 * p.nser) / d.bn, p.nser);
+			double rs = ceil(fr);
+			rs = pf_fmax(pf_fmin(rs, 20.), 2.);
+			rscale_switch = rs / p.re;
+			break;
+		}
+		case PK_MOFFAT: {
+			double ff = rscale * sqrt(pow(1 - 0.9999, 1 / (1 - p.con)) - 1);
+			double rs = pf_fmax(ff, 1.823 * p.fwhm);
+			rscale_switch = pf_fmax(pf_fmin(rs, 20.), 2.) / rscale;
+			break;
+		}
+		case PK_FERRER: rscale_switch = 0.5; break;
+		case PK_KING: rscale_switch = 0.5; break;
+		default: rscale_switch = 1; break;
+		}
+		unsigned res = (unsigned)ceil(160 / (rscale_switch * rscale));
+		res += res % 2;
+		res = res > 16U ? 16U : res;
+		res = res < 4U ? 4U : res;
+		resolution = res;
+		if (rscale_max == 0) {
+			switch (p.kind) {
+			case PK_SERSIC: {
+				double ff = p.re * pow(qgamma(0.9999, 2 * p.nser) / d.bn, p.nser);
+				rscale_max = ceil(pf_fmax(ff, 2.) / p.re);
+				break;
+			}
+			case PK_MOFFAT: {
+				double ff = rscale * sqrt(pow(1 - 0.9999, 1 / (1 - p.con)) - 1);
+				rscale_max = ceil(pf_fmax(ff, 2.) / rscale);
+				break;
+			}
+			case PK_FERRER: rscale_max = 1; break;
+			case PK_KING: rscale_max = 1.5; break;
+			default: rscale_max = 100; break;
+			}
+		}
+		if (p.kind == PK_SERSIC) {
+			acc /= sqrt(p.nser);
+			acc = pf_fmax(0.1, acc) / p.axrat;
+		}
+		else if (p.kind == PK_MOFFAT) {
+			acc = 0.1 / p.axrat;
+		}
+	}
+	d.acc = acc;
+	d.resolution = resolution;
+	d.max_rec = p.max_recursions;
+	d.r_switch = rscale_switch * rscale;
+	d.r_max = rscale_max > 0 ? rscale_max * rscale : 0;
+
+	double angrad = fmod(p.ang + 90, 360.) * M_PI / 180.;
+	d.cos_ang = cos(angrad);
+	d.sin_ang = sin(angrad);
+	d.cos_q = d.cos_ang / p.axrat;
+	d.sin_q = d.sin_ang / p.axrat;
+
+	double rescale_factor = 1;
+	if (p.kind == PK_SERSIC && p.adjust && p.rescale_flux) {
+		double flux_r = d.bn * pow(rscale_max / p.re, 1 / p.nser);
+		flux_r = pgamma(flux_r, 2 * p.nser);
+		rescale_factor = 1 / flux_r;
+	}
+	double flux_scale = g.sx * g.sy * ie;
+	if (p.kind == PK_SERSIC && p.rescale_flux) flux_scale *= rescale_factor;
+	d.flux_scale = flux_scale;
+	d.cx = p.xcen + g.offx * g.sx;
+	d.cy = p.ycen + g.offy * g.sy;
+	d.centre_override = (p.kind == PK_SERSIC && p.adjust && p.nser > 1) ? 1 : 0;
+	d.king_t = (p.kind == PK_KING) ? 1 / pow(1 + pow(p.rt / p.rc, 2), 1 / p.a) : 0;
+
+	// d log(flux_scale) / d parameter, used by the adjoint.
+	// flux_scale = sx sy 10^(-0.4(mag - mz)) r_box / (L axrat)
+	d.dlnI_dq = -1.0 / p.axrat;
+	{
+		// d ln r_box / dB with r_box = pi B / (2 Beta(1/B, 1/B))
+		double B = b2;
+		d.dlnI_dbox = 1.0 / B + (2.0 / (B * B)) * (digamma(1.0 / B) - digamma(2.0 / B));
+	}
+	if (p.kind == PK_SERSIC) {
+		// L = re^2 2 pi n Gamma(2n) e^bn / bn^(2n)
+		double n = p.nser, bn = d.bn;
+		double h = 1e-6 * n;
+		double dbn = (qgamma(0.5, 2 * (n + h)) - qgamma(0.5, 2 * (n - h))) / (2 * h);
+		d.dbn_dn = dbn;
+		d.dlnI_dp1 = -2.0 / p.re;  // re
+		double dlnL_dn = 1.0 / n + 2.0 * digamma(2 * n) + dbn - 2.0 * log(bn) - 2.0 * n * dbn / bn;
+		d.dlnI_dp2 = -dlnL_dn;     // nser
+	}
+	else if (p.kind == PK_MOFFAT) {
+		// L = rscale^2 pi / (con - 1), rscale = fwhm / (2 sqrt(2^(1/con) - 1))
+		double c = p.con;
+		double t = pow(2.0, 1.0 / c);
+		double drs_dc_over_rs = 0.5 * t * log(2.0) / (c * c * (t - 1.0));
+		d.dlnI_dp1 = -2.0 / p.fwhm;                       // fwhm
+		d.dlnI_dp2 = -(2.0 * drs_dc_over_rs - 1.0 / (c - 1.0));  // con
+	}
+}
+
+}  // namespace pf

@@ -1,0 +1,214 @@
+"""libprofit's Model / Profile API in Python, backed by the sm_100a library.
+
+Mirrors profit::Model (src/libprofit/src/profit/model.h:55-421) and
+profit::Profile::parameter (profile.h:150-177): same method names, the same
+parameter names and types, and the same errors (InvalidParameter for
+profit::invalid_parameter, UnknownParameter for profit::unknown_parameter).
+Images are numpy arrays of shape (height, width); pixel (x, y) is
+image[y, x], which is libprofit's x-fastest row-major layout.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Iterable, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import _capi
+from ._capi import PF_FP32, PF_FP64, check, lib, pf_param_ref
+
+BOOL_PARAMS = {"rough", "adjust", "force_cpu", "convolve", "rescale_flux"}
+UINT_PARAMS = {"resolution", "max_recursions"}
+
+
+class Profile:
+    """A profile added to a Model (profit::Profile)."""
+
+    def __init__(self, model: "Model", index: int, name: str):
+        self.model = model
+        self.index = index
+        self.name = name
+
+    def parameter(self, name: str, value=None) -> "Profile":
+        """Profile::parameter(name, value) or Profile::parameter("name = value")."""
+        L, h = lib(), self.model._h
+        if value is None:
+            check(L.pf_profile_set(h, self.index, name.encode()))
+        elif name in BOOL_PARAMS or isinstance(value, (bool, np.bool_)):
+            check(L.pf_profile_set_bool(h, self.index, name.encode(), int(bool(value))))
+        elif name in UINT_PARAMS:
+            check(L.pf_profile_set_uint(h, self.index, name.encode(), int(value)))
+        else:
+            check(L.pf_profile_set_double(h, self.index, name.encode(), float(value)))
+        return self
+
+    def get(self, name: str) -> float:
+        v = C.c_double()
+        check(lib().pf_profile_get_double(self.model._h, self.index, name.encode(), C.byref(v)))
+        return v.value
+
+    def __setitem__(self, name, value):
+        self.parameter(name, value)
+
+    def __getitem__(self, name):
+        return self.get(name)
+
+
+class Model:
+    """profit::Model on a B200.  One handle per host thread."""
+
+    def __init__(self, width: int, height: int, precision: int = PF_FP64):
+        h = C.c_void_p()
+        check(lib().pf_model_create(int(width), int(height), C.byref(h)))
+        self._h = h
+        self.width, self.height = int(width), int(height)
+        self.profiles: List[Profile] = []
+        if precision != PF_FP64:
+            self.set_precision(precision)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().pf_model_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # --- profiles -------------------------------------------------------
+    def add_profile(self, name: str, **params) -> Profile:
+        idx = C.c_int()
+        check(lib().pf_model_add_profile(self._h, name.encode(), C.byref(idx)))
+        p = Profile(self, idx.value, name)
+        self.profiles.append(p)
+        for k, v in params.items():
+            p.parameter(k, v)
+        return p
+
+    def clear_profiles(self):
+        check(lib().pf_model_clear_profiles(self._h))
+        self.profiles = []
+
+    # --- settings (model.h:142-343) --------------------------------------
+    def set_psf(self, psf: Optional[np.ndarray]):
+        if psf is None:
+            check(lib().pf_model_set_psf(self._h, None, 0, 0))
+            return
+        a = np.ascontiguousarray(psf, dtype=np.float64)
+        h, w = a.shape
+        check(lib().pf_model_set_psf(self._h, a.ctypes.data_as(_capi._dp), w, h))
+
+    def set_magzero(self, magzero: float):
+        check(lib().pf_model_set_magzero(self._h, float(magzero)))
+
+    def set_image_pixel_scale(self, sx: float, sy: float):
+        check(lib().pf_model_set_image_pixel_scale(self._h, float(sx), float(sy)))
+
+    def set_psf_pixel_scale(self, sx: float, sy: float):
+        check(lib().pf_model_set_psf_pixel_scale(self._h, float(sx), float(sy)))
+
+    def set_finesampling(self, fs: int):
+        check(lib().pf_model_set_finesampling(self._h, int(fs)))
+
+    def set_return_finesampled(self, value: bool):
+        check(lib().pf_model_set_return_finesampled(self._h, int(bool(value))))
+
+    def set_crop(self, value: bool):
+        check(lib().pf_model_set_crop(self._h, int(bool(value))))
+
+    def set_convolver(self, kind: str):
+        check(lib().pf_model_set_convolver(self._h, kind.encode()))
+
+    def set_precision(self, precision: int):
+        check(lib().pf_model_set_precision(self._h, int(precision)))
+
+    def set_debug(self, value: bool):
+        check(lib().pf_model_set_debug(self._h, int(bool(value))))
+
+    def drawing_dims(self) -> Tuple[int, int]:
+        w, h = C.c_uint(), C.c_uint()
+        check(lib().pf_model_drawing_dims(self._h, C.byref(w), C.byref(h)))
+        return w.value, h.value
+
+    # --- evaluation -------------------------------------------------------
+    def evaluate(self) -> Tuple[np.ndarray, Tuple[int, int]]:
+        """Model::evaluate: (image[height, width], (offset_x, offset_y))."""
+        dw, dh = self.drawing_dims()
+        cap = dw * dh
+        buf = np.empty(cap, dtype=np.float64)
+        w, h, ox, oy = C.c_uint(), C.c_uint(), C.c_int(), C.c_int()
+        check(lib().pf_model_evaluate(self._h, buf.ctypes.data_as(_capi._dp), cap, C.byref(w), C.byref(h),
+                                      C.byref(ox), C.byref(oy)))
+        return buf[: w.value * h.value].reshape(h.value, w.value).copy(), (ox.value, oy.value)
+
+    def set_data(self, image: np.ndarray, sigma: np.ndarray, region: Optional[np.ndarray] = None):
+        im = np.ascontiguousarray(image, dtype=np.float64)
+        sg = np.ascontiguousarray(sigma, dtype=np.float64)
+        if sg.shape != im.shape:
+            raise ValueError("sigma must have the image's shape")
+        rp = None
+        if region is not None:
+            rg = np.ascontiguousarray(region, dtype=np.uint8)
+            self._region = rg
+            rp = rg.ctypes.data_as(C.POINTER(C.c_uint8))
+        h, w = im.shape
+        check(lib().pf_model_set_data(self._h, im.ctypes.data_as(_capi._dp), sg.ctypes.data_as(_capi._dp), rp, w, h))
+
+    def loglike(self) -> float:
+        v = C.c_double()
+        check(lib().pf_model_loglike(self._h, C.byref(v)))
+        return v.value
+
+    @staticmethod
+    def _refs(params: Sequence[Tuple[int, str]]):
+        arr = (pf_param_ref * max(len(params), 1))()
+        keep = []
+        for i, (p, name) in enumerate(params):
+            b = name.encode()
+            keep.append(b)
+            arr[i].profile = int(p.index if isinstance(p, Profile) else p)
+            arr[i].name = b
+        return arr, keep
+
+    def loglike_grad(self, params: Sequence[Tuple[int, str]]) -> Tuple[float, np.ndarray]:
+        """logL and its adjoint gradient (FP32 path)."""
+        arr, keep = self._refs(params)
+        ll = C.c_double()
+        g = np.zeros(len(params), dtype=np.float64)
+        check(lib().pf_model_loglike_grad(self._h, arr, len(params), C.byref(ll), g.ctypes.data_as(_capi._dp)))
+        return ll.value, g
+
+    def loglike_grad_fd(self, params: Sequence[Tuple[int, str]], rel_step: float = 1e-6) -> Tuple[float, np.ndarray]:
+        """logL and central finite differences of the plain FP64 form."""
+        arr, keep = self._refs(params)
+        ll = C.c_double()
+        g = np.zeros(len(params), dtype=np.float64)
+        check(lib().pf_model_loglike_grad_fd(self._h, arr, len(params), float(rel_step), C.byref(ll),
+                                             g.ctypes.data_as(_capi._dp)))
+        return ll.value, g
+
+    # --- instrumentation ---------------------------------------------------
+    def decisions(self, profile: int) -> np.ndarray:
+        dw, dh = self.drawing_dims()
+        out = np.zeros(dw * dh, dtype=np.int32)
+        check(lib().pf_model_decisions(self._h, int(profile), out.ctypes.data_as(C.POINTER(C.c_int32)), out.size))
+        return out.reshape(dh, dw)
+
+    def level_counts(self, profile: int) -> List[int]:
+        out = (C.c_int64 * 16)()
+        n = C.c_int()
+        check(lib().pf_model_level_counts(self._h, int(profile), out, 16, C.byref(n)))
+        return [out[i] for i in range(n.value)]
+
+    def last_timings(self) -> List[float]:
+        out = (C.c_float * 4)()
+        check(lib().pf_model_last_timings(self._h, out, 4))
+        return list(out)

@@ -1,0 +1,167 @@
+"""Parity of the sm_100a library against the oracle (needs a B200).
+
+Plain FP64 form: images within 1e-12 (relative to the image maximum) of the
+compiled reference, the same subsampling decision for every pixel as the
+restatement, the same per-level counts as libprofit's PROFIT_DEBUG counters,
+and the same "norm" log-likelihood to 1e-12 relative.
+
+FP32 form: images within 1e-5 of the FP64 form; the adjoint gradient within
+the tolerances stated in each test of FP64 central finite differences.
+"""
+import numpy as np
+import pytest
+
+from oracle.pyoracle import OracleModel, RefModel, loglike_norm
+from profit_b200 import PF_FP32, PF_FP64, InvalidParameter, Model, UnknownParameter
+from profit_b200 import workloads as W
+
+from test_oracle import PROFILE_CASES
+
+pytestmark = pytest.mark.gpu
+
+IMG_TOL = 1e-12
+
+
+def _rel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+@pytest.mark.parametrize("case", range(len(PROFILE_CASES)))
+def test_render_fp64_matches_reference(case):
+    name, params = PROFILE_CASES[case]
+    ref = RefModel(100, 100)
+    ref.add_profile(name, **params)
+    expect, _ = ref.evaluate()
+    m = Model(100, 100)
+    m.set_debug(True)
+    m.add_profile(name, **params)
+    got, off = m.evaluate()
+    assert off == (0, 0)
+    assert _rel(got, expect) <= IMG_TOL
+    # decisions: pixel by pixel against the restatement, per level against PROFIT_DEBUG
+    ora = OracleModel(100, 100)
+    ora.add_profile(name, **params)
+    ora.evaluate()
+    assert np.array_equal(m.decisions(0), ora.decisions(0))
+    assert m.level_counts(0) == ora.level_counts(0)
+    dbg = RefModel(100, 100, debug=True)
+    dbg.set_omp_threads(1)
+    dbg.add_profile(name, **params)
+    dbg.evaluate()
+    assert m.level_counts(0) == dbg.integrations(0)
+
+
+@pytest.mark.parametrize("wl", [W.single_sersic(), W.single_sersic(seed_tag=11), W.bulge_disk_ps()],
+                         ids=["single_sersic", "single_sersic_b", "bulge_disk_ps"])
+def test_workload_fp64_image_and_loglike(wl):
+    ref = W.configure(RefModel(wl["width"], wl["height"]), wl)
+    ref.set_omp_threads(8)
+    ref.set_convolver("brute", 8)
+    expect, _ = ref.evaluate()
+    m = W.configure(Model(wl["width"], wl["height"]), wl)
+    got, _ = m.evaluate()
+    assert got.shape == expect.shape
+    assert _rel(got, expect) <= IMG_TOL
+    image, sigma = W.make_data(wl, expect)
+    m.set_data(image, sigma)
+    ll = m.loglike()
+    assert ll == pytest.approx(loglike_norm(image, sigma, expect), rel=IMG_TOL)
+
+
+def test_sky_and_psf_point_source_fp64():
+    psf = W.moffat_psf(15, 3.0, 2.5)
+    out = []
+    for M in (RefModel, Model):
+        m = M(60, 50)
+        m.set_psf(psf)
+        m.add_profile("sersic", xcen=30, ycen=25, re=4, nser=2, convolve=True)
+        m.add_profile("sky", bg=0.25)
+        m.add_profile("psf", xcen=12.3, ycen=40.6, mag=14)
+        m.add_profile("psf", xcen=-3.0, ycen=55.0, mag=13)  # partly outside the image
+        out.append(m.evaluate()[0])
+    assert _rel(out[1], out[0]) <= IMG_TOL
+
+
+def test_null_convolver_and_rough():
+    wl = W.single_sersic(seed_tag=3)
+    out = []
+    for M in (RefModel, Model):
+        m = W.configure(M(wl["width"], wl["height"]), wl)
+        m.set_convolver("null")
+        m.add_profile("sersic", xcen=20.5, ycen=70.2, re=3, nser=1.5, rough=True)
+        out.append(m.evaluate()[0])
+    assert _rel(out[1], out[0]) <= IMG_TOL
+
+
+def test_finesampling_downsampled():
+    wl = W.single_sersic(seed_tag=4, width=60, height=50, psf_size=11)
+    out = []
+    for M in (RefModel, Model):
+        m = W.configure(M(wl["width"], wl["height"]), wl)
+        m.set_finesampling(3)
+        m.set_return_finesampled(False)
+        out.append(m.evaluate()[0])
+    assert out[1].shape == out[0].shape == (50, 60)
+    assert _rel(out[1], out[0]) <= IMG_TOL
+
+
+def test_errors_match_libprofit():
+    m = Model(10, 10)
+    with pytest.raises(InvalidParameter):
+        m.add_profile("nonexistent")
+    p = m.add_profile("sersic")
+    with pytest.raises(UnknownParameter):
+        p.parameter("fwhm", 3.0)
+    p.parameter("axrat", 1.5)
+    with pytest.raises(InvalidParameter, match="axrat > 1"):
+        m.evaluate()
+    p.parameter("axrat = 0.5")
+    p.parameter("convolve", True)
+    with pytest.raises(InvalidParameter, match="No psf provided"):
+        m.evaluate()
+
+
+@pytest.mark.parametrize("wl", [W.single_sersic(), W.bulge_disk_ps()], ids=["single_sersic", "bulge_disk_ps"])
+def test_fp32_image_close_to_fp64(wl):
+    m64 = W.configure(Model(wl["width"], wl["height"]), wl)
+    a, _ = m64.evaluate()
+    m32 = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
+    b, _ = m32.evaluate()
+    assert _rel(b, a) <= 1e-5
+
+
+def test_fp32_loglike_close_to_fp64():
+    wl = W.bulge_disk_ps()
+    m64 = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = m64.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    m64.set_data(image, sigma)
+    ll64 = m64.loglike()
+    m32 = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
+    m32.set_data(image, sigma)
+    ll32 = m32.loglike()
+    assert ll32 == pytest.approx(ll64, rel=1e-5)
+
+
+def _gradient_case(wl, offset_scale):
+    """Data drawn at the truth, model evaluated at a displaced point so the
+    gradient is dominated by signal, not by noise."""
+    m64 = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = m64.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    w2 = W.perturbed(wl, seed=5, scale=offset_scale)
+    m = W.configure(Model(wl["width"], wl["height"]), w2)
+    m.set_data(image, sigma)
+    return m, w2
+
+
+def test_adjoint_gradient_matches_fd64():
+    wl = W.bulge_disk_ps()
+    m, w2 = _gradient_case(wl, 0.02)
+    ll_fd, g_fd = m.loglike_grad_fd(w2["grad"], rel_step=1e-6)
+    m.set_precision(PF_FP32)
+    ll_ad, g_ad = m.loglike_grad(w2["grad"])
+    assert ll_ad == pytest.approx(ll_fd, rel=1e-5)
+    scale = np.max(np.abs(g_fd))
+    err = np.abs(g_ad - g_fd) / scale
+    assert np.all(err <= 1e-3), list(zip(w2["grad"], g_fd, g_ad))
