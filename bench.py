@@ -1,0 +1,412 @@
+#!/usr/bin/env python
+"""Throughput of ProFit's likelihood-and-gradient on B200.
+
+Metric: LL+grad evaluations/s of the bulge + disk + point-source model
+(400x400 image, 51x51 Moffat PSF, brute-force convolution, 17-parameter
+gradient) with the FP32 path and its hand-written adjoint.  One step = one
+sampler proposal: write the 17 parameters, evaluate logL and d(logL)/d(theta),
+read them back.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Reported on one JSON line (rank 0):
+  value      device-side throughput: K / sum of the per-step device time of
+             the evaluation pipeline (CUDA events on the library's stream),
+             inputs (data, sigma, PSF) resident in HBM
+  e2e        the same metric through the public C ABI call with host buffers:
+             parameters in, logL + gradient out, per-step host<->device copies
+             inside the timed region (CUDA events around each call)
+  roofline   the dominant kernel (forward brute-force convolution) against the
+             measured FP32 FMA peak of this GPU
+  cpu_baseline  the reference's own libprofit C++ (compiled in place, OpenMP on
+             all host cores) computing logL + central finite differences
+  plain_fp64_fd  this library's plain FP64 form with finite differences, the
+             denominator of the FP32-adjoint speed-up target
+
+With --impl reference, rank 0 times the reference CPU implementation on the
+same workload and metric; other ranks exit.  With N > 1 every rank runs an
+independent replica (the path does not shard across GPUs): value is the
+aggregate, timed as the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "LL+grad evals/s, 1 B200: FP32 adjoint vs FP64 plain @rel err≤1e-5"
+UNIT = "evals/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from profit_b200 import workloads as W
+    return W.bulge_disk_ps()
+
+
+def config_dict(wl, n_gpus):
+    return {
+        "workload": "bulge_disk_ps: 400x400 image, Sersic bulge (nser logU[2,8]) + exponential disk + "
+                    "unconvolved Moffat point source, 51x51 Moffat PSF (fwhm 3, con 2.5), brute-force "
+                    "convolver, sigma map U[0.5,2], 17-parameter gradient",
+        "proposals": "each step a new sampler proposal: params = init + N(0, 0.02|init|)",
+        "image": [wl["width"], wl["height"]],
+        "psf": list(wl["psf"].shape),
+        "n_params": len(wl["grad"]),
+        "l2": "flushed by a 256 MiB device write between timed steps (working set ~30 MB < L2)",
+        "parallelism": f"replicas x{n_gpus}" if n_gpus > 1 else "single GPU",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except Exception:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ---------------------------------------------------------------------------
+# CPU reference (libprofit compiled in place) timing
+# ---------------------------------------------------------------------------
+
+def reference_ll_grad(wl, params, image, sigma, threads, n_grad=None, rel_step=1e-7):
+    """logL + central FD gradient with the reference's own C++; returns (ll, grad, n_model_evals)."""
+    from oracle.pyoracle import RefModel, loglike_norm
+
+    def ll_at(overrides):
+        m = RefModel(wl["width"], wl["height"])
+        m.set_magzero(wl["magzero"])
+        m.set_psf(wl["psf"])
+        m.set_omp_threads(threads)
+        m.set_convolver("brute", threads)
+        for i, (name, p) in enumerate(params):
+            q = dict(p)
+            q.update(overrides.get(i, {}))
+            m.add_profile(name, **q)
+        img, _ = m.evaluate()
+        return loglike_norm(image, sigma, img)
+
+    refs = wl["grad"] if n_grad is None else wl["grad"][:n_grad]
+    ll0 = ll_at({})
+    g = []
+    for (pi, k) in refs:
+        v = params[pi][1][k]
+        h = rel_step * max(abs(v), 1.0)
+        g.append((ll_at({pi: {k: v + h}}) - ll_at({pi: {k: v - h}})) / (2 * h))
+    return ll0, np.array(g), 1 + 2 * len(refs)
+
+
+def cpu_baseline(wl, image, sigma, budget_s=15.0):
+    """Reference CPU LL+grad evals/s on a bounded sample (rank 0, N=1)."""
+    from profit_b200 import workloads as W
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    n_full = 0
+    evals = 0
+    while True:
+        prop = W.perturbed(wl, seed=10_000 + n_full, scale=0.02)
+        _, _, ne = reference_ll_grad(wl, prop["profiles"], image, sigma, threads)
+        evals += ne
+        n_full += 1
+        if time.perf_counter() - t0 > budget_s or n_full >= 20:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n_full / dt, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{n_full} LL+grad evaluations ({evals} libprofit model evaluations, central FD over "
+                      f"{len(wl['grad'])} parameters) of the same workload, OpenMP {threads} threads, "
+                      f"{dt:.1f} s wall"}
+
+
+# ---------------------------------------------------------------------------
+# main (B200 arm)
+# ---------------------------------------------------------------------------
+
+def init_dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def main_b200(args):
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    world, rank, local = init_dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    from profit_b200 import PF_FP32, PF_FP64, Model, _capi
+    from profit_b200 import workloads as W
+
+    wl = workload()
+    truth_model = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = truth_model.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    truth_model.close()
+
+    refs = wl["grad"]
+    proposals = [W.perturbed(wl, seed=s, scale=0.02) for s in range(args.warmup + args.steps)]
+    pvals = [np.array([p["profiles"][i][1][k] for (i, k) in refs]) for p in proposals]
+
+    m = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), W.perturbed(wl, seed=0, scale=0.02))
+    m.set_data(image, sigma)
+    L = _capi.lib()
+    arr, keep = Model._refs(refs)
+    ll = ctypes.c_double()
+    grad = np.zeros(len(refs))
+    gptr = grad.ctypes.data_as(_capi._dp)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+
+    # accuracy of the FP32 adjoint against the plain FP64 form (FD), outside timing
+    m.set_parameters(refs, pvals[0])
+    m.set_precision(PF_FP64)
+    ll_fd, g_fd = m.loglike_grad_fd(refs, rel_step=1e-7)
+    m.set_precision(PF_FP32)
+    ll_ad, g_ad = m.loglike_grad(refs)
+    g_rel = np.abs(g_ad - g_fd) / np.abs(g_fd)
+    accuracy = {"vs": "plain FP64 form, central FD (rel step 1e-7) at the first proposal",
+                "loglike_rel_err": abs(ll_ad - ll_fd) / abs(ll_fd),
+                "grad_max_rel_err": float(g_rel.max()), "grad_median_rel_err": float(np.median(g_rel)),
+                "grad_err_over_max_grad": float(np.max(np.abs(g_ad - g_fd)) / np.max(np.abs(g_fd)))}
+
+    # plain FP64 + FD timing (the speed-up target's denominator), a few steps
+    m.set_precision(PF_FP64)
+    fd_times = []
+    for s in range(3 + 5):
+        m.set_parameters(refs, pvals[s % len(pvals)])
+        m.loglike_grad_fd(refs, rel_step=1e-7)
+        if s >= 3:
+            fd_times.append(m.last_timings()[0])
+    m.set_precision(PF_FP32)
+    fp64_fd_value = 1e3 / statistics.mean(fd_times)
+
+    def step(s):
+        L.pf_model_set_parameters(m._h, arr, len(refs), pvals[s].ctypes.data_as(_capi._dp))
+        st = L.pf_model_loglike_grad(m._h, arr, len(refs), ctypes.byref(ll), gptr)
+        if st != 0:
+            raise RuntimeError(L.pf_last_error().decode())
+
+    for s in range(args.warmup):
+        step(s)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = L.pf_kernel_launches()
+    dev_ms, e2e_ms, conv_ms, tim = [], [], [], (ctypes.c_float * 4)()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    for s in range(args.warmup, args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        step(s)
+        ev1.record()
+        ev1.synchronize()
+        e2e_ms.append(ev0.elapsed_time(ev1))
+        L.pf_model_last_timings(m._h, tim, 4)
+        dev_ms.append(tim[0])
+        conv_ms.append(tim[2])
+    torch.cuda.synchronize()
+    launches = L.pf_kernel_launches() - launches0
+    clk = clocks.stop()
+    if world > 1:
+        dist.barrier()
+
+    dev_total = sum(dev_ms) / 1e3
+    e2e_total = sum(e2e_ms) / 1e3
+    if world > 1:
+        t = torch.tensor([dev_total, e2e_total], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_total, e2e_total = t.tolist()
+
+    # roofline of the forward convolution (the dominant kernel)
+    P = wl["psf"].shape[0]
+    n_out = wl["width"] * wl["height"]
+    flop = 2.0 * P * P * n_out
+    conv_s = statistics.mean(conv_ms) / 1e3
+    peaks = measured_fp32_peak()
+    roof = {"kernel": "k_conv_tile<float,16,2> (forward brute-force convolution)", "bound": "fp32",
+            "achieved": flop / conv_s / 1e12, "peak": peaks, "unit": "TFLOP/s",
+            "frac": (flop / conv_s / 1e12) / peaks if peaks else None,
+            "traffic": recorded_traffic(),
+            "algorithmic": f"2*P^2*W*H = {flop:.3e} FLOP per launch (P={P}, W*H={n_out})",
+            "peak_source": "measured: dependent FMA streams, libpf_peaks.so, best of 5 (burst)"}
+
+    out = None
+    if rank == 0:
+        per_step_in = 8 * len(refs) + 16 * len(refs)  # values + parameter references
+        out = {
+            "metric": METRIC, "value": world * args.steps / dev_total, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded PCG64 images/sigma/PSF of the configuration's shapes (no public dataset)",
+            "config": config_dict(wl, world),
+            "e2e": {"value": world * args.steps / e2e_total, "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * len(refs), "d2h_bytes_per_step": 8 * (1 + len(refs)),
+                    "path": "pf_model_set_parameters + pf_model_loglike_grad (C ABI, host buffers)",
+                    "ms_per_step": 1e3 * e2e_total / args.steps},
+            "roofline": roof,
+            "gpu_launches": int(launches),
+            "clocks": clk,
+            "accuracy": accuracy,
+            "plain_fp64_fd": {"value": fp64_fd_value, "unit": UNIT,
+                              "speedup_fp32_adjoint": (world * args.steps / dev_total) / fp64_fd_value},
+        }
+    m.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        if not args.no_cpu_baseline and world == 1:
+            out["cpu_baseline"] = cpu_baseline(wl, image, sigma)
+        print(json.dumps(out), flush=True)
+
+
+def measured_fp32_peak():
+    path = os.path.join(ROOT, "profit_b200", "lib", "libpf_peaks.so")
+    try:
+        lib = ctypes.CDLL(path)
+        lib.pf_peak_fma_tflops.restype = ctypes.c_double
+        lib.pf_peak_fma_tflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        v = lib.pf_peak_fma_tflops(0, 4096, 5)
+        return v if v > 0 else None
+    except OSError:
+        return None
+
+
+def recorded_traffic():
+    """DRAM bytes per forward-convolution launch from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "conv_fwd_bulge_disk_ps.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+
+def main_reference(args):
+    world, rank, local = init_dist()
+    if rank != 0:
+        return
+    from profit_b200 import workloads as W
+    from oracle.pyoracle import RefModel
+    wl = workload()
+    threads = os.cpu_count() or 1
+    # data from the reference itself at the truth
+    m = W.configure(RefModel(wl["width"], wl["height"]), wl)
+    m.set_omp_threads(threads)
+    m.set_convolver("brute", threads)
+    truth, _ = m.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    n_all = len(wl["grad"])
+    # per-step sample: logL + FD over n_grad parameters, sized to ~2 min total
+    t0 = time.perf_counter()
+    reference_ll_grad(wl, W.perturbed(wl, seed=0, scale=0.02)["profiles"], image, sigma, threads, n_grad=1)
+    per_eval = (time.perf_counter() - t0) / 3
+    budget = 120.0
+    total_steps = args.warmup + args.steps
+    n_grad = int(max(1, min(n_all, ((budget / total_steps) / per_eval - 1) / 2)))
+    times = []
+    for s in range(total_steps):
+        prop = W.perturbed(wl, seed=s, scale=0.02)
+        t = time.perf_counter()
+        _, _, ne = reference_ll_grad(wl, prop["profiles"], image, sigma, threads, n_grad=n_grad)
+        dt = time.perf_counter() - t
+        if s >= args.warmup:
+            times.append(dt * (1 + 2 * n_all) / ne)   # scaled to a full LL+grad
+    per_full = statistics.mean(times)
+    value = 1.0 / per_full
+    sample = (f"each step: logL + central FD over {n_grad} of {n_all} parameters "
+              f"({1 + 2 * n_grad} libprofit evaluations), time scaled by {1 + 2 * n_all}/{1 + 2 * n_grad} "
+              f"to a full LL+grad; OpenMP {threads} threads, brute-force convolver")
+    out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": 1e3 * per_full, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "impl": "reference",
+           "data": "synthetic: seeded PCG64 images/sigma/PSF of the configuration's shapes (no public dataset)",
+           "config": config_dict(wl, 1),
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference", "sample": sample},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    a = parse_args()
+    if a.impl == "reference":
+        main_reference(a)
+    else:
+        main_b200(a)

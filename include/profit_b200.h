@@ -52,6 +52,11 @@ extern "C" {
  *           coordinates, and the likelihood sum.  Required for gradients. */
 #define PF_FP64 0
 #define PF_FP32 1
+/*  PF_FP32_CONV64: as PF_FP32, but the forward convolution and the model
+ *           image the likelihood sees are summed in FP64 (the adjoint stays
+ *           FP32).  For bright sources, where the residual data - model is a
+ *           small difference of large numbers. */
+#define PF_FP32_CONV64 2
 
 typedef struct pf_model pf_model;
 
@@ -135,6 +140,12 @@ typedef struct {
 	const char *name;
 } pf_param_ref;
 
+/* Sets values[i] on every double parameter params[i] in one call, the way a
+ * sampler moves to its next proposal (profitRemakeModellist writes the new
+ * parameter vector into the model list, R/profitRemakeModelList.R:27-166). */
+int pf_model_set_parameters(pf_model *m, const pf_param_ref *params, int n_params,
+                            const double *values);
+
 /* logL and d(logL)/d(parameter) for every entry of `params`, by the
  * hand-written adjoint (precision PF_FP32).  The reference has no gradient;
  * this is new.  Subsampling decisions are held fixed, as the derivative of
@@ -156,6 +167,9 @@ int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_para
 int pf_model_set_debug(pf_model *m, int value);
 int pf_model_decisions(pf_model *m, int profile, int32_t *out, size_t capacity);
 int pf_model_level_counts(pf_model *m, int profile, int64_t *out, int max_levels, int *n_levels);
+
+/* Number of CUDA kernels this library has launched in this process. */
+unsigned long long pf_kernel_launches(void);
 
 /* Device time (ms, CUDA events) of the last evaluation's phases:
  * [0] total, [1] render, [2] convolution, [3] likelihood/adjoint. */

@@ -22,6 +22,7 @@ PF_E_BUFFER = -5
 PF_E_STATE = -6
 PF_FP64 = 0
 PF_FP32 = 1
+PF_FP32_CONV64 = 2
 
 # Every symbol include/profit_b200.h declares.
 EXPORTED = (
@@ -33,6 +34,7 @@ EXPORTED = (
     "pf_model_set_convolver", "pf_model_set_precision", "pf_model_drawing_dims", "pf_model_evaluate",
     "pf_model_set_data", "pf_model_loglike", "pf_model_loglike_grad", "pf_model_loglike_grad_fd",
     "pf_model_set_debug", "pf_model_decisions", "pf_model_level_counts", "pf_model_last_timings",
+    "pf_kernel_launches",
 )
 
 
@@ -102,6 +104,8 @@ def lib() -> C.CDLL:
         L.pf_model_decisions.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.c_size_t]
         L.pf_model_level_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int)]
         L.pf_model_last_timings.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
+        L.pf_kernel_launches.restype = C.c_ulonglong
+        _late_bindings(L)
         _lib = L
     return _lib
 
@@ -115,3 +119,10 @@ def check(status: int) -> None:
     if status == PF_E_INVALID:
         raise InvalidParameter(status, msg)
     raise ProfitError(status, msg)
+
+
+def _late_bindings(L):
+    L.pf_model_set_parameters.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, _dp]
+
+
+EXPORTED = EXPORTED + ("pf_model_set_parameters",)

@@ -21,6 +21,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 OBJDIR = os.path.join(HERE, "_build")
 LIB = os.path.join(LIBDIR, "libprofit_b200.so")
+PEAKS_LIB = os.path.join(LIBDIR, "libpf_peaks.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + os.path.join(ROOT, "include"),
@@ -49,7 +50,7 @@ def _newest_source() -> float:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _newest_source():
+    if not force and os.path.exists(LIB) and os.path.exists(PEAKS_LIB) and os.path.getmtime(LIB) >= _newest_source():
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(OBJDIR, exist_ok=True)
@@ -75,6 +76,11 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if r.returncode != 0:
         raise RuntimeError("link failed:\n" + r.stdout.decode())
     os.replace(tmp, LIB)
+    # FMA-throughput probe used by the benchmark for roofline denominators
+    cmd = [nvcc] + ARCH + COMMON + ["-shared", "-o", PEAKS_LIB, os.path.join(CSRC, "peaks.cu")]
+    r = subprocess.run(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    if r.returncode != 0:
+        raise RuntimeError("peaks build failed:\n" + r.stdout.decode())
     return LIB
 
 

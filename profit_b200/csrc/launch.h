@@ -8,6 +8,9 @@
 
 namespace pf {
 
+// Adds n to the process-wide count of kernels launched by this library.
+void note_launches(int n);
+
 // render64.cu
 cudaError_t launch_pixels64(const DevProfile *profiles, int n_profiles, unsigned width, unsigned height, double sx,
                             double sy, double *img_conv, double *img_plain, const QueueSet &q, cudaStream_t s);
@@ -46,4 +49,13 @@ cudaError_t launch_loglike32(const float *model, const double *data, const doubl
 cudaError_t launch_crop32(const float *src, unsigned sw, unsigned ox, unsigned oy, float *out, unsigned ow,
                           unsigned oh, const float *add, int batch, unsigned src_stride, cudaStream_t s);
 
+}  // namespace pf
+
+namespace pf {
+// render64.cu: FP32 -> FP64 copy and the FP64 likelihood that also writes the
+// adjoint seed (mixed-precision path).
+cudaError_t launch_widen(const float *src, double *dst, size_t n, cudaStream_t s);
+cudaError_t launch_loglike64_seed(const double *model, const double *data, const double *sigma,
+                                  const uint8_t *region, int n, double2 *partials, int nparts, double *out,
+                                  float *wseed, cudaStream_t s);
 }  // namespace pf

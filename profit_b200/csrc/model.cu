@@ -8,6 +8,7 @@
 // convolved with the normalised PSF, the PSF padding is cropped, the second
 // is added, and finesampled images are summed back down when requested.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -19,6 +20,11 @@
 #include "profit_b200.h"
 
 using namespace pf;
+
+namespace pf {
+static std::atomic<unsigned long long> g_launches{0};
+void note_launches(int n) { g_launches += (unsigned long long)n; }
+}  // namespace pf
 
 namespace {
 
@@ -576,7 +582,24 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	                        jac, q, m->stream));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, m->stream));
 	PF_CUDA(cudaEventRecord(m->ev[1], m->stream));
-	if (a.conv && m->conv_kind != CONV_NULL) {
+	const bool conv64 = m->precision == PF_FP32_CONV64;
+	if (conv64) {
+		// forward model summed in FP64: the residual (data - model) of bright
+		// pixels is a small difference of large numbers
+		PF_CUDA(ensure(m->d_conv64, npix * 8));
+		PF_CUDA(ensure(m->d_plain64, npix * 8));
+		PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
+		PF_CUDA(launch_widen(conv, m->d_conv64.as<double>(), npix, m->stream));
+		PF_CUDA(launch_widen(plain, m->d_plain64.as<double>(), npix, m->stream));
+		if (a.conv && m->conv_kind != CONV_NULL)
+			PF_CUDA(launch_conv64(m->d_conv64.as<double>(), a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w,
+			                      m->psf_h, m->d_model64.as<double>(), a.cw, a.ch, m->d_plain64.as<double>(), a.dw,
+			                      a.padx, a.pady, m->stream));
+		else
+			PF_CUDA(launch_crop64(m->d_conv64.as<double>(), a.dw, a.padx, a.pady, m->d_model64.as<double>(), a.cw,
+			                      a.ch, m->d_plain64.as<double>(), m->stream));
+	}
+	else if (a.conv && m->conv_kind != CONV_NULL) {
 		PF_CUDA(launch_conv32(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model, a.cw, a.ch,
 		                      plain, a.dw, a.padx, a.pady, 1, 0, 0, m->stream));
 	}
@@ -591,9 +614,14 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(ensure(m->d_wseed, nout * 4));
 		wseed = m->d_wseed.as<float>();
 	}
-	PF_CUDA(launch_loglike32(model, m->d_data.as<double>(), m->d_sigma.as<double>(),
-	                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout, 1, 0,
-	                         m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
+	if (conv64)
+		PF_CUDA(launch_loglike64_seed(m->d_model64.as<double>(), m->d_data.as<double>(), m->d_sigma.as<double>(),
+		                              m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout,
+		                              m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
+	else
+		PF_CUDA(launch_loglike32(model, m->d_data.as<double>(), m->d_sigma.as<double>(),
+		                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout, 1, 0,
+		                         m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
 	if (want_grad) {
 		PF_CUDA(ensure(m->d_gconv, npix * 4));
 		PF_CUDA(ensure(m->d_gplain, npix * 4));
@@ -733,6 +761,8 @@ extern "C" {
 const char *pf_last_error(void) { return g_error.c_str(); }
 
 const char *pf_version(void) { return "profit_b200 0.1 (libprofit 1.9.3 API)"; }
+
+unsigned long long pf_kernel_launches(void) { return pf::g_launches.load(); }
 
 int pf_model_create(unsigned width, unsigned height, pf_model **out)
 {
@@ -923,7 +953,8 @@ int pf_model_set_convolver(pf_model *m, const char *type)
 int pf_model_set_precision(pf_model *m, int precision)
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");
-	if (precision != PF_FP64 && precision != PF_FP32) return set_error(PF_E_INVALID, "unknown precision");
+	if (precision != PF_FP64 && precision != PF_FP32 && precision != PF_FP32_CONV64)
+		return set_error(PF_E_INVALID, "unknown precision");
 	m->precision = precision;
 	return PF_OK;
 }
@@ -954,7 +985,11 @@ int pf_model_evaluate(pf_model *m, double *image, size_t capacity, unsigned *out
 	else {
 		PF_TRY(evaluate32(m, a, false, nullptr));
 		size_t n = (size_t)a.ow * a.oh;
-		if (image) {
+		if (image && m->precision == PF_FP32_CONV64) {
+			if (capacity < n) return set_error(PF_E_BUFFER, "output buffer too small");
+			PF_CUDA(cudaMemcpy(image, m->d_model64.p, n * 8, cudaMemcpyDeviceToHost));
+		}
+		else if (image) {
 			if (capacity < n) return set_error(PF_E_BUFFER, "output buffer too small");
 			std::vector<float> tmp(n);
 			PF_CUDA(cudaMemcpy(tmp.data(), m->d_model32.p, n * 4, cudaMemcpyDeviceToHost));
@@ -1010,6 +1045,13 @@ int pf_model_loglike(pf_model *m, double *loglike)
 	std::vector<double> res;
 	PF_TRY(evaluate32(m, a, false, &res));
 	*loglike = res[ResultLayout::LL];
+	return PF_OK;
+}
+
+int pf_model_set_parameters(pf_model *m, const pf_param_ref *params, int n_params, const double *values)
+{
+	if (!m || (n_params > 0 && (!params || !values))) return set_error(PF_E_INVALID, "null argument");
+	for (int i = 0; i < n_params; i++) PF_TRY(set_param(m, params[i].profile, params[i].name, T_DOUBLE, values[i], 0, 0));
 	return PF_OK;
 }
 

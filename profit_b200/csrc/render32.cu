@@ -453,6 +453,7 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
 {
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8), batch);
 	k_pixels32<<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac, q);
+	note_launches(1);
 	return cudaGetLastError();
 }
 
@@ -460,6 +461,7 @@ cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npi
                             float *jac, const QueueSet &q, cudaStream_t s)
 {
 	for (int l = 0; l < n_levels; l++) k_level32<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, q);
+	note_launches(n_levels);
 	return cudaGetLastError();
 }
 
@@ -470,6 +472,7 @@ cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float
 	if (bx < 1) bx = 1;
 	if (bx > 148 * 4) bx = 148 * 4;
 	k_jac_reduce<<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, out);
+	note_launches(1);
 	return cudaGetLastError();
 }
 
@@ -478,6 +481,7 @@ cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned
 {
 	dim3 block(32, 8), grid(cdiv(dw, 32), cdiv(dh, 8), batch);
 	k_embed_seed<<<grid, block, 0, s>>>(w, ow, oh, padx, pady, dw, dh, g_plain);
+	note_launches(1);
 	return cudaGetLastError();
 }
 
@@ -486,7 +490,8 @@ cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, cons
                           int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
 {
 	if (conv_smem_bytes<float, 16, 2>(kw, kh) <= 227 * 1024)
-		return launch_conv<float, 16, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox,
+		note_launches(1);
+	return launch_conv<float, 16, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox,
 		                                 add_oy, batch, batch_src_stride, batch_out_stride, s);
 	return launch_conv<float, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy,
 	                                batch, batch_src_stride, batch_out_stride, s);
@@ -499,6 +504,7 @@ cudaError_t launch_loglike32(const float *model, const double *data, const doubl
 	k_loglike_partial<float><<<dim3(nparts, batch), 256, 0, s>>>(model, data, sigma, region, n, partials, wseed,
 	                                                             data_batch_stride);
 	k_loglike_final<<<batch, 256, 0, s>>>(partials, nparts, out);
+	note_launches(2);
 	return cudaGetLastError();
 }
 
@@ -507,6 +513,7 @@ cudaError_t launch_crop32(const float *src, unsigned sw, unsigned ox, unsigned o
 {
 	dim3 block(32, 8), grid(cdiv(ow, 32), cdiv(oh, 8), batch);
 	k_crop32<<<grid, block, 0, s>>>(src, sw, ox, oy, out, ow, oh, add, src_stride);
+	note_launches(1);
 	return cudaGetLastError();
 }
 

@@ -264,6 +264,7 @@ cudaError_t launch_pixels64(const DevProfile *profiles, int n_profiles, unsigned
 {
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8));
 	k_pixels64<<<grid, block, 0, s>>>(profiles, n_profiles, width, height, sx, sy, img_conv, img_plain, q);
+	note_launches(1);
 	return cudaGetLastError();
 }
 
@@ -273,12 +274,14 @@ cudaError_t launch_levels64(const DevProfile *profiles, int n_levels, double *im
 	for (int l = 0; l < n_levels; l++) {
 		k_level64<<<148 * 8, 256, 0, s>>>(profiles, l, img_conv, img_plain, q);
 	}
+	note_launches(n_levels);
 	return cudaGetLastError();
 }
 
 cudaError_t launch_count_decisions(const QueueSet &q, int n_levels, size_t npix, cudaStream_t s)
 {
 	for (int l = 0; l < n_levels; l++) k_count_decisions<<<148 * 4, 256, 0, s>>>(q, l, npix);
+	note_launches(n_levels);
 	return cudaGetLastError();
 }
 
@@ -288,6 +291,7 @@ cudaError_t launch_psf_stamp64(const DevProfile *profiles, int p, const double *
 {
 	k_psf_stamp64<<<64, 256, 0, s>>>(profiles, p, psf, psf_w, psf_h, psf_sx, psf_sy, scale_x, scale_y, offx, offy,
 	                                  width, height, img_conv, img_plain);
+	note_launches(1);
 	return cudaGetLastError();
 }
 
@@ -296,7 +300,8 @@ cudaError_t launch_conv64(const double *src, int sw, int sh, int ox, int oy, con
                           cudaStream_t s)
 {
 	if (conv_smem_bytes<double, 8, 4>(kw, kh) <= 227 * 1024)
-		return launch_conv<double, 8, 4>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox,
+		note_launches(1);
+	return launch_conv<double, 8, 4>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox,
 		                                 add_oy, 1, 0, 0, s);
 	return launch_conv<double, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy,
 	                                 1, 0, 0, s);
@@ -307,6 +312,7 @@ cudaError_t launch_loglike64(const double *model, const double *data, const doub
 {
 	k_loglike_partial<double><<<dim3(nparts, 1), 256, 0, s>>>(model, data, sigma, region, n, partials, nullptr, 0);
 	k_loglike_final<<<1, 256, 0, s>>>(partials, nparts, out);
+	note_launches(2);
 	return cudaGetLastError();
 }
 
@@ -315,6 +321,7 @@ cudaError_t launch_crop64(const double *src, unsigned sw, unsigned ox, unsigned 
 {
 	dim3 block(32, 8), grid(cdiv(ow, 32), cdiv(oh, 8));
 	k_crop64<<<grid, block, 0, s>>>(src, sw, ox, oy, out, ow, oh, add);
+	note_launches(1);
 	return cudaGetLastError();
 }
 
@@ -323,6 +330,30 @@ cudaError_t launch_downsample64(const double *src, unsigned sw, unsigned sh, uns
 {
 	dim3 block(32, 8), grid(cdiv(ow, 32), cdiv(oh, 8));
 	k_downsample64<<<grid, block, 0, s>>>(src, sw, sh, fs, out, ow, oh);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+__global__ void k_widen(const float *__restrict__ src, double *__restrict__ dst, size_t n)
+{
+	for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+		dst[i] = (double)src[i];
+}
+
+cudaError_t launch_widen(const float *src, double *dst, size_t n, cudaStream_t s)
+{
+	k_widen<<<148 * 4, 256, 0, s>>>(src, dst, n);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_loglike64_seed(const double *model, const double *data, const double *sigma,
+                                  const uint8_t *region, int n, double2 *partials, int nparts, double *out,
+                                  float *wseed, cudaStream_t s)
+{
+	k_loglike_partial<double><<<dim3(nparts, 1), 256, 0, s>>>(model, data, sigma, region, n, partials, wseed, 0);
+	k_loglike_final<<<1, 256, 0, s>>>(partials, nparts, out);
+	note_launches(2);
 	return cudaGetLastError();
 }
 

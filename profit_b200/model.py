@@ -178,6 +178,12 @@ class Model:
             arr[i].name = b
         return arr, keep
 
+    def set_parameters(self, params: Sequence[Tuple[int, str]], values: Sequence[float]):
+        """Writes a whole parameter vector in one call (a sampler's next proposal)."""
+        arr, keep = self._refs(params)
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        check(lib().pf_model_set_parameters(self._h, arr, len(params), v.ctypes.data_as(_capi._dp)))
+
     def loglike_grad(self, params: Sequence[Tuple[int, str]]) -> Tuple[float, np.ndarray]:
         """logL and its adjoint gradient (FP32 path)."""
         arr, keep = self._refs(params)
