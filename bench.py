@@ -261,6 +261,7 @@ def main_b200(args):
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
+    torch.cuda.nvtx.range_push("timed")
     launches0 = L.pf_kernel_launches()
     dev_ms, e2e_ms, conv_ms, tim = [], [], [], (ctypes.c_float * 4)()
     ev0 = torch.cuda.Event(enable_timing=True)
@@ -278,6 +279,7 @@ def main_b200(args):
         conv_ms.append(tim[2])
     torch.cuda.synchronize()
     launches = L.pf_kernel_launches() - launches0
+    torch.cuda.nvtx.range_pop()
     clk = clocks.stop()
     if world > 1:
         dist.barrier()
