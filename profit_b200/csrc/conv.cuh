@@ -13,32 +13,50 @@
 //    oy = 1 - kh, K = the PSF itself: out(u) = sum_k w(u - k) ikrn(k) over
 //    the padded grid, the transpose of the forward map.
 //
-// A CTA owns a 32 x (TYT*RY) output tile.  The source tile with its
-// (kw-1, kh-1) halo and the whole kernel sit in shared memory; each thread
-// keeps RY vertically adjacent outputs in registers and slides an RY-row
-// window down the tile, so every tap costs one shared load, one broadcast
-// kernel load and RY FMAs.  An optional `add` image (the unconvolved
-// profiles) is added in the epilogue, which fuses model.cpp:377.
+// Work decomposition: a CTA owns a 32 x (TYT*RY) output tile; its source
+// tile with the (kw-1, kh-1) halo and the whole kernel sit in shared memory.
+// The kernel columns k are split over KS warp groups (threadIdx.z), so even a
+// single 400x400 image keeps ~16 warps per SM busy.  Each thread holds RY
+// vertically adjacent outputs and slides an RY-row window down the tile: per
+// tap one shared load of the source, a quarter of a vector load of the
+// kernel (stored transposed so four rows are contiguous) and RY FMAs.
+//
+// Precision: the taps of one kernel column are summed in T (FP32 on the fast
+// path); the column sums are accumulated in Acc (FP64), and the KS partial
+// results are added in a fixed order.  A 51x51 PSF then has 51-term FP32
+// sums instead of one 2601-term sum, which brings the FP32 convolution error
+// from ~1e-6 to a few 1e-8 of the value (the FP32 rounding of the inputs).
+// An optional `add` image (the unconvolved profiles) is added in the
+// epilogue, which fuses model.cpp:377.
 #pragma once
 
 #include <cuda_runtime.h>
 
 namespace pf {
 
-template <class T, int RY, int TYT>
-__global__ void __launch_bounds__(32 * TYT) k_conv_tile(const T *__restrict__ src, int sw, int sh, int ox, int oy,
-                                                        const T *__restrict__ K, int kw, int kh,
-                                                        T *__restrict__ out, int ow, int oh,
-                                                        const T *__restrict__ add, int add_stride, int add_ox,
-                                                        int add_oy, int batch_src_stride, int batch_out_stride)
+template <class T, class Acc>
+__host__ __device__ inline size_t conv_red_offset(int kw, int kh, int TY)
 {
-	extern __shared__ unsigned char smem_raw[];
-	T *s_src = reinterpret_cast<T *>(smem_raw);
+	size_t khp = (size_t)((kh + 3) & ~3);
+	size_t bytes = sizeof(T) * ((size_t)kw * khp + (size_t)(32 + kw - 1) * (TY + kh - 1));
+	return (bytes + 15) & ~(size_t)15;
+}
+
+template <class T, class Acc, class TOut, int RY, int TYT, int KS>
+__global__ void __launch_bounds__(32 * TYT * KS)
+    k_conv_tile(const T *__restrict__ src, int sw, int sh, int ox, int oy, const T *__restrict__ K, int kw, int kh,
+                TOut *__restrict__ out, int ow, int oh, const T *__restrict__ add, int add_stride, int add_ox,
+                int add_oy, int batch_src_stride, int batch_out_stride)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
 	constexpr int TX = 32;
 	constexpr int TY = TYT * RY;
 	const int tw = TX + kw - 1;
 	const int th = TY + kh - 1;
-	T *s_k = s_src + (size_t)tw * th;
+	const int khp = (kh + 3) & ~3;  // transposed kernel rows padded to 4
+	T *s_k = reinterpret_cast<T *>(smem_raw);             // [kw][khp], K(k, l) at k*khp + l
+	T *s_src = s_k + (size_t)kw * khp;                     // [th][tw]
+	Acc *s_red = reinterpret_cast<Acc *>(smem_raw + conv_red_offset<T, Acc>(kw, kh, TY));
 
 	const int b = blockIdx.z;
 	src += (size_t)b * batch_src_stride;
@@ -47,10 +65,13 @@ __global__ void __launch_bounds__(32 * TYT) k_conv_tile(const T *__restrict__ sr
 
 	const int i0 = blockIdx.x * TX;
 	const int j0 = blockIdx.y * TY;
-	const int nthr = TX * TYT;
-	const int tid = threadIdx.x + threadIdx.y * TX;
+	const int nthr = TX * TYT * KS;
+	const int tid = threadIdx.x + TX * (threadIdx.y + TYT * threadIdx.z);
 
-	for (int t = tid; t < kw * kh; t += nthr) s_k[t] = K[t];
+	for (int t = tid; t < kw * khp; t += nthr) {
+		int k = t / khp, l = t - k * khp;
+		s_k[t] = l < kh ? K[k + l * kw] : T(0);
+	}
 	for (int t = tid; t < tw * th; t += nthr) {
 		int ty = t / tw, tx = t - ty * tw;
 		int sx = i0 + ox + tx, sy = j0 + oy + ty;
@@ -62,24 +83,70 @@ __global__ void __launch_bounds__(32 * TYT) k_conv_tile(const T *__restrict__ sr
 
 	const int tx = threadIdx.x;
 	const int r0 = threadIdx.y * RY;
-	T acc[RY];
+	Acc tot[RY];
 #pragma unroll
-	for (int r = 0; r < RY; r++) acc[r] = T(0);
+	for (int r = 0; r < RY; r++) tot[r] = Acc(0);
 
-	for (int k = 0; k < kw; k++) {
+	for (int k = threadIdx.z; k < kw; k += KS) {
 		const T *col = s_src + tx + k;
+		const T *kcol = s_k + k * khp;
+		T acc[RY];
 		T win[RY];
 #pragma unroll
+		for (int r = 0; r < RY; r++) acc[r] = T(0);
+#pragma unroll
 		for (int r = 0; r < RY - 1; r++) win[r] = col[(r0 + r) * tw];
-		const T *krow = s_k + k;
-		for (int l = 0; l < kh; l++) {
+		int l = 0;
+		for (; l + 4 <= kh; l += 4) {
+			T c4[4];
+			if constexpr (sizeof(T) == 4) {
+				float4 v = *reinterpret_cast<const float4 *>(kcol + l);
+				c4[0] = v.x;
+				c4[1] = v.y;
+				c4[2] = v.z;
+				c4[3] = v.w;
+			}
+			else {
+				double2 v0 = *reinterpret_cast<const double2 *>(kcol + l);
+				double2 v1 = *reinterpret_cast<const double2 *>(kcol + l + 2);
+				c4[0] = v0.x;
+				c4[1] = v0.y;
+				c4[2] = v1.x;
+				c4[3] = v1.y;
+			}
+#pragma unroll
+			for (int q = 0; q < 4; q++) {
+				win[RY - 1] = col[(r0 + l + q + RY - 1) * tw];
+#pragma unroll
+				for (int r = 0; r < RY; r++) acc[r] += win[r] * c4[q];
+#pragma unroll
+				for (int r = 0; r < RY - 1; r++) win[r] = win[r + 1];
+			}
+		}
+		for (; l < kh; l++) {
 			win[RY - 1] = col[(r0 + l + RY - 1) * tw];
-			const T c = krow[l * kw];
+			const T c = kcol[l];
 #pragma unroll
 			for (int r = 0; r < RY; r++) acc[r] += win[r] * c;
 #pragma unroll
 			for (int r = 0; r < RY - 1; r++) win[r] = win[r + 1];
 		}
+#pragma unroll
+		for (int r = 0; r < RY; r++) tot[r] += (Acc)acc[r];
+	}
+
+	if (KS > 1) {
+		// groups 1..KS-1 hand their partial sums to group 0 (fixed order)
+		if (threadIdx.z > 0) {
+#pragma unroll
+			for (int r = 0; r < RY; r++) s_red[((threadIdx.z - 1) * TY + r0 + r) * TX + tx] = tot[r];
+		}
+		__syncthreads();
+		if (threadIdx.z > 0) return;
+#pragma unroll
+		for (int g = 1; g < KS; g++)
+#pragma unroll
+			for (int r = 0; r < RY; r++) tot[r] += s_red[((g - 1) * TY + r0 + r) * TX + tx];
 	}
 
 	const int i = i0 + tx;
@@ -88,38 +155,39 @@ __global__ void __launch_bounds__(32 * TYT) k_conv_tile(const T *__restrict__ sr
 	for (int r = 0; r < RY; r++) {
 		int j = j0 + r0 + r;
 		if (j < oh) {
-			T v = acc[r];
-			if (add) v += add[(i + add_ox) + (size_t)(j + add_oy) * add_stride];
-			out[i + (size_t)j * ow] = v;
+			Acc v = tot[r];
+			if (add) v += (Acc)add[(i + add_ox) + (size_t)(j + add_oy) * add_stride];
+			out[i + (size_t)j * ow] = (TOut)v;
 		}
 	}
 }
 
-template <class T, int RY, int TYT>
+template <class T, class Acc, int RY, int TYT, int KS>
 inline size_t conv_smem_bytes(int kw, int kh)
 {
-	return sizeof(T) * ((size_t)(32 + kw - 1) * (TYT * RY + kh - 1) + (size_t)kw * kh);
+	constexpr int TY = TYT * RY;
+	return conv_red_offset<T, Acc>(kw, kh, TY) + sizeof(Acc) * (size_t)(KS - 1) * TY * 32;
 }
 
-template <class T, int RY, int TYT>
-inline cudaError_t launch_conv(const T *src, int sw, int sh, int ox, int oy, const T *K, int kw, int kh, T *out,
+template <class T, class Acc, class TOut, int RY, int TYT, int KS>
+inline cudaError_t launch_conv(const T *src, int sw, int sh, int ox, int oy, const T *K, int kw, int kh, TOut *out,
                                int ow, int oh, const T *add, int add_stride, int add_ox, int add_oy, int batch,
                                int batch_src_stride, int batch_out_stride, cudaStream_t stream)
 {
-	size_t smem = conv_smem_bytes<T, RY, TYT>(kw, kh);
+	size_t smem = conv_smem_bytes<T, Acc, RY, TYT, KS>(kw, kh);
 	static bool configured = false;
 	if (!configured) {
-		cudaError_t e = cudaFuncSetAttribute(k_conv_tile<T, RY, TYT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-		                                     227 * 1024);
+		cudaError_t e = cudaFuncSetAttribute(k_conv_tile<T, Acc, TOut, RY, TYT, KS>,
+		                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 		if (e != cudaSuccess) return e;
 		configured = true;
 	}
 	if (smem > 227 * 1024) return cudaErrorInvalidValue;
-	dim3 block(32, TYT);
+	dim3 block(32, TYT, KS);
 	dim3 grid((ow + 31) / 32, (oh + TYT * RY - 1) / (TYT * RY), batch);
-	k_conv_tile<T, RY, TYT><<<grid, block, smem, stream>>>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add,
-	                                                       add_stride, add_ox, add_oy, batch_src_stride,
-	                                                       batch_out_stride);
+	k_conv_tile<T, Acc, TOut, RY, TYT, KS><<<grid, block, smem, stream>>>(
+	    src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch_src_stride,
+	    batch_out_stride);
 	return cudaGetLastError();
 }
 

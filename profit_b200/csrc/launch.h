@@ -40,6 +40,9 @@ cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float
                               const int *prof_batch, int n_profiles, unsigned npix, double *out, cudaStream_t s);
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
                               unsigned dh, int batch, float *g_plain, cudaStream_t s);
+cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
+                               double *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
+                               int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s);
 cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                           float *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
                           int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s);

@@ -582,30 +582,29 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	                        jac, q, m->stream));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, m->stream));
 	PF_CUDA(cudaEventRecord(m->ev[1], m->stream));
+	// The forward model image is kept in FP64: the residual (data - model) of
+	// bright pixels is a small difference of large numbers.
+	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
+	double *model64 = m->d_model64.as<double>();
 	const bool conv64 = m->precision == PF_FP32_CONV64;
-	if (conv64) {
-		// forward model summed in FP64: the residual (data - model) of bright
-		// pixels is a small difference of large numbers
+	if (conv64 || !(a.conv && m->conv_kind != CONV_NULL)) {
 		PF_CUDA(ensure(m->d_conv64, npix * 8));
 		PF_CUDA(ensure(m->d_plain64, npix * 8));
-		PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
 		PF_CUDA(launch_widen(conv, m->d_conv64.as<double>(), npix, m->stream));
 		PF_CUDA(launch_widen(plain, m->d_plain64.as<double>(), npix, m->stream));
 		if (a.conv && m->conv_kind != CONV_NULL)
 			PF_CUDA(launch_conv64(m->d_conv64.as<double>(), a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w,
-			                      m->psf_h, m->d_model64.as<double>(), a.cw, a.ch, m->d_plain64.as<double>(), a.dw,
-			                      a.padx, a.pady, m->stream));
+			                      m->psf_h, model64, a.cw, a.ch, m->d_plain64.as<double>(), a.dw, a.padx, a.pady,
+			                      m->stream));
 		else
-			PF_CUDA(launch_crop64(m->d_conv64.as<double>(), a.dw, a.padx, a.pady, m->d_model64.as<double>(), a.cw,
-			                      a.ch, m->d_plain64.as<double>(), m->stream));
-	}
-	else if (a.conv && m->conv_kind != CONV_NULL) {
-		PF_CUDA(launch_conv32(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model, a.cw, a.ch,
-		                      plain, a.dw, a.padx, a.pady, 1, 0, 0, m->stream));
+			PF_CUDA(launch_crop64(m->d_conv64.as<double>(), a.dw, a.padx, a.pady, model64, a.cw, a.ch,
+			                      m->d_plain64.as<double>(), m->stream));
 	}
 	else {
-		PF_CUDA(launch_crop32(conv, a.dw, a.padx, a.pady, model, a.cw, a.ch, plain, 1, 0, m->stream));
+		PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64,
+		                           a.cw, a.ch, plain, a.dw, a.padx, a.pady, 1, 0, 0, m->stream));
 	}
+	(void)model;
 	PF_CUDA(cudaEventRecord(m->ev[2], m->stream));
 	if (!m->has_data) return PF_OK;
 	PF_CUDA(ensure(m->d_partials, NPARTS * sizeof(double2)));
@@ -614,14 +613,9 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(ensure(m->d_wseed, nout * 4));
 		wseed = m->d_wseed.as<float>();
 	}
-	if (conv64)
-		PF_CUDA(launch_loglike64_seed(m->d_model64.as<double>(), m->d_data.as<double>(), m->d_sigma.as<double>(),
-		                              m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout,
-		                              m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
-	else
-		PF_CUDA(launch_loglike32(model, m->d_data.as<double>(), m->d_sigma.as<double>(),
-		                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout, 1, 0,
-		                         m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
+	PF_CUDA(launch_loglike64_seed(model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
+	                              m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout,
+	                              m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
 	if (want_grad) {
 		PF_CUDA(ensure(m->d_gconv, npix * 4));
 		PF_CUDA(ensure(m->d_gplain, npix * 4));
@@ -985,15 +979,9 @@ int pf_model_evaluate(pf_model *m, double *image, size_t capacity, unsigned *out
 	else {
 		PF_TRY(evaluate32(m, a, false, nullptr));
 		size_t n = (size_t)a.ow * a.oh;
-		if (image && m->precision == PF_FP32_CONV64) {
+		if (image) {
 			if (capacity < n) return set_error(PF_E_BUFFER, "output buffer too small");
 			PF_CUDA(cudaMemcpy(image, m->d_model64.p, n * 8, cudaMemcpyDeviceToHost));
-		}
-		else if (image) {
-			if (capacity < n) return set_error(PF_E_BUFFER, "output buffer too small");
-			std::vector<float> tmp(n);
-			PF_CUDA(cudaMemcpy(tmp.data(), m->d_model32.p, n * 4, cudaMemcpyDeviceToHost));
-			for (size_t i = 0; i < n; i++) image[i] = tmp[i];
 		}
 	}
 	if (out_w) *out_w = a.ow;

@@ -485,16 +485,35 @@ cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned
 	return cudaGetLastError();
 }
 
+// FP32 taps, FP64 column accumulation; FP32 output (adjoint) or FP64 output
+// (forward model, so the likelihood sees the full-precision sum).
+template <class TOut>
+static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
+                              TOut *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
+                              int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
+{
+	note_launches(1);
+	if (conv_smem_bytes<float, double, 8, 4, 4>(kw, kh) <= 227 * 1024)
+		return launch_conv<float, double, TOut, 8, 4, 4>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride,
+		                                                 add_ox, add_oy, batch, batch_src_stride, batch_out_stride, s);
+	return launch_conv<float, double, TOut, 4, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride,
+	                                                 add_ox, add_oy, batch, batch_src_stride, batch_out_stride, s);
+}
+
 cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                           float *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
                           int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
 {
-	if (conv_smem_bytes<float, 16, 2>(kw, kh) <= 227 * 1024)
-		note_launches(1);
-	return launch_conv<float, 16, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox,
-		                                 add_oy, batch, batch_src_stride, batch_out_stride, s);
-	return launch_conv<float, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy,
-	                                batch, batch_src_stride, batch_out_stride, s);
+	return conv32_any<float>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
+	                         batch_src_stride, batch_out_stride, s);
+}
+
+cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
+                               double *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
+                               int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
+{
+	return conv32_any<double>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
+	                          batch_src_stride, batch_out_stride, s);
 }
 
 cudaError_t launch_loglike32(const float *model, const double *data, const double *sigma, const uint8_t *region,

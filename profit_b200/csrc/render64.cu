@@ -299,12 +299,12 @@ cudaError_t launch_conv64(const double *src, int sw, int sh, int ox, int oy, con
                           double *out, int ow, int oh, const double *add, int add_stride, int add_ox, int add_oy,
                           cudaStream_t s)
 {
-	if (conv_smem_bytes<double, 8, 4>(kw, kh) <= 227 * 1024)
-		note_launches(1);
-	return launch_conv<double, 8, 4>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox,
-		                                 add_oy, 1, 0, 0, s);
-	return launch_conv<double, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy,
-	                                 1, 0, 0, s);
+	note_launches(1);
+	if (conv_smem_bytes<double, double, 8, 4, 2>(kw, kh) <= 227 * 1024)
+		return launch_conv<double, double, double, 8, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add,
+		                                                    add_stride, add_ox, add_oy, 1, 0, 0, s);
+	return launch_conv<double, double, double, 4, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride,
+	                                                    add_ox, add_oy, 1, 0, 0, s);
 }
 
 cudaError_t launch_loglike64(const double *model, const double *data, const double *sigma, const uint8_t *region,
