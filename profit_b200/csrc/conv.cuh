@@ -191,4 +191,45 @@ inline cudaError_t launch_conv(const T *src, int sw, int sh, int ox, int oy, con
 	return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Autotuned dispatch.  The best tile (RY x TYT rows, KS column groups) depends
+// on the output size, the PSF size and the batch: a single 400x400 image needs
+// small tiles and many column groups to spread over 148 SMs, a batch of
+// thousands prefers large tiles with little halo.  The first call for a given
+// (type, sizes) key times every candidate that fits in shared memory with
+// CUDA events and caches the fastest; later calls (and CUDA-graph captures)
+// use the cached choice.
+// ---------------------------------------------------------------------------
+
+struct ConvArgs {
+	const void *src;
+	int sw, sh, ox, oy;
+	const void *K;
+	int kw, kh;
+	void *out;
+	int ow, oh;
+	const void *add;
+	int add_stride, add_ox, add_oy, batch, batch_src_stride, batch_out_stride;
+};
+
+template <class T, class Acc, class TOut, int RY, int TYT, int KS>
+struct ConvVariant {
+	static size_t smem(int kw, int kh) { return conv_smem_bytes<T, Acc, RY, TYT, KS>(kw, kh); }
+	static cudaError_t run(const ConvArgs &a, cudaStream_t s)
+	{
+		return launch_conv<T, Acc, TOut, RY, TYT, KS>(
+		    static_cast<const T *>(a.src), a.sw, a.sh, a.ox, a.oy, static_cast<const T *>(a.K), a.kw, a.kh,
+		    static_cast<TOut *>(a.out), a.ow, a.oh, static_cast<const T *>(a.add), a.add_stride, a.add_ox, a.add_oy,
+		    a.batch, a.batch_src_stride, a.batch_out_stride, s);
+	}
+};
+
+struct ConvCandidate {
+	size_t (*smem)(int, int);
+	cudaError_t (*run)(const ConvArgs &, cudaStream_t);
+};
+
+cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag, const ConvArgs &a,
+                           cudaStream_t s);
+
 }  // namespace pf

@@ -12,10 +12,13 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <string>
 #include <vector>
 
+#include "conv.cuh"
 #include "launch.h"
 #include "profit_b200.h"
 
@@ -24,6 +27,61 @@ using namespace pf;
 namespace pf {
 static std::atomic<unsigned long long> g_launches{0};
 void note_launches(int n) { g_launches += (unsigned long long)n; }
+
+cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag, const ConvArgs &a, cudaStream_t s)
+{
+	using Key = std::tuple<int, int, int, int, int, int, int, int>;
+	static std::mutex mu;
+	static std::map<Key, int> choice;
+	Key key{type_tag, a.sw, a.sh, a.kw, a.kh, a.ow, a.oh, a.batch};
+	int pick = -1;
+	{
+		std::lock_guard<std::mutex> g(mu);
+		auto it = choice.find(key);
+		if (it != choice.end()) pick = it->second;
+	}
+	if (pick < 0) {
+		cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+		cudaStreamIsCapturing(s, &cap);
+		int first_fit = -1;
+		for (int c = 0; c < n_cands; c++)
+			if (cands[c].smem(a.kw, a.kh) <= 227 * 1024) {
+				first_fit = c;
+				break;
+			}
+		if (first_fit < 0) return cudaErrorInvalidValue;
+		if (cap != cudaStreamCaptureStatusNone) {
+			pick = first_fit;  // no timing inside a capture
+		}
+		else {
+			cudaEvent_t e0, e1;
+			cudaEventCreate(&e0);
+			cudaEventCreate(&e1);
+			float best = 1e30f;
+			for (int c = 0; c < n_cands; c++) {
+				if (cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
+				cudaError_t e = cands[c].run(a, s);  // warm-up (and attribute setup)
+				if (e != cudaSuccess) continue;
+				cudaEventRecord(e0, s);
+				for (int r = 0; r < 3; r++) cands[c].run(a, s);
+				cudaEventRecord(e1, s);
+				if (cudaEventSynchronize(e1) != cudaSuccess) break;
+				float ms = 0;
+				cudaEventElapsedTime(&ms, e0, e1);
+				if (ms < best) {
+					best = ms;
+					pick = c;
+				}
+			}
+			cudaEventDestroy(e0);
+			cudaEventDestroy(e1);
+			if (pick < 0) pick = first_fit;
+			std::lock_guard<std::mutex> g(mu);
+			choice[key] = pick;
+		}
+	}
+	return cands[pick].run(a, s);
+}
 }  // namespace pf
 
 namespace {
@@ -241,6 +299,13 @@ struct pf_model {
 	std::vector<uint32_t> caps;
 	bool has_data = false, has_region = false;
 	unsigned data_w = 0, data_h = 0;
+
+	// captured FP32 likelihood+gradient pipeline (replayed while its signature holds)
+	cudaGraphExec_t graph_exec = nullptr;
+	std::vector<uint64_t> graph_sig;
+	unsigned long long graph_kernels = 0;
+	bool use_graphs = true;
+	int prof_begin_n = -1;
 
 	// debug output of the last evaluation
 	std::vector<int32_t> decisions;
@@ -636,6 +701,59 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	return PF_OK;
 }
 
+// Everything one FP32 evaluation puts on the stream, from the upload of the
+// staged profile scalars to the download of logL, tangent reductions and
+// queue counters.  Run eagerly, or captured once and replayed as a graph.
+int enqueue_fp32(pf_model *m, const Analysis &a, bool want_grad, size_t nres, QueueSet &q)
+{
+	size_t n = (size_t)a.n_profiles;
+	PF_CUDA(cudaEventRecord(m->ev[0], m->stream));
+	PF_CUDA(cudaMemcpyAsync(m->d_fprof.p, m->h_fprof.p, n * sizeof(FProfile), cudaMemcpyHostToDevice, m->stream));
+	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, m->stream));
+	PF_TRY(run_fp32(m, a, m->d_fprof.as<FProfile>(), q, want_grad, m->d_results.as<double>()));
+	char *hr = m->h_results.as<char>();
+	PF_CUDA(cudaMemcpyAsync(hr, m->d_results.p, nres * 8, cudaMemcpyDeviceToHost, m->stream));
+	PF_CUDA(cudaMemcpyAsync(hr + nres * 8, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, m->stream));
+	return PF_OK;
+}
+
+void drop_graph(pf_model *m)
+{
+	if (m->graph_exec) cudaGraphExecDestroy(m->graph_exec);
+	m->graph_exec = nullptr;
+	m->graph_sig.clear();
+}
+
+// What a captured graph depends on: sizes, queue layout and buffer addresses.
+std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_grad, const QueueSet &q)
+{
+	std::vector<uint64_t> s = {a.dw, a.dh, a.ow, a.oh, (uint64_t)a.n_profiles, (uint64_t)a.levels, a.conv,
+	                           (uint64_t)m->conv_kind, (uint64_t)m->precision, m->psf_w, m->psf_h, m->has_data,
+	                           m->has_region, want_grad};
+	for (int l = 0; l < a.levels; l++) s.push_back(((uint64_t)q.off[l] << 32) | q.cap[l]);
+	const DevBuf *bufs[] = {&m->d_fprof, &m->d_prof_begin, &m->d_prof_batch, &m->d_conv32, &m->d_plain32,
+	                        &m->d_model64, &m->d_conv64, &m->d_plain64, &m->d_jac, &m->d_gconv, &m->d_gplain,
+	                        &m->d_wseed, &m->d_items, &m->d_ctrl, &m->d_partials, &m->d_results, &m->d_psf32,
+	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region};
+	for (auto *b : bufs) s.push_back((uint64_t)(uintptr_t)b->p);
+	s.push_back((uint64_t)(uintptr_t)m->h_fprof.p);
+	s.push_back((uint64_t)(uintptr_t)m->h_results.p);
+	return s;
+}
+
+void finish_timings32(pf_model *m)
+{
+	cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
+	cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
+	if (m->has_data) {
+		cudaEventElapsedTime(&m->timings[3], m->ev[2], m->ev[3]);
+		cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[3]);
+	}
+	else {
+		cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[2]);
+	}
+}
+
 int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *results)
 {
 	PF_TRY(ensure_stream(m));
@@ -646,44 +764,77 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 	if (m->has_data && (m->data_w != a.ow || m->data_h != a.oh))
 		return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
 	PF_TRY(upload_psf(m));
-	PF_CUDA(cudaEventRecord(m->ev[0], m->stream));
-	PF_TRY(derive_and_upload(m, a, m->profiles, 0, 1, true));
 	int nprof = a.n_profiles;
+	// profile scalars, staged in pinned memory (the upload is part of the pipeline)
 	{
+		ModelGeom g = geometry(m, a);
+		PF_CUDA(ensure(m->h_prof, nprof * sizeof(DevProfile)));
+		PF_CUDA(ensure(m->d_prof, nprof * sizeof(DevProfile)));
+		PF_CUDA(ensure(m->h_fprof, nprof * sizeof(FProfile)));
+		PF_CUDA(ensure(m->d_fprof, nprof * sizeof(FProfile)));
+		DevProfile *hp = m->h_prof.as<DevProfile>();
+		FProfile *hf = m->h_fprof.as<FProfile>();
+		for (int i = 0; i < nprof; i++) {
+			derive_profile(m->profiles[i], g, hp[i]);
+			hf[i] = to_fprofile(hp[i], m->profiles[i]);
+		}
+	}
+	if (m->prof_begin_n != nprof) {
 		std::vector<int> begin = {0, nprof};
 		std::vector<int> batch(nprof, 0);
 		PF_CUDA(ensure(m->d_prof_begin, 2 * 4));
 		PF_CUDA(ensure(m->d_prof_batch, nprof * 4));
-		PF_CUDA(cudaMemcpyAsync(m->d_prof_begin.p, begin.data(), 8, cudaMemcpyHostToDevice, m->stream));
-		PF_CUDA(cudaMemcpyAsync(m->d_prof_batch.p, batch.data(), nprof * 4, cudaMemcpyHostToDevice, m->stream));
+		PF_CUDA(cudaMemcpy(m->d_prof_begin.p, begin.data(), 8, cudaMemcpyHostToDevice));
+		PF_CUDA(cudaMemcpy(m->d_prof_batch.p, batch.data(), nprof * 4, cudaMemcpyHostToDevice));
+		m->prof_begin_n = nprof;
 	}
 	size_t nres = ResultLayout::T0 + (size_t)nprof * NTAN;
 	PF_CUDA(ensure(m->d_results, nres * 8));
 	PF_CUDA(ensure(m->h_results, nres * 8 + CTRL_WORDS * 4));
 	size_t npix = (size_t)a.dw * a.dh;
+	char *hr = m->h_results.as<char>();
+
 	for (int attempt = 0; attempt < 8; attempt++) {
 		QueueSet q;
 		PF_TRY(prepare_queue(m, a, npix * nprof, q, nullptr, nullptr));
-		PF_TRY(run_fp32(m, a, m->d_fprof.as<FProfile>(), q, want_grad, m->d_results.as<double>()));
-		char *hr = m->h_results.as<char>();
-		PF_CUDA(cudaMemcpyAsync(hr, m->d_results.p, nres * 8, cudaMemcpyDeviceToHost, m->stream));
-		PF_CUDA(cudaMemcpyAsync(hr + nres * 8, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, m->stream));
+		bool replayed = false;
+		if (want_grad && m->graph_exec && m->graph_sig == graph_signature(m, a, want_grad, q)) {
+			PF_CUDA(cudaGraphLaunch(m->graph_exec, m->stream));
+			note_launches((int)m->graph_kernels);
+			replayed = true;
+		}
+		else {
+			PF_TRY(enqueue_fp32(m, a, want_grad, nres, q));
+		}
 		PF_CUDA(cudaStreamSynchronize(m->stream));
 		int retry = 0;
 		PF_TRY(check_overflow(m, a, reinterpret_cast<uint32_t *>(hr + nres * 8), retry));
-		if (!retry) {
-			if (results) results->assign(reinterpret_cast<double *>(hr), reinterpret_cast<double *>(hr) + nres);
-			cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
-			cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
-			if (m->has_data) {
-				cudaEventElapsedTime(&m->timings[3], m->ev[2], m->ev[3]);
-				cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[3]);
-			}
-			else {
-				cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[2]);
-			}
-			return PF_OK;
+		if (retry) {
+			drop_graph(m);
+			continue;
 		}
+		if (results) results->assign(reinterpret_cast<double *>(hr), reinterpret_cast<double *>(hr) + nres);
+		finish_timings32(m);
+		if (want_grad && !replayed && m->use_graphs) {
+			// capture the pipeline that just ran for the next evaluations
+			drop_graph(m);
+			unsigned long long before = g_launches.load();
+			cudaGraph_t graph = nullptr;
+			PF_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+			int st = enqueue_fp32(m, a, want_grad, nres, q);
+			cudaError_t ce = cudaStreamEndCapture(m->stream, &graph);
+			m->graph_kernels = g_launches.load() - before;
+			g_launches -= m->graph_kernels;
+			if (st == PF_OK && ce == cudaSuccess && graph) {
+				if (cudaGraphInstantiate(&m->graph_exec, graph, 0) == cudaSuccess)
+					m->graph_sig = graph_signature(m, a, want_grad, q);
+				else
+					m->graph_exec = nullptr;
+			}
+			if (graph) cudaGraphDestroy(graph);
+			cudaGetLastError();
+		}
+		return PF_OK;
 	}
 	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
 }
@@ -786,6 +937,7 @@ int pf_model_destroy(pf_model *m)
 	if (!m) return PF_OK;
 	cudaSetDevice(m->device);
 	if (m->stream) cudaStreamSynchronize(m->stream);
+	drop_graph(m);
 	for (auto &e : m->ev)
 		if (e) cudaEventDestroy(e);
 	if (m->stream) cudaStreamDestroy(m->stream);

@@ -336,6 +336,43 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 	}
 }
 
+// One SubItem integrated by one warp (s_xy: this warp's 32 doubles).
+__device__ __forceinline__ void level32_item(const FProfile *__restrict__ profiles, const SubItem &it, int level,
+                                             unsigned npix, float *__restrict__ img_conv,
+                                             float *__restrict__ img_plain, float *__restrict__ jac,
+                                             const QueueSet &q, double *s_xy, int lane)
+{
+	const FProfile &p = profiles[it.profile];
+	const unsigned res = it.res;
+	const double half_xbin = (it.x1 - it.x0) / res / 2., half_ybin = (it.y1 - it.y0) / res / 2.;
+	if (lane < 16) {
+		if (lane < (int)res) s_xy[lane] = it.x0 + (2 * lane + 1) * half_xbin;
+	}
+	else if (lane - 16 < (int)res) {
+		s_xy[lane] = it.y0 + (2 * (lane - 16) + 1) * half_ybin;
+	}
+	__syncwarp();
+	float sums[NTAN];
+#pragma unroll
+	for (int k = 0; k < NTAN; k++) sums[k] = 0.f;
+	if (level >= 3) level_points<double>(p, it, level, s_xy, lane, q, sums);
+	else level_points<float>(p, it, level, s_xy, lane, q, sums);
+#pragma unroll
+	for (int k = 0; k < NTAN; k++) sums[k] = warp_sum(sums[k]);
+	if (lane == 0) {
+		const float wgt = (float)it.weight;
+		const uint32_t b = it.pixel / npix, pix = it.pixel - b * npix;
+		float *img = p.target == 0 ? img_conv : img_plain;
+		atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)sums[0]));
+		if (jac) {
+			float *jp = jac + (size_t)it.profile * NTAN * npix + pix;
+#pragma unroll
+			for (int k = 0; k < NTAN; k++) atomicAdd(&jp[(size_t)k * npix], wgt * sums[k]);
+		}
+	}
+	__syncwarp();
+}
+
 __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
                                                  float *__restrict__ img_conv, float *__restrict__ img_plain,
                                                  float *__restrict__ jac, QueueSet q)
@@ -346,38 +383,29 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
 	const uint32_t n = min(q.counts[level], q.cap[level]);
 	const SubItem *items = q.items + q.off[level];
 	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < n; w += nwarps)
+		level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane);
+}
 
-	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < n; w += nwarps) {
-		const SubItem it = items[w];
-		const FProfile &p = profiles[it.profile];
-		const unsigned res = it.res;
-		const double half_xbin = (it.x1 - it.x0) / res / 2., half_ybin = (it.y1 - it.y0) / res / 2.;
-		if (lane < 16) {
-			if (lane < (int)res) s_xy[wib][lane] = it.x0 + (2 * lane + 1) * half_xbin;
-		}
-		else if (lane - 16 < (int)res) {
-			s_xy[wib][lane] = it.y0 + (2 * (lane - 16) + 1) * half_ybin;
-		}
-		__syncwarp();
-		float sums[NTAN];
-#pragma unroll
-		for (int k = 0; k < NTAN; k++) sums[k] = 0.f;
-		if (level >= 3) level_points<double>(p, it, level, s_xy[wib], lane, q, sums);
-		else level_points<float>(p, it, level, s_xy[wib], lane, q, sums);
-#pragma unroll
-		for (int k = 0; k < NTAN; k++) sums[k] = warp_sum(sums[k]);
-		if (lane == 0) {
-			const float wgt = (float)it.weight;
-			const uint32_t b = it.pixel / npix, pix = it.pixel - b * npix;
-			float *img = p.target == 0 ? img_conv : img_plain;
-			atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)sums[0]));
-			if (jac) {
-				float *jp = jac + (size_t)it.profile * NTAN * npix + pix;
-#pragma unroll
-				for (int k = 0; k < NTAN; k++) atomicAdd(&jp[(size_t)k * npix], wgt * sums[k]);
-			}
-		}
-		__syncwarp();
+// Levels first..levels-1 in one CTA.  Only the Sersic central cusp
+// (max_recursions = 10) reaches these levels, a few hundred cells per level
+// at most, so one block walks them in order; __syncthreads separates the
+// levels, which makes every push of level L visible before level L+1 is read.
+__global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restrict__ profiles, int first, int levels,
+                                                        unsigned npix, float *__restrict__ img_conv,
+                                                        float *__restrict__ img_plain, float *__restrict__ jac,
+                                                        QueueSet q)
+{
+	__shared__ double s_xy[16][32];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	const uint32_t nwarps = blockDim.x >> 5;
+	for (int level = first; level < levels; level++) {
+		__syncthreads();
+		const uint32_t n = min(*(volatile uint32_t *)&q.counts[level], q.cap[level]);
+		const SubItem *items = q.items + q.off[level];
+		for (uint32_t w = wib; w < n; w += nwarps)
+			level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane);
 	}
 }
 
@@ -460,8 +488,13 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
                             float *jac, const QueueSet &q, cudaStream_t s)
 {
-	for (int l = 0; l < n_levels; l++) k_level32<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, q);
-	note_launches(n_levels);
+	const int wide = n_levels < 3 ? n_levels : 3;
+	for (int l = 0; l < wide; l++) k_level32<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, q);
+	note_launches(wide);
+	if (n_levels > wide) {
+		k_deep_levels32<<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, q);
+		note_launches(1);
+	}
 	return cudaGetLastError();
 }
 
@@ -493,11 +526,18 @@ static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, 
                               int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
 {
 	note_launches(1);
-	if (conv_smem_bytes<float, double, 8, 4, 4>(kw, kh) <= 227 * 1024)
-		return launch_conv<float, double, TOut, 8, 4, 4>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride,
-		                                                 add_ox, add_oy, batch, batch_src_stride, batch_out_stride, s);
-	return launch_conv<float, double, TOut, 4, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride,
-	                                                 add_ox, add_oy, batch, batch_src_stride, batch_out_stride, s);
+	static const ConvCandidate cands[] = {
+	    {ConvVariant<float, double, TOut, 8, 4, 4>::smem, ConvVariant<float, double, TOut, 8, 4, 4>::run},
+	    {ConvVariant<float, double, TOut, 8, 1, 8>::smem, ConvVariant<float, double, TOut, 8, 1, 8>::run},
+	    {ConvVariant<float, double, TOut, 8, 2, 4>::smem, ConvVariant<float, double, TOut, 8, 2, 4>::run},
+	    {ConvVariant<float, double, TOut, 4, 2, 8>::smem, ConvVariant<float, double, TOut, 4, 2, 8>::run},
+	    {ConvVariant<float, double, TOut, 16, 2, 2>::smem, ConvVariant<float, double, TOut, 16, 2, 2>::run},
+	    {ConvVariant<float, double, TOut, 8, 4, 1>::smem, ConvVariant<float, double, TOut, 8, 4, 1>::run},
+	    {ConvVariant<float, double, TOut, 4, 4, 2>::smem, ConvVariant<float, double, TOut, 4, 4, 2>::run},
+	};
+	ConvArgs a{src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
+	           batch_src_stride, batch_out_stride};
+	return conv_autotuned(cands, (int)(sizeof(cands) / sizeof(cands[0])), sizeof(TOut) == 8 ? 2 : 1, a, s);
 }
 
 cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,

@@ -80,19 +80,13 @@ __global__ void k_pixels64(const DevProfile *__restrict__ profiles, int n_profil
 	img_plain[pix] = acc[1];
 }
 
-// One warp per SubItem of `level`.
-__global__ void __launch_bounds__(256) k_level64(const DevProfile *__restrict__ profiles, int level, double *__restrict__ img_conv,
-                          double *__restrict__ img_plain, QueueSet q)
+// One SubItem of `level` integrated by one warp (s_xy: the warp's 32 doubles).
+__device__ __forceinline__ void level64_item(const DevProfile *__restrict__ profiles, const SubItem it, int level,
+                                             double *__restrict__ img_conv, double *__restrict__ img_plain,
+                                             const QueueSet &q, double *s_xy_w, int lane)
 {
-	__shared__ double s_xy[8][32];
-	const int lane = threadIdx.x & 31;
-	const int wib = threadIdx.x >> 5;
-	const uint32_t n = min(q.counts[level], q.cap[level]);
-	const SubItem *items = q.items + q.off[level];
-	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-
-	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < n; w += nwarps) {
-		const SubItem it = items[w];
+		double(*s_xy)[32] = reinterpret_cast<double(*)[32]>(s_xy_w);
+		const int wib = 0;
 		const DevProfile &d = profiles[it.profile];
 		const unsigned res = it.res;
 		const double xbin = (it.x1 - it.x0) / res;
@@ -161,6 +155,38 @@ __global__ void __launch_bounds__(256) k_level64(const DevProfile *__restrict__ 
 			atomicAdd(&img[it.pixel], it.weight * sum);
 		}
 		__syncwarp();
+}
+
+__global__ void __launch_bounds__(256) k_level64(const DevProfile *__restrict__ profiles, int level,
+                                                 double *__restrict__ img_conv, double *__restrict__ img_plain,
+                                                 QueueSet q)
+{
+	__shared__ double s_xy[8][32];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	const uint32_t n = min(q.counts[level], q.cap[level]);
+	const SubItem *items = q.items + q.off[level];
+	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < n; w += nwarps)
+		level64_item(profiles, items[w], level, img_conv, img_plain, q, s_xy[wib], lane);
+}
+
+// Levels first..levels-1 in one CTA (the Sersic central cusp only); see
+// k_deep_levels32 in render32.cu.
+__global__ void __launch_bounds__(512) k_deep_levels64(const DevProfile *__restrict__ profiles, int first, int levels,
+                                                        double *__restrict__ img_conv, double *__restrict__ img_plain,
+                                                        QueueSet q)
+{
+	__shared__ double s_xy[16][32];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	const uint32_t nwarps = blockDim.x >> 5;
+	for (int level = first; level < levels; level++) {
+		__syncthreads();
+		const uint32_t n = min(*(volatile uint32_t *)&q.counts[level], q.cap[level]);
+		const SubItem *items = q.items + q.off[level];
+		for (uint32_t w = wib; w < n; w += nwarps)
+			level64_item(profiles, items[w], level, img_conv, img_plain, q, s_xy[wib], lane);
 	}
 }
 
@@ -271,10 +297,13 @@ cudaError_t launch_pixels64(const DevProfile *profiles, int n_profiles, unsigned
 cudaError_t launch_levels64(const DevProfile *profiles, int n_levels, double *img_conv, double *img_plain,
                             const QueueSet &q, cudaStream_t s)
 {
-	for (int l = 0; l < n_levels; l++) {
-		k_level64<<<148 * 8, 256, 0, s>>>(profiles, l, img_conv, img_plain, q);
+	const int wide = n_levels < 3 ? n_levels : 3;
+	for (int l = 0; l < wide; l++) k_level64<<<148 * 8, 256, 0, s>>>(profiles, l, img_conv, img_plain, q);
+	note_launches(wide);
+	if (n_levels > wide) {
+		k_deep_levels64<<<1, 512, 0, s>>>(profiles, wide, n_levels, img_conv, img_plain, q);
+		note_launches(1);
 	}
-	note_launches(n_levels);
 	return cudaGetLastError();
 }
 
@@ -300,11 +329,15 @@ cudaError_t launch_conv64(const double *src, int sw, int sh, int ox, int oy, con
                           cudaStream_t s)
 {
 	note_launches(1);
-	if (conv_smem_bytes<double, double, 8, 4, 2>(kw, kh) <= 227 * 1024)
-		return launch_conv<double, double, double, 8, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add,
-		                                                    add_stride, add_ox, add_oy, 1, 0, 0, s);
-	return launch_conv<double, double, double, 4, 4, 2>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride,
-	                                                    add_ox, add_oy, 1, 0, 0, s);
+	static const ConvCandidate cands[] = {
+	    {ConvVariant<double, double, double, 8, 4, 2>::smem, ConvVariant<double, double, double, 8, 4, 2>::run},
+	    {ConvVariant<double, double, double, 8, 1, 8>::smem, ConvVariant<double, double, double, 8, 1, 8>::run},
+	    {ConvVariant<double, double, double, 4, 2, 8>::smem, ConvVariant<double, double, double, 4, 2, 8>::run},
+	    {ConvVariant<double, double, double, 8, 2, 4>::smem, ConvVariant<double, double, double, 8, 2, 4>::run},
+	    {ConvVariant<double, double, double, 4, 4, 2>::smem, ConvVariant<double, double, double, 4, 4, 2>::run},
+	};
+	ConvArgs a{src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, 1, 0, 0};
+	return conv_autotuned(cands, (int)(sizeof(cands) / sizeof(cands[0])), 3, a, s);
 }
 
 cudaError_t launch_loglike64(const double *model, const double *data, const double *sigma, const uint8_t *region,
