@@ -101,6 +101,17 @@ int set_error(int code, const std::string &msg)
 			return set_error(PF_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
 	} while (0)
 
+// Timing events must become graph nodes when the stream is being captured
+// (a plain record there only orders work); outside a capture the external
+// flag is not allowed.
+cudaError_t record_event(cudaEvent_t e, cudaStream_t s)
+{
+	cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+	cudaStreamIsCapturing(s, &st);
+	if (st == cudaStreamCaptureStatusActive) return cudaEventRecordWithFlags(e, s, cudaEventRecordExternal);
+	return cudaEventRecord(e, s);
+}
+
 #define PF_TRY(expr)          \
 	do {                      \
 		int st_ = (expr);     \
@@ -550,7 +561,7 @@ int run_plain64(pf_model *m, const Analysis &a, const DevProfile *dprof, QueueSe
 	}
 	PF_CUDA(launch_levels64(dprof, a.levels, conv, plain, q, m->stream));
 	if (q.decisions) PF_CUDA(launch_count_decisions(q, a.levels, npix, m->stream));
-	PF_CUDA(cudaEventRecordWithFlags(m->ev[1], m->stream, cudaEventRecordExternal));
+	PF_CUDA(record_event(m->ev[1], m->stream));
 
 	double *model = m->d_model64.as<double>();
 	if (a.conv && m->conv_kind != CONV_NULL) {
@@ -565,7 +576,7 @@ int run_plain64(pf_model *m, const Analysis &a, const DevProfile *dprof, QueueSe
 		PF_CUDA(cudaMemcpyAsync(conv, model, (size_t)a.cw * a.ch * 8, cudaMemcpyDeviceToDevice, m->stream));
 		PF_CUDA(launch_downsample64(conv, a.cw, a.ch, m->fs, model, a.ow, a.oh, m->stream));
 	}
-	PF_CUDA(cudaEventRecordWithFlags(m->ev[2], m->stream, cudaEventRecordExternal));
+	PF_CUDA(record_event(m->ev[2], m->stream));
 	return PF_OK;
 }
 
@@ -590,7 +601,7 @@ int evaluate64(pf_model *m, Analysis &a)
 	PF_TRY(ensure_stream(m));
 	PF_TRY(analyze(m, a));
 	PF_TRY(upload_psf(m));
-	PF_CUDA(cudaEventRecordWithFlags(m->ev[0], m->stream, cudaEventRecordExternal));
+	PF_CUDA(record_event(m->ev[0], m->stream));
 	PF_TRY(derive_and_upload(m, a, m->profiles, 0, 1, false));
 	size_t npix = (size_t)a.dw * a.dh;
 	PF_CUDA(ensure(m->h_ctrl, CTRL_WORDS * 4));
@@ -647,7 +658,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), 1, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain,
 	                        jac, q, m->stream));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, m->stream));
-	PF_CUDA(cudaEventRecordWithFlags(m->ev[1], m->stream, cudaEventRecordExternal));
+	PF_CUDA(record_event(m->ev[1], m->stream));
 	// The forward model image is kept in FP64: the residual (data - model) of
 	// bright pixels is a small difference of large numbers.
 	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
@@ -671,7 +682,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		                           a.cw, a.ch, plain, a.dw, a.padx, a.pady, 1, 0, 0, m->stream));
 	}
 	(void)model;
-	PF_CUDA(cudaEventRecordWithFlags(m->ev[2], m->stream, cudaEventRecordExternal));
+	PF_CUDA(record_event(m->ev[2], m->stream));
 	if (!m->has_data) return PF_OK;
 	PF_CUDA(ensure(m->d_partials, NPARTS * sizeof(double2)));
 	float *wseed = nullptr;
@@ -698,7 +709,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix,
 		                          d_out + ResultLayout::T0, m->stream));
 	}
-	PF_CUDA(cudaEventRecordWithFlags(m->ev[3], m->stream, cudaEventRecordExternal));
+	PF_CUDA(record_event(m->ev[3], m->stream));
 	return PF_OK;
 }
 
@@ -708,7 +719,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 int enqueue_fp32(pf_model *m, const Analysis &a, bool want_grad, size_t nres, QueueSet &q)
 {
 	size_t n = (size_t)a.n_profiles;
-	PF_CUDA(cudaEventRecordWithFlags(m->ev[0], m->stream, cudaEventRecordExternal));
+	PF_CUDA(record_event(m->ev[0], m->stream));
 	PF_CUDA(cudaMemcpyAsync(m->d_fprof.p, m->h_fprof.p, n * sizeof(FProfile), cudaMemcpyHostToDevice, m->stream));
 	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, m->stream));
 	PF_TRY(run_fp32(m, a, m->d_fprof.as<FProfile>(), q, want_grad, m->d_results.as<double>()));
@@ -1252,7 +1263,7 @@ int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_para
 	PF_CUDA(ensure(m->d_results, (size_t)n_eval * 8));
 	PF_CUDA(ensure(m->h_results, (size_t)n_eval * 8 + CTRL_WORDS * 4 * n_eval));
 	for (int attempt = 0; attempt < 8; attempt++) {
-		PF_CUDA(cudaEventRecordWithFlags(m->ev[0], m->stream, cudaEventRecordExternal));
+		PF_CUDA(record_event(m->ev[0], m->stream));
 		for (int e = 0; e < n_eval; e++) PF_TRY(derive_and_upload(m, a, sets[e], e, n_eval, false));
 		uint32_t *hctrl = reinterpret_cast<uint32_t *>(m->h_results.as<char>() + (size_t)n_eval * 8);
 		for (int e = 0; e < n_eval; e++) {
@@ -1267,7 +1278,7 @@ int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_para
 		}
 		PF_CUDA(cudaMemcpyAsync(m->h_results.p, m->d_results.p, (size_t)n_eval * 8, cudaMemcpyDeviceToHost,
 		                        m->stream));
-		PF_CUDA(cudaEventRecordWithFlags(m->ev[3], m->stream, cudaEventRecordExternal));
+		PF_CUDA(record_event(m->ev[3], m->stream));
 		PF_CUDA(cudaStreamSynchronize(m->stream));
 		int retry = 0;
 		for (int e = 0; e < n_eval; e++) {

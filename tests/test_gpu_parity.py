@@ -155,6 +155,30 @@ def _gradient_case(wl, offset_scale):
     return m, w2
 
 
+def test_graph_replay_matches_fresh_evaluation():
+    """After the first call the FP32 pipeline is replayed from a CUDA graph;
+    every proposal must give what a fresh model (first, eager call) gives."""
+    wl = W.bulge_disk_ps(width=200, height=180, psf_size=25)
+    m64 = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = m64.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    m = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
+    m.set_data(image, sigma)
+    refs = wl["grad"]
+    for s in range(4):
+        w2 = W.perturbed(wl, seed=100 + s, scale=0.02)
+        vals = [w2["profiles"][i][1][k] for (i, k) in refs]
+        m.set_parameters(refs, vals)
+        ll, g = m.loglike_grad(refs)
+        fresh = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), w2)
+        fresh.set_data(image, sigma)
+        ll_f, g_f = fresh.loglike_grad(refs)
+        assert ll == pytest.approx(ll_f, rel=1e-12)
+        np.testing.assert_allclose(g, g_f, rtol=1e-5, atol=1e-6 * np.max(np.abs(g_f)))
+        t = m.last_timings()
+        assert t[0] > 0 and t[0] < 1e3
+
+
 def test_adjoint_gradient_matches_fd64():
     wl = W.bulge_disk_ps()
     m, w2 = _gradient_case(wl, 0.02)
