@@ -304,6 +304,8 @@ def main_b200(args):
             "algorithmic": f"2*P^2*W*H = {flop:.3e} FLOP per launch (P={P}, W*H={n_out})",
             "peak_source": "measured: dependent FMA streams, libpf_peaks.so, best of 5 (burst)"}
 
+    sampler = sampler_batch_rate(args, torch, flush)
+
     out = None
     if rank == 0:
         per_step_in = 8 * len(refs) + 16 * len(refs)  # values + parameter references
@@ -323,6 +325,7 @@ def main_b200(args):
             "accuracy": accuracy,
             "plain_fp64_fd": {"value": fp64_fd_value, "unit": UNIT,
                               "speedup_fp32_adjoint": (world * args.steps / dev_total) / fp64_fd_value},
+            "sampler_batch": sampler,
         }
     m.close()
     if world > 1:
@@ -331,6 +334,48 @@ def main_b200(args):
         if not args.no_cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline(wl, image, sigma)
         print(json.dumps(out), flush=True)
+
+
+def sampler_batch_rate(args, torch, flush, n=4096, calls=3):
+    """4096 proposals of the single-Sersic model (200x200, 31x31 PSF) per
+    call, logL + 8-parameter adjoint gradient; compared with the plain FP64
+    form and FD on the same model.  Reported beside the headline metric."""
+    from profit_b200 import PF_FP32, PF_FP64, Model
+    from profit_b200 import workloads as W
+    wl, vals = W.sampler_batch(n)
+    refs = wl["grad"]
+    m = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = m.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    m.set_data(image, sigma)
+    fd = []
+    for s in range(4):
+        m.set_parameters(refs, vals[s])
+        m.loglike_grad_fd(refs, rel_step=1e-7)
+        if s >= 1:
+            fd.append(m.last_timings()[0])
+    fd_rate = 1e3 / statistics.mean(fd)
+    m.set_precision(PF_FP32)
+    m.loglike_grad_batch(refs, vals)  # warm-up: tuning, queue sizing, graph capture
+    times = []
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    for _ in range(calls):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        ll, g = m.loglike_grad_batch(refs, vals)
+        ev1.record()
+        ev1.synchronize()
+        times.append(ev0.elapsed_time(ev1) / 1e3)
+    m.close()
+    rate = n / statistics.mean(times)
+    return {"workload": "single Sersic 200x200, 31x31 Gaussian PSF, brute force, 8-parameter gradient; "
+                        f"{n} proposals init + N(0, 0.05|init|) per call through pf_model_loglike_grad_batch "
+                        "(host parameters in, logL + gradients out)",
+            "value": rate, "unit": UNIT, "ms_per_call": 1e3 * statistics.mean(times),
+            "plain_fp64_fd_value": fd_rate, "speedup_vs_plain_fp64_fd": rate / fd_rate,
+            "finite_fraction": float(np.isfinite(ll).mean())}
 
 
 def measured_fp32_peak():

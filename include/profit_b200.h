@@ -153,6 +153,18 @@ int pf_model_set_parameters(pf_model *m, const pf_param_ref *params, int n_param
 int pf_model_loglike_grad(pf_model *m, const pf_param_ref *params, int n_params,
                           double *loglike, double *grad);
 
+/* Batched proposals (new): logL[b] and grad[b][i] = d logL / d params[i] for
+ * `batch` proposals, proposal b being this model with params[i] set to
+ * values[b * n_params + i].  All proposals share the model's structure, PSF
+ * and data (a sampler's population or a batch of MCMC candidates).  The
+ * FP64 scalar prologue runs on the device; proposals are processed in chunks
+ * that fit a memory budget, each chunk's pipeline replayed from a CUDA graph.
+ * A proposal that fails libprofit's parameter validation gets
+ * logL = -INFINITY and a zero gradient instead of failing the call.  `grad`
+ * may be NULL. */
+int pf_model_loglike_grad_batch(pf_model *m, const pf_param_ref *params, int n_params, int batch,
+                                const double *values, double *loglike, double *grad);
+
 /* Same quantities by central finite differences of the plain form (FP64),
  * 2*n_params + 1 evaluations with relative step `rel_step` (absolute step
  * rel_step*max(|p|, 1)); the baseline that pf_model_loglike_grad replaces. */

@@ -123,6 +123,7 @@ def check(status: int) -> None:
 
 def _late_bindings(L):
     L.pf_model_set_parameters.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, _dp]
+    L.pf_model_loglike_grad_batch.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, C.c_int, _dp, _dp, _dp]
 
 
-EXPORTED = EXPORTED + ("pf_model_set_parameters",)
+EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch")

@@ -52,6 +52,77 @@ struct FProfile {
 	double cx, cy, img_sx, img_sy, flux_scale64;
 };
 
+PF_HD inline FProfile to_fprofile(const DevProfile &d, const ProfileParams &p)
+{
+	FProfile f = {};
+	f.kind = d.kind;
+	f.target = d.target;
+	f.rough = d.rough;
+	f.centre_override = d.centre_override;
+	f.resolution = d.resolution;
+	f.max_rec = d.max_rec;
+	f.cos_ang = (float)d.cos_ang;
+	f.sin_ang = (float)d.sin_ang;
+	f.cos_q = (float)d.cos_q;
+	f.sin_q = (float)d.sin_q;
+	f.r_switch = (float)d.r_switch;
+	f.r_max = (float)d.r_max;
+	f.acc = (float)d.acc;
+	f.re = (float)d.re;
+	f.nser = (float)d.nser;
+	f.bn = (float)d.bn;
+	f.B = (float)(p.box + 2);
+	f.inv_nB = (float)(1.0 / (p.nser * (p.box + 2)));
+	f.dbn_dn = (float)d.dbn_dn;
+	f.rscale = (float)d.rscale;
+	f.con = (float)d.con;
+	f.a = (float)d.a;
+	f.b = (float)d.b;
+	f.rb = (float)d.rb;
+	f.rc = (float)d.rc;
+	f.rt = (float)d.rt;
+	f.h1 = (float)d.h1;
+	f.h2 = (float)d.h2;
+	f.king_t = (float)d.king_t;
+	f.flux_scale = (float)d.flux_scale;
+	f.flux_scale64 = d.flux_scale;
+	f.cx = d.cx;
+	f.cy = d.cy;
+	f.img_sx = d.img_sx;
+	f.img_sy = d.img_sy;
+	if (d.kind == PK_SKY) f.flux_scale = (float)d.bg;
+	if (d.kind == PK_MOFFAT) {
+		// Moffat keeps 1/fwhm and d ln(rscale)/d con in the a, b slots
+		double c = p.con, t = pow(2.0, 1.0 / c);
+		f.a = (float)(1.0 / p.fwhm);
+		f.b = (float)(0.5 * t * log(2.0) / (c * c * (t - 1.0)));
+	}
+	return f;
+}
+
+// Parameters with a hand-written adjoint, and how their derivative is
+// assembled from the tangent reductions T[0..8] of the render pass:
+//   x' = dx c + dy s,  y' = (-dx s + dy c)/q,  theta = (ang + 90) pi/180,
+//   d x'/d xcen = -c, d y'/d xcen = s/q, d x'/d ycen = -s, d y'/d ycen = -c/q,
+//   d x'/d theta = q y', d y'/d theta = -x'/q, d y'/d q = -y'/q,
+// and flux_scale F carries d ln F / d(mag, q, box, shape) from the prologue.
+enum GradCode : int32_t { G_XCEN = 0, G_YCEN, G_MAG, G_ANG, G_AXRAT, G_BOX, G_SHAPE1, G_SHAPE2 };
+
+PF_HD inline double gradient_from_tangents(int code, double axrat, const DevProfile &d, const double *T)
+{
+	const double F = d.flux_scale, q = axrat, c = d.cos_ang, s = d.sin_ang;
+	switch (code) {
+	case G_XCEN: return F * (-c * T[1] + (s / q) * T[2]);
+	case G_YCEN: return F * (-s * T[1] - (c / q) * T[2]);
+	case G_MAG: return F * d.dlnI_dmag * T[0];
+	case G_ANG: return F * (M_PI / 180.0) * (q * T[3] - T[4] / q);
+	case G_AXRAT: return F * (-T[5] / q + d.dlnI_dq * T[0]);
+	case G_BOX: return F * (T[8] + d.dlnI_dbox * T[0]);
+	case G_SHAPE1: return F * (T[6] + d.dlnI_dp1 * T[0]);
+	default: return F * (T[7] + d.dlnI_dp2 * T[0]);
+	}
+}
+
 __device__ __forceinline__ uint32_t warp_push(uint32_t *counter)
 {
 	uint32_t mask = __activemask();

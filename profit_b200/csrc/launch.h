@@ -62,3 +62,16 @@ cudaError_t launch_loglike64_seed(const double *model, const double *data, const
                                   const uint8_t *region, int n, double2 *partials, int nparts, double *out,
                                   float *wseed, cudaStream_t s);
 }  // namespace pf
+
+namespace pf {
+// render32.cu: batched proposals
+cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batch, const int *ref_profile,
+                                  const int *ref_offset, int nrefs, const double *values, const ModelGeom &g,
+                                  DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s);
+cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, const int *ref_profile,
+                                  const int *ref_code, int nrefs, const double *T, const double *ll,
+                                  const int *invalid, double *out_ll, double *out_grad, cudaStream_t s);
+cudaError_t launch_loglike64_batch(const double *model, const double *data, const double *sigma,
+                                   const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
+                                   int nparts, double *out, float *wseed, cudaStream_t s);
+}  // namespace pf

@@ -282,6 +282,8 @@ struct ResultLayout {
 
 }  // namespace
 
+struct BatchState;
+
 struct pf_model {
 	unsigned width, height;
 	std::vector<ProfileParams> profiles;
@@ -317,6 +319,7 @@ struct pf_model {
 	unsigned long long graph_kernels = 0;
 	bool use_graphs = true;
 	int prof_begin_n = -1;
+	BatchState *batch = nullptr;
 
 	// debug output of the last evaluation
 	std::vector<int32_t> decisions;
@@ -388,54 +391,6 @@ ModelGeom geometry(const pf_model *m, const Analysis &a)
 	g.offy = a.pady;
 	g.finesampling = m->fs;
 	return g;
-}
-
-FProfile to_fprofile(const DevProfile &d, const ProfileParams &p)
-{
-	FProfile f;
-	std::memset(&f, 0, sizeof(f));
-	f.kind = d.kind;
-	f.target = d.target;
-	f.rough = d.rough;
-	f.centre_override = d.centre_override;
-	f.resolution = d.resolution;
-	f.max_rec = d.max_rec;
-	f.cos_ang = (float)d.cos_ang;
-	f.sin_ang = (float)d.sin_ang;
-	f.cos_q = (float)d.cos_q;
-	f.sin_q = (float)d.sin_q;
-	f.r_switch = (float)d.r_switch;
-	f.r_max = (float)d.r_max;
-	f.acc = (float)d.acc;
-	f.re = (float)d.re;
-	f.nser = (float)d.nser;
-	f.bn = (float)d.bn;
-	f.B = (float)(p.box + 2);
-	f.inv_nB = (float)(1.0 / (p.nser * (p.box + 2)));
-	f.dbn_dn = (float)d.dbn_dn;
-	f.rscale = (float)d.rscale;
-	f.con = (float)d.con;
-	f.a = (float)d.a;
-	f.b = (float)d.b;
-	f.rb = (float)d.rb;
-	f.rc = (float)d.rc;
-	f.rt = (float)d.rt;
-	f.h1 = (float)d.h1;
-	f.h2 = (float)d.h2;
-	f.king_t = (float)d.king_t;
-	f.flux_scale = (float)d.flux_scale;
-	f.flux_scale64 = d.flux_scale;
-	f.cx = d.cx;
-	f.cy = d.cy;
-	f.img_sx = d.img_sx;
-	f.img_sy = d.img_sy;
-	if (d.kind == PK_SKY) f.flux_scale = (float)d.bg;
-	if (d.kind == PK_MOFFAT) {
-		double c = p.con, t = std::pow(2.0, 1.0 / c);
-		f.a = (float)(1.0 / p.fwhm);
-		f.b = (float)(0.5 * t * std::log(2.0) / (c * c * (t - 1.0)));
-	}
-	return f;
 }
 
 int upload_psf(pf_model *m)
@@ -853,28 +808,277 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 }
 
 // d logL / d parameter from the tangent reductions T[0..8] of one profile.
-int combine_gradient(const ProfileParams &p, const DevProfile &d, const double *T, const char *name, double &g)
+int gradient_code(const ProfileParams &p, const char *name, int &code);
+int check_profile(pf_model *m, int index);
+
+// ---------------------------------------------------------------------------
+// Batched FP32 likelihood + adjoint gradient: B proposals of the model (its
+// profiles with the listed parameters replaced by values[b][.]), all against
+// the model's data.  The scalar prologue runs on the device, proposals are
+// processed in chunks that fit the memory budget, and each chunk's pipeline
+// is replayed from a CUDA graph after its first run.
+// ---------------------------------------------------------------------------
+
+}  // namespace
+
+struct BatchState {
+	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out_ll, d_out_grad, d_ll, d_T;
+	HostBuf h_tmpl, h_values, h_out;
+	int refs_n = -1, chunk = 0;
+	std::vector<int> refs_host;
+	cudaGraphExec_t graph = nullptr;
+	std::vector<uint64_t> sig;
+	unsigned long long graph_kernels = 0;
+	~BatchState()
+	{
+		if (graph) cudaGraphExecDestroy(graph);
+	}
+};
+
+namespace {
+
+constexpr size_t BATCH_BUDGET_BYTES = 24ull << 30;
+
+int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, int nrefs, const QueueSet &q)
 {
-	const double F = d.flux_scale, q = p.axrat, c = d.cos_ang, s = d.sin_ang;
-	const double deg = M_PI / 180.0;
+	const int nprof = a.n_profiles;
+	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
+	cudaStream_t s = m->stream;
+	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *jac = m->d_jac.as<float>();
+	double *model64 = m->d_model64.as<double>();
+	float *wseed = m->d_wseed.as<float>(), *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>();
+	const int *ref_profile = bs.d_refs.as<int>(), *ref_offset = ref_profile + nrefs, *ref_code = ref_offset + nrefs;
+
+	PF_CUDA(record_event(m->ev[0], s));
+	PF_CUDA(cudaMemcpyAsync(bs.d_tmpl.p, bs.h_tmpl.p, nprof * sizeof(ProfileParams), cudaMemcpyHostToDevice, s));
+	PF_CUDA(cudaMemcpyAsync(bs.d_values.p, bs.h_values.p, (size_t)C * nrefs * 8, cudaMemcpyHostToDevice, s));
+	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, s));
+	PF_CUDA(cudaMemsetAsync(bs.d_invalid.p, 0, (size_t)C * 4, s));
+	PF_CUDA(cudaMemsetAsync(bs.d_T.p, 0, (size_t)C * nprof * NTAN * 8, s));
+	PF_CUDA(launch_batch_prologue(bs.d_tmpl.as<ProfileParams>(), nprof, C, ref_profile, ref_offset, nrefs,
+	                              bs.d_values.as<double>(), geometry(m, a), bs.d_dev.as<DevProfile>(),
+	                              m->d_fprof.as<FProfile>(), bs.d_invalid.as<int>(), s));
+	const FProfile *fprof = m->d_fprof.as<FProfile>();
+	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx, m->sy, conv, plain, jac, q, s));
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, s));
+	PF_CUDA(record_event(m->ev[1], s));
+	if (a.conv && m->conv_kind != CONV_NULL) {
+		PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64,
+		                           a.cw, a.ch, plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout, s));
+	}
+	else {
+		PF_CUDA(launch_widen(conv, m->d_conv64.as<double>(), npix * C, s));
+		PF_CUDA(launch_widen(plain, m->d_plain64.as<double>(), npix * C, s));
+		for (int b = 0; b < C; b++)
+			PF_CUDA(launch_crop64(m->d_conv64.as<double>() + b * npix, a.dw, a.padx, a.pady, model64 + b * nout, a.cw,
+			                      a.ch, m->d_plain64.as<double>() + b * npix, s));
+	}
+	PF_CUDA(record_event(m->ev[2], s));
+	PF_CUDA(launch_loglike64_batch(model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
+	                               m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout, C, 0,
+	                               m->d_partials.as<double2>(), NPARTS, bs.d_ll.as<double>(), wseed, s));
+	PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
+	if (a.conv && m->conv_kind != CONV_NULL)
+		PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(),
+		                      m->psf_w, m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix, s));
+	else
+		gconv = gplain;
+	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix,
+	                          bs.d_T.as<double>(), s));
+	PF_CUDA(launch_batch_gradient(bs.d_dev.as<DevProfile>(), nprof, C, ref_profile, ref_code, nrefs,
+	                              bs.d_T.as<double>(), bs.d_ll.as<double>(), bs.d_invalid.as<int>(),
+	                              bs.d_out_ll.as<double>(), bs.d_out_grad.as<double>(), s));
+	PF_CUDA(record_event(m->ev[3], s));
+	char *ho = bs.h_out.as<char>();
+	PF_CUDA(cudaMemcpyAsync(ho, bs.d_out_ll.p, (size_t)C * 8, cudaMemcpyDeviceToHost, s));
+	PF_CUDA(cudaMemcpyAsync(ho + (size_t)C * 8, bs.d_out_grad.p, (size_t)C * nrefs * 8, cudaMemcpyDeviceToHost, s));
+	PF_CUDA(cudaMemcpyAsync(ho + (size_t)C * (1 + nrefs) * 8, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
+	return PF_OK;
+}
+
+int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, const double *values, double *ll_out,
+                    double *grad_out)
+{
+	PF_TRY(ensure_stream(m));
+	Analysis a;
+	PF_TRY(analyze(m, a));
+	if (m->fs != 1) return set_error(PF_E_INVALID, "the FP32 path does not support finesampling yet");
+	for (auto &p : m->profiles)
+		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
+	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
+	if (m->data_w != a.ow || m->data_h != a.oh)
+		return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
+	if (B < 1) return set_error(PF_E_INVALID, "batch size must be positive");
+	const int nprof = a.n_profiles;
+	if ((long long)B * nprof > 65535 && B > 1) {
+		// profile indices of queued cells are 16-bit: chunks keep B*nprof below that
+	}
+	PF_TRY(upload_psf(m));
+	if (!m->batch) m->batch = new BatchState();
+	BatchState &bs = *m->batch;
+
+	// parameter references -> (profile, byte offset, gradient code)
+	std::vector<int> host_refs(3 * (size_t)nrefs);
+	for (int i = 0; i < nrefs; i++) {
+		PF_TRY(check_profile(m, refs[i].profile));
+		const ProfileParams &p = m->profiles[refs[i].profile];
+		const ParamDesc *d = find_param(p.kind, refs[i].name);
+		if (!d || d->type != T_DOUBLE)
+			return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown double parameter: ") + refs[i].name);
+		int code = 0;
+		PF_TRY(gradient_code(p, refs[i].name, code));
+		host_refs[i] = refs[i].profile;
+		host_refs[nrefs + i] = (int)d->off;
+		host_refs[2 * nrefs + i] = code;
+	}
+	if (host_refs != bs.refs_host) {
+		PF_CUDA(ensure(bs.d_refs, host_refs.size() * 4 + 4));
+		if (nrefs) PF_CUDA(cudaMemcpy(bs.d_refs.p, host_refs.data(), host_refs.size() * 4, cudaMemcpyHostToDevice));
+		bs.refs_host = host_refs;
+		if (bs.graph) cudaGraphExecDestroy(bs.graph);
+		bs.graph = nullptr;
+	}
+
+	// chunk size from the memory budget (tangent planes dominate)
+	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
+	const size_t per = npix * (4 * 4 + 8 * 2 + (size_t)nprof * NTAN * 4) + nout * (8 + 4) + 4096;
+	int C = (int)std::min<size_t>((size_t)B, std::max<size_t>(1, BATCH_BUDGET_BYTES / per));
+	C = std::min(C, 65535 / std::max(nprof, 1));
+	C = std::max(C, 1);
+
+	// buffers for a chunk of C proposals
+	PF_CUDA(ensure(m->d_fprof, (size_t)C * nprof * sizeof(FProfile)));
+	PF_CUDA(ensure(bs.d_dev, (size_t)C * nprof * sizeof(DevProfile)));
+	PF_CUDA(ensure(bs.d_tmpl, nprof * sizeof(ProfileParams)));
+	PF_CUDA(ensure(bs.h_tmpl, nprof * sizeof(ProfileParams)));
+	PF_CUDA(ensure(bs.d_values, (size_t)C * nrefs * 8 + 8));
+	PF_CUDA(ensure(bs.h_values, (size_t)C * nrefs * 8 + 8));
+	PF_CUDA(ensure(bs.d_invalid, (size_t)C * 4));
+	PF_CUDA(ensure(bs.d_ll, (size_t)C * 8));
+	PF_CUDA(ensure(bs.d_out_ll, (size_t)C * 8));
+	PF_CUDA(ensure(bs.d_out_grad, (size_t)C * nrefs * 8 + 8));
+	PF_CUDA(ensure(bs.d_T, (size_t)C * nprof * NTAN * 8));
+	PF_CUDA(ensure(bs.h_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
+	PF_CUDA(ensure(m->d_conv32, npix * C * 4));
+	PF_CUDA(ensure(m->d_plain32, npix * C * 4));
+	PF_CUDA(ensure(m->d_jac, npix * NTAN * nprof * C * 4));
+	PF_CUDA(ensure(m->d_model64, nout * C * 8));
+	PF_CUDA(ensure(m->d_wseed, nout * C * 4));
+	PF_CUDA(ensure(m->d_gconv, npix * C * 4));
+	PF_CUDA(ensure(m->d_gplain, npix * C * 4));
+	PF_CUDA(ensure(m->d_partials, (size_t)NPARTS * C * sizeof(double2)));
+	if (!(a.conv && m->conv_kind != CONV_NULL)) {
+		PF_CUDA(ensure(m->d_conv64, npix * C * 8));
+		PF_CUDA(ensure(m->d_plain64, npix * C * 8));
+	}
+	if (m->prof_begin_n != C * nprof || bs.chunk != C) {
+		std::vector<int> begin(C + 1), pb((size_t)C * nprof);
+		for (int b = 0; b <= C; b++) begin[b] = b * nprof;
+		for (int i = 0; i < C * nprof; i++) pb[i] = i / nprof;
+		PF_CUDA(ensure(m->d_prof_begin, (C + 1) * 4));
+		PF_CUDA(ensure(m->d_prof_batch, (size_t)C * nprof * 4));
+		PF_CUDA(cudaMemcpy(m->d_prof_begin.p, begin.data(), (C + 1) * 4, cudaMemcpyHostToDevice));
+		PF_CUDA(cudaMemcpy(m->d_prof_batch.p, pb.data(), (size_t)C * nprof * 4, cudaMemcpyHostToDevice));
+		m->prof_begin_n = C * nprof;
+		bs.chunk = C;
+	}
+	std::memcpy(bs.h_tmpl.p, m->profiles.data(), nprof * sizeof(ProfileParams));
+
+	char *ho = bs.h_out.as<char>();
+	for (int b0 = 0; b0 < B; b0 += C) {
+		const int n = std::min(C, B - b0);
+		// the graph is recorded for full chunks; a short last chunk is padded
+		// with copies of its first proposal
+		double *hv = bs.h_values.as<double>();
+		std::memcpy(hv, values + (size_t)b0 * nrefs, (size_t)n * nrefs * 8);
+		for (int b = n; b < C; b++) std::memcpy(hv + (size_t)b * nrefs, values + (size_t)b0 * nrefs, (size_t)nrefs * 8);
+		bool done = false;
+		for (int attempt = 0; attempt < 8 && !done; attempt++) {
+			QueueSet q;
+			PF_TRY(prepare_queue(m, a, npix * nprof * C, q, nullptr, nullptr));
+			std::vector<uint64_t> sig = graph_signature(m, a, true, q);
+			sig.push_back((uint64_t)C);
+			sig.push_back((uint64_t)nrefs);
+			for (auto *buf : {&bs.d_tmpl, &bs.d_refs, &bs.d_values, &bs.d_dev, &bs.d_invalid, &bs.d_out_ll,
+			                  &bs.d_out_grad, &bs.d_ll, &bs.d_T})
+				sig.push_back((uint64_t)(uintptr_t)buf->p);
+			sig.push_back((uint64_t)(uintptr_t)bs.h_out.p);
+			sig.push_back((uint64_t)(uintptr_t)bs.h_values.p);
+			sig.push_back((uint64_t)(uintptr_t)bs.h_tmpl.p);
+			bool replayed = false;
+			if (bs.graph && bs.sig == sig) {
+				PF_CUDA(cudaGraphLaunch(bs.graph, m->stream));
+				note_launches((int)bs.graph_kernels);
+				replayed = true;
+			}
+			else {
+				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q));
+			}
+			PF_CUDA(cudaStreamSynchronize(m->stream));
+			int retry = 0;
+			PF_TRY(check_overflow(m, a, reinterpret_cast<uint32_t *>(ho + (size_t)C * (1 + nrefs) * 8), retry));
+			if (retry) {
+				if (bs.graph) cudaGraphExecDestroy(bs.graph);
+				bs.graph = nullptr;
+				continue;
+			}
+			done = true;
+			finish_timings32(m);
+			if (!replayed && m->use_graphs) {
+				if (bs.graph) cudaGraphExecDestroy(bs.graph);
+				bs.graph = nullptr;
+				unsigned long long before = g_launches.load();
+				cudaGraph_t graph = nullptr;
+				PF_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+				int st = enqueue_batch_chunk(m, bs, a, C, nrefs, q);
+				cudaError_t ce = cudaStreamEndCapture(m->stream, &graph);
+				bs.graph_kernels = g_launches.load() - before;
+				g_launches -= bs.graph_kernels;
+				if (st == PF_OK && ce == cudaSuccess && graph && cudaGraphInstantiate(&bs.graph, graph, 0) == cudaSuccess)
+					bs.sig = sig;
+				else
+					bs.graph = nullptr;
+				if (graph) cudaGraphDestroy(graph);
+				cudaGetLastError();
+			}
+		}
+		if (!done) return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+		if (ll_out) std::memcpy(ll_out + b0, ho, (size_t)n * 8);
+		if (grad_out) std::memcpy(grad_out + (size_t)b0 * nrefs, ho + (size_t)C * 8, (size_t)n * nrefs * 8);
+	}
+	return PF_OK;
+}
+
+// Which tangent combination gives d logL / d(name) for profile p (GradCode),
+// or an error for parameters without an adjoint.
+int gradient_code(const ProfileParams &p, const char *name, int &code)
+{
 	if (!is_radial_kind(p.kind))
 		return set_error(PF_E_INVALID, std::string("no gradient for parameters of ") + kind_name(p.kind) + " profiles");
 	if (p.kind != PK_SERSIC && p.kind != PK_MOFFAT)
 		return set_error(PF_E_INVALID, std::string("gradients of ") + kind_name(p.kind) + " profiles are not available yet");
 	if (p.kind == PK_SERSIC && p.rescale_flux)
 		return set_error(PF_E_INVALID, "gradients with rescale_flux are not available");
-	if (!std::strcmp(name, "xcen")) g = F * (-c * T[1] + (s / q) * T[2]);
-	else if (!std::strcmp(name, "ycen")) g = F * (-s * T[1] - (c / q) * T[2]);
-	else if (!std::strcmp(name, "mag")) g = F * d.dlnI_dmag * T[0];
-	else if (!std::strcmp(name, "ang")) g = F * deg * (q * T[3] - T[4] / q);
-	else if (!std::strcmp(name, "axrat")) g = F * (-T[5] / q + d.dlnI_dq * T[0]);
-	else if (!std::strcmp(name, "box")) g = F * (T[8] + d.dlnI_dbox * T[0]);
+	if (!std::strcmp(name, "xcen")) code = G_XCEN;
+	else if (!std::strcmp(name, "ycen")) code = G_YCEN;
+	else if (!std::strcmp(name, "mag")) code = G_MAG;
+	else if (!std::strcmp(name, "ang")) code = G_ANG;
+	else if (!std::strcmp(name, "axrat")) code = G_AXRAT;
+	else if (!std::strcmp(name, "box")) code = G_BOX;
 	else if ((p.kind == PK_SERSIC && !std::strcmp(name, "re")) || (p.kind == PK_MOFFAT && !std::strcmp(name, "fwhm")))
-		g = F * (T[6] + d.dlnI_dp1 * T[0]);
+		code = G_SHAPE1;
 	else if ((p.kind == PK_SERSIC && !std::strcmp(name, "nser")) || (p.kind == PK_MOFFAT && !std::strcmp(name, "con")))
-		g = F * (T[7] + d.dlnI_dp2 * T[0]);
+		code = G_SHAPE2;
 	else
 		return set_error(PF_E_INVALID, std::string("no gradient with respect to ") + name);
+	return PF_OK;
+}
+
+int combine_gradient(const ProfileParams &p, const DevProfile &d, const double *T, const char *name, double &g)
+{
+	int code = 0;
+	PF_TRY(gradient_code(p, name, code));
+	g = gradient_from_tangents(code, p.axrat, d, T);
 	return PF_OK;
 }
 
@@ -951,6 +1155,8 @@ int pf_model_destroy(pf_model *m)
 	cudaSetDevice(m->device);
 	if (m->stream) cudaStreamSynchronize(m->stream);
 	drop_graph(m);
+	delete m->batch;
+	m->batch = nullptr;
 	for (auto &e : m->ev)
 		if (e) cudaEventDestroy(e);
 	if (m->stream) cudaStreamDestroy(m->stream);
@@ -1212,18 +1418,28 @@ int pf_model_loglike_grad(pf_model *m, const pf_param_ref *params, int n_params,
 {
 	if (!m || (n_params > 0 && (!params || !grad))) return set_error(PF_E_INVALID, "null argument");
 	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
-	for (int i = 0; i < n_params; i++) PF_TRY(check_profile(m, params[i].profile));
-	Analysis a;
-	std::vector<double> res;
-	PF_TRY(evaluate32(m, a, true, &res));
-	if (loglike) *loglike = res[ResultLayout::LL];
-	const DevProfile *hp = m->h_prof.as<DevProfile>();
-	for (int i = 0; i < n_params; i++) {
-		int pi = params[i].profile;
-		PF_TRY(combine_gradient(m->profiles[pi], hp[pi], &res[ResultLayout::T0 + (size_t)pi * NTAN], params[i].name,
-		                        grad[i]));
-	}
+	// the current parameter values form a batch of one proposal
+	std::vector<double> vals(n_params > 0 ? n_params : 1);
+	for (int i = 0; i < n_params; i++) PF_TRY(pf_profile_get_double(m, params[i].profile, params[i].name, &vals[i]));
+	double ll = 0;
+	PF_TRY(eval_grad_batch(m, params, n_params, 1, vals.data(), &ll, grad));
+	if (!std::isfinite(ll)) return set_error(PF_E_INVALID, "invalid profile parameters");
+	if (loglike) *loglike = ll;
 	return PF_OK;
+}
+
+int pf_model_loglike_grad_batch(pf_model *m, const pf_param_ref *params, int n_params, int batch,
+                                const double *values, double *loglike, double *grad)
+{
+	if (!m || batch < 1 || (n_params > 0 && (!params || !values)) || !loglike)
+		return set_error(PF_E_INVALID, "null argument or empty batch");
+	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
+	std::vector<double> scratch;
+	if (!grad && n_params > 0) {
+		scratch.resize((size_t)batch * n_params);
+		grad = scratch.data();
+	}
+	return eval_grad_batch(m, params, n_params, batch, values, loglike, grad);
 }
 
 int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_params, double rel_step, double *loglike,

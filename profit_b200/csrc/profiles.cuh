@@ -62,6 +62,7 @@ struct DevProfile {
 	// derivatives of log(flux_scale) w.r.t. parameters (FP32+adjoint path)
 	double dlnI_dmag, dlnI_dq, dlnI_dbox, dlnI_dp1, dlnI_dp2;
 	double dbn_dn;
+	double axrat;
 };
 
 struct ModelGeom {
@@ -211,6 +212,23 @@ inline const char *validate_profile(const ProfileParams &p, bool have_psf)
 	return nullptr;
 }
 
+// Device-side form of validate_profile for batched proposals (a psf profile
+// is valid when the model has a PSF; the batch entry point checks that).
+PF_HD inline bool params_valid(const ProfileParams &p)
+{
+	if (!is_radial_kind(p.kind)) return true;
+	if (!(p.axrat > 0) || p.axrat > 1 || !(p.box > -2)) return false;
+	switch (p.kind) {
+	case PK_SERSIC: return p.re > 0 && p.nser > 0;
+	case PK_MOFFAT: return p.fwhm > 0 && p.con >= 0;
+	case PK_FERRER: return p.rout > 0 && p.a >= 0 && p.b <= 2;
+	case PK_CORESERSIC: return p.re > 0 && p.rb > 0 && p.nser > 0 && p.a > 0 && p.b <= 1.999;
+	case PK_KING: return p.rc > 0 && p.rt > 0 && p.a >= 0;
+	case PK_BROKENEXP: return p.h1 > 0 && p.h2 > 0 && p.rb > 0;
+	}
+	return true;
+}
+
 // ---- per-profile prologue ------------------------------------------------
 
 struct CoreSersicIntegrand {
@@ -244,6 +262,7 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 	d.dlnI_dq = d.dlnI_dbox = d.dlnI_dp1 = d.dlnI_dp2 = d.dbn_dn = 0;
 	d.centre_override = 0;
 	d.bn = 0;
+	d.axrat = p.axrat;
 
 	if (p.kind == PK_SKY) {
 		d.bg = p.bg / (g.finesampling * g.finesampling);

@@ -576,4 +576,83 @@ cudaError_t launch_crop32(const float *src, unsigned sw, unsigned ox, unsigned o
 	return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Batched proposals: device-side prologue and gradient assembly
+// ---------------------------------------------------------------------------
+
+// One thread per (proposal, profile): the model's parameters with this
+// proposal's values written in, checked like RadialProfile::validate, then the
+// FP64 scalar prologue (b_n, luminosity, Ie, auto-adjusted subsampling).  A
+// proposal with an invalid profile is flagged and its profiles become null
+// profiles, so nothing is drawn for it.
+__global__ void k_batch_prologue(const ProfileParams *__restrict__ tmpl, int nprof, int batch,
+                                 const int *__restrict__ ref_profile, const int *__restrict__ ref_offset, int nrefs,
+                                 const double *__restrict__ values, ModelGeom g, DevProfile *__restrict__ dev,
+                                 FProfile *__restrict__ fprof, int *__restrict__ invalid)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= batch * nprof) return;
+	const int b = t / nprof, p = t - b * nprof;
+	ProfileParams pp = tmpl[p];
+	for (int r = 0; r < nrefs; r++)
+		if (ref_profile[r] == p)
+			*reinterpret_cast<double *>(reinterpret_cast<char *>(&pp) + ref_offset[r]) = values[(size_t)b * nrefs + r];
+	if (!params_valid(pp)) {
+		invalid[b] = 1;
+		pp.kind = PK_NULL;
+	}
+	DevProfile d;
+	derive_profile(pp, g, d);
+	dev[t] = d;
+	fprof[t] = to_fprofile(d, pp);
+}
+
+// One thread per (proposal, parameter): d logL / d parameter from the tangent
+// reductions; invalid proposals get logL = -inf and a zero gradient.
+__global__ void k_batch_gradient(const DevProfile *__restrict__ dev, int nprof, int batch,
+                                 const int *__restrict__ ref_profile, const int *__restrict__ ref_code, int nrefs,
+                                 const double *__restrict__ T, const double *__restrict__ ll, const int *__restrict__ invalid,
+                                 double *__restrict__ out_ll, double *__restrict__ out_grad)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t < batch) out_ll[t] = invalid[t] ? -INFINITY : ll[t];
+	if (t >= batch * nrefs) return;
+	const int b = t / nrefs, r = t - b * nrefs;
+	const int pi = b * nprof + ref_profile[r];
+	out_grad[t] = invalid[b] ? 0.0 : gradient_from_tangents(ref_code[r], dev[pi].axrat, dev[pi], T + (size_t)pi * NTAN);
+}
+
+cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batch, const int *ref_profile,
+                                  const int *ref_offset, int nrefs, const double *values, const ModelGeom &g,
+                                  DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s)
+{
+	int n = batch * nprof;
+	k_batch_prologue<<<(n + 127) / 128, 128, 0, s>>>(tmpl, nprof, batch, ref_profile, ref_offset, nrefs, values, g,
+	                                                 dev, fprof, invalid);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, const int *ref_profile,
+                                  const int *ref_code, int nrefs, const double *T, const double *ll,
+                                  const int *invalid, double *out_ll, double *out_grad, cudaStream_t s)
+{
+	int n = batch * (nrefs > 1 ? nrefs : 1);
+	k_batch_gradient<<<(n + 255) / 256, 256, 0, s>>>(dev, nprof, batch, ref_profile, ref_code, nrefs, T, ll, invalid,
+	                                                 out_ll, out_grad);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_loglike64_batch(const double *model, const double *data, const double *sigma,
+                                   const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
+                                   int nparts, double *out, float *wseed, cudaStream_t s)
+{
+	k_loglike_partial<double><<<dim3(nparts, batch), 256, 0, s>>>(model, data, sigma, region, n, partials, wseed,
+	                                                              data_batch_stride);
+	k_loglike_final<<<batch, 256, 0, s>>>(partials, nparts, out);
+	note_launches(2);
+	return cudaGetLastError();
+}
+
 }  // namespace pf

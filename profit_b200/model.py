@@ -192,6 +192,18 @@ class Model:
         check(lib().pf_model_loglike_grad(self._h, arr, len(params), C.byref(ll), g.ctypes.data_as(_capi._dp)))
         return ll.value, g
 
+    def loglike_grad_batch(self, params: Sequence[Tuple[int, str]], values: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        """logL[b] and gradient[b, i] for every row of values[b, i] (a batch of proposals).
+        Invalid proposals get logL = -inf."""
+        arr, keep = self._refs(params)
+        v = np.ascontiguousarray(values, dtype=np.float64).reshape(-1, len(params))
+        B = v.shape[0]
+        ll = np.zeros(B, dtype=np.float64)
+        g = np.zeros((B, len(params)), dtype=np.float64)
+        check(lib().pf_model_loglike_grad_batch(self._h, arr, len(params), B, v.ctypes.data_as(_capi._dp),
+                                                ll.ctypes.data_as(_capi._dp), g.ctypes.data_as(_capi._dp)))
+        return ll, g
+
     def loglike_grad_fd(self, params: Sequence[Tuple[int, str]], rel_step: float = 1e-6) -> Tuple[float, np.ndarray]:
         """logL and central finite differences of the plain FP64 form."""
         arr, keep = self._refs(params)

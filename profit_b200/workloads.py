@@ -82,6 +82,30 @@ def bulge_disk_ps(seed_tag: int = 2, width: int = 400, height: int = 400, psf_si
                 sigma_range=(0.5, 2.0), seed_tag=seed_tag)
 
 
+def sampler_batch(n: int = 4096, seed_tag: int = 3) -> Tuple[Dict, np.ndarray]:
+    """The single-Sersic model at 200x200 with a 31x31 Gaussian PSF and n
+    sampler proposals params = init + N(0, 0.05 |init|) (redrawn until valid).
+    Returns (workload, values[n, 8]) for the 8 Sersic parameters."""
+    wl = single_sersic(seed_tag=seed_tag, width=200, height=200, psf_size=31)
+    refs = wl["grad"]
+    init = np.array([wl["profiles"][i][1][k] for (i, k) in refs])
+    r = np.random.Generator(np.random.PCG64([SEED, 91, seed_tag]))
+    vals = init + r.normal(size=(n, len(refs))) * 0.05 * np.abs(init)
+    for j, (_, k) in enumerate(refs):
+        lo = {"axrat": 0.05, "re": 1e-3, "nser": 0.3}.get(k)
+        hi = {"axrat": 1.0}.get(k)
+        for _ in range(100):
+            bad = np.zeros(n, dtype=bool)
+            if lo is not None:
+                bad |= vals[:, j] <= lo
+            if hi is not None:
+                bad |= vals[:, j] > hi
+            if not bad.any():
+                break
+            vals[bad, j] = init[j] + r.normal(size=bad.sum()) * 0.05 * abs(init[j])
+    return wl, vals
+
+
 def make_data(w: Dict, model_image: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """Data = model + N(0, sigma) with a per-pixel sigma map ~ U[sigma_range]."""
     r = _rng(1000 + w["seed_tag"])
