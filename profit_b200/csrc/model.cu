@@ -823,7 +823,7 @@ int check_profile(pf_model *m, int index);
 
 struct BatchState {
 	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out_ll, d_out_grad, d_ll, d_T;
-	HostBuf h_tmpl, h_values, h_out;
+	HostBuf h_tmpl, h_values, h_out, h_dev, h_fprof, h_invalid;
 	int refs_n = -1, chunk = 0;
 	std::vector<int> refs_host;
 	cudaGraphExec_t graph = nullptr;
@@ -839,7 +839,13 @@ namespace {
 
 constexpr size_t BATCH_BUDGET_BYTES = 24ull << 30;
 
-int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, int nrefs, const QueueSet &q)
+// A few proposals: the scalar prologue (qgamma's Newton iterations are one
+// long dependent FP64 chain) is faster on the host than in one GPU thread.
+// Many proposals: one GPU thread per (proposal, profile) runs them in parallel.
+constexpr int HOST_PROLOGUE_MAX = 16;
+
+int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, int nrefs, const QueueSet &q,
+                        bool host_prologue)
 {
 	const int nprof = a.n_profiles;
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
@@ -850,14 +856,23 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	const int *ref_profile = bs.d_refs.as<int>(), *ref_offset = ref_profile + nrefs, *ref_code = ref_offset + nrefs;
 
 	PF_CUDA(record_event(m->ev[0], s));
-	PF_CUDA(cudaMemcpyAsync(bs.d_tmpl.p, bs.h_tmpl.p, nprof * sizeof(ProfileParams), cudaMemcpyHostToDevice, s));
-	PF_CUDA(cudaMemcpyAsync(bs.d_values.p, bs.h_values.p, (size_t)C * nrefs * 8, cudaMemcpyHostToDevice, s));
 	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, s));
-	PF_CUDA(cudaMemsetAsync(bs.d_invalid.p, 0, (size_t)C * 4, s));
 	PF_CUDA(cudaMemsetAsync(bs.d_T.p, 0, (size_t)C * nprof * NTAN * 8, s));
-	PF_CUDA(launch_batch_prologue(bs.d_tmpl.as<ProfileParams>(), nprof, C, ref_profile, ref_offset, nrefs,
-	                              bs.d_values.as<double>(), geometry(m, a), bs.d_dev.as<DevProfile>(),
-	                              m->d_fprof.as<FProfile>(), bs.d_invalid.as<int>(), s));
+	if (host_prologue) {
+		PF_CUDA(cudaMemcpyAsync(bs.d_dev.p, bs.h_dev.p, (size_t)C * nprof * sizeof(DevProfile),
+		                        cudaMemcpyHostToDevice, s));
+		PF_CUDA(cudaMemcpyAsync(m->d_fprof.p, bs.h_fprof.p, (size_t)C * nprof * sizeof(FProfile),
+		                        cudaMemcpyHostToDevice, s));
+		PF_CUDA(cudaMemcpyAsync(bs.d_invalid.p, bs.h_invalid.p, (size_t)C * 4, cudaMemcpyHostToDevice, s));
+	}
+	else {
+		PF_CUDA(cudaMemcpyAsync(bs.d_tmpl.p, bs.h_tmpl.p, nprof * sizeof(ProfileParams), cudaMemcpyHostToDevice, s));
+		PF_CUDA(cudaMemcpyAsync(bs.d_values.p, bs.h_values.p, (size_t)C * nrefs * 8, cudaMemcpyHostToDevice, s));
+		PF_CUDA(cudaMemsetAsync(bs.d_invalid.p, 0, (size_t)C * 4, s));
+		PF_CUDA(launch_batch_prologue(bs.d_tmpl.as<ProfileParams>(), nprof, C, ref_profile, ref_offset, nrefs,
+		                              bs.d_values.as<double>(), geometry(m, a), bs.d_dev.as<DevProfile>(),
+		                              m->d_fprof.as<FProfile>(), bs.d_invalid.as<int>(), s));
+	}
 	const FProfile *fprof = m->d_fprof.as<FProfile>();
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx, m->sy, conv, plain, jac, q, s));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, s));
@@ -983,6 +998,13 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		bs.chunk = C;
 	}
 	std::memcpy(bs.h_tmpl.p, m->profiles.data(), nprof * sizeof(ProfileParams));
+	const bool host_prologue = C * nprof <= HOST_PROLOGUE_MAX;
+	if (host_prologue) {
+		PF_CUDA(ensure(bs.h_dev, (size_t)C * nprof * sizeof(DevProfile)));
+		PF_CUDA(ensure(bs.h_fprof, (size_t)C * nprof * sizeof(FProfile)));
+		PF_CUDA(ensure(bs.h_invalid, (size_t)C * 4));
+	}
+	const ModelGeom geom = geometry(m, a);
 
 	char *ho = bs.h_out.as<char>();
 	for (int b0 = 0; b0 < B; b0 += C) {
@@ -992,6 +1014,27 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		double *hv = bs.h_values.as<double>();
 		std::memcpy(hv, values + (size_t)b0 * nrefs, (size_t)n * nrefs * 8);
 		for (int b = n; b < C; b++) std::memcpy(hv + (size_t)b * nrefs, values + (size_t)b0 * nrefs, (size_t)nrefs * 8);
+		if (host_prologue) {
+			DevProfile *hd = bs.h_dev.as<DevProfile>();
+			FProfile *hf = bs.h_fprof.as<FProfile>();
+			int *hi = bs.h_invalid.as<int>();
+			for (int b = 0; b < C; b++) {
+				hi[b] = 0;
+				for (int p = 0; p < nprof; p++) {
+					ProfileParams pp = m->profiles[p];
+					for (int r = 0; r < nrefs; r++)
+						if (host_refs[r] == p)
+							*reinterpret_cast<double *>(reinterpret_cast<char *>(&pp) + host_refs[nrefs + r]) =
+							    hv[(size_t)b * nrefs + r];
+					if (!params_valid(pp)) {
+						hi[b] = 1;
+						pp.kind = PK_NULL;
+					}
+					derive_profile(pp, geom, hd[b * nprof + p]);
+					hf[b * nprof + p] = to_fprofile(hd[b * nprof + p], pp);
+				}
+			}
+		}
 		bool done = false;
 		for (int attempt = 0; attempt < 8 && !done; attempt++) {
 			QueueSet q;
@@ -999,6 +1042,10 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			std::vector<uint64_t> sig = graph_signature(m, a, true, q);
 			sig.push_back((uint64_t)C);
 			sig.push_back((uint64_t)nrefs);
+			sig.push_back((uint64_t)host_prologue);
+			sig.push_back((uint64_t)(uintptr_t)bs.h_dev.p);
+			sig.push_back((uint64_t)(uintptr_t)bs.h_fprof.p);
+			sig.push_back((uint64_t)(uintptr_t)bs.h_invalid.p);
 			for (auto *buf : {&bs.d_tmpl, &bs.d_refs, &bs.d_values, &bs.d_dev, &bs.d_invalid, &bs.d_out_ll,
 			                  &bs.d_out_grad, &bs.d_ll, &bs.d_T})
 				sig.push_back((uint64_t)(uintptr_t)buf->p);
@@ -1012,7 +1059,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				replayed = true;
 			}
 			else {
-				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q));
+				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue));
 			}
 			PF_CUDA(cudaStreamSynchronize(m->stream));
 			int retry = 0;
@@ -1030,7 +1077,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				unsigned long long before = g_launches.load();
 				cudaGraph_t graph = nullptr;
 				PF_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
-				int st = enqueue_batch_chunk(m, bs, a, C, nrefs, q);
+				int st = enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue);
 				cudaError_t ce = cudaStreamEndCapture(m->stream, &graph);
 				bs.graph_kernels = g_launches.load() - before;
 				g_launches -= bs.graph_kernels;
