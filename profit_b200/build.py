@@ -30,6 +30,7 @@ UNITS = {
     # file: extra flags
     "render64.cu": ["--fmad=false"],
     "render32.cu": [],
+    "fft.cu": [],
     "model.cu": ["--fmad=false"],
 }
 

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "conv.cuh"
+#include "fft.h"
 #include "launch.h"
 #include "profit_b200.h"
 
@@ -94,11 +95,11 @@ int set_error(int code, const std::string &msg)
 	return code;
 }
 
-#define PF_CUDA(expr)                                                                          \
-	do {                                                                                       \
-		cudaError_t e_ = (expr);                                                               \
-		if (e_ != cudaSuccess)                                                                 \
-			return set_error(PF_E_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e_)); \
+#define PF_CUDA(...)                                                                                  \
+	do {                                                                                              \
+		cudaError_t e_ = (__VA_ARGS__);                                                               \
+		if (e_ != cudaSuccess)                                                                        \
+			return set_error(PF_E_CUDA, std::string(#__VA_ARGS__) + ": " + cudaGetErrorString(e_)); \
 	} while (0)
 
 // Timing events must become graph nodes when the stream is being captured
@@ -313,6 +314,12 @@ struct pf_model {
 	bool has_data = false, has_region = false;
 	unsigned data_w = 0, data_h = 0;
 
+	// "fft" convolver: transforms, PSF spectra and work spectra
+	FftConv<double> fft64;
+	FftConv<float> fft32;
+	DevBuf d_kspec64, d_kspec32, d_fftwork64, d_fftwork32;
+	unsigned psf_version = 1, kspec64_version = 0, kspec32_version = 0;
+
 	// captured FP32 likelihood+gradient pipeline (replayed while its signature holds)
 	cudaGraphExec_t graph_exec = nullptr;
 	std::vector<uint64_t> graph_sig;
@@ -415,6 +422,52 @@ int upload_psf(pf_model *m)
 	return PF_OK;
 }
 
+// Where the cropped model reads the linear convolution c = psf * src (both
+// at the origin of the FFT grid): model(x, y) = c(x + dx, y + dy).
+// FFTConvolver returns c at offset_after_convolution (convolve.cpp:270-281):
+// src/2, minus one when the source or the kernel is even, less the kernel's
+// placement (src - krn)/2 (convolve.cpp:295); the model then crops psf/2
+// (model.cpp:307-324).
+void fft_offsets(const pf_model *m, const Analysis &a, int &dx, int &dy)
+{
+	int ox = (int)(a.dw / 2), oy = (int)(a.dh / 2);
+	if (a.dw % 2 == 0 || m->psf_w % 2 == 0) ox -= 1;
+	if (a.dh % 2 == 0 || m->psf_h % 2 == 0) oy -= 1;
+	dx = (int)a.padx + ox - (int)((a.dw - m->psf_w) / 2);
+	dy = (int)a.pady + oy - (int)((a.dh - m->psf_h) / 2);
+}
+
+// FFT grid and PSF spectra for the "fft" convolver (rebuilt when the PSF or
+// the drawing size changes).
+int prepare_fft(pf_model *m, const Analysis &a, int batch, bool need32)
+{
+	const int N = fft_good_size((int)a.dw + (int)m->psf_w - 1);
+	const int M = fft_good_size((int)a.dh + (int)m->psf_h - 1);
+	if (N > FFT_MAX_LEN || M > FFT_MAX_LEN)
+		return set_error(PF_E_INVALID, "image too large for the fft convolver (use brute)");
+	const bool resized = m->fft64.M != M || m->fft64.N != N;
+	PF_CUDA(m->fft64.setup(M, N));
+	const size_t spec = m->fft64.spectrum_elems();
+	PF_CUDA(ensure(m->d_kspec64, spec * sizeof(double2)));
+	PF_CUDA(ensure(m->d_fftwork64, spec * sizeof(double2) * batch));
+	if (resized || m->kspec64_version != m->psf_version) {
+		PF_CUDA(m->fft64.set_kernel(m->d_psf64.as<double>(), m->psf_w, m->psf_h, m->d_kspec64.as<double2>(), m->stream));
+		m->kspec64_version = m->psf_version;
+	}
+	if (need32) {
+		const bool resized32 = m->fft32.M != M || m->fft32.N != N;
+		PF_CUDA(m->fft32.setup(M, N));
+		PF_CUDA(ensure(m->d_kspec32, spec * sizeof(float2)));
+		PF_CUDA(ensure(m->d_fftwork32, spec * sizeof(float2) * batch));
+		if (resized32 || m->kspec32_version != m->psf_version) {
+			PF_CUDA(m->fft32.set_kernel(m->d_psf32.as<float>(), m->psf_w, m->psf_h, m->d_kspec32.as<float2>(),
+			                            m->stream));
+			m->kspec32_version = m->psf_version;
+		}
+	}
+	return PF_OK;
+}
+
 // Queue segments per level; capacities start from a pixel-count estimate and
 // grow after an overflow.
 int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q, int32_t *decisions,
@@ -498,6 +551,67 @@ int derive_and_upload(pf_model *m, const Analysis &a, const std::vector<ProfileP
 	return PF_OK;
 }
 
+// FP32 path, forward: the FP32 drawing images of `batch` proposals to the
+// cropped FP64 model images.  The model image is kept in FP64 because the
+// residual (data - model) of bright pixels is a small difference of large
+// numbers: brute force sums kernel columns in FP64, the "fft" convolver
+// transforms in FP64.
+int forward_conv32(pf_model *m, const Analysis &a, const float *conv, const float *plain, double *model64, int batch)
+{
+	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.cw * a.ch;
+	const bool conv_on = a.conv && m->conv_kind != CONV_NULL;
+	if (conv_on && m->conv_kind == CONV_FFT) {
+		PF_TRY(prepare_fft(m, a, batch, true));
+		int dx, dy;
+		fft_offsets(m, a, dx, dy);
+		PF_CUDA(m->fft64.convolve<float, double, float>(conv, a.dw, a.dh, 0, 0, m->d_kspec64.as<double2>(), false,
+		                                                m->d_fftwork64.as<double2>(), dx, dy, model64, a.cw, a.ch,
+		                                                plain, a.dw, a.padx, a.pady, batch, npix, nout, npix,
+		                                                m->stream));
+		note_launches(3);
+		return PF_OK;
+	}
+	if (m->precision == PF_FP32_CONV64 || !conv_on) {
+		PF_CUDA(ensure(m->d_conv64, npix * 8 * batch));
+		PF_CUDA(ensure(m->d_plain64, npix * 8 * batch));
+		PF_CUDA(launch_widen(conv, m->d_conv64.as<double>(), npix * batch, m->stream));
+		PF_CUDA(launch_widen(plain, m->d_plain64.as<double>(), npix * batch, m->stream));
+		for (int b = 0; b < batch; b++) {
+			const double *c64 = m->d_conv64.as<double>() + b * npix, *p64 = m->d_plain64.as<double>() + b * npix;
+			if (conv_on)
+				PF_CUDA(launch_conv64(c64, a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w, m->psf_h,
+				                      model64 + b * nout, a.cw, a.ch, p64, a.dw, a.padx, a.pady, m->stream));
+			else
+				PF_CUDA(launch_crop64(c64, a.dw, a.padx, a.pady, model64 + b * nout, a.cw, a.ch, p64, m->stream));
+		}
+		return PF_OK;
+	}
+	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64, a.cw,
+	                           a.ch, plain, a.dw, a.padx, a.pady, batch, (int)npix, (int)nout, m->stream));
+	return PF_OK;
+}
+
+// FP32 path, adjoint of the convolution: dlogL/dmodel on the output grid to
+// dlogL/d(drawing pixel) of the convolved image, for `batch` proposals.
+int adjoint_conv32(pf_model *m, const Analysis &a, const float *wseed, float *gconv, int batch)
+{
+	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
+	if (m->conv_kind == CONV_FFT) {
+		PF_TRY(prepare_fft(m, a, batch, true));
+		int dx, dy;
+		fft_offsets(m, a, dx, dy);
+		// g(U) = sum_x w(x) psf(x + d - U): correlation of w placed at d
+		PF_CUDA(m->fft32.convolve<float, float, float>(wseed, a.ow, a.oh, dx, dy, m->d_kspec32.as<float2>(), true,
+		                                               m->d_fftwork32.as<float2>(), 0, 0, gconv, a.dw, a.dh, nullptr,
+		                                               0, 0, 0, batch, nout, npix, 0, m->stream));
+		note_launches(3);
+		return PF_OK;
+	}
+	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(), m->psf_w,
+	                      m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, batch, (int)nout, (int)npix, m->stream));
+	return PF_OK;
+}
+
 // FP64 model image into d_model64 (out dims), queue-overflow checked by caller.
 int run_plain64(pf_model *m, const Analysis &a, const DevProfile *dprof, QueueSet &q)
 {
@@ -519,7 +633,16 @@ int run_plain64(pf_model *m, const Analysis &a, const DevProfile *dprof, QueueSe
 	PF_CUDA(record_event(m->ev[1], m->stream));
 
 	double *model = m->d_model64.as<double>();
-	if (a.conv && m->conv_kind != CONV_NULL) {
+	if (a.conv && m->conv_kind == CONV_FFT) {
+		PF_TRY(prepare_fft(m, a, 1, false));
+		int dx, dy;
+		fft_offsets(m, a, dx, dy);
+		PF_CUDA(m->fft64.convolve<double, double, double>(conv, a.dw, a.dh, 0, 0, m->d_kspec64.as<double2>(), false,
+		                                                  m->d_fftwork64.as<double2>(), dx, dy, model, a.cw, a.ch,
+		                                                  plain, a.dw, a.padx, a.pady, 1, 0, 0, 0, m->stream));
+		note_launches(3);
+	}
+	else if (a.conv && m->conv_kind != CONV_NULL) {
 		PF_CUDA(launch_conv64(conv, a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w, m->psf_h, model, a.cw,
 		                      a.ch, plain, a.dw, a.padx, a.pady, m->stream));
 	}
@@ -614,28 +737,9 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	                        jac, q, m->stream));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, m->stream));
 	PF_CUDA(record_event(m->ev[1], m->stream));
-	// The forward model image is kept in FP64: the residual (data - model) of
-	// bright pixels is a small difference of large numbers.
 	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
 	double *model64 = m->d_model64.as<double>();
-	const bool conv64 = m->precision == PF_FP32_CONV64;
-	if (conv64 || !(a.conv && m->conv_kind != CONV_NULL)) {
-		PF_CUDA(ensure(m->d_conv64, npix * 8));
-		PF_CUDA(ensure(m->d_plain64, npix * 8));
-		PF_CUDA(launch_widen(conv, m->d_conv64.as<double>(), npix, m->stream));
-		PF_CUDA(launch_widen(plain, m->d_plain64.as<double>(), npix, m->stream));
-		if (a.conv && m->conv_kind != CONV_NULL)
-			PF_CUDA(launch_conv64(m->d_conv64.as<double>(), a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w,
-			                      m->psf_h, model64, a.cw, a.ch, m->d_plain64.as<double>(), a.dw, a.padx, a.pady,
-			                      m->stream));
-		else
-			PF_CUDA(launch_crop64(m->d_conv64.as<double>(), a.dw, a.padx, a.pady, model64, a.cw, a.ch,
-			                      m->d_plain64.as<double>(), m->stream));
-	}
-	else {
-		PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64,
-		                           a.cw, a.ch, plain, a.dw, a.padx, a.pady, 1, 0, 0, m->stream));
-	}
+	PF_TRY(forward_conv32(m, a, conv, plain, model64, 1));
 	(void)model;
 	PF_CUDA(record_event(m->ev[2], m->stream));
 	if (!m->has_data) return PF_OK;
@@ -653,13 +757,10 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(ensure(m->d_gplain, npix * 4));
 		float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>();
 		PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, 1, gplain, m->stream));
-		if (a.conv && m->conv_kind != CONV_NULL) {
-			PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(),
-			                      m->psf_w, m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, 1, 0, 0, m->stream));
-		}
-		else {
+		if (a.conv && m->conv_kind != CONV_NULL)
+			PF_TRY(adjoint_conv32(m, a, wseed, gconv, 1));
+		else
 			gconv = gplain;
-		}
 		PF_CUDA(cudaMemsetAsync(d_out + ResultLayout::T0, 0, (size_t)nprof * NTAN * 8, m->stream));
 		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix,
 		                          d_out + ResultLayout::T0, m->stream));
@@ -877,25 +978,14 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx, m->sy, conv, plain, jac, q, s));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, s));
 	PF_CUDA(record_event(m->ev[1], s));
-	if (a.conv && m->conv_kind != CONV_NULL) {
-		PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64,
-		                           a.cw, a.ch, plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout, s));
-	}
-	else {
-		PF_CUDA(launch_widen(conv, m->d_conv64.as<double>(), npix * C, s));
-		PF_CUDA(launch_widen(plain, m->d_plain64.as<double>(), npix * C, s));
-		for (int b = 0; b < C; b++)
-			PF_CUDA(launch_crop64(m->d_conv64.as<double>() + b * npix, a.dw, a.padx, a.pady, model64 + b * nout, a.cw,
-			                      a.ch, m->d_plain64.as<double>() + b * npix, s));
-	}
+	PF_TRY(forward_conv32(m, a, conv, plain, model64, C));
 	PF_CUDA(record_event(m->ev[2], s));
 	PF_CUDA(launch_loglike64_batch(model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
 	                               m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout, C, 0,
 	                               m->d_partials.as<double2>(), NPARTS, bs.d_ll.as<double>(), wseed, s));
 	PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
 	if (a.conv && m->conv_kind != CONV_NULL)
-		PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(),
-		                      m->psf_w, m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix, s));
+		PF_TRY(adjoint_conv32(m, a, wseed, gconv, C));
 	else
 		gconv = gplain;
 	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix,
@@ -956,7 +1046,12 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 
 	// chunk size from the memory budget (tangent planes dominate)
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
-	const size_t per = npix * (4 * 4 + 8 * 2 + (size_t)nprof * NTAN * 4) + nout * (8 + 4) + 4096;
+	size_t per = npix * (4 * 4 + 8 * 2 + (size_t)nprof * NTAN * 4) + nout * (8 + 4) + 4096;
+	if (a.conv && m->conv_kind == CONV_FFT) {
+		const size_t spec = (size_t)fft_good_size((int)a.dh + (int)m->psf_h - 1) *
+		                    (fft_good_size((int)a.dw + (int)m->psf_w - 1) / 2 + 1);
+		per += spec * (sizeof(double2) + sizeof(float2));
+	}
 	int C = (int)std::min<size_t>((size_t)B, std::max<size_t>(1, BATCH_BUDGET_BYTES / per));
 	C = std::min(C, 65535 / std::max(nprof, 1));
 	C = std::max(C, 1);
@@ -1291,6 +1386,7 @@ int pf_model_set_psf(pf_model *m, const double *psf, unsigned width, unsigned he
 		m->psf.clear();
 		m->psf_w = m->psf_h = 0;
 		m->psf_dirty = true;
+	m->psf_version++;
 		return PF_OK;
 	}
 	size_t n = (size_t)width * height;
@@ -1303,6 +1399,7 @@ int pf_model_set_psf(pf_model *m, const double *psf, unsigned width, unsigned he
 	m->psf_w = width;
 	m->psf_h = height;
 	m->psf_dirty = true;
+	m->psf_version++;
 	return PF_OK;
 }
 
