@@ -184,6 +184,23 @@ def cpu_baseline(wl, image, sigma, budget_s=15.0):
 # main (B200 arm)
 # ---------------------------------------------------------------------------
 
+def max_over_ranks(values, dist=None, device="cpu"):
+    """Element-wise maximum over ranks of a list of floats (timed regions are
+    reported as the slowest rank's).  With no process group, the values."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return list(values)
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def aggregate_rate(steps, seconds, world):
+    """Whole-job throughput of `world` replicas that each ran `steps` steps,
+    the slowest taking `seconds`."""
+    return world * steps / seconds
+
+
 def init_dist():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -284,12 +301,8 @@ def main_b200(args):
     if world > 1:
         dist.barrier()
 
-    dev_total = sum(dev_ms) / 1e3
-    e2e_total = sum(e2e_ms) / 1e3
-    if world > 1:
-        t = torch.tensor([dev_total, e2e_total], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_total, e2e_total = t.tolist()
+    dev_total, e2e_total = max_over_ranks([sum(dev_ms) / 1e3, sum(e2e_ms) / 1e3],
+                                          dist if world > 1 else None, device="cuda")
 
     # roofline of the forward convolution (the dominant kernel)
     P = wl["psf"].shape[0]
@@ -310,12 +323,12 @@ def main_b200(args):
     if rank == 0:
         per_step_in = 8 * len(refs) + 16 * len(refs)  # values + parameter references
         out = {
-            "metric": METRIC, "value": world * args.steps / dev_total, "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": aggregate_rate(args.steps, dev_total, world), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dev_total / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded PCG64 images/sigma/PSF of the configuration's shapes (no public dataset)",
             "config": config_dict(wl, world),
-            "e2e": {"value": world * args.steps / e2e_total, "unit": UNIT,
+            "e2e": {"value": aggregate_rate(args.steps, e2e_total, world), "unit": UNIT,
                     "h2d_bytes_per_step": 8 * len(refs), "d2h_bytes_per_step": 8 * (1 + len(refs)),
                     "path": "pf_model_set_parameters + pf_model_loglike_grad (C ABI, host buffers)",
                     "ms_per_step": 1e3 * e2e_total / args.steps},
