@@ -165,6 +165,18 @@ int pf_model_loglike_grad(pf_model *m, const pf_param_ref *params, int n_params,
 int pf_model_loglike_grad_batch(pf_model *m, const pf_param_ref *params, int n_params, int batch,
                                 const double *values, double *loglike, double *grad);
 
+/* How the adjoint of the render is formed.  PF_ADJOINT_STORE keeps, per
+ * radial profile, nine FP32 tangent planes of the drawing size from the
+ * forward pass (fastest for a few profiles); PF_ADJOINT_RECOMPUTE records
+ * only the subsampling decisions and recomputes the tangents against the
+ * adjoint seed (no planes: for hundreds of profiles on large fields);
+ * PF_ADJOINT_AUTO (default) stores while the planes stay under 256 MB per
+ * proposal. */
+#define PF_ADJOINT_AUTO 0
+#define PF_ADJOINT_STORE 1
+#define PF_ADJOINT_RECOMPUTE 2
+int pf_model_set_adjoint_mode(pf_model *m, int mode);
+
 /* Same quantities by central finite differences of the plain form (FP64),
  * 2*n_params + 1 evaluations with relative step `rel_step` (absolute step
  * rel_step*max(|p|, 1)); the baseline that pf_model_loglike_grad replaces. */

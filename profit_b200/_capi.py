@@ -124,6 +124,11 @@ def check(status: int) -> None:
 def _late_bindings(L):
     L.pf_model_set_parameters.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, _dp]
     L.pf_model_loglike_grad_batch.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, C.c_int, _dp, _dp, _dp]
+    L.pf_model_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
 
 
-EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch")
+PF_ADJOINT_AUTO = 0
+PF_ADJOINT_STORE = 1
+PF_ADJOINT_RECOMPUTE = 2
+
+EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch", "pf_model_set_adjoint_mode")

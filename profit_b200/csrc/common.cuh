@@ -29,8 +29,12 @@ struct SubItem {
 // counts[L] keeps counting past cap[L]; the host reads it back to size a
 // retry, so an overflow is reported (never written out of bounds).
 constexpr int MAX_LEVELS = 16;
+// Accepted sub-points of an item (res^2 <= 256 bits), recorded by the
+// forward pass when the adjoint recomputes instead of storing tangents.
+constexpr int MASK_WORDS = 8;
 struct QueueSet {
 	SubItem *items;
+	uint32_t *masks;       // optional [items][MASK_WORDS], parallel to items
 	uint32_t *counts;      // [MAX_LEVELS]
 	uint32_t *overflow;    // set to 1 when an item had to be dropped
 	int32_t *decisions;    // optional [n_profiles][npix] subsample_pixel calls per pixel

@@ -75,3 +75,10 @@ cudaError_t launch_loglike64_batch(const double *model, const double *data, cons
                                    const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
                                    int nparts, double *out, float *wseed, cudaStream_t s);
 }  // namespace pf
+
+namespace pf {
+// render32.cu: recomputing adjoint of the render (no stored tangent planes)
+cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
+                                     unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
+                                     int levels, const QueueSet &q, double *T, cudaStream_t s);
+}  // namespace pf

@@ -306,7 +306,8 @@ struct pf_model {
 	DevBuf d_conv64, d_plain64, d_model64;
 	DevBuf d_conv32, d_plain32, d_model32, d_jac, d_gconv, d_gplain, d_wseed;
 	DevBuf d_psf64, d_psfrev64, d_psf32, d_psfrev32;
-	DevBuf d_items, d_ctrl, d_partials, d_results;
+	DevBuf d_items, d_masks, d_ctrl, d_partials, d_results;
+	int adjoint_mode = PF_ADJOINT_AUTO;
 	DevBuf d_decisions, d_level_counts;
 	DevBuf d_data, d_sigma, d_region;
 	HostBuf h_prof, h_fprof, h_results, h_ctrl;
@@ -471,7 +472,7 @@ int prepare_fft(pf_model *m, const Analysis &a, int batch, bool need32)
 // Queue segments per level; capacities start from a pixel-count estimate and
 // grow after an overflow.
 int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q, int32_t *decisions,
-                  unsigned long long *level_counts)
+                  unsigned long long *level_counts, bool with_masks = false)
 {
 	if (m->caps.size() != (size_t)MAX_LEVELS) {
 		m->caps.assign(MAX_LEVELS, 0);
@@ -494,6 +495,11 @@ int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q
 	if (total >= (1ull << 32)) return set_error(PF_E_CAPACITY, "subsampling work queue exceeds 2^32 items");
 	PF_CUDA(ensure(m->d_items, total * sizeof(SubItem)));
 	PF_CUDA(ensure(m->d_ctrl, CTRL_WORDS * 4));
+	q.masks = nullptr;
+	if (with_masks) {
+		PF_CUDA(ensure(m->d_masks, total * MASK_WORDS * sizeof(uint32_t)));
+		q.masks = m->d_masks.as<uint32_t>();
+	}
 	q.items = m->d_items.as<SubItem>();
 	q.counts = m->d_ctrl.as<uint32_t>();
 	q.overflow = m->d_ctrl.as<uint32_t>() + MAX_LEVELS;
@@ -946,12 +952,13 @@ constexpr size_t BATCH_BUDGET_BYTES = 24ull << 30;
 constexpr int HOST_PROLOGUE_MAX = 16;
 
 int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, int nrefs, const QueueSet &q,
-                        bool host_prologue)
+                        bool host_prologue, bool recompute)
 {
 	const int nprof = a.n_profiles;
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
 	cudaStream_t s = m->stream;
-	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *jac = m->d_jac.as<float>();
+	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>();
+	float *jac = recompute ? nullptr : m->d_jac.as<float>();
 	double *model64 = m->d_model64.as<double>();
 	float *wseed = m->d_wseed.as<float>(), *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>();
 	const int *ref_profile = bs.d_refs.as<int>(), *ref_offset = ref_profile + nrefs, *ref_code = ref_offset + nrefs;
@@ -988,8 +995,12 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		PF_TRY(adjoint_conv32(m, a, wseed, gconv, C));
 	else
 		gconv = gplain;
-	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix,
-	                          bs.d_T.as<double>(), s));
+	if (recompute)
+		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh, m->sx, m->sy, gconv,
+		                                 gplain, a.levels, q, bs.d_T.as<double>(), s));
+	else
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix,
+		                          bs.d_T.as<double>(), s));
 	PF_CUDA(launch_batch_gradient(bs.d_dev.as<DevProfile>(), nprof, C, ref_profile, ref_code, nrefs,
 	                              bs.d_T.as<double>(), bs.d_ll.as<double>(), bs.d_invalid.as<int>(),
 	                              bs.d_out_ll.as<double>(), bs.d_out_grad.as<double>(), s));
@@ -1046,7 +1057,10 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 
 	// chunk size from the memory budget (tangent planes dominate)
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
-	size_t per = npix * (4 * 4 + 8 * 2 + (size_t)nprof * NTAN * 4) + nout * (8 + 4) + 4096;
+	const size_t planes = npix * (size_t)nprof * NTAN * 4;
+	const bool recompute = m->adjoint_mode == PF_ADJOINT_RECOMPUTE ||
+	                       (m->adjoint_mode == PF_ADJOINT_AUTO && planes > (256ull << 20));
+	size_t per = npix * (4 * 4 + 8 * 2) + (recompute ? 0 : planes) + nout * (8 + 4) + 4096;
 	if (a.conv && m->conv_kind == CONV_FFT) {
 		const size_t spec = (size_t)fft_good_size((int)a.dh + (int)m->psf_h - 1) *
 		                    (fft_good_size((int)a.dw + (int)m->psf_w - 1) / 2 + 1);
@@ -1071,7 +1085,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	PF_CUDA(ensure(bs.h_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
 	PF_CUDA(ensure(m->d_conv32, npix * C * 4));
 	PF_CUDA(ensure(m->d_plain32, npix * C * 4));
-	PF_CUDA(ensure(m->d_jac, npix * NTAN * nprof * C * 4));
+	if (!recompute) PF_CUDA(ensure(m->d_jac, npix * NTAN * nprof * C * 4));
 	PF_CUDA(ensure(m->d_model64, nout * C * 8));
 	PF_CUDA(ensure(m->d_wseed, nout * C * 4));
 	PF_CUDA(ensure(m->d_gconv, npix * C * 4));
@@ -1133,11 +1147,13 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		bool done = false;
 		for (int attempt = 0; attempt < 8 && !done; attempt++) {
 			QueueSet q;
-			PF_TRY(prepare_queue(m, a, npix * nprof * C, q, nullptr, nullptr));
+			PF_TRY(prepare_queue(m, a, npix * nprof * C, q, nullptr, nullptr, recompute));
 			std::vector<uint64_t> sig = graph_signature(m, a, true, q);
 			sig.push_back((uint64_t)C);
 			sig.push_back((uint64_t)nrefs);
 			sig.push_back((uint64_t)host_prologue);
+			sig.push_back((uint64_t)recompute);
+			sig.push_back((uint64_t)(uintptr_t)m->d_masks.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_dev.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_fprof.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_invalid.p);
@@ -1154,7 +1170,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				replayed = true;
 			}
 			else {
-				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue));
+				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute));
 			}
 			PF_CUDA(cudaStreamSynchronize(m->stream));
 			int retry = 0;
@@ -1172,7 +1188,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				unsigned long long before = g_launches.load();
 				cudaGraph_t graph = nullptr;
 				PF_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
-				int st = enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue);
+				int st = enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute);
 				cudaError_t ce = cudaStreamEndCapture(m->stream, &graph);
 				bs.graph_kernels = g_launches.load() - before;
 				g_launches -= bs.graph_kernels;
@@ -1655,6 +1671,15 @@ int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_para
 		return PF_OK;
 	}
 	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+}
+
+int pf_model_set_adjoint_mode(pf_model *m, int mode)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (mode != PF_ADJOINT_AUTO && mode != PF_ADJOINT_STORE && mode != PF_ADJOINT_RECOMPUTE)
+		return set_error(PF_E_INVALID, "unknown adjoint mode");
+	m->adjoint_mode = mode;
+	return PF_OK;
 }
 
 int pf_model_set_debug(pf_model *m, int value)

@@ -207,6 +207,25 @@ __device__ __forceinline__ T eval_val(const FProfile &p, T xp, T yp)
 	return eval_tan<T>(p, xp, yp).f;
 }
 
+// How one drawing pixel is integrated for one radial profile
+// (radial.cpp:321-339): not at all (beyond rscale_max), by one evaluation,
+// or by subsampling.  The forward pass and the recomputing adjoint must agree
+// pixel for pixel, so this is written with round-to-nearest intrinsics,
+// which no contraction or reassociation can change between kernels.
+enum PixelDecision : int { PD_ZERO = 0, PD_DIRECT = 1, PD_SUBSAMPLE = 2 };
+
+__device__ __forceinline__ int pixel_decision32(const FProfile &p, double x, double y, float &xp, float &yp)
+{
+	const float dx = __double2float_rn(__dsub_rn(x, p.cx));
+	const float dy = __double2float_rn(__dsub_rn(y, p.cy));
+	xp = __fadd_rn(__fmul_rn(dx, p.cos_ang), __fmul_rn(dy, p.sin_ang));
+	yp = __fadd_rn(__fmul_rn(-dx, p.sin_q), __fmul_rn(dy, p.cos_q));
+	const float r = __fsqrt_rn(__fadd_rn(__fmul_rn(xp, xp), __fmul_rn(yp, yp)));
+	if (p.r_max > 0.f && r > p.r_max) return PD_ZERO;
+	if (p.rough || r > p.r_switch) return PD_DIRECT;
+	return PD_SUBSAMPLE;
+}
+
 __device__ __forceinline__ void tan_to_j(const Tan<float> &t, float xp, float yp, float w, float *j)
 {
 	j[0] += w * t.f;
@@ -245,17 +264,15 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 			continue;
 		}
 		if (!is_radial_kind(p.kind)) continue;
-		const float dx = (float)(x - p.cx), dy = (float)(y - p.cy);
-		const float xp = dx * p.cos_ang + dy * p.sin_ang;
-		const float yp = -dx * p.sin_q + dy * p.cos_q;
-		const float r = sqrtf(xp * xp + yp * yp);
+		float xp, yp;
+		const int decision = pixel_decision32(p, x, y, xp, yp);
 		float jl[NTAN];
 #pragma unroll
 		for (int k = 0; k < NTAN; k++) jl[k] = 0.f;
-		if (p.r_max > 0.f && r > p.r_max) {
+		if (decision == PD_ZERO) {
 			// zero
 		}
-		else if (p.rough || r > p.r_switch) {
+		else if (decision == PD_DIRECT) {
 			Tan<float> t = eval_tan<float>(p, xp, yp);
 			acc[p.target] += p.flux_scale * t.f;
 			tan_to_j(t, xp, yp, 1.0f, jl);
@@ -291,7 +308,7 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 
 template <class T>
 __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &it, int level, const double *s_xy,
-                                             int lane, const QueueSet &q, float *sums)
+                                             int lane, const QueueSet &q, float *sums, uint32_t *mask_out)
 {
 	const unsigned res = it.res;
 	const double xbin = (it.x1 - it.x0) / res, ybin = (it.y1 - it.y0) / res;
@@ -300,31 +317,70 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 	const T adyp = fabs((T)(-xbin * (double)p.sin_q + ybin * (double)p.cos_q));
 	const T cos_a = (T)p.cos_ang, sin_a = (T)p.sin_ang, cos_q = (T)p.cos_q, sin_q = (T)p.sin_q;
 	const unsigned nsub = res * res;
+	// sub-points in warp-wide chunks of 32 so each chunk's accept bits can be
+	// gathered with one ballot (mask_out: the item's 8 words, or null)
+	for (unsigned base = 0; base < nsub; base += 32) {
+		const unsigned k = base + lane;
+		bool accepted = false;
+		if (k < nsub) {
+			unsigned ii = k / res, jj = k - ii * res;
+			const double x = s_xy[ii], y = s_xy[16 + jj];
+			const T dx = (T)x, dy = (T)y;
+			const T xp = dx * cos_a + dy * sin_a;
+			const T yp = -dx * sin_q + dy * cos_q;
+			Tan<T> t = eval_tan<T>(p, xp, yp);
+			accepted = true;
+			if (recurse) {
+				T testval = eval_val<T>(p, fabs(xp), fabs(yp) + adyp);
+				if (fabs(testval - t.f) > (T)p.acc * t.f) {
+					accepted = false;
+					SubItem c;
+					c.x0 = x - half_xbin;
+					c.x1 = x + half_xbin;
+					c.y0 = y - half_ybin;
+					c.y1 = y + half_ybin;
+					c.weight = it.weight / nsub;
+					c.pixel = it.pixel;
+					c.profile = it.profile;
+					c.res = it.res;
+					c.max_rec = it.max_rec;
+					if ((uint32_t)level + 1 < q.levels) queue_push(q, level + 1, c);
+					else atomicOr(q.overflow, 2u);
+				}
+			}
+			if (accepted) {
+				Tan<float> tf;
+				tf.f = (float)t.f;
+				tf.fx = (float)t.fx;
+				tf.fy = (float)t.fy;
+				tf.s1 = (float)t.s1;
+				tf.s2 = (float)t.s2;
+				tf.s3 = (float)t.s3;
+				tan_to_j(tf, (float)xp, (float)yp, 1.0f, sums);
+			}
+		}
+		const unsigned bits = __ballot_sync(0xffffffffu, accepted);
+		if (mask_out && lane == 0) mask_out[base >> 5] = bits;
+	}
+}
+
+// Adjoint of one item with its frozen decisions: the tangents of the
+// sub-points the forward pass accepted (mask bit set), summed.
+template <class T>
+__device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem &it, const double *s_xy, int lane,
+                                               const uint32_t *mask, float *sums)
+{
+	const unsigned res = it.res;
+	const T cos_a = (T)p.cos_ang, sin_a = (T)p.sin_ang, cos_q = (T)p.cos_q, sin_q = (T)p.sin_q;
+	const unsigned nsub = res * res;
 	for (unsigned k = lane; k < nsub; k += 32) {
+		if (!((mask[k >> 5] >> (k & 31)) & 1u)) continue;
 		unsigned ii = k / res, jj = k - ii * res;
 		const double x = s_xy[ii], y = s_xy[16 + jj];
 		const T dx = (T)x, dy = (T)y;
 		const T xp = dx * cos_a + dy * sin_a;
 		const T yp = -dx * sin_q + dy * cos_q;
 		Tan<T> t = eval_tan<T>(p, xp, yp);
-		if (recurse) {
-			T testval = eval_val<T>(p, fabs(xp), fabs(yp) + adyp);
-			if (fabs(testval - t.f) > (T)p.acc * t.f) {
-				SubItem c;
-				c.x0 = x - half_xbin;
-				c.x1 = x + half_xbin;
-				c.y0 = y - half_ybin;
-				c.y1 = y + half_ybin;
-				c.weight = it.weight / nsub;
-				c.pixel = it.pixel;
-				c.profile = it.profile;
-				c.res = it.res;
-				c.max_rec = it.max_rec;
-				if ((uint32_t)level + 1 < q.levels) queue_push(q, level + 1, c);
-				else atomicOr(q.overflow, 2u);
-				continue;
-			}
-		}
 		Tan<float> tf;
 		tf.f = (float)t.f;
 		tf.fx = (float)t.fx;
@@ -340,7 +396,7 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profiles, const SubItem &it, int level,
                                              unsigned npix, float *__restrict__ img_conv,
                                              float *__restrict__ img_plain, float *__restrict__ jac,
-                                             const QueueSet &q, double *s_xy, int lane)
+                                             const QueueSet &q, double *s_xy, int lane, uint32_t *mask_out)
 {
 	const FProfile &p = profiles[it.profile];
 	const unsigned res = it.res;
@@ -355,8 +411,8 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 	float sums[NTAN];
 #pragma unroll
 	for (int k = 0; k < NTAN; k++) sums[k] = 0.f;
-	if (level >= 3) level_points<double>(p, it, level, s_xy, lane, q, sums);
-	else level_points<float>(p, it, level, s_xy, lane, q, sums);
+	if (level >= 3) level_points<double>(p, it, level, s_xy, lane, q, sums, mask_out);
+	else level_points<float>(p, it, level, s_xy, lane, q, sums, mask_out);
 #pragma unroll
 	for (int k = 0; k < NTAN; k++) sums[k] = warp_sum(sums[k]);
 	if (lane == 0) {
@@ -384,7 +440,8 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
 	const SubItem *items = q.items + q.off[level];
 	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
 	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < n; w += nwarps)
-		level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane);
+		level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
+			             q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr);
 }
 
 // Levels first..levels-1 in one CTA.  Only the Sersic central cusp
@@ -405,8 +462,129 @@ __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restric
 		const uint32_t n = min(*(volatile uint32_t *)&q.counts[level], q.cap[level]);
 		const SubItem *items = q.items + q.off[level];
 		for (uint32_t w = wib; w < n; w += nwarps)
-			level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane);
+			level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
+			             q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr);
 	}
+}
+
+// ---------------------------------------------------------------------------
+// Recomputing adjoint (no stored tangent planes): used when the planes would
+// not fit, e.g. hundreds of profiles on a large field.  The forward pass
+// rendered values only and recorded each queued cell's accepted sub-points;
+// these kernels recompute the tangents against the known seed g.
+// ---------------------------------------------------------------------------
+
+// Directly evaluated pixels, one profile per blockIdx.z, 64 x 32 pixel tiles.
+// A tile whose nearest pixel centre is farther than rscale_max (+2 px) from
+// the profile centre is skipped: the elliptical radius is never smaller than
+// the Euclidean distance, so such pixels were zeroed by the forward pass.
+__global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__restrict__ profiles,
+                                                          const int *__restrict__ prof_batch, unsigned width,
+                                                          unsigned height, double sx, double sy,
+                                                          const float *__restrict__ g_conv,
+                                                          const float *__restrict__ g_plain, double *__restrict__ T)
+{
+	const int pi = blockIdx.z;
+	const FProfile &p = profiles[pi];
+	if (!is_radial_kind(p.kind)) return;
+	const unsigned tx0 = blockIdx.x * 64, ty0 = blockIdx.y * 32;
+	const double half_xbin = sx / 2., half_ybin = sy / 2.;
+	if (p.r_max > 0.f) {
+		const unsigned tx1 = min(tx0 + 63, width - 1), ty1 = min(ty0 + 31, height - 1);
+		const double xlo = half_xbin + tx0 * sy, xhi = half_xbin + tx1 * sy;
+		const double ylo = half_ybin + ty0 * sx, yhi = half_ybin + ty1 * sx;
+		const double nx = fmin(fmax(p.cx, xlo), xhi) - p.cx, ny = fmin(fmax(p.cy, ylo), yhi) - p.cy;
+		if (sqrt(nx * nx + ny * ny) > (double)p.r_max + 2.0) return;
+	}
+	const size_t npix = (size_t)width * height;
+	const float *g = (p.target == 0 ? g_conv : g_plain) + (size_t)prof_batch[pi] * npix;
+	float acc[NTAN];
+#pragma unroll
+	for (int k = 0; k < NTAN; k++) acc[k] = 0.f;
+	const unsigned i = tx0 + (threadIdx.x & 63);
+	for (unsigned r = threadIdx.x >> 6; r < 32; r += 4) {
+		const unsigned j = ty0 + r;
+		if (i >= width || j >= height) continue;
+		const float gv = g[i + (size_t)j * width];
+		if (gv == 0.f) continue;
+		const double y = half_ybin + j * sx, x = half_xbin + i * sy;
+		float xp, yp;
+		if (pixel_decision32(p, x, y, xp, yp) != PD_DIRECT) continue;
+		Tan<float> t = eval_tan<float>(p, xp, yp);
+		tan_to_j(t, xp, yp, gv, acc);
+	}
+	__shared__ double s_red[NTAN][8];
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+	for (int k = 0; k < NTAN; k++) {
+		double v = warp_sum((double)acc[k]);
+		if (lane == 0) s_red[k][wid] = v;
+	}
+	__syncthreads();
+	if (threadIdx.x < NTAN) {
+		double v = 0;
+		for (int w = 0; w < 8; w++) v += s_red[threadIdx.x][w];
+		if (v != 0.0) atomicAdd(&T[(size_t)pi * NTAN + threadIdx.x], v);
+	}
+}
+
+// Every queued cell of every level, one warp per cell: the tangents of the
+// accepted sub-points, times the cell weight and g(pixel).
+__global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restrict__ profiles, int levels,
+                                                         const float *__restrict__ g_conv,
+                                                         const float *__restrict__ g_plain, QueueSet q,
+                                                         double *__restrict__ T)
+{
+	__shared__ double s_xy[8][32];
+	const int lane = threadIdx.x & 31;
+	const int wib = threadIdx.x >> 5;
+	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
+	const uint32_t gw = blockIdx.x * (blockDim.x >> 5) + wib;
+	for (int level = 0; level < levels; level++) {
+		const uint32_t n = min(q.counts[level], q.cap[level]);
+		const SubItem *items = q.items + q.off[level];
+		for (uint32_t w = gw; w < n; w += nwarps) {
+			const SubItem it = items[w];
+			const FProfile &p = profiles[it.profile];
+			const unsigned res = it.res;
+			const double half_xbin = (it.x1 - it.x0) / res / 2., half_ybin = (it.y1 - it.y0) / res / 2.;
+			if (lane < 16) {
+				if (lane < (int)res) s_xy[wib][lane] = it.x0 + (2 * lane + 1) * half_xbin;
+			}
+			else if (lane - 16 < (int)res) {
+				s_xy[wib][lane] = it.y0 + (2 * (lane - 16) + 1) * half_ybin;
+			}
+			__syncwarp();
+			const uint32_t *mask = q.masks + ((size_t)q.off[level] + w) * MASK_WORDS;
+			float sums[NTAN];
+#pragma unroll
+			for (int k = 0; k < NTAN; k++) sums[k] = 0.f;
+			if (level >= 3) adjoint_points<double>(p, it, s_xy[wib], lane, mask, sums);
+			else adjoint_points<float>(p, it, s_xy[wib], lane, mask, sums);
+#pragma unroll
+			for (int k = 0; k < NTAN; k++) sums[k] = warp_sum(sums[k]);
+			if (lane == 0) {
+				const float gv = (p.target == 0 ? g_conv : g_plain)[it.pixel];
+				const double coef = (double)gv * it.weight;
+				if (coef != 0.0) {
+#pragma unroll
+					for (int k = 0; k < NTAN; k++) atomicAdd(&T[(size_t)it.profile * NTAN + k], coef * (double)sums[k]);
+				}
+			}
+			__syncwarp();
+		}
+	}
+}
+
+cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
+                                     unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
+                                     int levels, const QueueSet &q, double *T, cudaStream_t s)
+{
+	dim3 grid((width + 63) / 64, (height + 31) / 32, n_profiles);
+	k_adjoint_pixels32<<<grid, 256, 0, s>>>(profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
+	k_adjoint_items32<<<148 * 8, 256, 0, s>>>(profiles, levels, g_conv, g_plain, q, T);
+	note_launches(2);
+	return cudaGetLastError();
 }
 
 // sum over pixels of g(pixel) * J_k(pixel) for each radial profile:

@@ -106,6 +106,25 @@ def sampler_batch(n: int = 4096, seed_tag: int = 3) -> Tuple[Dict, np.ndarray]:
     return wl, vals
 
 
+def large_field(n_profiles: int = 200, width: int = 2000, height: int = 2000, psf_size: int = 101,
+                seed_tag: int = 5, magzero: float = 30.0) -> Dict:
+    """Sersic components placed uniformly over a large field: mag ~ U[14, 22],
+    nser ~ logU[0.5, 8], re ~ logU[1, 60] px, ang ~ U[0, 180], axrat ~ U[0.3, 1];
+    Moffat PSF (fwhm 3, con 2.5) with the FFT convolver; all 8 parameters of
+    every component in the gradient."""
+    r = _rng(seed_tag)
+    profs = []
+    for _ in range(n_profiles):
+        profs.append(("sersic", dict(xcen=r.uniform(0, width), ycen=r.uniform(0, height), mag=r.uniform(14, 22),
+                                     nser=float(np.exp(r.uniform(np.log(0.5), np.log(8)))),
+                                     re=float(np.exp(r.uniform(0, np.log(60)))), ang=r.uniform(0, 180),
+                                     axrat=r.uniform(0.3, 1.0), box=0.0, convolve=True)))
+    grad = [(i, k) for i in range(n_profiles) for k in ("xcen", "ycen", "mag", "re", "nser", "ang", "axrat", "box")]
+    return dict(name="large_field", width=width, height=height, magzero=magzero,
+                psf=moffat_psf(psf_size, 3.0, 2.5), convolver="fft", profiles=profs, grad=grad,
+                sigma_range=(1.0, 1.0), seed_tag=seed_tag)
+
+
 def make_data(w: Dict, model_image: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
     """Data = model + N(0, sigma) with a per-pixel sigma map ~ U[sigma_range]."""
     r = _rng(1000 + w["seed_tag"])
