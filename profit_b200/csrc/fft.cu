@@ -487,6 +487,10 @@ template cudaError_t FftConv<double>::convolve<float, double, float>(const float
                                                                     bool, Cplx *, int, int, double *, int, int,
                                                                     const float *, int, int, int, int, size_t,
                                                                     size_t, size_t, cudaStream_t);
+template cudaError_t FftConv<double>::convolve<float, float, float>(const float *, int, int, int, int, const Cplx *,
+                                                                   bool, Cplx *, int, int, float *, int, int,
+                                                                   const float *, int, int, int, int, size_t, size_t,
+                                                                   size_t, cudaStream_t);
 template cudaError_t FftConv<float>::convolve<float, float, float>(const float *, int, int, int, int, const Cplx *,
                                                                   bool, Cplx *, int, int, float *, int, int,
                                                                   const float *, int, int, int, int, size_t, size_t,

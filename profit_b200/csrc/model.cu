@@ -567,7 +567,7 @@ int forward_conv32(pf_model *m, const Analysis &a, const float *conv, const floa
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.cw * a.ch;
 	const bool conv_on = a.conv && m->conv_kind != CONV_NULL;
 	if (conv_on && m->conv_kind == CONV_FFT) {
-		PF_TRY(prepare_fft(m, a, batch, true));
+		PF_TRY(prepare_fft(m, a, batch, false));
 		int dx, dy;
 		fft_offsets(m, a, dx, dy);
 		PF_CUDA(m->fft64.convolve<float, double, float>(conv, a.dw, a.dh, 0, 0, m->d_kspec64.as<double2>(), false,
@@ -603,12 +603,15 @@ int adjoint_conv32(pf_model *m, const Analysis &a, const float *wseed, float *gc
 {
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
 	if (m->conv_kind == CONV_FFT) {
-		PF_TRY(prepare_fft(m, a, batch, true));
+		PF_TRY(prepare_fft(m, a, batch, false));
 		int dx, dy;
 		fft_offsets(m, a, dx, dy);
-		// g(U) = sum_x w(x) psf(x + d - U): correlation of w placed at d
-		PF_CUDA(m->fft32.convolve<float, float, float>(wseed, a.ow, a.oh, dx, dy, m->d_kspec32.as<float2>(), true,
-		                                               m->d_fftwork32.as<float2>(), 0, 0, gconv, a.dw, a.dh, nullptr,
+		// g(U) = sum_x w(x) psf(x + d - U): correlation of w placed at d.  The
+		// transforms are FP64: FFT roundoff is spread over the whole grid, and
+		// in FP32 the error from a bright source's seed swamps the seed of a
+		// faint one elsewhere in the field.
+		PF_CUDA(m->fft64.convolve<float, float, float>(wseed, a.ow, a.oh, dx, dy, m->d_kspec64.as<double2>(), true,
+		                                               m->d_fftwork64.as<double2>(), 0, 0, gconv, a.dw, a.dh, nullptr,
 		                                               0, 0, 0, batch, nout, npix, 0, m->stream));
 		note_launches(3);
 		return PF_OK;
