@@ -163,13 +163,18 @@ def test_large_field_fft_fp64_and_recompute_gradient():
     refs = [(i, k) for (i, k) in w2["grad"] if i in (0, 5)]
     mp = W.configure(Model(wl["width"], wl["height"]), w2)
     mp.set_data(image, sigma)
-    _, g_fd = mp.loglike_grad_fd(refs, rel_step=1e-7)
+    # A subsampling decision that flips inside +-h puts a jump into a finite
+    # difference; two step sizes guard against it (the adjoint differentiates
+    # the quadrature with decisions held fixed).
+    _, g_fd7 = mp.loglike_grad_fd(refs, rel_step=1e-7)
+    _, g_fd6 = mp.loglike_grad_fd(refs, rel_step=1e-6)
     from profit_b200._capi import PF_ADJOINT_RECOMPUTE
     mp.set_precision(PF_FP32)
     mp.set_adjoint_mode(PF_ADJOINT_RECOMPUTE)
     _, g_ad = mp.loglike_grad(refs)
-    err = np.max(np.abs(g_ad - g_fd)) / np.max(np.abs(g_fd))
-    assert err <= 1e-5, list(zip(refs, g_fd, g_ad))
+    scale = np.max(np.abs(g_fd7))
+    err = np.minimum(np.abs(g_ad - g_fd7), np.abs(g_ad - g_fd6)) / scale
+    assert np.all(err <= 1e-5), list(zip(refs, g_fd7, g_fd6, g_ad))
 
 
 def test_errors_match_libprofit():
