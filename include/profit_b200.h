@@ -183,6 +183,47 @@ int pf_model_set_adjoint_mode(pf_model *m, int mode);
 int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_params,
                              double rel_step, double *loglike, double *grad);
 
+/* ---- Likelihood of device-resident images, allocating nothing ----------
+ * No counterpart in libprofit or ProFit: it is the "norm" log-likelihood of
+ * profitLikeModel (R/profitLikeModel.R:263-276), the sum pf_model_loglike
+ * forms, over images that the caller already keeps on the device.
+ *
+ * It exists for callers that cannot allocate device memory between
+ * evaluations.  A sampler that has reserved nearly all of the GPU's memory
+ * for its own pool of proposals would see a cudaMalloc fail; and cudaMalloc
+ * and cudaFree can synchronise the whole device, stalling every other stream
+ * the caller keeps busy.  So this call allocates nothing, on the device or on
+ * the host: its scratch (the per-block partial sums) is a fixed array inside
+ * this library, PF_LOGLIKE_NOALLOC_MAX_BATCH x 296 x 16 bytes (296 KiB) per
+ * device.
+ *
+ *   model    device, batch images of npix doubles each, back to back
+ *   data     device, npix doubles (the same image for every model)
+ *   sigma    device, npix doubles
+ *   region   device, npix bytes, nonzero = pixel used; NULL = all pixels
+ *   loglike  device, batch doubles, written by the call
+ *   stream   a cudaStream_t (NULL = the legacy default stream)
+ *
+ * The call only queues two kernels on `stream` on the calling thread's
+ * current device and returns; read `loglike` after the stream has finished.
+ * It forms pf_model_loglike's (PF_FP64) compensated sum over the same fixed
+ * grid of blocks, so equal images give equal results to the last bit.
+ * batch above PF_LOGLIKE_NOALLOC_MAX_BATCH, or npix above
+ * 2^31 - 1, fails with PF_E_CAPACITY before anything is queued.
+ *
+ * The first call on each device looks up the scratch array's address with
+ * that device current (cudaGetSymbolAddress, which may load this library's
+ * device code); make that first call before any stream capture begins.
+ * All calls on a device share the one array, which keeps the last call's
+ * contents (no call relies on it starting at zero).  Calls whose kernels can
+ * run at the same time on the GPU, i.e. on different streams with nothing
+ * ordering them, corrupt each other's sums: issue them on one stream, or
+ * order the streams with events. */
+#define PF_LOGLIKE_NOALLOC_MAX_BATCH 64
+int pf_loglike_norm_noalloc(const double *model, const double *data, const double *sigma,
+                            const uint8_t *region, size_t npix, int batch, double *loglike,
+                            void *stream);
+
 /* ---- Instrumentation ---------------------------------------------------
  * With debug on, evaluations record for each radial profile the number of
  * subsample_pixel calls per drawing pixel (-1 = beyond rscale_max, 0 =

@@ -125,10 +125,15 @@ def _late_bindings(L):
     L.pf_model_set_parameters.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, _dp]
     L.pf_model_loglike_grad_batch.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, C.c_int, _dp, _dp, _dp]
     L.pf_model_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
+    # device pointers travel as plain integers (e.g. a torch tensor's data_ptr())
+    L.pf_loglike_norm_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
+                                          C.c_void_p, C.c_void_p]
 
 
 PF_ADJOINT_AUTO = 0
 PF_ADJOINT_STORE = 1
 PF_ADJOINT_RECOMPUTE = 2
+PF_LOGLIKE_NOALLOC_MAX_BATCH = 64
 
-EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch", "pf_model_set_adjoint_mode")
+EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch", "pf_model_set_adjoint_mode",
+                       "pf_loglike_norm_noalloc")

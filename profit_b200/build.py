@@ -32,6 +32,7 @@ UNITS = {
     "render32.cu": [],
     "fft.cu": [],
     "model.cu": ["--fmad=false"],
+    "like_noalloc.cu": ["--fmad=false"],
 }
 
 

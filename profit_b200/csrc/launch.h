@@ -11,6 +11,9 @@ namespace pf {
 // Adds n to the process-wide count of kernels launched by this library.
 void note_launches(int n);
 
+// Stores `msg` as the calling thread's pf_last_error() text; returns `code`.
+int report_error(int code, const char *msg);
+
 // render64.cu
 cudaError_t launch_pixels64(const DevProfile *profiles, int n_profiles, unsigned width, unsigned height, double sx,
                             double sy, double *img_conv, double *img_plain, const QueueSet &q, cudaStream_t s);

@@ -1275,6 +1275,11 @@ std::string trim(const std::string &s)
 
 }  // namespace
 
+namespace pf {
+// Lets the other translation units of the C ABI report through pf_last_error().
+int report_error(int code, const char *msg) { return set_error(code, msg); }
+}  // namespace pf
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
