@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sampler-n", type=int, default=4096,
+                    help="proposals per call of the sampler-batch line (smaller for profiling runs)")
     return ap.parse_args()
 
 
@@ -317,7 +319,7 @@ def main_b200(args):
             "algorithmic": f"2*P^2*W*H = {flop:.3e} FLOP per launch (P={P}, W*H={n_out})",
             "peak_source": "measured: dependent FMA streams, libpf_peaks.so, best of 5 (burst)"}
 
-    sampler = sampler_batch_rate(args, torch, flush)
+    sampler = sampler_batch_rate(args, torch, flush, n=args.sampler_n)
 
     out = None
     if rank == 0:
@@ -373,6 +375,7 @@ def sampler_batch_rate(args, torch, flush, n=4096, calls=3):
     times = []
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("sampler")
     for _ in range(calls):
         flush.zero_()
         torch.cuda.synchronize()
@@ -381,6 +384,7 @@ def sampler_batch_rate(args, torch, flush, n=4096, calls=3):
         ev1.record()
         ev1.synchronize()
         times.append(ev0.elapsed_time(ev1) / 1e3)
+    torch.cuda.nvtx.range_pop()
     m.close()
     rate = n / statistics.mean(times)
     return {"workload": "single Sersic 200x200, 31x31 Gaussian PSF, brute force, 8-parameter gradient; "
@@ -397,7 +401,8 @@ def measured_fp32_peak():
         lib = ctypes.CDLL(path)
         lib.pf_peak_fma_tflops.restype = ctypes.c_double
         lib.pf_peak_fma_tflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
-        v = lib.pf_peak_fma_tflops(0, 4096, 5)
+        # the FP32 ceiling: plain FMA and packed FP32-pair FMA, whichever is higher
+        v = max(lib.pf_peak_fma_tflops(0, 4096, 5), lib.pf_peak_fma_tflops(2, 4096, 5))
         return v if v > 0 else None
     except OSError:
         return None

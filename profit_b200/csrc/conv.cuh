@@ -210,6 +210,8 @@ struct ConvArgs {
 	int ow, oh;
 	const void *add;
 	int add_stride, add_ox, add_oy, batch, batch_src_stride, batch_out_stride;
+	void *scratch = nullptr;  // FP64 partial images for kernels that split the kernel columns over CTAs
+	size_t scratch_bytes = 0;
 };
 
 template <class T, class Acc, class TOut, int RY, int TYT, int KS>

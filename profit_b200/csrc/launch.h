@@ -39,16 +39,26 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
                             const QueueSet &q, cudaStream_t s);
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
                             float *jac, const QueueSet &q, cudaStream_t s);
+// partials: n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN doubles;
+// tickets: n_profiles zero-initialised counters (left at zero again).
+unsigned jac_reduce_blocks(unsigned npix, int n_profiles);
 cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
-                              const int *prof_batch, int n_profiles, unsigned npix, double *out, cudaStream_t s);
+                              const int *prof_batch, int n_profiles, unsigned npix, double *partials,
+                              unsigned *tickets, double *out, cudaStream_t s);
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
                               unsigned dh, int batch, float *g_plain, cudaStream_t s);
 cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                                double *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
-                               int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s);
+                               int batch, int batch_src_stride, int batch_out_stride, double *scratch,
+                               size_t scratch_bytes, cudaStream_t s);
 cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                           float *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
-                          int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s);
+                          int batch, int batch_src_stride, int batch_out_stride, double *scratch, size_t scratch_bytes,
+                          cudaStream_t s);
+// FP64 scratch (bytes) that lets the FP32 convolution split kernel columns
+// over CTAs for `batch` outputs of ow x oh; 0 when the batch is large enough
+// to fill the GPU without it.
+size_t conv32_scratch_bytes(int ow, int oh, int batch);
 cudaError_t launch_loglike32(const float *model, const double *data, const double *sigma, const uint8_t *region,
                              int n, int batch, int data_batch_stride, double2 *partials, int nparts, double *out,
                              float *wseed, cudaStream_t s);

@@ -11,6 +11,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -35,6 +36,16 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 	static std::mutex mu;
 	static std::map<Key, int> choice;
 	Key key{type_tag, a.sw, a.sh, a.kw, a.kh, a.ow, a.oh, a.batch};
+	// PF_CONV_FORCE=<index> runs that candidate whenever it applies (tests
+	// check every candidate against the FP64 form this way)
+	if (const char *fv = getenv("PF_CONV_FORCE")) {
+		int f = fv[0] ? atoi(fv) : -1;
+		if (f >= 0 && f < n_cands && cands[f].smem(a.kw, a.kh) <= 227 * 1024) {
+			cudaError_t e = cands[f].run(a, s);
+			if (e != cudaErrorInvalidValue) return e;
+			cudaGetLastError();  // not applicable here: use the tuned choice
+		}
+	}
 	int pick = -1;
 	{
 		std::lock_guard<std::mutex> g(mu);
@@ -59,6 +70,9 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 			cudaEventCreate(&e0);
 			cudaEventCreate(&e1);
 			float best = 1e30f;
+			// PF_AUTOTUNE_LOG=1 prints every candidate's time to stderr
+			const char *lv = getenv("PF_AUTOTUNE_LOG");
+			const bool log = lv && lv[0] == '1';
 			for (int c = 0; c < n_cands; c++) {
 				if (cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
 				cudaError_t e = cands[c].run(a, s);  // warm-up (and attribute setup)
@@ -69,6 +83,9 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 				if (cudaEventSynchronize(e1) != cudaSuccess) break;
 				float ms = 0;
 				cudaEventElapsedTime(&ms, e0, e1);
+				if (log)
+					fprintf(stderr, "[profit_b200 autotune] type %d src %dx%d psf %dx%d out %dx%d batch %d: candidate %d %.4f ms\n",
+					        type_tag, a.sw, a.sh, a.kw, a.kh, a.ow, a.oh, a.batch, c, ms / 3);
 				if (ms < best) {
 					best = ms;
 					pick = c;
@@ -77,6 +94,7 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 			cudaEventDestroy(e0);
 			cudaEventDestroy(e1);
 			if (pick < 0) pick = first_fit;
+			if (log) fprintf(stderr, "[profit_b200 autotune] type %d: picked candidate %d\n", type_tag, pick);
 			std::lock_guard<std::mutex> g(mu);
 			choice[key] = pick;
 		}
@@ -306,6 +324,8 @@ struct pf_model {
 	DevBuf d_conv64, d_plain64, d_model64;
 	DevBuf d_conv32, d_plain32, d_model32, d_jac, d_gconv, d_gplain, d_wseed;
 	DevBuf d_psf64, d_psfrev64, d_psf32, d_psfrev32;
+	DevBuf d_convsplit;  // FP64 partial images of column-split convolutions
+	DevBuf d_jac_partials, d_jac_tickets;  // per-block sums and tickets of the tangent reduction
 	DevBuf d_items, d_masks, d_ctrl, d_partials, d_results;
 	int adjoint_mode = PF_ADJOINT_AUTO;
 	DevBuf d_decisions, d_level_counts;
@@ -592,8 +612,11 @@ int forward_conv32(pf_model *m, const Analysis &a, const float *conv, const floa
 		}
 		return PF_OK;
 	}
+	size_t sb = conv32_scratch_bytes(a.cw, a.ch, batch);
+	if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
 	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64, a.cw,
-	                           a.ch, plain, a.dw, a.padx, a.pady, batch, (int)npix, (int)nout, m->stream));
+	                           a.ch, plain, a.dw, a.padx, a.pady, batch, (int)npix, (int)nout,
+	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, m->stream));
 	return PF_OK;
 }
 
@@ -616,8 +639,11 @@ int adjoint_conv32(pf_model *m, const Analysis &a, const float *wseed, float *gc
 		note_launches(3);
 		return PF_OK;
 	}
+	size_t sb = conv32_scratch_bytes(a.dw, a.dh, batch);
+	if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
 	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(), m->psf_w,
-	                      m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, batch, (int)nout, (int)npix, m->stream));
+	                      m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, batch, (int)nout, (int)npix,
+	                      sb ? m->d_convsplit.as<double>() : nullptr, sb, m->stream));
 	return PF_OK;
 }
 
@@ -728,6 +754,20 @@ int evaluate64(pf_model *m, Analysis &a)
 // FP32 path with forward tangents and the adjoint reduction
 // ---------------------------------------------------------------------------
 
+// Scratch of launch_jac_reduce for n_profiles profiles over npix pixels; the
+// tickets start at zero when allocated and the kernel leaves them at zero.
+int jac_scratch(pf_model *m, unsigned npix, int n_profiles, double **partials, unsigned **tickets)
+{
+	const size_t pb = (size_t)n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN * sizeof(double);
+	PF_CUDA(ensure(m->d_jac_partials, pb));
+	void *before = m->d_jac_tickets.p;
+	PF_CUDA(ensure(m->d_jac_tickets, (size_t)n_profiles * sizeof(unsigned)));
+	if (m->d_jac_tickets.p != before) PF_CUDA(cudaMemsetAsync(m->d_jac_tickets.p, 0, m->d_jac_tickets.bytes, m->stream));
+	*partials = m->d_jac_partials.as<double>();
+	*tickets = m->d_jac_tickets.as<unsigned>();
+	return PF_OK;
+}
+
 int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q, bool want_grad, double *d_out)
 {
 	size_t npix = (size_t)a.dw * a.dh;
@@ -771,8 +811,11 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		else
 			gconv = gplain;
 		PF_CUDA(cudaMemsetAsync(d_out + ResultLayout::T0, 0, (size_t)nprof * NTAN * 8, m->stream));
-		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix,
-		                          d_out + ResultLayout::T0, m->stream));
+		double *jpart;
+		unsigned *jtick;
+		PF_TRY(jac_scratch(m, (unsigned)npix, nprof, &jpart, &jtick));
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix, jpart,
+		                          jtick, d_out + ResultLayout::T0, m->stream));
 	}
 	PF_CUDA(record_event(m->ev[3], m->stream));
 	return PF_OK;
@@ -811,7 +854,7 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 	const DevBuf *bufs[] = {&m->d_fprof, &m->d_prof_begin, &m->d_prof_batch, &m->d_conv32, &m->d_plain32,
 	                        &m->d_model64, &m->d_conv64, &m->d_plain64, &m->d_jac, &m->d_gconv, &m->d_gplain,
 	                        &m->d_wseed, &m->d_items, &m->d_ctrl, &m->d_partials, &m->d_results, &m->d_psf32,
-	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region};
+	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region, &m->d_convsplit, &m->d_jac_partials, &m->d_jac_tickets};
 	for (auto *b : bufs) s.push_back((uint64_t)(uintptr_t)b->p);
 	s.push_back((uint64_t)(uintptr_t)m->h_fprof.p);
 	s.push_back((uint64_t)(uintptr_t)m->h_results.p);
@@ -1001,9 +1044,13 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	if (recompute)
 		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh, m->sx, m->sy, gconv,
 		                                 gplain, a.levels, q, bs.d_T.as<double>(), s));
-	else
+	else {
+		double *jpart;
+		unsigned *jtick;
+		PF_TRY(jac_scratch(m, (unsigned)npix, C * nprof, &jpart, &jtick));
 		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix,
-		                          bs.d_T.as<double>(), s));
+		                          jpart, jtick, bs.d_T.as<double>(), s));
+	}
 	PF_CUDA(launch_batch_gradient(bs.d_dev.as<DevProfile>(), nprof, C, ref_profile, ref_code, nrefs,
 	                              bs.d_T.as<double>(), bs.d_ll.as<double>(), bs.d_invalid.as<int>(),
 	                              bs.d_out_ll.as<double>(), bs.d_out_grad.as<double>(), s));

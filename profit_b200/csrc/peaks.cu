@@ -26,7 +26,31 @@ __global__ void k_fma(T *out, int iters, T a, T b)
 	out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
 }
 
-template <class T>
+// The same with packed FP32 pairs (fma.rn.f32x2 on sm_100): 16 FMAs per
+// thread and step from 8 packed instructions.
+__global__ void k_fma2(float *out, int iters, float a, float b)
+{
+	const float2 A = make_float2(a, a), B = make_float2(b, b);
+	float t = threadIdx.x;
+	float2 x0 = make_float2(t, t + 1), x1 = make_float2(t + 2, t + 3), x2 = make_float2(t + 4, t + 5),
+	       x3 = make_float2(t + 6, t + 7), x4 = make_float2(t + 8, t + 9), x5 = make_float2(t + 10, t + 11),
+	       x6 = make_float2(t + 12, t + 13), x7 = make_float2(t + 14, t + 15);
+	for (int i = 0; i < iters; i++) {
+		x0 = __ffma2_rn(x0, A, B);
+		x1 = __ffma2_rn(x1, A, B);
+		x2 = __ffma2_rn(x2, A, B);
+		x3 = __ffma2_rn(x3, A, B);
+		x4 = __ffma2_rn(x4, A, B);
+		x5 = __ffma2_rn(x5, A, B);
+		x6 = __ffma2_rn(x6, A, B);
+		x7 = __ffma2_rn(x7, A, B);
+	}
+	float s = x0.x + x0.y + x1.x + x1.y + x2.x + x2.y + x3.x + x3.y + x4.x + x4.y + x5.x + x5.y + x6.x + x6.y +
+	          x7.x + x7.y;
+	out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+template <class T, bool Packed = false>
 double run(int iters, int reps)
 {
 	int dev = 0, sms = 0;
@@ -38,11 +62,17 @@ double run(int iters, int reps)
 	cudaEvent_t e0, e1;
 	cudaEventCreate(&e0);
 	cudaEventCreate(&e1);
-	k_fma<T><<<blocks, threads>>>(out, iters, (T)0.999999, (T)1e-6);
+	auto launch = [&]() {
+		if constexpr (Packed)
+			k_fma2<<<blocks, threads>>>(out, iters, 0.999999f, 1e-6f);
+		else
+			k_fma<T><<<blocks, threads>>>(out, iters, (T)0.999999, (T)1e-6);
+	};
+	launch();
 	float best = 1e30f;
 	for (int r = 0; r < reps; r++) {
 		cudaEventRecord(e0);
-		k_fma<T><<<blocks, threads>>>(out, iters, (T)0.999999, (T)1e-6);
+		launch();
 		cudaEventRecord(e1);
 		cudaEventSynchronize(e1);
 		float ms = 0;
@@ -53,7 +83,7 @@ double run(int iters, int reps)
 	cudaEventDestroy(e1);
 	cudaFree(out);
 	if (cudaGetLastError() != cudaSuccess) return -1;
-	double flops = 2.0 * 8.0 * iters * threads * (double)blocks;
+	double flops = 2.0 * (Packed ? 16.0 : 8.0) * iters * threads * (double)blocks;
 	return flops / (best * 1e-3) / 1e12;
 }
 
@@ -62,8 +92,11 @@ double run(int iters, int reps)
 extern "C" {
 
 // TFLOP/s of dependent-chain FMA streams, best of `reps` launches.
-double pf_peak_fma_tflops(int fp64, int iters, int reps)
+// kind: 0 = FP32 FMA, 1 = FP64 FMA, 2 = packed FP32 pairs (FFMA2).
+double pf_peak_fma_tflops(int kind, int iters, int reps)
 {
-	return fp64 ? run<double>(iters, reps) : run<float>(iters, reps);
+	if (kind == 1) return run<double>(iters, reps);
+	if (kind == 2) return run<float, true>(iters, reps);
+	return run<float>(iters, reps);
 }
 }

@@ -24,6 +24,7 @@
 
 #include "common.cuh"
 #include "conv.cuh"
+#include "conv2.cuh"
 #include "launch.h"
 #include "like.cuh"
 
@@ -588,12 +589,20 @@ cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_b
 }
 
 // sum over pixels of g(pixel) * J_k(pixel) for each radial profile:
-// blockIdx.y = profile, grid-stride over pixels, one FP64 atomic per block
-// and tangent component.
-__global__ void k_jac_reduce(const float *__restrict__ jac, const float *__restrict__ g_conv,
-                             const float *__restrict__ g_plain, const FProfile *__restrict__ profiles,
-                             const int *__restrict__ prof_batch, unsigned npix, double *__restrict__ out)
+// blockIdx.y = profile, blockIdx.x strides over the pixels, four pixels per
+// thread and step with every load issued before the products (enough bytes
+// in flight to stream the tangent planes at HBM speed).  Each block writes
+// its NTAN sums to `partials`; the block that finishes last (an atomic
+// ticket per profile, no waiting) adds the partials in block order and
+// resets the ticket, so the result does not depend on block scheduling.
+__global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ jac, const float *__restrict__ g_conv,
+                                                    const float *__restrict__ g_plain,
+                                                    const FProfile *__restrict__ profiles,
+                                                    const int *__restrict__ prof_batch, unsigned npix,
+                                                    double *__restrict__ partials, unsigned *__restrict__ tickets,
+                                                    double *__restrict__ out)
 {
+	constexpr int U = 4;
 	const int pi = blockIdx.y;
 	const FProfile &p = profiles[pi];
 	if (!is_radial_kind(p.kind)) return;
@@ -603,13 +612,26 @@ __global__ void k_jac_reduce(const float *__restrict__ jac, const float *__restr
 	double acc[NTAN];
 #pragma unroll
 	for (int k = 0; k < NTAN; k++) acc[k] = 0.0;
-	for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < npix; t += gridDim.x * blockDim.x) {
-		float gv = g[t];
-		if (gv == 0.f) continue;
+	const unsigned step = gridDim.x * blockDim.x * U;
+	for (unsigned t0 = blockIdx.x * blockDim.x * U + threadIdx.x; t0 < npix; t0 += step) {
+		float gv[U], jv[U][NTAN];
 #pragma unroll
-		for (int k = 0; k < NTAN; k++) acc[k] += (double)(gv * jp[(size_t)k * npix + t]);
+		for (int u = 0; u < U; u++) {
+			const unsigned t = t0 + u * blockDim.x;
+			const bool in = t < npix;
+			gv[u] = in ? g[t] : 0.f;
+#pragma unroll
+			for (int k = 0; k < NTAN; k++) jv[u][k] = in ? jp[(size_t)k * npix + t] : 0.f;
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++)
+			if (gv[u] != 0.f) {
+#pragma unroll
+				for (int k = 0; k < NTAN; k++) acc[k] += (double)(gv[u] * jv[u][k]);
+			}
 	}
 	__shared__ double s_red[NTAN][8];
+	__shared__ bool s_last;
 	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
 	for (int k = 0; k < NTAN; k++) {
@@ -617,11 +639,25 @@ __global__ void k_jac_reduce(const float *__restrict__ jac, const float *__restr
 		if (lane == 0) s_red[k][wid] = v;
 	}
 	__syncthreads();
+	double *mine = partials + ((size_t)pi * gridDim.x + blockIdx.x) * NTAN;
 	if (threadIdx.x < NTAN) {
 		double v = 0;
 		for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += s_red[threadIdx.x][w];
-		atomicAdd(&out[(size_t)pi * NTAN + threadIdx.x], v);
+		mine[threadIdx.x] = v;
+		__threadfence();
 	}
+	__syncthreads();
+	if (threadIdx.x == 0) s_last = atomicAdd(&tickets[pi], 1u) == gridDim.x - 1;
+	__syncthreads();
+	if (!s_last) return;
+	__threadfence();
+	if (threadIdx.x < NTAN) {
+		const double *all = partials + (size_t)pi * gridDim.x * NTAN;
+		double v = 0;
+		for (unsigned blk = 0; blk < gridDim.x; blk++) v += ((volatile const double *)all)[blk * NTAN + threadIdx.x];
+		out[(size_t)pi * NTAN + threadIdx.x] = v;
+	}
+	if (threadIdx.x == 0) tickets[pi] = 0;
 }
 
 // Scatter the residual weights w (cropped grid) into the padded grid of the
@@ -676,13 +712,21 @@ cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npi
 	return cudaGetLastError();
 }
 
-cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
-                              const int *prof_batch, int n_profiles, unsigned npix, double *out, cudaStream_t s)
+unsigned jac_reduce_blocks(unsigned npix, int n_profiles)
 {
-	unsigned bx = cdiv(npix, 256 * 8);
-	if (bx < 1) bx = 1;
-	if (bx > 148 * 4) bx = 148 * 4;
-	k_jac_reduce<<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, out);
+	unsigned bx = cdiv(npix, 256 * 4);
+	const unsigned target = cdiv(148u * 8u, (unsigned)n_profiles);  // about 8 blocks per SM in all
+	if (bx > target) bx = target;
+	return bx < 1 ? 1 : bx;
+}
+
+cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
+                              const int *prof_batch, int n_profiles, unsigned npix, double *partials,
+                              unsigned *tickets, double *out, cudaStream_t s)
+{
+	const unsigned bx = jac_reduce_blocks(npix, n_profiles);
+	k_jac_reduce<<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, partials,
+	                                                  tickets, out);
 	note_launches(1);
 	return cudaGetLastError();
 }
@@ -701,37 +745,57 @@ cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned
 template <class TOut>
 static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                               TOut *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
-                              int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
+                              int batch, int batch_src_stride, int batch_out_stride, double *scratch,
+                              size_t scratch_bytes, cudaStream_t s)
 {
 	note_launches(1);
 	static const ConvCandidate cands[] = {
-	    {ConvVariant<float, double, TOut, 8, 4, 4>::smem, ConvVariant<float, double, TOut, 8, 4, 4>::run},
+	    // packed-FMA kernels: (lanes per row, rows per thread, row groups, column groups, column splits)
+	    {Conv3Variant<TOut, 32, 8, 2, 4, 1>::smem, Conv3Variant<TOut, 32, 8, 2, 4, 1>::run},
+	    {Conv3Variant<TOut, 32, 8, 4, 1, 1>::smem, Conv3Variant<TOut, 32, 8, 4, 1, 1>::run},
+	    {Conv3Variant<TOut, 32, 12, 4, 1, 1>::smem, Conv3Variant<TOut, 32, 12, 4, 1, 1>::run},
+	    {Conv3Variant<TOut, 32, 8, 1, 8, 1>::smem, Conv3Variant<TOut, 32, 8, 1, 8, 1>::run},
+	    {Conv3Variant<TOut, 16, 8, 2, 1, 1>::smem, Conv3Variant<TOut, 16, 8, 2, 1, 1>::run},
+	    {Conv3Variant<TOut, 16, 8, 4, 1, 1>::smem, Conv3Variant<TOut, 16, 8, 4, 1, 1>::run},
+	    {Conv3Variant<TOut, 16, 12, 2, 1, 1>::smem, Conv3Variant<TOut, 16, 12, 2, 1, 1>::run},
+	    {Conv3Variant<TOut, 16, 8, 1, 4, 1>::smem, Conv3Variant<TOut, 16, 8, 1, 4, 1>::run},
+	    {Conv3Variant<TOut, 16, 8, 1, 8, 1>::smem, Conv3Variant<TOut, 16, 8, 1, 8, 1>::run},
+	    {Conv3Variant<TOut, 16, 8, 1, 4, 2>::smem, Conv3Variant<TOut, 16, 8, 1, 4, 2>::run},
+	    {Conv3Variant<TOut, 16, 8, 1, 4, 4>::smem, Conv3Variant<TOut, 16, 8, 1, 4, 4>::run},
+	    {Conv3Variant<TOut, 16, 8, 1, 2, 4>::smem, Conv3Variant<TOut, 16, 8, 1, 2, 4>::run},
+	    {Conv3Variant<TOut, 16, 8, 2, 2, 2>::smem, Conv3Variant<TOut, 16, 8, 2, 2, 2>::run},
+	    {Conv3Variant<TOut, 32, 8, 1, 4, 2>::smem, Conv3Variant<TOut, 32, 8, 1, 4, 2>::run},
+	    // one-column-per-lane kernels
 	    {ConvVariant<float, double, TOut, 8, 1, 8>::smem, ConvVariant<float, double, TOut, 8, 1, 8>::run},
 	    {ConvVariant<float, double, TOut, 8, 2, 4>::smem, ConvVariant<float, double, TOut, 8, 2, 4>::run},
-	    {ConvVariant<float, double, TOut, 4, 2, 8>::smem, ConvVariant<float, double, TOut, 4, 2, 8>::run},
-	    {ConvVariant<float, double, TOut, 16, 2, 2>::smem, ConvVariant<float, double, TOut, 16, 2, 2>::run},
-	    {ConvVariant<float, double, TOut, 8, 4, 1>::smem, ConvVariant<float, double, TOut, 8, 4, 1>::run},
-	    {ConvVariant<float, double, TOut, 4, 4, 2>::smem, ConvVariant<float, double, TOut, 4, 4, 2>::run},
 	};
 	ConvArgs a{src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
-	           batch_src_stride, batch_out_stride};
+	           batch_src_stride, batch_out_stride, scratch, scratch_bytes};
 	return conv_autotuned(cands, (int)(sizeof(cands) / sizeof(cands[0])), sizeof(TOut) == 8 ? 2 : 1, a, s);
+}
+
+size_t conv32_scratch_bytes(int ow, int oh, int batch)
+{
+	const size_t bytes = (size_t)ow * oh * batch * 4 * sizeof(double);  // up to 4 column splits
+	return bytes <= ((size_t)64 << 20) ? bytes : 0;
 }
 
 cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                           float *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
-                          int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
+                          int batch, int batch_src_stride, int batch_out_stride, double *scratch, size_t scratch_bytes,
+                          cudaStream_t s)
 {
 	return conv32_any<float>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
-	                         batch_src_stride, batch_out_stride, s);
+	                         batch_src_stride, batch_out_stride, scratch, scratch_bytes, s);
 }
 
 cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                                double *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
-                               int batch, int batch_src_stride, int batch_out_stride, cudaStream_t s)
+                               int batch, int batch_src_stride, int batch_out_stride, double *scratch,
+                               size_t scratch_bytes, cudaStream_t s)
 {
 	return conv32_any<double>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
-	                          batch_src_stride, batch_out_stride, s);
+	                          batch_src_stride, batch_out_stride, scratch, scratch_bytes, s);
 }
 
 cudaError_t launch_loglike32(const float *model, const double *data, const double *sigma, const uint8_t *region,

@@ -202,6 +202,51 @@ def test_fp32_image_close_to_fp64(wl):
     assert _rel(b, a) <= 1e-5
 
 
+# Number of FP32 convolution kernels the autotuner chooses from (render32.cu).
+N_FP32_CONV_CANDIDATES = 16
+
+
+@pytest.mark.parametrize("cand", range(N_FP32_CONV_CANDIDATES))
+def test_every_fp32_convolution_candidate(cand, monkeypatch):
+    """Each tile shape, column split and packed/unpacked FMA kernel gives the
+    FP64 image to FP32 accuracy, and the same adjoint gradient, on odd sizes
+    (partial tiles, kernel rows not a multiple of the unroll) and in a batch."""
+    wl = W.single_sersic(seed_tag=11, width=157, height=93, psf_size=21)
+    wl["magzero"] = 25.0
+    m64 = W.configure(Model(wl["width"], wl["height"]), wl)
+    ref, _ = m64.evaluate()
+    image, sigma = W.make_data(wl, ref)
+    refs = wl["grad"]
+    props = [W.perturbed(wl, seed=300 + s, scale=0.03) for s in range(3)]
+    vals = np.array([[p["profiles"][i][1][k] for (i, k) in refs] for p in props])
+
+    base = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), props[0])
+    base.set_data(image, sigma)
+    ll0, g0 = base.loglike_grad(refs)
+
+    monkeypatch.setenv("PF_CONV_FORCE", str(cand))
+    m32 = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
+    img, _ = m32.evaluate()
+    assert _rel(img, ref) <= 1e-6
+    one = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), props[0])
+    one.set_data(image, sigma)
+    for _ in range(2):  # eager, then graph replay
+        ll, g = one.loglike_grad(refs)
+        assert ll == pytest.approx(ll0, rel=1e-7)
+        np.testing.assert_allclose(g, g0, rtol=1e-5, atol=1e-6 * np.max(np.abs(g0)))
+    mb = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
+    mb.set_data(image, sigma)
+    ll_b, g_b = mb.loglike_grad_batch(refs, vals)
+    assert ll_b[0] == pytest.approx(ll0, rel=1e-7)
+    np.testing.assert_allclose(g_b[0], g0, rtol=1e-5, atol=1e-6 * np.max(np.abs(g0)))
+    for s in (1, 2):
+        p = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), props[s])
+        p.set_data(image, sigma)
+        ll, g = p.loglike_grad(refs)
+        assert ll_b[s] == pytest.approx(ll, rel=1e-7)
+        np.testing.assert_allclose(g_b[s], g, rtol=1e-5, atol=1e-6 * np.max(np.abs(g)))
+
+
 def test_fp32_loglike_close_to_fp64():
     wl = W.bulge_disk_ps()
     m64 = W.configure(Model(wl["width"], wl["height"]), wl)
