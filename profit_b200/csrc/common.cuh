@@ -39,6 +39,7 @@ struct QueueSet {
 	uint32_t *overflow;    // set to 1 when an item had to be dropped
 	int32_t *decisions;    // optional [n_profiles][npix] subsample_pixel calls per pixel
 	unsigned long long *level_counts;  // optional [n_profiles][MAX_LEVELS]
+	uint32_t *maxres = nullptr;  // optional: largest resolution of the level-0 items pushed
 	uint32_t levels;
 	uint32_t off[MAX_LEVELS];
 	uint32_t cap[MAX_LEVELS];
@@ -137,6 +138,15 @@ __device__ __forceinline__ uint32_t warp_push(uint32_t *counter)
 	if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
 	base = __shfl_sync(mask, base, leader);
 	return base + rank;
+}
+
+// Raises *q.maxres to `res` (one atomic per warp of pushing threads).
+__device__ __forceinline__ void note_max_res(const QueueSet &q, uint32_t res)
+{
+	if (!q.maxres) return;
+	const uint32_t mask = __activemask();
+	const uint32_t m = __reduce_max_sync(mask, res);
+	if ((int)(threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(q.maxres, m);
 }
 
 __device__ __forceinline__ void queue_push(const QueueSet &q, uint32_t level, const SubItem &it)

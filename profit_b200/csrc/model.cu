@@ -523,6 +523,7 @@ int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q
 	q.items = m->d_items.as<SubItem>();
 	q.counts = m->d_ctrl.as<uint32_t>();
 	q.overflow = m->d_ctrl.as<uint32_t>() + MAX_LEVELS;
+	q.maxres = m->d_ctrl.as<uint32_t>() + MAX_LEVELS + 1;
 	q.levels = (uint32_t)a.levels;
 	q.decisions = decisions;
 	q.level_counts = level_counts;

@@ -296,6 +296,7 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 			it.res = (uint8_t)res;
 			it.max_rec = (uint8_t)max_rec;
 			queue_push(q, 0, it);
+			note_max_res(q, res);
 		}
 		if (jac) {
 			float *jp = jac + (size_t)pi * NTAN * npix + pix;
@@ -307,9 +308,12 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 	img_plain[(size_t)b * npix + pix] = acc[1];
 }
 
+// Sub-points [base0, base1) of an item (multiples of 32), one per lane and
+// chunk.
 template <class T>
 __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &it, int level, const double *s_xy,
-                                             int lane, const QueueSet &q, float *sums, uint32_t *mask_out)
+                                             int lane, const QueueSet &q, float *sums, uint32_t *mask_out,
+                                             unsigned base0, unsigned base1)
 {
 	const unsigned res = it.res;
 	const double xbin = (it.x1 - it.x0) / res, ybin = (it.y1 - it.y0) / res;
@@ -320,7 +324,7 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 	const unsigned nsub = res * res;
 	// sub-points in warp-wide chunks of 32 so each chunk's accept bits can be
 	// gathered with one ballot (mask_out: the item's 8 words, or null)
-	for (unsigned base = 0; base < nsub; base += 32) {
+	for (unsigned base = base0; base < base1 && base < nsub; base += 32) {
 		const unsigned k = base + lane;
 		bool accepted = false;
 		if (k < nsub) {
@@ -329,10 +333,12 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 			const T dx = (T)x, dy = (T)y;
 			const T xp = dx * cos_a + dy * sin_a;
 			const T yp = -dx * sin_q + dy * cos_q;
+			// the test point is evaluated beside the sub-point (independent
+			// chains the scheduler can interleave)
 			Tan<T> t = eval_tan<T>(p, xp, yp);
+			const T testval = recurse ? eval_val<T>(p, fabs(xp), fabs(yp) + adyp) : T(0);
 			accepted = true;
 			if (recurse) {
-				T testval = eval_val<T>(p, fabs(xp), fabs(yp) + adyp);
 				if (fabs(testval - t.f) > (T)p.acc * t.f) {
 					accepted = false;
 					SubItem c;
@@ -393,11 +399,14 @@ __device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem 
 	}
 }
 
-// One SubItem integrated by one warp (s_xy: this warp's 32 doubles).
+// Sub-points [base0, base1) of one SubItem integrated by one warp (s_xy:
+// this warp's 32 doubles); FP64 sub-points from level 3 on (the Sersic cusp).
+template <bool Deep>
 __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profiles, const SubItem &it, int level,
                                              unsigned npix, float *__restrict__ img_conv,
                                              float *__restrict__ img_plain, float *__restrict__ jac,
-                                             const QueueSet &q, double *s_xy, int lane, uint32_t *mask_out)
+                                             const QueueSet &q, double *s_xy, int lane, uint32_t *mask_out,
+                                             unsigned base0, unsigned base1)
 {
 	const FProfile &p = profiles[it.profile];
 	const unsigned res = it.res;
@@ -412,8 +421,8 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 	float sums[NTAN];
 #pragma unroll
 	for (int k = 0; k < NTAN; k++) sums[k] = 0.f;
-	if (level >= 3) level_points<double>(p, it, level, s_xy, lane, q, sums, mask_out);
-	else level_points<float>(p, it, level, s_xy, lane, q, sums, mask_out);
+	if constexpr (Deep) level_points<double>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
+	else level_points<float>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
 #pragma unroll
 	for (int k = 0; k < NTAN; k++) sums[k] = warp_sum(sums[k]);
 	if (lane == 0) {
@@ -440,9 +449,25 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
 	const uint32_t n = min(q.counts[level], q.cap[level]);
 	const SubItem *items = q.items + q.off[level];
 	const uint32_t nwarps = gridDim.x * (blockDim.x >> 5);
-	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < n; w += nwarps)
-		level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
-			             q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr);
+	// Fewer items than warps (a single image): one warp per (item, chunk of
+	// 32 sub-points), so an item's chunks run side by side; otherwise one warp
+	// per item.
+	uint32_t cpi = 1;
+	if (n < nwarps) {
+		uint32_t maxres = q.maxres ? *q.maxres : 16u;
+		if (maxres == 0 || maxres > 16) maxres = 16;
+		cpi = (maxres * maxres + 31) / 32;
+	}
+	const uint32_t total = n * cpi;
+	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < total; w += nwarps) {
+		const uint32_t item = w / cpi, chunk = w - item * cpi;
+		const SubItem it = items[item];
+		const unsigned base0 = cpi == 1 ? 0u : chunk * 32, base1 = cpi == 1 ? 256u : base0 + 32;
+		if (base0 >= (unsigned)it.res * it.res) continue;
+		level32_item<false>(profiles, it, level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
+		                    q.masks ? q.masks + ((size_t)q.off[level] + item) * MASK_WORDS : nullptr, base0,
+		                    base1);
+	}
 }
 
 // Levels first..levels-1 in one CTA.  Only the Sersic central cusp
@@ -463,8 +488,8 @@ __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restric
 		const uint32_t n = min(*(volatile uint32_t *)&q.counts[level], q.cap[level]);
 		const SubItem *items = q.items + q.off[level];
 		for (uint32_t w = wib; w < n; w += nwarps)
-			level32_item(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
-			             q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr);
+			level32_item<true>(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
+			                   q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr, 0, 256);
 	}
 }
 
