@@ -312,12 +312,17 @@ def main_b200(args):
     flop = 2.0 * P * P * n_out
     conv_s = statistics.mean(conv_ms) / 1e3
     peaks = measured_fp32_peak()
-    roof = {"kernel": "k_conv_tile<float,16,2> (forward brute-force convolution)", "bound": "fp32",
+    roof = {"kernel": "k_conv3_tile (forward brute-force convolution, packed FP32 FMA, autotuned tile)",
+            "bound": "fp32",
             "achieved": flop / conv_s / 1e12, "peak": peaks, "unit": "TFLOP/s",
             "frac": (flop / conv_s / 1e12) / peaks if peaks else None,
             "traffic": recorded_traffic(),
             "algorithmic": f"2*P^2*W*H = {flop:.3e} FLOP per launch (P={P}, W*H={n_out})",
-            "peak_source": "measured: dependent FMA streams, libpf_peaks.so, best of 5 (burst)"}
+            "peak_source": "measured on this GPU: dependent FP32 FMA chains, plain and packed (FFMA2), the higher "
+                           "of the two, libpf_peaks.so, best of 5 (burst); the convolution is FP32-pipe bound, so "
+                           "neither the HBM nor the bf16 tensor peak applies",
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one forward launch "
+                              "(profiles/conv_fwd_bulge_disk_ps.txt)"}
 
     sampler = sampler_batch_rate(args, torch, flush, n=args.sampler_n)
 
