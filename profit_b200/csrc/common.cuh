@@ -8,10 +8,15 @@
 
 namespace pf {
 
-// Number of per-pixel tangent sums kept for each radial profile by the FP32
-// path: f, df/dx', df/dy', df/dx'*y', df/dy'*x', df/dy'*y', and the three
-// shape partials (Sersic: re, nser, box; Moffat: fwhm, con, box).
-constexpr int NTAN = 9;
+// Tangent slots per radial profile: f, df/dx', df/dy', df/dx' y', df/dy' x',
+// df/dy' y', then the shape-parameter partials (per kind, shape_count of
+// them) and df/dbox.  Models whose profiles need fewer slots store fewer
+// planes (tangent_stride).
+constexpr int NTAN = 12;
+constexpr int NTAN_GEOM = 6;
+
+// Tangent slots a profile of this kind fills (geometry, shape, box).
+PF_HD inline int tangent_count(int kind) { return NTAN_GEOM + shape_count(kind) + 1; }
 
 // One cell waiting to be integrated by adaptive subsampling
 // (one pending call of RadialProfile::subsample_pixel, radial.cpp:54).
@@ -111,7 +116,8 @@ PF_HD inline FProfile to_fprofile(const DevProfile &d, const ProfileParams &p)
 //   d x'/d xcen = -c, d y'/d xcen = s/q, d x'/d ycen = -s, d y'/d ycen = -c/q,
 //   d x'/d theta = q y', d y'/d theta = -x'/q, d y'/d q = -y'/q,
 // and flux_scale F carries d ln F / d(mag, q, box, shape) from the prologue.
-enum GradCode : int32_t { G_XCEN = 0, G_YCEN, G_MAG, G_ANG, G_AXRAT, G_BOX, G_SHAPE1, G_SHAPE2 };
+// G_SHAPE + k: shape parameter k of the profile's kind (shape_count order).
+enum GradCode : int32_t { G_XCEN = 0, G_YCEN, G_MAG, G_ANG, G_AXRAT, G_BOX, G_SHAPE };
 
 PF_HD inline double gradient_from_tangents(int code, double axrat, const DevProfile &d, const double *T)
 {
@@ -122,9 +128,11 @@ PF_HD inline double gradient_from_tangents(int code, double axrat, const DevProf
 	case G_MAG: return F * d.dlnI_dmag * T[0];
 	case G_ANG: return F * (M_PI / 180.0) * (q * T[3] - T[4] / q);
 	case G_AXRAT: return F * (-T[5] / q + d.dlnI_dq * T[0]);
-	case G_BOX: return F * (T[8] + d.dlnI_dbox * T[0]);
-	case G_SHAPE1: return F * (T[6] + d.dlnI_dp1 * T[0]);
-	default: return F * (T[7] + d.dlnI_dp2 * T[0]);
+	case G_BOX: return F * (T[NTAN_GEOM + shape_count(d.kind)] + d.dlnI_dbox * T[0]);
+	default: {
+		const int k = code - G_SHAPE;
+		return F * (T[NTAN_GEOM + k] + d.dlnI_dp[k] * T[0]);
+	}
 	}
 }
 

@@ -34,16 +34,18 @@ cudaError_t launch_downsample64(const double *src, unsigned sw, unsigned sh, uns
                                 unsigned oh, cudaStream_t s);
 
 // render32.cu
+// jac: tangent planes, nt per profile (tangent_stride of the model);
+// all_kinds: the model has radial profiles other than Sersic and Moffat.
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
-                            const QueueSet &q, cudaStream_t s);
+                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s);
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
-                            float *jac, const QueueSet &q, cudaStream_t s);
+                            float *jac, int nt, bool all_kinds, const QueueSet &q, cudaStream_t s);
 // partials: n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN doubles;
 // tickets: n_profiles zero-initialised counters (left at zero again).
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles);
 cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
-                              const int *prof_batch, int n_profiles, unsigned npix, double *partials,
+                              const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
                               unsigned *tickets, double *out, cudaStream_t s);
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
                               unsigned dh, int batch, float *g_plain, cudaStream_t s);
@@ -93,5 +95,5 @@ namespace pf {
 // render32.cu: recomputing adjoint of the render (no stored tangent planes)
 cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
                                      unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
-                                     int levels, const QueueSet &q, double *T, cudaStream_t s);
+                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s);
 }  // namespace pf

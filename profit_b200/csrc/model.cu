@@ -755,6 +755,25 @@ int evaluate64(pf_model *m, Analysis &a)
 // FP32 path with forward tangents and the adjoint reduction
 // ---------------------------------------------------------------------------
 
+// Tangent planes kept per radial profile: the most any profile of the model
+// fills (9 for Sersic and Moffat models, up to 12 with core-Sersic).
+int tangent_stride(const pf_model *m)
+{
+	int nt = NTAN_GEOM + 3;
+	for (auto &p : m->profiles)
+		if (is_radial_kind(p.kind)) nt = std::max(nt, tangent_count(p.kind));
+	return nt;
+}
+
+// Whether the model has radial profiles beyond Sersic and Moffat (selects the
+// FP32 kernels that carry every kind's tangents).
+bool all_kinds(const pf_model *m)
+{
+	for (auto &p : m->profiles)
+		if (is_radial_kind(p.kind) && p.kind != PK_SERSIC && p.kind != PK_MOFFAT) return true;
+	return false;
+}
+
 // Scratch of launch_jac_reduce for n_profiles profiles over npix pixels; the
 // tickets start at zero when allocated and the kernel leaves them at zero.
 int jac_scratch(pf_model *m, unsigned npix, int n_profiles, double **partials, unsigned **tickets)
@@ -779,13 +798,14 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	PF_CUDA(ensure(m->d_model32, (size_t)a.cw * a.ch * 4 + 4));
 	float *jac = nullptr;
 	if (want_grad) {
-		PF_CUDA(ensure(m->d_jac, npix * NTAN * nprof * 4));
+		PF_CUDA(ensure(m->d_jac, npix * tangent_stride(m) * nprof * 4));
 		jac = m->d_jac.as<float>();
 	}
 	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *model = m->d_model32.as<float>();
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), 1, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain,
-	                        jac, q, m->stream));
-	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, m->stream));
+	                        jac, tangent_stride(m), all_kinds(m), q, m->stream));
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, tangent_stride(m), all_kinds(m), q,
+	                        m->stream));
 	PF_CUDA(record_event(m->ev[1], m->stream));
 	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
 	double *model64 = m->d_model64.as<double>();
@@ -815,7 +835,8 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		double *jpart;
 		unsigned *jtick;
 		PF_TRY(jac_scratch(m, (unsigned)npix, nprof, &jpart, &jtick));
-		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix, jpart,
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix,
+		                          tangent_stride(m), jpart,
 		                          jtick, d_out + ResultLayout::T0, m->stream));
 	}
 	PF_CUDA(record_event(m->ev[3], m->stream));
@@ -1029,8 +1050,11 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		                              m->d_fprof.as<FProfile>(), bs.d_invalid.as<int>(), s));
 	}
 	const FProfile *fprof = m->d_fprof.as<FProfile>();
-	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx, m->sy, conv, plain, jac, q, s));
-	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, q, s));
+	const int nt = tangent_stride(m);
+	const bool ak = all_kinds(m);
+	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx, m->sy, conv, plain, jac, nt, ak, q,
+	                        s));
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, nt, ak, q, s));
 	PF_CUDA(record_event(m->ev[1], s));
 	PF_TRY(forward_conv32(m, a, conv, plain, model64, C));
 	PF_CUDA(record_event(m->ev[2], s));
@@ -1044,12 +1068,12 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		gconv = gplain;
 	if (recompute)
 		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh, m->sx, m->sy, gconv,
-		                                 gplain, a.levels, q, bs.d_T.as<double>(), s));
+		                                 gplain, a.levels, ak, q, bs.d_T.as<double>(), s));
 	else {
 		double *jpart;
 		unsigned *jtick;
 		PF_TRY(jac_scratch(m, (unsigned)npix, C * nprof, &jpart, &jtick));
-		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix,
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix, nt,
 		                          jpart, jtick, bs.d_T.as<double>(), s));
 	}
 	PF_CUDA(launch_batch_gradient(bs.d_dev.as<DevProfile>(), nprof, C, ref_profile, ref_code, nrefs,
@@ -1108,7 +1132,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 
 	// chunk size from the memory budget (tangent planes dominate)
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
-	const size_t planes = npix * (size_t)nprof * NTAN * 4;
+	const size_t planes = npix * (size_t)nprof * tangent_stride(m) * 4;
 	const bool recompute = m->adjoint_mode == PF_ADJOINT_RECOMPUTE ||
 	                       (m->adjoint_mode == PF_ADJOINT_AUTO && planes > (256ull << 20));
 	size_t per = npix * (4 * 4 + 8 * 2) + (recompute ? 0 : planes) + nout * (8 + 4) + 4096;
@@ -1136,7 +1160,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	PF_CUDA(ensure(bs.h_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
 	PF_CUDA(ensure(m->d_conv32, npix * C * 4));
 	PF_CUDA(ensure(m->d_plain32, npix * C * 4));
-	if (!recompute) PF_CUDA(ensure(m->d_jac, npix * NTAN * nprof * C * 4));
+	if (!recompute) PF_CUDA(ensure(m->d_jac, npix * tangent_stride(m) * nprof * C * 4));
 	PF_CUDA(ensure(m->d_model64, nout * C * 8));
 	PF_CUDA(ensure(m->d_wseed, nout * C * 4));
 	PF_CUDA(ensure(m->d_gconv, npix * C * 4));
@@ -1264,8 +1288,6 @@ int gradient_code(const ProfileParams &p, const char *name, int &code)
 {
 	if (!is_radial_kind(p.kind))
 		return set_error(PF_E_INVALID, std::string("no gradient for parameters of ") + kind_name(p.kind) + " profiles");
-	if (p.kind != PK_SERSIC && p.kind != PK_MOFFAT)
-		return set_error(PF_E_INVALID, std::string("gradients of ") + kind_name(p.kind) + " profiles are not available yet");
 	if (p.kind == PK_SERSIC && p.rescale_flux)
 		return set_error(PF_E_INVALID, "gradients with rescale_flux are not available");
 	if (!std::strcmp(name, "xcen")) code = G_XCEN;
@@ -1274,12 +1296,17 @@ int gradient_code(const ProfileParams &p, const char *name, int &code)
 	else if (!std::strcmp(name, "ang")) code = G_ANG;
 	else if (!std::strcmp(name, "axrat")) code = G_AXRAT;
 	else if (!std::strcmp(name, "box")) code = G_BOX;
-	else if ((p.kind == PK_SERSIC && !std::strcmp(name, "re")) || (p.kind == PK_MOFFAT && !std::strcmp(name, "fwhm")))
-		code = G_SHAPE1;
-	else if ((p.kind == PK_SERSIC && !std::strcmp(name, "nser")) || (p.kind == PK_MOFFAT && !std::strcmp(name, "con")))
-		code = G_SHAPE2;
-	else
+	else {
+		ProfileParams q = p;
+		for (int k = 0; k < shape_count(p.kind); k++) {
+			const ParamDesc *d = find_param(p.kind, name);
+			if (d && reinterpret_cast<char *>(shape_param(q, k)) - reinterpret_cast<char *>(&q) == (ptrdiff_t)d->off) {
+				code = G_SHAPE + k;
+				return PF_OK;
+			}
+		}
 		return set_error(PF_E_INVALID, std::string("no gradient with respect to ") + name);
+	}
 	return PF_OK;
 }
 

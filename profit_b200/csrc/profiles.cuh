@@ -30,6 +30,23 @@ enum ProfileKind : int32_t {
 
 PF_HD inline bool is_radial_kind(int k) { return k >= PK_SERSIC && k <= PK_BROKENEXP; }
 
+// Shape parameters with an adjoint, per radial kind, in tangent-slot order:
+// sersic (re, nser), moffat (fwhm, con), ferrer (rout, a, b), coresersic
+// (re, rb, nser, a, b), king (rc, rt, a), brokenexp (h1, h2, rb, a).
+constexpr int MAX_SHAPE = 5;
+PF_HD inline int shape_count(int kind)
+{
+	switch (kind) {
+	case PK_SERSIC: return 2;
+	case PK_MOFFAT: return 2;
+	case PK_FERRER: return 3;
+	case PK_CORESERSIC: return 5;
+	case PK_KING: return 3;
+	case PK_BROKENEXP: return 4;
+	default: return 0;
+	}
+}
+
 // Sersic r_factor forms of sersic.cpp:78-189
 enum SersicForm : int32_t { SF_GENERAL = 0, SF_HALF, SF_ONE, SF_TWO, SF_THREE, SF_FOUR, SF_EIGHT, SF_SIXTEEN };
 
@@ -59,8 +76,10 @@ struct DevProfile {
 	double img_sx, img_sy;             // image pixel scale (centre-pixel test)
 	double bg;                         // sky value per drawing pixel
 	double psf_flux, px, py;           // psf point source: 10^(-0.4(mag-magzero)), centre
-	// derivatives of log(flux_scale) w.r.t. parameters (FP32+adjoint path)
-	double dlnI_dmag, dlnI_dq, dlnI_dbox, dlnI_dp1, dlnI_dp2;
+	// derivatives of log(flux_scale) w.r.t. parameters (FP32+adjoint path):
+	// magnitude, axis ratio, box, and the shape parameters in the order of
+	// shape_param_name()
+	double dlnI_dmag, dlnI_dq, dlnI_dbox, dlnI_dp[MAX_SHAPE];
 	double dbn_dn;
 	double axrat;
 };
@@ -249,6 +268,52 @@ struct BrokenExpIntegrand {
 // libprofit writes back into the profile (acc, rscale_switch, resolution,
 // rscale_max) are derived here without touching `p`, which is what a fresh
 // profit::Model per evaluation (R_profit_make_model) observes.
+// Total luminosity of a radial profile before the axis-ratio and box
+// factors (the get_lumtot overrides: sersic.cpp:291-313, moffat.cpp,
+// ferrer.cpp, coresersic.cpp:106-117, king.cpp, brokenexponential.cpp).
+// bn: Sersic / core-Sersic b_n; rscale: the profile's scale radius.
+PF_HD inline double profile_lum(const ProfileParams &p, double bn, double rscale)
+{
+	switch (p.kind) {
+	case PK_SERSIC: {
+		double g_factor = gamma_fn(2 * p.nser);
+		return pow(p.re, 2) * 2 * M_PI * p.nser * g_factor * exp(bn) / pow(bn, 2 * p.nser);
+	}
+	case PK_MOFFAT: return pow(rscale, 2) * M_PI / (p.con - 1);
+	case PK_FERRER: {
+		double g_factor = p.a * beta_fn(p.a, 1 + 2 / (2 - p.b));
+		return pow(p.rout, 2) * M_PI * g_factor;
+	}
+	case PK_CORESERSIC: {
+		CoreSersicIntegrand f{p.rb, p.a, p.b, p.re, p.nser, bn};
+		return 2 * M_PI * integrate_qagi(f, 0.0);
+	}
+	case PK_KING: {
+		KingIntegrand f{p.rc, p.rt, p.a};
+		return 2 * M_PI * integrate_qags(f, 0.0, p.rt);
+	}
+	default: {
+		BrokenExpIntegrand f{p.h1, p.h2, p.rb, p.a};
+		return 2 * M_PI * integrate_qagi(f, 0.0);
+	}
+	}
+}
+
+// Shape parameter k of a profile kind (the tangent slot order), or null.
+PF_HD inline double *shape_param(ProfileParams &p, int k)
+{
+	switch (p.kind) {
+	case PK_SERSIC: return k == 0 ? &p.re : k == 1 ? &p.nser : nullptr;
+	case PK_MOFFAT: return k == 0 ? &p.fwhm : k == 1 ? &p.con : nullptr;
+	case PK_FERRER: return k == 0 ? &p.rout : k == 1 ? &p.a : k == 2 ? &p.b : nullptr;
+	case PK_CORESERSIC:
+		return k == 0 ? &p.re : k == 1 ? &p.rb : k == 2 ? &p.nser : k == 3 ? &p.a : k == 4 ? &p.b : nullptr;
+	case PK_KING: return k == 0 ? &p.rc : k == 1 ? &p.rt : k == 2 ? &p.a : nullptr;
+	case PK_BROKENEXP: return k == 0 ? &p.h1 : k == 1 ? &p.h2 : k == 2 ? &p.rb : k == 3 ? &p.a : nullptr;
+	default: return nullptr;
+	}
+}
+
 PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, DevProfile &d)
 {
 	d.kind = p.kind;
@@ -259,7 +324,8 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 	d.img_sx = g.img_sx;
 	d.img_sy = g.img_sy;
 	d.dlnI_dmag = -0.4 * 2.302585092994045684;
-	d.dlnI_dq = d.dlnI_dbox = d.dlnI_dp1 = d.dlnI_dp2 = d.dbn_dn = 0;
+	d.dlnI_dq = d.dlnI_dbox = d.dbn_dn = 0;
+	for (int k = 0; k < MAX_SHAPE; k++) d.dlnI_dp[k] = 0;
 	d.centre_override = 0;
 	d.bn = 0;
 	d.axrat = p.axrat;
@@ -318,35 +384,7 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 	d.rscale = rscale;
 
 	// lumtot (get_lumtot overrides)
-	double lum;
-	switch (p.kind) {
-	case PK_SERSIC: {
-		double g_factor = gamma_fn(2 * p.nser);
-		lum = pow(p.re, 2) * 2 * M_PI * p.nser * g_factor * exp(d.bn) / pow(d.bn, 2 * p.nser);
-		break;
-	}
-	case PK_MOFFAT: lum = pow(rscale, 2) * M_PI / (p.con - 1); break;
-	case PK_FERRER: {
-		double g_factor = p.a * beta_fn(p.a, 1 + 2 / (2 - p.b));
-		lum = pow(p.rout, 2) * M_PI * g_factor;
-		break;
-	}
-	case PK_CORESERSIC: {
-		CoreSersicIntegrand f{p.rb, p.a, p.b, p.re, p.nser, d.bn};
-		lum = 2 * M_PI * integrate_qagi(f, 0.0);
-		break;
-	}
-	case PK_KING: {
-		KingIntegrand f{p.rc, p.rt, p.a};
-		lum = 2 * M_PI * integrate_qags(f, 0.0, p.rt);
-		break;
-	}
-	default: {
-		BrokenExpIntegrand f{p.h1, p.h2, p.rb, p.a};
-		lum = 2 * M_PI * integrate_qagi(f, 0.0);
-		break;
-	}
-	}
+	const double lum = profile_lum(p, d.bn, rscale);
 
 	double b2 = p.box + 2;
 	double r_box = M_PI * b2 / (2 * beta_fn(1 / b2, 1 / b2));
@@ -438,23 +476,40 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 		double B = b2;
 		d.dlnI_dbox = 1.0 / B + (2.0 / (B * B)) * (digamma(1.0 / B) - digamma(2.0 / B));
 	}
+	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) {
+		const double n = p.nser, h = 1e-6 * n;
+		d.dbn_dn = (qgamma(0.5, 2 * (n + h)) - qgamma(0.5, 2 * (n - h))) / (2 * h);
+	}
 	if (p.kind == PK_SERSIC) {
 		// L = re^2 2 pi n Gamma(2n) e^bn / bn^(2n)
-		double n = p.nser, bn = d.bn;
-		double h = 1e-6 * n;
-		double dbn = (qgamma(0.5, 2 * (n + h)) - qgamma(0.5, 2 * (n - h))) / (2 * h);
-		d.dbn_dn = dbn;
-		d.dlnI_dp1 = -2.0 / p.re;  // re
+		const double n = p.nser, bn = d.bn, dbn = d.dbn_dn;
+		d.dlnI_dp[0] = -2.0 / p.re;  // re
 		double dlnL_dn = 1.0 / n + 2.0 * digamma(2 * n) + dbn - 2.0 * log(bn) - 2.0 * n * dbn / bn;
-		d.dlnI_dp2 = -dlnL_dn;     // nser
+		d.dlnI_dp[1] = -dlnL_dn;     // nser
 	}
 	else if (p.kind == PK_MOFFAT) {
 		// L = rscale^2 pi / (con - 1), rscale = fwhm / (2 sqrt(2^(1/con) - 1))
 		double c = p.con;
 		double t = pow(2.0, 1.0 / c);
 		double drs_dc_over_rs = 0.5 * t * log(2.0) / (c * c * (t - 1.0));
-		d.dlnI_dp1 = -2.0 / p.fwhm;                       // fwhm
-		d.dlnI_dp2 = -(2.0 * drs_dc_over_rs - 1.0 / (c - 1.0));  // con
+		d.dlnI_dp[0] = -2.0 / p.fwhm;                          // fwhm
+		d.dlnI_dp[1] = -(2.0 * drs_dc_over_rs - 1.0 / (c - 1.0));  // con
+	}
+	else {
+		// Ferrer (Beta function), core-Sersic, King and broken exponential
+		// (QUADPACK): central differences of the same FP64 luminosity, so the
+		// gradient differentiates exactly the normalisation the image uses.
+		ProfileParams q = p;
+		for (int k = 0; k < shape_count(p.kind); k++) {
+			double *v = shape_param(q, k);
+			const double v0 = *v, h = 1e-6 * fabs(v0) + 1e-9;
+			*v = v0 + h;
+			const double lp = profile_lum(q, q.kind == PK_CORESERSIC ? qgamma(0.5, 2 * q.nser) : 0.0, rscale);
+			*v = v0 - h;
+			const double lm = profile_lum(q, q.kind == PK_CORESERSIC ? qgamma(0.5, 2 * q.nser) : 0.0, rscale);
+			*v = v0;
+			d.dlnI_dp[k] = -(log(lp) - log(lm)) / (2 * h);
+		}
 	}
 }
 

@@ -30,9 +30,13 @@
 
 namespace pf {
 
+// Value, position partials and parameter partials of one profile evaluation:
+// s[0 .. shape_count(kind) - 1] are df/d(shape parameter k), s[shape_count]
+// is df/dbox.
 template <class T>
 struct Tan {
-	T f, fx, fy, s1, s2, s3;
+	T f, fx, fy;
+	T s[MAX_SHAPE + 1];
 };
 
 template <class T>
@@ -68,12 +72,12 @@ __device__ __forceinline__ T xlogx(T x)
 }
 
 // Sersic: f = exp(-bn (base^(1/(n B)) - 1)), base = |x/re|^B + |y/re|^B.
-// Shape partials: s1 = df/dre, s2 = df/dnser (including dbn/dnser),
-// s3 = df/dbox.
+// Shape partials: s[0] = df/dre, s[1] = df/dnser (including dbn/dnser),
+// s[2] = df/dbox.
 template <class T>
 __device__ __forceinline__ Tan<T> sersic_tan(const FProfile &p, T xp, T yp)
 {
-	Tan<T> t;
+	Tan<T> t = {};
 	const T re = (T)p.re, B = (T)p.B, n = (T)p.nser, bn = (T)p.bn;
 	const T u = fabs(xp) / re, v = fabs(yp) / re;
 	T uB, vB, base;
@@ -88,7 +92,6 @@ __device__ __forceinline__ Tan<T> sersic_tan(const FProfile &p, T xp, T yp)
 	base = uB + vB;
 	if (!(base > T(0))) {
 		t.f = t_exp<T>(bn);
-		t.fx = t.fy = t.s1 = t.s2 = t.s3 = T(0);
 		return t;
 	}
 	const T inv_nB = T(1) / (n * B);
@@ -101,27 +104,24 @@ __device__ __forceinline__ Tan<T> sersic_tan(const FProfile &p, T xp, T yp)
 	t.f = f;
 	t.fx = xp != T(0) ? g * B * uB / xp : T(0);
 	t.fy = yp != T(0) ? g * B * vB / yp : T(0);
-	t.s1 = -dfdrf * rf / (n * re);
-	t.s2 = dfdrf * (-rf * lnb * inv_nB / n) - (rf - T(1)) * f * (T)p.dbn_dn;
+	t.s[0] = -dfdrf * rf / (n * re);
+	t.s[1] = dfdrf * (-rf * lnb * inv_nB / n) - (rf - T(1)) * f * (T)p.dbn_dn;
 	const T dbase_dB = (u > T(0) ? uB * t_log<T>(u) : T(0)) + (v > T(0) ? vB * t_log<T>(v) : T(0));
-	t.s3 = dfdrf * rf * inv_nB * (dbase_dB / base - lnb / B);
+	t.s[2] = dfdrf * rf * inv_nB * (dbase_dB / base - lnb / B);
 	return t;
 }
 
-// Moffat: f = (1 + (r/rscale)^2)^-con, r = boxy radius.  Shape partials:
-// s1 = df/dfwhm, s2 = df/dcon, s3 = df/dbox.
+// Boxy radius r = (|x'|^B + |y'|^B)^(1/B) (radial.h:93-102) and its partials
+// in x', y' and B.
 template <class T>
-__device__ __forceinline__ Tan<T> moffat_tan(const FProfile &p, T xp, T yp)
+__device__ __forceinline__ void boxy_radius(const FProfile &p, T xp, T yp, T &r, T &drdx, T &drdy, T &drdB)
 {
-	Tan<T> t;
-	const T B = (T)p.B, rs = (T)p.rscale, con = (T)p.con;
-	const T ax = fabs(xp), ay = fabs(yp);
-	T r, drdx, drdy, drdB;
+	const T B = (T)p.B, ax = fabs(xp), ay = fabs(yp);
 	if (B == T(2)) {
-		r = t_sqrt<T>(xp * xp + yp * yp);
+		const T S = xp * xp + yp * yp;
+		r = t_sqrt<T>(S);
 		drdx = r > T(0) ? xp / r : T(0);
 		drdy = r > T(0) ? yp / r : T(0);
-		const T S = xp * xp + yp * yp;
 		drdB = S > T(0) ? r * ((xlogx<T>(ax) * ax + xlogx<T>(ay) * ay) / (B * S) - t_log<T>(S) / (B * B)) : T(0);
 	}
 	else {
@@ -130,82 +130,192 @@ __device__ __forceinline__ Tan<T> moffat_tan(const FProfile &p, T xp, T yp)
 		r = S > T(0) ? t_pow<T>(S, T(1) / B) : T(0);
 		drdx = (r > T(0) && xp != T(0)) ? (xB / S) * r / xp : T(0);
 		drdy = (r > T(0) && yp != T(0)) ? (yB / S) * r / yp : T(0);
-		T lx = ax > T(0) ? xB * t_log<T>(ax) : T(0);
-		T ly = ay > T(0) ? yB * t_log<T>(ay) : T(0);
+		const T lx = ax > T(0) ? xB * t_log<T>(ax) : T(0);
+		const T ly = ay > T(0) ? yB * t_log<T>(ay) : T(0);
 		drdB = S > T(0) ? r * ((lx + ly) / (B * S) - t_log<T>(S) / (B * B)) : T(0);
 	}
+}
+
+// Fills fx, fy and df/dbox (slot ns) from df/dr.
+template <class T>
+__device__ __forceinline__ void radial_chain(Tan<T> &t, T fr, T drdx, T drdy, T drdB, int ns)
+{
+	t.fx = fr * drdx;
+	t.fy = fr * drdy;
+	t.s[ns] = fr * drdB;
+}
+
+// Moffat: f = (1 + (r/rscale)^2)^-con.  s[0] = df/dfwhm, s[1] = df/dcon,
+// s[2] = df/dbox.
+template <class T>
+__device__ __forceinline__ Tan<T> moffat_tan(const FProfile &p, T xp, T yp)
+{
+	Tan<T> t = {};
+	const T rs = (T)p.rscale, con = (T)p.con;
+	T r, drdx, drdy, drdB;
+	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
 	const T rf = r / rs;
 	const T q = T(1) + rf * rf;
 	const T lq = t_log<T>(q);
 	const T f = t_exp<T>(-con * lq);
 	const T dfdrf = -T(2) * con * rf * f / q;
 	t.f = f;
-	t.fx = dfdrf * drdx / rs;
-	t.fy = dfdrf * drdy / rs;
-	t.s1 = dfdrf * (-rf) * (T)p.a;          // a holds 1/fwhm for Moffat
-	t.s2 = -lq * f + dfdrf * (-rf) * (T)p.b; // b holds dln(rscale)/dcon
-	t.s3 = dfdrf * drdB / rs;
+	radial_chain<T>(t, dfdrf / rs, drdx, drdy, drdB, 2);
+	t.s[0] = dfdrf * (-rf) * (T)p.a;           // a holds 1/fwhm for Moffat
+	t.s[1] = -lq * f + dfdrf * (-rf) * (T)p.b;  // b holds dln(rscale)/dcon
 	return t;
 }
 
+// Ferrer: f = (1 - (r/rout)^(2-b))^a inside rout (ferrer.cpp:50-60).
+// s[0] = df/drout, s[1] = df/da, s[2] = df/db, s[3] = df/dbox.
 template <class T>
-__device__ __forceinline__ T boxy_r_t(const FProfile &p, T x, T y)
+__device__ __forceinline__ Tan<T> ferrer_tan(const FProfile &p, T xp, T yp)
 {
-	if (p.B == 2.0f) return t_sqrt<T>(x * x + y * y);
-	T B = (T)p.B;
-	return t_pow<T>(t_pow<T>(fabs(x), B) + t_pow<T>(fabs(y), B), T(1) / B);
-}
-
-// Value-only evaluation for the profiles without a hand-written tangent.
-template <class T>
-__device__ __forceinline__ Tan<T> other_tan(const FProfile &p, T xp, T yp)
-{
-	Tan<T> t;
-	t.fx = t.fy = t.s1 = t.s2 = t.s3 = T(0);
-	T r = boxy_r_t<T>(p, xp, yp);
-	switch (p.kind) {
-	case PK_FERRER: {
-		T rf = r / (T)p.rscale;
-		t.f = rf < T(1) ? t_pow<T>(T(1) - t_pow<T>(rf, T(2) - (T)p.b), (T)p.a) : T(0);
-		break;
-	}
-	case PK_CORESERSIC: {
-		T a = (T)p.a;
-		t.f = t_pow<T>(T(1) + t_pow<T>(r / (T)p.rb, -a), (T)p.b / a) *
-		      t_exp<T>(-(T)p.bn * t_pow<T>((t_pow<T>(r, a) + t_pow<T>((T)p.rb, a)) / t_pow<T>((T)p.re, a),
-		                                   T(1) / ((T)p.nser * a)));
-		break;
-	}
-	case PK_KING: {
-		T a = (T)p.a;
-		t.f = r < (T)p.rt ? t_pow<T>(T(1) / t_pow<T>(T(1) + (r / (T)p.rc) * (r / (T)p.rc), T(1) / a) - (T)p.king_t, a)
-		                  : T(0);
-		break;
-	}
-	case PK_BROKENEXP: {
-		T a = (T)p.a, base = r - (T)p.rb;
-		T expo = T(1) / (T)p.h1 - T(1) / (T)p.h2;
-		if (a * base < T(40)) base = t_log<T>(T(1) + t_exp<T>(a * base)) / a;
-		t.f = t_exp<T>(-r / (T)p.h1 + expo * base);
-		break;
-	}
-	default: t.f = T(0);
-	}
+	Tan<T> t = {};
+	T r, drdx, drdy, drdB;
+	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	const T rout = (T)p.rscale, a = (T)p.a, e = T(2) - (T)p.b;
+	const T rf = r / rout;
+	if (!(rf < T(1))) return t;
+	const T rfe = t_pow<T>(rf, e);
+	const T g = T(1) - rfe;
+	const T f = t_pow<T>(g, a);
+	t.f = f;
+	if (!(g > T(0)) || !(r > T(0))) return t;
+	const T fr = -a * e * f * rfe / (g * r);
+	radial_chain<T>(t, fr, drdx, drdy, drdB, 3);
+	t.s[0] = -fr * r / rout;
+	t.s[1] = f * t_log<T>(g);
+	t.s[2] = a * f * rfe * t_log<T>(rf) / g;
 	return t;
 }
 
+// King: f = ((1 + (r/rc)^2)^(-1/a) - (1 + (rt/rc)^2)^(-1/a))^a inside rt
+// (king.cpp:51-59).  s[0] = df/drc, s[1] = df/drt, s[2] = df/da, s[3] = df/dbox.
 template <class T>
+__device__ __forceinline__ Tan<T> king_tan(const FProfile &p, T xp, T yp)
+{
+	Tan<T> t = {};
+	T r, drdx, drdy, drdB;
+	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	const T rc = (T)p.rc, rt = (T)p.rt, a = (T)p.a, kt = (T)p.king_t;
+	if (!(r < rt)) return t;
+	const T X = T(1) + (r / rc) * (r / rc);
+	const T u = T(1) / t_pow<T>(X, T(1) / a);
+	const T D = u - kt;
+	const T f = t_pow<T>(D, a);
+	t.f = f;
+	if (!(D > T(0))) return t;
+	const T Y = T(1) + (rt / rc) * (rt / rc);
+	const T du_dr = -T(2) * r * u / (a * rc * rc * X);
+	const T du_drc = T(2) * r * r * u / (a * rc * rc * rc * X);
+	const T dt_drc = T(2) * rt * rt * kt / (a * rc * rc * rc * Y);
+	const T dt_drt = -T(2) * rt * kt / (a * rc * rc * Y);
+	const T du_da = u * t_log<T>(X) / (a * a), dt_da = kt * t_log<T>(Y) / (a * a);
+	const T c = a * f / D;
+	radial_chain<T>(t, c * du_dr, drdx, drdy, drdB, 3);
+	t.s[0] = c * (du_drc - dt_drc);
+	t.s[1] = -c * dt_drt;
+	t.s[2] = f * t_log<T>(D) + c * (du_da - dt_da);
+	return t;
+}
+
+// Broken exponential (brokenexponential.cpp:38-94): f = exp(-r/h1 +
+// (1/h1 - 1/h2) base), base = log(1 + exp(a (r - rb)))/a, or r - rb where
+// a (r - rb) >= 40.  s[0] = df/dh1, s[1] = df/dh2, s[2] = df/drb, s[3] = df/da,
+// s[4] = df/dbox.
+template <class T>
+__device__ __forceinline__ Tan<T> brokenexp_tan(const FProfile &p, T xp, T yp)
+{
+	Tan<T> t = {};
+	T r, drdx, drdy, drdB;
+	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	const T a = (T)p.a, h1 = (T)p.h1, h2 = (T)p.h2, z = r - (T)p.rb;
+	const T expo = T(1) / h1 - T(1) / h2;
+	T base = z, dbase_dr = T(1), dbase_da = T(0);
+	if (a * z < T(40)) {
+		const T ez = t_exp<T>(a * z);
+		base = t_log<T>(T(1) + ez) / a;
+		const T sig = ez / (T(1) + ez);
+		dbase_dr = sig;
+		dbase_da = z * sig / a - base / a;
+	}
+	const T f = t_exp<T>(-r / h1 + expo * base);
+	t.f = f;
+	radial_chain<T>(t, f * (-T(1) / h1 + expo * dbase_dr), drdx, drdy, drdB, 4);
+	t.s[0] = f * (r - base) / (h1 * h1);
+	t.s[1] = f * base / (h2 * h2);
+	t.s[2] = -f * expo * dbase_dr;
+	t.s[3] = f * expo * dbase_da;
+	return t;
+}
+
+// Core-Sersic (coresersic.cpp:51-59): f = (1 + (r/rb)^-a)^(b/a)
+// exp(-bn ((r^a + rb^a)/re^a)^(1/(n a))).  s[0] = df/dre, s[1] = df/drb,
+// s[2] = df/dnser (including dbn/dnser), s[3] = df/da, s[4] = df/db,
+// s[5] = df/dbox.
+template <class T>
+__device__ __forceinline__ Tan<T> coresersic_tan(const FProfile &p, T xp, T yp)
+{
+	Tan<T> t = {};
+	T r, drdx, drdy, drdB;
+	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	const T a = (T)p.a, b = (T)p.b, rb = (T)p.rb, re = (T)p.re, n = (T)p.nser, bn = (T)p.bn;
+	const T ra = t_pow<T>(r, a), rba = t_pow<T>(rb, a), rea = t_pow<T>(re, a);
+	const T rho = t_pow<T>(r / rb, -a);
+	const T A = T(1) + rho;
+	const T Q = (ra + rba) / rea;
+	const T W = t_pow<T>(Q, T(1) / (n * a));
+	const T f = t_pow<T>(A, b / a) * t_exp<T>(-bn * W);
+	t.f = f;
+	if (!(r > T(0)) || !(f > T(0))) return t;
+	const T lnA = t_log<T>(A), lnQ = t_log<T>(Q);
+	const T dA_dr = -a * rho / r, dA_drb = a * rho / rb, dA_da = -rho * t_log<T>(r / rb);
+	const T dQ_dr = a * ra / (r * rea), dQ_drb = a * rba / (rb * rea), dQ_dre = -a * Q / re;
+	const T dlnQ_da = (ra * t_log<T>(r) + rba * t_log<T>(rb)) / (ra + rba) - t_log<T>(re);
+	const T wq = W / (n * a * Q);  // dW/dQ
+	const T dW_dn = -W * lnQ / (n * n * a);
+	const T dW_da = W * (dlnQ_da / (n * a) - lnQ / (n * a * a));
+	radial_chain<T>(t, f * ((b / a) * dA_dr / A - bn * wq * dQ_dr), drdx, drdy, drdB, 5);
+	t.s[0] = f * (-bn * wq * dQ_dre);
+	t.s[1] = f * ((b / a) * dA_drb / A - bn * wq * dQ_drb);
+	t.s[2] = f * (-(T)p.dbn_dn * W - bn * dW_dn);
+	t.s[3] = f * (-(b / (a * a)) * lnA + (b / a) * dA_da / A - bn * dW_da);
+	t.s[4] = f * lnA / a;
+	return t;
+}
+
+// AK (all kinds): false compiles only the Sersic and Moffat tangents, the
+// kinds most models use, which keeps those kernels' code and registers as
+// small as before the other kinds had gradients.
+template <class T, bool AK>
 __device__ __forceinline__ Tan<T> eval_tan(const FProfile &p, T xp, T yp)
 {
 	if (p.kind == PK_SERSIC) return sersic_tan<T>(p, xp, yp);
 	if (p.kind == PK_MOFFAT) return moffat_tan<T>(p, xp, yp);
-	return other_tan<T>(p, xp, yp);
+	if constexpr (AK) {
+		switch (p.kind) {
+		case PK_FERRER: return ferrer_tan<T>(p, xp, yp);
+		case PK_CORESERSIC: return coresersic_tan<T>(p, xp, yp);
+		case PK_KING: return king_tan<T>(p, xp, yp);
+		case PK_BROKENEXP: return brokenexp_tan<T>(p, xp, yp);
+		default: break;
+		}
+	}
+	return Tan<T>{};
 }
 
-template <class T>
+template <class T, bool AK>
 __device__ __forceinline__ T eval_val(const FProfile &p, T xp, T yp)
 {
-	return eval_tan<T>(p, xp, yp).f;
+	return eval_tan<T, AK>(p, xp, yp).f;
+}
+
+// Tangent slots the kernels of a kind set carry.
+template <bool AK>
+constexpr int ntk()
+{
+	return AK ? NTAN : NTAN_GEOM + 3;
 }
 
 // How one drawing pixel is integrated for one radial profile
@@ -227,6 +337,7 @@ __device__ __forceinline__ int pixel_decision32(const FProfile &p, double x, dou
 	return PD_SUBSAMPLE;
 }
 
+template <int NT>
 __device__ __forceinline__ void tan_to_j(const Tan<float> &t, float xp, float yp, float w, float *j)
 {
 	j[0] += w * t.f;
@@ -235,16 +346,28 @@ __device__ __forceinline__ void tan_to_j(const Tan<float> &t, float xp, float yp
 	j[3] += w * t.fx * yp;
 	j[4] += w * t.fy * xp;
 	j[5] += w * t.fy * yp;
-	j[6] += w * t.s1;
-	j[7] += w * t.s2;
-	j[8] += w * t.s3;
+#pragma unroll
+	for (int k = 0; k < NT - NTAN_GEOM; k++) j[NTAN_GEOM + k] += w * t.s[k];
+}
+
+template <class T>
+__device__ __forceinline__ Tan<float> to_float(const Tan<T> &t)
+{
+	Tan<float> r;
+	r.f = (float)t.f;
+	r.fx = (float)t.fx;
+	r.fy = (float)t.fy;
+#pragma unroll
+	for (int k = 0; k <= MAX_SHAPE; k++) r.s[k] = (float)t.s[k];
+	return r;
 }
 
 // One thread per drawing pixel and per batch entry (blockIdx.z).  `model_of`
 // maps the profile range of each batch entry; profiles are FProfile records.
+template <bool AK>
 __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__restrict__ prof_begin,
                            unsigned width, unsigned height, double sx, double sy, float *__restrict__ img_conv,
-                           float *__restrict__ img_plain, float *__restrict__ jac, QueueSet q)
+                           float *__restrict__ img_plain, float *__restrict__ jac, int nt, QueueSet q)
 {
 	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
 	const unsigned j = blockIdx.y * blockDim.y + threadIdx.y;
@@ -267,16 +390,17 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 		if (!is_radial_kind(p.kind)) continue;
 		float xp, yp;
 		const int decision = pixel_decision32(p, x, y, xp, yp);
-		float jl[NTAN];
+		constexpr int NT = ntk<AK>();
+		float jl[NT];
 #pragma unroll
-		for (int k = 0; k < NTAN; k++) jl[k] = 0.f;
+		for (int k = 0; k < NT; k++) jl[k] = 0.f;
 		if (decision == PD_ZERO) {
 			// zero
 		}
 		else if (decision == PD_DIRECT) {
-			Tan<float> t = eval_tan<float>(p, xp, yp);
+			Tan<float> t = eval_tan<float, AK>(p, xp, yp);
 			acc[p.target] += p.flux_scale * t.f;
-			tan_to_j(t, xp, yp, 1.0f, jl);
+			tan_to_j<NT>(t, xp, yp, 1.0f, jl);
 		}
 		else {
 			unsigned res = p.resolution, max_rec = p.max_rec;
@@ -299,9 +423,10 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 			note_max_res(q, res);
 		}
 		if (jac) {
-			float *jp = jac + (size_t)pi * NTAN * npix + pix;
+			float *jp = jac + (size_t)pi * nt * npix + pix;
 #pragma unroll
-			for (int k = 0; k < NTAN; k++) jp[(size_t)k * npix] = jl[k];
+			for (int k = 0; k < NT; k++)
+				if (k < nt) jp[(size_t)k * npix] = jl[k];
 		}
 	}
 	img_conv[(size_t)b * npix + pix] = acc[0];
@@ -310,7 +435,7 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 
 // Sub-points [base0, base1) of an item (multiples of 32), one per lane and
 // chunk.
-template <class T>
+template <class T, bool AK>
 __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &it, int level, const double *s_xy,
                                              int lane, const QueueSet &q, float *sums, uint32_t *mask_out,
                                              unsigned base0, unsigned base1)
@@ -335,8 +460,8 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 			const T yp = -dx * sin_q + dy * cos_q;
 			// the test point is evaluated beside the sub-point (independent
 			// chains the scheduler can interleave)
-			Tan<T> t = eval_tan<T>(p, xp, yp);
-			const T testval = recurse ? eval_val<T>(p, fabs(xp), fabs(yp) + adyp) : T(0);
+			Tan<T> t = eval_tan<T, AK>(p, xp, yp);
+			const T testval = recurse ? eval_val<T, AK>(p, fabs(xp), fabs(yp) + adyp) : T(0);
 			accepted = true;
 			if (recurse) {
 				if (fabs(testval - t.f) > (T)p.acc * t.f) {
@@ -356,14 +481,7 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 				}
 			}
 			if (accepted) {
-				Tan<float> tf;
-				tf.f = (float)t.f;
-				tf.fx = (float)t.fx;
-				tf.fy = (float)t.fy;
-				tf.s1 = (float)t.s1;
-				tf.s2 = (float)t.s2;
-				tf.s3 = (float)t.s3;
-				tan_to_j(tf, (float)xp, (float)yp, 1.0f, sums);
+				tan_to_j<ntk<AK>()>(to_float<T>(t), (float)xp, (float)yp, 1.0f, sums);
 			}
 		}
 		const unsigned bits = __ballot_sync(0xffffffffu, accepted);
@@ -373,7 +491,7 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 
 // Adjoint of one item with its frozen decisions: the tangents of the
 // sub-points the forward pass accepted (mask bit set), summed.
-template <class T>
+template <class T, bool AK>
 __device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem &it, const double *s_xy, int lane,
                                                const uint32_t *mask, float *sums)
 {
@@ -387,24 +505,17 @@ __device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem 
 		const T dx = (T)x, dy = (T)y;
 		const T xp = dx * cos_a + dy * sin_a;
 		const T yp = -dx * sin_q + dy * cos_q;
-		Tan<T> t = eval_tan<T>(p, xp, yp);
-		Tan<float> tf;
-		tf.f = (float)t.f;
-		tf.fx = (float)t.fx;
-		tf.fy = (float)t.fy;
-		tf.s1 = (float)t.s1;
-		tf.s2 = (float)t.s2;
-		tf.s3 = (float)t.s3;
-		tan_to_j(tf, (float)xp, (float)yp, 1.0f, sums);
+		Tan<T> t = eval_tan<T, AK>(p, xp, yp);
+		tan_to_j<ntk<AK>()>(to_float<T>(t), (float)xp, (float)yp, 1.0f, sums);
 	}
 }
 
 // Sub-points [base0, base1) of one SubItem integrated by one warp (s_xy:
 // this warp's 32 doubles); FP64 sub-points from level 3 on (the Sersic cusp).
-template <bool Deep>
+template <bool Deep, bool AK>
 __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profiles, const SubItem &it, int level,
                                              unsigned npix, float *__restrict__ img_conv,
-                                             float *__restrict__ img_plain, float *__restrict__ jac,
+                                             float *__restrict__ img_plain, float *__restrict__ jac, int nt,
                                              const QueueSet &q, double *s_xy, int lane, uint32_t *mask_out,
                                              unsigned base0, unsigned base1)
 {
@@ -418,30 +529,35 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 		s_xy[lane] = it.y0 + (2 * (lane - 16) + 1) * half_ybin;
 	}
 	__syncwarp();
-	float sums[NTAN];
+	constexpr int NT = ntk<AK>();
+	float sums[NT];
 #pragma unroll
-	for (int k = 0; k < NTAN; k++) sums[k] = 0.f;
-	if constexpr (Deep) level_points<double>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
-	else level_points<float>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
+	for (int k = 0; k < NT; k++) sums[k] = 0.f;
+	if constexpr (Deep) level_points<double, AK>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
+	else level_points<float, AK>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
+	const int nk = tangent_count(p.kind);  // warp-uniform
 #pragma unroll
-	for (int k = 0; k < NTAN; k++) sums[k] = warp_sum(sums[k]);
+	for (int k = 0; k < NT; k++)
+		if (k < nk) sums[k] = warp_sum(sums[k]);
 	if (lane == 0) {
 		const float wgt = (float)it.weight;
 		const uint32_t b = it.pixel / npix, pix = it.pixel - b * npix;
 		float *img = p.target == 0 ? img_conv : img_plain;
 		atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)sums[0]));
 		if (jac) {
-			float *jp = jac + (size_t)it.profile * NTAN * npix + pix;
+			float *jp = jac + (size_t)it.profile * nt * npix + pix;
 #pragma unroll
-			for (int k = 0; k < NTAN; k++) atomicAdd(&jp[(size_t)k * npix], wgt * sums[k]);
+			for (int k = 0; k < NT; k++)
+				if (k < nk) atomicAdd(&jp[(size_t)k * npix], wgt * sums[k]);
 		}
 	}
 	__syncwarp();
 }
 
+template <bool AK>
 __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
                                                  float *__restrict__ img_conv, float *__restrict__ img_plain,
-                                                 float *__restrict__ jac, QueueSet q)
+                                                 float *__restrict__ jac, int nt, QueueSet q)
 {
 	__shared__ double s_xy[8][32];
 	const int lane = threadIdx.x & 31;
@@ -464,7 +580,7 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
 		const SubItem it = items[item];
 		const unsigned base0 = cpi == 1 ? 0u : chunk * 32, base1 = cpi == 1 ? 256u : base0 + 32;
 		if (base0 >= (unsigned)it.res * it.res) continue;
-		level32_item<false>(profiles, it, level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
+		level32_item<false, AK>(profiles, it, level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
 		                    q.masks ? q.masks + ((size_t)q.off[level] + item) * MASK_WORDS : nullptr, base0,
 		                    base1);
 	}
@@ -474,10 +590,11 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
 // (max_recursions = 10) reaches these levels, a few hundred cells per level
 // at most, so one block walks them in order; __syncthreads separates the
 // levels, which makes every push of level L visible before level L+1 is read.
+template <bool AK>
 __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restrict__ profiles, int first, int levels,
                                                         unsigned npix, float *__restrict__ img_conv,
                                                         float *__restrict__ img_plain, float *__restrict__ jac,
-                                                        QueueSet q)
+                                                        int nt, QueueSet q)
 {
 	__shared__ double s_xy[16][32];
 	const int lane = threadIdx.x & 31;
@@ -488,7 +605,7 @@ __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restric
 		const uint32_t n = min(*(volatile uint32_t *)&q.counts[level], q.cap[level]);
 		const SubItem *items = q.items + q.off[level];
 		for (uint32_t w = wib; w < n; w += nwarps)
-			level32_item<true>(profiles, items[w], level, npix, img_conv, img_plain, jac, q, s_xy[wib], lane,
+			level32_item<true, AK>(profiles, items[w], level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
 			                   q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr, 0, 256);
 	}
 }
@@ -504,6 +621,7 @@ __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restric
 // A tile whose nearest pixel centre is farther than rscale_max (+2 px) from
 // the profile centre is skipped: the elliptical radius is never smaller than
 // the Euclidean distance, so such pixels were zeroed by the forward pass.
+template <bool AK>
 __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__restrict__ profiles,
                                                           const int *__restrict__ prof_batch, unsigned width,
                                                           unsigned height, double sx, double sy,
@@ -524,9 +642,10 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 	}
 	const size_t npix = (size_t)width * height;
 	const float *g = (p.target == 0 ? g_conv : g_plain) + (size_t)prof_batch[pi] * npix;
-	float acc[NTAN];
+	constexpr int NT = ntk<AK>();
+	float acc[NT];
 #pragma unroll
-	for (int k = 0; k < NTAN; k++) acc[k] = 0.f;
+	for (int k = 0; k < NT; k++) acc[k] = 0.f;
 	const unsigned i = tx0 + (threadIdx.x & 63);
 	for (unsigned r = threadIdx.x >> 6; r < 32; r += 4) {
 		const unsigned j = ty0 + r;
@@ -536,18 +655,18 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 		const double y = half_ybin + j * sx, x = half_xbin + i * sy;
 		float xp, yp;
 		if (pixel_decision32(p, x, y, xp, yp) != PD_DIRECT) continue;
-		Tan<float> t = eval_tan<float>(p, xp, yp);
-		tan_to_j(t, xp, yp, gv, acc);
+		Tan<float> t = eval_tan<float, AK>(p, xp, yp);
+		tan_to_j<NT>(t, xp, yp, gv, acc);
 	}
-	__shared__ double s_red[NTAN][8];
+	__shared__ double s_red[NT][8];
 	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-	for (int k = 0; k < NTAN; k++) {
+	for (int k = 0; k < NT; k++) {
 		double v = warp_sum((double)acc[k]);
 		if (lane == 0) s_red[k][wid] = v;
 	}
 	__syncthreads();
-	if (threadIdx.x < NTAN) {
+	if (threadIdx.x < NT) {
 		double v = 0;
 		for (int w = 0; w < 8; w++) v += s_red[threadIdx.x][w];
 		if (v != 0.0) atomicAdd(&T[(size_t)pi * NTAN + threadIdx.x], v);
@@ -556,6 +675,7 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 
 // Every queued cell of every level, one warp per cell: the tangents of the
 // accepted sub-points, times the cell weight and g(pixel).
+template <bool AK>
 __global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restrict__ profiles, int levels,
                                                          const float *__restrict__ g_conv,
                                                          const float *__restrict__ g_plain, QueueSet q,
@@ -582,19 +702,20 @@ __global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restr
 			}
 			__syncwarp();
 			const uint32_t *mask = q.masks + ((size_t)q.off[level] + w) * MASK_WORDS;
-			float sums[NTAN];
+			constexpr int NT = ntk<AK>();
+			float sums[NT];
 #pragma unroll
-			for (int k = 0; k < NTAN; k++) sums[k] = 0.f;
-			if (level >= 3) adjoint_points<double>(p, it, s_xy[wib], lane, mask, sums);
-			else adjoint_points<float>(p, it, s_xy[wib], lane, mask, sums);
+			for (int k = 0; k < NT; k++) sums[k] = 0.f;
+			if (level >= 3) adjoint_points<double, AK>(p, it, s_xy[wib], lane, mask, sums);
+			else adjoint_points<float, AK>(p, it, s_xy[wib], lane, mask, sums);
 #pragma unroll
-			for (int k = 0; k < NTAN; k++) sums[k] = warp_sum(sums[k]);
+			for (int k = 0; k < NT; k++) sums[k] = warp_sum(sums[k]);
 			if (lane == 0) {
 				const float gv = (p.target == 0 ? g_conv : g_plain)[it.pixel];
 				const double coef = (double)gv * it.weight;
 				if (coef != 0.0) {
 #pragma unroll
-					for (int k = 0; k < NTAN; k++) atomicAdd(&T[(size_t)it.profile * NTAN + k], coef * (double)sums[k]);
+					for (int k = 0; k < NT; k++) atomicAdd(&T[(size_t)it.profile * NTAN + k], coef * (double)sums[k]);
 				}
 			}
 			__syncwarp();
@@ -604,11 +725,17 @@ __global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restr
 
 cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
                                      unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
-                                     int levels, const QueueSet &q, double *T, cudaStream_t s)
+                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s)
 {
 	dim3 grid((width + 63) / 64, (height + 31) / 32, n_profiles);
-	k_adjoint_pixels32<<<grid, 256, 0, s>>>(profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
-	k_adjoint_items32<<<148 * 8, 256, 0, s>>>(profiles, levels, g_conv, g_plain, q, T);
+	if (all_kinds) {
+		k_adjoint_pixels32<true><<<grid, 256, 0, s>>>(profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
+		k_adjoint_items32<true><<<148 * 8, 256, 0, s>>>(profiles, levels, g_conv, g_plain, q, T);
+	}
+	else {
+		k_adjoint_pixels32<false><<<grid, 256, 0, s>>>(profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
+		k_adjoint_items32<false><<<148 * 8, 256, 0, s>>>(profiles, levels, g_conv, g_plain, q, T);
+	}
 	note_launches(2);
 	return cudaGetLastError();
 }
@@ -620,10 +747,11 @@ cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_b
 // its NTAN sums to `partials`; the block that finishes last (an atomic
 // ticket per profile, no waiting) adds the partials in block order and
 // resets the ticket, so the result does not depend on block scheduling.
+template <int NT>
 __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ jac, const float *__restrict__ g_conv,
                                                     const float *__restrict__ g_plain,
                                                     const FProfile *__restrict__ profiles,
-                                                    const int *__restrict__ prof_batch, unsigned npix,
+                                                    const int *__restrict__ prof_batch, unsigned npix, int nt,
                                                     double *__restrict__ partials, unsigned *__restrict__ tickets,
                                                     double *__restrict__ out)
 {
@@ -631,41 +759,42 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
 	const int pi = blockIdx.y;
 	const FProfile &p = profiles[pi];
 	if (!is_radial_kind(p.kind)) return;
+	const int nk = tangent_count(p.kind);  // <= nt <= NT
 	const int b = prof_batch[pi];
 	const float *g = (p.target == 0 ? g_conv : g_plain) + (size_t)b * npix;
-	const float *jp = jac + (size_t)pi * NTAN * npix;
-	double acc[NTAN];
+	const float *jp = jac + (size_t)pi * nt * npix;
+	double acc[NT];
 #pragma unroll
-	for (int k = 0; k < NTAN; k++) acc[k] = 0.0;
+	for (int k = 0; k < NT; k++) acc[k] = 0.0;
 	const unsigned step = gridDim.x * blockDim.x * U;
 	for (unsigned t0 = blockIdx.x * blockDim.x * U + threadIdx.x; t0 < npix; t0 += step) {
-		float gv[U], jv[U][NTAN];
+		float gv[U], jv[U][NT];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const unsigned t = t0 + u * blockDim.x;
 			const bool in = t < npix;
 			gv[u] = in ? g[t] : 0.f;
 #pragma unroll
-			for (int k = 0; k < NTAN; k++) jv[u][k] = in ? jp[(size_t)k * npix + t] : 0.f;
+			for (int k = 0; k < NT; k++) jv[u][k] = (in && k < nk) ? jp[(size_t)k * npix + t] : 0.f;
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++)
 			if (gv[u] != 0.f) {
 #pragma unroll
-				for (int k = 0; k < NTAN; k++) acc[k] += (double)(gv[u] * jv[u][k]);
+				for (int k = 0; k < NT; k++) acc[k] += (double)(gv[u] * jv[u][k]);
 			}
 	}
-	__shared__ double s_red[NTAN][8];
+	__shared__ double s_red[NT][8];
 	__shared__ bool s_last;
 	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-	for (int k = 0; k < NTAN; k++) {
+	for (int k = 0; k < NT; k++) {
 		double v = warp_sum(acc[k]);
 		if (lane == 0) s_red[k][wid] = v;
 	}
 	__syncthreads();
 	double *mine = partials + ((size_t)pi * gridDim.x + blockIdx.x) * NTAN;
-	if (threadIdx.x < NTAN) {
+	if (threadIdx.x < NT) {
 		double v = 0;
 		for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += s_red[threadIdx.x][w];
 		mine[threadIdx.x] = v;
@@ -676,7 +805,7 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
 	__syncthreads();
 	if (!s_last) return;
 	__threadfence();
-	if (threadIdx.x < NTAN) {
+	if (threadIdx.x < NT) {
 		const double *all = partials + (size_t)pi * gridDim.x * NTAN;
 		double v = 0;
 		for (unsigned blk = 0; blk < gridDim.x; blk++) v += ((volatile const double *)all)[blk * NTAN + threadIdx.x];
@@ -716,22 +845,33 @@ static inline unsigned cdiv(unsigned a, unsigned b) { return (a + b - 1) / b; }
 
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
-                            const QueueSet &q, cudaStream_t s)
+                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s)
 {
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8), batch);
-	k_pixels32<<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac, q);
+	if (all_kinds)
+		k_pixels32<true><<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac,
+		                                        nt, q);
+	else
+		k_pixels32<false><<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac,
+		                                         nt, q);
 	note_launches(1);
 	return cudaGetLastError();
 }
 
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
-                            float *jac, const QueueSet &q, cudaStream_t s)
+                            float *jac, int nt, bool all_kinds, const QueueSet &q, cudaStream_t s)
 {
 	const int wide = n_levels < 3 ? n_levels : 3;
-	for (int l = 0; l < wide; l++) k_level32<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, q);
+	for (int l = 0; l < wide; l++) {
+		if (all_kinds) k_level32<true><<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
+		else k_level32<false><<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
+	}
 	note_launches(wide);
 	if (n_levels > wide) {
-		k_deep_levels32<<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, q);
+		if (all_kinds)
+			k_deep_levels32<true><<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, nt, q);
+		else
+			k_deep_levels32<false><<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, nt, q);
 		note_launches(1);
 	}
 	return cudaGetLastError();
@@ -746,12 +886,16 @@ unsigned jac_reduce_blocks(unsigned npix, int n_profiles)
 }
 
 cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
-                              const int *prof_batch, int n_profiles, unsigned npix, double *partials,
+                              const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
                               unsigned *tickets, double *out, cudaStream_t s)
 {
 	const unsigned bx = jac_reduce_blocks(npix, n_profiles);
-	k_jac_reduce<<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, partials,
-	                                                  tickets, out);
+	if (nt <= 9)
+		k_jac_reduce<9><<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, nt,
+		                                                     partials, tickets, out);
+	else
+		k_jac_reduce<NTAN><<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, nt,
+		                                                        partials, tickets, out);
 	note_launches(1);
 	return cudaGetLastError();
 }
