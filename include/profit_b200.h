@@ -183,6 +183,39 @@ int pf_model_set_adjoint_mode(pf_model *m, int mode);
 int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_params,
                              double rel_step, double *loglike, double *grad);
 
+/* ---- Catalogue batches --------------------------------------------------
+ * No counterpart in libprofit: ProFit fits one galaxy at a time, one
+ * profitMakeModel / profitLikeModel call per galaxy (R/profitLikeModel.R:
+ * 225-379).  A catalogue holds many galaxies, each with its own image size,
+ * data, sigma map, PSF and 1+ radial profiles, and evaluates logL and the
+ * gradient of every galaxy in one call on the FP32 adjoint path.  Galaxies of
+ * a similar size and the same PSF size are batched together on the device.
+ *
+ * pf_catalogue_add_galaxy: data and sigma are width x height row-major
+ * doubles, the PSF psf_w x psf_h (normalised on copy); all pixels count.
+ * pf_catalogue_add_profile: a radial profile (sersic, moffat, ferrer,
+ * coresersic, king, brokenexp) with n_params "name"/value pairs over
+ * libprofit's defaults; convolve defaults to true here.
+ * pf_catalogue_loglike_grad: loglike[galaxy]; grad holds, galaxy after
+ * galaxy and profile after profile, d logL / d(xcen, ycen, mag, ang, axrat,
+ * box, then the kind's shape parameters: sersic re, nser; moffat fwhm, con;
+ * ferrer rout, a, b; coresersic re, rb, nser, a, b; king rc, rt, a;
+ * brokenexp h1, h2, rb, a).  pf_catalogue_gradient_offset gives a galaxy's
+ * slice, pf_catalogue_size the totals. */
+typedef struct pf_catalogue pf_catalogue;
+int pf_catalogue_create(pf_catalogue **out);
+int pf_catalogue_destroy(pf_catalogue *c);
+int pf_catalogue_set_magzero(pf_catalogue *c, double magzero);
+int pf_catalogue_add_galaxy(pf_catalogue *c, unsigned width, unsigned height, const double *data,
+                            const double *sigma, const double *psf, unsigned psf_w, unsigned psf_h, int *index);
+int pf_catalogue_add_profile(pf_catalogue *c, int galaxy, const char *kind, int n_params,
+                             const char *const *names, const double *values);
+int pf_catalogue_size(pf_catalogue *c, int *n_galaxies, int *n_grad);
+int pf_catalogue_gradient_offset(pf_catalogue *c, int galaxy, int *offset, int *count);
+int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad);
+/* Device time (ms, CUDA events) of the last pf_catalogue_loglike_grad. */
+int pf_catalogue_last_time(pf_catalogue *c, float *ms);
+
 /* ---- Likelihood of device-resident images, allocating nothing ----------
  * No counterpart in libprofit or ProFit: it is the "norm" log-likelihood of
  * profitLikeModel (R/profitLikeModel.R:263-276), the sum pf_model_loglike

@@ -125,6 +125,17 @@ def _late_bindings(L):
     L.pf_model_set_parameters.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, _dp]
     L.pf_model_loglike_grad_batch.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, C.c_int, _dp, _dp, _dp]
     L.pf_model_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
+    vp = C.c_void_p
+    L.pf_catalogue_create.argtypes = [C.POINTER(vp)]
+    L.pf_catalogue_destroy.argtypes = [vp]
+    L.pf_catalogue_set_magzero.argtypes = [vp, C.c_double]
+    L.pf_catalogue_add_galaxy.argtypes = [vp, C.c_uint, C.c_uint, _dp, _dp, _dp, C.c_uint, C.c_uint,
+                                          C.POINTER(C.c_int)]
+    L.pf_catalogue_add_profile.argtypes = [vp, C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_char_p), _dp]
+    L.pf_catalogue_size.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.pf_catalogue_gradient_offset.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.pf_catalogue_loglike_grad.argtypes = [vp, _dp, _dp]
+    L.pf_catalogue_last_time.argtypes = [vp, C.POINTER(C.c_float)]
     # device pointers travel as plain integers (e.g. a torch tensor's data_ptr())
     L.pf_loglike_norm_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
                                           C.c_void_p, C.c_void_p]
@@ -136,4 +147,7 @@ PF_ADJOINT_RECOMPUTE = 2
 PF_LOGLIKE_NOALLOC_MAX_BATCH = 64
 
 EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch", "pf_model_set_adjoint_mode",
-                       "pf_loglike_norm_noalloc")
+                       "pf_loglike_norm_noalloc", "pf_catalogue_create", "pf_catalogue_destroy",
+                       "pf_catalogue_set_magzero", "pf_catalogue_add_galaxy", "pf_catalogue_add_profile",
+                       "pf_catalogue_size", "pf_catalogue_gradient_offset", "pf_catalogue_loglike_grad",
+                       "pf_catalogue_last_time")

@@ -46,7 +46,7 @@ template <class T, class Acc, class TOut, int RY, int TYT, int KS>
 __global__ void __launch_bounds__(32 * TYT * KS)
     k_conv_tile(const T *__restrict__ src, int sw, int sh, int ox, int oy, const T *__restrict__ K, int kw, int kh,
                 TOut *__restrict__ out, int ow, int oh, const T *__restrict__ add, int add_stride, int add_ox,
-                int add_oy, int batch_src_stride, int batch_out_stride)
+                int add_oy, int batch_src_stride, int batch_out_stride, int batch_k_stride)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	constexpr int TX = 32;
@@ -61,6 +61,7 @@ __global__ void __launch_bounds__(32 * TYT * KS)
 	const int b = blockIdx.z;
 	src += (size_t)b * batch_src_stride;
 	out += (size_t)b * batch_out_stride;
+	K += (size_t)b * batch_k_stride;
 	if (add) add += (size_t)b * batch_src_stride;
 
 	const int i0 = blockIdx.x * TX;
@@ -172,7 +173,7 @@ inline size_t conv_smem_bytes(int kw, int kh)
 template <class T, class Acc, class TOut, int RY, int TYT, int KS>
 inline cudaError_t launch_conv(const T *src, int sw, int sh, int ox, int oy, const T *K, int kw, int kh, TOut *out,
                                int ow, int oh, const T *add, int add_stride, int add_ox, int add_oy, int batch,
-                               int batch_src_stride, int batch_out_stride, cudaStream_t stream)
+                               int batch_src_stride, int batch_out_stride, int batch_k_stride, cudaStream_t stream)
 {
 	size_t smem = conv_smem_bytes<T, Acc, RY, TYT, KS>(kw, kh);
 	static bool configured = false;
@@ -187,7 +188,7 @@ inline cudaError_t launch_conv(const T *src, int sw, int sh, int ox, int oy, con
 	dim3 grid((ow + 31) / 32, (oh + TYT * RY - 1) / (TYT * RY), batch);
 	k_conv_tile<T, Acc, TOut, RY, TYT, KS><<<grid, block, smem, stream>>>(
 	    src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch_src_stride,
-	    batch_out_stride);
+	    batch_out_stride, batch_k_stride);
 	return cudaGetLastError();
 }
 
@@ -212,6 +213,7 @@ struct ConvArgs {
 	int add_stride, add_ox, add_oy, batch, batch_src_stride, batch_out_stride;
 	void *scratch = nullptr;  // FP64 partial images for kernels that split the kernel columns over CTAs
 	size_t scratch_bytes = 0;
+	int batch_k_stride = 0;   // kernel elements between batch entries (0: one kernel for all)
 };
 
 template <class T, class Acc, class TOut, int RY, int TYT, int KS>
@@ -222,7 +224,7 @@ struct ConvVariant {
 		return launch_conv<T, Acc, TOut, RY, TYT, KS>(
 		    static_cast<const T *>(a.src), a.sw, a.sh, a.ox, a.oy, static_cast<const T *>(a.K), a.kw, a.kh,
 		    static_cast<TOut *>(a.out), a.ow, a.oh, static_cast<const T *>(a.add), a.add_stride, a.add_ox, a.add_oy,
-		    a.batch, a.batch_src_stride, a.batch_out_stride, s);
+		    a.batch, a.batch_src_stride, a.batch_out_stride, a.batch_k_stride, s);
 	}
 };
 

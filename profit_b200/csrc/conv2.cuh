@@ -124,7 +124,8 @@ template <class TOut, int HL, int RY, int TYT, int KS, int KSPLIT>
 __global__ void __launch_bounds__(32 * TYT * KS)
     k_conv3_tile(const float *__restrict__ src, int sw, int sh, int ox, int oy, const float *__restrict__ K, int kw,
                  int kh, TOut *__restrict__ out, int ow, int oh, const float *__restrict__ add, int add_stride,
-                 int add_ox, int add_oy, int batch_src_stride, int batch_out_stride, double *__restrict__ part)
+                 int add_ox, int add_oy, int batch_src_stride, int batch_out_stride, int batch_k_stride,
+                 double *__restrict__ part)
 {
 	using S = Conv3Shape<HL, RY, TYT, KS, KSPLIT>;
 	static_assert(RY % 2 == 0, "taps are consumed in pairs");
@@ -141,6 +142,7 @@ __global__ void __launch_bounds__(32 * TYT * KS)
 	float2 *s_src = s_k + (size_t)ncol * khp;            // [twj][thp], transposed pairs
 
 	src += (size_t)b * batch_src_stride;
+	K += (size_t)b * batch_k_stride;
 	const int i0 = blockIdx.x * S::TX;
 	const int j0 = blockIdx.y * S::TY;
 	constexpr int NWARPS = TYT * KS;
@@ -289,7 +291,7 @@ struct Conv3Variant {
 		k_conv3_tile<TOut, HL, RY, TYT, KS, KSPLIT><<<grid, block, smem, s>>>(
 		    static_cast<const float *>(a.src), a.sw, a.sh, a.ox, a.oy, static_cast<const float *>(a.K), a.kw, a.kh,
 		    static_cast<TOut *>(a.out), a.ow, a.oh, static_cast<const float *>(a.add), a.add_stride, a.add_ox,
-		    a.add_oy, a.batch_src_stride, a.batch_out_stride, static_cast<double *>(a.scratch));
+		    a.add_oy, a.batch_src_stride, a.batch_out_stride, a.batch_k_stride, static_cast<double *>(a.scratch));
 		if (KSPLIT > 1) {
 			size_t n = (size_t)a.ow * a.oh * a.batch;
 			int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);

@@ -52,11 +52,13 @@ cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned
 cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                                double *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
                                int batch, int batch_src_stride, int batch_out_stride, double *scratch,
-                               size_t scratch_bytes, cudaStream_t s);
+                               size_t scratch_bytes, int batch_k_stride, cudaStream_t s);
+// batch_k_stride: elements between the kernels of consecutive batch entries
+// (0: one kernel for the whole batch)
 cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                           float *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
                           int batch, int batch_src_stride, int batch_out_stride, double *scratch, size_t scratch_bytes,
-                          cudaStream_t s);
+                          int batch_k_stride, cudaStream_t s);
 // FP64 scratch (bytes) that lets the FP32 convolution split kernel columns
 // over CTAs for `batch` outputs of ow x oh; 0 when the batch is large enough
 // to fill the GPU without it.
@@ -96,4 +98,12 @@ namespace pf {
 cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
                                      unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
                                      int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s);
+}  // namespace pf
+
+namespace pf {
+// render32.cu: catalogue batches (each entry with its own profiles)
+cudaError_t launch_cat_prologue(const ProfileParams *params, int n, const ModelGeom &g, DevProfile *dev,
+                                FProfile *fprof, cudaStream_t s);
+cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,
+                                cudaStream_t s);
 }  // namespace pf

@@ -14,6 +14,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <tuple>
 #include <string>
@@ -617,7 +618,7 @@ int forward_conv32(pf_model *m, const Analysis &a, const float *conv, const floa
 	if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
 	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64, a.cw,
 	                           a.ch, plain, a.dw, a.padx, a.pady, batch, (int)npix, (int)nout,
-	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, m->stream));
+	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, 0, m->stream));
 	return PF_OK;
 }
 
@@ -644,7 +645,7 @@ int adjoint_conv32(pf_model *m, const Analysis &a, const float *wseed, float *gc
 	if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
 	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(), m->psf_w,
 	                      m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, batch, (int)nout, (int)npix,
-	                      sb ? m->d_convsplit.as<double>() : nullptr, sb, m->stream));
+	                      sb ? m->d_convsplit.as<double>() : nullptr, sb, 0, m->stream));
 	return PF_OK;
 }
 
@@ -1799,6 +1800,423 @@ int pf_model_last_timings(pf_model *m, float *ms, int n)
 {
 	if (!m || !ms) return set_error(PF_E_INVALID, "null argument");
 	for (int i = 0; i < n && i < 4; i++) ms[i] = m->timings[i];
+	return PF_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Catalogue batches: many galaxies, each with its own image size, PSF, data
+// and profiles, evaluated together.  Galaxies are grouped into buckets of one
+// canvas size and one PSF size; inside a bucket each galaxy sits at the
+// top-left of the canvas, its extra pixels carry zero weight (region mask),
+// and its own PSF and data are picked by batch index.  A larger canvas leaves
+// the cropped model of a galaxy unchanged: the PSF reaches only psf/2 pixels
+// beyond the image, and that border is drawn for every galaxy.
+// ===========================================================================
+
+namespace {
+
+struct CatGalaxy {
+	unsigned w = 0, h = 0, pw = 0, ph = 0;
+	std::vector<double> data, sigma, psf;  // psf normalised
+	std::vector<ProfileParams> profiles;
+};
+
+// One launch group: galaxies of one bucket, static inputs resident.
+struct CatChunk {
+	unsigned W = 0, H = 0, pw = 0, ph = 0;
+	std::vector<int> members;           // galaxy indices
+	std::vector<int> member_grad_off;   // offset of each member's gradient in the chunk's buffer
+	int nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3;
+	bool ak = false;
+	DevBuf params, data, sigma, region, psf32, psfrev32, prof_begin, prof_batch, grad_off, dev, T, ll, grad;
+	HostBuf h_ll, h_grad, h_ctrl;
+};
+
+constexpr size_t CAT_BUDGET_BYTES = 12ull << 30;
+constexpr unsigned CAT_SIDE_STEP = 64;
+
+}  // namespace
+
+struct pf_catalogue {
+	std::vector<CatGalaxy> gal;
+	double magzero = 0;
+	pf_model *engine = nullptr;  // stream, scratch buffers, queue capacities
+	bool built = false;
+	std::vector<std::unique_ptr<CatChunk>> chunks;
+	std::vector<int> grad_off;
+	int grad_total = 0;
+	float last_ms = 0;
+	cudaEvent_t ev[2] = {};
+};
+
+namespace {
+
+int cat_set_param(ProfileParams &p, const char *name, double value)
+{
+	const ParamDesc *d = find_param(p.kind, name);
+	if (!d)
+		return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown parameter in profile ") + kind_name(p.kind) + ": " +
+		                                         name);
+	char *base = reinterpret_cast<char *>(&p) + d->off;
+	if (d->type == T_DOUBLE) *reinterpret_cast<double *>(base) = value;
+	else if (d->type == T_UINT) *reinterpret_cast<uint32_t *>(base) = (uint32_t)value;
+	else *reinterpret_cast<int32_t *>(base) = value != 0;
+	return PF_OK;
+}
+
+// Groups galaxies into chunks and uploads each chunk's static inputs.
+int cat_build(pf_catalogue *c)
+{
+	// gradient layout: per galaxy, per profile (xcen, ycen, mag, ang, axrat, box, shape...)
+	c->grad_off.assign(c->gal.size(), 0);
+	int total = 0;
+	for (size_t g = 0; g < c->gal.size(); g++) {
+		c->grad_off[g] = total;
+		for (auto &p : c->gal[g].profiles) total += 6 + shape_count(p.kind);
+	}
+	c->grad_total = total;
+	// buckets: canvas side class x PSF size
+	std::map<std::tuple<unsigned, unsigned, unsigned>, std::vector<int>> buckets;
+	for (size_t g = 0; g < c->gal.size(); g++) {
+		const CatGalaxy &G = c->gal[g];
+		unsigned side = std::max(G.w, G.h);
+		unsigned cls = (side + CAT_SIDE_STEP - 1) / CAT_SIDE_STEP;
+		buckets[std::make_tuple(cls, G.pw, G.ph)].push_back((int)g);
+	}
+	c->chunks.clear();
+	for (auto &kv : buckets) {
+		const auto &mem = kv.second;
+		unsigned W = 0, H = 0;
+		for (int g : mem) {
+			W = std::max(W, c->gal[g].w);
+			H = std::max(H, c->gal[g].h);
+		}
+		const unsigned pw = std::get<1>(kv.first), ph = std::get<2>(kv.first);
+		const size_t npix = (size_t)(W + 2 * (pw / 2)) * (H + 2 * (ph / 2)), nout = (size_t)W * H;
+		size_t start = 0;
+		while (start < mem.size()) {
+			// members of this chunk: scratch within the budget, profile index within 16 bits
+			size_t bytes = 0, end = start;
+			int np = 0;
+			while (end < mem.size()) {
+				const int g = mem[end];
+				const int gp = (int)c->gal[g].profiles.size();
+				const size_t b = npix * (8 + 12) + nout * (8 + 4) + (size_t)gp * NTAN * npix * 4;
+				if (end > start && (bytes + b > CAT_BUDGET_BYTES || np + gp > 60000)) break;
+				bytes += b;
+				np += gp;
+				end++;
+			}
+			auto ch = std::make_unique<CatChunk>();
+			ch->W = W;
+			ch->H = H;
+			ch->pw = pw;
+			ch->ph = ph;
+			ch->members.assign(mem.begin() + start, mem.begin() + end);
+			start = end;
+			c->chunks.push_back(std::move(ch));
+		}
+	}
+	// static inputs
+	for (auto &chp : c->chunks) {
+		CatChunk &ch = *chp;
+		const int C = (int)ch.members.size();
+		const size_t nout = (size_t)ch.W * ch.H, nk = (size_t)ch.pw * ch.ph;
+		std::vector<ProfileParams> params;
+		std::vector<int> prof_begin(C + 1, 0), prof_batch, goff;
+		std::vector<double> data(nout * C, 0.0), sigma(nout * C, 1.0);
+		std::vector<uint8_t> region(nout * C, 0);
+		std::vector<float> psf(nk * C), psfrev(nk * C);
+		ch.member_grad_off.assign(C, 0);
+		int gtot = 0;
+		ch.levels = 1;
+		ch.nt = NTAN_GEOM + 3;
+		ch.ak = false;
+		for (int i = 0; i < C; i++) {
+			const CatGalaxy &G = c->gal[ch.members[i]];
+			ch.member_grad_off[i] = gtot;
+			for (auto &p : G.profiles) {
+				params.push_back(p);
+				prof_batch.push_back(i);
+				goff.push_back(gtot);
+				gtot += 6 + shape_count(p.kind);
+				unsigned mr = p.max_recursions;
+				if (p.kind == PK_SERSIC && p.adjust && p.nser > 1) mr = std::max(mr, 10u);
+				ch.levels = std::max(ch.levels, (int)mr + 1);
+				ch.nt = std::max(ch.nt, tangent_count(p.kind));
+				if (p.kind != PK_SERSIC && p.kind != PK_MOFFAT) ch.ak = true;
+			}
+			prof_begin[i + 1] = (int)params.size();
+			for (unsigned y = 0; y < G.h; y++)
+				for (unsigned x = 0; x < G.w; x++) {
+					const size_t o = (size_t)i * nout + x + (size_t)y * ch.W;
+					data[o] = G.data[x + (size_t)y * G.w];
+					sigma[o] = G.sigma[x + (size_t)y * G.w];
+					region[o] = 1;
+				}
+			for (size_t k = 0; k < nk; k++) {
+				psf[(size_t)i * nk + k] = (float)G.psf[k];
+				psfrev[(size_t)i * nk + k] = (float)G.psf[nk - 1 - k];
+			}
+		}
+		ch.nprof = (int)params.size();
+		ch.ngrad = gtot;
+		auto up = [&](DevBuf &b, const void *src, size_t bytes) -> int {
+			PF_CUDA(ensure(b, bytes));
+			PF_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
+			return PF_OK;
+		};
+		PF_TRY(up(ch.params, params.data(), params.size() * sizeof(ProfileParams)));
+		PF_TRY(up(ch.prof_begin, prof_begin.data(), prof_begin.size() * 4));
+		PF_TRY(up(ch.prof_batch, prof_batch.data(), prof_batch.size() * 4));
+		PF_TRY(up(ch.grad_off, goff.data(), goff.size() * 4));
+		PF_TRY(up(ch.data, data.data(), data.size() * 8));
+		PF_TRY(up(ch.sigma, sigma.data(), sigma.size() * 8));
+		PF_TRY(up(ch.region, region.data(), region.size()));
+		PF_TRY(up(ch.psf32, psf.data(), psf.size() * 4));
+		PF_TRY(up(ch.psfrev32, psfrev.data(), psfrev.size() * 4));
+		PF_CUDA(ensure(ch.dev, params.size() * sizeof(DevProfile)));
+		PF_CUDA(ensure(ch.T, params.size() * NTAN * 8));
+		PF_CUDA(ensure(ch.ll, (size_t)C * 8));
+		PF_CUDA(ensure(ch.grad, (size_t)std::max(gtot, 1) * 8));
+		PF_CUDA(ensure(ch.h_ll, (size_t)C * 8));
+		PF_CUDA(ensure(ch.h_grad, (size_t)std::max(gtot, 1) * 8));
+		PF_CUDA(ensure(ch.h_ctrl, CTRL_WORDS * 4));
+	}
+	c->built = true;
+	return PF_OK;
+}
+
+// One chunk on the engine's stream; returns with its results in the host
+// staging buffers (after a synchronisation), re-running on queue overflow.
+int cat_run_chunk(pf_catalogue *c, CatChunk &ch)
+{
+	pf_model *m = c->engine;
+	cudaStream_t s = m->stream;
+	const int C = (int)ch.members.size();
+	Analysis a;
+	a.conv = true;
+	a.padx = ch.pw / 2;
+	a.pady = ch.ph / 2;
+	a.cw = ch.W;
+	a.ch = ch.H;
+	a.dw = ch.W + 2 * a.padx;
+	a.dh = ch.H + 2 * a.pady;
+	a.ow = ch.W;
+	a.oh = ch.H;
+	a.levels = ch.levels;
+	a.n_profiles = ch.nprof;
+	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
+	PF_CUDA(ensure(m->d_conv32, npix * 4 * C));
+	PF_CUDA(ensure(m->d_plain32, npix * 4 * C));
+	PF_CUDA(ensure(m->d_gconv, npix * 4 * C));
+	PF_CUDA(ensure(m->d_gplain, npix * 4 * C));
+	PF_CUDA(ensure(m->d_model64, nout * 8 * C));
+	PF_CUDA(ensure(m->d_wseed, nout * 4 * C));
+	PF_CUDA(ensure(m->d_jac, npix * (size_t)ch.nt * ch.nprof * 4));
+	PF_CUDA(ensure(m->d_partials, (size_t)C * NPARTS * sizeof(double2)));
+	PF_CUDA(ensure(m->d_fprof, (size_t)ch.nprof * sizeof(FProfile)));
+	ModelGeom g;
+	g.magzero = c->magzero;
+	g.sx = g.sy = g.img_sx = g.img_sy = 1;
+	g.offx = a.padx;
+	g.offy = a.pady;
+	g.finesampling = 1;
+	for (int attempt = 0; attempt < 8; attempt++) {
+		QueueSet q;
+		PF_TRY(prepare_queue(m, a, npix * C, q, nullptr, nullptr));
+		float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *jac = m->d_jac.as<float>();
+		float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>(), *wseed = m->d_wseed.as<float>();
+		double *model64 = m->d_model64.as<double>();
+		FProfile *fprof = m->d_fprof.as<FProfile>();
+		PF_CUDA(cudaMemsetAsync(ch.T.p, 0, (size_t)ch.nprof * NTAN * 8, s));
+		PF_CUDA(launch_cat_prologue(ch.params.as<ProfileParams>(), ch.nprof, g, ch.dev.as<DevProfile>(), fprof, s));
+		PF_CUDA(launch_pixels32(fprof, ch.prof_begin.as<int>(), C, a.dw, a.dh, 1.0, 1.0, conv, plain, jac, ch.nt, ch.ak,
+		                        q, s));
+		PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, q, s));
+		const int kstride = (int)(ch.pw * ch.ph);
+		size_t sb = conv32_scratch_bytes(a.cw, a.ch, C);
+		if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
+		PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, ch.psfrev32.as<float>(), ch.pw, ch.ph, model64, a.cw, a.ch,
+		                           plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout,
+		                           sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
+		PF_CUDA(launch_loglike64_batch(model64, ch.data.as<double>(), ch.sigma.as<double>(), ch.region.as<uint8_t>(),
+		                               (int)nout, C, (int)nout, m->d_partials.as<double2>(), NPARTS,
+		                               ch.ll.as<double>(), wseed, s));
+		PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
+		sb = conv32_scratch_bytes(a.dw, a.dh, C);
+		if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
+		PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)ch.pw, 1 - (int)ch.ph, ch.psf32.as<float>(), ch.pw, ch.ph,
+		                      gconv, a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix,
+		                      sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
+		double *jpart;
+		unsigned *jtick;
+		PF_TRY(jac_scratch(m, (unsigned)npix, ch.nprof, &jpart, &jtick));
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, ch.prof_batch.as<int>(), ch.nprof, (unsigned)npix, ch.nt,
+		                          jpart, jtick, ch.T.as<double>(), s));
+		PF_CUDA(launch_cat_gradient(ch.dev.as<DevProfile>(), ch.nprof, ch.T.as<double>(), ch.grad_off.as<int>(),
+		                            ch.grad.as<double>(), s));
+		PF_CUDA(cudaMemcpyAsync(ch.h_ll.p, ch.ll.p, (size_t)C * 8, cudaMemcpyDeviceToHost, s));
+		PF_CUDA(cudaMemcpyAsync(ch.h_grad.p, ch.grad.p, (size_t)std::max(ch.ngrad, 1) * 8, cudaMemcpyDeviceToHost, s));
+		PF_CUDA(cudaMemcpyAsync(ch.h_ctrl.p, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
+		PF_CUDA(cudaStreamSynchronize(s));
+		int retry = 0;
+		PF_TRY(check_overflow(m, a, ch.h_ctrl.as<uint32_t>(), retry));
+		if (!retry) return PF_OK;
+	}
+	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+}
+
+}  // namespace
+
+extern "C" {
+
+int pf_catalogue_create(pf_catalogue **out)
+{
+	if (!out) return set_error(PF_E_INVALID, "null output pointer");
+	pf_catalogue *c = new pf_catalogue();
+	int st = pf_model_create(1, 1, &c->engine);
+	if (st != PF_OK) {
+		delete c;
+		return st;
+	}
+	c->engine->precision = PF_FP32;
+	for (auto &e : c->ev) cudaEventCreate(&e);
+	*out = c;
+	return PF_OK;
+}
+
+int pf_catalogue_destroy(pf_catalogue *c)
+{
+	if (!c) return PF_OK;
+	c->chunks.clear();
+	for (auto &e : c->ev)
+		if (e) cudaEventDestroy(e);
+	pf_model_destroy(c->engine);
+	delete c;
+	return PF_OK;
+}
+
+int pf_catalogue_set_magzero(pf_catalogue *c, double magzero)
+{
+	if (!c) return set_error(PF_E_INVALID, "null catalogue");
+	c->magzero = magzero;
+	c->built = false;
+	return PF_OK;
+}
+
+int pf_catalogue_add_galaxy(pf_catalogue *c, unsigned width, unsigned height, const double *data,
+                            const double *sigma, const double *psf, unsigned psf_w, unsigned psf_h, int *index)
+{
+	if (!c || !data || !sigma || !psf) return set_error(PF_E_INVALID, "null argument");
+	if (width == 0 || height == 0 || psf_w == 0 || psf_h == 0) return set_error(PF_E_INVALID, "empty image or psf");
+	if (width > 4096 || height > 4096 || psf_w > 255 || psf_h > 255)
+		return set_error(PF_E_INVALID, "catalogue galaxies are limited to 4096 x 4096 images and 255 x 255 PSFs");
+	CatGalaxy G;
+	G.w = width;
+	G.h = height;
+	G.pw = psf_w;
+	G.ph = psf_h;
+	G.data.assign(data, data + (size_t)width * height);
+	G.sigma.assign(sigma, sigma + (size_t)width * height);
+	for (double s : G.sigma)
+		if (!(s > 0)) return set_error(PF_E_INVALID, "sigma must be positive");
+	double sum = 0;
+	for (size_t k = 0; k < (size_t)psf_w * psf_h; k++) sum += psf[k];
+	if (!(sum > 0)) return set_error(PF_E_INVALID, "psf must have a positive sum");
+	G.psf.assign(psf, psf + (size_t)psf_w * psf_h);
+	for (double &v : G.psf) v /= sum;
+	c->gal.push_back(std::move(G));
+	c->built = false;
+	if (index) *index = (int)c->gal.size() - 1;
+	return PF_OK;
+}
+
+int pf_catalogue_add_profile(pf_catalogue *c, int galaxy, const char *kind, int n_params, const char *const *names,
+                             const double *values)
+{
+	if (!c || !kind || (n_params > 0 && (!names || !values))) return set_error(PF_E_INVALID, "null argument");
+	if (galaxy < 0 || galaxy >= (int)c->gal.size()) return set_error(PF_E_INVALID, "galaxy index out of range");
+	int k = kind_from_name(kind);
+	if (k < 0) return set_error(PF_E_INVALID, std::string("Unknown profile name: ") + kind);
+	if (!is_radial_kind(k)) return set_error(PF_E_INVALID, "catalogue galaxies take radial profiles only");
+	ProfileParams p = default_params(k);
+	p.convolve = 1;
+	for (int i = 0; i < n_params; i++) PF_TRY(cat_set_param(p, names[i], values[i]));
+	const char *err = validate_profile(p, true);
+	if (err) return set_error(PF_E_INVALID, err);
+	if (!params_valid(p)) return set_error(PF_E_INVALID, "invalid profile parameters");
+	if (p.kind == PK_SERSIC && p.rescale_flux) return set_error(PF_E_INVALID, "gradients with rescale_flux are not available");
+	if (!p.adjust && !p.rough && (p.resolution == 0 || p.resolution > 16))
+		return set_error(PF_E_INVALID, "resolution must be in [1, 16] when adjust is false");
+	if (p.max_recursions + 1 > (unsigned)MAX_LEVELS) return set_error(PF_E_INVALID, "max_recursions above 15 is not supported");
+	c->gal[galaxy].profiles.push_back(p);
+	c->built = false;
+	return PF_OK;
+}
+
+int pf_catalogue_size(pf_catalogue *c, int *n_galaxies, int *n_grad)
+{
+	if (!c) return set_error(PF_E_INVALID, "null catalogue");
+	int total = 0;
+	for (auto &G : c->gal)
+		for (auto &p : G.profiles) total += 6 + shape_count(p.kind);
+	if (n_galaxies) *n_galaxies = (int)c->gal.size();
+	if (n_grad) *n_grad = total;
+	return PF_OK;
+}
+
+int pf_catalogue_gradient_offset(pf_catalogue *c, int galaxy, int *offset, int *count)
+{
+	if (!c) return set_error(PF_E_INVALID, "null catalogue");
+	if (galaxy < 0 || galaxy >= (int)c->gal.size()) return set_error(PF_E_INVALID, "galaxy index out of range");
+	int off = 0;
+	for (int g = 0; g < galaxy; g++)
+		for (auto &p : c->gal[g].profiles) off += 6 + shape_count(p.kind);
+	int n = 0;
+	for (auto &p : c->gal[galaxy].profiles) n += 6 + shape_count(p.kind);
+	if (offset) *offset = off;
+	if (count) *count = n;
+	return PF_OK;
+}
+
+int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
+{
+	if (!c || !loglike) return set_error(PF_E_INVALID, "null argument");
+	if (c->gal.empty()) return PF_OK;
+	for (auto &G : c->gal)
+		if (G.profiles.empty()) return set_error(PF_E_STATE, "a catalogue galaxy has no profiles");
+	PF_TRY(ensure_stream(c->engine));
+	if (!c->built) PF_TRY(cat_build(c));
+	cudaStream_t s = c->engine->stream;
+	PF_CUDA(cudaEventRecord(c->ev[0], s));
+	for (auto &chp : c->chunks) {
+		CatChunk &ch = *chp;
+		PF_TRY(cat_run_chunk(c, ch));
+		const double *hl = ch.h_ll.as<double>(), *hg = ch.h_grad.as<double>();
+		for (size_t i = 0; i < ch.members.size(); i++) {
+			const int g = ch.members[i];
+			loglike[g] = hl[i];
+			if (grad) {
+				int n = 0;
+				for (auto &p : c->gal[g].profiles) n += 6 + shape_count(p.kind);
+				std::memcpy(grad + c->grad_off[g], hg + ch.member_grad_off[i], (size_t)n * 8);
+			}
+		}
+	}
+	PF_CUDA(cudaEventRecord(c->ev[1], s));
+	PF_CUDA(cudaEventSynchronize(c->ev[1]));
+	cudaEventElapsedTime(&c->last_ms, c->ev[0], c->ev[1]);
+	cudaGetLastError();
+	return PF_OK;
+}
+
+int pf_catalogue_last_time(pf_catalogue *c, float *ms)
+{
+	if (!c || !ms) return set_error(PF_E_INVALID, "null argument");
+	*ms = c->last_ms;
 	return PF_OK;
 }
 

@@ -915,7 +915,7 @@ template <class TOut>
 static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                               TOut *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
                               int batch, int batch_src_stride, int batch_out_stride, double *scratch,
-                              size_t scratch_bytes, cudaStream_t s)
+                              size_t scratch_bytes, int batch_k_stride, cudaStream_t s)
 {
 	note_launches(1);
 	static const ConvCandidate cands[] = {
@@ -939,7 +939,7 @@ static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, 
 	    {ConvVariant<float, double, TOut, 8, 2, 4>::smem, ConvVariant<float, double, TOut, 8, 2, 4>::run},
 	};
 	ConvArgs a{src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
-	           batch_src_stride, batch_out_stride, scratch, scratch_bytes};
+	           batch_src_stride, batch_out_stride, scratch, scratch_bytes, batch_k_stride};
 	return conv_autotuned(cands, (int)(sizeof(cands) / sizeof(cands[0])), sizeof(TOut) == 8 ? 2 : 1, a, s);
 }
 
@@ -952,19 +952,19 @@ size_t conv32_scratch_bytes(int ow, int oh, int batch)
 cudaError_t launch_conv32(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                           float *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
                           int batch, int batch_src_stride, int batch_out_stride, double *scratch, size_t scratch_bytes,
-                          cudaStream_t s)
+                          int batch_k_stride, cudaStream_t s)
 {
 	return conv32_any<float>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
-	                         batch_src_stride, batch_out_stride, scratch, scratch_bytes, s);
+	                         batch_src_stride, batch_out_stride, scratch, scratch_bytes, batch_k_stride, s);
 }
 
 cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
                                double *out, int ow, int oh, const float *add, int add_stride, int add_ox, int add_oy,
                                int batch, int batch_src_stride, int batch_out_stride, double *scratch,
-                               size_t scratch_bytes, cudaStream_t s)
+                               size_t scratch_bytes, int batch_k_stride, cudaStream_t s)
 {
 	return conv32_any<double>(src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
-	                          batch_src_stride, batch_out_stride, scratch, scratch_bytes, s);
+	                          batch_src_stride, batch_out_stride, scratch, scratch_bytes, batch_k_stride, s);
 }
 
 cudaError_t launch_loglike32(const float *model, const double *data, const double *sigma, const uint8_t *region,
@@ -1051,6 +1051,54 @@ cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, c
 	int n = batch * (nrefs > 1 ? nrefs : 1);
 	k_batch_gradient<<<(n + 255) / 256, 256, 0, s>>>(dev, nprof, batch, ref_profile, ref_code, nrefs, T, ll, invalid,
 	                                                 out_ll, out_grad);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+// Catalogue batches: every galaxy brings its own profiles, so the prologue
+// reads one parameter record per profile (validated when the galaxy was
+// added) instead of a template plus a value matrix.
+__global__ void k_cat_prologue(const ProfileParams *__restrict__ params, int n, ModelGeom g,
+                               DevProfile *__restrict__ dev, FProfile *__restrict__ fprof)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n) return;
+	const ProfileParams pp = params[t];
+	DevProfile d;
+	derive_profile(pp, g, d);
+	dev[t] = d;
+	fprof[t] = to_fprofile(d, pp);
+}
+
+// One thread per profile: d logL / d(every parameter of the profile) from its
+// tangent reductions, in the order xcen, ycen, mag, ang, axrat, box, then the
+// kind's shape parameters, written at grad_off[profile].
+__global__ void k_cat_gradient(const DevProfile *__restrict__ dev, int n, const double *__restrict__ T,
+                               const int *__restrict__ grad_off, double *__restrict__ grad)
+{
+	const int t = blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= n) return;
+	const DevProfile &d = dev[t];
+	if (!is_radial_kind(d.kind)) return;
+	const double *Tp = T + (size_t)t * NTAN;
+	double *out = grad + grad_off[t];
+	const int codes[6] = {G_XCEN, G_YCEN, G_MAG, G_ANG, G_AXRAT, G_BOX};
+	for (int c = 0; c < 6; c++) out[c] = gradient_from_tangents(codes[c], d.axrat, d, Tp);
+	for (int k = 0; k < shape_count(d.kind); k++) out[6 + k] = gradient_from_tangents(G_SHAPE + k, d.axrat, d, Tp);
+}
+
+cudaError_t launch_cat_prologue(const ProfileParams *params, int n, const ModelGeom &g, DevProfile *dev,
+                                FProfile *fprof, cudaStream_t s)
+{
+	k_cat_prologue<<<(n + 127) / 128, 128, 0, s>>>(params, n, g, dev, fprof);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,
+                                cudaStream_t s)
+{
+	k_cat_gradient<<<(n + 127) / 128, 128, 0, s>>>(dev, n, T, grad_off, grad);
 	note_launches(1);
 	return cudaGetLastError();
 }

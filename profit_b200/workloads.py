@@ -160,3 +160,51 @@ def perturbed(w: Dict, seed: int, scale: float = 0.05) -> Dict:
                 break
     out["profiles"] = profs
     return out
+
+
+def catalogue_galaxy_profiles(r: np.random.Generator, side: int) -> List[Tuple[str, Dict]]:
+    """1-3 components drawn from the six radial kinds: nser ~ logU[0.5, 10],
+    re ~ logU[1, 50] px (capped at the image side), axrat ~ U[0.1, 1],
+    ang ~ U[0, 180], box ~ U[-0.3, 0.3].  Non-Sersic kinds map (re, nser) to
+    their own parameters: moffat fwhm = re, con = 1 + nser; ferrer rout = 2 re,
+    a = 1, b = 1; king rt = 3 re, rc = re, a = 2; brokenexp h1 = re, h2 = re/2,
+    rb = 2 re, a = 1; coresersic re, nser, rb = re/4, a = 2, b = 0.5."""
+    kinds = ("sersic", "coresersic", "moffat", "ferrer", "king", "brokenexp")
+    out = []
+    cx, cy = side / 2.0 + r.uniform(-2, 2), side / 2.0 + r.uniform(-2, 2)
+    for _ in range(int(r.integers(1, 4))):
+        kind = kinds[int(r.integers(0, len(kinds)))]
+        nser = float(np.exp(r.uniform(np.log(0.5), np.log(10))))
+        re = float(min(np.exp(r.uniform(0, np.log(50))), side / 2.0))
+        common = dict(xcen=cx + r.uniform(-1, 1), ycen=cy + r.uniform(-1, 1), mag=float(r.uniform(17, 21)),
+                      ang=float(r.uniform(0, 180)), axrat=float(r.uniform(0.1, 1)), box=float(r.uniform(-0.3, 0.3)))
+        if kind == "sersic":
+            shape = dict(re=re, nser=nser)
+        elif kind == "moffat":
+            shape = dict(fwhm=re, con=1 + nser)
+        elif kind == "ferrer":
+            shape = dict(rout=2 * re, a=1.0, b=1.0)
+        elif kind == "king":
+            shape = dict(rt=3 * re, rc=re, a=2.0)
+        elif kind == "brokenexp":
+            shape = dict(h1=re, h2=re / 2, rb=2 * re, a=1.0)
+        else:
+            shape = dict(re=re, nser=nser, rb=re / 4, a=2.0, b=0.5)
+        out.append((kind, dict(common, **shape)))
+    return out
+
+
+def catalogue(n: int = 10000, seed_tag: int = 6, side_range=(32, 512), magzero: float = 30.0):
+    """Uneven catalogue: n galaxies, square side ~ logU[side_range], per-galaxy
+    Gaussian or Moffat PSF of odd side in [15, 65] (FWHM ~ U[2, 4]), profiles as
+    catalogue_galaxy_profiles.  Returns a list of dicts (side, psf, profiles);
+    data and sigma come from catalogue_data()."""
+    r = _rng(seed_tag)
+    gals = []
+    for _ in range(n):
+        side = int(round(np.exp(r.uniform(np.log(side_range[0]), np.log(side_range[1])))))
+        psf_side = int(r.integers(7, 33)) * 2 + 1
+        fwhm = float(r.uniform(2, 4))
+        psf = gaussian_psf(psf_side, fwhm) if r.uniform() < 0.5 else moffat_psf(psf_side, fwhm, 2.5)
+        gals.append(dict(side=side, psf=psf, profiles=catalogue_galaxy_profiles(r, side), magzero=magzero))
+    return gals
