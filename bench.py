@@ -59,6 +59,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sampler-n", type=int, default=4096,
                     help="proposals per call of the sampler-batch line (smaller for profiling runs)")
+    ap.add_argument("--catalogue-n", type=int, default=10000,
+                    help="galaxies of the uneven-catalogue line (0 skips it)")
     return ap.parse_args()
 
 
@@ -325,6 +327,7 @@ def main_b200(args):
                               "(profiles/conv_fwd_bulge_disk_ps.txt)"}
 
     sampler = sampler_batch_rate(args, torch, flush, n=args.sampler_n)
+    catalogue = catalogue_rate(args, torch, flush, n=args.catalogue_n) if args.catalogue_n > 0 else None
 
     out = None
     if rank == 0:
@@ -346,6 +349,7 @@ def main_b200(args):
             "plain_fp64_fd": {"value": fp64_fd_value, "unit": UNIT,
                               "speedup_fp32_adjoint": (world * args.steps / dev_total) / fp64_fd_value},
             "sampler_batch": sampler,
+            "catalogue_batch": catalogue,
         }
     m.close()
     if world > 1:
@@ -397,6 +401,67 @@ def sampler_batch_rate(args, torch, flush, n=4096, calls=3):
                         "(host parameters in, logL + gradients out)",
             "value": rate, "unit": UNIT, "ms_per_call": 1e3 * statistics.mean(times),
             "plain_fp64_fd_value": fd_rate, "speedup_vs_plain_fp64_fd": rate / fd_rate,
+            "finite_fraction": float(np.isfinite(ll).mean())}
+
+
+def catalogue_rate(args, torch, flush, n=10000, calls=2, fd_sample=6):
+    """Uneven catalogue: n galaxies, side ~ logU[32, 512], odd PSF sides in
+    [15, 65], 1-3 components of the six radial kinds, logL + full gradient per
+    galaxy through pf_catalogue_loglike_grad.  The data are N(0, 1) noise with
+    sigma = 1 (the timing does not depend on the data values).  The plain
+    FP64 form with FD gradients is timed on the first fd_sample galaxies."""
+    from profit_b200 import PF_FP64, Model
+    from profit_b200 import workloads as W
+    from profit_b200.catalogue import Catalogue, grad_names
+    gals = W.catalogue(n)
+    r = np.random.Generator(np.random.PCG64([W.SEED, 93]))
+    cat = Catalogue(magzero=gals[0]["magzero"])
+    npix = 0
+    for g in gals:
+        side = g["side"]
+        npix += side * side
+        cat.add_galaxy(r.normal(size=(side, side)), np.ones((side, side)), g["psf"], g["profiles"])
+    _, ngrad = cat.size()
+    t0 = time.perf_counter()
+    cat.loglike_grad()  # warm-up: uploads, bucketing, convolution tuning
+    first_s = time.perf_counter() - t0
+    dev, wall = [], []
+    for _ in range(calls):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ll, _ = cat.loglike_grad()
+        wall.append(time.perf_counter() - t0)
+        dev.append(cat.last_time_ms() / 1e3)
+    cat.close()
+    # plain FP64 + FD on a sample of the same galaxies
+    fd_t, fd_n = 0.0, 0
+    for g in gals[:fd_sample]:
+        side = g["side"]
+        m = Model(side, side)
+        m.set_magzero(g["magzero"])
+        m.set_psf(g["psf"])
+        for kind, params in g["profiles"]:
+            m.add_profile(kind, convolve=True, **params)
+        m.set_data(r.normal(size=(side, side)), np.ones((side, side)))
+        refs = [(i, k) for i, (kind, _) in enumerate(g["profiles"]) for k in grad_names(kind)]
+        m.set_precision(PF_FP64)
+        m.loglike_grad_fd(refs, rel_step=1e-7)
+        t0 = time.perf_counter()
+        m.loglike_grad_fd(refs, rel_step=1e-7)
+        fd_t += time.perf_counter() - t0
+        fd_n += 1
+        m.close()
+    rate = n / statistics.mean(dev)
+    fd_rate = fd_n / fd_t if fd_t > 0 else None
+    return {"workload": f"uneven catalogue: {n} galaxies, side logU[32,512], odd PSF side in [15,65] (Gaussian or "
+                        "Moffat), 1-3 components from sersic/coresersic/moffat/ferrer/king/brokenexp, logL + full "
+                        "gradient per galaxy (pf_catalogue_loglike_grad); data N(0,1), sigma 1",
+            "value": rate, "unit": "galaxy LL+grad evals/s", "seconds_per_catalogue": statistics.mean(dev),
+            "wall_seconds_per_catalogue": statistics.mean(wall), "first_call_seconds": first_s,
+            "pixels": npix, "gradient_components": ngrad,
+            "plain_fp64_fd_value": fd_rate, "plain_fp64_fd_sample": f"first {fd_n} galaxies, host wall clock",
+            "speedup_vs_plain_fp64_fd": (rate / fd_rate) if fd_rate else None,
             "finite_fraction": float(np.isfinite(ll).mean())}
 
 

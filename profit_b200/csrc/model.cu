@@ -1813,6 +1813,11 @@ int pf_model_last_timings(pf_model *m, float *ms, int n)
 // and its own PSF and data are picked by batch index.  A larger canvas leaves
 // the cropped model of a galaxy unchanged: the PSF reaches only psf/2 pixels
 // beyond the image, and that border is drawn for every galaxy.
+//
+// One evaluation: one FP64 prologue launch for every profile of the
+// catalogue, then every chunk's pipeline back to back on one stream (scratch
+// and queue sized up front for the largest chunk), one synchronisation, and
+// a re-run of any chunk whose subsampling queue overflowed.
 // ===========================================================================
 
 namespace {
@@ -1828,10 +1833,12 @@ struct CatChunk {
 	unsigned W = 0, H = 0, pw = 0, ph = 0;
 	std::vector<int> members;           // galaxy indices
 	std::vector<int> member_grad_off;   // offset of each member's gradient in the chunk's buffer
-	int nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3;
+	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3;
 	bool ak = false;
-	DevBuf params, data, sigma, region, psf32, psfrev32, prof_begin, prof_batch, grad_off, dev, T, ll, grad;
+	DevBuf data, sigma, region, psf32, psfrev32, prof_begin, prof_batch, grad_off, T, ll, grad;
 	HostBuf h_ll, h_grad, h_ctrl;
+	size_t npix() const { return (size_t)(W + 2 * (pw / 2)) * (H + 2 * (ph / 2)); }
+	size_t nout() const { return (size_t)W * H; }
 };
 
 constexpr size_t CAT_BUDGET_BYTES = 12ull << 30;
@@ -1845,6 +1852,8 @@ struct pf_catalogue {
 	pf_model *engine = nullptr;  // stream, scratch buffers, queue capacities
 	bool built = false;
 	std::vector<std::unique_ptr<CatChunk>> chunks;
+	DevBuf params, pad, dev, fprof;  // every profile of the catalogue, chunk after chunk
+	int nprof = 0;
 	std::vector<int> grad_off;
 	int grad_total = 0;
 	float last_ms = 0;
@@ -1866,7 +1875,24 @@ int cat_set_param(ProfileParams &p, const char *name, double value)
 	return PF_OK;
 }
 
-// Groups galaxies into chunks and uploads each chunk's static inputs.
+Analysis cat_analysis(const CatChunk &ch)
+{
+	Analysis a;
+	a.conv = true;
+	a.padx = ch.pw / 2;
+	a.pady = ch.ph / 2;
+	a.cw = ch.W;
+	a.ch = ch.H;
+	a.dw = ch.W + 2 * a.padx;
+	a.dh = ch.H + 2 * a.pady;
+	a.ow = ch.W;
+	a.oh = ch.H;
+	a.levels = ch.levels;
+	a.n_profiles = ch.nprof;
+	return a;
+}
+
+// Groups galaxies into chunks and uploads the static inputs.
 int cat_build(pf_catalogue *c)
 {
 	// gradient layout: per galaxy, per profile (xcen, ycen, mag, ang, axrat, box, shape...)
@@ -1920,25 +1946,25 @@ int cat_build(pf_catalogue *c)
 		}
 	}
 	// static inputs
+	std::vector<ProfileParams> params;
+	std::vector<int2> pad;
 	for (auto &chp : c->chunks) {
 		CatChunk &ch = *chp;
 		const int C = (int)ch.members.size();
-		const size_t nout = (size_t)ch.W * ch.H, nk = (size_t)ch.pw * ch.ph;
-		std::vector<ProfileParams> params;
+		const size_t nout = ch.nout(), nk = (size_t)ch.pw * ch.ph;
 		std::vector<int> prof_begin(C + 1, 0), prof_batch, goff;
 		std::vector<double> data(nout * C, 0.0), sigma(nout * C, 1.0);
 		std::vector<uint8_t> region(nout * C, 0);
 		std::vector<float> psf(nk * C), psfrev(nk * C);
 		ch.member_grad_off.assign(C, 0);
+		ch.p0 = (int)params.size();
 		int gtot = 0;
-		ch.levels = 1;
-		ch.nt = NTAN_GEOM + 3;
-		ch.ak = false;
 		for (int i = 0; i < C; i++) {
 			const CatGalaxy &G = c->gal[ch.members[i]];
 			ch.member_grad_off[i] = gtot;
 			for (auto &p : G.profiles) {
 				params.push_back(p);
+				pad.push_back(make_int2((int)(ch.pw / 2), (int)(ch.ph / 2)));
 				prof_batch.push_back(i);
 				goff.push_back(gtot);
 				gtot += 6 + shape_count(p.kind);
@@ -1948,7 +1974,7 @@ int cat_build(pf_catalogue *c)
 				ch.nt = std::max(ch.nt, tangent_count(p.kind));
 				if (p.kind != PK_SERSIC && p.kind != PK_MOFFAT) ch.ak = true;
 			}
-			prof_begin[i + 1] = (int)params.size();
+			prof_begin[i + 1] = (int)params.size() - ch.p0;
 			for (unsigned y = 0; y < G.h; y++)
 				for (unsigned x = 0; x < G.w; x++) {
 					const size_t o = (size_t)i * nout + x + (size_t)y * ch.W;
@@ -1961,14 +1987,13 @@ int cat_build(pf_catalogue *c)
 				psfrev[(size_t)i * nk + k] = (float)G.psf[nk - 1 - k];
 			}
 		}
-		ch.nprof = (int)params.size();
+		ch.nprof = (int)params.size() - ch.p0;
 		ch.ngrad = gtot;
 		auto up = [&](DevBuf &b, const void *src, size_t bytes) -> int {
 			PF_CUDA(ensure(b, bytes));
 			PF_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
 			return PF_OK;
 		};
-		PF_TRY(up(ch.params, params.data(), params.size() * sizeof(ProfileParams)));
 		PF_TRY(up(ch.prof_begin, prof_begin.data(), prof_begin.size() * 4));
 		PF_TRY(up(ch.prof_batch, prof_batch.data(), prof_batch.size() * 4));
 		PF_TRY(up(ch.grad_off, goff.data(), goff.size() * 4));
@@ -1977,96 +2002,102 @@ int cat_build(pf_catalogue *c)
 		PF_TRY(up(ch.region, region.data(), region.size()));
 		PF_TRY(up(ch.psf32, psf.data(), psf.size() * 4));
 		PF_TRY(up(ch.psfrev32, psfrev.data(), psfrev.size() * 4));
-		PF_CUDA(ensure(ch.dev, params.size() * sizeof(DevProfile)));
-		PF_CUDA(ensure(ch.T, params.size() * NTAN * 8));
+		PF_CUDA(ensure(ch.T, (size_t)ch.nprof * NTAN * 8));
 		PF_CUDA(ensure(ch.ll, (size_t)C * 8));
 		PF_CUDA(ensure(ch.grad, (size_t)std::max(gtot, 1) * 8));
 		PF_CUDA(ensure(ch.h_ll, (size_t)C * 8));
 		PF_CUDA(ensure(ch.h_grad, (size_t)std::max(gtot, 1) * 8));
 		PF_CUDA(ensure(ch.h_ctrl, CTRL_WORDS * 4));
 	}
+	c->nprof = (int)params.size();
+	PF_CUDA(ensure(c->params, params.size() * sizeof(ProfileParams)));
+	PF_CUDA(cudaMemcpy(c->params.p, params.data(), params.size() * sizeof(ProfileParams), cudaMemcpyHostToDevice));
+	PF_CUDA(ensure(c->pad, pad.size() * sizeof(int2)));
+	PF_CUDA(cudaMemcpy(c->pad.p, pad.data(), pad.size() * sizeof(int2), cudaMemcpyHostToDevice));
+	PF_CUDA(ensure(c->dev, params.size() * sizeof(DevProfile)));
+	PF_CUDA(ensure(c->fprof, params.size() * sizeof(FProfile)));
+
+	// engine scratch and queue for the largest chunk, so nothing is
+	// reallocated while chunks are queued
+	pf_model *m = c->engine;
+	size_t conv = 0, model = 0, seed = 0, jac = 0, parts = 0, qpix = 0, jp = 0;
+	int levels = 1, maxprof = 0;
+	for (auto &chp : c->chunks) {
+		const CatChunk &ch = *chp;
+		const size_t C = ch.members.size();
+		conv = std::max(conv, ch.npix() * 4 * C);
+		model = std::max(model, ch.nout() * 8 * C);
+		seed = std::max(seed, ch.nout() * 4 * C);
+		jac = std::max(jac, ch.npix() * (size_t)ch.nt * ch.nprof * 4);
+		parts = std::max(parts, C * NPARTS * sizeof(double2));
+		qpix = std::max(qpix, ch.npix() * C);
+		jp = std::max(jp, (size_t)ch.nprof * jac_reduce_blocks((unsigned)ch.npix(), ch.nprof) * NTAN * 8);
+		levels = std::max(levels, ch.levels);
+		maxprof = std::max(maxprof, ch.nprof);
+	}
+	PF_CUDA(ensure(m->d_conv32, conv));
+	PF_CUDA(ensure(m->d_plain32, conv));
+	PF_CUDA(ensure(m->d_gconv, conv));
+	PF_CUDA(ensure(m->d_gplain, conv));
+	PF_CUDA(ensure(m->d_model64, model));
+	PF_CUDA(ensure(m->d_wseed, seed));
+	PF_CUDA(ensure(m->d_jac, jac));
+	PF_CUDA(ensure(m->d_partials, parts));
+	PF_CUDA(ensure(m->d_convsplit, (size_t)64 << 20));
+	PF_CUDA(ensure(m->d_jac_partials, jp));
+	void *before = m->d_jac_tickets.p;
+	PF_CUDA(ensure(m->d_jac_tickets, (size_t)maxprof * sizeof(unsigned)));
+	if (m->d_jac_tickets.p != before)
+		PF_CUDA(cudaMemsetAsync(m->d_jac_tickets.p, 0, m->d_jac_tickets.bytes, m->stream));
+	Analysis a;
+	a.levels = levels;
+	QueueSet q;
+	PF_TRY(prepare_queue(m, a, qpix, q, nullptr, nullptr));
+	PF_CUDA(cudaStreamSynchronize(m->stream));
 	c->built = true;
 	return PF_OK;
 }
 
-// One chunk on the engine's stream; returns with its results in the host
-// staging buffers (after a synchronisation), re-running on queue overflow.
-int cat_run_chunk(pf_catalogue *c, CatChunk &ch)
+// Queues one chunk's pipeline (prologue already run); results and queue
+// counters land in the chunk's pinned buffers when the stream gets there.
+int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
 {
 	pf_model *m = c->engine;
 	cudaStream_t s = m->stream;
 	const int C = (int)ch.members.size();
-	Analysis a;
-	a.conv = true;
-	a.padx = ch.pw / 2;
-	a.pady = ch.ph / 2;
-	a.cw = ch.W;
-	a.ch = ch.H;
-	a.dw = ch.W + 2 * a.padx;
-	a.dh = ch.H + 2 * a.pady;
-	a.ow = ch.W;
-	a.oh = ch.H;
-	a.levels = ch.levels;
-	a.n_profiles = ch.nprof;
-	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
-	PF_CUDA(ensure(m->d_conv32, npix * 4 * C));
-	PF_CUDA(ensure(m->d_plain32, npix * 4 * C));
-	PF_CUDA(ensure(m->d_gconv, npix * 4 * C));
-	PF_CUDA(ensure(m->d_gplain, npix * 4 * C));
-	PF_CUDA(ensure(m->d_model64, nout * 8 * C));
-	PF_CUDA(ensure(m->d_wseed, nout * 4 * C));
-	PF_CUDA(ensure(m->d_jac, npix * (size_t)ch.nt * ch.nprof * 4));
-	PF_CUDA(ensure(m->d_partials, (size_t)C * NPARTS * sizeof(double2)));
-	PF_CUDA(ensure(m->d_fprof, (size_t)ch.nprof * sizeof(FProfile)));
-	ModelGeom g;
-	g.magzero = c->magzero;
-	g.sx = g.sy = g.img_sx = g.img_sy = 1;
-	g.offx = a.padx;
-	g.offy = a.pady;
-	g.finesampling = 1;
-	for (int attempt = 0; attempt < 8; attempt++) {
-		QueueSet q;
-		PF_TRY(prepare_queue(m, a, npix * C, q, nullptr, nullptr));
-		float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *jac = m->d_jac.as<float>();
-		float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>(), *wseed = m->d_wseed.as<float>();
-		double *model64 = m->d_model64.as<double>();
-		FProfile *fprof = m->d_fprof.as<FProfile>();
-		PF_CUDA(cudaMemsetAsync(ch.T.p, 0, (size_t)ch.nprof * NTAN * 8, s));
-		PF_CUDA(launch_cat_prologue(ch.params.as<ProfileParams>(), ch.nprof, g, ch.dev.as<DevProfile>(), fprof, s));
-		PF_CUDA(launch_pixels32(fprof, ch.prof_begin.as<int>(), C, a.dw, a.dh, 1.0, 1.0, conv, plain, jac, ch.nt, ch.ak,
-		                        q, s));
-		PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, q, s));
-		const int kstride = (int)(ch.pw * ch.ph);
-		size_t sb = conv32_scratch_bytes(a.cw, a.ch, C);
-		if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
-		PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, ch.psfrev32.as<float>(), ch.pw, ch.ph, model64, a.cw, a.ch,
-		                           plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout,
-		                           sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
-		PF_CUDA(launch_loglike64_batch(model64, ch.data.as<double>(), ch.sigma.as<double>(), ch.region.as<uint8_t>(),
-		                               (int)nout, C, (int)nout, m->d_partials.as<double2>(), NPARTS,
-		                               ch.ll.as<double>(), wseed, s));
-		PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
-		sb = conv32_scratch_bytes(a.dw, a.dh, C);
-		if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
-		PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)ch.pw, 1 - (int)ch.ph, ch.psf32.as<float>(), ch.pw, ch.ph,
-		                      gconv, a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix,
-		                      sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
-		double *jpart;
-		unsigned *jtick;
-		PF_TRY(jac_scratch(m, (unsigned)npix, ch.nprof, &jpart, &jtick));
-		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, ch.prof_batch.as<int>(), ch.nprof, (unsigned)npix, ch.nt,
-		                          jpart, jtick, ch.T.as<double>(), s));
-		PF_CUDA(launch_cat_gradient(ch.dev.as<DevProfile>(), ch.nprof, ch.T.as<double>(), ch.grad_off.as<int>(),
-		                            ch.grad.as<double>(), s));
-		PF_CUDA(cudaMemcpyAsync(ch.h_ll.p, ch.ll.p, (size_t)C * 8, cudaMemcpyDeviceToHost, s));
-		PF_CUDA(cudaMemcpyAsync(ch.h_grad.p, ch.grad.p, (size_t)std::max(ch.ngrad, 1) * 8, cudaMemcpyDeviceToHost, s));
-		PF_CUDA(cudaMemcpyAsync(ch.h_ctrl.p, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
-		PF_CUDA(cudaStreamSynchronize(s));
-		int retry = 0;
-		PF_TRY(check_overflow(m, a, ch.h_ctrl.as<uint32_t>(), retry));
-		if (!retry) return PF_OK;
-	}
-	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+	const Analysis a = cat_analysis(ch);
+	const size_t npix = ch.npix(), nout = ch.nout();
+	QueueSet q;
+	PF_TRY(prepare_queue(m, a, npix * C, q, nullptr, nullptr));
+	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *jac = m->d_jac.as<float>();
+	float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>(), *wseed = m->d_wseed.as<float>();
+	double *model64 = m->d_model64.as<double>();
+	const FProfile *fprof = c->fprof.as<FProfile>() + ch.p0;
+	const DevProfile *dev = c->dev.as<DevProfile>() + ch.p0;
+	PF_CUDA(cudaMemsetAsync(ch.T.p, 0, (size_t)ch.nprof * NTAN * 8, s));
+	PF_CUDA(launch_pixels32(fprof, ch.prof_begin.as<int>(), C, a.dw, a.dh, 1.0, 1.0, conv, plain, jac, ch.nt, ch.ak, q,
+	                        s));
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, q, s));
+	const int kstride = (int)(ch.pw * ch.ph);
+	size_t sb = conv32_scratch_bytes(a.cw, a.ch, C);
+	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, ch.psfrev32.as<float>(), ch.pw, ch.ph, model64, a.cw, a.ch,
+	                           plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout,
+	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
+	PF_CUDA(launch_loglike64_batch(model64, ch.data.as<double>(), ch.sigma.as<double>(), ch.region.as<uint8_t>(),
+	                               (int)nout, C, (int)nout, m->d_partials.as<double2>(), NPARTS, ch.ll.as<double>(),
+	                               wseed, s));
+	PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
+	sb = conv32_scratch_bytes(a.dw, a.dh, C);
+	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)ch.pw, 1 - (int)ch.ph, ch.psf32.as<float>(), ch.pw, ch.ph, gconv,
+	                      a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix,
+	                      sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
+	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, ch.prof_batch.as<int>(), ch.nprof, (unsigned)npix, ch.nt,
+	                          m->d_jac_partials.as<double>(), m->d_jac_tickets.as<unsigned>(), ch.T.as<double>(), s));
+	PF_CUDA(launch_cat_gradient(dev, ch.nprof, ch.T.as<double>(), ch.grad_off.as<int>(), ch.grad.as<double>(), s));
+	PF_CUDA(cudaMemcpyAsync(ch.h_ll.p, ch.ll.p, (size_t)C * 8, cudaMemcpyDeviceToHost, s));
+	PF_CUDA(cudaMemcpyAsync(ch.h_grad.p, ch.grad.p, (size_t)std::max(ch.ngrad, 1) * 8, cudaMemcpyDeviceToHost, s));
+	PF_CUDA(cudaMemcpyAsync(ch.h_ctrl.p, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
+	return PF_OK;
 }
 
 }  // namespace
@@ -2103,7 +2134,6 @@ int pf_catalogue_set_magzero(pf_catalogue *c, double magzero)
 {
 	if (!c) return set_error(PF_E_INVALID, "null catalogue");
 	c->magzero = magzero;
-	c->built = false;
 	return PF_OK;
 }
 
@@ -2190,24 +2220,57 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 		if (G.profiles.empty()) return set_error(PF_E_STATE, "a catalogue galaxy has no profiles");
 	PF_TRY(ensure_stream(c->engine));
 	if (!c->built) PF_TRY(cat_build(c));
-	cudaStream_t s = c->engine->stream;
+	pf_model *m = c->engine;
+	cudaStream_t s = m->stream;
 	PF_CUDA(cudaEventRecord(c->ev[0], s));
+	ModelGeom g;
+	g.magzero = c->magzero;
+	g.sx = g.sy = g.img_sx = g.img_sy = 1;
+	g.offx = g.offy = 0;
+	g.finesampling = 1;
+	PF_CUDA(launch_cat_prologue(c->params.as<ProfileParams>(), c->pad.as<int2>(), c->nprof, g,
+	                            c->dev.as<DevProfile>(), c->fprof.as<FProfile>(), s));
+	std::vector<CatChunk *> todo;
+	for (auto &chp : c->chunks) todo.push_back(chp.get());
+	for (int attempt = 0; attempt < 8 && !todo.empty(); attempt++) {
+		for (CatChunk *ch : todo) PF_TRY(cat_enqueue_chunk(c, *ch));
+		PF_CUDA(cudaStreamSynchronize(s));
+		// every chunk is judged against the capacities it ran with; only then
+		// do the capacities grow (one chunk's growth must not hide another's
+		// overflow)
+		const std::vector<uint32_t> used = m->caps;
+		std::vector<CatChunk *> again;
+		for (CatChunk *ch : todo) {
+			const uint32_t *ctrl = ch->h_ctrl.as<uint32_t>();
+			if (ctrl[MAX_LEVELS] & 2u) return set_error(PF_E_CAPACITY, "recursion deeper than the configured levels");
+			bool over = false;
+			for (int l = 0; l < ch->levels; l++)
+				if (ctrl[l] > used[l]) {
+					over = true;
+					uint64_t want = (uint64_t)ctrl[l] + ctrl[l] / 2 + 1024;
+					if (want > (1ull << 30)) return set_error(PF_E_CAPACITY, "subsampling work queue overflow");
+					m->caps[l] = std::max(m->caps[l], (uint32_t)want);
+				}
+			if (over) again.push_back(ch);
+		}
+		todo.swap(again);
+	}
+	if (!todo.empty()) return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+	PF_CUDA(cudaEventRecord(c->ev[1], s));
+	PF_CUDA(cudaEventSynchronize(c->ev[1]));
 	for (auto &chp : c->chunks) {
-		CatChunk &ch = *chp;
-		PF_TRY(cat_run_chunk(c, ch));
+		const CatChunk &ch = *chp;
 		const double *hl = ch.h_ll.as<double>(), *hg = ch.h_grad.as<double>();
 		for (size_t i = 0; i < ch.members.size(); i++) {
-			const int g = ch.members[i];
-			loglike[g] = hl[i];
+			const int gi = ch.members[i];
+			loglike[gi] = hl[i];
 			if (grad) {
 				int n = 0;
-				for (auto &p : c->gal[g].profiles) n += 6 + shape_count(p.kind);
-				std::memcpy(grad + c->grad_off[g], hg + ch.member_grad_off[i], (size_t)n * 8);
+				for (auto &p : c->gal[gi].profiles) n += 6 + shape_count(p.kind);
+				std::memcpy(grad + c->grad_off[gi], hg + ch.member_grad_off[i], (size_t)n * 8);
 			}
 		}
 	}
-	PF_CUDA(cudaEventRecord(c->ev[1], s));
-	PF_CUDA(cudaEventSynchronize(c->ev[1]));
 	cudaEventElapsedTime(&c->last_ms, c->ev[0], c->ev[1]);
 	cudaGetLastError();
 	return PF_OK;

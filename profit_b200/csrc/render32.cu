@@ -1058,12 +1058,15 @@ cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, c
 // Catalogue batches: every galaxy brings its own profiles, so the prologue
 // reads one parameter record per profile (validated when the galaxy was
 // added) instead of a template plus a value matrix.
-__global__ void k_cat_prologue(const ProfileParams *__restrict__ params, int n, ModelGeom g,
-                               DevProfile *__restrict__ dev, FProfile *__restrict__ fprof)
+// pad[t]: the PSF padding of the bucket that draws profile t.
+__global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const int2 *__restrict__ pad, int n,
+                               ModelGeom g, DevProfile *__restrict__ dev, FProfile *__restrict__ fprof)
 {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n) return;
 	const ProfileParams pp = params[t];
+	g.offx = pad[t].x;
+	g.offy = pad[t].y;
 	DevProfile d;
 	derive_profile(pp, g, d);
 	dev[t] = d;
@@ -1087,10 +1090,10 @@ __global__ void k_cat_gradient(const DevProfile *__restrict__ dev, int n, const 
 	for (int k = 0; k < shape_count(d.kind); k++) out[6 + k] = gradient_from_tangents(G_SHAPE + k, d.axrat, d, Tp);
 }
 
-cudaError_t launch_cat_prologue(const ProfileParams *params, int n, const ModelGeom &g, DevProfile *dev,
-                                FProfile *fprof, cudaStream_t s)
+cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, int n, const ModelGeom &g,
+                                DevProfile *dev, FProfile *fprof, cudaStream_t s)
 {
-	k_cat_prologue<<<(n + 127) / 128, 128, 0, s>>>(params, n, g, dev, fprof);
+	k_cat_prologue<<<(n + 63) / 64, 64, 0, s>>>(params, pad, n, g, dev, fprof);
 	note_launches(1);
 	return cudaGetLastError();
 }
