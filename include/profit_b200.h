@@ -128,9 +128,19 @@ int pf_model_evaluate(pf_model *m, double *image, size_t capacity,
 int pf_model_set_data(pf_model *m, const double *image, const double *sigma,
                       const uint8_t *region, unsigned width, unsigned height);
 
-/* logL = sum over region of log dnorm((image - model)/sigma), the value of
- * profitLikeModel's LL for like.func = "norm". */
+/* logL of profitLikeModel for the model's likelihood function
+ * (pf_model_set_likelihood; "norm" by default: the sum over the region of
+ * log dnorm((image - model)/sigma)). */
 int pf_model_loglike(pf_model *m, double *loglike);
+
+/* The likelihood function, profitLikeModel's like.func with the aliases of
+ * profitParseLikefunc (R/profitUtility.R:99-121): "norm" (default), "chisq",
+ * "t" (dof from the residual variance, R/profitLikeModel.R:281-287), "pois"
+ * (R/profitLikeModel.R:321-327).  It applies to pf_model_loglike, the FD
+ * gradient, pf_model_loglike_grad and its batch form.  "st" (skew-t, whose
+ * parameters profitLikeModel fits with LaplacesDemon) fails with
+ * PF_E_INVALID, as does an unknown name. */
+int pf_model_set_likelihood(pf_model *m, const char *name);
 
 /* Parameters the gradient is taken with respect to.  Each entry names a
  * profile index and one of its double parameters ("xcen", "ycen", "mag",

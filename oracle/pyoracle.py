@@ -356,3 +356,39 @@ def loglike_norm(image: np.ndarray, sigma: np.ndarray, model: np.ndarray,
         rg = r.ctypes.data_as(C.POINTER(C.c_uint8))
     return lib.pfo_loglike_norm(im.ctypes.data_as(_dp), sg.ctypes.data_as(_dp),
                                 md.ctypes.data_as(_dp), rg, im.size)
+
+
+def loglike_other(kind: str, image: np.ndarray, sigma: np.ndarray, model: np.ndarray,
+                  region: Optional[np.ndarray] = None) -> float:
+    """profitLikeModel's chisq, t and pois log-likelihoods (oracle restatement,
+    R/profitLikeModel.R:263-287 and 321-327), in FP64 with compensated sums:
+      chisq: log dchisq(sum x^2, n), x = (image - model)/sigma over the region;
+      t:     sum log dt(x, nu), nu = max(1, 2 v/(v - 1)), v = var(x) (n - 1 denominator);
+      pois:  -sum(m - d log m) after scaling model and image by
+             s = max(|image|/sigma^2) when s lies outside [0.1, 10]."""
+    import math
+    im = np.asarray(image, dtype=np.float64).ravel()
+    sg = np.asarray(sigma, dtype=np.float64).ravel()
+    md = np.asarray(model, dtype=np.float64).ravel()
+    if region is not None:
+        keep = np.asarray(region).ravel().astype(bool)
+        im, sg, md = im[keep], sg[keep], md[keep]
+    if kind == "pois":
+        s = float(np.max(np.abs(im) / np.abs(sg) ** 2))
+        if s < 0.1 or s > 10:
+            md, im = md * s, im * s
+        return -math.fsum(md - im * np.log(md))
+    x = (im - md) / sg
+    n = x.size
+    if kind == "chisq":
+        X2 = math.fsum(x * x)
+        return (n / 2 - 1) * math.log(X2) - X2 / 2 - (n / 2) * math.log(2.0) - math.lgamma(n / 2)
+    if kind == "t":
+        mean = math.fsum(x) / n
+        v = math.fsum((x - mean) ** 2) / (n - 1)
+        nu = math.inf if v == 1 else max(1.0, 2 * v / (v - 1))
+        if math.isinf(nu):
+            return math.fsum(-(0.5 * math.log(2 * math.pi) + 0.5 * x * x))
+        c0 = math.lgamma((nu + 1) / 2) - math.lgamma(nu / 2) - 0.5 * math.log(nu * math.pi)
+        return n * c0 + math.fsum(-0.5 * (nu + 1) * np.log1p(x * x / nu))
+    raise ValueError(kind)

@@ -125,6 +125,7 @@ def _late_bindings(L):
     L.pf_model_set_parameters.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, _dp]
     L.pf_model_loglike_grad_batch.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, C.c_int, _dp, _dp, _dp]
     L.pf_model_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
+    L.pf_model_set_likelihood.argtypes = [C.c_void_p, C.c_char_p]
     vp = C.c_void_p
     L.pf_catalogue_create.argtypes = [C.POINTER(vp)]
     L.pf_catalogue_destroy.argtypes = [vp]
@@ -150,4 +151,4 @@ EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch",
                        "pf_loglike_norm_noalloc", "pf_catalogue_create", "pf_catalogue_destroy",
                        "pf_catalogue_set_magzero", "pf_catalogue_add_galaxy", "pf_catalogue_add_profile",
                        "pf_catalogue_size", "pf_catalogue_gradient_offset", "pf_catalogue_loglike_grad",
-                       "pf_catalogue_last_time")
+                       "pf_catalogue_last_time", "pf_model_set_likelihood")

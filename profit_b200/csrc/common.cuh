@@ -13,6 +13,10 @@ namespace pf {
 // them) and df/dbox.  Models whose profiles need fewer slots store fewer
 // planes (tangent_stride).
 constexpr int NTAN = 12;
+
+// profitLikeModel's like.func (R/profitUtility.R:99-121, without "st").
+enum LikeKind : int { LIKE_NORM = 0, LIKE_CHISQ = 1, LIKE_T = 2, LIKE_POIS = 3 };
+constexpr int LIKE_SCRATCH_PER_IMAGE = 5;  // doubles of launch_like64's stats scratch per image
 constexpr int NTAN_GEOM = 6;
 
 // Tangent slots a profile of this kind fills (geometry, shape, box).

@@ -108,3 +108,13 @@ cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, in
 cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,
                                 cudaStream_t s);
 }  // namespace pf
+
+namespace pf {
+// render64.cu: the likelihood of kind `kind` (LikeKind: norm, chisq, t, pois)
+// for `batch` model images against data with the given batch stride (0:
+// one data image); writes logL per image and, with wseed, the adjoint seed.
+// partials: batch * nparts * 2 double2; stats: batch * LIKE_SCRATCH_PER_IMAGE doubles.
+cudaError_t launch_like64(int kind, const double *model, const double *data, const double *sigma,
+                          const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
+                          int nparts, double *stats, double *out, float *wseed, cudaStream_t s);
+}  // namespace pf

@@ -8,6 +8,7 @@
 // convolved with the normalised PSF, the PSF padding is cropped, the second
 // is added, and finesampled images are summed back down when requested.
 #include <algorithm>
+#include <cctype>
 #include <atomic>
 #include <cmath>
 #include <cstdio>
@@ -331,6 +332,8 @@ struct pf_model {
 	int adjoint_mode = PF_ADJOINT_AUTO;
 	DevBuf d_decisions, d_level_counts;
 	DevBuf d_data, d_sigma, d_region;
+	int like_kind = LIKE_NORM;
+	DevBuf d_likestats;
 	HostBuf h_prof, h_fprof, h_results, h_ctrl;
 	std::vector<uint32_t> caps;
 	bool has_data = false, has_region = false;
@@ -756,6 +759,18 @@ int evaluate64(pf_model *m, Analysis &a)
 // FP32 path with forward tangents and the adjoint reduction
 // ---------------------------------------------------------------------------
 
+// The model's likelihood (pf_model_set_likelihood) of `batch` images against
+// its data, with the adjoint seed when wseed is given.
+int enqueue_like(pf_model *m, const double *model64, int nout, int batch, double *out, float *wseed, cudaStream_t s)
+{
+	PF_CUDA(ensure(m->d_partials, (size_t)NPARTS * batch * 2 * sizeof(double2)));
+	PF_CUDA(ensure(m->d_likestats, (size_t)batch * LIKE_SCRATCH_PER_IMAGE * 8));
+	PF_CUDA(launch_like64(m->like_kind, model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
+	                      m->has_region ? m->d_region.as<uint8_t>() : nullptr, nout, batch, 0,
+	                      m->d_partials.as<double2>(), NPARTS, m->d_likestats.as<double>(), out, wseed, s));
+	return PF_OK;
+}
+
 // Tangent planes kept per radial profile: the most any profile of the model
 // fills (9 for Sersic and Moffat models, up to 12 with core-Sersic).
 int tangent_stride(const pf_model *m)
@@ -814,15 +829,12 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	(void)model;
 	PF_CUDA(record_event(m->ev[2], m->stream));
 	if (!m->has_data) return PF_OK;
-	PF_CUDA(ensure(m->d_partials, NPARTS * sizeof(double2)));
 	float *wseed = nullptr;
 	if (want_grad) {
 		PF_CUDA(ensure(m->d_wseed, nout * 4));
 		wseed = m->d_wseed.as<float>();
 	}
-	PF_CUDA(launch_loglike64_seed(model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
-	                              m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout,
-	                              m->d_partials.as<double2>(), NPARTS, d_out + ResultLayout::LL, wseed, m->stream));
+	PF_TRY(enqueue_like(m, model64, (int)nout, 1, d_out + ResultLayout::LL, wseed, m->stream));
 	if (want_grad) {
 		PF_CUDA(ensure(m->d_gconv, npix * 4));
 		PF_CUDA(ensure(m->d_gplain, npix * 4));
@@ -872,12 +884,12 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 {
 	std::vector<uint64_t> s = {a.dw, a.dh, a.ow, a.oh, (uint64_t)a.n_profiles, (uint64_t)a.levels, a.conv,
 	                           (uint64_t)m->conv_kind, (uint64_t)m->precision, m->psf_w, m->psf_h, m->has_data,
-	                           m->has_region, want_grad};
+	                           m->has_region, want_grad, (uint64_t)m->like_kind};
 	for (int l = 0; l < a.levels; l++) s.push_back(((uint64_t)q.off[l] << 32) | q.cap[l]);
 	const DevBuf *bufs[] = {&m->d_fprof, &m->d_prof_begin, &m->d_prof_batch, &m->d_conv32, &m->d_plain32,
 	                        &m->d_model64, &m->d_conv64, &m->d_plain64, &m->d_jac, &m->d_gconv, &m->d_gplain,
 	                        &m->d_wseed, &m->d_items, &m->d_ctrl, &m->d_partials, &m->d_results, &m->d_psf32,
-	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region, &m->d_convsplit, &m->d_jac_partials, &m->d_jac_tickets};
+	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region, &m->d_convsplit, &m->d_jac_partials, &m->d_jac_tickets, &m->d_likestats};
 	for (auto *b : bufs) s.push_back((uint64_t)(uintptr_t)b->p);
 	s.push_back((uint64_t)(uintptr_t)m->h_fprof.p);
 	s.push_back((uint64_t)(uintptr_t)m->h_results.p);
@@ -1059,9 +1071,7 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	PF_CUDA(record_event(m->ev[1], s));
 	PF_TRY(forward_conv32(m, a, conv, plain, model64, C));
 	PF_CUDA(record_event(m->ev[2], s));
-	PF_CUDA(launch_loglike64_batch(model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
-	                               m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)nout, C, 0,
-	                               m->d_partials.as<double2>(), NPARTS, bs.d_ll.as<double>(), wseed, s));
+	PF_TRY(enqueue_like(m, model64, (int)nout, C, bs.d_ll.as<double>(), wseed, s));
 	PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
 	if (a.conv && m->conv_kind != CONV_NULL)
 		PF_TRY(adjoint_conv32(m, a, wseed, gconv, C));
@@ -1636,11 +1646,9 @@ int pf_model_loglike(pf_model *m, double *loglike)
 		PF_TRY(evaluate64(m, a));
 		if (m->data_w != a.ow || m->data_h != a.oh)
 			return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
-		PF_CUDA(ensure(m->d_partials, NPARTS * sizeof(double2)));
 		PF_CUDA(ensure(m->d_results, 64));
-		PF_CUDA(launch_loglike64(m->d_model64.as<double>(), m->d_data.as<double>(), m->d_sigma.as<double>(),
-		                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)(a.ow * a.oh),
-		                         m->d_partials.as<double2>(), NPARTS, m->d_results.as<double>(), m->stream));
+		PF_TRY(enqueue_like(m, m->d_model64.as<double>(), (int)(a.ow * a.oh), 1, m->d_results.as<double>(), nullptr,
+		                    m->stream));
 		PF_CUDA(cudaMemcpyAsync(loglike, m->d_results.p, 8, cudaMemcpyDeviceToHost, m->stream));
 		PF_CUDA(cudaStreamSynchronize(m->stream));
 		return PF_OK;
@@ -1730,9 +1738,8 @@ int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_para
 			QueueSet q;
 			PF_TRY(prepare_queue(m, a, npix * a.n_profiles, q, nullptr, nullptr));
 			PF_TRY(run_plain64(m, a, m->d_prof.as<DevProfile>() + (size_t)e * a.n_profiles, q));
-			PF_CUDA(launch_loglike64(m->d_model64.as<double>(), m->d_data.as<double>(), m->d_sigma.as<double>(),
-			                         m->has_region ? m->d_region.as<uint8_t>() : nullptr, (int)(a.ow * a.oh),
-			                         m->d_partials.as<double2>(), NPARTS, m->d_results.as<double>() + e, m->stream));
+			PF_TRY(enqueue_like(m, m->d_model64.as<double>(), (int)(a.ow * a.oh), 1, m->d_results.as<double>() + e,
+			                    nullptr, m->stream));
 			PF_CUDA(cudaMemcpyAsync(hctrl + (size_t)e * CTRL_WORDS, m->d_ctrl.p, CTRL_WORDS * 4,
 			                        cudaMemcpyDeviceToHost, m->stream));
 		}
@@ -1755,6 +1762,25 @@ int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_para
 		return PF_OK;
 	}
 	return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+}
+
+int pf_model_set_likelihood(pf_model *m, const char *name)
+{
+	if (!m || !name) return set_error(PF_E_INVALID, "null argument");
+	std::string f(name);
+	for (auto &ch : f) ch = (char)std::tolower((unsigned char)ch);
+	int kind;
+	if (f == "norm" || f == "normal") kind = LIKE_NORM;
+	else if (f == "chisq" || f == "chi-sq") kind = LIKE_CHISQ;
+	else if (f == "t" || f == "student" || f == "student-t") kind = LIKE_T;
+	else if (f == "pois" || f == "poisson" || f == "cash" || f == "c") kind = LIKE_POIS;
+	else if (f == "st" || f == "skewt" || f == "skew-t")
+		return set_error(PF_E_INVALID, "the skew-t likelihood (LaplacesDemon fit of its parameters) is not available");
+	else
+		return set_error(PF_E_INVALID, std::string("Error: unknown likelihood function: '") + f + "'");
+	if (kind != m->like_kind) drop_graph(m);
+	m->like_kind = kind;
+	return PF_OK;
 }
 
 int pf_model_set_adjoint_mode(pf_model *m, int mode)

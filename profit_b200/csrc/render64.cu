@@ -22,6 +22,7 @@
 #include "conv.cuh"
 #include "launch.h"
 #include "like.cuh"
+#include "like_kinds.cuh"
 
 namespace pf {
 
@@ -377,6 +378,54 @@ cudaError_t launch_widen(const float *src, double *dst, size_t n, cudaStream_t s
 {
 	k_widen<<<148 * 4, 256, 0, s>>>(src, dst, n);
 	note_launches(1);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_like64(int kind, const double *model, const double *data, const double *sigma,
+                          const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
+                          int nparts, double *stats, double *out, float *wseed, cudaStream_t s)
+{
+	const dim3 grid(nparts, batch);
+	if (kind == LIKE_NORM) {
+		k_loglike_partial<double><<<grid, 256, 0, s>>>(model, data, sigma, region, n, partials, wseed,
+		                                               data_batch_stride);
+		k_loglike_final<<<batch, 256, 0, s>>>(partials, nparts, out);
+		note_launches(2);
+		return cudaGetLastError();
+	}
+	double *p1 = reinterpret_cast<double *>(partials);
+	double *coef = stats + (size_t)batch * LIKE_STATS;
+	switch (kind) {
+	case LIKE_CHISQ:
+		k_like_stats<LIKE_CHISQ><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, p1);
+		k_like_stats_final<<<batch, 32, 0, s>>>(p1, nparts, stats);
+		k_like_terms<LIKE_CHISQ><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats,
+		                                               partials, wseed);
+		k_like_terms_final<LIKE_CHISQ><<<batch, 32, 0, s>>>(partials, nparts, stats, out, coef);
+		note_launches(4);
+		break;
+	case LIKE_T:
+		k_like_stats<LIKE_T><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, p1);
+		k_like_stats_final<<<batch, 32, 0, s>>>(p1, nparts, stats);
+		k_like_terms<LIKE_T><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats, partials,
+		                                           nullptr);
+		k_like_terms_final<LIKE_T><<<batch, 32, 0, s>>>(partials, nparts, stats, out, coef);
+		note_launches(4);
+		if (wseed) {
+			k_like_t_seed<<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats, coef, wseed);
+			note_launches(1);
+		}
+		break;
+	case LIKE_POIS:
+		k_like_stats<LIKE_POIS><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, p1);
+		k_like_stats_final<<<batch, 32, 0, s>>>(p1, nparts, stats);
+		k_like_terms<LIKE_POIS><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats,
+		                                              partials, wseed);
+		k_like_terms_final<LIKE_POIS><<<batch, 32, 0, s>>>(partials, nparts, stats, out, coef);
+		note_launches(4);
+		break;
+	default: return cudaErrorInvalidValue;
+	}
 	return cudaGetLastError();
 }
 

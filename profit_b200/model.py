@@ -130,6 +130,10 @@ class Model:
     def set_precision(self, precision: int):
         check(lib().pf_model_set_precision(self._h, int(precision)))
 
+    def set_likelihood(self, name: str):
+        """profitLikeModel's like.func: "norm", "chisq", "t" or "pois" (and their aliases)."""
+        check(lib().pf_model_set_likelihood(self._h, name.encode()))
+
     def set_adjoint_mode(self, mode: int):
         """PF_ADJOINT_AUTO / PF_ADJOINT_STORE / PF_ADJOINT_RECOMPUTE (see profit_b200.h)."""
         check(lib().pf_model_set_adjoint_mode(self._h, int(mode)))

@@ -376,3 +376,54 @@ def test_shape_gradients_of_every_profile_kind(kind):
     spread = 2 * np.abs(g6 - g5) / scale
     assert np.all(err <= np.maximum(1e-5, spread)), list(zip(refs, g6, g5, g))
     assert np.sum(spread > 1e-5) <= 2
+
+
+@pytest.mark.parametrize("kind", ["chisq", "t", "pois"])
+def test_other_likelihoods_and_their_gradients(kind):
+    """profitLikeModel's chisq, t (dof from the residual variance) and pois
+    likelihoods: the FP64 value against the oracle's restatement, the FP32
+    value against FP64, and the FP32 adjoint gradient (through the t dof as
+    well) against FP64 central differences."""
+    from oracle.pyoracle import loglike_other
+    wl = W.single_sersic(seed_tag=13, width=90, height=80, psf_size=15)
+    wl["magzero"] = 25.0
+    wl["profiles"] = wl["profiles"] + [("sky", dict(bg=5.0))]
+    m64 = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = m64.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    region = (np.random.Generator(np.random.PCG64(8)).uniform(size=image.shape) < 0.9).astype(np.uint8)
+    w2 = W.perturbed(wl, seed=9, scale=0.02)
+    m = W.configure(Model(wl["width"], wl["height"]), w2)
+    m.set_data(image, sigma, region)
+    m.set_likelihood(kind)
+    ll64 = m.loglike()
+    model_img, _ = m.evaluate()
+    assert ll64 == pytest.approx(loglike_other(kind, image, sigma, model_img, region), rel=1e-11)
+    refs = w2["grad"]
+    _, g6 = m.loglike_grad_fd(refs, rel_step=1e-6)
+    _, g5 = m.loglike_grad_fd(refs, rel_step=1e-5)
+    m.set_precision(PF_FP32)
+    ll32, g = m.loglike_grad(refs)
+    assert ll32 == pytest.approx(ll64, rel=1e-5, abs=1e-6 * abs(ll64) + 1e-6)
+    scale = np.max(np.abs(g6))
+    err = np.minimum(np.abs(g - g6), np.abs(g - g5)) / scale
+    spread = 2 * np.abs(g6 - g5) / scale
+    assert np.all(err <= np.maximum(1e-5, spread)), list(zip(refs, g6, g5, g))
+    if kind == "t":
+        vals = np.array([[p["profiles"][i][1][k] for (i, k) in refs] for p in
+                         [W.perturbed(wl, seed=30 + s, scale=0.02) for s in range(3)]])
+        ll_b, g_b = m.loglike_grad_batch(refs, vals)
+        for s in range(3):
+            m.set_parameters(refs, vals[s])
+            l1, g1 = m.loglike_grad(refs)
+            assert ll_b[s] == pytest.approx(l1, rel=1e-7)
+            np.testing.assert_allclose(g_b[s], g1, rtol=1e-5, atol=1e-6 * np.max(np.abs(g1)))
+
+
+def test_unknown_and_skew_t_likelihoods_are_rejected():
+    m = Model(10, 10)
+    with pytest.raises(InvalidParameter):
+        m.set_likelihood("st")
+    with pytest.raises(InvalidParameter):
+        m.set_likelihood("nonsense")
+    m.set_likelihood("Student-T")  # aliases and case as profitParseLikefunc

@@ -181,3 +181,31 @@ def test_fft_geometry_restatement_matches_numpy_fft():
         pad = 3
         expect = full[pad:pad + h, pad:pad + w]
         assert np.max(np.abs(got - expect)) <= 1e-12 * np.max(np.abs(expect))
+
+
+@pytest.mark.parametrize("kind", ["chisq", "t", "pois"])
+def test_other_likelihoods_restatement_matches_scipy(kind):
+    """The oracle's chisq / t / pois likelihoods against scipy.stats' densities
+    (the same closed forms R's dchisq and dt evaluate by saddle-point
+    expansions)."""
+    import scipy.stats as st
+    from oracle.pyoracle import loglike_other
+    r = np.random.Generator(np.random.PCG64(3))
+    model = r.uniform(5, 50, size=(30, 40))
+    sigma = r.uniform(0.5, 2, size=model.shape)
+    image = model + r.standard_t(5, size=model.shape) * sigma * 1.3
+    region = r.uniform(size=model.shape) < 0.9
+    got = loglike_other(kind, image, sigma, model, region)
+    x = ((image - model) / sigma)[region]
+    if kind == "chisq":
+        want = st.chi2.logpdf(np.sum(x * x), x.size)
+    elif kind == "t":
+        v = np.var(x, ddof=1)
+        want = np.sum(st.t.logpdf(x, max(1.0, 2 * v / (v - 1))))
+    else:
+        im, md, sg = image[region], model[region], sigma[region]
+        s = np.max(np.abs(im) / sg ** 2)
+        if s < 0.1 or s > 10:
+            im, md = im * s, md * s
+        want = -np.sum(md - im * np.log(md))
+    assert got == pytest.approx(want, rel=1e-12)
