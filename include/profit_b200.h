@@ -101,6 +101,16 @@ int pf_model_set_image_pixel_scale(pf_model *m, double scale_x, double scale_y);
 int pf_model_set_psf_pixel_scale(pf_model *m, double scale_x, double scale_y);
 int pf_model_set_finesampling(pf_model *m, unsigned finesampling);
 int pf_model_set_return_finesampled(pf_model *m, int value);
+/* Calculation mask, like Model::set_mask / set_adjust_mask (model.h:196-214):
+ * width x height bytes, nonzero = compute the pixel; NULL clears it.  With
+ * adjust_mask (the default) the mask has the model's dimensions and is
+ * upsampled, padded and dilated by psf/2 for the drawing, the PSF padding is
+ * left out when the mask keeps psf/2 pixels clear of the edges, and the
+ * result is zeroed outside the mask (model.cpp:152-183, 230-246, 330-334).
+ * Without it the mask must have the drawing dimensions.  Plain (FP64) form
+ * only for now. */
+int pf_model_set_mask(pf_model *m, const uint8_t *mask, unsigned width, unsigned height);
+int pf_model_set_adjust_mask(pf_model *m, int value);
 /* Only crop = true is supported (ProFit's returncrop default). */
 int pf_model_set_crop(pf_model *m, int value);
 /* "brute" (default, like Model::ensure_convolver, model.cpp:144-150),

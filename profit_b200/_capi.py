@@ -126,6 +126,8 @@ def _late_bindings(L):
     L.pf_model_loglike_grad_batch.argtypes = [C.c_void_p, C.POINTER(pf_param_ref), C.c_int, C.c_int, _dp, _dp, _dp]
     L.pf_model_set_adjoint_mode.argtypes = [C.c_void_p, C.c_int]
     L.pf_model_set_likelihood.argtypes = [C.c_void_p, C.c_char_p]
+    L.pf_model_set_mask.argtypes = [C.c_void_p, C.POINTER(C.c_uint8), C.c_uint, C.c_uint]
+    L.pf_model_set_adjust_mask.argtypes = [C.c_void_p, C.c_int]
     vp = C.c_void_p
     L.pf_catalogue_create.argtypes = [C.POINTER(vp)]
     L.pf_catalogue_destroy.argtypes = [vp]
@@ -151,4 +153,5 @@ EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch",
                        "pf_loglike_norm_noalloc", "pf_catalogue_create", "pf_catalogue_destroy",
                        "pf_catalogue_set_magzero", "pf_catalogue_add_galaxy", "pf_catalogue_add_profile",
                        "pf_catalogue_size", "pf_catalogue_gradient_offset", "pf_catalogue_loglike_grad",
-                       "pf_catalogue_last_time", "pf_model_set_likelihood")
+                       "pf_catalogue_last_time", "pf_model_set_likelihood", "pf_model_set_mask",
+                       "pf_model_set_adjust_mask")

@@ -15,8 +15,15 @@ void note_launches(int n);
 int report_error(int code, const char *msg);
 
 // render64.cu
+// mask: optional drawing-size calculation mask (radial and sky profiles skip its zeros)
 cudaError_t launch_pixels64(const DevProfile *profiles, int n_profiles, unsigned width, unsigned height, double sx,
-                            double sy, double *img_conv, double *img_plain, const QueueSet &q, cudaStream_t s);
+                            double sy, double *img_conv, double *img_plain, const uint8_t *mask, const QueueSet &q,
+                            cudaStream_t s);
+// out(i, j) = plain(i + ox, j + oy) where the drawing mask is 0 (masked convolution)
+cudaError_t launch_mask_select64(double *out, unsigned ow, unsigned oh, const double *plain, const uint8_t *mask,
+                                 unsigned dw, unsigned ox, unsigned oy, cudaStream_t s);
+// out &= mask
+cudaError_t launch_mask_and64(double *out, const uint8_t *mask, size_t n, cudaStream_t s);
 cudaError_t launch_levels64(const DevProfile *profiles, int n_levels, double *img_conv, double *img_plain,
                             const QueueSet &q, cudaStream_t s);
 cudaError_t launch_count_decisions(const QueueSet &q, int n_levels, size_t npix, cudaStream_t s);

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -293,6 +294,11 @@ struct Analysis {
 	unsigned ow, oh;              // output dims
 	int levels;
 	int n_profiles;
+	// calculation mask (Model::analyze_expansion_requirements, model.cpp:152-183)
+	bool mask = false;          // a drawing-size mask is in effect
+	bool mask_adjusted = false; // it was built from the user's mask (adjust_mask)
+	bool mask_conv = false;     // the convolution is masked by it
+	bool mask_psf_pad = false;  // the user's mask needed the PSF padding
 };
 
 // Per-evaluation device results: [0] logL, [1..] tangent reductions.
@@ -332,6 +338,12 @@ struct pf_model {
 	int adjoint_mode = PF_ADJOINT_AUTO;
 	DevBuf d_decisions, d_level_counts;
 	DevBuf d_data, d_sigma, d_region;
+	// calculation mask (Model::set_mask / set_adjust_mask, model.h:196-214)
+	std::vector<uint8_t> mask;
+	unsigned mask_w = 0, mask_h = 0;
+	bool adjust_mask = true;
+	std::vector<uint64_t> mask_key;  // what the device masks were built for
+	DevBuf d_mask_draw, d_mask_out;
 	int like_kind = LIKE_NORM;
 	DevBuf d_likestats;
 	HostBuf h_prof, h_fprof, h_results, h_ctrl;
@@ -392,8 +404,40 @@ int analyze(pf_model *m, Analysis &a)
 		}
 	}
 	if (m->profiles.size() > 65535) return set_error(PF_E_INVALID, "too many profiles");
-	a.padx = a.conv ? m->psf_w / 2 : 0;
-	a.pady = a.conv ? m->psf_h / 2 : 0;
+	const bool has_mask = !m->mask.empty();
+	if (has_mask && m->adjust_mask && (m->mask_w != m->width || m->mask_h != m->height))
+		return set_error(PF_E_INVALID, "Mask dimensions != model dimensions");
+	bool pad = a.conv;
+	a.mask = has_mask;
+	a.mask_adjusted = a.mask_conv = a.mask_psf_pad = false;
+	if (has_mask && !m->adjust_mask) {
+		// the mask is given at drawing size: padding iff it is larger than the image
+		pad = m->mask_w > m->width * m->fs && m->mask_h > m->height * m->fs;
+	}
+	else if (has_mask && a.conv) {
+		// no padding when the mask keeps psf/2 pixels clear of every edge
+		unsigned lbx = m->mask_w, lby = m->mask_h, ubx = 0, uby = 0;
+		bool any = false;
+		for (unsigned j = 0; j < m->mask_h; j++)
+			for (unsigned i = 0; i < m->mask_w; i++)
+				if (m->mask[i + (size_t)j * m->mask_w]) {
+					lbx = std::min(lbx, i);
+					lby = std::min(lby, j);
+					ubx = std::max(ubx, i + 1);
+					uby = std::max(uby, j + 1);
+					any = true;
+				}
+		if (!any) lbx = lby = ubx = uby = 0;
+		const unsigned fs = m->fs, nx = m->psf_w / 2, ny = m->psf_h / 2;
+		const unsigned low_x = lbx * fs, low_y = lby * fs;
+		const unsigned up_x = m->mask_w * fs - ubx * fs, up_y = m->mask_h * fs - uby * fs;
+		pad = !(low_x >= nx && low_y >= ny) || !(up_x >= nx && up_y >= ny);
+		a.mask_conv = true;
+		a.mask_psf_pad = pad;
+	}
+	if (has_mask && m->adjust_mask) a.mask_adjusted = a.mask_conv || a.mask_psf_pad || m->fs > 1;
+	a.padx = pad ? m->psf_w / 2 : 0;
+	a.pady = pad ? m->psf_h / 2 : 0;
 	a.cw = m->width * m->fs;
 	a.ch = m->height * m->fs;
 	a.dw = a.cw + 2 * a.padx;
@@ -408,6 +452,77 @@ int analyze(pf_model *m, Analysis &a)
 		a.oh = a.ch;
 	}
 	a.n_profiles = (int)m->profiles.size();
+	if (has_mask && !m->adjust_mask && (m->mask_w != a.dw || m->mask_h != a.dh))
+		return set_error(PF_E_INVALID, "Mask dimensions != drawing dimensions: " + std::to_string(m->mask_w) + "x" +
+		                                   std::to_string(m->mask_h) + " != " + std::to_string(a.dw) + "x" +
+		                                   std::to_string(a.dh));
+	return PF_OK;
+}
+
+// The drawing-size mask the profiles and the convolver see (Model::adjust,
+// model.cpp:230-246): the user's mask upsampled by the finesampling factor,
+// placed inside the PSF padding, and dilated by psf/2 pixels when the
+// convolution is masked (Mask::expand_by, image.cpp:113-157, a box dilation,
+// done here as a row pass then a column pass).  Without adjust_mask the
+// user's mask is used as it is.  Also uploads the user's mask for the final
+// image &= mask.  Rebuilt only when its inputs change.
+int upload_masks(pf_model *m, const Analysis &a)
+{
+	if (!a.mask) return PF_OK;
+	std::vector<uint64_t> key = {m->mask_w, m->mask_h, m->adjust_mask, m->fs, m->psf_w, m->psf_h, a.dw, a.dh,
+	                             a.mask_conv, a.mask_psf_pad, (uint64_t)std::hash<std::string>{}(
+	                                 std::string(m->mask.begin(), m->mask.end()))};
+	if (key == m->mask_key && m->d_mask_draw.p) return PF_OK;
+	std::vector<uint8_t> draw;
+	if (!m->adjust_mask) {
+		draw = m->mask;
+	}
+	else {
+		const unsigned fs = m->fs;
+		draw.assign((size_t)a.dw * a.dh, 0);
+		for (unsigned j = 0; j < m->mask_h * fs; j++)
+			for (unsigned i = 0; i < m->mask_w * fs; i++)
+				draw[(i + a.padx) + (size_t)(j + a.pady) * a.dw] = m->mask[i / fs + (size_t)(j / fs) * m->mask_w] ? 1 : 0;
+		if (a.mask_conv) {
+			const unsigned px = m->psf_w / 2, py = m->psf_h / 2;
+			std::vector<uint8_t> rows(draw.size(), 0);
+			for (unsigned j = 0; j < a.dh; j++) {
+				const uint8_t *in = &draw[(size_t)j * a.dw];
+				uint8_t *out = &rows[(size_t)j * a.dw];
+				int last = -1;  // last set column seen so far
+				std::vector<int> next(a.dw + 1, -1);
+				int nx = -1;
+				for (int i = (int)a.dw - 1; i >= 0; i--) {
+					if (in[i]) nx = i;
+					next[i] = nx;
+				}
+				for (unsigned i = 0; i < a.dw; i++) {
+					if (in[i]) last = (int)i;
+					bool hit = (last >= 0 && (int)i - last <= (int)px) || (next[i] >= 0 && next[i] - (int)i <= (int)px);
+					out[i] = hit;
+				}
+			}
+			for (unsigned i = 0; i < a.dw; i++) {
+				int last = -1;
+				std::vector<int> next(a.dh + 1, -1);
+				int ny = -1;
+				for (int j = (int)a.dh - 1; j >= 0; j--) {
+					if (rows[i + (size_t)j * a.dw]) ny = j;
+					next[j] = ny;
+				}
+				for (unsigned j = 0; j < a.dh; j++) {
+					if (rows[i + (size_t)j * a.dw]) last = (int)j;
+					bool hit = (last >= 0 && (int)j - last <= (int)py) || (next[j] >= 0 && next[j] - (int)j <= (int)py);
+					draw[i + (size_t)j * a.dw] = hit;
+				}
+			}
+		}
+	}
+	PF_CUDA(ensure(m->d_mask_draw, draw.size()));
+	PF_CUDA(cudaMemcpy(m->d_mask_draw.p, draw.data(), draw.size(), cudaMemcpyHostToDevice));
+	PF_CUDA(ensure(m->d_mask_out, m->mask.size()));
+	PF_CUDA(cudaMemcpy(m->d_mask_out.p, m->mask.data(), m->mask.size(), cudaMemcpyHostToDevice));
+	m->mask_key = key;
 	return PF_OK;
 }
 
@@ -660,7 +775,10 @@ int run_plain64(pf_model *m, const Analysis &a, const DevProfile *dprof, QueueSe
 	PF_CUDA(ensure(m->d_plain64, npix * 8));
 	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
 	double *conv = m->d_conv64.as<double>(), *plain = m->d_plain64.as<double>();
-	PF_CUDA(launch_pixels64(dprof, a.n_profiles, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain, q, m->stream));
+	PF_TRY(upload_masks(m, a));
+	const uint8_t *mask = a.mask ? m->d_mask_draw.as<uint8_t>() : nullptr;
+	PF_CUDA(launch_pixels64(dprof, a.n_profiles, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain, mask, q,
+	                        m->stream));
 	for (int p = 0; p < a.n_profiles; p++) {
 		if (m->profiles[p].kind == PK_PSF) {
 			PF_CUDA(launch_psf_stamp64(dprof, p, m->d_psf64.as<double>(), m->psf_w, m->psf_h, m->psf_sx, m->psf_sy,
@@ -683,17 +801,28 @@ int run_plain64(pf_model *m, const Analysis &a, const DevProfile *dprof, QueueSe
 		note_launches(3);
 	}
 	else if (a.conv && m->conv_kind != CONV_NULL) {
-		PF_CUDA(launch_conv64(conv, a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w, m->psf_h, model, a.cw,
+		// output (i, j) is drawing pixel (i + padx, j + pady); its window starts
+		// psf/2 before that (0 with the usual padding, -psf/2 when a mask let the
+		// padding go)
+		const int ox = (int)a.padx - (int)(m->psf_w / 2), oy = (int)a.pady - (int)(m->psf_h / 2);
+		PF_CUDA(launch_conv64(conv, a.dw, a.dh, ox, oy, m->d_psfrev64.as<double>(), m->psf_w, m->psf_h, model, a.cw,
 		                      a.ch, plain, a.dw, a.padx, a.pady, m->stream));
 	}
 	else {
 		PF_CUDA(launch_crop64(conv, a.dw, a.padx, a.pady, model, a.cw, a.ch, plain, m->stream));
 	}
+	if (a.conv && a.mask && m->conv_kind != CONV_NULL && (a.mask_conv || !m->adjust_mask))
+		PF_CUDA(launch_mask_select64(model, a.cw, a.ch, plain, m->d_mask_draw.as<uint8_t>(), a.dw, a.padx, a.pady,
+		                             m->stream));
 	if (a.ow != a.cw || a.oh != a.ch) {
 		// finesampled output summed down (model.cpp:326-329); reuse conv as scratch
 		PF_CUDA(cudaMemcpyAsync(conv, model, (size_t)a.cw * a.ch * 8, cudaMemcpyDeviceToDevice, m->stream));
 		PF_CUDA(launch_downsample64(conv, a.cw, a.ch, m->fs, model, a.ow, a.oh, m->stream));
 	}
+	// image &= mask when the mask was adjusted (model.cpp:330-334); the user's
+	// mask has the output's size unless the finesampled image is returned
+	if (a.mask_adjusted && a.ow == m->mask_w && a.oh == m->mask_h)
+		PF_CUDA(launch_mask_and64(model, m->d_mask_out.as<uint8_t>(), (size_t)a.ow * a.oh, m->stream));
 	PF_CUDA(record_event(m->ev[2], m->stream));
 	return PF_OK;
 }
@@ -915,6 +1044,7 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 	PF_TRY(ensure_stream(m));
 	PF_TRY(analyze(m, a));
 	if (m->fs != 1) return set_error(PF_E_INVALID, "the FP32 path does not support finesampling yet");
+	if (!m->mask.empty()) return set_error(PF_E_INVALID, "the FP32 path does not support calculation masks yet");
 	for (auto &p : m->profiles)
 		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
 	if (m->has_data && (m->data_w != a.ow || m->data_h != a.oh))
@@ -1105,6 +1235,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	Analysis a;
 	PF_TRY(analyze(m, a));
 	if (m->fs != 1) return set_error(PF_E_INVALID, "the FP32 path does not support finesampling yet");
+	if (!m->mask.empty()) return set_error(PF_E_INVALID, "the FP32 path does not support calculation masks yet");
 	for (auto &p : m->profiles)
 		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
 	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
@@ -1548,6 +1679,28 @@ int pf_model_set_return_finesampled(pf_model *m, int value)
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");
 	m->return_fine = value != 0;
+	return PF_OK;
+}
+
+int pf_model_set_mask(pf_model *m, const uint8_t *mask, unsigned width, unsigned height)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (!mask || width == 0 || height == 0) {
+		m->mask.clear();
+		m->mask_w = m->mask_h = 0;
+		return PF_OK;
+	}
+	m->mask.assign(mask, mask + (size_t)width * height);
+	for (auto &v : m->mask) v = v ? 1 : 0;
+	m->mask_w = width;
+	m->mask_h = height;
+	return PF_OK;
+}
+
+int pf_model_set_adjust_mask(pf_model *m, int value)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->adjust_mask = value != 0;
 	return PF_OK;
 }
 

@@ -26,14 +26,21 @@
 
 namespace pf {
 
+// mask (optional, drawing size): radial and sky profiles skip the pixels it
+// leaves out (radial.cpp:306, sky.cpp:56-58); psf profiles ignore it.
 __global__ void k_pixels64(const DevProfile *__restrict__ profiles, int n_profiles, unsigned width,
                            unsigned height, double sx, double sy, double *__restrict__ img_conv,
-                           double *__restrict__ img_plain, QueueSet q)
+                           double *__restrict__ img_plain, const uint8_t *__restrict__ mask, QueueSet q)
 {
 	unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
 	unsigned j = blockIdx.y * blockDim.y + threadIdx.y;
 	if (i >= width || j >= height) return;
 	const uint32_t pix = i + j * width;
+	if (mask && !mask[pix]) {
+		img_conv[pix] = 0.0;
+		img_plain[pix] = 0.0;
+		return;
+	}
 	double acc[2] = {0.0, 0.0};
 	double half_xbin = sx / 2., half_ybin = sy / 2.;
 	// radial.cpp:313-314 computes y with scale.x and x with scale.y
@@ -287,10 +294,46 @@ __global__ void k_downsample64(const double *__restrict__ src, unsigned sw, unsi
 static inline unsigned cdiv(unsigned a, unsigned b) { return (a + b - 1) / b; }
 
 cudaError_t launch_pixels64(const DevProfile *profiles, int n_profiles, unsigned width, unsigned height, double sx,
-                            double sy, double *img_conv, double *img_plain, const QueueSet &q, cudaStream_t s)
+                            double sy, double *img_conv, double *img_plain, const uint8_t *mask, const QueueSet &q,
+                            cudaStream_t s)
 {
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8));
-	k_pixels64<<<grid, block, 0, s>>>(profiles, n_profiles, width, height, sx, sy, img_conv, img_plain, q);
+	k_pixels64<<<grid, block, 0, s>>>(profiles, n_profiles, width, height, sx, sy, img_conv, img_plain, mask, q);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+// Masked convolution (convolve.cpp:185, model.cpp:372-376): an output pixel
+// the drawing mask leaves out gets no convolved flux, only the unconvolved
+// image, out(i, j) = plain(i + ox, j + oy) there.
+__global__ void k_mask_select64(double *__restrict__ out, unsigned ow, unsigned oh, const double *__restrict__ plain,
+                                const uint8_t *__restrict__ mask, unsigned dw, unsigned ox, unsigned oy)
+{
+	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
+	if (i >= ow || j >= oh) return;
+	const size_t d = (i + ox) + (size_t)(j + oy) * dw;
+	if (!mask[d]) out[i + (size_t)j * ow] = plain[d];
+}
+
+// image &= mask (image.cpp:369-381).
+__global__ void k_mask_and64(double *__restrict__ out, const uint8_t *__restrict__ mask, size_t n)
+{
+	for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x)
+		if (!mask[t]) out[t] = 0.0;
+}
+
+cudaError_t launch_mask_select64(double *out, unsigned ow, unsigned oh, const double *plain, const uint8_t *mask,
+                                 unsigned dw, unsigned ox, unsigned oy, cudaStream_t s)
+{
+	dim3 block(32, 8), grid(cdiv(ow, 32), cdiv(oh, 8));
+	k_mask_select64<<<grid, block, 0, s>>>(out, ow, oh, plain, mask, dw, ox, oy);
+	note_launches(1);
+	return cudaGetLastError();
+}
+
+cudaError_t launch_mask_and64(double *out, const uint8_t *mask, size_t n, cudaStream_t s)
+{
+	k_mask_and64<<<148 * 4, 256, 0, s>>>(out, mask, n);
 	note_launches(1);
 	return cudaGetLastError();
 }

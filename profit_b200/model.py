@@ -130,6 +130,18 @@ class Model:
     def set_precision(self, precision: int):
         check(lib().pf_model_set_precision(self._h, int(precision)))
 
+    def set_mask(self, mask: Optional[np.ndarray], adjust: bool = True):
+        """Model::set_mask and set_adjust_mask: mask[height, width], nonzero = compute."""
+        L = lib()
+        if mask is None:
+            check(L.pf_model_set_mask(self._h, None, 0, 0))
+        else:
+            mk = np.ascontiguousarray(mask, dtype=np.uint8)
+            self._mask = mk
+            h, w = mk.shape
+            check(L.pf_model_set_mask(self._h, mk.ctypes.data_as(C.POINTER(C.c_uint8)), w, h))
+        check(L.pf_model_set_adjust_mask(self._h, int(bool(adjust))))
+
     def set_likelihood(self, name: str):
         """profitLikeModel's like.func: "norm", "chisq", "t" or "pois" (and their aliases)."""
         check(lib().pf_model_set_likelihood(self._h, name.encode()))
