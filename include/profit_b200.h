@@ -111,6 +111,15 @@ int pf_model_set_return_finesampled(pf_model *m, int value);
  * only for now. */
 int pf_model_set_mask(pf_model *m, const uint8_t *mask, unsigned width, unsigned height);
 int pf_model_set_adjust_mask(pf_model *m, int value);
+/* Model::set_dimensions (model.h:142-147); a width or height of 0 makes the
+ * next evaluation fail with "Model's requested dimensions are 0". */
+int pf_model_set_dimensions(pf_model *m, unsigned width, unsigned height);
+/* Model::set_dry_run (model.h:293-296): evaluations check their inputs and
+ * return a zeroed image of the drawing dimensions (model.cpp:279-286). */
+int pf_model_set_dry_run(pf_model *m, int value);
+/* Model::set_omp_threads (model.h:333-336): accepted for compatibility; the
+ * work runs on the GPU, so the value has no effect. */
+int pf_model_set_omp_threads(pf_model *m, unsigned threads);
 /* Only crop = true is supported (ProFit's returncrop default). */
 int pf_model_set_crop(pf_model *m, int value);
 /* "brute" (default, like Model::ensure_convolver, model.cpp:144-150),

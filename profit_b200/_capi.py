@@ -128,6 +128,9 @@ def _late_bindings(L):
     L.pf_model_set_likelihood.argtypes = [C.c_void_p, C.c_char_p]
     L.pf_model_set_mask.argtypes = [C.c_void_p, C.POINTER(C.c_uint8), C.c_uint, C.c_uint]
     L.pf_model_set_adjust_mask.argtypes = [C.c_void_p, C.c_int]
+    L.pf_model_set_dimensions.argtypes = [C.c_void_p, C.c_uint, C.c_uint]
+    L.pf_model_set_dry_run.argtypes = [C.c_void_p, C.c_int]
+    L.pf_model_set_omp_threads.argtypes = [C.c_void_p, C.c_uint]
     vp = C.c_void_p
     L.pf_catalogue_create.argtypes = [C.POINTER(vp)]
     L.pf_catalogue_destroy.argtypes = [vp]
@@ -154,4 +157,5 @@ EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch",
                        "pf_catalogue_set_magzero", "pf_catalogue_add_galaxy", "pf_catalogue_add_profile",
                        "pf_catalogue_size", "pf_catalogue_gradient_offset", "pf_catalogue_loglike_grad",
                        "pf_catalogue_last_time", "pf_model_set_likelihood", "pf_model_set_mask",
-                       "pf_model_set_adjust_mask")
+                       "pf_model_set_adjust_mask", "pf_model_set_dimensions", "pf_model_set_dry_run",
+                       "pf_model_set_omp_threads")

@@ -342,6 +342,7 @@ struct pf_model {
 	std::vector<uint8_t> mask;
 	unsigned mask_w = 0, mask_h = 0;
 	bool adjust_mask = true;
+	bool dry_run = false;
 	std::vector<uint64_t> mask_key;  // what the device masks were built for
 	DevBuf d_mask_draw, d_mask_out;
 	int like_kind = LIKE_NORM;
@@ -1697,6 +1698,28 @@ int pf_model_set_mask(pf_model *m, const uint8_t *mask, unsigned width, unsigned
 	return PF_OK;
 }
 
+int pf_model_set_dimensions(pf_model *m, unsigned width, unsigned height)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->width = width;
+	m->height = height;
+	return PF_OK;
+}
+
+int pf_model_set_dry_run(pf_model *m, int value)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->dry_run = value != 0;
+	return PF_OK;
+}
+
+int pf_model_set_omp_threads(pf_model *m, unsigned threads)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	(void)threads;
+	return PF_OK;
+}
+
 int pf_model_set_adjust_mask(pf_model *m, int value)
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");
@@ -1746,6 +1769,20 @@ int pf_model_evaluate(pf_model *m, double *image, size_t capacity, unsigned *out
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");
 	Analysis a;
+	if (m->dry_run) {
+		// model.cpp:279-286: inputs checked, a zeroed drawing-size image returned
+		PF_TRY(analyze(m, a));
+		size_t n = (size_t)a.dw * a.dh;
+		if (image) {
+			if (capacity < n) return set_error(PF_E_BUFFER, "output buffer too small");
+			std::memset(image, 0, n * 8);
+		}
+		if (out_w) *out_w = a.dw;
+		if (out_h) *out_h = a.dh;
+		if (offset_x) *offset_x = 0;
+		if (offset_y) *offset_y = 0;
+		return PF_OK;
+	}
 	if (m->precision == PF_FP64) {
 		PF_TRY(evaluate64(m, a));
 		size_t n = (size_t)a.ow * a.oh;

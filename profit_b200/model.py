@@ -142,6 +142,16 @@ class Model:
             check(L.pf_model_set_mask(self._h, mk.ctypes.data_as(C.POINTER(C.c_uint8)), w, h))
         check(L.pf_model_set_adjust_mask(self._h, int(bool(adjust))))
 
+    def set_dimensions(self, width: int, height: int):
+        check(lib().pf_model_set_dimensions(self._h, int(width), int(height)))
+
+    def set_dry_run(self, value: bool):
+        check(lib().pf_model_set_dry_run(self._h, int(bool(value))))
+
+    def set_omp_threads(self, n: int):
+        """Accepted for libprofit compatibility; no effect (the work runs on the GPU)."""
+        check(lib().pf_model_set_omp_threads(self._h, int(n)))
+
     def set_likelihood(self, name: str):
         """profitLikeModel's like.func: "norm", "chisq", "t" or "pois" (and their aliases)."""
         check(lib().pf_model_set_likelihood(self._h, name.encode()))

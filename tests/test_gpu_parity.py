@@ -512,3 +512,22 @@ def test_calculation_mask_fft_equals_brute(kind):
         m.set_mask(_mask_case(kind))
         out.append(m.evaluate()[0])
     assert _rel(out[1], out[0]) <= IMG_TOL
+
+
+def test_dimensions_dry_run_and_threads():
+    """Model::set_dimensions, set_dry_run (a zeroed drawing-size image, model.cpp:
+    279-286) and set_omp_threads (accepted, no effect)."""
+    m = Model(40, 30)
+    m.set_psf(W.gaussian_psf(9, 2.0))
+    m.add_profile("sersic", xcen=20, ycen=15, re=3, convolve=True)
+    m.set_omp_threads(8)
+    assert m.evaluate()[0].shape == (30, 40)
+    m.set_dimensions(50, 20)
+    img, _ = m.evaluate()
+    assert img.shape == (20, 50) and img.max() > 0
+    m.set_dry_run(True)
+    img, off = m.evaluate()
+    assert img.shape == (28, 58) and not img.any() and off == (0, 0)
+    m.set_dimensions(0, 20)
+    with pytest.raises(InvalidParameter):
+        m.evaluate()
