@@ -81,15 +81,15 @@ __device__ __forceinline__ C mul_mi(C a, T sign)
 }
 
 // In-place DFT of size R on v (forward: sign = +1 gives exp(-2 pi i nk/R)).
-template <class T, class C>
-__device__ __forceinline__ void small_dft(C *v, int R, T sign)
+template <int R, class T, class C>
+__device__ __forceinline__ void small_dft(C *v, T sign)
 {
-	if (R == 2) {
+	if constexpr (R == 2) {
 		C a = v[0], b = v[1];
 		v[0] = cadd(a, b);
 		v[1] = csub(a, b);
 	}
-	else if (R == 4) {
+	else if constexpr (R == 4) {
 		C s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
 		C s13 = cadd(v[1], v[3]), d13 = csub(v[1], v[3]);
 		v[0] = cadd(s02, s13);
@@ -98,7 +98,7 @@ __device__ __forceinline__ void small_dft(C *v, int R, T sign)
 		v[1] = cadd(d02, t);
 		v[3] = csub(d02, t);
 	}
-	else if (R == 3) {
+	else if constexpr (R == 3) {
 		const T h = T(0.86602540378443864676372317075294);  // sin(2 pi/3)
 		C s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
 		C x0 = v[0];
@@ -113,6 +113,7 @@ __device__ __forceinline__ void small_dft(C *v, int R, T sign)
 		v[2] = csub(m, t);
 	}
 	else {  // R == 5
+		static_assert(R == 5, "radix");
 		const T c1 = T(0.30901699437494742410229341718282);   // cos(2 pi/5)
 		const T c2 = T(-0.80901699437494742410229341718282);  // cos(4 pi/5)
 		const T s1 = T(0.95105651629515357211643933337938);   // sin(2 pi/5)
@@ -138,52 +139,100 @@ __device__ __forceinline__ void small_dft(C *v, int R, T sign)
 	}
 }
 
-// Stockham FFT of `cols` interleaved vectors of length n held in shared
-// memory: element t of vector c at buf[t * cols + c].  Returns the buffer
-// holding the result (a or b).  tw[t] = exp(-2 pi i t / n).
-template <class T, class C>
-__device__ C *fft_block(C *a, C *b, int n, int cols, const FftPlan &plan, const C *__restrict__ tw, bool inverse)
+// One radix-R Stockham stage over COLS interleaved vectors (element t of
+// vector c at buf[t * COLS + c]); stw: twiddles exp(-2 pi i t / n) in shared
+// memory.  Butterfly j = q ns + k reads in[j + r nb] and writes
+// out[q ns R + k + r ns] = out[(j - k) R + k + r ns].
+template <int R, int COLS, class T, class C>
+__device__ __forceinline__ void fft_stage(const C *in, C *out, const C *stw, int nb, int ns, unsigned magic,
+                                          int tstep, bool inverse)
 {
 	const T sign = inverse ? T(-1) : T(1);
-	int Ns = 1;
+	for (int t = threadIdx.x; t < nb * COLS; t += blockDim.x) {
+		const int j = t / COLS, c = t - j * COLS;
+		const int q = ns == 1 ? j : (int)__umulhi((unsigned)j, magic);
+		const int k = j - q * ns;
+		C v[R];
+#pragma unroll
+		for (int r = 0; r < R; r++) v[r] = in[(j + r * nb) * COLS + c];
+#pragma unroll
+		for (int r = 1; r < R; r++) {
+			C w = stw[r * k * tstep];
+			if (inverse) w.y = -w.y;
+			v[r] = cmul(v[r], w);
+		}
+		small_dft<R, T, C>(v, sign);
+		const int idx = (j - k) * R + k;
+#pragma unroll
+		for (int r = 0; r < R; r++) out[(idx + r * ns) * COLS + c] = v[r];
+	}
+}
+
+// Stockham FFT of COLS interleaved vectors of length plan.n held in shared
+// memory (buffers a and b); returns the buffer holding the result.  The
+// caller has filled stw and synchronised.
+template <int COLS, class T, class C>
+__device__ __forceinline__ C *fft_block(C *a, C *b, const FftPlan &plan, const C *stw, bool inverse)
+{
 	C *in = a, *out = b;
 	for (int s = 0; s < plan.nstages; s++) {
-		const int R = plan.radix[s];
-		const int nb = n / R;
-		const int tstep = n / (Ns * R);
-		for (int t = threadIdx.x; t < nb * cols; t += blockDim.x) {
-			const int j = t / cols, c = t - j * cols;
-			const int k = j % Ns;
-			C v[5];
-#pragma unroll
-			for (int r = 0; r < 5; r++)
-				if (r < R) v[r] = in[(j + r * nb) * cols + c];
-#pragma unroll
-			for (int r = 1; r < 5; r++) {
-				if (r < R) {
-					C w = tw[r * k * tstep];
-					if (inverse) w.y = -w.y;
-					v[r] = cmul(v[r], w);
-				}
-			}
-			small_dft<T, C>(v, R, sign);
-			const int idx = (j / Ns) * Ns * R + k;
-#pragma unroll
-			for (int r = 0; r < 5; r++)
-				if (r < R) out[(idx + r * Ns) * cols + c] = v[r];
+		const int nb = plan.nb[s], ns = plan.ns[s], ts = plan.tstep[s];
+		const unsigned mg = plan.ns_magic[s];
+		switch (plan.radix[s]) {
+		case 2: fft_stage<2, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 3: fft_stage<3, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 4: fft_stage<4, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		default: fft_stage<5, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
 		}
 		__syncthreads();
 		C *tmp = in;
 		in = out;
 		out = tmp;
-		Ns *= R;
 	}
 	return in;
 }
 
+// 16-byte asynchronous global -> shared copy (both addresses 16-byte
+// aligned); completed by cp_async_wait() before the barrier that publishes
+// the buffer.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+	unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+	asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait()
+{
+	asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+// One complex element global -> shared: asynchronous for 16-byte elements,
+// a plain copy otherwise.
+template <class C>
+__device__ __forceinline__ void cp_async_elem(C *dst, const C *src)
+{
+	if constexpr (sizeof(C) == 16) cp_async16(dst, src);
+	else *dst = *src;
+}
+
+// Starts the copy of the twiddle table into shared memory (when it fits
+// beside the buffers, TWS), else returns the global table, read through L1.
+// Complex values of 8 or 16 bytes: 16-byte copies cover the table (n is
+// even).  TWS is a template argument so that the stages' twiddle loads are
+// compiled as shared-memory loads.
+template <bool TWS, class C>
+__device__ __forceinline__ const C *load_twiddles(C *smem, const C *__restrict__ tw, int n)
+{
+	if constexpr (!TWS) return tw;
+	constexpr int PER = 16 / sizeof(C);
+	for (int t = threadIdx.x; t * PER < n; t += blockDim.x) cp_async16(smem + t * PER, tw + t * PER);
+	return smem;
+}
+
 // Row pass, forward.  Rows y0 = 2*blockIdx.x and y0 + 1 of the source (placed
 // at (sx0, sy0) of the M x N grid, zero elsewhere) -> half spectra.
-template <class T, class TIn>
+// Shared memory: two N-element buffers and the N twiddles.
+template <class T, class TIn, bool TWS>
 __global__ void k_fft_rows_fwd(const TIn *__restrict__ src, int sw, int sh, int sx0, int sy0, int N, FftPlan plan,
                                const typename Cx<T>::type *__restrict__ tw, typename Cx<T>::type *__restrict__ spec,
                                int spec_ld, size_t src_batch, size_t spec_batch)
@@ -197,16 +246,36 @@ __global__ void k_fft_rows_fwd(const TIn *__restrict__ src, int sw, int sh, int 
 	const int y0 = 2 * blockIdx.x;
 	const int ra = y0 - sy0, rb = y0 + 1 - sy0;
 	const bool has_a = ra >= 0 && ra < sh, has_b = rb >= 0 && rb < sh;
-	for (int x = threadIdx.x; x < N; x += blockDim.x) {
-		int sx = x - sx0;
-		C z;
-		z.x = (has_a && sx >= 0 && sx < sw) ? (T)src[(size_t)ra * sw + sx] : T(0);
-		z.y = (has_b && sx >= 0 && sx < sw) ? (T)src[(size_t)rb * sw + sx] : T(0);
-		a[x] = z;
-	}
-	__syncthreads();
-	C *Z = (has_a || has_b) ? fft_block<T, C>(a, b, N, 1, plan, tw, false) : a;
 	C *ra_out = spec + (size_t)y0 * spec_ld, *rb_out = ra_out + spec_ld;
+	if (!has_a && !has_b) {
+		C z;
+		z.x = T(0);
+		z.y = T(0);
+		for (int k = threadIdx.x; k <= N / 2; k += blockDim.x) {
+			ra_out[k] = z;
+			rb_out[k] = z;
+		}
+		return;
+	}
+	const C *stw = load_twiddles<TWS>(b + N, tw, N);
+	// U elements per thread in flight before any is stored
+	constexpr int U = 4;
+	for (int x0 = threadIdx.x; x0 < N; x0 += U * blockDim.x) {
+		C z[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const int x = x0 + u * blockDim.x, sx = x - sx0;
+			const bool in = x < N && sx >= 0 && sx < sw;
+			z[u].x = (has_a && in) ? (T)src[(size_t)ra * sw + sx] : T(0);
+			z[u].y = (has_b && in) ? (T)src[(size_t)rb * sw + sx] : T(0);
+		}
+#pragma unroll
+		for (int u = 0; u < U; u++)
+			if (x0 + u * blockDim.x < N) a[x0 + u * blockDim.x] = z[u];
+	}
+	cp_async_wait();
+	__syncthreads();
+	C *Z = fft_block<1, T, C>(a, b, plan, stw, false);
 	for (int k = threadIdx.x; k <= N / 2; k += blockDim.x) {
 		C zk = Z[k], zm = Z[(N - k) % N];
 		C A, B;
@@ -222,11 +291,11 @@ __global__ void k_fft_rows_fwd(const TIn *__restrict__ src, int sw, int sh, int 
 
 // Column pass: CB columns of the half spectrum per CTA.  mode 0: forward FFT
 // only (PSF spectrum); mode 1: forward, times K, inverse; mode 2: forward,
-// times conj(K), inverse.
-template <class T, int CB>
+// times conj(K), inverse.  Shared memory: two M x CB buffers and M twiddles.
+template <class T, int CB, bool TWS>
 __global__ void k_fft_cols(typename Cx<T>::type *__restrict__ spec, int spec_ld, int ncols, int M, FftPlan plan,
                            const typename Cx<T>::type *__restrict__ tw, const typename Cx<T>::type *__restrict__ K,
-                           int mode, size_t spec_batch)
+                           int mode, size_t spec_batch, bool k_smem)
 {
 	using C = typename Cx<T>::type;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -234,16 +303,30 @@ __global__ void k_fft_cols(typename Cx<T>::type *__restrict__ spec, int spec_ld,
 	C *b = a + (size_t)M * CB;
 	spec += blockIdx.y * spec_batch;
 	const int c0 = blockIdx.x * CB;
+	const C *stw = load_twiddles<TWS>(b + (size_t)M * CB, tw, M);
+	// the kernel spectrum's columns, fetched with the data (k_smem: after the
+	// twiddles in shared memory)
+	C *sk = b + (size_t)M * CB + (TWS ? M : 0);
+	if (mode != 0 && k_smem)
+		for (int t = threadIdx.x; t < M * CB; t += blockDim.x) {
+			int row = t / CB, c = t - row * CB;
+			if (c0 + c < ncols) cp_async_elem(sk + t, K + (size_t)row * spec_ld + c0 + c);
+		}
 	for (int t = threadIdx.x; t < M * CB; t += blockDim.x) {
 		int row = t / CB, c = t - row * CB;
-		C v;
-		v.x = T(0);
-		v.y = T(0);
-		if (c0 + c < ncols) v = spec[(size_t)row * spec_ld + c0 + c];
-		a[t] = v;
+		if (c0 + c < ncols) {
+			cp_async_elem(a + t, spec + (size_t)row * spec_ld + c0 + c);
+		}
+		else {
+			C v;
+			v.x = T(0);
+			v.y = T(0);
+			a[t] = v;
+		}
 	}
+	cp_async_wait();
 	__syncthreads();
-	C *S = fft_block<T, C>(a, b, M, CB, plan, tw, false);
+	C *S = fft_block<CB, T, C>(a, b, plan, stw, false);
 	if (mode == 0) {
 		for (int t = threadIdx.x; t < M * CB; t += blockDim.x) {
 			int row = t / CB, c = t - row * CB;
@@ -254,14 +337,14 @@ __global__ void k_fft_cols(typename Cx<T>::type *__restrict__ spec, int spec_ld,
 	for (int t = threadIdx.x; t < M * CB; t += blockDim.x) {
 		int row = t / CB, c = t - row * CB;
 		if (c0 + c < ncols) {
-			C k = K[(size_t)row * spec_ld + c0 + c];
+			C k = k_smem ? sk[t] : K[(size_t)row * spec_ld + c0 + c];
 			if (mode == 2) k.y = -k.y;
 			S[t] = cmul(S[t], k);
 		}
 	}
 	__syncthreads();
 	C *other = (S == a) ? b : a;
-	C *R = fft_block<T, C>(S, other, M, CB, plan, tw, true);
+	C *R = fft_block<CB, T, C>(S, other, plan, stw, true);
 	for (int t = threadIdx.x; t < M * CB; t += blockDim.x) {
 		int row = t / CB, c = t - row * CB;
 		if (c0 + c < ncols) spec[(size_t)row * spec_ld + c0 + c] = R[t];
@@ -270,7 +353,7 @@ __global__ void k_fft_cols(typename Cx<T>::type *__restrict__ spec, int spec_ld,
 
 // Inverse row pass: rows y0, y0+1 of the result; out(x, y) = c(x + dx, y + dy)
 // / (M N) (+ add) for the output window [0, ow) x [0, oh).
-template <class T, class TOut, class TAdd>
+template <class T, class TOut, class TAdd, bool TWS>
 __global__ void k_fft_rows_inv(const typename Cx<T>::type *__restrict__ spec, int spec_ld, int N, int M, FftPlan plan,
                                const typename Cx<T>::type *__restrict__ tw, int dx, int dy, TOut *__restrict__ out,
                                int ow, int oh, const TAdd *__restrict__ add, int add_stride, int add_ox, int add_oy,
@@ -287,16 +370,23 @@ __global__ void k_fft_rows_inv(const typename Cx<T>::type *__restrict__ spec, in
 	const int oa = y0 - dy, ob = y0 + 1 - dy;  // output rows fed by this pair
 	const bool want_a = oa >= 0 && oa < oh, want_b = ob >= 0 && ob < oh;
 	if (!want_a && !want_b) return;
+	// the two half-spectrum rows land in b[0 .. N/2] and b[N/2+1 .. N+1]
+	// (b holds N + 2 elements), the twiddles after them
+	const int h = N / 2 + 1;
+	const C *stw = load_twiddles<TWS>(b + N + 2, tw, N);
 	const C *ra = spec + (size_t)y0 * spec_ld, *rb = ra + spec_ld;
+	for (int k = threadIdx.x; k < 2 * h; k += blockDim.x) cp_async_elem(b + k, k < h ? ra + k : rb + (k - h));
+	cp_async_wait();
+	__syncthreads();
 	for (int k = threadIdx.x; k < N; k += blockDim.x) {
 		C A, B;
-		if (k <= N / 2) {
-			A = ra[k];
-			B = rb[k];
+		if (k < h) {
+			A = b[k];
+			B = b[h + k];
 		}
 		else {
-			A = ra[N - k];
-			B = rb[N - k];
+			A = b[N - k];
+			B = b[h + N - k];
 			A.y = -A.y;
 			B.y = -B.y;
 		}
@@ -306,21 +396,29 @@ __global__ void k_fft_rows_inv(const typename Cx<T>::type *__restrict__ spec, in
 		a[k] = z;
 	}
 	__syncthreads();
-	C *Z = fft_block<T, C>(a, b, N, 1, plan, tw, true);
+	C *Z = fft_block<1, T, C>(a, b, plan, stw, true);
 	const T scale = T(1) / ((T)M * (T)N);
-	for (int x = threadIdx.x; x < ow; x += blockDim.x) {
-		int X = x + dx;
-		T va = (X >= 0 && X < N) ? Z[X].x * scale : T(0);
-		T vb = (X >= 0 && X < N) ? Z[X].y * scale : T(0);
-		if (want_a) {
-			T v = va;
-			if (add) v += (T)add[(size_t)(oa + add_oy) * add_stride + x + add_ox];
-			out[(size_t)oa * ow + x] = (TOut)v;
+	// U outputs per thread, their `add` loads in flight together
+	constexpr int U = 4;
+	const TAdd *adda = add ? add + (size_t)(oa + add_oy) * add_stride + add_ox : nullptr;
+	const TAdd *addb = add ? add + (size_t)(ob + add_oy) * add_stride + add_ox : nullptr;
+	for (int x0 = threadIdx.x; x0 < ow; x0 += U * blockDim.x) {
+		T pa[U], pb[U];
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const int x = x0 + u * blockDim.x;
+			pa[u] = (add && want_a && x < ow) ? (T)adda[x] : T(0);
+			pb[u] = (add && want_b && x < ow) ? (T)addb[x] : T(0);
 		}
-		if (want_b) {
-			T v = vb;
-			if (add) v += (T)add[(size_t)(ob + add_oy) * add_stride + x + add_ox];
-			out[(size_t)ob * ow + x] = (TOut)v;
+#pragma unroll
+		for (int u = 0; u < U; u++) {
+			const int x = x0 + u * blockDim.x;
+			if (x >= ow) break;
+			const int X = x + dx;
+			const T va = (X >= 0 && X < N) ? Z[X].x * scale : T(0);
+			const T vb = (X >= 0 && X < N) ? Z[X].y * scale : T(0);
+			if (want_a) out[(size_t)oa * ow + x] = (TOut)(va + pa[u]);
+			if (want_b) out[(size_t)ob * ow + x] = (TOut)(vb + pb[u]);
 		}
 	}
 }
@@ -328,6 +426,19 @@ __global__ void k_fft_rows_inv(const typename Cx<T>::type *__restrict__ spec, in
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
+
+void fft_plan_stages(FftPlan &plan)
+{
+	int ns = 1;
+	for (int s = 0; s < plan.nstages; s++) {
+		const int R = plan.radix[s];
+		plan.ns[s] = ns;
+		plan.nb[s] = plan.n / R;
+		plan.tstep[s] = plan.n / (ns * R);
+		plan.ns_magic[s] = ns > 1 ? (unsigned)((0x100000000ull + ns - 1) / ns) : 0u;
+		ns *= R;
+	}
+}
 
 static bool factor_235(int n, FftPlan &plan)
 {
@@ -344,6 +455,7 @@ static bool factor_235(int n, FftPlan &plan)
 			plan.radix[plan.nstages++] = r;
 			m /= r;
 		}
+	fft_plan_stages(plan);
 	return m == 1;
 }
 
@@ -377,16 +489,41 @@ static const typename Cx<T>::type *twiddles(int n)
 	return d;
 }
 
-template <class T>
-static int cols_per_block(int M)
+static int sm_count()
 {
-	// two ping-pong buffers of M x CB complex values within 200 KB
-	size_t per = 2 * sizeof(typename Cx<T>::type) * (size_t)M;
-	int cb = (int)((200 * 1024) / per);
-	if (cb >= 8) return 8;
-	if (cb >= 4) return 4;
-	if (cb >= 2) return 2;
-	return 1;
+	static int n = 0;
+	if (n <= 0) {
+		int dev = 0;
+		cudaGetDevice(&dev);
+		if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+		cudaGetLastError();
+	}
+	return n;
+}
+
+// Threads for `cols` interleaved transforms of length plan.n: one per
+// butterfly of the widest stage (n / smallest radix), in whole warps.
+static int fft_threads(const FftPlan &plan, int cols)
+{
+	int rmin = 5;
+	for (int s = 0; s < plan.nstages; s++) rmin = plan.radix[s] < rmin ? plan.radix[s] : rmin;
+	int t = (plan.n / rmin) * cols;
+	t = (t + 31) / 32 * 32;
+	return t < 64 ? 64 : (t > 512 ? 512 : t);
+}
+
+// Columns per CTA of the column pass: as many as share memory allows (two
+// ping-pong buffers of M x CB complex values within 200 KB) while the grid
+// still gives every SM two CTAs; a lone small transform leaves the rest of
+// the GPU idle, so parallelism wins over sector efficiency.
+template <class T>
+static int cols_per_block(int M, int ncols, int batch)
+{
+	const size_t per = 2 * sizeof(typename Cx<T>::type) * (size_t)M;
+	int cb = 8;
+	while (cb > 1 && (per * cb + per / 2 > 200 * 1024 || (size_t)((ncols + cb - 1) / cb) * batch < 2 * (size_t)sm_count()))
+		cb /= 2;
+	return cb;
 }
 
 template <class T, int CB>
@@ -394,10 +531,19 @@ static cudaError_t launch_cols(typename Cx<T>::type *spec, int spec_ld, int ncol
                                const typename Cx<T>::type *tw, const typename Cx<T>::type *K, int mode, int batch,
                                size_t spec_batch, cudaStream_t s)
 {
-	size_t smem = 2 * sizeof(typename Cx<T>::type) * (size_t)M * CB;
-	cudaFuncSetAttribute(k_fft_cols<T, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+	const size_t e = sizeof(typename Cx<T>::type);
+	size_t smem = e * (size_t)M * 2 * CB;
+	const bool tws = smem + e * (size_t)M <= FFT_SMEM_BYTES;
+	if (tws) smem += e * (size_t)M;
+	// the kernel columns in shared memory only while two CTAs still fit an SM
+	const bool ks = mode != 0 && 2 * (smem + e * (size_t)M * CB) <= FFT_SMEM_BYTES;
+	if (ks) smem += e * (size_t)M * CB;
+	auto kern = tws ? k_fft_cols<T, CB, true> : k_fft_cols<T, CB, false>;
+	static bool configured[2] = {false, false};  // per instantiation; setting it twice is harmless
+	if (!configured[tws]) configured[tws] = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                                               FFT_SMEM_BYTES) == cudaSuccess;
 	dim3 grid((ncols + CB - 1) / CB, batch);
-	k_fft_cols<T, CB><<<grid, 256, smem, s>>>(spec, spec_ld, ncols, M, pm, tw, K, mode, spec_batch);
+	kern<<<grid, fft_threads(pm, CB), smem, s>>>(spec, spec_ld, ncols, M, pm, tw, K, mode, spec_batch, ks);
 	return cudaGetLastError();
 }
 
@@ -406,7 +552,7 @@ static cudaError_t cols_any(typename Cx<T>::type *spec, int spec_ld, int ncols, 
                             const typename Cx<T>::type *tw, const typename Cx<T>::type *K, int mode, int batch,
                             size_t spec_batch, cudaStream_t s)
 {
-	switch (cols_per_block<T>(M)) {
+	switch (cols_per_block<T>(M, ncols, batch)) {
 	case 8: return launch_cols<T, 8>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, s);
 	case 4: return launch_cols<T, 4>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, s);
 	case 2: return launch_cols<T, 2>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, s);
@@ -426,12 +572,6 @@ cudaError_t FftConv<T>::setup(int M_, int N_)
 	tw_n = twiddles<T>(N);
 	if (!tw_m || !tw_n) return cudaErrorMemoryAllocation;
 	ld = N / 2 + 1;
-	for (int f : {0, 1})
-		cudaFuncSetAttribute(f ? (const void *)k_fft_rows_fwd<T, float> : (const void *)k_fft_rows_fwd<T, double>,
-		                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-	cudaFuncSetAttribute(k_fft_rows_inv<T, double, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-	cudaFuncSetAttribute(k_fft_rows_inv<T, double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-	cudaFuncSetAttribute(k_fft_rows_inv<T, float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 	have_kernel = false;
 	return cudaGetLastError();
 }
@@ -441,10 +581,15 @@ template <class TIn>
 cudaError_t FftConv<T>::forward_rows(const TIn *src, int sw, int sh, int sx0, int sy0, Cplx *spec, int batch,
                                      size_t src_batch, cudaStream_t s)
 {
-	size_t smem = 2 * sizeof(Cplx) * (size_t)N;
+	const bool tws = 3 * sizeof(Cplx) * (size_t)N <= FFT_SMEM_BYTES;
+	size_t smem = (tws ? 3 : 2) * sizeof(Cplx) * (size_t)N;
 	dim3 grid(M / 2, batch);
-	k_fft_rows_fwd<T, TIn><<<grid, 256, smem, s>>>(src, sw, sh, sx0, sy0, N, plan_n, tw_n, spec, ld, src_batch,
-	                                               (size_t)M * ld);
+	auto kern = tws ? k_fft_rows_fwd<T, TIn, true> : k_fft_rows_fwd<T, TIn, false>;
+	static bool configured[2] = {false, false};  // per instantiation; setting it twice is harmless
+	if (!configured[tws]) configured[tws] = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                                               FFT_SMEM_BYTES) == cudaSuccess;
+	kern<<<grid, fft_threads(plan_n, 1), smem, s>>>(src, sw, sh, sx0, sy0, N, plan_n, tw_n, spec, ld, src_batch,
+	                                                (size_t)M * ld);
 	return cudaGetLastError();
 }
 
@@ -469,11 +614,15 @@ cudaError_t FftConv<T>::convolve(const TIn *src, int sw, int sh, int sx0, int sy
 	if (e != cudaSuccess) return e;
 	e = cols_any<T>(work, ld, ld, M, plan_m, tw_m, kspec, adjoint ? 2 : 1, batch, (size_t)M * ld, s);
 	if (e != cudaSuccess) return e;
-	size_t smem = 2 * sizeof(Cplx) * (size_t)N;
+	const bool tws = sizeof(Cplx) * (3 * (size_t)N + 2) <= FFT_SMEM_BYTES;
+	size_t smem = sizeof(Cplx) * ((tws ? 3 : 2) * (size_t)N + 2);
 	dim3 grid(M / 2, batch);
-	k_fft_rows_inv<T, TOut, TAdd><<<grid, 256, smem, s>>>(work, ld, N, M, plan_n, tw_n, dx, dy, out, ow, oh, add,
-	                                                      add_stride, add_ox, add_oy, (size_t)M * ld, out_batch,
-	                                                      add_batch);
+	auto kern = tws ? k_fft_rows_inv<T, TOut, TAdd, true> : k_fft_rows_inv<T, TOut, TAdd, false>;
+	static bool configured[2] = {false, false};  // per instantiation; setting it twice is harmless
+	if (!configured[tws]) configured[tws] = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+	                                                               FFT_SMEM_BYTES) == cudaSuccess;
+	kern<<<grid, fft_threads(plan_n, 1), smem, s>>>(work, ld, N, M, plan_n, tw_n, dx, dy, out, ow, oh, add, add_stride,
+	                                                add_ox, add_oy, (size_t)M * ld, out_batch, add_batch);
 	return cudaGetLastError();
 }
 

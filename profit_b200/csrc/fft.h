@@ -11,12 +11,24 @@ namespace pf {
 constexpr int FFT_MAX_STAGES = 16;
 // one row (two ping-pong buffers of complex doubles) must fit in shared memory
 constexpr int FFT_MAX_LEN = 6912;
+constexpr size_t FFT_SMEM_BYTES = 227 * 1024;
 
+// Stockham stages of a length-n transform: stage s has radix R = radix[s],
+// ns[s] = product of the earlier radices, nb[s] = n / R butterflies and
+// twiddle stride tstep[s] = n / (ns R); j / ns = umulhi(j, ns_magic) for
+// j < 2^16 (ns_magic = ceil(2^32 / ns), unused when ns = 1).
 struct FftPlan {
 	int n;
 	int nstages;
 	int radix[FFT_MAX_STAGES];
+	int ns[FFT_MAX_STAGES];
+	int nb[FFT_MAX_STAGES];
+	int tstep[FFT_MAX_STAGES];
+	unsigned ns_magic[FFT_MAX_STAGES];
 };
+
+// Fills the stage tables of plan from plan.n and plan.radix.
+void fft_plan_stages(FftPlan &plan);
 
 // Smallest even size >= need whose prime factors are 2, 3 and 5.
 int fft_good_size(int need);

@@ -46,8 +46,13 @@ cudaError_t launch_downsample64(const double *src, unsigned sw, unsigned sh, uns
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
                             int nt, bool all_kinds, const QueueSet &q, cudaStream_t s);
+// Levels >= 3 (reached only by Sersic centre cusps) run in one CTA when the
+// launch holds at most this many cusps, else one grid-wide launch per level.
+constexpr int DEEP_ONE_CTA_MAX_CUSPS = 8;
+// cusps: Sersic profiles with adjust across the launch's batch entries (those
+// that may recurse past level 2).
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
-                            float *jac, int nt, bool all_kinds, const QueueSet &q, cudaStream_t s);
+                            float *jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s);
 // partials: n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN doubles;
 // tickets: n_profiles zero-initialised counters (left at zero again).
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles);

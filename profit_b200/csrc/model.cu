@@ -326,6 +326,7 @@ struct pf_model {
 	cudaStream_t stream = nullptr;
 	cudaEvent_t ev[5] = {};
 	float timings[4] = {0, 0, 0, 0};
+	bool timings_lazy = false;  // timings still to be read from ev[] (FP32 pipeline)
 
 	// device buffers
 	DevBuf d_prof, d_fprof, d_prof_begin, d_prof_batch;
@@ -612,7 +613,7 @@ int prepare_fft(pf_model *m, const Analysis &a, int batch, bool need32)
 // Queue segments per level; capacities start from a pixel-count estimate and
 // grow after an overflow.
 int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q, int32_t *decisions,
-                  unsigned long long *level_counts, bool with_masks = false)
+                  unsigned long long *level_counts, bool with_masks = false, bool reset = true)
 {
 	if (m->caps.size() != (size_t)MAX_LEVELS) {
 		m->caps.assign(MAX_LEVELS, 0);
@@ -647,7 +648,7 @@ int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q
 	q.levels = (uint32_t)a.levels;
 	q.decisions = decisions;
 	q.level_counts = level_counts;
-	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, m->stream));
+	if (reset) PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, m->stream));
 	return PF_OK;
 }
 
@@ -875,6 +876,7 @@ int evaluate64(pf_model *m, Analysis &a)
 			if (m->debug) PF_TRY(fetch_debug(m, a));
 			float t = 0;
 			cudaEventElapsedTime(&t, m->ev[0], m->ev[2]);
+			m->timings_lazy = false;
 			m->timings[0] = t;
 			cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
 			cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
@@ -909,6 +911,16 @@ int tangent_stride(const pf_model *m)
 	for (auto &p : m->profiles)
 		if (is_radial_kind(p.kind)) nt = std::max(nt, tangent_count(p.kind));
 	return nt;
+}
+
+// Sersic profiles with adjust: those whose centre cusp may recurse past
+// level 2 (the count picks how the deep levels are launched).
+int cusp_count(const pf_model *m)
+{
+	int n = 0;
+	for (auto &p : m->profiles)
+		if (p.kind == PK_SERSIC && p.adjust) n++;
+	return n;
 }
 
 // Whether the model has radial profiles beyond Sersic and Moffat (selects the
@@ -950,7 +962,8 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *model = m->d_model32.as<float>();
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), 1, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain,
 	                        jac, tangent_stride(m), all_kinds(m), q, m->stream));
-	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, tangent_stride(m), all_kinds(m), q,
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, tangent_stride(m), all_kinds(m),
+	                        cusp_count(m), q,
 	                        m->stream));
 	PF_CUDA(record_event(m->ev[1], m->stream));
 	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
@@ -1026,8 +1039,14 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 	return s;
 }
 
-void finish_timings32(pf_model *m)
+// The FP32 pipeline's phase times are read from its events only when asked
+// for (pf_model_last_timings), which keeps the event queries off the
+// evaluation's own path.
+void finish_timings32(pf_model *m) { m->timings_lazy = true; }
+
+void resolve_timings32(pf_model *m)
 {
+	m->timings_lazy = false;
 	cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
 	cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
 	if (m->has_data) {
@@ -1140,11 +1159,27 @@ int check_profile(pf_model *m, int index);
 
 }  // namespace
 
+// Host-prologue staging: one pinned block [DevProfile x n | FProfile x n |
+// invalid flags x C] uploaded with one copy; results [logL x C | gradient x
+// C*nrefs | queue counters] downloaded with one copy.
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+struct StageLayout {
+	size_t f = 0, inv = 0, total = 0;
+	StageLayout(int C, int nprof)
+	{
+		f = align256((size_t)C * nprof * sizeof(DevProfile));
+		inv = f + align256((size_t)C * nprof * sizeof(FProfile));
+		total = inv + align256((size_t)C * 4);
+	}
+};
+
 struct BatchState {
-	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out_ll, d_out_grad, d_ll, d_T;
-	HostBuf h_tmpl, h_values, h_out, h_dev, h_fprof, h_invalid;
+	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out, d_ll, d_T, d_stage;
+	HostBuf h_tmpl, h_values, h_out, h_stage;
 	int refs_n = -1, chunk = 0;
 	std::vector<int> refs_host;
+	// (profile, kind, rescale_flux, name) of the references refs_host was resolved for
+	std::vector<std::tuple<int, int, int, std::string>> refs_key;
 	cudaGraphExec_t graph = nullptr;
 	std::vector<uint64_t> sig;
 	unsigned long long graph_kernels = 0;
@@ -1175,15 +1210,19 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	float *wseed = m->d_wseed.as<float>(), *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>();
 	const int *ref_profile = bs.d_refs.as<int>(), *ref_offset = ref_profile + nrefs, *ref_code = ref_offset + nrefs;
 
+	const StageLayout L(C, nprof);
+	const DevProfile *dev = host_prologue ? bs.d_stage.as<DevProfile>() : bs.d_dev.as<DevProfile>();
+	const FProfile *fprof = host_prologue ? reinterpret_cast<const FProfile *>(bs.d_stage.as<char>() + L.f)
+	                                      : m->d_fprof.as<FProfile>();
+	const int *invalid = host_prologue ? reinterpret_cast<const int *>(bs.d_stage.as<char>() + L.inv)
+	                                   : bs.d_invalid.as<int>();
+	double *out_ll = bs.d_out.as<double>(), *out_grad = out_ll + C;
+
 	PF_CUDA(record_event(m->ev[0], s));
-	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, s));
+	PF_CUDA(cudaMemsetAsync(q.counts, 0, CTRL_WORDS * 4, s));
 	PF_CUDA(cudaMemsetAsync(bs.d_T.p, 0, (size_t)C * nprof * NTAN * 8, s));
 	if (host_prologue) {
-		PF_CUDA(cudaMemcpyAsync(bs.d_dev.p, bs.h_dev.p, (size_t)C * nprof * sizeof(DevProfile),
-		                        cudaMemcpyHostToDevice, s));
-		PF_CUDA(cudaMemcpyAsync(m->d_fprof.p, bs.h_fprof.p, (size_t)C * nprof * sizeof(FProfile),
-		                        cudaMemcpyHostToDevice, s));
-		PF_CUDA(cudaMemcpyAsync(bs.d_invalid.p, bs.h_invalid.p, (size_t)C * 4, cudaMemcpyHostToDevice, s));
+		PF_CUDA(cudaMemcpyAsync(bs.d_stage.p, bs.h_stage.p, L.total, cudaMemcpyHostToDevice, s));
 	}
 	else {
 		PF_CUDA(cudaMemcpyAsync(bs.d_tmpl.p, bs.h_tmpl.p, nprof * sizeof(ProfileParams), cudaMemcpyHostToDevice, s));
@@ -1193,12 +1232,11 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		                              bs.d_values.as<double>(), geometry(m, a), bs.d_dev.as<DevProfile>(),
 		                              m->d_fprof.as<FProfile>(), bs.d_invalid.as<int>(), s));
 	}
-	const FProfile *fprof = m->d_fprof.as<FProfile>();
 	const int nt = tangent_stride(m);
 	const bool ak = all_kinds(m);
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx, m->sy, conv, plain, jac, nt, ak, q,
 	                        s));
-	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, nt, ak, q, s));
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, nt, ak, C * cusp_count(m), q, s));
 	PF_CUDA(record_event(m->ev[1], s));
 	PF_TRY(forward_conv32(m, a, conv, plain, model64, C));
 	PF_CUDA(record_event(m->ev[2], s));
@@ -1218,14 +1256,11 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix, nt,
 		                          jpart, jtick, bs.d_T.as<double>(), s));
 	}
-	PF_CUDA(launch_batch_gradient(bs.d_dev.as<DevProfile>(), nprof, C, ref_profile, ref_code, nrefs,
-	                              bs.d_T.as<double>(), bs.d_ll.as<double>(), bs.d_invalid.as<int>(),
-	                              bs.d_out_ll.as<double>(), bs.d_out_grad.as<double>(), s));
+	PF_CUDA(launch_batch_gradient(dev, nprof, C, ref_profile, ref_code, nrefs, bs.d_T.as<double>(),
+	                              bs.d_ll.as<double>(), invalid, out_ll, out_grad, s));
 	PF_CUDA(record_event(m->ev[3], s));
 	char *ho = bs.h_out.as<char>();
-	PF_CUDA(cudaMemcpyAsync(ho, bs.d_out_ll.p, (size_t)C * 8, cudaMemcpyDeviceToHost, s));
-	PF_CUDA(cudaMemcpyAsync(ho + (size_t)C * 8, bs.d_out_grad.p, (size_t)C * nrefs * 8, cudaMemcpyDeviceToHost, s));
-	PF_CUDA(cudaMemcpyAsync(ho + (size_t)C * (1 + nrefs) * 8, m->d_ctrl.p, CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
+	PF_CUDA(cudaMemcpyAsync(ho, bs.d_out.p, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
 	return PF_OK;
 }
 
@@ -1251,19 +1286,44 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	if (!m->batch) m->batch = new BatchState();
 	BatchState &bs = *m->batch;
 
-	// parameter references -> (profile, byte offset, gradient code)
-	std::vector<int> host_refs(3 * (size_t)nrefs);
-	for (int i = 0; i < nrefs; i++) {
-		PF_TRY(check_profile(m, refs[i].profile));
-		const ProfileParams &p = m->profiles[refs[i].profile];
-		const ParamDesc *d = find_param(p.kind, refs[i].name);
-		if (!d || d->type != T_DOUBLE)
-			return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown double parameter: ") + refs[i].name);
-		int code = 0;
-		PF_TRY(gradient_code(p, refs[i].name, code));
-		host_refs[i] = refs[i].profile;
-		host_refs[nrefs + i] = (int)d->off;
-		host_refs[2 * nrefs + i] = code;
+	// parameter references -> (profile, byte offset, gradient code); the
+	// resolution of the previous call is reused while the references and
+	// what they resolve against (kind, rescale_flux) are the same
+	bool same = (int)bs.refs_key.size() == nrefs && (int)bs.refs_host.size() == 3 * nrefs;
+	for (int i = 0; same && i < nrefs; i++) {
+		const int pi = refs[i].profile;
+		same = pi >= 0 && pi < (int)m->profiles.size() && refs[i].name &&
+		       std::get<0>(bs.refs_key[i]) == pi && std::get<1>(bs.refs_key[i]) == m->profiles[pi].kind &&
+		       std::get<2>(bs.refs_key[i]) == m->profiles[pi].rescale_flux && std::get<3>(bs.refs_key[i]) == refs[i].name;
+	}
+	std::vector<int> host_refs;
+	if (same) host_refs = bs.refs_host;
+	else {
+		host_refs.resize(3 * (size_t)nrefs);
+		bs.refs_key.clear();
+		for (int i = 0; i < nrefs; i++) {
+			PF_TRY(check_profile(m, refs[i].profile));
+			const ProfileParams &p = m->profiles[refs[i].profile];
+			const ParamDesc *d = find_param(p.kind, refs[i].name);
+			if (!d || d->type != T_DOUBLE)
+				return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown double parameter: ") + refs[i].name);
+			int code = 0;
+			PF_TRY(gradient_code(p, refs[i].name, code));
+			host_refs[i] = refs[i].profile;
+			host_refs[nrefs + i] = (int)d->off;
+			host_refs[2 * nrefs + i] = code;
+		}
+		for (int i = 0; i < nrefs; i++)
+			bs.refs_key.emplace_back(refs[i].profile, m->profiles[refs[i].profile].kind,
+			                         m->profiles[refs[i].profile].rescale_flux, std::string(refs[i].name));
+	}
+	std::vector<double> current;
+	if (!values) {
+		current.resize(nrefs > 0 ? nrefs : 1);
+		for (int i = 0; i < nrefs; i++)
+			current[i] = *reinterpret_cast<const double *>(
+			    reinterpret_cast<const char *>(&m->profiles[host_refs[i]]) + host_refs[nrefs + i]);
+		values = current.data();
 	}
 	if (host_refs != bs.refs_host) {
 		PF_CUDA(ensure(bs.d_refs, host_refs.size() * 4 + 4));
@@ -1297,8 +1357,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	PF_CUDA(ensure(bs.h_values, (size_t)C * nrefs * 8 + 8));
 	PF_CUDA(ensure(bs.d_invalid, (size_t)C * 4));
 	PF_CUDA(ensure(bs.d_ll, (size_t)C * 8));
-	PF_CUDA(ensure(bs.d_out_ll, (size_t)C * 8));
-	PF_CUDA(ensure(bs.d_out_grad, (size_t)C * nrefs * 8 + 8));
+	PF_CUDA(ensure(bs.d_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
 	PF_CUDA(ensure(bs.d_T, (size_t)C * nprof * NTAN * 8));
 	PF_CUDA(ensure(bs.h_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
 	PF_CUDA(ensure(m->d_conv32, npix * C * 4));
@@ -1327,9 +1386,9 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	std::memcpy(bs.h_tmpl.p, m->profiles.data(), nprof * sizeof(ProfileParams));
 	const bool host_prologue = C * nprof <= HOST_PROLOGUE_MAX;
 	if (host_prologue) {
-		PF_CUDA(ensure(bs.h_dev, (size_t)C * nprof * sizeof(DevProfile)));
-		PF_CUDA(ensure(bs.h_fprof, (size_t)C * nprof * sizeof(FProfile)));
-		PF_CUDA(ensure(bs.h_invalid, (size_t)C * 4));
+		const StageLayout L(C, nprof);
+		PF_CUDA(ensure(bs.h_stage, L.total));
+		PF_CUDA(ensure(bs.d_stage, L.total));
 	}
 	const ModelGeom geom = geometry(m, a);
 
@@ -1342,9 +1401,10 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		std::memcpy(hv, values + (size_t)b0 * nrefs, (size_t)n * nrefs * 8);
 		for (int b = n; b < C; b++) std::memcpy(hv + (size_t)b * nrefs, values + (size_t)b0 * nrefs, (size_t)nrefs * 8);
 		if (host_prologue) {
-			DevProfile *hd = bs.h_dev.as<DevProfile>();
-			FProfile *hf = bs.h_fprof.as<FProfile>();
-			int *hi = bs.h_invalid.as<int>();
+			const StageLayout L(C, nprof);
+			DevProfile *hd = bs.h_stage.as<DevProfile>();
+			FProfile *hf = reinterpret_cast<FProfile *>(bs.h_stage.as<char>() + L.f);
+			int *hi = reinterpret_cast<int *>(bs.h_stage.as<char>() + L.inv);
 			for (int b = 0; b < C; b++) {
 				hi[b] = 0;
 				for (int p = 0; p < nprof; p++) {
@@ -1365,18 +1425,21 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		bool done = false;
 		for (int attempt = 0; attempt < 8 && !done; attempt++) {
 			QueueSet q;
-			PF_TRY(prepare_queue(m, a, npix * nprof * C, q, nullptr, nullptr, recompute));
+			// the pipeline zeroes the counters itself; they sit behind the
+			// results so that one copy brings both back
+			PF_TRY(prepare_queue(m, a, npix * nprof * C, q, nullptr, nullptr, recompute, false));
+			q.counts = reinterpret_cast<uint32_t *>(bs.d_out.as<char>() + (size_t)C * (1 + nrefs) * 8);
+			q.overflow = q.counts + MAX_LEVELS;
+			q.maxres = q.counts + MAX_LEVELS + 1;
 			std::vector<uint64_t> sig = graph_signature(m, a, true, q);
 			sig.push_back((uint64_t)C);
 			sig.push_back((uint64_t)nrefs);
 			sig.push_back((uint64_t)host_prologue);
 			sig.push_back((uint64_t)recompute);
 			sig.push_back((uint64_t)(uintptr_t)m->d_masks.p);
-			sig.push_back((uint64_t)(uintptr_t)bs.h_dev.p);
-			sig.push_back((uint64_t)(uintptr_t)bs.h_fprof.p);
-			sig.push_back((uint64_t)(uintptr_t)bs.h_invalid.p);
-			for (auto *buf : {&bs.d_tmpl, &bs.d_refs, &bs.d_values, &bs.d_dev, &bs.d_invalid, &bs.d_out_ll,
-			                  &bs.d_out_grad, &bs.d_ll, &bs.d_T})
+			sig.push_back((uint64_t)(uintptr_t)bs.h_stage.p);
+			for (auto *buf : {&bs.d_tmpl, &bs.d_refs, &bs.d_values, &bs.d_dev, &bs.d_invalid, &bs.d_out, &bs.d_ll,
+			                  &bs.d_T, &bs.d_stage})
 				sig.push_back((uint64_t)(uintptr_t)buf->p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_out.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_values.p);
@@ -1860,11 +1923,10 @@ int pf_model_loglike_grad(pf_model *m, const pf_param_ref *params, int n_params,
 {
 	if (!m || (n_params > 0 && (!params || !grad))) return set_error(PF_E_INVALID, "null argument");
 	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
-	// the current parameter values form a batch of one proposal
-	std::vector<double> vals(n_params > 0 ? n_params : 1);
-	for (int i = 0; i < n_params; i++) PF_TRY(pf_profile_get_double(m, params[i].profile, params[i].name, &vals[i]));
+	// the current parameter values form a batch of one proposal (values
+	// null: read from the profiles)
 	double ll = 0;
-	PF_TRY(eval_grad_batch(m, params, n_params, 1, vals.data(), &ll, grad));
+	PF_TRY(eval_grad_batch(m, params, n_params, 1, nullptr, &ll, grad));
 	if (!std::isfinite(ll)) return set_error(PF_E_INVALID, "invalid profile parameters");
 	if (loglike) *loglike = ll;
 	return PF_OK;
@@ -1947,6 +2009,7 @@ int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_para
 		const double *ll = m->h_results.as<double>();
 		if (loglike) *loglike = ll[0];
 		for (int i = 0; i < n_params; i++) grad[i] = (ll[1 + 2 * i] - ll[2 + 2 * i]) / (2 * steps[i]);
+		m->timings_lazy = false;
 		cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[3]);
 		cudaGetLastError();
 		return PF_OK;
@@ -2015,6 +2078,7 @@ int pf_model_level_counts(pf_model *m, int profile, int64_t *out, int max_levels
 int pf_model_last_timings(pf_model *m, float *ms, int n)
 {
 	if (!m || !ms) return set_error(PF_E_INVALID, "null argument");
+	if (m->timings_lazy) resolve_timings32(m);
 	for (int i = 0; i < n && i < 4; i++) ms[i] = m->timings[i];
 	return PF_OK;
 }
@@ -2049,7 +2113,7 @@ struct CatChunk {
 	unsigned W = 0, H = 0, pw = 0, ph = 0;
 	std::vector<int> members;           // galaxy indices
 	std::vector<int> member_grad_off;   // offset of each member's gradient in the chunk's buffer
-	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3;
+	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3, cusps = 0;
 	bool ak = false;
 	DevBuf data, sigma, region, psf32, psfrev32, prof_begin, prof_batch, grad_off, T, ll, grad;
 	HostBuf h_ll, h_grad, h_ctrl;
@@ -2185,7 +2249,10 @@ int cat_build(pf_catalogue *c)
 				goff.push_back(gtot);
 				gtot += 6 + shape_count(p.kind);
 				unsigned mr = p.max_recursions;
-				if (p.kind == PK_SERSIC && p.adjust && p.nser > 1) mr = std::max(mr, 10u);
+				if (p.kind == PK_SERSIC && p.adjust && p.nser > 1) {
+					mr = std::max(mr, 10u);
+					ch.cusps++;
+				}
 				ch.levels = std::max(ch.levels, (int)mr + 1);
 				ch.nt = std::max(ch.nt, tangent_count(p.kind));
 				if (p.kind != PK_SERSIC && p.kind != PK_MOFFAT) ch.ak = true;
@@ -2293,7 +2360,7 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
 	PF_CUDA(cudaMemsetAsync(ch.T.p, 0, (size_t)ch.nprof * NTAN * 8, s));
 	PF_CUDA(launch_pixels32(fprof, ch.prof_begin.as<int>(), C, a.dw, a.dh, 1.0, 1.0, conv, plain, jac, ch.nt, ch.ak, q,
 	                        s));
-	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, q, s));
+	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, ch.cusps, q, s));
 	const int kstride = (int)(ch.pw * ch.ph);
 	size_t sb = conv32_scratch_bytes(a.cw, a.ch, C);
 	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, ch.psfrev32.as<float>(), ch.pw, ch.ph, model64, a.cw, a.ch,

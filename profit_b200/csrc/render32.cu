@@ -362,9 +362,14 @@ __device__ __forceinline__ Tan<float> to_float(const Tan<T> &t)
 	return r;
 }
 
-// One thread per drawing pixel and per batch entry (blockIdx.z).  `model_of`
-// maps the profile range of each batch entry; profiles are FProfile records.
-template <bool AK>
+// One thread per drawing pixel and per batch entry (blockIdx.z); prof_begin
+// maps each batch entry to its range of FProfile records.  J: the tangents
+// are written to the planes `jac` (false: values only, the tangent arithmetic
+// is compiled out).  A profile whose rscale_max lies more than 2 px short of
+// the block's nearest pixel centre is skipped for the whole block: the
+// elliptical radius is never smaller than the Euclidean distance, so every
+// pixel of the block would take the zero decision.
+template <bool AK, bool J>
 __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__restrict__ prof_begin,
                            unsigned width, unsigned height, double sx, double sy, float *__restrict__ img_conv,
                            float *__restrict__ img_plain, float *__restrict__ jac, int nt, QueueSet q)
@@ -380,6 +385,11 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 	const double half_xbin = sx / 2., half_ybin = sy / 2.;
 	const double y = half_ybin + j * sx;
 	const double x = half_xbin + i * sy;
+	// pixel centres of this block (same expressions as x and y)
+	const unsigned tx0 = blockIdx.x * blockDim.x, ty0 = blockIdx.y * blockDim.y;
+	const unsigned tx1 = min(tx0 + blockDim.x - 1, width - 1), ty1 = min(ty0 + blockDim.y - 1, height - 1);
+	const double xlo = half_xbin + tx0 * sy, xhi = half_xbin + tx1 * sy;
+	const double ylo = half_ybin + ty0 * sx, yhi = half_ybin + ty1 * sx;
 
 	for (int pi = p0; pi < p1; pi++) {
 		const FProfile &p = profiles[pi];
@@ -388,41 +398,54 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 			continue;
 		}
 		if (!is_radial_kind(p.kind)) continue;
-		float xp, yp;
-		const int decision = pixel_decision32(p, x, y, xp, yp);
 		constexpr int NT = ntk<AK>();
 		float jl[NT];
 #pragma unroll
 		for (int k = 0; k < NT; k++) jl[k] = 0.f;
-		if (decision == PD_ZERO) {
-			// zero
+		bool culled = false;
+		if (p.r_max > 0.f) {  // block-uniform
+			const double nx = fmin(fmax(p.cx, xlo), xhi) - p.cx, ny = fmin(fmax(p.cy, ylo), yhi) - p.cy;
+			const double lim = (double)p.r_max + 2.0;
+			culled = nx * nx + ny * ny > lim * lim;
 		}
-		else if (decision == PD_DIRECT) {
-			Tan<float> t = eval_tan<float, AK>(p, xp, yp);
-			acc[p.target] += p.flux_scale * t.f;
-			tan_to_j<NT>(t, xp, yp, 1.0f, jl);
-		}
-		else {
-			unsigned res = p.resolution, max_rec = p.max_rec;
-			if (p.centre_override && fabs(x - p.cx) < p.img_sx && fabs(y - p.cy) < p.img_sy) {
-				res = 8;
-				max_rec = 10;
+		if (!culled) {
+			float xp, yp;
+			const int decision = pixel_decision32(p, x, y, xp, yp);
+			if (decision == PD_ZERO) {
+				// zero
 			}
-			SubItem it;
-			const double ddx = x - p.cx, ddy = y - p.cy;
-			it.x0 = ddx - half_xbin;
-			it.x1 = ddx + half_xbin;
-			it.y0 = ddy - half_ybin;
-			it.y1 = ddy + half_ybin;
-			it.weight = 1.0 / (res * res);
-			it.pixel = pix + (uint32_t)(b * npix);
-			it.profile = (uint16_t)pi;
-			it.res = (uint8_t)res;
-			it.max_rec = (uint8_t)max_rec;
-			queue_push(q, 0, it);
-			note_max_res(q, res);
+			else if (decision == PD_DIRECT) {
+				if constexpr (J) {
+					Tan<float> t = eval_tan<float, AK>(p, xp, yp);
+					acc[p.target] += p.flux_scale * t.f;
+					tan_to_j<NT>(t, xp, yp, 1.0f, jl);
+				}
+				else {
+					acc[p.target] += p.flux_scale * eval_val<float, AK>(p, xp, yp);
+				}
+			}
+			else {
+				unsigned res = p.resolution, max_rec = p.max_rec;
+				if (p.centre_override && fabs(x - p.cx) < p.img_sx && fabs(y - p.cy) < p.img_sy) {
+					res = 8;
+					max_rec = 10;
+				}
+				SubItem it;
+				const double ddx = x - p.cx, ddy = y - p.cy;
+				it.x0 = ddx - half_xbin;
+				it.x1 = ddx + half_xbin;
+				it.y0 = ddy - half_ybin;
+				it.y1 = ddy + half_ybin;
+				it.weight = 1.0 / (res * res);
+				it.pixel = pix + (uint32_t)(b * npix);
+				it.profile = (uint16_t)pi;
+				it.res = (uint8_t)res;
+				it.max_rec = (uint8_t)max_rec;
+				queue_push(q, 0, it);
+				note_max_res(q, res);
+			}
 		}
-		if (jac) {
+		if constexpr (J) {
 			float *jp = jac + (size_t)pi * nt * npix + pix;
 #pragma unroll
 			for (int k = 0; k < NT; k++)
@@ -435,7 +458,7 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 
 // Sub-points [base0, base1) of an item (multiples of 32), one per lane and
 // chunk.
-template <class T, bool AK>
+template <class T, bool AK, bool J>
 __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &it, int level, const double *s_xy,
                                              int lane, const QueueSet &q, float *sums, uint32_t *mask_out,
                                              unsigned base0, unsigned base1)
@@ -481,7 +504,8 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 				}
 			}
 			if (accepted) {
-				tan_to_j<ntk<AK>()>(to_float<T>(t), (float)xp, (float)yp, 1.0f, sums);
+				if constexpr (J) tan_to_j<ntk<AK>()>(to_float<T>(t), (float)xp, (float)yp, 1.0f, sums);
+				else sums[0] += (float)t.f;
 			}
 		}
 		const unsigned bits = __ballot_sync(0xffffffffu, accepted);
@@ -512,7 +536,9 @@ __device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem 
 
 // Sub-points [base0, base1) of one SubItem integrated by one warp (s_xy:
 // this warp's 32 doubles); FP64 sub-points from level 3 on (the Sersic cusp).
-template <bool Deep, bool AK>
+// J: tangents are accumulated into the planes `jac` (false: values only, the
+// tangent arithmetic is compiled out).
+template <bool Deep, bool AK, bool J>
 __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profiles, const SubItem &it, int level,
                                              unsigned npix, float *__restrict__ img_conv,
                                              float *__restrict__ img_plain, float *__restrict__ jac, int nt,
@@ -533,9 +559,9 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 	float sums[NT];
 #pragma unroll
 	for (int k = 0; k < NT; k++) sums[k] = 0.f;
-	if constexpr (Deep) level_points<double, AK>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
-	else level_points<float, AK>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
-	const int nk = tangent_count(p.kind);  // warp-uniform
+	if constexpr (Deep) level_points<double, AK, J>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
+	else level_points<float, AK, J>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
+	const int nk = J ? tangent_count(p.kind) : 1;  // warp-uniform
 #pragma unroll
 	for (int k = 0; k < NT; k++)
 		if (k < nk) sums[k] = warp_sum(sums[k]);
@@ -544,7 +570,7 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 		const uint32_t b = it.pixel / npix, pix = it.pixel - b * npix;
 		float *img = p.target == 0 ? img_conv : img_plain;
 		atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)sums[0]));
-		if (jac) {
+		if (J) {
 			float *jp = jac + (size_t)it.profile * nt * npix + pix;
 #pragma unroll
 			for (int k = 0; k < NT; k++)
@@ -554,7 +580,8 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 	__syncwarp();
 }
 
-template <bool AK>
+// Deep: FP64 sub-points (levels >= 3, the Sersic cusp).
+template <bool AK, bool J, bool Deep>
 __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
                                                  float *__restrict__ img_conv, float *__restrict__ img_plain,
                                                  float *__restrict__ jac, int nt, QueueSet q)
@@ -580,7 +607,7 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
 		const SubItem it = items[item];
 		const unsigned base0 = cpi == 1 ? 0u : chunk * 32, base1 = cpi == 1 ? 256u : base0 + 32;
 		if (base0 >= (unsigned)it.res * it.res) continue;
-		level32_item<false, AK>(profiles, it, level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
+		level32_item<Deep, AK, J>(profiles, it, level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
 		                    q.masks ? q.masks + ((size_t)q.off[level] + item) * MASK_WORDS : nullptr, base0,
 		                    base1);
 	}
@@ -590,7 +617,7 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
 // (max_recursions = 10) reaches these levels, a few hundred cells per level
 // at most, so one block walks them in order; __syncthreads separates the
 // levels, which makes every push of level L visible before level L+1 is read.
-template <bool AK>
+template <bool AK, bool J>
 __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restrict__ profiles, int first, int levels,
                                                         unsigned npix, float *__restrict__ img_conv,
                                                         float *__restrict__ img_plain, float *__restrict__ jac,
@@ -605,7 +632,7 @@ __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restric
 		const uint32_t n = min(*(volatile uint32_t *)&q.counts[level], q.cap[level]);
 		const SubItem *items = q.items + q.off[level];
 		for (uint32_t w = wib; w < n; w += nwarps)
-			level32_item<true, AK>(profiles, items[w], level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
+			level32_item<true, AK, J>(profiles, items[w], level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
 			                   q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr, 0, 256);
 	}
 }
@@ -848,30 +875,35 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
                             int nt, bool all_kinds, const QueueSet &q, cudaStream_t s)
 {
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8), batch);
-	if (all_kinds)
-		k_pixels32<true><<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac,
-		                                        nt, q);
-	else
-		k_pixels32<false><<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac,
-		                                         nt, q);
+	auto k = all_kinds ? (jac ? k_pixels32<true, true> : k_pixels32<true, false>)
+	                   : (jac ? k_pixels32<false, true> : k_pixels32<false, false>);
+	k<<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac, nt, q);
 	note_launches(1);
 	return cudaGetLastError();
 }
 
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
-                            float *jac, int nt, bool all_kinds, const QueueSet &q, cudaStream_t s)
+                            float *jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s)
 {
 	const int wide = n_levels < 3 ? n_levels : 3;
 	for (int l = 0; l < wide; l++) {
-		if (all_kinds) k_level32<true><<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
-		else k_level32<false><<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
+		auto k = all_kinds ? (jac ? k_level32<true, true, false> : k_level32<true, false, false>)
+		                   : (jac ? k_level32<false, true, false> : k_level32<false, false, false>);
+		k<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
 	}
 	note_launches(wide);
-	if (n_levels > wide) {
-		if (all_kinds)
-			k_deep_levels32<true><<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, nt, q);
-		else
-			k_deep_levels32<false><<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, nt, q);
+	if (n_levels > wide && cusps > DEEP_ONE_CTA_MAX_CUSPS) {
+		// many cusps (a large field, a batch): one grid-wide launch per level
+		auto k = all_kinds ? (jac ? k_level32<true, true, true> : k_level32<true, false, true>)
+		                   : (jac ? k_level32<false, true, true> : k_level32<false, false, true>);
+		for (int l = wide; l < n_levels; l++)
+			k<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
+		note_launches(n_levels - wide);
+	}
+	else if (n_levels > wide) {
+		auto k = all_kinds ? (jac ? k_deep_levels32<true, true> : k_deep_levels32<true, false>)
+		                   : (jac ? k_deep_levels32<false, true> : k_deep_levels32<false, false>);
+		k<<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, nt, q);
 		note_launches(1);
 	}
 	return cudaGetLastError();
