@@ -231,6 +231,7 @@ struct ConvVariant {
 struct ConvCandidate {
 	size_t (*smem)(int, int);
 	cudaError_t (*run)(const ConvArgs &, cudaStream_t);
+	bool tuned = true;  // false: only run when forced (PF_CONV_FORCE), never picked by the autotuner
 };
 
 cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag, const ConvArgs &a,

@@ -60,7 +60,7 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 		cudaStreamIsCapturing(s, &cap);
 		int first_fit = -1;
 		for (int c = 0; c < n_cands; c++)
-			if (cands[c].smem(a.kw, a.kh) <= 227 * 1024) {
+			if (cands[c].tuned && cands[c].smem(a.kw, a.kh) <= 227 * 1024) {
 				first_fit = c;
 				break;
 			}
@@ -77,7 +77,7 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 			const char *lv = getenv("PF_AUTOTUNE_LOG");
 			const bool log = lv && lv[0] == '1';
 			for (int c = 0; c < n_cands; c++) {
-				if (cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
+				if (!cands[c].tuned || cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
 				cudaError_t e = cands[c].run(a, s);  // warm-up (and attribute setup)
 				if (e != cudaSuccess) continue;
 				cudaEventRecord(e0, s);

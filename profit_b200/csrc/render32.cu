@@ -25,6 +25,7 @@
 #include "common.cuh"
 #include "conv.cuh"
 #include "conv2.cuh"
+#include "conv_tc.cuh"
 #include "launch.h"
 #include "like.cuh"
 
@@ -966,9 +967,24 @@ static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, 
 	    {Conv3Variant<TOut, 16, 8, 1, 2, 4>::smem, Conv3Variant<TOut, 16, 8, 1, 2, 4>::run},
 	    {Conv3Variant<TOut, 16, 8, 2, 2, 2>::smem, Conv3Variant<TOut, 16, 8, 2, 2, 2>::run},
 	    {Conv3Variant<TOut, 32, 8, 1, 4, 2>::smem, Conv3Variant<TOut, 32, 8, 1, 4, 2>::run},
+	    // taller tiles: fewer CTAs, so that one image's grid fits the resident
+	    // slots in one wave instead of leaving a partial second wave
+	    {Conv3Variant<TOut, 32, 10, 1, 8, 1>::smem, Conv3Variant<TOut, 32, 10, 1, 8, 1>::run},
+	    {Conv3Variant<TOut, 32, 12, 1, 8, 1>::smem, Conv3Variant<TOut, 32, 12, 1, 8, 1>::run},
+	    {Conv3Variant<TOut, 32, 6, 1, 8, 1>::smem, Conv3Variant<TOut, 32, 6, 1, 8, 1>::run},
+	    {Conv3Variant<TOut, 16, 10, 1, 8, 1>::smem, Conv3Variant<TOut, 16, 10, 1, 8, 1>::run},
 	    // one-column-per-lane kernels
 	    {ConvVariant<float, double, TOut, 8, 1, 8>::smem, ConvVariant<float, double, TOut, 8, 1, 8>::run},
 	    {ConvVariant<float, double, TOut, 8, 2, 4>::smem, ConvVariant<float, double, TOut, 8, 2, 4>::run},
+	    // tensor-core kernels (tcgen05, 3xTF32): 32 output columns per tile,
+	    // kernel rows split over 1, 2 or 4 CTAs.  Never picked by the
+	    // autotuner, only when forced: on a 400x400 image with a 51x51 PSF they
+	    // take 76-133 us against 35 us for the FMA kernels, and the tensor
+	    // cores' FP32 accumulation leaves logL ~2e-7 and single gradient
+	    // components up to ~9e-5 from the FP64 form (FMA kernels: 2e-8, 9e-6)
+	    {ConvTcVariant<TOut, 32, 1>::smem, ConvTcVariant<TOut, 32, 1>::run, false},
+	    {ConvTcVariant<TOut, 32, 2>::smem, ConvTcVariant<TOut, 32, 2>::run, false},
+	    {ConvTcVariant<TOut, 32, 4>::smem, ConvTcVariant<TOut, 32, 4>::run, false},
 	};
 	ConvArgs a{src, sw, sh, ox, oy, K, kw, kh, out, ow, oh, add, add_stride, add_ox, add_oy, batch,
 	           batch_src_stride, batch_out_stride, scratch, scratch_bytes, batch_k_stride};

@@ -204,7 +204,11 @@ def test_fp32_image_close_to_fp64(wl):
 
 
 # Number of FP32 convolution kernels the autotuner chooses from (render32.cu).
-N_FP32_CONV_CANDIDATES = 16
+N_FP32_CONV_CANDIDATES = 23
+# candidates from this index on run on the tensor cores (3xTF32 split
+# products): their FP32-level sums differ from the FMA kernels' by a few
+# 1e-7 of logL, so logL is compared at 1e-6 there
+FIRST_TC_CONV_CANDIDATE = 20
 
 
 @pytest.mark.parametrize("cand", range(N_FP32_CONV_CANDIDATES))
@@ -231,14 +235,15 @@ def test_every_fp32_convolution_candidate(cand, monkeypatch):
     assert _rel(img, ref) <= 1e-6
     one = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), props[0])
     one.set_data(image, sigma)
+    ll_rel = 1e-6 if cand >= FIRST_TC_CONV_CANDIDATE else 1e-7
     for _ in range(2):  # eager, then graph replay
         ll, g = one.loglike_grad(refs)
-        assert ll == pytest.approx(ll0, rel=1e-7)
+        assert ll == pytest.approx(ll0, rel=ll_rel)
         np.testing.assert_allclose(g, g0, rtol=1e-5, atol=1e-6 * np.max(np.abs(g0)))
     mb = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
     mb.set_data(image, sigma)
     ll_b, g_b = mb.loglike_grad_batch(refs, vals)
-    assert ll_b[0] == pytest.approx(ll0, rel=1e-7)
+    assert ll_b[0] == pytest.approx(ll0, rel=ll_rel)
     np.testing.assert_allclose(g_b[0], g0, rtol=1e-5, atol=1e-6 * np.max(np.abs(g0)))
     for s in (1, 2):
         p = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), props[s])
