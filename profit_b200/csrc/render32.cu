@@ -833,11 +833,27 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
 	__syncthreads();
 	if (!s_last) return;
 	__threadfence();
+	// the last block merges the partials with all its threads: thread t adds
+	// blocks t, t + 256, ... in order, then warps and the block reduce in a
+	// fixed order, so the result still does not depend on scheduling
+	const volatile double *all = partials + (size_t)pi * gridDim.x * NTAN;
+	double v[NT];
+#pragma unroll
+	for (int k = 0; k < NT; k++) v[k] = 0.0;
+	for (unsigned blk = threadIdx.x; blk < gridDim.x; blk += blockDim.x)
+#pragma unroll
+		for (int k = 0; k < NT; k++)
+			if (k < nk) v[k] += all[(size_t)blk * NTAN + k];
+#pragma unroll
+	for (int k = 0; k < NT; k++) {
+		const double w = warp_sum(v[k]);
+		if (lane == 0) s_red[k][wid] = w;
+	}
+	__syncthreads();
 	if (threadIdx.x < NT) {
-		const double *all = partials + (size_t)pi * gridDim.x * NTAN;
-		double v = 0;
-		for (unsigned blk = 0; blk < gridDim.x; blk++) v += ((volatile const double *)all)[blk * NTAN + threadIdx.x];
-		out[(size_t)pi * NTAN + threadIdx.x] = v;
+		double t = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_red[threadIdx.x][w];
+		out[(size_t)pi * NTAN + threadIdx.x] = t;
 	}
 	if (threadIdx.x == 0) tickets[pi] = 0;
 }
