@@ -8,6 +8,37 @@
 
 namespace pf {
 
+// Programmatic dependent launch.  The kernels of the FP32 pipeline are
+// launched with programmatic stream serialisation (launch_pdl): the next
+// kernel of the stream may be scheduled onto free SM slots while this one
+// runs, and it waits in griddepcontrol.wait until this grid has finished and
+// its writes are visible, which hides the launch gap between dependent
+// kernels.  Every kernel launched that way calls pdl_enter() before its first
+// access to memory that an earlier kernel of the stream writes or reads; for
+// an ordinary launch both instructions are no-ops.
+__device__ __forceinline__ void pdl_enter()
+{
+	asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+	asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                              Args... args)
+{
+	cudaLaunchConfig_t cfg = {};
+	cfg.gridDim = grid;
+	cfg.blockDim = block;
+	cfg.dynamicSmemBytes = smem;
+	cfg.stream = s;
+	cudaLaunchAttribute attr[1];
+	attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+	attr[0].val.programmaticStreamSerializationAllowed = 1;
+	cfg.attrs = attr;
+	cfg.numAttrs = 1;
+	return cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Tangent slots per radial profile: f, df/dx', df/dy', df/dx' y', df/dy' x',
 // df/dy' y', then the shape-parameter partials (per kind, shape_count of
 // them) and df/dbox.  Models whose profiles need fewer slots store fewer

@@ -158,6 +158,8 @@ __global__ void __launch_bounds__(32 * TYT * KS)
 			cp_async4_zfill(d, g, v);
 			cp_async4_zfill(d + 1, g, v);
 		}
+	// the kernel taps are static; the source is the previous kernel's output
+	pdl_enter();
 	for (int ty = wid; ty < th; ty += NWARPS) {
 		const int sy = j0 + oy + ty;
 		const bool rv = sy >= 0 && sy < sh;
@@ -256,6 +258,7 @@ __global__ void k_conv_split_sum(const double *__restrict__ part, int ksplit, TO
                                  int batch, const float *__restrict__ add, int add_stride, int add_ox, int add_oy,
                                  int batch_src_stride, int batch_out_stride)
 {
+	pdl_enter();
 	const size_t n = (size_t)ow * oh;
 	for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n * batch; t += (size_t)gridDim.x * blockDim.x) {
 		const size_t b = t / n, p = t - b * n;
@@ -288,18 +291,21 @@ struct Conv3Variant {
 		}
 		dim3 block(32, TYT, KS);
 		dim3 grid((a.ow + S::TX - 1) / S::TX, (a.oh + S::TY - 1) / S::TY, a.batch * KSPLIT);
-		k_conv3_tile<TOut, HL, RY, TYT, KS, KSPLIT><<<grid, block, smem, s>>>(
-		    static_cast<const float *>(a.src), a.sw, a.sh, a.ox, a.oy, static_cast<const float *>(a.K), a.kw, a.kh,
-		    static_cast<TOut *>(a.out), a.ow, a.oh, static_cast<const float *>(a.add), a.add_stride, a.add_ox,
-		    a.add_oy, a.batch_src_stride, a.batch_out_stride, a.batch_k_stride, static_cast<double *>(a.scratch));
+		cudaError_t e = launch_pdl(
+		    k_conv3_tile<TOut, HL, RY, TYT, KS, KSPLIT>, grid, block, smem, s, static_cast<const float *>(a.src), a.sw,
+		    a.sh, a.ox, a.oy, static_cast<const float *>(a.K), a.kw, a.kh, static_cast<TOut *>(a.out), a.ow, a.oh,
+		    static_cast<const float *>(a.add), a.add_stride, a.add_ox, a.add_oy, a.batch_src_stride,
+		    a.batch_out_stride, a.batch_k_stride, static_cast<double *>(a.scratch));
+		if (e != cudaSuccess) return e;
 		if (KSPLIT > 1) {
 			size_t n = (size_t)a.ow * a.oh * a.batch;
 			int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 8);
-			k_conv_split_sum<TOut><<<blocks, 256, 0, s>>>(static_cast<const double *>(a.scratch), KSPLIT,
-			                                              static_cast<TOut *>(a.out), a.ow, a.oh, a.batch,
-			                                              static_cast<const float *>(a.add), a.add_stride, a.add_ox,
-			                                              a.add_oy, a.batch_src_stride, a.batch_out_stride);
+			e = launch_pdl(k_conv_split_sum<TOut>, dim3(blocks), dim3(256), 0, s,
+			               static_cast<const double *>(a.scratch), KSPLIT, static_cast<TOut *>(a.out), a.ow, a.oh,
+			               a.batch, static_cast<const float *>(a.add), a.add_stride, a.add_ox, a.add_oy,
+			               a.batch_src_stride, a.batch_out_stride);
 			note_launches(1);
+			if (e != cudaSuccess) return e;
 		}
 		return cudaGetLastError();
 	}

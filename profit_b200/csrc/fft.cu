@@ -28,6 +28,7 @@
 #include <mutex>
 #include <vector>
 
+#include "common.cuh"
 #include "fft.h"
 
 namespace pf {
@@ -237,6 +238,7 @@ __global__ void k_fft_rows_fwd(const TIn *__restrict__ src, int sw, int sh, int 
                                const typename Cx<T>::type *__restrict__ tw, typename Cx<T>::type *__restrict__ spec,
                                int spec_ld, size_t src_batch, size_t spec_batch)
 {
+	pdl_enter();
 	using C = typename Cx<T>::type;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *a = reinterpret_cast<C *>(smem_raw);
@@ -297,6 +299,7 @@ __global__ void k_fft_cols(typename Cx<T>::type *__restrict__ spec, int spec_ld,
                            const typename Cx<T>::type *__restrict__ tw, const typename Cx<T>::type *__restrict__ K,
                            int mode, size_t spec_batch, bool k_smem)
 {
+	pdl_enter();
 	using C = typename Cx<T>::type;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *a = reinterpret_cast<C *>(smem_raw);
@@ -359,6 +362,7 @@ __global__ void k_fft_rows_inv(const typename Cx<T>::type *__restrict__ spec, in
                                int ow, int oh, const TAdd *__restrict__ add, int add_stride, int add_ox, int add_oy,
                                size_t spec_batch, size_t out_batch, size_t add_batch)
 {
+	pdl_enter();
 	using C = typename Cx<T>::type;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	C *a = reinterpret_cast<C *>(smem_raw);
@@ -543,8 +547,8 @@ static cudaError_t launch_cols(typename Cx<T>::type *spec, int spec_ld, int ncol
 	if (!configured[tws]) configured[tws] = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                                                               FFT_SMEM_BYTES) == cudaSuccess;
 	dim3 grid((ncols + CB - 1) / CB, batch);
-	kern<<<grid, fft_threads(pm, CB), smem, s>>>(spec, spec_ld, ncols, M, pm, tw, K, mode, spec_batch, ks);
-	return cudaGetLastError();
+	return launch_pdl(kern, grid, dim3(fft_threads(pm, CB)), smem, s, spec, spec_ld, ncols, M, pm, tw, K, mode,
+	                  spec_batch, ks);
 }
 
 template <class T>
@@ -588,9 +592,8 @@ cudaError_t FftConv<T>::forward_rows(const TIn *src, int sw, int sh, int sx0, in
 	static bool configured[2] = {false, false};  // per instantiation; setting it twice is harmless
 	if (!configured[tws]) configured[tws] = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                                                               FFT_SMEM_BYTES) == cudaSuccess;
-	kern<<<grid, fft_threads(plan_n, 1), smem, s>>>(src, sw, sh, sx0, sy0, N, plan_n, tw_n, spec, ld, src_batch,
-	                                                (size_t)M * ld);
-	return cudaGetLastError();
+	return launch_pdl(kern, grid, dim3(fft_threads(plan_n, 1)), smem, s, src, sw, sh, sx0, sy0, N, plan_n, tw_n, spec,
+	                  ld, src_batch, (size_t)M * ld);
 }
 
 template <class T>
@@ -621,9 +624,8 @@ cudaError_t FftConv<T>::convolve(const TIn *src, int sw, int sh, int sx0, int sy
 	static bool configured[2] = {false, false};  // per instantiation; setting it twice is harmless
 	if (!configured[tws]) configured[tws] = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
 	                                                               FFT_SMEM_BYTES) == cudaSuccess;
-	kern<<<grid, fft_threads(plan_n, 1), smem, s>>>(work, ld, N, M, plan_n, tw_n, dx, dy, out, ow, oh, add, add_stride,
-	                                                add_ox, add_oy, (size_t)M * ld, out_batch, add_batch);
-	return cudaGetLastError();
+	return launch_pdl(kern, grid, dim3(fft_threads(plan_n, 1)), smem, s, (const Cplx *)work, ld, N, M, plan_n, tw_n, dx,
+	                  dy, out, ow, oh, add, add_stride, add_ox, add_oy, (size_t)M * ld, out_batch, add_batch);
 }
 
 template struct FftConv<double>;

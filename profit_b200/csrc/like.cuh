@@ -11,6 +11,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "common.cuh"
+
 namespace pf {
 
 struct Neumaier {
@@ -77,6 +79,7 @@ __global__ void k_loglike_partial(const T *__restrict__ model, const double *__r
                                   double2 *__restrict__ partials, float *__restrict__ wseed,
                                   int data_batch_stride)
 {
+	pdl_enter();
 	const int b = blockIdx.y;
 	model += (size_t)b * n;
 	data += (size_t)b * data_batch_stride;
@@ -101,6 +104,7 @@ __global__ void k_loglike_partial(const T *__restrict__ model, const double *__r
 
 static __global__ void k_loglike_final(const double2 *__restrict__ partials, int nparts, double *__restrict__ out)
 {
+	pdl_enter();
 	const int b = blockIdx.x;
 	Neumaier acc{0.0, 0.0};
 	for (int k = threadIdx.x; k < nparts; k += blockDim.x) {

@@ -75,6 +75,7 @@ __global__ void k_like_stats(const double *__restrict__ model, const double *__r
                              const double *__restrict__ sigma, const uint8_t *__restrict__ region, int n,
                              int data_batch_stride, double *__restrict__ partials)
 {
+	pdl_enter();
 	const int b = blockIdx.y;
 	model += (size_t)b * n;
 	data += (size_t)b * data_batch_stride;
@@ -122,6 +123,7 @@ __global__ void k_like_stats(const double *__restrict__ model, const double *__r
 // Merges the pass-1 partials of each image (blockIdx.x) in block order.
 __global__ void k_like_stats_final(const double *__restrict__ partials, int nparts, double *__restrict__ stats)
 {
+	pdl_enter();
 	const int b = blockIdx.x;
 	if (threadIdx.x != 0) return;
 	Neumaier a0{0, 0}, a1{0, 0}, a2{0, 0};
@@ -148,6 +150,7 @@ __global__ void k_like_terms(const double *__restrict__ model, const double *__r
                              int data_batch_stride, const double *__restrict__ stats, double2 *__restrict__ partials,
                              float *__restrict__ wseed)
 {
+	pdl_enter();
 	const int b = blockIdx.y;
 	model += (size_t)b * n;
 	data += (size_t)b * data_batch_stride;
@@ -205,6 +208,7 @@ template <int KIND>
 __global__ void k_like_terms_final(const double2 *__restrict__ partials, int nparts, const double *__restrict__ stats,
                                    double *__restrict__ out, double *__restrict__ coef)
 {
+	pdl_enter();
 	const int b = blockIdx.x;
 	if (threadIdx.x != 0) return;
 	Neumaier a0{0, 0}, a1{0, 0};
@@ -246,6 +250,7 @@ __global__ void k_like_t_seed(const double *__restrict__ model, const double *__
                               int data_batch_stride, const double *__restrict__ stats, const double *__restrict__ coef,
                               float *__restrict__ wseed)
 {
+	pdl_enter();
 	const int b = blockIdx.y;
 	model += (size_t)b * n;
 	data += (size_t)b * data_batch_stride;

@@ -375,6 +375,7 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
                            unsigned width, unsigned height, double sx, double sy, float *__restrict__ img_conv,
                            float *__restrict__ img_plain, float *__restrict__ jac, int nt, QueueSet q)
 {
+	pdl_enter();
 	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
 	const unsigned j = blockIdx.y * blockDim.y + threadIdx.y;
 	const int b = blockIdx.z;
@@ -587,6 +588,7 @@ __global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ pr
                                                  float *__restrict__ img_conv, float *__restrict__ img_plain,
                                                  float *__restrict__ jac, int nt, QueueSet q)
 {
+	pdl_enter();
 	__shared__ double s_xy[8][32];
 	const int lane = threadIdx.x & 31;
 	const int wib = threadIdx.x >> 5;
@@ -624,6 +626,7 @@ __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restric
                                                         float *__restrict__ img_plain, float *__restrict__ jac,
                                                         int nt, QueueSet q)
 {
+	pdl_enter();
 	__shared__ double s_xy[16][32];
 	const int lane = threadIdx.x & 31;
 	const int wib = threadIdx.x >> 5;
@@ -656,6 +659,7 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
                                                           const float *__restrict__ g_conv,
                                                           const float *__restrict__ g_plain, double *__restrict__ T)
 {
+	pdl_enter();
 	const int pi = blockIdx.z;
 	const FProfile &p = profiles[pi];
 	if (!is_radial_kind(p.kind)) return;
@@ -709,6 +713,7 @@ __global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restr
                                                          const float *__restrict__ g_plain, QueueSet q,
                                                          double *__restrict__ T)
 {
+	pdl_enter();
 	__shared__ double s_xy[8][32];
 	const int lane = threadIdx.x & 31;
 	const int wib = threadIdx.x >> 5;
@@ -756,16 +761,12 @@ cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_b
                                      int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s)
 {
 	dim3 grid((width + 63) / 64, (height + 31) / 32, n_profiles);
-	if (all_kinds) {
-		k_adjoint_pixels32<true><<<grid, 256, 0, s>>>(profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
-		k_adjoint_items32<true><<<148 * 8, 256, 0, s>>>(profiles, levels, g_conv, g_plain, q, T);
-	}
-	else {
-		k_adjoint_pixels32<false><<<grid, 256, 0, s>>>(profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
-		k_adjoint_items32<false><<<148 * 8, 256, 0, s>>>(profiles, levels, g_conv, g_plain, q, T);
-	}
+	auto kp = all_kinds ? k_adjoint_pixels32<true> : k_adjoint_pixels32<false>;
+	auto ki = all_kinds ? k_adjoint_items32<true> : k_adjoint_items32<false>;
+	cudaError_t e = launch_pdl(kp, grid, dim3(256), 0, s, profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
+	if (e == cudaSuccess) e = launch_pdl(ki, dim3(148 * 8), dim3(256), 0, s, profiles, levels, g_conv, g_plain, q, T);
 	note_launches(2);
-	return cudaGetLastError();
+	return e;
 }
 
 // sum over pixels of g(pixel) * J_k(pixel) for each radial profile:
@@ -783,6 +784,7 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
                                                     double *__restrict__ partials, unsigned *__restrict__ tickets,
                                                     double *__restrict__ out)
 {
+	pdl_enter();
 	constexpr int U = 4;
 	const int pi = blockIdx.y;
 	const FProfile &p = profiles[pi];
@@ -863,6 +865,7 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
 __global__ void k_embed_seed(const float *__restrict__ w, unsigned ow, unsigned oh, unsigned padx, unsigned pady,
                              unsigned dw, unsigned dh, float *__restrict__ g_plain)
 {
+	pdl_enter();
 	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
 	const unsigned j = blockIdx.y * blockDim.y + threadIdx.y;
 	const int b = blockIdx.z;
@@ -876,6 +879,7 @@ __global__ void k_crop32(const float *__restrict__ src, unsigned sw, unsigned ox
                          float *__restrict__ out, unsigned ow, unsigned oh, const float *__restrict__ add,
                          unsigned src_stride)
 {
+	pdl_enter();
 	unsigned i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y * blockDim.y + threadIdx.y;
 	const int b = blockIdx.z;
 	if (i >= ow || j >= oh) return;
@@ -894,9 +898,9 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8), batch);
 	auto k = all_kinds ? (jac ? k_pixels32<true, true> : k_pixels32<true, false>)
 	                   : (jac ? k_pixels32<false, true> : k_pixels32<false, false>);
-	k<<<grid, block, 0, s>>>(profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac, nt, q);
 	note_launches(1);
-	return cudaGetLastError();
+	return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac, nt,
+	                  q);
 }
 
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
@@ -906,22 +910,28 @@ cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npi
 	for (int l = 0; l < wide; l++) {
 		auto k = all_kinds ? (jac ? k_level32<true, true, false> : k_level32<true, false, false>)
 		                   : (jac ? k_level32<false, true, false> : k_level32<false, false, false>);
-		k<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
+		cudaError_t e = launch_pdl(k, dim3(148 * 8), dim3(256), 0, s, profiles, l, npix, img_conv, img_plain, jac, nt, q);
+		if (e != cudaSuccess) return e;
 	}
 	note_launches(wide);
 	if (n_levels > wide && cusps > DEEP_ONE_CTA_MAX_CUSPS) {
 		// many cusps (a large field, a batch): one grid-wide launch per level
 		auto k = all_kinds ? (jac ? k_level32<true, true, true> : k_level32<true, false, true>)
 		                   : (jac ? k_level32<false, true, true> : k_level32<false, false, true>);
-		for (int l = wide; l < n_levels; l++)
-			k<<<148 * 8, 256, 0, s>>>(profiles, l, npix, img_conv, img_plain, jac, nt, q);
+		for (int l = wide; l < n_levels; l++) {
+			cudaError_t e =
+			    launch_pdl(k, dim3(148 * 8), dim3(256), 0, s, profiles, l, npix, img_conv, img_plain, jac, nt, q);
+			if (e != cudaSuccess) return e;
+		}
 		note_launches(n_levels - wide);
 	}
 	else if (n_levels > wide) {
 		auto k = all_kinds ? (jac ? k_deep_levels32<true, true> : k_deep_levels32<true, false>)
 		                   : (jac ? k_deep_levels32<false, true> : k_deep_levels32<false, false>);
-		k<<<1, 512, 0, s>>>(profiles, wide, n_levels, npix, img_conv, img_plain, jac, nt, q);
+		cudaError_t e = launch_pdl(k, dim3(1), dim3(512), 0, s, profiles, wide, n_levels, npix, img_conv, img_plain, jac,
+		                           nt, q);
 		note_launches(1);
+		if (e != cudaSuccess) return e;
 	}
 	return cudaGetLastError();
 }
@@ -939,22 +949,19 @@ cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float
                               unsigned *tickets, double *out, cudaStream_t s)
 {
 	const unsigned bx = jac_reduce_blocks(npix, n_profiles);
-	if (nt <= 9)
-		k_jac_reduce<9><<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, nt,
-		                                                     partials, tickets, out);
-	else
-		k_jac_reduce<NTAN><<<dim3(bx, n_profiles), 256, 0, s>>>(jac, g_conv, g_plain, profiles, prof_batch, npix, nt,
-		                                                        partials, tickets, out);
+	auto k = nt <= 9 ? k_jac_reduce<9> : k_jac_reduce<NTAN>;
 	note_launches(1);
-	return cudaGetLastError();
+	return launch_pdl(k, dim3(bx, n_profiles), dim3(256), 0, s, jac, g_conv, g_plain, profiles, prof_batch, npix, nt,
+	                  partials, tickets, out);
 }
 
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
                               unsigned dh, int batch, float *g_plain, cudaStream_t s)
 {
 	dim3 block(32, 8), grid(cdiv(dw, 32), cdiv(dh, 8), batch);
-	k_embed_seed<<<grid, block, 0, s>>>(w, ow, oh, padx, pady, dw, dh, g_plain);
+	cudaError_t e = launch_pdl(k_embed_seed, grid, block, 0, s, w, ow, oh, padx, pady, dw, dh, g_plain);
 	note_launches(1);
+	if (e != cudaSuccess) return e;
 	return cudaGetLastError();
 }
 
@@ -1035,20 +1042,19 @@ cudaError_t launch_loglike32(const float *model, const double *data, const doubl
                              int n, int batch, int data_batch_stride, double2 *partials, int nparts, double *out,
                              float *wseed, cudaStream_t s)
 {
-	k_loglike_partial<float><<<dim3(nparts, batch), 256, 0, s>>>(model, data, sigma, region, n, partials, wseed,
-	                                                             data_batch_stride);
-	k_loglike_final<<<batch, 256, 0, s>>>(partials, nparts, out);
+	cudaError_t e = launch_pdl(k_loglike_partial<float>, dim3(nparts, batch), dim3(256), 0, s, model, data, sigma,
+	                           region, n, partials, wseed, data_batch_stride);
+	if (e == cudaSuccess) e = launch_pdl(k_loglike_final, dim3(batch), dim3(256), 0, s, partials, nparts, out);
 	note_launches(2);
-	return cudaGetLastError();
+	return e;
 }
 
 cudaError_t launch_crop32(const float *src, unsigned sw, unsigned ox, unsigned oy, float *out, unsigned ow,
                           unsigned oh, const float *add, int batch, unsigned src_stride, cudaStream_t s)
 {
 	dim3 block(32, 8), grid(cdiv(ow, 32), cdiv(oh, 8), batch);
-	k_crop32<<<grid, block, 0, s>>>(src, sw, ox, oy, out, ow, oh, add, src_stride);
 	note_launches(1);
-	return cudaGetLastError();
+	return launch_pdl(k_crop32, grid, block, 0, s, src, sw, ox, oy, out, ow, oh, add, src_stride);
 }
 
 // ---------------------------------------------------------------------------
@@ -1065,6 +1071,7 @@ __global__ void k_batch_prologue(const ProfileParams *__restrict__ tmpl, int npr
                                  const double *__restrict__ values, ModelGeom g, DevProfile *__restrict__ dev,
                                  FProfile *__restrict__ fprof, int *__restrict__ invalid)
 {
+	pdl_enter();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= batch * nprof) return;
 	const int b = t / nprof, p = t - b * nprof;
@@ -1089,6 +1096,7 @@ __global__ void k_batch_gradient(const DevProfile *__restrict__ dev, int nprof, 
                                  const double *__restrict__ T, const double *__restrict__ ll, const int *__restrict__ invalid,
                                  double *__restrict__ out_ll, double *__restrict__ out_grad)
 {
+	pdl_enter();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t < batch) out_ll[t] = invalid[t] ? -INFINITY : ll[t];
 	if (t >= batch * nrefs) return;
@@ -1102,10 +1110,9 @@ cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batc
                                   DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s)
 {
 	int n = batch * nprof;
-	k_batch_prologue<<<(n + 127) / 128, 128, 0, s>>>(tmpl, nprof, batch, ref_profile, ref_offset, nrefs, values, g,
-	                                                 dev, fprof, invalid);
 	note_launches(1);
-	return cudaGetLastError();
+	return launch_pdl(k_batch_prologue, dim3((n + 127) / 128), dim3(128), 0, s, tmpl, nprof, batch, ref_profile,
+	                  ref_offset, nrefs, values, g, dev, fprof, invalid);
 }
 
 cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, const int *ref_profile,
@@ -1113,10 +1120,9 @@ cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, c
                                   const int *invalid, double *out_ll, double *out_grad, cudaStream_t s)
 {
 	int n = batch * (nrefs > 1 ? nrefs : 1);
-	k_batch_gradient<<<(n + 255) / 256, 256, 0, s>>>(dev, nprof, batch, ref_profile, ref_code, nrefs, T, ll, invalid,
-	                                                 out_ll, out_grad);
 	note_launches(1);
-	return cudaGetLastError();
+	return launch_pdl(k_batch_gradient, dim3((n + 255) / 256), dim3(256), 0, s, dev, nprof, batch, ref_profile,
+	                  ref_code, nrefs, T, ll, invalid, out_ll, out_grad);
 }
 
 // Catalogue batches: every galaxy brings its own profiles, so the prologue
@@ -1126,6 +1132,7 @@ cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, c
 __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const int2 *__restrict__ pad, int n,
                                ModelGeom g, DevProfile *__restrict__ dev, FProfile *__restrict__ fprof)
 {
+	pdl_enter();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n) return;
 	const ProfileParams pp = params[t];
@@ -1143,6 +1150,7 @@ __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const i
 __global__ void k_cat_gradient(const DevProfile *__restrict__ dev, int n, const double *__restrict__ T,
                                const int *__restrict__ grad_off, double *__restrict__ grad)
 {
+	pdl_enter();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= n) return;
 	const DevProfile &d = dev[t];
@@ -1157,28 +1165,26 @@ __global__ void k_cat_gradient(const DevProfile *__restrict__ dev, int n, const 
 cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, int n, const ModelGeom &g,
                                 DevProfile *dev, FProfile *fprof, cudaStream_t s)
 {
-	k_cat_prologue<<<(n + 63) / 64, 64, 0, s>>>(params, pad, n, g, dev, fprof);
 	note_launches(1);
-	return cudaGetLastError();
+	return launch_pdl(k_cat_prologue, dim3((n + 63) / 64), dim3(64), 0, s, params, pad, n, g, dev, fprof);
 }
 
 cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,
                                 cudaStream_t s)
 {
-	k_cat_gradient<<<(n + 127) / 128, 128, 0, s>>>(dev, n, T, grad_off, grad);
 	note_launches(1);
-	return cudaGetLastError();
+	return launch_pdl(k_cat_gradient, dim3((n + 127) / 128), dim3(128), 0, s, dev, n, T, grad_off, grad);
 }
 
 cudaError_t launch_loglike64_batch(const double *model, const double *data, const double *sigma,
                                    const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
                                    int nparts, double *out, float *wseed, cudaStream_t s)
 {
-	k_loglike_partial<double><<<dim3(nparts, batch), 256, 0, s>>>(model, data, sigma, region, n, partials, wseed,
-	                                                              data_batch_stride);
-	k_loglike_final<<<batch, 256, 0, s>>>(partials, nparts, out);
+	cudaError_t e = launch_pdl(k_loglike_partial<double>, dim3(nparts, batch), dim3(256), 0, s, model, data, sigma,
+	                           region, n, partials, wseed, data_batch_stride);
+	if (e == cudaSuccess) e = launch_pdl(k_loglike_final, dim3(batch), dim3(256), 0, s, partials, nparts, out);
 	note_launches(2);
-	return cudaGetLastError();
+	return e;
 }
 
 }  // namespace pf

@@ -428,48 +428,60 @@ cudaError_t launch_like64(int kind, const double *model, const double *data, con
                           const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
                           int nparts, double *stats, double *out, float *wseed, cudaStream_t s)
 {
-	const dim3 grid(nparts, batch);
+	// launched with programmatic serialisation: these kernels run inside the
+	// FP32 pipeline's graph right after the convolution
+	const dim3 grid(nparts, batch), b256(256), b32(32), gb(batch);
+	cudaError_t e = cudaSuccess;
+	auto go = [&](cudaError_t r) {
+		if (e == cudaSuccess) e = r;
+	};
 	if (kind == LIKE_NORM) {
-		k_loglike_partial<double><<<grid, 256, 0, s>>>(model, data, sigma, region, n, partials, wseed,
-		                                               data_batch_stride);
-		k_loglike_final<<<batch, 256, 0, s>>>(partials, nparts, out);
+		go(launch_pdl(k_loglike_partial<double>, grid, b256, 0, s, model, data, sigma, region, n, partials, wseed,
+		              data_batch_stride));
+		go(launch_pdl(k_loglike_final, gb, b256, 0, s, (const double2 *)partials, nparts, out));
 		note_launches(2);
-		return cudaGetLastError();
+		return e;
 	}
 	double *p1 = reinterpret_cast<double *>(partials);
 	double *coef = stats + (size_t)batch * LIKE_STATS;
 	switch (kind) {
 	case LIKE_CHISQ:
-		k_like_stats<LIKE_CHISQ><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, p1);
-		k_like_stats_final<<<batch, 32, 0, s>>>(p1, nparts, stats);
-		k_like_terms<LIKE_CHISQ><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats,
-		                                               partials, wseed);
-		k_like_terms_final<LIKE_CHISQ><<<batch, 32, 0, s>>>(partials, nparts, stats, out, coef);
+		go(launch_pdl(k_like_stats<LIKE_CHISQ>, grid, b256, 0, s, model, data, sigma, region, n, data_batch_stride,
+		              p1));
+		go(launch_pdl(k_like_stats_final, gb, b32, 0, s, (const double *)p1, nparts, stats));
+		go(launch_pdl(k_like_terms<LIKE_CHISQ>, grid, b256, 0, s, model, data, sigma, region, n, data_batch_stride,
+		              (const double *)stats, partials, wseed));
+		go(launch_pdl(k_like_terms_final<LIKE_CHISQ>, gb, b32, 0, s, (const double2 *)partials, nparts,
+		              (const double *)stats, out, coef));
 		note_launches(4);
 		break;
 	case LIKE_T:
-		k_like_stats<LIKE_T><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, p1);
-		k_like_stats_final<<<batch, 32, 0, s>>>(p1, nparts, stats);
-		k_like_terms<LIKE_T><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats, partials,
-		                                           nullptr);
-		k_like_terms_final<LIKE_T><<<batch, 32, 0, s>>>(partials, nparts, stats, out, coef);
+		go(launch_pdl(k_like_stats<LIKE_T>, grid, b256, 0, s, model, data, sigma, region, n, data_batch_stride, p1));
+		go(launch_pdl(k_like_stats_final, gb, b32, 0, s, (const double *)p1, nparts, stats));
+		go(launch_pdl(k_like_terms<LIKE_T>, grid, b256, 0, s, model, data, sigma, region, n, data_batch_stride,
+		              (const double *)stats, partials, (float *)nullptr));
+		go(launch_pdl(k_like_terms_final<LIKE_T>, gb, b32, 0, s, (const double2 *)partials, nparts,
+		              (const double *)stats, out, coef));
 		note_launches(4);
 		if (wseed) {
-			k_like_t_seed<<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats, coef, wseed);
+			go(launch_pdl(k_like_t_seed, grid, b256, 0, s, model, data, sigma, region, n, data_batch_stride,
+			              (const double *)stats, (const double *)coef, wseed));
 			note_launches(1);
 		}
 		break;
 	case LIKE_POIS:
-		k_like_stats<LIKE_POIS><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, p1);
-		k_like_stats_final<<<batch, 32, 0, s>>>(p1, nparts, stats);
-		k_like_terms<LIKE_POIS><<<grid, 256, 0, s>>>(model, data, sigma, region, n, data_batch_stride, stats,
-		                                              partials, wseed);
-		k_like_terms_final<LIKE_POIS><<<batch, 32, 0, s>>>(partials, nparts, stats, out, coef);
+		go(launch_pdl(k_like_stats<LIKE_POIS>, grid, b256, 0, s, model, data, sigma, region, n, data_batch_stride,
+		              p1));
+		go(launch_pdl(k_like_stats_final, gb, b32, 0, s, (const double *)p1, nparts, stats));
+		go(launch_pdl(k_like_terms<LIKE_POIS>, grid, b256, 0, s, model, data, sigma, region, n, data_batch_stride,
+		              (const double *)stats, partials, wseed));
+		go(launch_pdl(k_like_terms_final<LIKE_POIS>, gb, b32, 0, s, (const double2 *)partials, nparts,
+		              (const double *)stats, out, coef));
 		note_launches(4);
 		break;
 	default: return cudaErrorInvalidValue;
 	}
-	return cudaGetLastError();
+	return e;
 }
 
 cudaError_t launch_loglike64_seed(const double *model, const double *data, const double *sigma,
