@@ -125,6 +125,16 @@ int pf_model_set_crop(pf_model *m, int value);
 /* "brute" (default, like Model::ensure_convolver, model.cpp:144-150),
  * "brute-old", "fft" or "null" (create_convolver, convolve.cpp:526-594). */
 int pf_model_set_convolver(pf_model *m, const char *type);
+/* The convolver choice of profitSetupData with benchmarking
+ * (profitDataBenchmark, R/profitSetupData.R:95-110: profitBenchmark, then
+ * profitBenchmarkResultBest, R/profitBenchmark.R:16-38): times "brute" and
+ * "fft" over nbench evaluations of the model as set up (FP32: logL and its
+ * adjoint gradient; FP64: logL; the image when no data are set), keeps the
+ * faster one as the model's convolver and writes its name to best (NUL
+ * terminated, best_cap bytes).  ms_brute / ms_fft (optional) receive the mean
+ * device times in ms (-1 where a convolver does not apply). */
+int pf_model_benchmark_convolvers(pf_model *m, int nbench, char *best, size_t best_cap, double *ms_brute,
+                                  double *ms_fft);
 int pf_model_set_precision(pf_model *m, int precision);
 
 /* Dimensions the profiles are drawn on before convolution and crop

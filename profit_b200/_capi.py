@@ -131,6 +131,7 @@ def _late_bindings(L):
     L.pf_model_set_dimensions.argtypes = [C.c_void_p, C.c_uint, C.c_uint]
     L.pf_model_set_dry_run.argtypes = [C.c_void_p, C.c_int]
     L.pf_model_set_omp_threads.argtypes = [C.c_void_p, C.c_uint]
+    L.pf_model_benchmark_convolvers.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t, _dp, _dp]
     vp = C.c_void_p
     L.pf_catalogue_create.argtypes = [C.POINTER(vp)]
     L.pf_catalogue_destroy.argtypes = [vp]
@@ -158,4 +159,4 @@ EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch",
                        "pf_catalogue_size", "pf_catalogue_gradient_offset", "pf_catalogue_loglike_grad",
                        "pf_catalogue_last_time", "pf_model_set_likelihood", "pf_model_set_mask",
                        "pf_model_set_adjust_mask", "pf_model_set_dimensions", "pf_model_set_dry_run",
-                       "pf_model_set_omp_threads")
+                       "pf_model_set_omp_threads", "pf_model_benchmark_convolvers")

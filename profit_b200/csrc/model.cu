@@ -1808,6 +1808,60 @@ int pf_model_set_convolver(pf_model *m, const char *type)
 	return PF_OK;
 }
 
+// profitDataBenchmark's convolver choice (R/profitSetupData.R:95-110):
+// profitBenchmark times each convolver on the model as set up and
+// profitBenchmarkResultBest (R/profitBenchmark.R:16-38) keeps the fastest.
+// Here "brute" and "fft" are timed on the device (CUDA events) over nbench
+// evaluations of what a fit evaluates: logL and its adjoint gradient in the
+// FP32 form, logL in the FP64 form, the image when no data are set.
+int pf_model_benchmark_convolvers(pf_model *m, int nbench, char *best, size_t best_cap, double *ms_brute,
+                                  double *ms_fft)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (nbench < 1) return set_error(PF_E_INVALID, "nbench must be positive");
+	const int saved = m->conv_kind;
+	const int kinds[2] = {CONV_BRUTE, CONV_FFT};
+	const char *names[2] = {"brute", "fft"};
+	double ms[2] = {-1, -1};
+	std::vector<double> image;
+	for (int c = 0; c < 2; c++) {
+		m->conv_kind = kinds[c];
+		double total = 0;
+		int st = PF_OK;
+		for (int r = 0; r <= nbench && st == PF_OK; r++) {  // r = 0: warm-up (plans, autotuning, graph capture)
+			double ll = 0;
+			if (m->has_data && m->precision != PF_FP64) st = pf_model_loglike_grad(m, nullptr, 0, &ll, nullptr);
+			else if (m->has_data) st = pf_model_loglike(m, &ll);
+			else {
+				unsigned w = 0, h = 0;
+				int ox = 0, oy = 0;
+				st = pf_model_drawing_dims(m, &w, &h);
+				image.resize((size_t)w * h);
+				if (st == PF_OK) st = pf_model_evaluate(m, image.data(), image.size(), &w, &h, &ox, &oy);
+			}
+			if (st == PF_OK && r > 0) {
+				float t[4];
+				pf_model_last_timings(m, t, 4);
+				total += t[0];
+			}
+		}
+		if (st == PF_OK) ms[c] = total / nbench;
+		else if (c == 0) {
+			m->conv_kind = saved;
+			return st;  // the model itself does not evaluate
+		}
+	}
+	const int pick = (ms[1] >= 0 && ms[1] < ms[0]) ? 1 : 0;
+	m->conv_kind = kinds[pick];
+	if (ms_brute) *ms_brute = ms[0];
+	if (ms_fft) *ms_fft = ms[1];
+	if (best && best_cap) {
+		std::strncpy(best, names[pick], best_cap - 1);
+		best[best_cap - 1] = 0;
+	}
+	return PF_OK;
+}
+
 int pf_model_set_precision(pf_model *m, int precision)
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");

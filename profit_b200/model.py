@@ -152,6 +152,15 @@ class Model:
         """Accepted for libprofit compatibility; no effect (the work runs on the GPU)."""
         check(lib().pf_model_set_omp_threads(self._h, int(n)))
 
+    def benchmark_convolvers(self, nbench: int = 10):
+        """profitSetupData's benchmarked convolver choice: times "brute" and
+        "fft" on this model as set up, keeps the faster one and returns
+        (name, {"brute": ms, "fft": ms}) (mean device times; -1: not applicable)."""
+        buf = C.create_string_buffer(16)
+        tb, tf = C.c_double(), C.c_double()
+        check(lib().pf_model_benchmark_convolvers(self._h, int(nbench), buf, 16, C.byref(tb), C.byref(tf)))
+        return buf.value.decode(), {"brute": tb.value, "fft": tf.value}
+
     def set_likelihood(self, name: str):
         """profitLikeModel's like.func: "norm", "chisq", "t" or "pois" (and their aliases)."""
         check(lib().pf_model_set_likelihood(self._h, name.encode()))

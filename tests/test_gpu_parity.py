@@ -536,3 +536,35 @@ def test_dimensions_dry_run_and_threads():
     m.set_dimensions(0, 20)
     with pytest.raises(InvalidParameter):
         m.evaluate()
+
+
+@pytest.mark.gpu
+def test_convolver_benchmark_keeps_the_faster_convolver():
+    """profitSetupData's benchmarked convolver choice (profitBenchmark +
+    profitBenchmarkResultBest): both convolvers are timed, the faster one is
+    kept, and the model then evaluates exactly as with that convolver set."""
+    wl = W.single_sersic(seed_tag=21)
+    m64 = W.configure(Model(wl["width"], wl["height"]), wl)
+    ref, _ = m64.evaluate()
+    image, sigma = W.make_data(wl, ref)
+    # FP64 image (no data): the choice is one of the two, with both timed
+    name, ms = m64.benchmark_convolvers(nbench=3)
+    assert name in ("brute", "fft") and ms["brute"] > 0 and ms["fft"] > 0
+    assert name == ("fft" if ms["fft"] < ms["brute"] else "brute")
+    img, _ = m64.evaluate()
+    assert _rel(img, ref) <= 1e-12
+    # FP32 logL + gradient with data
+    m32 = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
+    m32.set_data(image, sigma)
+    name, ms = m32.benchmark_convolvers(nbench=3)
+    assert name in ("brute", "fft") and ms["brute"] > 0 and ms["fft"] > 0
+    ll, g = m32.loglike_grad(wl["grad"])
+    same = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), dict(wl, convolver=name))
+    same.set_data(image, sigma)
+    ll2, g2 = same.loglike_grad(wl["grad"])
+    # (cells add to their pixel atomically, so two FP32 renders agree to
+    # rounding, not bit for bit)
+    assert ll == pytest.approx(ll2, rel=1e-7)
+    np.testing.assert_allclose(g, g2, rtol=1e-5, atol=1e-6 * np.max(np.abs(g2)))
+    with pytest.raises(InvalidParameter):
+        m32.benchmark_convolvers(nbench=0)
