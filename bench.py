@@ -385,6 +385,7 @@ def convolver_choice_rate(torch, flush, wl, image, sigma, refs, pvals, steps=30)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     dev, e2e = [], []
+    torch.cuda.nvtx.range_push("convolver_choice")
     for s in range(steps + 3):
         flush.zero_()
         torch.cuda.synchronize()
@@ -398,6 +399,7 @@ def convolver_choice_rate(torch, flush, wl, image, sigma, refs, pvals, steps=30)
             e2e.append(ev0.elapsed_time(ev1) / 1e3)
             L.pf_model_last_timings(m._h, tim, 4)
             dev.append(tim[0] / 1e3)
+    torch.cuda.nvtx.range_pop()
     m.close()
     return {"workload": "the headline workload with the benchmark-chosen convolver",
             "benchmark": {"chosen": best, "mean_device_ms": ms, "nbench": 10},
@@ -474,6 +476,7 @@ def large_field_rate(args, torch, flush, calls=3):
     mm.set_data(image, sigma)
     mm.loglike_grad(refs)  # warm-up: FFT plans, queue sizing, graph capture
     dev, wall, phases = [], [], []
+    torch.cuda.nvtx.range_push("large_field")
     for _ in range(calls):
         flush.zero_()
         torch.cuda.synchronize()
@@ -483,6 +486,7 @@ def large_field_rate(args, torch, flush, calls=3):
         t = mm.last_timings()
         dev.append(t[0] / 1e3)
         phases.append(list(t))
+    torch.cuda.nvtx.range_pop()
     mm.close()
     fd_s = (2 * len(refs) + 1) * statistics.mean(t64)
     ph = np.mean(np.array(phases), axis=0)
