@@ -107,8 +107,8 @@ int pf_model_set_return_finesampled(pf_model *m, int value);
  * upsampled, padded and dilated by psf/2 for the drawing, the PSF padding is
  * left out when the mask keeps psf/2 pixels clear of the edges, and the
  * result is zeroed outside the mask (model.cpp:152-183, 230-246, 330-334).
- * Without it the mask must have the drawing dimensions.  Plain (FP64) form
- * only for now. */
+ * Without it the mask must have the drawing dimensions.  Both forms (FP64
+ * plain, FP32 with the adjoint gradient). */
 int pf_model_set_mask(pf_model *m, const uint8_t *mask, unsigned width, unsigned height);
 int pf_model_set_adjust_mask(pf_model *m, int value);
 /* Model::set_dimensions (model.h:142-147); a width or height of 0 makes the

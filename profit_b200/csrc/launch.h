@@ -43,9 +43,19 @@ cudaError_t launch_downsample64(const double *src, unsigned sw, unsigned sh, uns
 // render32.cu
 // jac: tangent planes, nt per profile (tangent_stride of the model);
 // all_kinds: the model has radial profiles other than Sersic and Moffat.
+// mask: optional drawing-size calculation mask shared by the batch entries
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
-                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s);
+                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask = nullptr);
+// Masked convolution select, finesampling sum-down and output mask of the
+// FP32 pipeline (sel, mask_out optional), and their adjoint seeds.
+cudaError_t launch_model_finish32(const double *fine, unsigned cw, unsigned ch, const float *plain, const uint8_t *sel,
+                                  unsigned dw, unsigned dh, unsigned padx, unsigned pady, unsigned fs,
+                                  const uint8_t *mask_out, double *out, unsigned ow, unsigned oh, int batch,
+                                  cudaStream_t s);
+cudaError_t launch_seed_finish32(const float *w, unsigned ow, unsigned oh, const uint8_t *mask_out, const uint8_t *sel,
+                                 unsigned fs, unsigned cw, unsigned ch, unsigned padx, unsigned pady, unsigned dw,
+                                 unsigned dh, int batch, float *seed_conv, float *g_plain, cudaStream_t s);
 // Levels >= 3 (reached only by Sersic centre cusps) run in one CTA when the
 // launch holds at most this many cusps, else one grid-wide launch per level.
 constexpr int DEEP_ONE_CTA_MAX_CUSPS = 8;
@@ -109,7 +119,8 @@ namespace pf {
 // render32.cu: recomputing adjoint of the render (no stored tangent planes)
 cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
                                      unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
-                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s);
+                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s,
+                                     const uint8_t *mask = nullptr);
 }  // namespace pf
 
 namespace pf {

@@ -345,6 +345,8 @@ struct pf_model {
 	bool adjust_mask = true;
 	bool dry_run = false;
 	std::vector<uint64_t> mask_key;  // what the device masks were built for
+	uint64_t mask_version = 0;       // bumped by pf_model_set_mask
+	DevBuf d_model_fine, d_seed_fine;  // FP32 pipeline: convolved fine image, fine seed
 	DevBuf d_mask_draw, d_mask_out;
 	int like_kind = LIKE_NORM;
 	DevBuf d_likestats;
@@ -471,9 +473,9 @@ int analyze(pf_model *m, Analysis &a)
 int upload_masks(pf_model *m, const Analysis &a)
 {
 	if (!a.mask) return PF_OK;
-	std::vector<uint64_t> key = {m->mask_w, m->mask_h, m->adjust_mask, m->fs, m->psf_w, m->psf_h, a.dw, a.dh,
-	                             a.mask_conv, a.mask_psf_pad, (uint64_t)std::hash<std::string>{}(
-	                                 std::string(m->mask.begin(), m->mask.end()))};
+	std::vector<uint64_t> key = {m->mask_w, m->mask_h, m->adjust_mask, m->fs,  m->psf_w,
+	                             m->psf_h,  a.dw,      a.dh,           a.mask_conv, a.mask_psf_pad,
+	                             m->mask_version};
 	if (key == m->mask_key && m->d_mask_draw.p) return PF_OK;
 	std::vector<uint8_t> draw;
 	if (!m->adjust_mask) {
@@ -704,10 +706,61 @@ int derive_and_upload(pf_model *m, const Analysis &a, const std::vector<ProfileP
 // residual (data - model) of bright pixels is a small difference of large
 // numbers: brute force sums kernel columns in FP64, the "fft" convolver
 // transforms in FP64.
+// What the FP32 pipeline does beyond one plain crop of the convolved image,
+// as run_plain64 does in FP64 (model.cpp:307-334): the drawing-size
+// calculation mask for the profiles (draw), the masked convolution's select
+// of the unconvolved pixel (sel), the finesampling sum-down (output smaller
+// than the crop window) and the output mask (out).  The device masks are
+// those upload_masks built for this analysis.
+struct Finish32 {
+	const uint8_t *draw = nullptr, *sel = nullptr, *out = nullptr;
+	bool any = false;
+};
+
+Finish32 finish32_of(pf_model *m, const Analysis &a)
+{
+	Finish32 f;
+	if (a.mask) {
+		f.draw = m->d_mask_draw.as<uint8_t>();
+		if (a.conv && m->conv_kind != CONV_NULL && (a.mask_conv || !m->adjust_mask)) f.sel = f.draw;
+		if (a.mask_adjusted && a.ow == m->mask_w && a.oh == m->mask_h) f.out = m->d_mask_out.as<uint8_t>();
+	}
+	f.any = f.sel || f.out || a.ow != a.cw || a.oh != a.ch;
+	return f;
+}
+
+// Output (i, j) of the crop window is drawing pixel (i + padx, j + pady); its
+// convolution window starts psf/2 before that (0 with the usual padding,
+// -psf/2 when a mask let the padding go).
+inline int conv_ox(const pf_model *m, const Analysis &a) { return (int)a.padx - (int)(m->psf_w / 2); }
+inline int conv_oy(const pf_model *m, const Analysis &a) { return (int)a.pady - (int)(m->psf_h / 2); }
+
+int convolve_crop32(pf_model *m, const Analysis &a, const float *conv, const float *plain, double *model64, int batch,
+                    bool conv_on);
+
 int forward_conv32(pf_model *m, const Analysis &a, const float *conv, const float *plain, double *model64, int batch)
 {
-	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.cw * a.ch;
+	const size_t nout = (size_t)a.cw * a.ch;
 	const bool conv_on = a.conv && m->conv_kind != CONV_NULL;
+	const Finish32 fin = finish32_of(m, a);
+	double *dst = model64;  // the crop window, then finished into model64 when needed
+	if (fin.any) {
+		PF_CUDA(ensure(m->d_model_fine, nout * 8 * batch));
+		dst = m->d_model_fine.as<double>();
+	}
+	PF_TRY(convolve_crop32(m, a, conv, plain, dst, batch, conv_on));
+	if (fin.any)
+		PF_CUDA(launch_model_finish32(dst, a.cw, a.ch, plain, fin.sel, a.dw, a.dh, a.padx, a.pady, m->fs, fin.out,
+		                              model64, a.ow, a.oh, batch, m->stream));
+	return PF_OK;
+}
+
+// The convolved image plus the unconvolved one on the crop window, FP64.
+int convolve_crop32(pf_model *m, const Analysis &a, const float *conv, const float *plain, double *model64, int batch,
+                    bool conv_on)
+{
+	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.cw * a.ch;
+	const int ox = conv_ox(m, a), oy = conv_oy(m, a);
 	if (conv_on && m->conv_kind == CONV_FFT) {
 		PF_TRY(prepare_fft(m, a, batch, false));
 		int dx, dy;
@@ -727,7 +780,7 @@ int forward_conv32(pf_model *m, const Analysis &a, const float *conv, const floa
 		for (int b = 0; b < batch; b++) {
 			const double *c64 = m->d_conv64.as<double>() + b * npix, *p64 = m->d_plain64.as<double>() + b * npix;
 			if (conv_on)
-				PF_CUDA(launch_conv64(c64, a.dw, a.dh, 0, 0, m->d_psfrev64.as<double>(), m->psf_w, m->psf_h,
+				PF_CUDA(launch_conv64(c64, a.dw, a.dh, ox, oy, m->d_psfrev64.as<double>(), m->psf_w, m->psf_h,
 				                      model64 + b * nout, a.cw, a.ch, p64, a.dw, a.padx, a.pady, m->stream));
 			else
 				PF_CUDA(launch_crop64(c64, a.dw, a.padx, a.pady, model64 + b * nout, a.cw, a.ch, p64, m->stream));
@@ -736,8 +789,8 @@ int forward_conv32(pf_model *m, const Analysis &a, const float *conv, const floa
 	}
 	size_t sb = conv32_scratch_bytes(a.cw, a.ch, batch);
 	if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
-	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64, a.cw,
-	                           a.ch, plain, a.dw, a.padx, a.pady, batch, (int)npix, (int)nout,
+	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, ox, oy, m->d_psfrev32.as<float>(), m->psf_w, m->psf_h, model64,
+	                           a.cw, a.ch, plain, a.dw, a.padx, a.pady, batch, (int)npix, (int)nout,
 	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, 0, m->stream));
 	return PF_OK;
 }
@@ -763,9 +816,40 @@ int adjoint_conv32(pf_model *m, const Analysis &a, const float *wseed, float *gc
 	}
 	size_t sb = conv32_scratch_bytes(a.dw, a.dh, batch);
 	if (sb) PF_CUDA(ensure(m->d_convsplit, sb));
-	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w, 1 - (int)m->psf_h, m->d_psf32.as<float>(), m->psf_w,
-	                      m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, batch, (int)nout, (int)npix,
-	                      sb ? m->d_convsplit.as<double>() : nullptr, sb, 0, m->stream));
+	// the adjoint of a correlation at offset ox is the correlation with the
+	// unreversed PSF at offset 1 - psf - ox
+	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)m->psf_w - conv_ox(m, a), 1 - (int)m->psf_h - conv_oy(m, a),
+	                      m->d_psf32.as<float>(), m->psf_w, m->psf_h, gconv, a.dw, a.dh, nullptr, 0, 0, 0, batch,
+	                      (int)nout, (int)npix, sb ? m->d_convsplit.as<double>() : nullptr, sb, 0, m->stream));
+	return PF_OK;
+}
+
+// The adjoint's seeds from dlogL/dmodel (wseed, output grid): g_plain for
+// the unconvolved profiles (drawing size) and g_conv for the convolved ones
+// (g_conv = g_plain when nothing is convolved).
+int adjoint_seed32(pf_model *m, const Analysis &a, const float *wseed, float *&gconv, float *gplain, int batch)
+{
+	const Finish32 fin = finish32_of(m, a);
+	const bool conv_on = a.conv && m->conv_kind != CONV_NULL;
+	if (!fin.any) {
+		PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, batch, gplain, m->stream));
+		if (conv_on) PF_TRY(adjoint_conv32(m, a, wseed, gconv, batch));
+		else gconv = gplain;
+		return PF_OK;
+	}
+	PF_CUDA(ensure(m->d_seed_fine, (size_t)a.cw * a.ch * 4 * batch));
+	float *seed = m->d_seed_fine.as<float>();
+	PF_CUDA(launch_seed_finish32(wseed, a.ow, a.oh, fin.out, fin.sel, m->fs, a.cw, a.ch, a.padx, a.pady, a.dw, a.dh,
+	                             batch, seed, gplain, m->stream));
+	if (conv_on) {
+		Analysis af = a;  // the seed of the convolution lives on the fine crop window
+		af.ow = a.cw;
+		af.oh = a.ch;
+		PF_TRY(adjoint_conv32(m, af, seed, gconv, batch));
+	}
+	else {
+		gconv = gplain;
+	}
 	return PF_OK;
 }
 
@@ -961,7 +1045,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	}
 	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *model = m->d_model32.as<float>();
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), 1, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain,
-	                        jac, tangent_stride(m), all_kinds(m), q, m->stream));
+	                        jac, tangent_stride(m), all_kinds(m), q, m->stream, finish32_of(m, a).draw));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, tangent_stride(m), all_kinds(m),
 	                        cusp_count(m), q,
 	                        m->stream));
@@ -982,11 +1066,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(ensure(m->d_gconv, npix * 4));
 		PF_CUDA(ensure(m->d_gplain, npix * 4));
 		float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>();
-		PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, 1, gplain, m->stream));
-		if (a.conv && m->conv_kind != CONV_NULL)
-			PF_TRY(adjoint_conv32(m, a, wseed, gconv, 1));
-		else
-			gconv = gplain;
+		PF_TRY(adjoint_seed32(m, a, wseed, gconv, gplain, 1));
 		PF_CUDA(cudaMemsetAsync(d_out + ResultLayout::T0, 0, (size_t)nprof * NTAN * 8, m->stream));
 		double *jpart;
 		unsigned *jtick;
@@ -1034,7 +1114,14 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 	                        &m->d_wseed, &m->d_items, &m->d_ctrl, &m->d_partials, &m->d_results, &m->d_psf32,
 	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region, &m->d_convsplit, &m->d_jac_partials, &m->d_jac_tickets, &m->d_likestats};
 	for (auto *b : bufs) s.push_back((uint64_t)(uintptr_t)b->p);
-	s.push_back((uint64_t)(uintptr_t)m->h_fprof.p);
+	// calculation mask and finesampling steps (finish32_of) and their buffers
+	for (const DevBuf *b : {&m->d_mask_draw, &m->d_mask_out, &m->d_model_fine, &m->d_seed_fine})
+		s.push_back((uint64_t)(uintptr_t)b->p);
+	s.push_back(((uint64_t)a.mask << 0) | ((uint64_t)a.mask_conv << 1) | ((uint64_t)a.mask_adjusted << 2) |
+	            ((uint64_t)m->adjust_mask << 3) | ((uint64_t)m->fs << 8) | ((uint64_t)a.cw << 24));
+	s.push_back(((uint64_t)a.ch << 32) | ((uint64_t)m->mask_w << 16) | m->mask_h);
+	s.push_back(((uint64_t)a.padx << 32) | a.pady);
+	s.push_back((uint64_t)m->profiles.size());
 	s.push_back((uint64_t)(uintptr_t)m->h_results.p);
 	return s;
 }
@@ -1063,13 +1150,12 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 {
 	PF_TRY(ensure_stream(m));
 	PF_TRY(analyze(m, a));
-	if (m->fs != 1) return set_error(PF_E_INVALID, "the FP32 path does not support finesampling yet");
-	if (!m->mask.empty()) return set_error(PF_E_INVALID, "the FP32 path does not support calculation masks yet");
 	for (auto &p : m->profiles)
 		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
 	if (m->has_data && (m->data_w != a.ow || m->data_h != a.oh))
 		return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
 	PF_TRY(upload_psf(m));
+	PF_TRY(upload_masks(m, a));  // before any capture: it copies synchronously when the mask changed
 	int nprof = a.n_profiles;
 	// profile scalars, staged in pinned memory (the upload is part of the pipeline)
 	{
@@ -1234,21 +1320,19 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	}
 	const int nt = tangent_stride(m);
 	const bool ak = all_kinds(m);
-	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx, m->sy, conv, plain, jac, nt, ak, q,
-	                        s));
+	const Finish32 fin = finish32_of(m, a);
+	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain,
+	                        jac, nt, ak, q, s, fin.draw));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, nt, ak, C * cusp_count(m), q, s));
 	PF_CUDA(record_event(m->ev[1], s));
 	PF_TRY(forward_conv32(m, a, conv, plain, model64, C));
 	PF_CUDA(record_event(m->ev[2], s));
 	PF_TRY(enqueue_like(m, model64, (int)nout, C, bs.d_ll.as<double>(), wseed, s));
-	PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
-	if (a.conv && m->conv_kind != CONV_NULL)
-		PF_TRY(adjoint_conv32(m, a, wseed, gconv, C));
-	else
-		gconv = gplain;
+	PF_TRY(adjoint_seed32(m, a, wseed, gconv, gplain, C));
 	if (recompute)
-		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh, m->sx, m->sy, gconv,
-		                                 gplain, a.levels, ak, q, bs.d_T.as<double>(), s));
+		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh, m->sx / m->fs,
+		                                 m->sy / m->fs, gconv, gplain, a.levels, ak, q, bs.d_T.as<double>(), s,
+		                                 fin.draw));
 	else {
 		double *jpart;
 		unsigned *jtick;
@@ -1270,8 +1354,6 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	PF_TRY(ensure_stream(m));
 	Analysis a;
 	PF_TRY(analyze(m, a));
-	if (m->fs != 1) return set_error(PF_E_INVALID, "the FP32 path does not support finesampling yet");
-	if (!m->mask.empty()) return set_error(PF_E_INVALID, "the FP32 path does not support calculation masks yet");
 	for (auto &p : m->profiles)
 		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
 	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
@@ -1283,6 +1365,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		// profile indices of queued cells are 16-bit: chunks keep B*nprof below that
 	}
 	PF_TRY(upload_psf(m));
+	PF_TRY(upload_masks(m, a));
 	if (!m->batch) m->batch = new BatchState();
 	BatchState &bs = *m->batch;
 
@@ -1338,7 +1421,8 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	const size_t planes = npix * (size_t)nprof * tangent_stride(m) * 4;
 	const bool recompute = m->adjoint_mode == PF_ADJOINT_RECOMPUTE ||
 	                       (m->adjoint_mode == PF_ADJOINT_AUTO && planes > (256ull << 20));
-	size_t per = npix * (4 * 4 + 8 * 2) + (recompute ? 0 : planes) + nout * (8 + 4) + 4096;
+	size_t per = npix * (4 * 4 + 8 * 2) + (recompute ? 0 : planes) + nout * (8 + 4) + 4096 +
+	             (size_t)a.cw * a.ch * (8 + 4);  // crop window: fine model, fine seed (masks, finesampling)
 	if (a.conv && m->conv_kind == CONV_FFT) {
 		const size_t spec = (size_t)fft_good_size((int)a.dh + (int)m->psf_h - 1) *
 		                    (fft_good_size((int)a.dw + (int)m->psf_w - 1) / 2 + 1);
@@ -1758,6 +1842,7 @@ int pf_model_set_mask(pf_model *m, const uint8_t *mask, unsigned width, unsigned
 	for (auto &v : m->mask) v = v ? 1 : 0;
 	m->mask_w = width;
 	m->mask_h = height;
+	m->mask_version++;
 	return PF_OK;
 }
 

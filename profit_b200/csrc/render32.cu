@@ -369,11 +369,14 @@ __device__ __forceinline__ Tan<float> to_float(const Tan<T> &t)
 // is compiled out).  A profile whose rscale_max lies more than 2 px short of
 // the block's nearest pixel centre is skipped for the whole block: the
 // elliptical radius is never smaller than the Euclidean distance, so every
-// pixel of the block would take the zero decision.
+// pixel of the block would take the zero decision.  mask (optional, one
+// drawing-size calculation mask for every batch entry): pixels where it is 0
+// are not drawn by the radial and sky profiles (radial.cpp:306, sky.cpp:47-63).
 template <bool AK, bool J>
 __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__restrict__ prof_begin,
                            unsigned width, unsigned height, double sx, double sy, float *__restrict__ img_conv,
-                           float *__restrict__ img_plain, float *__restrict__ jac, int nt, QueueSet q)
+                           float *__restrict__ img_plain, float *__restrict__ jac, int nt, QueueSet q,
+                           const uint8_t *__restrict__ mask)
 {
 	pdl_enter();
 	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -392,9 +395,19 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 	const unsigned tx1 = min(tx0 + blockDim.x - 1, width - 1), ty1 = min(ty0 + blockDim.y - 1, height - 1);
 	const double xlo = half_xbin + tx0 * sy, xhi = half_xbin + tx1 * sy;
 	const double ylo = half_ybin + ty0 * sx, yhi = half_ybin + ty1 * sx;
+	const bool drawn = !mask || mask[pix];
 
 	for (int pi = p0; pi < p1; pi++) {
 		const FProfile &p = profiles[pi];
+		if (!drawn) {
+			if constexpr (J) {
+				if (is_radial_kind(p.kind)) {
+					float *jp = jac + (size_t)pi * nt * npix + pix;
+					for (int k = 0; k < nt; k++) jp[(size_t)k * npix] = 0.f;
+				}
+			}
+			continue;
+		}
 		if (p.kind == PK_SKY) {
 			acc[p.target] += p.flux_scale;  // sky value is kept in flux_scale
 			continue;
@@ -657,7 +670,8 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
                                                           const int *__restrict__ prof_batch, unsigned width,
                                                           unsigned height, double sx, double sy,
                                                           const float *__restrict__ g_conv,
-                                                          const float *__restrict__ g_plain, double *__restrict__ T)
+                                                          const float *__restrict__ g_plain, double *__restrict__ T,
+                                                          const uint8_t *__restrict__ mask)
 {
 	pdl_enter();
 	const int pi = blockIdx.z;
@@ -682,6 +696,7 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 	for (unsigned r = threadIdx.x >> 6; r < 32; r += 4) {
 		const unsigned j = ty0 + r;
 		if (i >= width || j >= height) continue;
+		if (mask && !mask[i + (size_t)j * width]) continue;  // not drawn by the forward pass
 		const float gv = g[i + (size_t)j * width];
 		if (gv == 0.f) continue;
 		const double y = half_ybin + j * sx, x = half_xbin + i * sy;
@@ -758,12 +773,14 @@ __global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restr
 
 cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
                                      unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
-                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s)
+                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s,
+                                     const uint8_t *mask)
 {
 	dim3 grid((width + 63) / 64, (height + 31) / 32, n_profiles);
 	auto kp = all_kinds ? k_adjoint_pixels32<true> : k_adjoint_pixels32<false>;
 	auto ki = all_kinds ? k_adjoint_items32<true> : k_adjoint_items32<false>;
-	cudaError_t e = launch_pdl(kp, grid, dim3(256), 0, s, profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T);
+	cudaError_t e = launch_pdl(kp, grid, dim3(256), 0, s, profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T,
+	                           mask);
 	if (e == cudaSuccess) e = launch_pdl(ki, dim3(148 * 8), dim3(256), 0, s, profiles, levels, g_conv, g_plain, q, T);
 	note_launches(2);
 	return e;
@@ -893,14 +910,14 @@ static inline unsigned cdiv(unsigned a, unsigned b) { return (a + b - 1) / b; }
 
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
-                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s)
+                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask)
 {
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8), batch);
 	auto k = all_kinds ? (jac ? k_pixels32<true, true> : k_pixels32<true, false>)
 	                   : (jac ? k_pixels32<false, true> : k_pixels32<false, false>);
 	note_launches(1);
 	return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac, nt,
-	                  q);
+	                  q, mask);
 }
 
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
@@ -963,6 +980,83 @@ cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned
 	note_launches(1);
 	if (e != cudaSuccess) return e;
 	return cudaGetLastError();
+}
+
+// The FP32 pipeline's model image from the convolved fine image, for the
+// cases beyond one plain crop (Model::evaluate, model.cpp:307-334):
+//   fine(i, j) = plain drawing pixel where the drawing mask is 0 and the
+//                convolution was masked (sel, drawing size, optional);
+//   out(I, J)  = sum of the fs x fs fine pixels of the output pixel (the
+//                finesampled image summed down), 0 where the output mask
+//                (mask_out, output size, optional) is 0.
+// Strides: fine nfine, plain npix, out nout per batch entry (blockIdx.z).
+__global__ void k_model_finish32(const double *__restrict__ fine, unsigned cw, unsigned ch, size_t nfine,
+                                 const float *__restrict__ plain, const uint8_t *__restrict__ sel, unsigned dw,
+                                 size_t npix, unsigned padx, unsigned pady, unsigned fs,
+                                 const uint8_t *__restrict__ mask_out, double *__restrict__ out, unsigned ow,
+                                 unsigned oh, size_t nout)
+{
+	pdl_enter();
+	const unsigned I = blockIdx.x * blockDim.x + threadIdx.x, J = blockIdx.y * blockDim.y + threadIdx.y;
+	const int b = blockIdx.z;
+	if (I >= ow || J >= oh) return;
+	fine += (size_t)b * nfine;
+	plain += (size_t)b * npix;
+	double v = 0;
+	for (unsigned row = J * fs; row < min((J + 1) * fs, ch); row++)
+		for (unsigned col = I * fs; col < min((I + 1) * fs, cw); col++) {
+			const size_t d = (col + padx) + (size_t)(row + pady) * dw;
+			v += (sel && !sel[d]) ? (double)plain[d] : fine[col + (size_t)row * cw];
+		}
+	if (mask_out && !mask_out[I + (size_t)J * ow]) v = 0.0;
+	out[(size_t)b * nout + I + (size_t)J * ow] = v;
+}
+
+// Adjoint of k_model_finish32 and of the crop: from dlogL/dout (w, output
+// size) to the seed of the convolved image on the fine crop window (seed_conv,
+// cw x ch) and to dlogL/d(unconvolved drawing pixel) (g_plain, drawing size,
+// 0 outside the crop window).  A fine pixel receives its output pixel's w
+// (the sum down), 0 where the output mask is 0; its convolved part also 0
+// where the masked convolution kept the plain pixel.
+__global__ void k_seed_finish32(const float *__restrict__ w, unsigned ow, unsigned oh, size_t nout,
+                                const uint8_t *__restrict__ mask_out, const uint8_t *__restrict__ sel, unsigned fs,
+                                unsigned cw, unsigned ch, size_t nfine, unsigned padx, unsigned pady, unsigned dw,
+                                unsigned dh, size_t npix, float *__restrict__ seed_conv, float *__restrict__ g_plain)
+{
+	pdl_enter();
+	const unsigned u = blockIdx.x * blockDim.x + threadIdx.x, v = blockIdx.y * blockDim.y + threadIdx.y;
+	const int b = blockIdx.z;
+	if (u >= dw || v >= dh) return;
+	const size_t d = u + (size_t)v * dw;
+	float g = 0.f;
+	if (u >= padx && v >= pady && u - padx < cw && v - pady < ch) {
+		const unsigned i = u - padx, j = v - pady;
+		const size_t o = i / fs + (size_t)(j / fs) * ow;
+		g = (mask_out && !mask_out[o]) ? 0.f : w[(size_t)b * nout + o];
+		seed_conv[(size_t)b * nfine + i + (size_t)j * cw] = (sel && !sel[d]) ? 0.f : g;
+	}
+	g_plain[(size_t)b * npix + d] = g;
+}
+
+cudaError_t launch_model_finish32(const double *fine, unsigned cw, unsigned ch, const float *plain, const uint8_t *sel,
+                                  unsigned dw, unsigned dh, unsigned padx, unsigned pady, unsigned fs,
+                                  const uint8_t *mask_out, double *out, unsigned ow, unsigned oh, int batch,
+                                  cudaStream_t s)
+{
+	dim3 block(32, 8), grid(cdiv(ow, 32), cdiv(oh, 8), batch);
+	note_launches(1);
+	return launch_pdl(k_model_finish32, grid, block, 0, s, fine, cw, ch, (size_t)cw * ch, plain, sel, dw,
+	                  (size_t)dw * dh, padx, pady, fs, mask_out, out, ow, oh, (size_t)ow * oh);
+}
+
+cudaError_t launch_seed_finish32(const float *w, unsigned ow, unsigned oh, const uint8_t *mask_out, const uint8_t *sel,
+                                 unsigned fs, unsigned cw, unsigned ch, unsigned padx, unsigned pady, unsigned dw,
+                                 unsigned dh, int batch, float *seed_conv, float *g_plain, cudaStream_t s)
+{
+	dim3 block(32, 8), grid(cdiv(dw, 32), cdiv(dh, 8), batch);
+	note_launches(1);
+	return launch_pdl(k_seed_finish32, grid, block, 0, s, w, ow, oh, (size_t)ow * oh, mask_out, sel, fs, cw, ch,
+	                  (size_t)cw * ch, padx, pady, dw, dh, (size_t)dw * dh, seed_conv, g_plain);
 }
 
 // FP32 taps, FP64 column accumulation; FP32 output (adjoint) or FP64 output

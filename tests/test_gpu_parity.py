@@ -495,9 +495,11 @@ def test_calculation_mask_errors():
     with pytest.raises(InvalidParameter):
         m.evaluate()  # Mask dimensions != model dimensions
     m.set_mask(np.ones((30, 40), dtype=np.uint8))
+    m.evaluate()
     m.set_precision(PF_FP32)
+    m.set_mask(np.ones((10, 10), dtype=np.uint8))
     with pytest.raises(InvalidParameter):
-        m.evaluate()  # the FP32 path does not take masks yet
+        m.evaluate()  # the FP32 form checks the same way
 
 
 @pytest.mark.parametrize("kind", ["central", "edge"])
@@ -568,3 +570,100 @@ def test_convolver_benchmark_keeps_the_faster_convolver():
     np.testing.assert_allclose(g, g2, rtol=1e-5, atol=1e-6 * np.max(np.abs(g2)))
     with pytest.raises(InvalidParameter):
         m32.benchmark_convolvers(nbench=0)
+
+
+def _fs_mask_model(mask, fs, precision=PF_FP32, conv="brute", adjust=True, retfine=False):
+    """The calculation-mask case of the FP64 tests without the psf point
+    source (not in the FP32 form): a convolved bright Sersic, an unconvolved
+    Moffat and sky, finesampling fs."""
+    m = Model(100, 90, precision=precision)
+    m.set_magzero(30.0)
+    m.set_psf(W.moffat_psf(15, 3.0, 2.5))
+    m.set_convolver(conv)
+    m.set_finesampling(fs)
+    m.set_return_finesampled(retfine)
+    m.add_profile("sersic", xcen=52.3, ycen=44.1, re=6, nser=2.5, ang=30, axrat=0.6, convolve=True)
+    m.add_profile("moffat", xcen=20.5, ycen=70.2, fwhm=3, con=2.5, mag=19, convolve=False)
+    m.add_profile("sky", bg=0.1)
+    if mask is not None:
+        m.set_mask(mask, adjust)
+    return m
+
+
+@pytest.mark.parametrize("kind,fs,conv,retfine", [
+    (None, 2, "brute", False), (None, 3, "fft", True), ("central", 1, "brute", False), ("edge", 1, "brute", False),
+    ("central", 2, "fft", False), ("edge", 3, "brute", False), ("edge", 1, "fft", False)])
+def test_fp32_masks_and_finesampling_match_fp64(kind, fs, conv, retfine):
+    """The FP32 form with a calculation mask (masked profiles, masked
+    convolution, image &= mask) and finesampling (summed down, or the fine
+    image returned) against the plain FP64 form, to FP32 accuracy."""
+    mask = None if kind is None else _mask_case(kind)
+    m64 = _fs_mask_model(mask, fs, PF_FP64, conv, retfine=retfine)
+    m32 = _fs_mask_model(mask, fs, PF_FP32, conv, retfine=retfine)
+    assert m32.drawing_dims() == m64.drawing_dims()
+    img64, off64 = m64.evaluate()
+    img32, off32 = m32.evaluate()
+    assert img32.shape == img64.shape and off32 == off64
+    assert _rel(img32, img64) <= 1e-6
+    if mask is not None:
+        assert np.all(img32[mask == 0] == 0)
+
+
+def test_fp32_mask_without_adjustment_matches_fp64():
+    """adjust_mask = false: the drawing-size mask is used as given (masked
+    profiles and convolution, no final mask)."""
+    m64 = _fs_mask_model(None, 1, PF_FP64)
+    dw, dh = m64.drawing_dims()
+    yy, xx = np.mgrid[0:dh, 0:dw]
+    mask = (((xx - 60) / 30.0) ** 2 + ((yy - 50) / 25.0) ** 2 < 1).astype(np.uint8)
+    imgs = []
+    for prec in (PF_FP64, PF_FP32):
+        m = _fs_mask_model(None, 1, prec)
+        m.set_mask(mask, adjust=False)
+        imgs.append(m.evaluate()[0])
+    assert _rel(imgs[1], imgs[0]) <= 1e-6
+
+
+@pytest.mark.parametrize("kind,fs,conv", [("central", 1, "brute"), ("edge", 2, "brute"), ("edge", 1, "fft"),
+                                          (None, 2, "fft")])
+def test_fp32_adjoint_with_mask_and_finesampling_matches_fd64(kind, fs, conv):
+    """d logL / d(parameters) through masked rendering, masked convolution,
+    the sum-down of the finesampled image and image &= mask, against FP64
+    central differences of the plain form (store and recompute adjoints, one
+    proposal and a batch)."""
+    from profit_b200._capi import PF_ADJOINT_RECOMPUTE, PF_ADJOINT_STORE
+    mask = None if kind is None else _mask_case(kind)
+    truth = _fs_mask_model(mask, fs, PF_FP64, conv)
+    img, _ = truth.evaluate()
+    rng = np.random.Generator(np.random.PCG64(31))
+    sigma = 1.0 + 0.1 * np.sqrt(np.abs(img))
+    image = img + rng.normal(0.0, 1.0, img.shape) * sigma
+    refs = [(0, "xcen"), (0, "ycen"), (0, "mag"), (0, "re"), (0, "nser"), (0, "ang"), (0, "axrat"),
+            (1, "xcen"), (1, "ycen"), (1, "mag")]
+    prop = [52.6, 43.8, 15.05, 6.2, 2.45, 31.0, 0.62, 20.3, 70.4, 19.03]
+    m = _fs_mask_model(mask, fs, PF_FP64, conv)
+    m.set_data(image, sigma)
+    m.set_parameters(refs, prop)
+    ll64 = m.loglike()
+    _, g6 = m.loglike_grad_fd(refs, rel_step=1e-6)
+    _, g5 = m.loglike_grad_fd(refs, rel_step=1e-5)
+    scale = np.max(np.abs(g6))
+    spread = 2 * np.abs(g6 - g5) / scale
+    m.set_precision(PF_FP32)
+    for mode in (PF_ADJOINT_STORE, PF_ADJOINT_RECOMPUTE):
+        m.set_adjoint_mode(mode)
+        for _ in range(2):  # eager, then graph replay
+            ll32, g = m.loglike_grad(refs)
+            assert ll32 == pytest.approx(ll64, rel=1e-5)
+            err = np.minimum(np.abs(g - g6), np.abs(g - g5)) / scale
+            assert np.all(err <= np.maximum(1e-5, spread)), (mode, list(zip(refs, g6, g5, g)))
+    m.set_adjoint_mode(PF_ADJOINT_STORE)
+    vals = np.array([prop, [v * (1 + 1e-3) for v in prop]])
+    ll_b, g_b = m.loglike_grad_batch(refs, vals)
+    for s in range(2):
+        m.set_parameters(refs, vals[s])
+        l1, g1 = m.loglike_grad(refs)
+        # (a batch of two may run other autotuned convolution tiles than one
+        # proposal: FP32 sums in another order)
+        assert ll_b[s] == pytest.approx(l1, rel=1e-6)
+        np.testing.assert_allclose(g_b[s], g1, rtol=1e-5, atol=1e-6 * np.max(np.abs(g1)))
