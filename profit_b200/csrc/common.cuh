@@ -156,6 +156,16 @@ enum GradCode : int32_t { G_XCEN = 0, G_YCEN, G_MAG, G_ANG, G_AXRAT, G_BOX, G_SH
 
 PF_HD inline double gradient_from_tangents(int code, double axrat, const DevProfile &d, const double *T)
 {
+	if (d.kind == PK_PSF) {
+		// psf point source: T = sums of g times its stamp and the stamp's
+		// derivatives in xcen and ycen (k_psf_adjoint32), flux 10^(-0.4(mag-mz))
+		switch (code) {
+		case G_XCEN: return d.psf_flux * T[1];
+		case G_YCEN: return d.psf_flux * T[2];
+		case G_MAG: return d.psf_flux * d.dlnI_dmag * T[0];
+		default: return 0.0;
+		}
+	}
 	const double F = d.flux_scale, q = axrat, c = d.cos_ang, s = d.sin_ang;
 	switch (code) {
 	case G_XCEN: return F * (-c * T[1] + (s / q) * T[2]);
@@ -169,6 +179,16 @@ PF_HD inline double gradient_from_tangents(int code, double axrat, const DevProf
 		return F * (T[NTAN_GEOM + k] + d.dlnI_dp[k] * T[0]);
 	}
 	}
+}
+
+// floor(value) bounded to [0, max] (libprofit's bind for the psf profile's
+// pixel ranges, psf.cpp:40-50).
+__device__ __forceinline__ unsigned bind_u(double value, unsigned max)
+{
+	int intval = (int)floor(value);
+	if (intval < 0) return 0;
+	unsigned u = (unsigned)intval;
+	return u < max ? u : max;
 }
 
 __device__ __forceinline__ uint32_t warp_push(uint32_t *counter)

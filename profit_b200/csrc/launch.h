@@ -47,6 +47,16 @@ cudaError_t launch_downsample64(const double *src, unsigned sw, unsigned sh, uns
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
                             int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask = nullptr);
+// psf point-source profiles in the FP32 pipeline: the stamp (forward) and the
+// sums of the adjoint image against the stamp and its centre derivatives.
+cudaError_t launch_psf_stamp32(const DevProfile *dev, const int *prof_begin, int batch, const double *psf,
+                               unsigned psf_w, unsigned psf_h, double psf_sx, double psf_sy, double scale_x,
+                               double scale_y, double offx, double offy, unsigned width, unsigned height,
+                               float *img_conv, float *img_plain, cudaStream_t s);
+cudaError_t launch_psf_adjoint32(const DevProfile *dev, const int *prof_begin, int batch, int nprof_max,
+                                 const double *psf, unsigned psf_w, unsigned psf_h, double psf_sx, double psf_sy,
+                                 double scale_x, double scale_y, double offx, double offy, unsigned width,
+                                 unsigned height, const float *g_conv, const float *g_plain, double *T, cudaStream_t s);
 // Masked convolution select, finesampling sum-down and output mask of the
 // FP32 pipeline (sel, mask_out optional), and their adjoint seeds.
 cudaError_t launch_model_finish32(const double *fine, unsigned cw, unsigned ch, const float *plain, const uint8_t *sel,

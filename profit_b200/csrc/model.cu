@@ -997,6 +997,13 @@ int tangent_stride(const pf_model *m)
 	return nt;
 }
 
+bool has_psf_profile(const pf_model *m)
+{
+	for (auto &p : m->profiles)
+		if (p.kind == PK_PSF) return true;
+	return false;
+}
+
 // Sersic profiles with adjust: those whose centre cusp may recurse past
 // level 2 (the count picks how the deep levels are launched).
 int cusp_count(const pf_model *m)
@@ -1049,6 +1056,10 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, tangent_stride(m), all_kinds(m),
 	                        cusp_count(m), q,
 	                        m->stream));
+	if (has_psf_profile(m))
+		PF_CUDA(launch_psf_stamp32(m->d_prof.as<DevProfile>(), m->d_prof_begin.as<int>(), 1, m->d_psf64.as<double>(),
+		                           m->psf_w, m->psf_h, m->psf_sx, m->psf_sy, m->sx / m->fs, m->sy / m->fs, a.padx,
+		                           a.pady, a.dw, a.dh, conv, plain, m->stream));
 	PF_CUDA(record_event(m->ev[1], m->stream));
 	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
 	double *model64 = m->d_model64.as<double>();
@@ -1074,6 +1085,11 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix,
 		                          tangent_stride(m), jpart,
 		                          jtick, d_out + ResultLayout::T0, m->stream));
+		if (has_psf_profile(m))
+			PF_CUDA(launch_psf_adjoint32(m->d_prof.as<DevProfile>(), m->d_prof_begin.as<int>(), 1, nprof,
+			                             m->d_psf64.as<double>(), m->psf_w, m->psf_h, m->psf_sx, m->psf_sy,
+			                             m->sx / m->fs, m->sy / m->fs, a.padx, a.pady, a.dw, a.dh, gconv, gplain,
+			                             d_out + ResultLayout::T0, m->stream));
 	}
 	PF_CUDA(record_event(m->ev[3], m->stream));
 	return PF_OK;
@@ -1087,6 +1103,8 @@ int enqueue_fp32(pf_model *m, const Analysis &a, bool want_grad, size_t nres, Qu
 	size_t n = (size_t)a.n_profiles;
 	PF_CUDA(record_event(m->ev[0], m->stream));
 	PF_CUDA(cudaMemcpyAsync(m->d_fprof.p, m->h_fprof.p, n * sizeof(FProfile), cudaMemcpyHostToDevice, m->stream));
+	if (has_psf_profile(m))  // the psf stamp reads the FP64 records
+		PF_CUDA(cudaMemcpyAsync(m->d_prof.p, m->h_prof.p, n * sizeof(DevProfile), cudaMemcpyHostToDevice, m->stream));
 	PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, m->stream));
 	PF_TRY(run_fp32(m, a, m->d_fprof.as<FProfile>(), q, want_grad, m->d_results.as<double>()));
 	char *hr = m->h_results.as<char>();
@@ -1122,6 +1140,8 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 	s.push_back(((uint64_t)a.ch << 32) | ((uint64_t)m->mask_w << 16) | m->mask_h);
 	s.push_back(((uint64_t)a.padx << 32) | a.pady);
 	s.push_back((uint64_t)m->profiles.size());
+	for (const DevBuf *b : {&m->d_prof, &m->d_psf64}) s.push_back((uint64_t)(uintptr_t)b->p);
+	for (auto &p : m->profiles) s.push_back((uint64_t)p.kind);  // which kernels run (AK variants, psf stamps)
 	s.push_back((uint64_t)(uintptr_t)m->h_results.p);
 	return s;
 }
@@ -1150,8 +1170,6 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 {
 	PF_TRY(ensure_stream(m));
 	PF_TRY(analyze(m, a));
-	for (auto &p : m->profiles)
-		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
 	if (m->has_data && (m->data_w != a.ow || m->data_h != a.oh))
 		return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
 	PF_TRY(upload_psf(m));
@@ -1324,6 +1342,10 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	PF_CUDA(launch_pixels32(fprof, m->d_prof_begin.as<int>(), C, a.dw, a.dh, m->sx / m->fs, m->sy / m->fs, conv, plain,
 	                        jac, nt, ak, q, s, fin.draw));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, nt, ak, C * cusp_count(m), q, s));
+	if (has_psf_profile(m))
+		PF_CUDA(launch_psf_stamp32(dev, m->d_prof_begin.as<int>(), C, m->d_psf64.as<double>(), m->psf_w, m->psf_h,
+		                           m->psf_sx, m->psf_sy, m->sx / m->fs, m->sy / m->fs, a.padx, a.pady, a.dw, a.dh,
+		                           conv, plain, s));
 	PF_CUDA(record_event(m->ev[1], s));
 	PF_TRY(forward_conv32(m, a, conv, plain, model64, C));
 	PF_CUDA(record_event(m->ev[2], s));
@@ -1340,6 +1362,10 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix, nt,
 		                          jpart, jtick, bs.d_T.as<double>(), s));
 	}
+	if (has_psf_profile(m))
+		PF_CUDA(launch_psf_adjoint32(dev, m->d_prof_begin.as<int>(), C, nprof, m->d_psf64.as<double>(), m->psf_w,
+		                             m->psf_h, m->psf_sx, m->psf_sy, m->sx / m->fs, m->sy / m->fs, a.padx, a.pady,
+		                             a.dw, a.dh, gconv, gplain, bs.d_T.as<double>(), s));
 	PF_CUDA(launch_batch_gradient(dev, nprof, C, ref_profile, ref_code, nrefs, bs.d_T.as<double>(),
 	                              bs.d_ll.as<double>(), invalid, out_ll, out_grad, s));
 	PF_CUDA(record_event(m->ev[3], s));
@@ -1354,8 +1380,6 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	PF_TRY(ensure_stream(m));
 	Analysis a;
 	PF_TRY(analyze(m, a));
-	for (auto &p : m->profiles)
-		if (p.kind == PK_PSF) return set_error(PF_E_INVALID, "the FP32 path does not support psf profiles yet");
 	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
 	if (m->data_w != a.ow || m->data_h != a.oh)
 		return set_error(PF_E_STATE, "data dimensions differ from the model's output dimensions");
@@ -1576,6 +1600,13 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 // or an error for parameters without an adjoint.
 int gradient_code(const ProfileParams &p, const char *name, int &code)
 {
+	if (p.kind == PK_PSF) {  // point source: its centre and magnitude
+		if (!std::strcmp(name, "xcen")) code = G_XCEN;
+		else if (!std::strcmp(name, "ycen")) code = G_YCEN;
+		else if (!std::strcmp(name, "mag")) code = G_MAG;
+		else return set_error(PF_E_INVALID, std::string("no gradient with respect to ") + name);
+		return PF_OK;
+	}
 	if (!is_radial_kind(p.kind))
 		return set_error(PF_E_INVALID, std::string("no gradient for parameters of ") + kind_name(p.kind) + " profiles");
 	if (p.kind == PK_SERSIC && p.rescale_flux)

@@ -982,6 +982,162 @@ cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned
 	return cudaGetLastError();
 }
 
+// libprofit's psf profile (psf.cpp:58-145) in the FP32 pipeline: the FP64
+// area-overlap stamp of the normalised PSF image that k_psf_stamp64 draws
+// (same ranges and quirks), and for the adjoint its derivatives in the
+// centre.  The stamp origin moves with xcen (px) and ycen (py), so for each
+// overlap ix = min(x + sx, psf_x + psf_sx) - max(x, psf_x),
+// d ix / d px = [psf_x + psf_sx < x + sx] - [psf_x > x] (likewise in y);
+// PSF pixels entering or leaving a range do so at zero overlap.
+struct PsfStamp {
+	double origin_x, origin_y;
+	unsigned x0, y0, nx, ny;
+};
+
+__device__ __forceinline__ bool psf_stamp_geom(const DevProfile &d, unsigned psf_w, unsigned psf_h, double psf_sx,
+                                               double psf_sy, double scale_x, double scale_y, double offx, double offy,
+                                               unsigned width, unsigned height, PsfStamp &g)
+{
+	g.origin_x = d.px + offx * scale_x - psf_w * psf_sx / 2;
+	const double end_x = d.px + offy * scale_y + psf_w * psf_sx / 2;
+	g.origin_y = d.py + offx * scale_x - psf_h * psf_sy / 2;
+	const double end_y = d.py + offy * scale_y + psf_h * psf_sy / 2;
+	g.x0 = bind_u(g.origin_x / scale_x, width - 1);
+	g.y0 = bind_u(g.origin_y / scale_y, height - 1);
+	const unsigned x1 = bind_u(end_x / scale_x, width - 1), y1 = bind_u(end_y / scale_y, height - 1);
+	if (x1 < g.x0 || y1 < g.y0) return false;
+	g.nx = x1 - g.x0 + 1;
+	g.ny = y1 - g.y0 + 1;
+	return true;
+}
+
+// Stamp value at target pixel (pix_x, pix_y) (flux 1); with D also its
+// derivatives in px and py.
+template <bool D>
+__device__ __forceinline__ double psf_stamp_pixel(const double *__restrict__ psf, unsigned psf_w, unsigned psf_h,
+                                                  double psf_sx, double psf_sy, double scale_x, double scale_y,
+                                                  const PsfStamp &g, unsigned pix_x, unsigned pix_y, double &dvx,
+                                                  double &dvy)
+{
+	const double y = pix_y * scale_y, x = pix_x * scale_x;
+	const int px0 = (int)bind_u(floor((x - g.origin_x) / psf_sx), psf_w - 1);
+	int px1 = (int)bind_u(floor((x - g.origin_x + scale_x) / psf_sx), psf_h - 1);
+	int py0 = (int)bind_u(floor((y - g.origin_y) / psf_sy), psf_w - 1);
+	const int py1 = (int)bind_u(floor((y - g.origin_y + scale_y) / psf_sy), psf_h - 1);
+	px1 = min(px1, (int)psf_w - 1);
+	py0 = min(py0, (int)psf_h - 1);
+	double val = 0;
+	dvx = dvy = 0;
+	for (int yy = py0; yy <= py1; yy++) {
+		const double psf_y = yy * psf_sy + g.origin_y;
+		const double iy = fmin(y + scale_y, psf_y + psf_sy) - fmax(y, psf_y);
+		const double diy = (psf_y + psf_sy < y + scale_y ? 1.0 : 0.0) - (psf_y > y ? 1.0 : 0.0);
+		for (int xx = px0; xx <= px1; xx++) {
+			const double psf_x = xx * psf_sx + g.origin_x;
+			const double ix = fmin(x + scale_x, psf_x + psf_sx) - fmax(x, psf_x);
+			const double w = psf[xx + yy * psf_w] / (psf_sx * psf_sy);
+			val += psf[xx + yy * psf_w] * (ix * iy) / (psf_sx * psf_sy);
+			if constexpr (D) {
+				const double dix = (psf_x + psf_sx < x + scale_x ? 1.0 : 0.0) - (psf_x > x ? 1.0 : 0.0);
+				dvx += w * dix * iy;
+				dvy += w * ix * diy;
+			}
+		}
+	}
+	return val;
+}
+
+// Forward: every psf profile of batch entry blockIdx.y adds flux x stamp to
+// its target image (after the radial pixel and level kernels).
+__global__ void k_psf_stamp32(const DevProfile *__restrict__ dev, const int *__restrict__ prof_begin,
+                              const double *__restrict__ psf, unsigned psf_w, unsigned psf_h, double psf_sx,
+                              double psf_sy, double scale_x, double scale_y, double offx, double offy, unsigned width,
+                              unsigned height, float *__restrict__ img_conv, float *__restrict__ img_plain)
+{
+	pdl_enter();
+	const int b = blockIdx.y;
+	const size_t npix = (size_t)width * height;
+	for (int pi = prof_begin[b]; pi < prof_begin[b + 1]; pi++) {
+		const DevProfile &d = dev[pi];
+		if (d.kind != PK_PSF) continue;
+		PsfStamp g;
+		if (!psf_stamp_geom(d, psf_w, psf_h, psf_sx, psf_sy, scale_x, scale_y, offx, offy, width, height, g)) continue;
+		float *img = (d.target == 0 ? img_conv : img_plain) + (size_t)b * npix;
+		for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < g.nx * g.ny; t += gridDim.x * blockDim.x) {
+			const unsigned pix_x = g.x0 + t % g.nx, pix_y = g.y0 + t / g.nx;
+			double dvx, dvy;
+			const double val = psf_stamp_pixel<false>(psf, psf_w, psf_h, psf_sx, psf_sy, scale_x, scale_y, g, pix_x,
+			                                          pix_y, dvx, dvy);
+			atomicAdd(&img[pix_x + (size_t)pix_y * width], (float)(val * d.psf_flux));
+		}
+	}
+}
+
+// Adjoint: block (blockIdx.x, blockIdx.y) = local profile index and batch
+// entry; a psf profile's T[0..2] = sum over its stamp of g x (stamp,
+// d stamp / d xcen, d stamp / d ycen), summed in FP64 in a fixed order.
+__global__ void __launch_bounds__(256)
+    k_psf_adjoint32(const DevProfile *__restrict__ dev, const int *__restrict__ prof_begin,
+                    const double *__restrict__ psf, unsigned psf_w, unsigned psf_h, double psf_sx, double psf_sy,
+                    double scale_x, double scale_y, double offx, double offy, unsigned width, unsigned height,
+                    const float *__restrict__ g_conv, const float *__restrict__ g_plain, double *__restrict__ T)
+{
+	pdl_enter();
+	const int b = blockIdx.y, pi = prof_begin[b] + (int)blockIdx.x;
+	if (pi >= prof_begin[b + 1]) return;
+	const DevProfile &d = dev[pi];
+	if (d.kind != PK_PSF) return;
+	PsfStamp g;
+	double acc[3] = {0, 0, 0};
+	if (psf_stamp_geom(d, psf_w, psf_h, psf_sx, psf_sy, scale_x, scale_y, offx, offy, width, height, g)) {
+		const float *gi = (d.target == 0 ? g_conv : g_plain) + (size_t)b * width * height;
+		for (unsigned t = threadIdx.x; t < g.nx * g.ny; t += blockDim.x) {
+			const unsigned pix_x = g.x0 + t % g.nx, pix_y = g.y0 + t / g.nx;
+			const double gv = gi[pix_x + (size_t)pix_y * width];
+			if (gv == 0.0) continue;
+			double dvx, dvy;
+			const double val = psf_stamp_pixel<true>(psf, psf_w, psf_h, psf_sx, psf_sy, scale_x, scale_y, g, pix_x,
+			                                         pix_y, dvx, dvy);
+			acc[0] += gv * val;
+			acc[1] += gv * dvx;
+			acc[2] += gv * dvy;
+		}
+	}
+	__shared__ double s_red[3][8];
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+	for (int k = 0; k < 3; k++) {
+		const double v = warp_sum(acc[k]);
+		if (lane == 0) s_red[k][wid] = v;
+	}
+	__syncthreads();
+	if (threadIdx.x < 3) {
+		double v = 0;
+		for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += s_red[threadIdx.x][w];
+		T[(size_t)pi * NTAN + threadIdx.x] = v;
+	}
+}
+
+cudaError_t launch_psf_stamp32(const DevProfile *dev, const int *prof_begin, int batch, const double *psf,
+                               unsigned psf_w, unsigned psf_h, double psf_sx, double psf_sy, double scale_x,
+                               double scale_y, double offx, double offy, unsigned width, unsigned height,
+                               float *img_conv, float *img_plain, cudaStream_t s)
+{
+	note_launches(1);
+	return launch_pdl(k_psf_stamp32, dim3(16, batch), dim3(256), 0, s, dev, prof_begin, psf, psf_w, psf_h, psf_sx,
+	                  psf_sy, scale_x, scale_y, offx, offy, width, height, img_conv, img_plain);
+}
+
+cudaError_t launch_psf_adjoint32(const DevProfile *dev, const int *prof_begin, int batch, int nprof_max,
+                                 const double *psf, unsigned psf_w, unsigned psf_h, double psf_sx, double psf_sy,
+                                 double scale_x, double scale_y, double offx, double offy, unsigned width,
+                                 unsigned height, const float *g_conv, const float *g_plain, double *T, cudaStream_t s)
+{
+	note_launches(1);
+	return launch_pdl(k_psf_adjoint32, dim3(nprof_max, batch), dim3(256), 0, s, dev, prof_begin, psf, psf_w, psf_h,
+	                  psf_sx, psf_sy, scale_x, scale_y, offx, offy, width, height, g_conv, g_plain, T);
+}
+
 // The FP32 pipeline's model image from the convolved fine image, for the
 // cases beyond one plain crop (Model::evaluate, model.cpp:307-334):
 //   fine(i, j) = plain drawing pixel where the drawing mask is 0 and the

@@ -214,13 +214,6 @@ __global__ void k_count_decisions(QueueSet q, int level, size_t npix)
 // libprofit's psf profile (psf.cpp:58-145): area-weighted resampling of the
 // normalised PSF image, one thread per covered target pixel.  The x/y offset
 // quirks of psf.cpp:79-82 and the height bound at psf.cpp:106 are kept.
-__device__ __forceinline__ unsigned bind_u(double value, unsigned max)
-{
-	int intval = (int)floor(value);
-	if (intval < 0) return 0;
-	unsigned u = (unsigned)intval;
-	return u < max ? u : max;
-}
 
 __global__ void k_psf_stamp64(const DevProfile *__restrict__ profiles, int p, const double *__restrict__ psf, unsigned psf_w,
                               unsigned psf_h, double psf_sx, double psf_sy, double scale_x, double scale_y,

@@ -573,9 +573,9 @@ def test_convolver_benchmark_keeps_the_faster_convolver():
 
 
 def _fs_mask_model(mask, fs, precision=PF_FP32, conv="brute", adjust=True, retfine=False):
-    """The calculation-mask case of the FP64 tests without the psf point
-    source (not in the FP32 form): a convolved bright Sersic, an unconvolved
-    Moffat and sky, finesampling fs."""
+    """The calculation-mask case of the FP64 tests: a convolved bright Sersic,
+    an unconvolved Moffat, sky and a psf point source (profile 3),
+    finesampling fs."""
     m = Model(100, 90, precision=precision)
     m.set_magzero(30.0)
     m.set_psf(W.moffat_psf(15, 3.0, 2.5))
@@ -585,6 +585,7 @@ def _fs_mask_model(mask, fs, precision=PF_FP32, conv="brute", adjust=True, retfi
     m.add_profile("sersic", xcen=52.3, ycen=44.1, re=6, nser=2.5, ang=30, axrat=0.6, convolve=True)
     m.add_profile("moffat", xcen=20.5, ycen=70.2, fwhm=3, con=2.5, mag=19, convolve=False)
     m.add_profile("sky", bg=0.1)
+    m.add_profile("psf", xcen=70.2, ycen=29.7, mag=16)
     if mask is not None:
         m.set_mask(mask, adjust)
     return m
@@ -628,7 +629,8 @@ def test_fp32_mask_without_adjustment_matches_fp64():
                                           (None, 2, "fft")])
 def test_fp32_adjoint_with_mask_and_finesampling_matches_fd64(kind, fs, conv):
     """d logL / d(parameters) through masked rendering, masked convolution,
-    the sum-down of the finesampled image and image &= mask, against FP64
+    the sum-down of the finesampled image and image &= mask, and the centre
+    and magnitude of a psf point source (its area-overlap stamp), against FP64
     central differences of the plain form (store and recompute adjoints, one
     proposal and a batch)."""
     from profit_b200._capi import PF_ADJOINT_RECOMPUTE, PF_ADJOINT_STORE
@@ -639,8 +641,8 @@ def test_fp32_adjoint_with_mask_and_finesampling_matches_fd64(kind, fs, conv):
     sigma = 1.0 + 0.1 * np.sqrt(np.abs(img))
     image = img + rng.normal(0.0, 1.0, img.shape) * sigma
     refs = [(0, "xcen"), (0, "ycen"), (0, "mag"), (0, "re"), (0, "nser"), (0, "ang"), (0, "axrat"),
-            (1, "xcen"), (1, "ycen"), (1, "mag")]
-    prop = [52.6, 43.8, 15.05, 6.2, 2.45, 31.0, 0.62, 20.3, 70.4, 19.03]
+            (1, "xcen"), (1, "ycen"), (1, "mag"), (3, "xcen"), (3, "ycen"), (3, "mag")]
+    prop = [52.6, 43.8, 15.05, 6.2, 2.45, 31.0, 0.62, 20.3, 70.4, 19.03, 70.35, 29.6, 16.03]
     m = _fs_mask_model(mask, fs, PF_FP64, conv)
     m.set_data(image, sigma)
     m.set_parameters(refs, prop)
