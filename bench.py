@@ -447,12 +447,27 @@ def sampler_batch_rate(args, torch, flush, n=4096, calls=3):
         ev1.synchronize()
         times.append(ev0.elapsed_time(ev1) / 1e3)
     torch.cuda.nvtx.range_pop()
+    # the same batch with the FFT convolver (the configuration names brute
+    # force; reported beside it, as the benchmark-chosen convolver would be)
+    m.set_convolver("fft")
+    m.loglike_grad_batch(refs, vals)
+    fft_times = []
+    for _ in range(calls):
+        flush.zero_()
+        torch.cuda.synchronize()
+        ev0.record()
+        m.loglike_grad_batch(refs, vals)
+        ev1.record()
+        ev1.synchronize()
+        fft_times.append(ev0.elapsed_time(ev1) / 1e3)
     m.close()
     rate = n / statistics.mean(times)
     return {"workload": "single Sersic 200x200, 31x31 Gaussian PSF, brute force, 8-parameter gradient; "
                         f"{n} proposals init + N(0, 0.05|init|) per call through pf_model_loglike_grad_batch "
                         "(host parameters in, logL + gradients out)",
             "value": rate, "unit": UNIT, "ms_per_call": 1e3 * statistics.mean(times),
+            "fft_convolver": {"value": n / statistics.mean(fft_times), "unit": UNIT,
+                              "ms_per_call": 1e3 * statistics.mean(fft_times)},
             "plain_fp64_fd_value": fd_rate, "speedup_vs_plain_fp64_fd": rate / fd_rate,
             "finite_fraction": float(np.isfinite(ll).mean())}
 
