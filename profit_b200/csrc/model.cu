@@ -1631,14 +1631,6 @@ int gradient_code(const ProfileParams &p, const char *name, int &code)
 	return PF_OK;
 }
 
-int combine_gradient(const ProfileParams &p, const DevProfile &d, const double *T, const char *name, double &g)
-{
-	int code = 0;
-	PF_TRY(gradient_code(p, name, code));
-	g = gradient_from_tangents(code, p.axrat, d, T);
-	return PF_OK;
-}
-
 int check_profile(pf_model *m, int index)
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");
