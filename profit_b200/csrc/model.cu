@@ -379,6 +379,17 @@ struct pf_model {
 namespace {
 
 constexpr int NPARTS = 296;  // likelihood partial sums (2 per SM)
+
+// Partial sums per image for the FP32 pipelines' likelihood of `batch`
+// images of n pixels: enough blocks in all to fill the GPU, at least about
+// eight pixels per thread (a batch of thousands of small images would
+// otherwise spend its time reducing near-empty blocks), at most NPARTS.
+inline int like_parts(int n, int batch)
+{
+	const int fill = (148 * 16 + batch - 1) / std::max(batch, 1);
+	const int work = (n + 2047) / 2048;
+	return std::max(1, std::min(NPARTS, std::min(fill, work)));
+}
 constexpr size_t CTRL_WORDS = 64;  // counts[16], overflow, ...
 
 int analyze(pf_model *m, Analysis &a)
@@ -983,7 +994,8 @@ int enqueue_like(pf_model *m, const double *model64, int nout, int batch, double
 	PF_CUDA(ensure(m->d_likestats, (size_t)batch * LIKE_SCRATCH_PER_IMAGE * 8));
 	PF_CUDA(launch_like64(m->like_kind, model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
 	                      m->has_region ? m->d_region.as<uint8_t>() : nullptr, nout, batch, 0,
-	                      m->d_partials.as<double2>(), NPARTS, m->d_likestats.as<double>(), out, wseed, s));
+	                      m->d_partials.as<double2>(), like_parts(nout, batch), m->d_likestats.as<double>(), out,
+	                      wseed, s));
 	return PF_OK;
 }
 
@@ -2529,8 +2541,8 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
 	                           plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout,
 	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
 	PF_CUDA(launch_loglike64_batch(model64, ch.data.as<double>(), ch.sigma.as<double>(), ch.region.as<uint8_t>(),
-	                               (int)nout, C, (int)nout, m->d_partials.as<double2>(), NPARTS, ch.ll.as<double>(),
-	                               wseed, s));
+	                               (int)nout, C, (int)nout, m->d_partials.as<double2>(), like_parts((int)nout, C),
+	                               ch.ll.as<double>(), wseed, s));
 	PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
 	sb = conv32_scratch_bytes(a.dw, a.dh, C);
 	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)ch.pw, 1 - (int)ch.ph, ch.psf32.as<float>(), ch.pw, ch.ph, gconv,
