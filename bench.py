@@ -545,6 +545,7 @@ def catalogue_rate(args, torch, flush, n=10000, calls=2, fd_sample=6):
     cat.loglike_grad()  # warm-up: uploads, bucketing, convolution tuning
     first_s = time.perf_counter() - t0
     dev, wall = [], []
+    torch.cuda.nvtx.range_push("catalogue")
     for _ in range(calls):
         flush.zero_()
         torch.cuda.synchronize()
@@ -552,6 +553,7 @@ def catalogue_rate(args, torch, flush, n=10000, calls=2, fd_sample=6):
         ll, _ = cat.loglike_grad()
         wall.append(time.perf_counter() - t0)
         dev.append(cat.last_time_ms() / 1e3)
+    torch.cuda.nvtx.range_pop()
     cat.close()
     # plain FP64 + FD on a sample of the same galaxies
     fd_t, fd_n = 0.0, 0

@@ -597,7 +597,7 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 
 // Deep: FP64 sub-points (levels >= 3, the Sersic cusp).
 template <bool AK, bool J, bool Deep>
-__global__ void __launch_bounds__(256) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
+__global__ void __launch_bounds__(256, (AK && !Deep) ? 3 : 2) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
                                                  float *__restrict__ img_conv, float *__restrict__ img_plain,
                                                  float *__restrict__ jac, int nt, QueueSet q)
 {
