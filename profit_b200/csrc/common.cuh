@@ -69,6 +69,10 @@ struct SubItem {
 // counts[L] keeps counting past cap[L]; the host reads it back to size a
 // retry, so an overflow is reported (never written out of bounds).
 constexpr int MAX_LEVELS = 16;
+// Control words after counts[MAX_LEVELS], overflow and maxres: per wide level
+// (0..2) a histogram of the items' radial kinds and the scatter cursors.
+constexpr int KIND_CTR = MAX_LEVELS + 2;
+constexpr int N_RADIAL_KINDS = 6;
 // Accepted sub-points of an item (res^2 <= 256 bits), recorded by the
 // forward pass when the adjoint recomputes instead of storing tangents.
 constexpr int MASK_WORDS = 8;
@@ -80,6 +84,9 @@ struct QueueSet {
 	int32_t *decisions;    // optional [n_profiles][npix] subsample_pixel calls per pixel
 	unsigned long long *level_counts;  // optional [n_profiles][MAX_LEVELS]
 	uint32_t *maxres = nullptr;  // optional: largest resolution of the level-0 items pushed
+	// optional: per level, the items' indices grouped by profile kind (filled
+	// by launch_levels32 before each wide level when set; same offsets as items)
+	uint32_t *perm = nullptr;
 	uint32_t levels;
 	uint32_t off[MAX_LEVELS];
 	uint32_t cap[MAX_LEVELS];

@@ -347,6 +347,7 @@ struct pf_model {
 	std::vector<uint64_t> mask_key;  // what the device masks were built for
 	uint64_t mask_version = 0;       // bumped by pf_model_set_mask
 	DevBuf d_model_fine, d_seed_fine;  // FP32 pipeline: convolved fine image, fine seed
+	DevBuf d_perm;                     // level items grouped by profile kind (QueueSet::perm)
 	DevBuf d_mask_draw, d_mask_out;
 	int like_kind = LIKE_NORM;
 	DevBuf d_likestats;
@@ -625,8 +626,11 @@ int prepare_fft(pf_model *m, const Analysis &a, int batch, bool need32)
 
 // Queue segments per level; capacities start from a pixel-count estimate and
 // grow after an overflow.
+// kind_groups: the level items are taken kind by kind (models with profiles
+// of every kind, launch_levels32), which needs an index buffer beside them.
 int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q, int32_t *decisions,
-                  unsigned long long *level_counts, bool with_masks = false, bool reset = true)
+                  unsigned long long *level_counts, bool with_masks = false, bool reset = true,
+                  bool kind_groups = false)
 {
 	if (m->caps.size() != (size_t)MAX_LEVELS) {
 		m->caps.assign(MAX_LEVELS, 0);
@@ -653,6 +657,11 @@ int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q
 	if (with_masks) {
 		PF_CUDA(ensure(m->d_masks, total * MASK_WORDS * sizeof(uint32_t)));
 		q.masks = m->d_masks.as<uint32_t>();
+	}
+	q.perm = nullptr;
+	if (kind_groups) {
+		PF_CUDA(ensure(m->d_perm, total * sizeof(uint32_t)));
+		q.perm = m->d_perm.as<uint32_t>();
 	}
 	q.items = m->d_items.as<SubItem>();
 	q.counts = m->d_ctrl.as<uint32_t>();
@@ -1145,7 +1154,7 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region, &m->d_convsplit, &m->d_jac_partials, &m->d_jac_tickets, &m->d_likestats};
 	for (auto *b : bufs) s.push_back((uint64_t)(uintptr_t)b->p);
 	// calculation mask and finesampling steps (finish32_of) and their buffers
-	for (const DevBuf *b : {&m->d_mask_draw, &m->d_mask_out, &m->d_model_fine, &m->d_seed_fine})
+	for (const DevBuf *b : {&m->d_mask_draw, &m->d_mask_out, &m->d_model_fine, &m->d_seed_fine, &m->d_perm})
 		s.push_back((uint64_t)(uintptr_t)b->p);
 	s.push_back(((uint64_t)a.mask << 0) | ((uint64_t)a.mask_conv << 1) | ((uint64_t)a.mask_adjusted << 2) |
 	            ((uint64_t)m->adjust_mask << 3) | ((uint64_t)m->fs << 8) | ((uint64_t)a.cw << 24));
@@ -1218,7 +1227,7 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 
 	for (int attempt = 0; attempt < 8; attempt++) {
 		QueueSet q;
-		PF_TRY(prepare_queue(m, a, npix * nprof, q, nullptr, nullptr));
+		PF_TRY(prepare_queue(m, a, npix * nprof, q, nullptr, nullptr, false, true, all_kinds(m)));
 		bool replayed = false;
 		if (want_grad && m->graph_exec && m->graph_sig == graph_signature(m, a, want_grad, q)) {
 			PF_CUDA(cudaGraphLaunch(m->graph_exec, m->stream));
@@ -1547,7 +1556,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			QueueSet q;
 			// the pipeline zeroes the counters itself; they sit behind the
 			// results so that one copy brings both back
-			PF_TRY(prepare_queue(m, a, npix * nprof * C, q, nullptr, nullptr, recompute, false));
+			PF_TRY(prepare_queue(m, a, npix * nprof * C, q, nullptr, nullptr, recompute, false, all_kinds(m)));
 			q.counts = reinterpret_cast<uint32_t *>(bs.d_out.as<char>() + (size_t)C * (1 + nrefs) * 8);
 			q.overflow = q.counts + MAX_LEVELS;
 			q.maxres = q.counts + MAX_LEVELS + 1;
@@ -2509,7 +2518,7 @@ int cat_build(pf_catalogue *c)
 	Analysis a;
 	a.levels = levels;
 	QueueSet q;
-	PF_TRY(prepare_queue(m, a, qpix, q, nullptr, nullptr));
+	PF_TRY(prepare_queue(m, a, qpix, q, nullptr, nullptr, false, true, true));  // sizes the kind-group buffer too
 	PF_CUDA(cudaStreamSynchronize(m->stream));
 	c->built = true;
 	return PF_OK;
@@ -2525,7 +2534,7 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
 	const Analysis a = cat_analysis(ch);
 	const size_t npix = ch.npix(), nout = ch.nout();
 	QueueSet q;
-	PF_TRY(prepare_queue(m, a, npix * C, q, nullptr, nullptr));
+	PF_TRY(prepare_queue(m, a, npix * C, q, nullptr, nullptr, false, true, ch.ak));
 	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *jac = m->d_jac.as<float>();
 	float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>(), *wseed = m->d_wseed.as<float>();
 	double *model64 = m->d_model64.as<double>();

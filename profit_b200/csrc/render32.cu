@@ -618,8 +618,11 @@ __global__ void __launch_bounds__(256, (AK && !Deep) ? 3 : 2) k_level32(const FP
 		cpi = (maxres * maxres + 31) / 32;
 	}
 	const uint32_t total = n * cpi;
+	// kind-grouped order when the items were grouped (models with every kind)
+	const uint32_t *perm = (!Deep && q.perm) ? q.perm + q.off[level] : nullptr;
 	for (uint32_t w = blockIdx.x * (blockDim.x >> 5) + wib; w < total; w += nwarps) {
-		const uint32_t item = w / cpi, chunk = w - item * cpi;
+		const uint32_t slot = w / cpi, chunk = w - slot * cpi;
+		const uint32_t item = perm ? perm[slot] : slot;
 		const SubItem it = items[item];
 		const unsigned base0 = cpi == 1 ? 0u : chunk * 32, base1 = cpi == 1 ? 256u : base0 + 32;
 		if (base0 >= (unsigned)it.res * it.res) continue;
@@ -920,11 +923,78 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
 	                  q, mask);
 }
 
+// Kind grouping of one wide level's items (models with profiles of every
+// kind): the level kernel then takes the items kind by kind, so the warps
+// resident on an SM run one profile function at a time instead of all six
+// (the code of all six does not fit the instruction cache).  Each block
+// takes a contiguous range of items: it counts kinds in shared memory,
+// reserves its slots per kind with one global atomic per kind (after the
+// histogram pass fixed the kind bases), then scatters the item indices.
+constexpr int KG_ITEMS_PER_BLOCK = 2048;
+
+__global__ void k_kind_hist(const FProfile *__restrict__ profiles, QueueSet q, int level)
+{
+	pdl_enter();
+	const uint32_t n = min(q.counts[level], q.cap[level]);
+	const SubItem *items = q.items + q.off[level];
+	__shared__ uint32_t s_h[N_RADIAL_KINDS];
+	if (threadIdx.x < N_RADIAL_KINDS) s_h[threadIdx.x] = 0;
+	__syncthreads();
+	const uint32_t i0 = blockIdx.x * KG_ITEMS_PER_BLOCK, i1 = min(n, i0 + KG_ITEMS_PER_BLOCK);
+	for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+		const int k = profiles[items[i].profile].kind - PK_SERSIC;
+		if (k >= 0 && k < N_RADIAL_KINDS) atomicAdd(&s_h[k], 1u);
+	}
+	__syncthreads();
+	uint32_t *hist = q.counts + KIND_CTR + level * 2 * N_RADIAL_KINDS;
+	if (threadIdx.x < N_RADIAL_KINDS && s_h[threadIdx.x]) atomicAdd(&hist[threadIdx.x], s_h[threadIdx.x]);
+}
+
+__global__ void k_kind_scatter(const FProfile *__restrict__ profiles, QueueSet q, int level)
+{
+	pdl_enter();
+	const uint32_t n = min(q.counts[level], q.cap[level]);
+	const SubItem *items = q.items + q.off[level];
+	const uint32_t *hist = q.counts + KIND_CTR + level * 2 * N_RADIAL_KINDS;
+	uint32_t *cursor = q.counts + KIND_CTR + level * 2 * N_RADIAL_KINDS + N_RADIAL_KINDS;
+	__shared__ uint32_t s_n[N_RADIAL_KINDS], s_at[N_RADIAL_KINDS];
+	if (threadIdx.x < N_RADIAL_KINDS) s_n[threadIdx.x] = 0;
+	__syncthreads();
+	const uint32_t i0 = blockIdx.x * KG_ITEMS_PER_BLOCK, i1 = min(n, i0 + KG_ITEMS_PER_BLOCK);
+	for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+		const int k = profiles[items[i].profile].kind - PK_SERSIC;
+		if (k >= 0 && k < N_RADIAL_KINDS) atomicAdd(&s_n[k], 1u);
+	}
+	__syncthreads();
+	if (threadIdx.x < N_RADIAL_KINDS) {
+		uint32_t base = 0;
+		for (int k = 0; k < (int)threadIdx.x; k++) base += hist[k];
+		s_at[threadIdx.x] = s_n[threadIdx.x] ? base + atomicAdd(&cursor[threadIdx.x], s_n[threadIdx.x]) : 0;
+	}
+	__syncthreads();
+	uint32_t *perm = q.perm + q.off[level];
+	for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+		const int k = profiles[items[i].profile].kind - PK_SERSIC;
+		// every queued item is a radial profile's; an out-of-range kind would
+		// leave its slot to the identity
+		const uint32_t pos = (k >= 0 && k < N_RADIAL_KINDS) ? atomicAdd(&s_at[k], 1u) : i;
+		perm[pos] = i;
+	}
+}
+
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
                             float *jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s)
 {
 	const int wide = n_levels < 3 ? n_levels : 3;
 	for (int l = 0; l < wide; l++) {
+		if (q.perm) {
+			// grid over the level's capacity (its count is only known on the device)
+			const unsigned blocks = q.cap[l] / KG_ITEMS_PER_BLOCK + 1;
+			cudaError_t e = launch_pdl(k_kind_hist, dim3(blocks), dim3(256), 0, s, profiles, q, l);
+			if (e == cudaSuccess) e = launch_pdl(k_kind_scatter, dim3(blocks), dim3(256), 0, s, profiles, q, l);
+			note_launches(2);
+			if (e != cudaSuccess) return e;
+		}
 		auto k = all_kinds ? (jac ? k_level32<true, true, false> : k_level32<true, false, false>)
 		                   : (jac ? k_level32<false, true, false> : k_level32<false, false, false>);
 		cudaError_t e = launch_pdl(k, dim3(148 * 8), dim3(256), 0, s, profiles, l, npix, img_conv, img_plain, jac, nt, q);
