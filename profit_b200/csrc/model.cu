@@ -383,12 +383,12 @@ constexpr int NPARTS = 296;  // likelihood partial sums (2 per SM)
 
 // Partial sums per image for the FP32 pipelines' likelihood of `batch`
 // images of n pixels: enough blocks in all to fill the GPU, at least about
-// eight pixels per thread (a batch of thousands of small images would
+// two pixels per thread (a batch of thousands of small images would
 // otherwise spend its time reducing near-empty blocks), at most NPARTS.
 inline int like_parts(int n, int batch)
 {
 	const int fill = (148 * 16 + batch - 1) / std::max(batch, 1);
-	const int work = (n + 2047) / 2048;
+	const int work = (n + 511) / 512;
 	return std::max(1, std::min(NPARTS, std::min(fill, work)));
 }
 constexpr size_t CTRL_WORDS = 64;  // counts[16], overflow, ...
