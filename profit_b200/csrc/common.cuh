@@ -101,6 +101,17 @@ struct FProfile {
 	float re, nser, bn, B, inv_nB, dbn_dn;
 	float rscale, con, a, b, rb, rc, rt, h1, h2, king_t;
 	float flux_scale;
+	// Per-profile constants of the FP32 profile functions, formed in FP64 and
+	// rounded once (an FP32 reciprocal of an FP32 parameter would round twice,
+	// and that error is the same at every pixel): inv_B = 1/B and
+	// box_e = (2 - B)/(2 B) for the boxy radius, and by kind
+	//   sersic:     1/re, 1/nser
+	//   moffat:     1/rscale;  ferrer: 1/rout
+	//   king:       1/a, 1/rc, 1/(1 + (rt/rc)^2), ln(1 + (rt/rc)^2)
+	//   brokenexp:  1/h1, 1/h2, 1/a
+	//   coresersic: 1/a, 1/nser, ln rb, ln re, rb^a, re^-a, 1/(nser a)
+	float inv_B, box_e;
+	float k[7];
 	double cx, cy, img_sx, img_sy, flux_scale64;
 };
 
@@ -148,6 +159,40 @@ PF_HD inline FProfile to_fprofile(const DevProfile &d, const ProfileParams &p)
 		double c = p.con, t = pow(2.0, 1.0 / c);
 		f.a = (float)(1.0 / p.fwhm);
 		f.b = (float)(0.5 * t * log(2.0) / (c * c * (t - 1.0)));
+	}
+	const double B = p.box + 2;
+	f.inv_B = (float)(1.0 / B);
+	f.box_e = (float)((2.0 - B) / (2.0 * B));
+	switch (d.kind) {
+	case PK_SERSIC:
+		f.k[0] = (float)(1.0 / d.re);
+		f.k[1] = (float)(1.0 / d.nser);
+		break;
+	case PK_MOFFAT:
+	case PK_FERRER: f.k[0] = (float)(1.0 / d.rscale); break;
+	case PK_KING: {
+		const double Y = 1.0 + (d.rt / d.rc) * (d.rt / d.rc);
+		f.k[0] = (float)(1.0 / d.a);
+		f.k[1] = (float)(1.0 / d.rc);
+		f.k[2] = (float)(1.0 / Y);
+		f.k[3] = (float)log(Y);
+		break;
+	}
+	case PK_BROKENEXP:
+		f.k[0] = (float)(1.0 / d.h1);
+		f.k[1] = (float)(1.0 / d.h2);
+		f.k[2] = (float)(1.0 / d.a);
+		break;
+	case PK_CORESERSIC:
+		f.k[0] = (float)(1.0 / d.a);
+		f.k[1] = (float)(1.0 / d.nser);
+		f.k[2] = (float)log(d.rb);
+		f.k[3] = (float)log(d.re);
+		f.k[4] = (float)pow(d.rb, d.a);
+		f.k[5] = (float)pow(d.re, -d.a);
+		f.k[6] = (float)(1.0 / (d.nser * d.a));
+		break;
+	default: break;
 	}
 	return f;
 }

@@ -65,11 +65,45 @@ __device__ __forceinline__ float t_sqrt<float>(float x) { return sqrtf(x); }
 template <>
 __device__ __forceinline__ double t_sqrt<double>(double x) { return sqrt(x); }
 
-// x * log(x) with the limit 0 at x = 0
+// a / b for divisors that vary from point to point.  The FP32 form takes the
+// approximate quotient (reciprocal and one multiply, within 2 ulp; every
+// divisor here is a normal number or guarded), a fraction of the IEEE
+// division's instructions; the FP64 form keeps the IEEE quotient.  Per-profile
+// constants (1/re, 1/n, ...) stay IEEE divisions: their rounding is the same
+// at every pixel, so an approximate reciprocal would act as a shifted
+// parameter, while the per-point errors average out over the image.
 template <class T>
-__device__ __forceinline__ T xlogx(T x)
+__device__ __forceinline__ T qdiv(T a, T b);
+template <>
+__device__ __forceinline__ float qdiv<float>(float a, float b) { return __fdividef(a, b); }
+template <>
+__device__ __forceinline__ double qdiv<double>(double a, double b) { return a / b; }
+
+// x^y for x >= 0 given lx = ln x: exp(y lx), with pow's values at x = 0.
+// The profiles need ln x for their partials anyway, so a power costs one
+// exponential instead of pow's own logarithm and exponential.
+template <class T>
+__device__ __forceinline__ T pow_ln(T x, T lx, T y)
 {
-	return x > T(0) ? x * t_log<T>(x) : T(0);
+	if (x > T(0)) return t_exp<T>(y * lx);
+	return y > T(0) ? T(0) : (y == T(0) ? T(1) : T(INFINITY));
+}
+
+// x^B for x >= 0 and a boxiness exponent B = 2 + box near 2, given lx = ln x:
+// x^2 exp((B - 2) lx).  The exponential's argument stays small, so the
+// rounding of lx is not amplified by |B lx| as in exp(B lx).
+template <class T>
+__device__ __forceinline__ T pow_box(T x, T lx, T B)
+{
+	if (x > T(0)) return x * x * t_exp<T>((B - T(2)) * lx);
+	return pow_ln<T>(x, lx, B);
+}
+
+// ln x for x > 0, else 0 (every use multiplies it by a factor that is 0 there)
+template <class T>
+__device__ __forceinline__ T ln_pos(T x)
+{
+	return x > T(0) ? t_log<T>(x) : T(0);
 }
 
 // Sersic: f = exp(-bn (base^(1/(n B)) - 1)), base = |x/re|^B + |y/re|^B.
@@ -79,36 +113,44 @@ template <class T>
 __device__ __forceinline__ Tan<T> sersic_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
-	const T re = (T)p.re, B = (T)p.B, n = (T)p.nser, bn = (T)p.bn;
-	const T u = fabs(xp) / re, v = fabs(yp) / re;
-	T uB, vB, base;
+	const T B = (T)p.B, n = (T)p.nser, bn = (T)p.bn;
+	const T ire = (T)p.k[0], in = (T)p.k[1], iB = (T)p.inv_B;
+	const T u = fabs(xp) * ire, v = fabs(yp) * ire;
+	const T lu = ln_pos<T>(u), lv = ln_pos<T>(v);
+	T uB, vB;
 	if (B == T(2)) {
 		uB = u * u;
 		vB = v * v;
 	}
 	else {
-		uB = t_pow<T>(u, B);
-		vB = t_pow<T>(v, B);
+		uB = pow_box<T>(u, lu, B);
+		vB = pow_box<T>(v, lv, B);
 	}
-	base = uB + vB;
+	const T base = uB + vB;
 	if (!(base > T(0))) {
 		t.f = t_exp<T>(bn);
 		return t;
 	}
-	const T inv_nB = T(1) / (n * B);
+	const T inv_nB = (T)p.inv_nB;
 	const T lnb = t_log<T>(base);
 	const T rf = t_exp<T>(lnb * inv_nB);
 	const T f = t_exp<T>(-bn * (rf - T(1)));
 	const T dfdrf = -bn * f;
-	const T g = dfdrf * rf * inv_nB / base;  // df/dbase
-	// dbase/dx' = B * uB / x'
+	const T h = dfdrf * rf * inv_nB;   // df/d ln(base)
+	const T g = qdiv<T>(h, base);      // df/dbase
 	t.f = f;
-	t.fx = xp != T(0) ? g * B * uB / xp : T(0);
-	t.fy = yp != T(0) ? g * B * vB / yp : T(0);
-	t.s[0] = -dfdrf * rf / (n * re);
-	t.s[1] = dfdrf * (-rf * lnb * inv_nB / n) - (rf - T(1)) * f * (T)p.dbn_dn;
-	const T dbase_dB = (u > T(0) ? uB * t_log<T>(u) : T(0)) + (v > T(0) ? vB * t_log<T>(v) : T(0));
-	t.s[2] = dfdrf * rf * inv_nB * (dbase_dB / base - lnb / B);
+	// dbase/dx' = B uB / x' (= 2 x' / re^2 at B = 2)
+	if (B == T(2)) {
+		t.fx = g * T(2) * xp * ire * ire;
+		t.fy = g * T(2) * yp * ire * ire;
+	}
+	else {
+		t.fx = xp != T(0) ? g * B * qdiv<T>(uB, xp) : T(0);
+		t.fy = yp != T(0) ? g * B * qdiv<T>(vB, yp) : T(0);
+	}
+	t.s[0] = -dfdrf * rf * in * ire;
+	t.s[1] = -h * lnb * in - (rf - T(1)) * f * (T)p.dbn_dn;
+	t.s[2] = h * (qdiv<T>(uB * lu + vB * lv, base) - lnb * iB);
 	return t;
 }
 
@@ -118,22 +160,27 @@ template <class T>
 __device__ __forceinline__ void boxy_radius(const FProfile &p, T xp, T yp, T &r, T &drdx, T &drdy, T &drdB)
 {
 	const T B = (T)p.B, ax = fabs(xp), ay = fabs(yp);
+	const T lx = ln_pos<T>(ax), ly = ln_pos<T>(ay);
 	if (B == T(2)) {
 		const T S = xp * xp + yp * yp;
 		r = t_sqrt<T>(S);
-		drdx = r > T(0) ? xp / r : T(0);
-		drdy = r > T(0) ? yp / r : T(0);
-		drdB = S > T(0) ? r * ((xlogx<T>(ax) * ax + xlogx<T>(ay) * ay) / (B * S) - t_log<T>(S) / (B * B)) : T(0);
+		const T ir = r > T(0) ? qdiv<T>(T(1), r) : T(0);
+		drdx = xp * ir;
+		drdy = yp * ir;
+		// r ((x'^2 ln|x'| + y'^2 ln|y'|) / (2 S) - ln S / 4)
+		drdB = S > T(0) ? r * ((ax * ax * lx + ay * ay * ly) * ir * ir * T(0.5) - t_log<T>(S) * T(0.25)) : T(0);
 	}
 	else {
-		const T xB = t_pow<T>(ax, B), yB = t_pow<T>(ay, B);
+		const T xB = pow_box<T>(ax, lx, B), yB = pow_box<T>(ay, ly, B);
 		const T S = xB + yB;
-		r = S > T(0) ? t_pow<T>(S, T(1) / B) : T(0);
-		drdx = (r > T(0) && xp != T(0)) ? (xB / S) * r / xp : T(0);
-		drdy = (r > T(0) && yp != T(0)) ? (yB / S) * r / yp : T(0);
-		const T lx = ax > T(0) ? xB * t_log<T>(ax) : T(0);
-		const T ly = ay > T(0) ? yB * t_log<T>(ay) : T(0);
-		drdB = S > T(0) ? r * ((lx + ly) / (B * S) - t_log<T>(S) / (B * B)) : T(0);
+		const T iB = (T)p.inv_B;
+		const T lS = ln_pos<T>(S);
+		// S^(1/B) = sqrt(S) S^(1/B - 1/2), the second factor's exponent small
+		r = S > T(0) ? t_sqrt<T>(S) * t_exp<T>(lS * (T)p.box_e) : T(0);
+		const T iS = S > T(0) ? qdiv<T>(T(1), S) : T(0);
+		drdx = (r > T(0) && xp != T(0)) ? qdiv<T>(xB * iS * r, xp) : T(0);
+		drdy = (r > T(0) && yp != T(0)) ? qdiv<T>(yB * iS * r, yp) : T(0);
+		drdB = S > T(0) ? r * iB * ((xB * lx + yB * ly) * iS - lS * iB) : T(0);
 	}
 }
 
@@ -152,16 +199,16 @@ template <class T>
 __device__ __forceinline__ Tan<T> moffat_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
-	const T rs = (T)p.rscale, con = (T)p.con;
+	const T irs = (T)p.k[0], con = (T)p.con;
 	T r, drdx, drdy, drdB;
 	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
-	const T rf = r / rs;
+	const T rf = r * irs;
 	const T q = T(1) + rf * rf;
 	const T lq = t_log<T>(q);
 	const T f = t_exp<T>(-con * lq);
-	const T dfdrf = -T(2) * con * rf * f / q;
+	const T dfdrf = qdiv<T>(-T(2) * con * rf * f, q);
 	t.f = f;
-	radial_chain<T>(t, dfdrf / rs, drdx, drdy, drdB, 2);
+	radial_chain<T>(t, dfdrf * irs, drdx, drdy, drdB, 2);
 	t.s[0] = dfdrf * (-rf) * (T)p.a;           // a holds 1/fwhm for Moffat
 	t.s[1] = -lq * f + dfdrf * (-rf) * (T)p.b;  // b holds dln(rscale)/dcon
 	return t;
@@ -175,19 +222,22 @@ __device__ __forceinline__ Tan<T> ferrer_tan(const FProfile &p, T xp, T yp)
 	Tan<T> t = {};
 	T r, drdx, drdy, drdB;
 	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
-	const T rout = (T)p.rscale, a = (T)p.a, e = T(2) - (T)p.b;
-	const T rf = r / rout;
+	const T irout = (T)p.k[0], a = (T)p.a, e = T(2) - (T)p.b;
+	const T rf = r * irout;
 	if (!(rf < T(1))) return t;
-	const T rfe = t_pow<T>(rf, e);
+	const T lrf = ln_pos<T>(rf);
+	const T rfe = pow_ln<T>(rf, lrf, e);
 	const T g = T(1) - rfe;
-	const T f = t_pow<T>(g, a);
+	const T lg = ln_pos<T>(g);
+	const T f = pow_ln<T>(g, lg, a);
 	t.f = f;
 	if (!(g > T(0)) || !(r > T(0))) return t;
-	const T fr = -a * e * f * rfe / (g * r);
+	const T ig = qdiv<T>(T(1), g);
+	const T fr = -a * e * f * rfe * ig * qdiv<T>(T(1), r);
 	radial_chain<T>(t, fr, drdx, drdy, drdB, 3);
-	t.s[0] = -fr * r / rout;
-	t.s[1] = f * t_log<T>(g);
-	t.s[2] = a * f * rfe * t_log<T>(rf) / g;
+	t.s[0] = -fr * r * irout;
+	t.s[1] = f * lg;
+	t.s[2] = a * f * rfe * lrf * ig;
 	return t;
 }
 
@@ -201,23 +251,28 @@ __device__ __forceinline__ Tan<T> king_tan(const FProfile &p, T xp, T yp)
 	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
 	const T rc = (T)p.rc, rt = (T)p.rt, a = (T)p.a, kt = (T)p.king_t;
 	if (!(r < rt)) return t;
-	const T X = T(1) + (r / rc) * (r / rc);
-	const T u = T(1) / t_pow<T>(X, T(1) / a);
+	const T ia = (T)p.k[0], irc = (T)p.k[1];
+	const T X = T(1) + (r * irc) * (r * irc);
+	const T lX = t_log<T>(X);
+	const T u = t_exp<T>(-lX * ia);
 	const T D = u - kt;
-	const T f = t_pow<T>(D, a);
+	// D <= 0 only by rounding at r ~ rt, where pow keeps its own sign rules
+	const T lD = ln_pos<T>(D);
+	const T f = D > T(0) ? t_exp<T>(a * lD) : t_pow<T>(D, a);
 	t.f = f;
 	if (!(D > T(0))) return t;
-	const T Y = T(1) + (rt / rc) * (rt / rc);
-	const T du_dr = -T(2) * r * u / (a * rc * rc * X);
-	const T du_drc = T(2) * r * r * u / (a * rc * rc * rc * X);
-	const T dt_drc = T(2) * rt * rt * kt / (a * rc * rc * rc * Y);
-	const T dt_drt = -T(2) * rt * kt / (a * rc * rc * Y);
-	const T du_da = u * t_log<T>(X) / (a * a), dt_da = kt * t_log<T>(Y) / (a * a);
-	const T c = a * f / D;
+	const T iX = qdiv<T>(T(1), X), iY = (T)p.k[2];
+	const T k2 = T(2) * ia * irc * irc;
+	const T du_dr = -k2 * r * u * iX;
+	const T du_drc = k2 * r * r * u * irc * iX;
+	const T dt_drc = k2 * rt * rt * kt * irc * iY;
+	const T dt_drt = -k2 * rt * kt * iY;
+	const T du_da = u * lX * ia * ia, dt_da = kt * (T)p.k[3] * ia * ia;
+	const T c = a * f * qdiv<T>(T(1), D);
 	radial_chain<T>(t, c * du_dr, drdx, drdy, drdB, 3);
 	t.s[0] = c * (du_drc - dt_drc);
 	t.s[1] = -c * dt_drt;
-	t.s[2] = f * t_log<T>(D) + c * (du_da - dt_da);
+	t.s[2] = f * lD + c * (du_da - dt_da);
 	return t;
 }
 
@@ -231,21 +286,22 @@ __device__ __forceinline__ Tan<T> brokenexp_tan(const FProfile &p, T xp, T yp)
 	Tan<T> t = {};
 	T r, drdx, drdy, drdB;
 	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
-	const T a = (T)p.a, h1 = (T)p.h1, h2 = (T)p.h2, z = r - (T)p.rb;
-	const T expo = T(1) / h1 - T(1) / h2;
+	const T a = (T)p.a, z = r - (T)p.rb;
+	const T ih1 = (T)p.k[0], ih2 = (T)p.k[1], ia = (T)p.k[2];
+	const T expo = ih1 - ih2;
 	T base = z, dbase_dr = T(1), dbase_da = T(0);
 	if (a * z < T(40)) {
 		const T ez = t_exp<T>(a * z);
-		base = t_log<T>(T(1) + ez) / a;
-		const T sig = ez / (T(1) + ez);
+		base = t_log<T>(T(1) + ez) * ia;
+		const T sig = qdiv<T>(ez, T(1) + ez);
 		dbase_dr = sig;
-		dbase_da = z * sig / a - base / a;
+		dbase_da = (z * sig - base) * ia;
 	}
-	const T f = t_exp<T>(-r / h1 + expo * base);
+	const T f = t_exp<T>(-r * ih1 + expo * base);
 	t.f = f;
-	radial_chain<T>(t, f * (-T(1) / h1 + expo * dbase_dr), drdx, drdy, drdB, 4);
-	t.s[0] = f * (r - base) / (h1 * h1);
-	t.s[1] = f * base / (h2 * h2);
+	radial_chain<T>(t, f * (-ih1 + expo * dbase_dr), drdx, drdy, drdB, 4);
+	t.s[0] = f * (r - base) * ih1 * ih1;
+	t.s[1] = f * base * ih2 * ih2;
 	t.s[2] = -f * expo * dbase_dr;
 	t.s[3] = f * expo * dbase_da;
 	return t;
@@ -262,27 +318,34 @@ __device__ __forceinline__ Tan<T> coresersic_tan(const FProfile &p, T xp, T yp)
 	T r, drdx, drdy, drdB;
 	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
 	const T a = (T)p.a, b = (T)p.b, rb = (T)p.rb, re = (T)p.re, n = (T)p.nser, bn = (T)p.bn;
-	const T ra = t_pow<T>(r, a), rba = t_pow<T>(rb, a), rea = t_pow<T>(re, a);
-	const T rho = t_pow<T>(r / rb, -a);
+	const T ia = (T)p.k[0], in = (T)p.k[1];
+	const T lr = ln_pos<T>(r), lrb = (T)p.k[2], lre = (T)p.k[3];
+	const T ra = pow_ln<T>(r, lr, a), rba = (T)p.k[4], irea = (T)p.k[5];
+	// (r/rb)^-a, infinite at r = 0 for a > 0 as pow gives it
+	const T rho = r > T(0) ? t_exp<T>(-a * (lr - lrb)) : pow_ln<T>(T(0), T(0), -a);
 	const T A = T(1) + rho;
-	const T Q = (ra + rba) / rea;
-	const T W = t_pow<T>(Q, T(1) / (n * a));
-	const T f = t_pow<T>(A, b / a) * t_exp<T>(-bn * W);
+	const T Q = (ra + rba) * irea;
+	const T lnQ = t_log<T>(Q);
+	const T ina = (T)p.k[6];
+	const T W = t_exp<T>(lnQ * ina);
+	const T lnA = t_log<T>(A);
+	const T ba = b * ia;
+	const T f = t_exp<T>(ba == T(0) ? -bn * W : ba * lnA - bn * W);
 	t.f = f;
 	if (!(r > T(0)) || !(f > T(0))) return t;
-	const T lnA = t_log<T>(A), lnQ = t_log<T>(Q);
-	const T dA_dr = -a * rho / r, dA_drb = a * rho / rb, dA_da = -rho * t_log<T>(r / rb);
-	const T dQ_dr = a * ra / (r * rea), dQ_drb = a * rba / (rb * rea), dQ_dre = -a * Q / re;
-	const T dlnQ_da = (ra * t_log<T>(r) + rba * t_log<T>(rb)) / (ra + rba) - t_log<T>(re);
-	const T wq = W / (n * a * Q);  // dW/dQ
-	const T dW_dn = -W * lnQ / (n * n * a);
-	const T dW_da = W * (dlnQ_da / (n * a) - lnQ / (n * a * a));
-	radial_chain<T>(t, f * ((b / a) * dA_dr / A - bn * wq * dQ_dr), drdx, drdy, drdB, 5);
+	const T ir = qdiv<T>(T(1), r), irb = qdiv<T>(T(1), rb), iA = qdiv<T>(T(1), A), iQ = qdiv<T>(T(1), Q);
+	const T dA_dr = -a * rho * ir, dA_drb = a * rho * irb, dA_da = -rho * (lr - lrb);
+	const T dQ_dr = a * ra * ir * irea, dQ_drb = a * rba * irb * irea, dQ_dre = -a * Q / re;
+	const T dlnQ_da = qdiv<T>(ra * lr + rba * lrb, ra + rba) - lre;
+	const T wq = W * ina * iQ;  // dW/dQ
+	const T dW_dn = -W * lnQ * ina * in;
+	const T dW_da = W * ina * (dlnQ_da - lnQ * ia);
+	radial_chain<T>(t, f * (ba * dA_dr * iA - bn * wq * dQ_dr), drdx, drdy, drdB, 5);
 	t.s[0] = f * (-bn * wq * dQ_dre);
-	t.s[1] = f * ((b / a) * dA_drb / A - bn * wq * dQ_drb);
+	t.s[1] = f * (ba * dA_drb * iA - bn * wq * dQ_drb);
 	t.s[2] = f * (-(T)p.dbn_dn * W - bn * dW_dn);
-	t.s[3] = f * (-(b / (a * a)) * lnA + (b / a) * dA_da / A - bn * dW_da);
-	t.s[4] = f * lnA / a;
+	t.s[3] = f * (-(ba * ia) * lnA + ba * dA_da * iA - bn * dW_da);
+	t.s[4] = f * lnA * ia;
 	return t;
 }
 
@@ -471,6 +534,15 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 	img_plain[(size_t)b * npix + pix] = acc[1];
 }
 
+// k / res == (k * div_magic(res)) >> 16 for every sub-point index k < 256
+// and resolution 1 <= res <= 16: the magic ceil(2^16 / res) exceeds 2^16 / res
+// by less than 1, so the product overshoots k / res by less than 256 / 2^16,
+// short of the 1 / res gap to the next integer.
+__device__ __forceinline__ unsigned div_magic(unsigned res)
+{
+	return (65536u + res - 1) / res;
+}
+
 // Sub-points [base0, base1) of an item (multiples of 32), one per lane and
 // chunk.
 template <class T, bool AK, bool J>
@@ -484,14 +556,14 @@ __device__ __forceinline__ void level_points(const FProfile &p, const SubItem &i
 	const bool recurse = res > 1 && (unsigned)level < it.max_rec;
 	const T adyp = fabs((T)(-xbin * (double)p.sin_q + ybin * (double)p.cos_q));
 	const T cos_a = (T)p.cos_ang, sin_a = (T)p.sin_ang, cos_q = (T)p.cos_q, sin_q = (T)p.sin_q;
-	const unsigned nsub = res * res;
+	const unsigned nsub = res * res, mres = div_magic(res);
 	// sub-points in warp-wide chunks of 32 so each chunk's accept bits can be
 	// gathered with one ballot (mask_out: the item's 8 words, or null)
 	for (unsigned base = base0; base < base1 && base < nsub; base += 32) {
 		const unsigned k = base + lane;
 		bool accepted = false;
 		if (k < nsub) {
-			unsigned ii = k / res, jj = k - ii * res;
+			unsigned ii = (k * mres) >> 16, jj = k - ii * res;
 			const double x = s_xy[ii], y = s_xy[16 + jj];
 			const T dx = (T)x, dy = (T)y;
 			const T xp = dx * cos_a + dy * sin_a;
@@ -536,10 +608,10 @@ __device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem 
 {
 	const unsigned res = it.res;
 	const T cos_a = (T)p.cos_ang, sin_a = (T)p.sin_ang, cos_q = (T)p.cos_q, sin_q = (T)p.sin_q;
-	const unsigned nsub = res * res;
+	const unsigned nsub = res * res, mres = div_magic(res);
 	for (unsigned k = lane; k < nsub; k += 32) {
 		if (!((mask[k >> 5] >> (k & 31)) & 1u)) continue;
-		unsigned ii = k / res, jj = k - ii * res;
+		unsigned ii = (k * mres) >> 16, jj = k - ii * res;
 		const double x = s_xy[ii], y = s_xy[16 + jj];
 		const T dx = (T)x, dy = (T)y;
 		const T xp = dx * cos_a + dy * sin_a;
