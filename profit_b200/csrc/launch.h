@@ -74,11 +74,23 @@ constexpr int DEEP_ONE_CTA_MAX_CUSPS = 8;
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
                             float *jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s);
 // partials: n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN doubles;
-// tickets: n_profiles zero-initialised counters (left at zero again).
+// tickets: n_profiles zero-initialised counters (left at zero again), one
+// more when grad is given.  grad (optional): the arguments of
+// launch_batch_gradient; the reduction then also runs that step (in the block
+// that completes the last profile) and the separate launch is not needed.
+// Only valid when nothing else writes T after the reduction (no psf profile).
+struct GradStepArgs {
+	const DevProfile *dev;
+	int nprof, batch, nrefs;
+	const int *ref_profile, *ref_code;
+	const double *ll;
+	const int *invalid;
+	double *out_ll, *out_grad;
+};
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles);
 cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
                               const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
-                              unsigned *tickets, double *out, cudaStream_t s);
+                              unsigned *tickets, double *out, cudaStream_t s, const GradStepArgs *grad = nullptr);
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
                               unsigned dh, int batch, float *g_plain, cudaStream_t s);
 cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,
@@ -122,7 +134,8 @@ cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, c
                                   const int *invalid, double *out_ll, double *out_grad, cudaStream_t s);
 cudaError_t launch_loglike64_batch(const double *model, const double *data, const double *sigma,
                                    const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
-                                   int nparts, double *out, float *wseed, cudaStream_t s);
+                                   int nparts, double *out, float *wseed, cudaStream_t s,
+                                   unsigned *tickets = nullptr);
 }  // namespace pf
 
 namespace pf {
@@ -147,7 +160,11 @@ namespace pf {
 // for `batch` model images against data with the given batch stride (0:
 // one data image); writes logL per image and, with wseed, the adjoint seed.
 // partials: batch * nparts * 2 double2; stats: batch * LIKE_SCRATCH_PER_IMAGE doubles.
+// tickets (optional, batch zero-initialised words the kernel leaves at zero):
+// the norm likelihood then runs as one launch whose last block per image
+// merges the partials.
 cudaError_t launch_like64(int kind, const double *model, const double *data, const double *sigma,
                           const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
-                          int nparts, double *stats, double *out, float *wseed, cudaStream_t s);
+                          int nparts, double *stats, double *out, float *wseed, cudaStream_t s,
+                          unsigned *tickets = nullptr);
 }  // namespace pf

@@ -71,16 +71,15 @@ __device__ __forceinline__ Neumaier neumaier_block(Neumaier v)
 
 constexpr double LN_SQRT_2PI = 0.918938533204672741780329736406;
 
-// n pixels per image, `batch` images laid out back to back; one partial
-// (s, c) per block in partials[batch][gridDim.x].
+// The terms of image b handled by this block (grid-stride over its n
+// pixels), Neumaier-summed per thread and merged over the block (the total
+// is valid in thread 0); writes the adjoint seed when wseed is set.
 template <class T>
-__global__ void k_loglike_partial(const T *__restrict__ model, const double *__restrict__ data,
-                                  const double *__restrict__ sigma, const uint8_t *__restrict__ region, int n,
-                                  double2 *__restrict__ partials, float *__restrict__ wseed,
-                                  int data_batch_stride)
+__device__ __forceinline__ Neumaier loglike_block_terms(const T *__restrict__ model, const double *__restrict__ data,
+                                                        const double *__restrict__ sigma,
+                                                        const uint8_t *__restrict__ region, int n,
+                                                        float *__restrict__ wseed, int data_batch_stride, int b)
 {
-	pdl_enter();
-	const int b = blockIdx.y;
 	model += (size_t)b * n;
 	data += (size_t)b * data_batch_stride;
 	sigma += (size_t)b * data_batch_stride;
@@ -98,7 +97,36 @@ __global__ void k_loglike_partial(const T *__restrict__ model, const double *__r
 		}
 		if (wseed) wseed[k] = use ? (float)(diff / (s * s)) : 0.0f;
 	}
+	return neumaier_block(acc);
+}
+
+// logL of one image from its nparts partials: thread t merges partials t,
+// t + blockDim, ... in order, then the block merges in a fixed order, so
+// the value does not depend on which blocks produced the partials first.
+// The partials are read from L2 (they may have been written by other SMs in
+// this same kernel).
+__device__ __forceinline__ void loglike_merge_partials(const double2 *partials, int nparts, double *out)
+{
+	Neumaier acc{0.0, 0.0};
+	for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
+		double2 p = __ldcg(partials + k);
+		acc = neumaier_merge(acc, Neumaier{p.x, p.y});
+	}
 	acc = neumaier_block(acc);
+	if (threadIdx.x == 0) *out = acc.s + acc.c;
+}
+
+// n pixels per image, `batch` images laid out back to back; one partial
+// (s, c) per block in partials[batch][gridDim.x].
+template <class T>
+__global__ void k_loglike_partial(const T *__restrict__ model, const double *__restrict__ data,
+                                  const double *__restrict__ sigma, const uint8_t *__restrict__ region, int n,
+                                  double2 *__restrict__ partials, float *__restrict__ wseed,
+                                  int data_batch_stride)
+{
+	pdl_enter();
+	const int b = blockIdx.y;
+	const Neumaier acc = loglike_block_terms<T>(model, data, sigma, region, n, wseed, data_batch_stride, b);
 	if (threadIdx.x == 0) partials[(size_t)b * gridDim.x + blockIdx.x] = make_double2(acc.s, acc.c);
 }
 
@@ -106,13 +134,33 @@ static __global__ void k_loglike_final(const double2 *__restrict__ partials, int
 {
 	pdl_enter();
 	const int b = blockIdx.x;
-	Neumaier acc{0.0, 0.0};
-	for (int k = threadIdx.x; k < nparts; k += blockDim.x) {
-		double2 p = partials[(size_t)b * nparts + k];
-		acc = neumaier_merge(acc, Neumaier{p.x, p.y});
+	loglike_merge_partials(partials + (size_t)b * nparts, nparts, out + b);
+}
+
+// k_loglike_partial and k_loglike_final in one launch: the block that
+// finishes image b last (a ticket per image, counted with atomics after each
+// block's partial is visible) merges its partials exactly as the final
+// kernel does and resets the ticket.  tickets[batch] start at zero.
+template <class T>
+__global__ void k_loglike_fused(const T *__restrict__ model, const double *__restrict__ data,
+                                const double *__restrict__ sigma, const uint8_t *__restrict__ region, int n,
+                                double2 *__restrict__ partials, float *__restrict__ wseed, int data_batch_stride,
+                                unsigned *__restrict__ tickets, double *__restrict__ out)
+{
+	pdl_enter();
+	const int b = blockIdx.y;
+	const Neumaier acc = loglike_block_terms<T>(model, data, sigma, region, n, wseed, data_batch_stride, b);
+	__shared__ bool s_last;
+	if (threadIdx.x == 0) {
+		partials[(size_t)b * gridDim.x + blockIdx.x] = make_double2(acc.s, acc.c);
+		__threadfence();
+		s_last = atomicAdd(&tickets[b], 1u) == gridDim.x - 1;
 	}
-	acc = neumaier_block(acc);
-	if (threadIdx.x == 0) out[b] = acc.s + acc.c;
+	__syncthreads();  // also orders this block's reuse of neumaier_block's shared arrays
+	if (!s_last) return;
+	__threadfence();
+	loglike_merge_partials(partials + (size_t)b * gridDim.x, gridDim.x, out + b);
+	if (threadIdx.x == 0) tickets[b] = 0;
 }
 
 }  // namespace pf

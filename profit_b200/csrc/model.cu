@@ -335,6 +335,7 @@ struct pf_model {
 	DevBuf d_psf64, d_psfrev64, d_psf32, d_psfrev32;
 	DevBuf d_convsplit;  // FP64 partial images of column-split convolutions
 	DevBuf d_jac_partials, d_jac_tickets;  // per-block sums and tickets of the tangent reduction
+	DevBuf d_like_tickets;  // per-image tickets of the one-launch norm likelihood
 	DevBuf d_items, d_masks, d_ctrl, d_partials, d_results;
 	int adjoint_mode = PF_ADJOINT_AUTO;
 	DevBuf d_decisions, d_level_counts;
@@ -852,7 +853,12 @@ int adjoint_seed32(pf_model *m, const Analysis &a, const float *wseed, float *&g
 	const Finish32 fin = finish32_of(m, a);
 	const bool conv_on = a.conv && m->conv_kind != CONV_NULL;
 	if (!fin.any) {
-		PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, batch, gplain, m->stream));
+		// the seed of the unconvolved image is read by profiles drawn without
+		// convolution only (and by every profile when nothing is convolved)
+		bool plain = !conv_on;
+		for (const auto &p : m->profiles) plain = plain || !p.convolve;
+		if (plain)
+			PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, batch, gplain, m->stream));
 		if (conv_on) PF_TRY(adjoint_conv32(m, a, wseed, gconv, batch));
 		else gconv = gplain;
 		return PF_OK;
@@ -997,14 +1003,28 @@ int evaluate64(pf_model *m, Analysis &a)
 
 // The model's likelihood (pf_model_set_likelihood) of `batch` images against
 // its data, with the adjoint seed when wseed is given.
+// Ticket words of the one-launch norm likelihood, one per image: zeroed when
+// the buffer is (re)allocated, left at zero by every launch.
+int like_tickets(pf_model *m, int batch, unsigned **tickets)
+{
+	void *before = m->d_like_tickets.p;
+	PF_CUDA(ensure(m->d_like_tickets, (size_t)batch * sizeof(unsigned)));
+	if (m->d_like_tickets.p != before)
+		PF_CUDA(cudaMemsetAsync(m->d_like_tickets.p, 0, m->d_like_tickets.bytes, m->stream));
+	*tickets = m->d_like_tickets.as<unsigned>();
+	return PF_OK;
+}
+
 int enqueue_like(pf_model *m, const double *model64, int nout, int batch, double *out, float *wseed, cudaStream_t s)
 {
 	PF_CUDA(ensure(m->d_partials, (size_t)NPARTS * batch * 2 * sizeof(double2)));
 	PF_CUDA(ensure(m->d_likestats, (size_t)batch * LIKE_SCRATCH_PER_IMAGE * 8));
+	unsigned *tickets = nullptr;
+	if (m->like_kind == LIKE_NORM) PF_TRY(like_tickets(m, batch, &tickets));
 	PF_CUDA(launch_like64(m->like_kind, model64, m->d_data.as<double>(), m->d_sigma.as<double>(),
 	                      m->has_region ? m->d_region.as<uint8_t>() : nullptr, nout, batch, 0,
 	                      m->d_partials.as<double2>(), like_parts(nout, batch), m->d_likestats.as<double>(), out,
-	                      wseed, s));
+	                      wseed, s, tickets));
 	return PF_OK;
 }
 
@@ -1045,13 +1065,14 @@ bool all_kinds(const pf_model *m)
 }
 
 // Scratch of launch_jac_reduce for n_profiles profiles over npix pixels; the
-// tickets start at zero when allocated and the kernel leaves them at zero.
+// tickets (one per profile and one for the folded gradient step) start at
+// zero when allocated and the kernel leaves them at zero.
 int jac_scratch(pf_model *m, unsigned npix, int n_profiles, double **partials, unsigned **tickets)
 {
 	const size_t pb = (size_t)n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN * sizeof(double);
 	PF_CUDA(ensure(m->d_jac_partials, pb));
 	void *before = m->d_jac_tickets.p;
-	PF_CUDA(ensure(m->d_jac_tickets, (size_t)n_profiles * sizeof(unsigned)));
+	PF_CUDA(ensure(m->d_jac_tickets, (size_t)(n_profiles + 1) * sizeof(unsigned)));
 	if (m->d_jac_tickets.p != before) PF_CUDA(cudaMemsetAsync(m->d_jac_tickets.p, 0, m->d_jac_tickets.bytes, m->stream));
 	*partials = m->d_jac_partials.as<double>();
 	*tickets = m->d_jac_tickets.as<unsigned>();
@@ -1151,7 +1172,7 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 	const DevBuf *bufs[] = {&m->d_fprof, &m->d_prof_begin, &m->d_prof_batch, &m->d_conv32, &m->d_plain32,
 	                        &m->d_model64, &m->d_conv64, &m->d_plain64, &m->d_jac, &m->d_gconv, &m->d_gplain,
 	                        &m->d_wseed, &m->d_items, &m->d_ctrl, &m->d_partials, &m->d_results, &m->d_psf32,
-	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region, &m->d_convsplit, &m->d_jac_partials, &m->d_jac_tickets, &m->d_likestats};
+	                        &m->d_psfrev32, &m->d_psfrev64, &m->d_data, &m->d_sigma, &m->d_region, &m->d_convsplit, &m->d_jac_partials, &m->d_jac_tickets, &m->d_likestats, &m->d_like_tickets};
 	for (auto *b : bufs) s.push_back((uint64_t)(uintptr_t)b->p);
 	// calculation mask and finesampling steps (finish32_of) and their buffers
 	for (const DevBuf *b : {&m->d_mask_draw, &m->d_mask_out, &m->d_model_fine, &m->d_seed_fine, &m->d_perm})
@@ -1162,7 +1183,9 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 	s.push_back(((uint64_t)a.padx << 32) | a.pady);
 	s.push_back((uint64_t)m->profiles.size());
 	for (const DevBuf *b : {&m->d_prof, &m->d_psf64}) s.push_back((uint64_t)(uintptr_t)b->p);
-	for (auto &p : m->profiles) s.push_back((uint64_t)p.kind);  // which kernels run (AK variants, psf stamps)
+	// which kernels run: AK variants and psf stamps by kind, the seed of the
+	// unconvolved image when a profile is drawn without convolution
+	for (auto &p : m->profiles) s.push_back((uint64_t)p.kind | ((uint64_t)(p.convolve ? 1 : 0) << 32));
 	s.push_back((uint64_t)(uintptr_t)m->h_results.p);
 	return s;
 }
@@ -1345,7 +1368,9 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 
 	PF_CUDA(record_event(m->ev[0], s));
 	PF_CUDA(cudaMemsetAsync(q.counts, 0, CTRL_WORDS * 4, s));
-	PF_CUDA(cudaMemsetAsync(bs.d_T.p, 0, (size_t)C * nprof * NTAN * 8, s));
+	// the recomputing adjoint accumulates the tangent sums with atomics; the
+	// stored-plane reduction writes every slot the gradient reads
+	if (recompute) PF_CUDA(cudaMemsetAsync(bs.d_T.p, 0, (size_t)C * nprof * NTAN * 8, s));
 	if (host_prologue) {
 		PF_CUDA(cudaMemcpyAsync(bs.d_stage.p, bs.h_stage.p, L.total, cudaMemcpyHostToDevice, s));
 	}
@@ -1376,19 +1401,25 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh, m->sx / m->fs,
 		                                 m->sy / m->fs, gconv, gplain, a.levels, ak, q, bs.d_T.as<double>(), s,
 		                                 fin.draw));
-	else {
+	// small batches without psf profiles (nothing writes T after the
+	// reduction): the gradient step runs inside the reduction's last block
+	const bool fold_grad = !recompute && !has_psf_profile(m) && (long long)C * std::max(nrefs, 1) <= 1024;
+	const GradStepArgs gargs = {dev, nprof, C, nrefs, ref_profile, ref_code, bs.d_ll.as<double>(), invalid, out_ll,
+	                            out_grad};
+	if (!recompute) {
 		double *jpart;
 		unsigned *jtick;
 		PF_TRY(jac_scratch(m, (unsigned)npix, C * nprof, &jpart, &jtick));
 		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix, nt,
-		                          jpart, jtick, bs.d_T.as<double>(), s));
+		                          jpart, jtick, bs.d_T.as<double>(), s, fold_grad ? &gargs : nullptr));
 	}
 	if (has_psf_profile(m))
 		PF_CUDA(launch_psf_adjoint32(dev, m->d_prof_begin.as<int>(), C, nprof, m->d_psf64.as<double>(), m->psf_w,
 		                             m->psf_h, m->psf_sx, m->psf_sy, m->sx / m->fs, m->sy / m->fs, a.padx, a.pady,
 		                             a.dw, a.dh, gconv, gplain, bs.d_T.as<double>(), s));
-	PF_CUDA(launch_batch_gradient(dev, nprof, C, ref_profile, ref_code, nrefs, bs.d_T.as<double>(),
-	                              bs.d_ll.as<double>(), invalid, out_ll, out_grad, s));
+	if (!fold_grad)
+		PF_CUDA(launch_batch_gradient(dev, nprof, C, ref_profile, ref_code, nrefs, bs.d_T.as<double>(),
+		                              bs.d_ll.as<double>(), invalid, out_ll, out_grad, s));
 	PF_CUDA(record_event(m->ev[3], s));
 	char *ho = bs.h_out.as<char>();
 	PF_CUDA(cudaMemcpyAsync(ho, bs.d_out.p, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
@@ -2298,6 +2329,7 @@ struct CatChunk {
 	std::vector<int> member_grad_off;   // offset of each member's gradient in the chunk's buffer
 	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3, cusps = 0;
 	bool ak = false;
+	bool plain = false;  // a profile drawn without convolution (reads the seed of the plain image)
 	DevBuf data, sigma, region, psf32, psfrev32, prof_begin, prof_batch, grad_off, T, ll, grad;
 	HostBuf h_ll, h_grad, h_ctrl;
 	size_t npix() const { return (size_t)(W + 2 * (pw / 2)) * (H + 2 * (ph / 2)); }
@@ -2439,6 +2471,7 @@ int cat_build(pf_catalogue *c)
 				ch.levels = std::max(ch.levels, (int)mr + 1);
 				ch.nt = std::max(ch.nt, tangent_count(p.kind));
 				if (p.kind != PK_SERSIC && p.kind != PK_MOFFAT) ch.ak = true;
+				if (!p.convolve) ch.plain = true;
 			}
 			prof_begin[i + 1] = (int)params.size() - ch.p0;
 			for (unsigned y = 0; y < G.h; y++)
@@ -2487,10 +2520,11 @@ int cat_build(pf_catalogue *c)
 	// reallocated while chunks are queued
 	pf_model *m = c->engine;
 	size_t conv = 0, model = 0, seed = 0, jac = 0, parts = 0, qpix = 0, jp = 0;
-	int levels = 1, maxprof = 0;
+	int levels = 1, maxprof = 0, maxc = 1;
 	for (auto &chp : c->chunks) {
 		const CatChunk &ch = *chp;
 		const size_t C = ch.members.size();
+		maxc = std::max(maxc, (int)C);
 		conv = std::max(conv, ch.npix() * 4 * C);
 		model = std::max(model, ch.nout() * 8 * C);
 		seed = std::max(seed, ch.nout() * 4 * C);
@@ -2515,6 +2549,8 @@ int cat_build(pf_catalogue *c)
 	PF_CUDA(ensure(m->d_jac_tickets, (size_t)maxprof * sizeof(unsigned)));
 	if (m->d_jac_tickets.p != before)
 		PF_CUDA(cudaMemsetAsync(m->d_jac_tickets.p, 0, m->d_jac_tickets.bytes, m->stream));
+	unsigned *like_tk;
+	PF_TRY(like_tickets(m, maxc, &like_tk));
 	Analysis a;
 	a.levels = levels;
 	QueueSet q;
@@ -2540,7 +2576,6 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
 	double *model64 = m->d_model64.as<double>();
 	const FProfile *fprof = c->fprof.as<FProfile>() + ch.p0;
 	const DevProfile *dev = c->dev.as<DevProfile>() + ch.p0;
-	PF_CUDA(cudaMemsetAsync(ch.T.p, 0, (size_t)ch.nprof * NTAN * 8, s));
 	PF_CUDA(launch_pixels32(fprof, ch.prof_begin.as<int>(), C, a.dw, a.dh, 1.0, 1.0, conv, plain, jac, ch.nt, ch.ak, q,
 	                        s));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, ch.cusps, q, s));
@@ -2551,8 +2586,8 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
 	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
 	PF_CUDA(launch_loglike64_batch(model64, ch.data.as<double>(), ch.sigma.as<double>(), ch.region.as<uint8_t>(),
 	                               (int)nout, C, (int)nout, m->d_partials.as<double2>(), like_parts((int)nout, C),
-	                               ch.ll.as<double>(), wseed, s));
-	PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
+	                               ch.ll.as<double>(), wseed, s, m->d_like_tickets.as<unsigned>()));
+	if (ch.plain) PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
 	sb = conv32_scratch_bytes(a.dw, a.dh, C);
 	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)ch.pw, 1 - (int)ch.ph, ch.psf32.as<float>(), ch.pw, ch.ph, gconv,
 	                      a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix,

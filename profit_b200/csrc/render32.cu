@@ -861,6 +861,46 @@ cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_b
 	return e;
 }
 
+// The batch gradient step: logL and d logL / d parameter of every
+// (proposal, parameter) from the tangent reductions T.  k_batch_gradient runs
+// it as its own launch; k_jac_reduce can run it in the block that completes
+// the last profile (ticket: one zero-initialised word over all profiles,
+// left at zero), which saves the launch when the batch is small.
+
+// Entry t of the gradient step (t < batch also writes logL of proposal t).
+// T is read from L2: in the fused form other SMs wrote it in the same launch.
+__device__ __forceinline__ void batch_gradient_at(const GradStepArgs &g, const double *T, int t)
+{
+	if (t < g.batch) g.out_ll[t] = g.invalid[t] ? -INFINITY : g.ll[t];
+	if (t >= g.batch * g.nrefs) return;
+	const int b = t / g.nrefs, r = t - b * g.nrefs;
+	const int pi = b * g.nprof + g.ref_profile[r];
+	if (g.invalid[b]) {
+		g.out_grad[t] = 0.0;
+		return;
+	}
+	double Tp[NTAN];
+#pragma unroll
+	for (int k = 0; k < NTAN; k++) Tp[k] = __ldcg(T + (size_t)pi * NTAN + k);
+	g.out_grad[t] = gradient_from_tangents(g.ref_code[r], g.dev[pi].axrat, g.dev[pi], Tp);
+}
+
+// Called by one block per profile once that profile's T is written (or its
+// blocks have nothing to reduce); the last of the gridDim.y calls runs the
+// gradient step with all its threads.  Writers of T fence before the call.
+__device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigned *ticket, const double *T)
+{
+	__shared__ bool s_all;
+	__syncthreads();
+	if (threadIdx.x == 0) s_all = atomicAdd(ticket, 1u) == gridDim.y - 1;
+	__syncthreads();
+	if (!s_all) return;
+	__threadfence();
+	const int n = g.batch * max(g.nrefs, 1);
+	for (int t = threadIdx.x; t < n; t += blockDim.x) batch_gradient_at(g, T, t);
+	if (threadIdx.x == 0) *ticket = 0;
+}
+
 // sum over pixels of g(pixel) * J_k(pixel) for each radial profile:
 // blockIdx.y = profile, blockIdx.x strides over the pixels, four pixels per
 // thread and step with every load issued before the products (enough bytes
@@ -874,13 +914,17 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
                                                     const FProfile *__restrict__ profiles,
                                                     const int *__restrict__ prof_batch, unsigned npix, int nt,
                                                     double *__restrict__ partials, unsigned *__restrict__ tickets,
-                                                    double *__restrict__ out)
+                                                    double *__restrict__ out, GradStepArgs grad,
+                                                    unsigned *__restrict__ grad_ticket)
 {
 	pdl_enter();
 	constexpr int U = 4;
 	const int pi = blockIdx.y;
 	const FProfile &p = profiles[pi];
-	if (!is_radial_kind(p.kind)) return;
+	if (!is_radial_kind(p.kind)) {
+		if (grad_ticket && blockIdx.x == 0) jac_gradient_tail(grad, grad_ticket, out);
+		return;
+	}
 	const int nk = tangent_count(p.kind);  // <= nt <= NT
 	const int b = prof_batch[pi];
 	const float *g = (p.target == 0 ? g_conv : g_plain) + (size_t)b * npix;
@@ -948,8 +992,10 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
 		double t = 0;
 		for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += s_red[threadIdx.x][w];
 		out[(size_t)pi * NTAN + threadIdx.x] = t;
+		if (grad_ticket) __threadfence();
 	}
 	if (threadIdx.x == 0) tickets[pi] = 0;
+	if (grad_ticket) jac_gradient_tail(grad, grad_ticket, out);
 }
 
 // Scatter the residual weights w (cropped grid) into the padded grid of the
@@ -1105,13 +1151,14 @@ unsigned jac_reduce_blocks(unsigned npix, int n_profiles)
 
 cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
                               const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
-                              unsigned *tickets, double *out, cudaStream_t s)
+                              unsigned *tickets, double *out, cudaStream_t s, const GradStepArgs *grad)
 {
 	const unsigned bx = jac_reduce_blocks(npix, n_profiles);
 	auto k = nt <= 9 ? k_jac_reduce<9> : k_jac_reduce<NTAN>;
+	const GradStepArgs g = grad ? *grad : GradStepArgs{};
 	note_launches(1);
 	return launch_pdl(k, dim3(bx, n_profiles), dim3(256), 0, s, jac, g_conv, g_plain, profiles, prof_batch, npix, nt,
-	                  partials, tickets, out);
+	                  partials, tickets, out, g, grad ? tickets + n_profiles : (unsigned *)nullptr);
 }
 
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
@@ -1489,12 +1536,8 @@ __global__ void k_batch_gradient(const DevProfile *__restrict__ dev, int nprof, 
                                  double *__restrict__ out_ll, double *__restrict__ out_grad)
 {
 	pdl_enter();
-	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t < batch) out_ll[t] = invalid[t] ? -INFINITY : ll[t];
-	if (t >= batch * nrefs) return;
-	const int b = t / nrefs, r = t - b * nrefs;
-	const int pi = b * nprof + ref_profile[r];
-	out_grad[t] = invalid[b] ? 0.0 : gradient_from_tangents(ref_code[r], dev[pi].axrat, dev[pi], T + (size_t)pi * NTAN);
+	const GradStepArgs g = {dev, nprof, batch, nrefs, ref_profile, ref_code, ll, invalid, out_ll, out_grad};
+	batch_gradient_at(g, T, (int)(blockIdx.x * blockDim.x + threadIdx.x));
 }
 
 cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batch, const int *ref_profile,
@@ -1570,8 +1613,13 @@ cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, c
 
 cudaError_t launch_loglike64_batch(const double *model, const double *data, const double *sigma,
                                    const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
-                                   int nparts, double *out, float *wseed, cudaStream_t s)
+                                   int nparts, double *out, float *wseed, cudaStream_t s, unsigned *tickets)
 {
+	if (tickets) {
+		note_launches(1);
+		return launch_pdl(k_loglike_fused<double>, dim3(nparts, batch), dim3(256), 0, s, model, data, sigma, region, n,
+		                  partials, wseed, data_batch_stride, tickets, out);
+	}
 	cudaError_t e = launch_pdl(k_loglike_partial<double>, dim3(nparts, batch), dim3(256), 0, s, model, data, sigma,
 	                           region, n, partials, wseed, data_batch_stride);
 	if (e == cudaSuccess) e = launch_pdl(k_loglike_final, dim3(batch), dim3(256), 0, s, partials, nparts, out);

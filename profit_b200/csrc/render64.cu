@@ -419,7 +419,7 @@ cudaError_t launch_widen(const float *src, double *dst, size_t n, cudaStream_t s
 
 cudaError_t launch_like64(int kind, const double *model, const double *data, const double *sigma,
                           const uint8_t *region, int n, int batch, int data_batch_stride, double2 *partials,
-                          int nparts, double *stats, double *out, float *wseed, cudaStream_t s)
+                          int nparts, double *stats, double *out, float *wseed, cudaStream_t s, unsigned *tickets)
 {
 	// launched with programmatic serialisation: these kernels run inside the
 	// FP32 pipeline's graph right after the convolution
@@ -428,6 +428,12 @@ cudaError_t launch_like64(int kind, const double *model, const double *data, con
 	auto go = [&](cudaError_t r) {
 		if (e == cudaSuccess) e = r;
 	};
+	if (kind == LIKE_NORM && tickets) {
+		go(launch_pdl(k_loglike_fused<double>, grid, b256, 0, s, model, data, sigma, region, n, partials, wseed,
+		              data_batch_stride, tickets, out));
+		note_launches(1);
+		return e;
+	}
 	if (kind == LIKE_NORM) {
 		go(launch_pdl(k_loglike_partial<double>, grid, b256, 0, s, model, data, sigma, region, n, partials, wseed,
 		              data_batch_stride));
