@@ -330,6 +330,31 @@ def test_batch_matches_single_proposals():
         np.testing.assert_allclose(g_b[s], g, rtol=1e-5, atol=1e-6 * np.max(np.abs(g)))
 
 
+def test_large_batch_matches_single_proposals():
+    """Batches above 1024 (proposal, parameter) pairs assemble the gradient in
+    their own launch, small ones inside the tangent reduction; both give what
+    one-proposal calls give."""
+    wl = W.single_sersic(width=96, height=90, psf_size=15)
+    wl["magzero"] = 25.0
+    m = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = m.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    refs = wl["grad"]
+    n = 1024 // len(refs) + 20
+    props = [W.perturbed(wl, seed=300 + s, scale=0.05) for s in range(n)]
+    vals = np.array([[p["profiles"][i][1][k] for (i, k) in refs] for p in props])
+    mb = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), wl)
+    mb.set_data(image, sigma)
+    ll_b, g_b = mb.loglike_grad_batch(refs, vals)
+    assert np.all(np.isfinite(ll_b))
+    for s in (0, n // 2, n - 1):
+        one = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), props[s])
+        one.set_data(image, sigma)
+        ll, g = one.loglike_grad(refs)
+        assert ll_b[s] == pytest.approx(ll, rel=1e-7)
+        np.testing.assert_allclose(g_b[s], g, rtol=1e-5, atol=1e-6 * np.max(np.abs(g)))
+
+
 def test_adjoint_gradient_matches_fd64():
     wl = W.bulge_disk_ps()
     m, w2 = _gradient_case(wl, 0.02)
