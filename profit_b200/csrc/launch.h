@@ -86,11 +86,21 @@ struct GradStepArgs {
 	const double *ll;
 	const int *invalid;
 	double *out_ll, *out_grad;
+	// optional (folded form): after the step, ctrl_in[0 .. ctrl_words) is
+	// copied to ctrl_out (e.g. the queue counters into a mapped host buffer)
+	const uint32_t *ctrl_in = nullptr;
+	uint32_t *ctrl_out = nullptr;
+	int ctrl_words = 0;
 };
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles);
 cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
                               const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
                               unsigned *tickets, double *out, cudaStream_t s, const GradStepArgs *grad = nullptr);
+// Copies `bytes` (a multiple of 16, both addresses 16-byte aligned) from
+// pinned host memory mapped into the device's address space to dst, and
+// zeroes ctrl[0 .. ctrl_words); one launch in place of a copy and a memset.
+cudaError_t launch_stage_in(void *dst, const void *host_src, size_t bytes, uint32_t *ctrl, int ctrl_words,
+                            cudaStream_t s);
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
                               unsigned dh, int batch, float *g_plain, cudaStream_t s);
 cudaError_t launch_conv32_to64(const float *src, int sw, int sh, int ox, int oy, const float *K, int kw, int kh,

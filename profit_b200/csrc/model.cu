@@ -1311,6 +1311,9 @@ int check_profile(pf_model *m, int index);
 // invalid flags x C] uploaded with one copy; results [logL x C | gradient x
 // C*nrefs | queue counters] downloaded with one copy.
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+// Largest staged upload read by launch_stage_in instead of a copy.
+constexpr size_t STAGE_IN_MAX_BYTES = 64 << 10;
+
 struct StageLayout {
 	size_t f = 0, inv = 0, total = 0;
 	StageLayout(int C, int nprof)
@@ -1324,6 +1327,8 @@ struct StageLayout {
 struct BatchState {
 	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out, d_ll, d_T, d_stage;
 	HostBuf h_tmpl, h_values, h_out, h_stage;
+	void *h_stage_dev = nullptr;  // h_stage as the device addresses it (mapped pinned memory), or null
+	void *h_out_dev = nullptr;    // likewise h_out
 	int refs_n = -1, chunk = 0;
 	std::vector<int> refs_host;
 	// (profile, kind, rescale_flux, name) of the references refs_host was resolved for
@@ -1367,14 +1372,21 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	double *out_ll = bs.d_out.as<double>(), *out_grad = out_ll + C;
 
 	PF_CUDA(record_event(m->ev[0], s));
-	PF_CUDA(cudaMemsetAsync(q.counts, 0, CTRL_WORDS * 4, s));
+	// a small stage is read by a kernel straight from the pinned buffer, which
+	// also zeroes the queue counters (one programmatic launch instead of a
+	// memset and a copy); a large one goes by copy
+	void *hmap = host_prologue && L.total <= STAGE_IN_MAX_BYTES ? bs.h_stage_dev : nullptr;
+	if (hmap) {
+		PF_CUDA(launch_stage_in(bs.d_stage.p, hmap, L.total, q.counts, CTRL_WORDS, s));
+	}
+	else {
+		PF_CUDA(cudaMemsetAsync(q.counts, 0, CTRL_WORDS * 4, s));
+		if (host_prologue) PF_CUDA(cudaMemcpyAsync(bs.d_stage.p, bs.h_stage.p, L.total, cudaMemcpyHostToDevice, s));
+	}
 	// the recomputing adjoint accumulates the tangent sums with atomics; the
 	// stored-plane reduction writes every slot the gradient reads
 	if (recompute) PF_CUDA(cudaMemsetAsync(bs.d_T.p, 0, (size_t)C * nprof * NTAN * 8, s));
-	if (host_prologue) {
-		PF_CUDA(cudaMemcpyAsync(bs.d_stage.p, bs.h_stage.p, L.total, cudaMemcpyHostToDevice, s));
-	}
-	else {
+	if (!host_prologue) {
 		PF_CUDA(cudaMemcpyAsync(bs.d_tmpl.p, bs.h_tmpl.p, nprof * sizeof(ProfileParams), cudaMemcpyHostToDevice, s));
 		PF_CUDA(cudaMemcpyAsync(bs.d_values.p, bs.h_values.p, (size_t)C * nrefs * 8, cudaMemcpyHostToDevice, s));
 		PF_CUDA(cudaMemsetAsync(bs.d_invalid.p, 0, (size_t)C * 4, s));
@@ -1404,8 +1416,18 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	// small batches without psf profiles (nothing writes T after the
 	// reduction): the gradient step runs inside the reduction's last block
 	const bool fold_grad = !recompute && !has_psf_profile(m) && (long long)C * std::max(nrefs, 1) <= 1024;
-	const GradStepArgs gargs = {dev, nprof, C, nrefs, ref_profile, ref_code, bs.d_ll.as<double>(), invalid, out_ll,
-	                            out_grad};
+	GradStepArgs gargs = {dev, nprof, C, nrefs, ref_profile, ref_code, bs.d_ll.as<double>(), invalid, out_ll, out_grad};
+	// folded, the step writes logL, the gradient and the queue counters
+	// straight into the pinned result buffer (no download afterwards)
+	const bool direct_out = fold_grad && bs.h_out_dev;
+	if (direct_out) {
+		char *hd = static_cast<char *>(bs.h_out_dev);
+		gargs.out_ll = reinterpret_cast<double *>(hd);
+		gargs.out_grad = gargs.out_ll + C;
+		gargs.ctrl_in = q.counts;
+		gargs.ctrl_out = reinterpret_cast<uint32_t *>(hd + (size_t)C * (1 + nrefs) * 8);
+		gargs.ctrl_words = CTRL_WORDS;
+	}
 	if (!recompute) {
 		double *jpart;
 		unsigned *jtick;
@@ -1422,7 +1444,9 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		                              bs.d_ll.as<double>(), invalid, out_ll, out_grad, s));
 	PF_CUDA(record_event(m->ev[3], s));
 	char *ho = bs.h_out.as<char>();
-	PF_CUDA(cudaMemcpyAsync(ho, bs.d_out.p, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4, cudaMemcpyDeviceToHost, s));
+	if (!direct_out)
+		PF_CUDA(cudaMemcpyAsync(ho, bs.d_out.p, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4, cudaMemcpyDeviceToHost,
+		                        s));
 	return PF_OK;
 }
 
@@ -1519,7 +1543,14 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	PF_CUDA(ensure(bs.d_ll, (size_t)C * 8));
 	PF_CUDA(ensure(bs.d_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
 	PF_CUDA(ensure(bs.d_T, (size_t)C * nprof * NTAN * 8));
+	void *out_before = bs.h_out.p;
 	PF_CUDA(ensure(bs.h_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
+	if (bs.h_out.p != out_before || !bs.h_out_dev) {
+		if (cudaHostGetDevicePointer(&bs.h_out_dev, bs.h_out.p, 0) != cudaSuccess) {
+			cudaGetLastError();
+			bs.h_out_dev = nullptr;
+		}
+	}
 	PF_CUDA(ensure(m->d_conv32, npix * C * 4));
 	PF_CUDA(ensure(m->d_plain32, npix * C * 4));
 	if (!recompute) PF_CUDA(ensure(m->d_jac, npix * tangent_stride(m) * nprof * C * 4));
@@ -1547,7 +1578,14 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	const bool host_prologue = C * nprof <= HOST_PROLOGUE_MAX;
 	if (host_prologue) {
 		const StageLayout L(C, nprof);
+		void *stage_before = bs.h_stage.p;
 		PF_CUDA(ensure(bs.h_stage, L.total));
+		if (bs.h_stage.p != stage_before || !bs.h_stage_dev) {
+			if (cudaHostGetDevicePointer(&bs.h_stage_dev, bs.h_stage.p, 0) != cudaSuccess) {
+				cudaGetLastError();
+				bs.h_stage_dev = nullptr;
+			}
+		}
 		PF_CUDA(ensure(bs.d_stage, L.total));
 	}
 	const ModelGeom geom = geometry(m, a);

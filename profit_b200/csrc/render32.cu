@@ -669,7 +669,7 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 
 // Deep: FP64 sub-points (levels >= 3, the Sersic cusp).
 template <bool AK, bool J, bool Deep>
-__global__ void __launch_bounds__(256, (AK && !Deep) ? 3 : 2) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
+__global__ void __launch_bounds__(256, Deep ? 2 : (AK ? 3 : 4)) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
                                                  float *__restrict__ img_conv, float *__restrict__ img_plain,
                                                  float *__restrict__ jac, int nt, QueueSet q)
 {
@@ -898,6 +898,8 @@ __device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigne
 	__threadfence();
 	const int n = g.batch * max(g.nrefs, 1);
 	for (int t = threadIdx.x; t < n; t += blockDim.x) batch_gradient_at(g, T, t);
+	if (g.ctrl_out)
+		for (int i = threadIdx.x; i < g.ctrl_words; i += blockDim.x) g.ctrl_out[i] = __ldcg(g.ctrl_in + i);
 	if (threadIdx.x == 0) *ticket = 0;
 }
 
@@ -1028,6 +1030,30 @@ __global__ void k_crop32(const float *__restrict__ src, unsigned sw, unsigned ox
 }
 
 static inline unsigned cdiv(unsigned a, unsigned b) { return (a + b - 1) / b; }
+
+// The start of one small FP32 evaluation in one launch: the staged profile
+// scalars are read straight from pinned host memory (mapped into the device's
+// address space) into their device buffer, and the queue's control words are
+// zeroed.  This replaces a host-to-device copy and a memset, which cannot
+// overlap the kernels around them the way a programmatic launch does.
+__global__ void k_stage_in(uint4 *__restrict__ dst, const uint4 *__restrict__ src, size_t n16,
+                           uint32_t *__restrict__ ctrl, int ctrl_words)
+{
+	pdl_enter();
+	const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x, step = (size_t)gridDim.x * blockDim.x;
+	for (size_t i = t; i < n16; i += step) dst[i] = src[i];
+	for (size_t i = t; i < (size_t)ctrl_words; i += step) ctrl[i] = 0u;
+}
+
+cudaError_t launch_stage_in(void *dst, const void *host_src, size_t bytes, uint32_t *ctrl, int ctrl_words,
+                            cudaStream_t s)
+{
+	const size_t n16 = bytes / 16;
+	const unsigned blocks = (unsigned)std::min<size_t>(std::max<size_t>((n16 + 255) / 256, 1), 148);
+	note_launches(1);
+	return launch_pdl(k_stage_in, dim3(blocks), dim3(256), 0, s, static_cast<uint4 *>(dst),
+	                  static_cast<const uint4 *>(host_src), n16, ctrl, ctrl_words);
+}
 
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
@@ -1536,7 +1562,8 @@ __global__ void k_batch_gradient(const DevProfile *__restrict__ dev, int nprof, 
                                  double *__restrict__ out_ll, double *__restrict__ out_grad)
 {
 	pdl_enter();
-	const GradStepArgs g = {dev, nprof, batch, nrefs, ref_profile, ref_code, ll, invalid, out_ll, out_grad};
+	const GradStepArgs g = {dev, nprof, batch, nrefs, ref_profile, ref_code, ll, invalid, out_ll, out_grad,
+	                        nullptr, nullptr, 0};
 	batch_gradient_at(g, T, (int)(blockIdx.x * blockDim.x + threadIdx.x));
 }
 
