@@ -333,6 +333,7 @@ def main_b200(args):
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one forward launch "
                               "(profiles/conv_fwd_bulge_disk_ps.txt)"}
 
+    render = render_rate(wl, image, sigma, refs, pvals)
     conv_choice = convolver_choice_rate(torch, flush, wl, image, sigma, refs, pvals)
     sampler = sampler_batch_rate(args, torch, flush, n=args.sampler_n)
     catalogue = catalogue_rate(args, torch, flush, n=args.catalogue_n) if args.catalogue_n > 0 else None
@@ -357,6 +358,7 @@ def main_b200(args):
             "accuracy": accuracy,
             "plain_fp64_fd": {"value": fp64_fd_value, "unit": UNIT,
                               "speedup_fp32_adjoint": (world * args.steps / dev_total) / fp64_fd_value},
+            "render": render,
             "convolver_choice": conv_choice,
             "sampler_batch": sampler,
             "catalogue_batch": catalogue,
@@ -369,6 +371,44 @@ def main_b200(args):
         if not args.no_cpu_baseline and world == 1:
             out["cpu_baseline"] = cpu_baseline(wl, image, sigma)
         print(json.dumps(out), flush=True)
+
+
+def render_rate(wl, image, sigma, refs, pvals, steps=20):
+    """Render work of the headline evaluation, outside the timed region:
+    libprofit's evaluate_at calls for the first proposal (direct pixels plus
+    subsampling points, counted by the plain FP64 form's debug counters, whose
+    decisions are the reference's pixel for pixel), over the render phase of
+    the FP32 LL+grad pipeline (CUDA events around the pixel and level kernels,
+    median over proposals; each evaluation there also forms the profile's
+    parameter tangents).  The render is compute bound and its working set is
+    in L2 either way, so no flush here."""
+    from profit_b200 import PF_FP32, Model
+    from profit_b200 import workloads as W
+    try:
+        m = W.configure(Model(wl["width"], wl["height"]), wl)
+        m.set_parameters(refs, pvals[0])
+        m.set_debug(True)
+        m.evaluate()
+        counts = [m.evaluation_counts(i)[0] for i in range(len(wl["profiles"]))]
+        m.set_debug(False)
+        m.set_precision(PF_FP32)
+        m.set_data(image, sigma)
+        ts = []
+        for s in range(3 + steps):
+            m.set_parameters(refs, pvals[s % len(pvals)])
+            m.loglike_grad(refs)
+            if s >= 3:
+                ts.append(m.last_timings()[1])
+        m.close()
+    except Exception as e:  # an auxiliary figure: report, never lose the bench line
+        return {"error": str(e)}
+    n_eval = int(sum(counts))
+    render_ms = statistics.median(ts)
+    return {"evaluations": n_eval, "per_profile": [int(c) for c in counts], "render_ms": render_ms,
+            "evaluations_per_s": n_eval / (render_ms / 1e3),
+            "definition": "evaluate_at calls of the first proposal (plain FP64 debug counters) over the "
+                          "FP32 render phase (value + parameter tangents per evaluation), median of "
+                          f"{steps} proposals; pipe utilisation in profiles/render_bulge_disk_ps.txt"}
 
 
 def convolver_choice_rate(torch, flush, wl, image, sigma, refs, pvals, steps=30):

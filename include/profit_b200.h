@@ -304,6 +304,12 @@ int pf_loglike_norm_noalloc(const double *model, const double *data, const doubl
 int pf_model_set_debug(pf_model *m, int value);
 int pf_model_decisions(pf_model *m, int profile, int32_t *out, size_t capacity);
 int pf_model_level_counts(pf_model *m, int profile, int64_t *out, int max_levels, int *n_levels);
+/* Profile evaluations (evaluate_at calls, radial.cpp:54-134,291-344) of the
+ * last debug evaluation for one profile: out[0] the pixels evaluated
+ * directly, out[1 + L] the sub-point evaluations at recursion level L (two
+ * per sub-point where the level may recurse, else one); *total their sum.
+ * No counter of its own in libprofit: it is the work count of the render. */
+int pf_model_evaluation_counts(pf_model *m, int profile, int64_t *out, int max_levels, int64_t *total);
 
 /* Number of CUDA kernels this library has launched in this process. */
 unsigned long long pf_kernel_launches(void);

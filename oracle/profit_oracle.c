@@ -132,6 +132,7 @@ typedef struct {
 	int *decisions;
 	size_t n_decisions;
 	long level_counts[MAX_LEVELS];
+	long n_evals; /* evaluate_at calls of the last evaluation */
 } profile_t;
 
 struct pfo_model {
@@ -562,6 +563,9 @@ static double subsample_pixel(profile_t *p, double x0, double x1, double y0, dou
 #pragma omp atomic
 		p->level_counts[recur_level]++;
 	}
+	/* res^2 sub-points below, each evaluated twice when testing */
+#pragma omp atomic
+	p->n_evals += (long)resolution * resolution * (recurse ? 2 : 1);
 
 	double *pts = NULL;
 	size_t npts = 0;
@@ -621,6 +625,7 @@ static void radial_evaluate(const pfo_model *m, profile_t *p, double *image, uns
 	p->cx = p->xcen + offx * sx;
 	p->cy = p->ycen + offy * sy;
 	memset(p->level_counts, 0, sizeof(p->level_counts));
+	p->n_evals = 0;
 	free(p->decisions);
 	p->n_decisions = (size_t)width * height;
 	p->decisions = (int *)calloc(p->n_decisions, sizeof(int));
@@ -647,6 +652,8 @@ static void radial_evaluate(const pfo_model *m, profile_t *p, double *image, uns
 			}
 			else if (p->rough || r_prof > p->d_rscale_switch * p->rscale) {
 				pixel_val = evaluate_at(p, xp, yp);
+#pragma omp atomic
+				p->n_evals++;
 			}
 			else {
 				unsigned res = p->d_resolution, maxrec = p->max_recursions;
@@ -1020,6 +1027,12 @@ int pfo_decisions(pfo_model *m, int idx, int *out, size_t cap)
 	if (p->n_decisions > cap) return fail("buffer too small%s", NULL);
 	memcpy(out, p->decisions, sizeof(int) * p->n_decisions);
 	return (int)p->n_decisions;
+}
+
+long pfo_evaluations(pfo_model *m, int idx)
+{
+	if (idx < 0 || idx >= m->n_profiles) return fail("profile index out of range%s", NULL);
+	return m->profiles[idx].n_evals;
 }
 
 int pfo_level_counts(pfo_model *m, int idx, long *out, int max_levels)

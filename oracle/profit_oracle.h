@@ -41,6 +41,8 @@ int pfo_evaluate(pfo_model *m, double *out, size_t cap, unsigned *w, unsigned *h
 int pfo_decisions(pfo_model *m, int idx, int *out, size_t cap);
 /* Per-level subsample_pixel counts of profile idx (last evaluation). */
 int pfo_level_counts(pfo_model *m, int idx, long *out, int max_levels);
+/* evaluate_at calls of the last evaluation of profile idx (direct + sub-points) */
+long pfo_evaluations(pfo_model *m, int idx);
 /* Derived per-profile scalars of the last evaluation (rscale, ie, bn, acc,
  * rscale_switch, rscale_max, resolution, flux_scale, ...). */
 int pfo_profile_scalars(pfo_model *m, int idx, double *out, int n);

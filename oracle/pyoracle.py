@@ -238,6 +238,8 @@ class _OracleLib:
                                          C.POINTER(C.c_uint), C.POINTER(C.c_int), C.POINTER(C.c_int)]
             lib.pfo_decisions.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.c_size_t]
             lib.pfo_level_counts.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_long), C.c_int]
+            lib.pfo_evaluations.argtypes = [C.c_void_p, C.c_int]
+            lib.pfo_evaluations.restype = C.c_long
             lib.pfo_profile_scalars.argtypes = [C.c_void_p, C.c_int, _dp, C.c_int]
             lib.pfo_loglike_norm.restype = C.c_double
             lib.pfo_loglike_norm.argtypes = [_dp, _dp, _dp, C.POINTER(C.c_uint8), C.c_size_t]
@@ -336,6 +338,12 @@ class OracleModel:
         n = self.lib.pfo_level_counts(self.h, idx, out, max_levels)
         self._check(n)
         return [out[i] for i in range(n)]
+
+    def evaluations(self, idx: int) -> int:
+        """evaluate_at calls of the last evaluation of profile idx."""
+        n = self.lib.pfo_evaluations(self.h, idx)
+        self._check(n)
+        return int(n)
 
     def scalars(self, idx: int) -> Dict[str, float]:
         out = np.zeros(len(SCALAR_NAMES))

@@ -33,7 +33,7 @@ EXPORTED = (
     "pf_model_set_finesampling", "pf_model_set_return_finesampled", "pf_model_set_crop",
     "pf_model_set_convolver", "pf_model_set_precision", "pf_model_drawing_dims", "pf_model_evaluate",
     "pf_model_set_data", "pf_model_loglike", "pf_model_loglike_grad", "pf_model_loglike_grad_fd",
-    "pf_model_set_debug", "pf_model_decisions", "pf_model_level_counts", "pf_model_last_timings",
+    "pf_model_set_debug", "pf_model_decisions", "pf_model_level_counts", "pf_model_evaluation_counts", "pf_model_last_timings",
     "pf_kernel_launches",
 )
 
@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
         L.pf_model_set_debug.argtypes = [vp, C.c_int]
         L.pf_model_decisions.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.c_size_t]
         L.pf_model_level_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int)]
+        L.pf_model_evaluation_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int64)]
         L.pf_model_last_timings.argtypes = [vp, C.POINTER(C.c_float), C.c_int]
         L.pf_kernel_launches.restype = C.c_ulonglong
         _late_bindings(L)

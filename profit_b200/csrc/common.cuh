@@ -83,6 +83,9 @@ struct QueueSet {
 	uint32_t *overflow;    // set to 1 when an item had to be dropped
 	int32_t *decisions;    // optional [n_profiles][npix] subsample_pixel calls per pixel
 	unsigned long long *level_counts;  // optional [n_profiles][MAX_LEVELS]
+	// optional [n_profiles][1 + MAX_LEVELS]: profile evaluations (evaluate_at
+	// calls in libprofit's terms), the direct ones first, then per level
+	unsigned long long *evals = nullptr;
 	uint32_t *maxres = nullptr;  // optional: largest resolution of the level-0 items pushed
 	// optional: per level, the items' indices grouped by profile kind (filled
 	// by launch_levels32 before each wide level when set; same offsets as items)

@@ -374,6 +374,7 @@ struct pf_model {
 	// debug output of the last evaluation
 	std::vector<int32_t> decisions;
 	std::vector<unsigned long long> level_counts;
+	std::vector<unsigned long long> evals;  // [n_profiles][1 + MAX_LEVELS]
 	unsigned dec_npix = 0;
 	int dec_levels = 0;
 };
@@ -671,6 +672,8 @@ int prepare_queue(pf_model *m, const Analysis &a, size_t npix_total, QueueSet &q
 	q.levels = (uint32_t)a.levels;
 	q.decisions = decisions;
 	q.level_counts = level_counts;
+	// the debug counter buffer holds the evaluation counts after the level counts
+	q.evals = level_counts ? level_counts + (size_t)MAX_LEVELS * a.n_profiles : nullptr;
 	if (reset) PF_CUDA(cudaMemsetAsync(m->d_ctrl.p, 0, CTRL_WORDS * 4, m->stream));
 	return PF_OK;
 }
@@ -944,10 +947,13 @@ int fetch_debug(pf_model *m, const Analysis &a)
 	size_t npix = (size_t)a.dw * a.dh;
 	m->decisions.resize(npix * a.n_profiles);
 	m->level_counts.resize((size_t)MAX_LEVELS * a.n_profiles);
+	m->evals.resize((size_t)(1 + MAX_LEVELS) * a.n_profiles);
 	PF_CUDA(cudaMemcpyAsync(m->decisions.data(), m->d_decisions.p, npix * a.n_profiles * 4, cudaMemcpyDeviceToHost,
 	                        m->stream));
 	PF_CUDA(cudaMemcpyAsync(m->level_counts.data(), m->d_level_counts.p, (size_t)MAX_LEVELS * a.n_profiles * 8,
 	                        cudaMemcpyDeviceToHost, m->stream));
+	PF_CUDA(cudaMemcpyAsync(m->evals.data(), m->d_level_counts.as<unsigned long long>() + (size_t)MAX_LEVELS * a.n_profiles,
+	                        (size_t)(1 + MAX_LEVELS) * a.n_profiles * 8, cudaMemcpyDeviceToHost, m->stream));
 	PF_CUDA(cudaStreamSynchronize(m->stream));
 	m->dec_npix = (unsigned)npix;
 	m->dec_levels = a.levels;
@@ -969,9 +975,10 @@ int evaluate64(pf_model *m, Analysis &a)
 		unsigned long long *lc = nullptr;
 		if (m->debug) {
 			PF_CUDA(ensure(m->d_decisions, npix * a.n_profiles * 4));
-			PF_CUDA(ensure(m->d_level_counts, (size_t)MAX_LEVELS * a.n_profiles * 8));
+			const size_t counter_bytes = (size_t)(2 * MAX_LEVELS + 1) * a.n_profiles * 8;  // level counts, evaluations
+			PF_CUDA(ensure(m->d_level_counts, counter_bytes));
 			PF_CUDA(cudaMemsetAsync(m->d_decisions.p, 0, npix * a.n_profiles * 4, m->stream));
-			PF_CUDA(cudaMemsetAsync(m->d_level_counts.p, 0, (size_t)MAX_LEVELS * a.n_profiles * 8, m->stream));
+			PF_CUDA(cudaMemsetAsync(m->d_level_counts.p, 0, counter_bytes, m->stream));
 			dec = m->d_decisions.as<int32_t>();
 			lc = m->d_level_counts.as<unsigned long long>();
 		}
@@ -2324,6 +2331,20 @@ int pf_model_level_counts(pf_model *m, int profile, int64_t *out, int max_levels
 		if (c) n = l + 1;
 	}
 	if (n_levels) *n_levels = n;
+	return PF_OK;
+}
+
+int pf_model_evaluation_counts(pf_model *m, int profile, int64_t *out, int max_levels, int64_t *total)
+{
+	PF_TRY(check_profile(m, profile));
+	if (m->evals.empty()) return set_error(PF_E_STATE, "no counters recorded: enable debug and evaluate");
+	const unsigned long long *e = m->evals.data() + (size_t)profile * (1 + MAX_LEVELS);
+	unsigned long long sum = 0;
+	for (int l = 0; l < 1 + MAX_LEVELS; l++) {
+		if (out && l < max_levels) out[l] = (int64_t)e[l];
+		sum += e[l];
+	}
+	if (total) *total = (int64_t)sum;
 	return PF_OK;
 }
 

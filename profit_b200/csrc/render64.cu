@@ -63,6 +63,7 @@ __global__ void k_pixels64(const DevProfile *__restrict__ profiles, int n_profil
 		}
 		else if (d.rough || r > d.r_switch) {
 			acc[d.target] += d.flux_scale * eval64(d, xp, yp);
+			if (q.evals) atomicAdd(&q.evals[(size_t)p * (1 + MAX_LEVELS)], 1ull);
 		}
 		else {
 			unsigned res = d.resolution, max_rec = d.max_rec;
@@ -208,6 +209,13 @@ __global__ void k_count_decisions(QueueSet q, int level, size_t npix)
 		const SubItem &it = items[t];
 		atomicAdd(&q.decisions[(size_t)it.profile * npix + it.pixel], 1);
 		atomicAdd(&q.level_counts[(size_t)it.profile * MAX_LEVELS + level], 1ull);
+		// res^2 sub-points, each evaluated twice (value and test point) when the
+		// level may still recurse (radial.cpp:54-134)
+		if (q.evals) {
+			const unsigned long long res = it.res;
+			const bool recurse = res > 1 && (unsigned)level < it.max_rec;
+			atomicAdd(&q.evals[(size_t)it.profile * (1 + MAX_LEVELS) + 1 + level], res * res * (recurse ? 2ull : 1ull));
+		}
 	}
 }
 

@@ -265,6 +265,17 @@ class Model:
         check(lib().pf_model_level_counts(self._h, int(profile), out, 16, C.byref(n)))
         return [out[i] for i in range(n.value)]
 
+    def evaluation_counts(self, profile: int) -> Tuple[int, List[int]]:
+        """Profile evaluations of the last debug evaluation: (total, [direct,
+        level 0, level 1, ...]) with trailing empty levels dropped."""
+        out = (C.c_int64 * 17)()
+        tot = C.c_int64()
+        check(lib().pf_model_evaluation_counts(self._h, int(profile), out, 17, C.byref(tot)))
+        per = [out[i] for i in range(17)]
+        while len(per) > 1 and per[-1] == 0:
+            per.pop()
+        return tot.value, per
+
     def last_timings(self) -> List[float]:
         out = (C.c_float * 4)()
         check(lib().pf_model_last_timings(self._h, out, 4))

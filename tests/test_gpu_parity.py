@@ -44,6 +44,7 @@ def test_render_fp64_matches_reference(case):
     ora.evaluate()
     assert np.array_equal(m.decisions(0), ora.decisions(0))
     assert m.level_counts(0) == ora.level_counts(0)
+    assert m.evaluation_counts(0)[0] == ora.evaluations(0)
     dbg = RefModel(100, 100, debug=True)
     dbg.set_omp_threads(1)
     dbg.add_profile(name, **params)

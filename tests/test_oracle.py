@@ -138,6 +138,37 @@ def test_decision_counts_match_profit_debug(case):
     assert int(d[d > 0].sum()) == sum(ref.integrations(0))
 
 
+@pytest.mark.parametrize("case", [7, 9, 11])
+def test_evaluation_count_from_profit_debug(case):
+    """The oracle's evaluate_at count: one per directly evaluated pixel, and
+    res^2 sub-points per subsample_pixel call, each evaluated twice (value and
+    test point) below max_recursions = 2 and once at the last level
+    (radial.cpp:54-134).  Profiles without a centre override use one
+    resolution for every cell, so the count follows from PROFIT_DEBUG's
+    per-level counters of the compiled reference."""
+    name, params = PROFILE_CASES[case]
+    ref = RefModel(100, 100, debug=True)
+    ref.set_omp_threads(1)
+    ref.add_profile(name, **params)
+    ref.evaluate()
+    ora = OracleModel(100, 100)
+    ora.add_profile(name, **params)
+    ora.evaluate()
+    res = int(ora.scalars(0)["resolution"])
+    direct = int(np.sum(ora.decisions(0) == 0))
+    sub_evals = sum(c * res * res * (2 if level < 2 else 1) for level, c in enumerate(ref.integrations(0)))
+    assert ora.evaluations(0) == direct + sub_evals
+
+
+def test_evaluation_count_rough():
+    """rough = true evaluates each pixel inside rscale_max once."""
+    name, params = PROFILE_CASES[0]
+    ora = OracleModel(100, 100)
+    ora.add_profile(name, rough=True, **params)
+    ora.evaluate()
+    assert ora.evaluations(0) == int(np.sum(ora.decisions(0) == 0))
+
+
 def test_loglike_restatement():
     r = np.random.default_rng(5)
     model = r.uniform(0, 3, size=(40, 30))
