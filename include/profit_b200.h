@@ -120,7 +120,12 @@ int pf_model_set_dry_run(pf_model *m, int value);
 /* Model::set_omp_threads (model.h:333-336): accepted for compatibility; the
  * work runs on the GPU, so the value has no effect. */
 int pf_model_set_omp_threads(pf_model *m, unsigned threads);
-/* Only crop = true is supported (ProFit's returncrop default). */
+/* Model::set_crop (model.h:281-283; evaluate, model.cpp:307-322).  With the
+ * brute-force ("brute", "brute-old") and null convolvers crop = false returns
+ * the same image as crop = true, as libprofit does (those convolvers add no
+ * padding of their own).  With the "fft" convolver crop = false, whose result
+ * is the convolver's whole 2 max(image, psf) buffer, fails with PF_E_INVALID
+ * at evaluation. */
 int pf_model_set_crop(pf_model *m, int value);
 /* "brute" (default, like Model::ensure_convolver, model.cpp:144-150),
  * "brute-old", "fft" or "null" (create_convolver, convolve.cpp:526-594). */
@@ -204,6 +209,51 @@ int pf_model_loglike_grad(pf_model *m, const pf_param_ref *params, int n_params,
 int pf_model_loglike_grad_batch(pf_model *m, const pf_param_ref *params, int n_params, int batch,
                                 const double *values, double *loglike, double *grad);
 
+/* ---- Fit space: LP and d LP / d parm for batches of sampler proposals ----
+ * ProFit's samplers move a vector parm of fitted values, which
+ * profitRemakeModellist (R/profitRemakeModelList.R:27-166) turns into model
+ * parameters, and profitLikeModel returns LP = LL + priors
+ * (R/profitLikeModel.R:225-240, 342) with profitMakePriors' normal priors
+ * (R/profitUtility.R:124-176).  pf_model_set_fit_space installs that mapping
+ * on the model; pf_model_lp_grad_batch then evaluates LP and its gradient with
+ * respect to parm for a batch of fitted vectors (new: the reference has no
+ * gradient), the mapping and the chain rule running on the device, one thread
+ * per proposal (on the host for a few proposals).
+ *
+ * The n entries are model parameters in unlist(modellist) order:
+ *   params[i]   the profile and double parameter the entry sets
+ *   init[i]     its value in the model list (model space, not logged)
+ *   tofit[i]    1 fitted, 0 fixed at init, -1 takes the value of entry i-1
+ *               (R's NA in tofit; not allowed for entry 0)
+ *   tolog[i]    (NULL: none) a fitted entry is sampled as log10 of its value
+ *   lower/upper (NULL, or NaN entries: no limit) interval limits; an entry
+ *               the interval moves gets a zero gradient
+ *   offset      (NULL: none) R's offset: xcen += offset[0], ycen +=
+ *               offset[1], ang += offset[2] (NaN: none), then re, fwhm, rb,
+ *               rout, rc, rt, xcen and ycen *= offset[3] (NaN: none)
+ *   prior_sigma (NULL: no priors) sigma of a normal prior per entry, > 0;
+ *               +inf is a flat prior (profitMakePriors' allowflat)
+ *   prior_mean  (NULL: init) its mean (model space)
+ *   prior_tolog (NULL: tolog) the prior is on log10 of the value
+ *   prior_on    (NULL: every entry, profitMakePriors without tofit) which
+ *               entries carry a prior (pass tofit == 1 for its tofit form)
+ * Fixed entries' values (offsets and limits applied) are set on the profiles.
+ * Free and tied entries must have an adjoint (pf_model_loglike_grad). */
+int pf_model_set_fit_space(pf_model *m, int n, const pf_param_ref *params, const double *init, const int *tofit,
+                           const int *tolog, const double *lower, const double *upper, const double *offset,
+                           const double *prior_sigma, const double *prior_mean, const int *prior_tolog,
+                           const int *prior_on);
+/* Number of fitted entries (the length of parm) and of all entries. */
+int pf_model_fit_size(pf_model *m, int *n_fit, int *n_entries);
+/* For `batch` fitted vectors parm[b * n_fit + j]: lp[b] = LL + log prior,
+ * grad[b * n_fit + j] = d LP / d parm_j, parm_out[b * n_fit + j] the vector
+ * profitRemakeModellist hands back (limits applied, logged again), loglike[b]
+ * = LL.  grad, parm_out and loglike may be NULL.  A proposal whose model
+ * parameters fail validation gets lp = loglike = -INFINITY and a zero
+ * gradient. */
+int pf_model_lp_grad_batch(pf_model *m, int batch, const double *parm, double *lp, double *grad, double *parm_out,
+                           double *loglike);
+
 /* How the adjoint of the render is formed.  PF_ADJOINT_STORE keeps, per
  * radial profile, nine FP32 tangent planes of the drawing size from the
  * forward pass (fastest for a few profiles); PF_ADJOINT_RECOMPUTE records
@@ -278,14 +328,18 @@ int pf_catalogue_last_time(pf_catalogue *c, float *ms);
  *
  * The call only queues two kernels on `stream` on the calling thread's
  * current device and returns; read `loglike` after the stream has finished.
- * It forms pf_model_loglike's (PF_FP64) compensated sum over the same fixed
- * grid of blocks, so equal images give equal results to the last bit.
+ * It forms pf_model_loglike's (PF_FP64) compensated sum over the same grid
+ * of blocks for every image size (like_parts(npix, 1): at most 296 blocks,
+ * fewer for images under 151,552 pixels) and merges the partials in the same
+ * order, so equal images give equal results to the last bit.
  * batch above PF_LOGLIKE_NOALLOC_MAX_BATCH, or npix above
  * 2^31 - 1, fails with PF_E_CAPACITY before anything is queued.
  *
- * The first call on each device looks up the scratch array's address with
- * that device current (cudaGetSymbolAddress, which may load this library's
- * device code); make that first call before any stream capture begins.
+ * The first call in each CUDA context (per device: the primary context, and
+ * again after a cudaDeviceReset or with another context current) looks up
+ * the scratch array's address with that device current (cudaGetSymbolAddress,
+ * which may load this library's device code); make that first call before any
+ * stream capture begins.
  * All calls on a device share the one array, which keeps the last call's
  * contents (no call relies on it starting at zero).  Calls whose kernels can
  * run at the same time on the GPU, i.e. on different streams with nothing

@@ -48,6 +48,23 @@ constexpr int NTAN = 12;
 // profitLikeModel's like.func (R/profitUtility.R:99-121, without "st").
 enum LikeKind : int { LIKE_NORM = 0, LIKE_CHISQ = 1, LIKE_T = 2, LIKE_POIS = 3 };
 constexpr int LIKE_SCRATCH_PER_IMAGE = 5;  // doubles of launch_like64's stats scratch per image
+
+// Partial sums per image of the likelihood reduction (its grid) for `batch`
+// images of n pixels: enough blocks in all to fill the GPU, at least about
+// two pixels per thread (a batch of thousands of small images would
+// otherwise spend its time reducing near-empty blocks), at most
+// LIKE_MAX_PARTS.  The merge order of the partials, hence the last bit of
+// logL, follows from this count.
+constexpr int LIKE_MAX_PARTS = 296;  // 2 per SM
+inline int like_parts(int n, int batch)
+{
+	const int b = batch > 1 ? batch : 1;
+	const int fill = (148 * 16 + b - 1) / b;
+	const int work = (n + 511) / 512;
+	int p = fill < work ? fill : work;
+	p = p < LIKE_MAX_PARTS ? p : LIKE_MAX_PARTS;
+	return p > 1 ? p : 1;
+}
 constexpr int NTAN_GEOM = 6;
 
 // Tangent slots a profile of this kind fills (geometry, shape, box).

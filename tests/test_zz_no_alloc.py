@@ -100,3 +100,42 @@ def test_static_scratch_loglike_rejects_batches_beyond_its_size():
     got = d_ll.cpu().numpy()
     assert np.allclose(got[: n - 1], -npix * 0.5 * np.log(2 * np.pi), rtol=1e-14)
     assert np.isnan(got[n - 1])
+
+
+@pytest.mark.parametrize("w,h", [(100, 100), (37, 23), (400, 380)])
+def test_static_scratch_loglike_equals_model_loglike_bit_for_bit(w, h):
+    """Images below 151,552 pixels reduce over fewer than 296 blocks in
+    pf_model_loglike; the static-scratch call must use the same grid and give
+    the same logL to the last bit.  A rough profile (no subsampling, so no
+    atomically summed cells) and sky make the FP64 model image reproducible,
+    so both calls see the same image."""
+    import torch
+
+    psf = W.gaussian_psf(9, 2.0)
+    m = Model(w, h)
+    m.set_magzero(25.0)
+    m.set_psf(psf)
+    m.add_profile("sersic", xcen=w * 0.45, ycen=h * 0.55, mag=15.0, re=w * 0.1, nser=2.0, ang=30.0, axrat=0.7,
+                  rough=True, convolve=True)
+    m.add_profile("sky", bg=0.5)
+    img, _ = m.evaluate()
+    image, sigma = W.make_data(dict(sigma_range=(0.5, 2.0), seed_tag=71), img)
+    m.set_data(image, sigma)
+    ll = m.loglike()
+    again, _ = m.evaluate()
+    assert np.array_equal(again, img)
+
+    dev = torch.device("cuda:0")
+    d_model = torch.tensor(np.stack([img, img]), dtype=torch.float64, device=dev)
+    d_data = torch.tensor(image, dtype=torch.float64, device=dev)
+    d_sigma = torch.tensor(sigma, dtype=torch.float64, device=dev)
+    d_ll = torch.full((2,), float("nan"), dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    L = lib()
+    for _ in range(2):  # the second call runs on the scratch the first left
+        d_ll.fill_(float("nan"))
+        check(L.pf_loglike_norm_noalloc(d_model.data_ptr(), d_data.data_ptr(), d_sigma.data_ptr(), None, img.size,
+                                        2, d_ll.data_ptr(), stream.cuda_stream))
+        stream.synchronize()
+        got = d_ll.cpu().numpy()
+        assert got[0] == ll and got[1] == ll
