@@ -137,12 +137,33 @@ class ClockSampler:
 # CPU reference (libprofit compiled in place) timing
 # ---------------------------------------------------------------------------
 
-def reference_ll_grad(wl, params, image, sigma, threads, n_grad=None, rel_step=1e-7):
+def fastest_reference_build(wl, threads, reps=3):
+    """The build of the compiled reference that evaluates the workload's model
+    fastest on this host, among those it can run (the -O3 -march=x86-64-v4 /
+    v3 speed builds and the parity build); one warm-up and `reps` timed
+    evaluations each.  Returns (build, {build: seconds per evaluation})."""
+    from profit_b200 import workloads as W
+    from oracle.pyoracle import RefModel, runnable_reference_builds
+    times = {}
+    for b in runnable_reference_builds():
+        m = W.configure(RefModel(wl["width"], wl["height"], build=b), wl)
+        m.set_omp_threads(threads)
+        m.set_convolver("brute", threads)
+        m.evaluate()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            m.evaluate()
+        times[b] = (time.perf_counter() - t0) / reps
+    best = min(times, key=times.get)
+    return best, times
+
+
+def reference_ll_grad(wl, params, image, sigma, threads, n_grad=None, rel_step=1e-7, build="parity"):
     """logL + central FD gradient with the reference's own C++; returns (ll, grad, n_model_evals)."""
     from oracle.pyoracle import RefModel, loglike_norm
 
     def ll_at(overrides):
-        m = RefModel(wl["width"], wl["height"])
+        m = RefModel(wl["width"], wl["height"], build=build)
         m.set_magzero(wl["magzero"])
         m.set_psf(wl["psf"])
         m.set_omp_threads(threads)
@@ -168,12 +189,13 @@ def cpu_baseline(wl, image, sigma, budget_s=15.0):
     """Reference CPU LL+grad evals/s on a bounded sample (rank 0, N=1)."""
     from profit_b200 import workloads as W
     threads = os.cpu_count() or 1
+    build, _ = fastest_reference_build(wl, threads)
     t0 = time.perf_counter()
     n_full = 0
     evals = 0
     while True:
         prop = W.perturbed(wl, seed=10_000 + n_full, scale=0.02)
-        _, _, ne = reference_ll_grad(wl, prop["profiles"], image, sigma, threads)
+        _, _, ne = reference_ll_grad(wl, prop["profiles"], image, sigma, threads, build=build)
         evals += ne
         n_full += 1
         if time.perf_counter() - t0 > budget_s or n_full >= 20:
@@ -182,7 +204,13 @@ def cpu_baseline(wl, image, sigma, budget_s=15.0):
     return {"value": n_full / dt, "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"{n_full} LL+grad evaluations ({evals} libprofit model evaluations, central FD over "
                       f"{len(wl['grad'])} parameters) of the same workload, OpenMP {threads} threads, "
-                      f"{dt:.1f} s wall"}
+                      f"{dt:.1f} s wall, libprofit built {build_flags(build)}"}
+
+
+def build_flags(build):
+    return {"parity": "-O3 -mavx -ffp-contract=off (parity build)",
+            "x86-64-v3": "-O3 -march=x86-64-v3 (AVX2+FMA speed build)",
+            "x86-64-v4": "-O3 -march=x86-64-v4 (AVX-512 speed build)"}[build]
 
 
 # ---------------------------------------------------------------------------
@@ -663,8 +691,9 @@ def main_reference(args):
     from oracle.pyoracle import RefModel
     wl = workload()
     threads = os.cpu_count() or 1
+    build, build_times = fastest_reference_build(wl, threads)
     # data from the reference itself at the truth
-    m = W.configure(RefModel(wl["width"], wl["height"]), wl)
+    m = W.configure(RefModel(wl["width"], wl["height"], build=build), wl)
     m.set_omp_threads(threads)
     m.set_convolver("brute", threads)
     truth, _ = m.evaluate()
@@ -672,7 +701,8 @@ def main_reference(args):
     n_all = len(wl["grad"])
     # per-step sample: logL + FD over n_grad parameters, sized to ~2 min total
     t0 = time.perf_counter()
-    reference_ll_grad(wl, W.perturbed(wl, seed=0, scale=0.02)["profiles"], image, sigma, threads, n_grad=1)
+    reference_ll_grad(wl, W.perturbed(wl, seed=0, scale=0.02)["profiles"], image, sigma, threads, n_grad=1,
+                      build=build)
     per_eval = (time.perf_counter() - t0) / 3
     budget = 120.0
     total_steps = args.warmup + args.steps
@@ -681,7 +711,7 @@ def main_reference(args):
     for s in range(total_steps):
         prop = W.perturbed(wl, seed=s, scale=0.02)
         t = time.perf_counter()
-        _, _, ne = reference_ll_grad(wl, prop["profiles"], image, sigma, threads, n_grad=n_grad)
+        _, _, ne = reference_ll_grad(wl, prop["profiles"], image, sigma, threads, n_grad=n_grad, build=build)
         dt = time.perf_counter() - t
         if s >= args.warmup:
             times.append(dt * (1 + 2 * n_all) / ne)   # scaled to a full LL+grad
@@ -689,7 +719,9 @@ def main_reference(args):
     value = 1.0 / per_full
     sample = (f"each step: logL + central FD over {n_grad} of {n_all} parameters "
               f"({1 + 2 * n_grad} libprofit evaluations), time scaled by {1 + 2 * n_all}/{1 + 2 * n_grad} "
-              f"to a full LL+grad; OpenMP {threads} threads, brute-force convolver")
+              f"to a full LL+grad; OpenMP {threads} threads, brute-force convolver; libprofit built "
+              f"{build_flags(build)}, the fastest on this host of "
+              + ", ".join(f"{b} {1e3 * t:.1f} ms" for b, t in build_times.items()) + " per model evaluation")
     out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": 1e3 * per_full, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f64", "impl": "reference",

@@ -21,6 +21,17 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_SO = os.path.join(HERE, "_ref", "libprofit_ref.so")
 REF_DBG_SO = os.path.join(HERE, "_ref", "libprofit_ref_dbg.so")
+# Speed builds of the same sources for the timed CPU baseline (oracle/Makefile):
+# ISA level -> library, and the /proc/cpuinfo flags each level needs.
+REF_FAST_SO = {
+    "x86-64-v4": os.path.join(HERE, "_ref", "libprofit_ref_v4.so"),
+    "x86-64-v3": os.path.join(HERE, "_ref", "libprofit_ref_v3.so"),
+}
+_ISA_FLAGS = {
+    "x86-64-v3": {"avx", "avx2", "bmi1", "bmi2", "f16c", "fma", "abm", "movbe", "xsave"},
+    "x86-64-v4": {"avx", "avx2", "bmi1", "bmi2", "f16c", "fma", "abm", "movbe", "xsave",
+                  "avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"},
+}
 ORACLE_SO = os.path.join(HERE, "_build", "liboracle.so")
 
 _dp = C.POINTER(C.c_double)
@@ -41,8 +52,8 @@ class _RefLib:
     _libs: Dict[str, C.CDLL] = {}
 
     @classmethod
-    def get(cls, debug: bool = False) -> C.CDLL:
-        path = REF_DBG_SO if debug else REF_SO
+    def get(cls, debug: bool = False, build: str = "parity") -> C.CDLL:
+        path = REF_DBG_SO if debug else (REF_SO if build == "parity" else REF_FAST_SO[build])
         if path not in cls._libs:
             lib = _load(path)
             lib.pfref_model_new.restype = C.c_void_p
@@ -89,11 +100,35 @@ class RefError(RuntimeError):
     pass
 
 
-class RefModel:
-    """profit::Model from the compiled reference, configured like R_profit_make_model."""
+def host_cpu_flags() -> set:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
 
-    def __init__(self, width: int, height: int, debug: bool = False):
-        self.lib = _RefLib.get(debug)
+
+def runnable_reference_builds() -> list:
+    """The builds of the reference this host can run: the speed builds whose
+    ISA level the CPU supports (highest first), then the parity build."""
+    flags = host_cpu_flags()
+    out = [b for b in ("x86-64-v4", "x86-64-v3")
+           if _ISA_FLAGS[b] <= flags and os.path.exists(REF_FAST_SO[b])]
+    return out + ["parity"]
+
+
+class RefModel:
+    """profit::Model from the compiled reference, configured like R_profit_make_model.
+
+    build: "parity" (-O3 -mavx -ffp-contract=off, the build parity is pinned
+    on), or a speed build "x86-64-v3" / "x86-64-v4" (-O3 -march=..., GNU
+    mode) for timing; debug selects the PROFIT_DEBUG parity build."""
+
+    def __init__(self, width: int, height: int, debug: bool = False, build: str = "parity"):
+        self.lib = _RefLib.get(debug, build)
         self.debug = debug
         self.h = self.lib.pfref_model_new(width, height)
         self.nprof = 0

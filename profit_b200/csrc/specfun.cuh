@@ -130,9 +130,11 @@ PF_HD inline double qgamma(double p, double a)
 	return x;
 }
 
-// digamma(x) for x > 0.
+// digamma(x) for x > 0; NaN for x <= 0 or NaN (the recurrence below would
+// never reach 10 from -inf, and no caller needs the negative axis).
 PF_HD inline double digamma(double x)
 {
+	if (!(x > 0.0)) return NAN;
 	double r = 0;
 	while (x < 10.0) {
 		r -= 1.0 / x;

@@ -7,9 +7,10 @@ import struct
 import numpy as np
 import pytest
 
+from oracle.refpath import reference_root
 from profit_b200.fits import FitsError, read_cutout, read_fits, setup_region, write_fits
 
-KIDS = "/root/reference/inst/extdata/KiDS/G266035"
+KIDS = os.path.join(reference_root(), "inst", "extdata", "KiDS", "G266035")
 
 
 @pytest.mark.parametrize("bitpix", [-64, -32, 8, 16, 32, 64])
