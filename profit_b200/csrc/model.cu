@@ -371,6 +371,15 @@ struct pf_model {
 	int prof_begin_n = -1;
 	BatchState *batch = nullptr;
 
+	// fit space (pf_model_set_fit_space): the entries, the gradient
+	// references of their free and tied entries, and the entries' device copy
+	std::vector<FitEntry> fit_entries;
+	std::vector<std::pair<int, std::string>> fit_refs;
+	FitOffset fit_off{0.0, 0.0, 0.0, 1.0};
+	int fit_nfit = 0;
+	DevBuf d_fit_entries;
+	uint64_t fit_version = 0;
+
 	// debug output of the last evaluation
 	std::vector<int32_t> decisions;
 	std::vector<unsigned long long> level_counts;
@@ -381,18 +390,7 @@ struct pf_model {
 
 namespace {
 
-constexpr int NPARTS = 296;  // likelihood partial sums (2 per SM)
-
-// Partial sums per image for the FP32 pipelines' likelihood of `batch`
-// images of n pixels: enough blocks in all to fill the GPU, at least about
-// two pixels per thread (a batch of thousands of small images would
-// otherwise spend its time reducing near-empty blocks), at most NPARTS.
-inline int like_parts(int n, int batch)
-{
-	const int fill = (148 * 16 + batch - 1) / std::max(batch, 1);
-	const int work = (n + 511) / 512;
-	return std::max(1, std::min(NPARTS, std::min(fill, work)));
-}
+constexpr int NPARTS = LIKE_MAX_PARTS;  // likelihood partial sums (like_parts, common.cuh)
 constexpr size_t CTRL_WORDS = 64;  // counts[16], overflow, ...
 
 int analyze(pf_model *m, Analysis &a)
@@ -470,6 +468,15 @@ int analyze(pf_model *m, Analysis &a)
 		a.oh = a.ch;
 	}
 	a.n_profiles = (int)m->profiles.size();
+	// crop = false (Model::evaluate, model.cpp:307-322) changes the result
+	// only through the convolver's own padding: the brute-force and null
+	// convolvers add none (Convolver::padding, convolve.cpp:50-53), so their
+	// uncropped image is the cropped one.  The FFT convolver returns its whole
+	// 2 max(src, psf) buffer (convolve.cpp:81-95, 263-268); that form is not
+	// provided.
+	if (!m->crop && a.conv && m->conv_kind == CONV_FFT)
+		return set_error(PF_E_INVALID,
+		                 "crop = false is supported with the brute, brute-old and null convolvers, not with fft");
 	if (has_mask && !m->adjust_mask && (m->mask_w != a.dw || m->mask_h != a.dh))
 		return set_error(PF_E_INVALID, "Mask dimensions != drawing dimensions: " + std::to_string(m->mask_w) + "x" +
 		                                   std::to_string(m->mask_h) + " != " + std::to_string(a.dw) + "x" +
@@ -1331,9 +1338,20 @@ struct StageLayout {
 	}
 };
 
+// A batch evaluated in ProFit's fit space (pf_model_lp_grad_batch): the
+// proposals are fitted vectors parm (nfit per row) instead of model values.
+struct FitRun {
+	FitSpaceView host;  // entries in host memory (few-proposal path)
+	FitSpaceView dev;   // entries in device memory
+	double *lp, *grad, *parm_out, *ll;  // caller's outputs (any but lp may be null)
+};
+
 struct BatchState {
 	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out, d_ll, d_T, d_stage;
 	HostBuf h_tmpl, h_values, h_out, h_stage;
+	// fit space: parm of the chunk, [C] LP, [C][nfit] gradient, [C] LL, [C][nfit] parm_out
+	DevBuf d_fit_parm, d_fit_out;
+	HostBuf h_fit_out;
 	void *h_stage_dev = nullptr;  // h_stage as the device addresses it (mapped pinned memory), or null
 	void *h_out_dev = nullptr;    // likewise h_out
 	int refs_n = -1, chunk = 0;
@@ -1359,7 +1377,7 @@ constexpr size_t BATCH_BUDGET_BYTES = 24ull << 30;
 constexpr int HOST_PROLOGUE_MAX = 16;
 
 int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, int nrefs, const QueueSet &q,
-                        bool host_prologue, bool recompute)
+                        bool host_prologue, bool recompute, const FitRun *fit)
 {
 	const int nprof = a.n_profiles;
 	const size_t npix = (size_t)a.dw * a.dh, nout = (size_t)a.ow * a.oh;
@@ -1395,7 +1413,16 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	if (recompute) PF_CUDA(cudaMemsetAsync(bs.d_T.p, 0, (size_t)C * nprof * NTAN * 8, s));
 	if (!host_prologue) {
 		PF_CUDA(cudaMemcpyAsync(bs.d_tmpl.p, bs.h_tmpl.p, nprof * sizeof(ProfileParams), cudaMemcpyHostToDevice, s));
-		PF_CUDA(cudaMemcpyAsync(bs.d_values.p, bs.h_values.p, (size_t)C * nrefs * 8, cudaMemcpyHostToDevice, s));
+		if (fit) {
+			// the fitted vectors in, the model values of the proposals from them
+			const int nfit = fit->dev.nfit;
+			PF_CUDA(cudaMemcpyAsync(bs.d_fit_parm.p, bs.h_values.p, (size_t)C * nfit * 8, cudaMemcpyHostToDevice, s));
+			PF_CUDA(launch_fit_remake(fit->dev, C, bs.d_fit_parm.as<double>(), bs.d_values.as<double>(),
+			                          bs.d_fit_out.as<double>() + (size_t)C * (2 + nfit), s));
+		}
+		else {
+			PF_CUDA(cudaMemcpyAsync(bs.d_values.p, bs.h_values.p, (size_t)C * nrefs * 8, cudaMemcpyHostToDevice, s));
+		}
 		PF_CUDA(cudaMemsetAsync(bs.d_invalid.p, 0, (size_t)C * 4, s));
 		PF_CUDA(launch_batch_prologue(bs.d_tmpl.as<ProfileParams>(), nprof, C, ref_profile, ref_offset, nrefs,
 		                              bs.d_values.as<double>(), geometry(m, a), bs.d_dev.as<DevProfile>(),
@@ -1426,7 +1453,7 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	GradStepArgs gargs = {dev, nprof, C, nrefs, ref_profile, ref_code, bs.d_ll.as<double>(), invalid, out_ll, out_grad};
 	// folded, the step writes logL, the gradient and the queue counters
 	// straight into the pinned result buffer (no download afterwards)
-	const bool direct_out = fold_grad && bs.h_out_dev;
+	const bool direct_out = fold_grad && bs.h_out_dev && !fit;
 	if (direct_out) {
 		char *hd = static_cast<char *>(bs.h_out_dev);
 		gargs.out_ll = reinterpret_cast<double *>(hd);
@@ -1449,6 +1476,14 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	if (!fold_grad)
 		PF_CUDA(launch_batch_gradient(dev, nprof, C, ref_profile, ref_code, nrefs, bs.d_T.as<double>(),
 		                              bs.d_ll.as<double>(), invalid, out_ll, out_grad, s));
+	if (fit && !host_prologue) {
+		// LP and d LP / d parm from logL and d logL / d theta
+		const int nfit = fit->dev.nfit;
+		PF_CUDA(launch_fit_finish(fit->dev, C, bs.d_fit_parm.as<double>(), bs.d_values.as<double>(), out_ll, out_grad,
+		                          bs.d_fit_out.as<double>(), s));
+		PF_CUDA(cudaMemcpyAsync(bs.h_fit_out.p, bs.d_fit_out.p, (size_t)C * (2 + 2 * nfit) * 8, cudaMemcpyDeviceToHost,
+		                        s));
+	}
 	PF_CUDA(record_event(m->ev[3], s));
 	char *ho = bs.h_out.as<char>();
 	if (!direct_out)
@@ -1457,8 +1492,12 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	return PF_OK;
 }
 
+// B proposals, values[b * nrefs + i] the value of refs[i] in proposal b (null:
+// one proposal at the model's current values).  With fit, values holds the
+// fitted vectors (fit->host.nfit per proposal) and the results go to fit's
+// outputs (LP, d LP / d parm, LL, parm_out) instead of ll_out / grad_out.
 int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, const double *values, double *ll_out,
-                    double *grad_out)
+                    double *grad_out, const FitRun *fit = nullptr)
 {
 	PF_TRY(ensure_stream(m));
 	Analysis a;
@@ -1544,8 +1583,16 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	PF_CUDA(ensure(bs.d_dev, (size_t)C * nprof * sizeof(DevProfile)));
 	PF_CUDA(ensure(bs.d_tmpl, nprof * sizeof(ProfileParams)));
 	PF_CUDA(ensure(bs.h_tmpl, nprof * sizeof(ProfileParams)));
+	// one row of `values` per proposal: model values, or fitted vectors
+	const int row = fit ? fit->host.nfit : nrefs;
 	PF_CUDA(ensure(bs.d_values, (size_t)C * nrefs * 8 + 8));
-	PF_CUDA(ensure(bs.h_values, (size_t)C * nrefs * 8 + 8));
+	PF_CUDA(ensure(bs.h_values, (size_t)C * std::max(nrefs, row) * 8 + 8));
+	if (fit) {
+		const size_t fo = (size_t)C * (2 + 2 * (size_t)row) * 8;
+		PF_CUDA(ensure(bs.d_fit_parm, (size_t)C * row * 8 + 8));
+		PF_CUDA(ensure(bs.d_fit_out, fo));
+		PF_CUDA(ensure(bs.h_fit_out, fo));
+	}
 	PF_CUDA(ensure(bs.d_invalid, (size_t)C * 4));
 	PF_CUDA(ensure(bs.d_ll, (size_t)C * 8));
 	PF_CUDA(ensure(bs.d_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
@@ -1598,13 +1645,27 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 	const ModelGeom geom = geometry(m, a);
 
 	char *ho = bs.h_out.as<char>();
+	// few-proposal path in fit space: the remake and the chain rule run on the
+	// host (the same code as the device kernels)
+	std::vector<double> fit_vals, fit_pout;
+	if (fit && host_prologue) {
+		fit_vals.resize((size_t)C * std::max(nrefs, 1));
+		fit_pout.resize((size_t)C * std::max(row, 1));
+	}
 	for (int b0 = 0; b0 < B; b0 += C) {
 		const int n = std::min(C, B - b0);
 		// the graph is recorded for full chunks; a short last chunk is padded
 		// with copies of its first proposal
 		double *hv = bs.h_values.as<double>();
-		std::memcpy(hv, values + (size_t)b0 * nrefs, (size_t)n * nrefs * 8);
-		for (int b = n; b < C; b++) std::memcpy(hv + (size_t)b * nrefs, values + (size_t)b0 * nrefs, (size_t)nrefs * 8);
+		std::memcpy(hv, values + (size_t)b0 * row, (size_t)n * row * 8);
+		for (int b = n; b < C; b++) std::memcpy(hv + (size_t)b * row, values + (size_t)b0 * row, (size_t)row * 8);
+		const double *vals = hv;  // model values of the chunk's proposals
+		if (fit && host_prologue) {
+			for (int b = 0; b < C; b++)
+				fit_remake(fit->host, hv + (size_t)b * row, fit_vals.data() + (size_t)b * nrefs,
+				           fit_pout.data() + (size_t)b * row);
+			vals = fit_vals.data();
+		}
 		if (host_prologue) {
 			const StageLayout L(C, nprof);
 			DevProfile *hd = bs.h_stage.as<DevProfile>();
@@ -1617,7 +1678,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 					for (int r = 0; r < nrefs; r++)
 						if (host_refs[r] == p)
 							*reinterpret_cast<double *>(reinterpret_cast<char *>(&pp) + host_refs[nrefs + r]) =
-							    hv[(size_t)b * nrefs + r];
+							    vals[(size_t)b * nrefs + r];
 					if (!params_valid(pp)) {
 						hi[b] = 1;
 						pp.kind = PK_NULL;
@@ -1649,6 +1710,11 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			sig.push_back((uint64_t)(uintptr_t)bs.h_out.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_values.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_tmpl.p);
+			sig.push_back(fit ? 1 + m->fit_version : 0);
+			if (fit)
+				for (const void *p : std::initializer_list<const void *>{fit->dev.e, bs.d_fit_parm.p, bs.d_fit_out.p,
+				                                                         bs.h_fit_out.p})
+					sig.push_back((uint64_t)(uintptr_t)p);
 			bool replayed = false;
 			if (bs.graph && bs.sig == sig) {
 				PF_CUDA(cudaGraphLaunch(bs.graph, m->stream));
@@ -1656,7 +1722,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				replayed = true;
 			}
 			else {
-				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute));
+				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute, fit));
 			}
 			PF_CUDA(cudaStreamSynchronize(m->stream));
 			int retry = 0;
@@ -1674,7 +1740,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				unsigned long long before = g_launches.load();
 				cudaGraph_t graph = nullptr;
 				PF_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
-				int st = enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute);
+				int st = enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute, fit);
 				cudaError_t ce = cudaStreamEndCapture(m->stream, &graph);
 				bs.graph_kernels = g_launches.load() - before;
 				g_launches -= bs.graph_kernels;
@@ -1687,6 +1753,32 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			}
 		}
 		if (!done) return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+		if (fit) {
+			const double *ll = reinterpret_cast<const double *>(ho), *g = ll + C;
+			for (int b = 0; b < n; b++) {
+				double lp, llb, *dlp = fit->grad ? fit->grad + (size_t)(b0 + b) * row : nullptr;
+				if (host_prologue) {
+					std::vector<double> tmp(dlp ? 0 : row);
+					fit_finish_one(fit->host, hv + (size_t)b * row, vals + (size_t)b * nrefs, ll[b], g + (size_t)b * nrefs,
+					               &lp, dlp ? dlp : tmp.data(), &llb);
+					if (fit->parm_out)
+						std::memcpy(fit->parm_out + (size_t)(b0 + b) * row, fit_pout.data() + (size_t)b * row,
+						            (size_t)row * 8);
+				}
+				else {
+					const double *fo = bs.h_fit_out.as<double>();
+					lp = fo[b];
+					llb = fo[(size_t)C * (1 + row) + b];
+					if (dlp) std::memcpy(dlp, fo + C + (size_t)b * row, (size_t)row * 8);
+					if (fit->parm_out)
+						std::memcpy(fit->parm_out + (size_t)(b0 + b) * row, fo + (size_t)C * (2 + row) + (size_t)b * row,
+						            (size_t)row * 8);
+				}
+				fit->lp[b0 + b] = lp;
+				if (fit->ll) fit->ll[b0 + b] = llb;
+			}
+			continue;
+		}
 		if (ll_out) std::memcpy(ll_out + b0, ho, (size_t)n * 8);
 		if (grad_out) std::memcpy(grad_out + (size_t)b0 * nrefs, ho + (size_t)C * 8, (size_t)n * nrefs * 8);
 	}
@@ -1998,8 +2090,7 @@ int pf_model_set_adjust_mask(pf_model *m, int value)
 int pf_model_set_crop(pf_model *m, int value)
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");
-	if (!value) return set_error(PF_E_INVALID, "crop = false is not supported");
-	m->crop = true;
+	m->crop = value != 0;
 	return PF_OK;
 }
 
@@ -2203,6 +2294,119 @@ int pf_model_loglike_grad_batch(pf_model *m, const pf_param_ref *params, int n_p
 		grad = scratch.data();
 	}
 	return eval_grad_batch(m, params, n_params, batch, values, loglike, grad);
+}
+
+// ProFit's fit space (profitRemakeModellist, R/profitRemakeModelList.R:27-166;
+// profitMakePriors, R/profitUtility.R:124-176), fitspace.cuh.
+int pf_model_set_fit_space(pf_model *m, int n, const pf_param_ref *params, const double *init, const int *tofit,
+                           const int *tolog, const double *lower, const double *upper, const double *offset,
+                           const double *prior_sigma, const double *prior_mean, const int *prior_tolog,
+                           const int *prior_on)
+{
+	if (!m || n < 1 || !params || !init || !tofit) return set_error(PF_E_INVALID, "null argument or no entries");
+	PF_TRY(ensure_stream(m));
+	FitOffset off{0.0, 0.0, 0.0, 1.0};
+	if (offset) {
+		if (!std::isfinite(offset[0]) || !std::isfinite(offset[1]))
+			return set_error(PF_E_INVALID, "offset x and y must be finite");
+		off.x = offset[0];
+		off.y = offset[1];
+		off.ang = std::isnan(offset[2]) ? 0.0 : offset[2];
+		off.size = std::isnan(offset[3]) ? 1.0 : offset[3];
+	}
+	std::vector<FitEntry> E((size_t)n);
+	std::vector<std::pair<int, std::string>> refs;
+	int nfit = 0;
+	for (int i = 0; i < n; i++) {
+		const int pi = params[i].profile;
+		const char *name = params[i].name;
+		if (!name) return set_error(PF_E_INVALID, "null parameter name");
+		PF_TRY(check_profile(m, pi));
+		const ParamDesc *d = find_param(m->profiles[pi].kind, name);
+		if (!d || d->type != T_DOUBLE)
+			return set_error(PF_E_UNKNOWN_PARAM, std::string("Unknown double parameter: ") + name);
+		FitEntry e;
+		std::memset(&e, 0, sizeof e);
+		e.fit = tofit[i] > 0 ? FIT_FREE : tofit[i] < 0 ? FIT_TIED : FIT_FIXED;
+		if (i == 0 && e.fit == FIT_TIED)
+			return set_error(PF_E_INVALID, "the first entry cannot take its value from the entry before it");
+		// R unlogs the entries that are both tolog and fitted (tounlogIDs)
+		e.tolog = tolog && tolog[i] && e.fit == FIT_FREE;
+		e.fit_index = e.fit == FIT_FREE ? nfit++ : -1;
+		e.ref_index = -1;
+		if (e.fit != FIT_FIXED) {
+			int code = 0;
+			PF_TRY(gradient_code(m->profiles[pi], name, code));
+			e.ref_index = (int)refs.size();
+			refs.emplace_back(pi, std::string(name));
+		}
+		if (offset) {
+			const std::string nm(name);
+			if (nm == "xcen") e.offset_bits = OFS_X | OFS_SIZE;
+			else if (nm == "ycen") e.offset_bits = OFS_Y | OFS_SIZE;
+			else if (nm == "ang") e.offset_bits = OFS_ANG;
+			else if (nm == "re" || nm == "fwhm" || nm == "rb" || nm == "rout" || nm == "rc" || nm == "rt")
+				e.offset_bits = OFS_SIZE;
+		}
+		const double lo = lower ? lower[i] : NAN, hi = upper ? upper[i] : NAN;
+		e.limited = !(std::isnan(lo) && std::isnan(hi));
+		e.lo = std::isnan(lo) ? -INFINITY : lo;
+		e.hi = std::isnan(hi) ? INFINITY : hi;
+		e.init = init[i];
+		if (prior_sigma) {
+			const double sg = prior_sigma[i];
+			if (!(sg > 0)) return set_error(PF_E_INVALID, "prior sigmas must be positive (inf: flat)");
+			const bool on = prior_on ? prior_on[i] != 0 : true;
+			e.prior = on && std::isfinite(sg);
+			e.prior_sigma = sg;
+			e.prior_mean = prior_mean ? prior_mean[i] : init[i];
+			e.prior_tolog = prior_tolog ? prior_tolog[i] != 0 : (tolog && tolog[i]);
+		}
+		E[i] = e;
+	}
+	if (nfit == 0) return set_error(PF_E_INVALID, "no fitted entry (tofit = 1)");
+	// fixed entries do not move with parm: their model value (offsets and
+	// clamp applied to init) goes on the profile once
+	for (int i = 0; i < n; i++)
+		if (E[i].fit == FIT_FIXED)
+			PF_TRY(set_param(m, params[i].profile, params[i].name, T_DOUBLE, fit_clamp(E[i], fit_pre_value(E[i], off, nullptr)),
+			                 0, 0));
+	PF_CUDA(ensure(m->d_fit_entries, E.size() * sizeof(FitEntry)));
+	PF_CUDA(cudaMemcpy(m->d_fit_entries.p, E.data(), E.size() * sizeof(FitEntry), cudaMemcpyHostToDevice));
+	m->fit_entries = std::move(E);
+	m->fit_refs = std::move(refs);
+	m->fit_off = off;
+	m->fit_nfit = nfit;
+	m->fit_version++;
+	return PF_OK;
+}
+
+int pf_model_fit_size(pf_model *m, int *n_fit, int *n_entries)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	if (n_fit) *n_fit = m->fit_nfit;
+	if (n_entries) *n_entries = (int)m->fit_entries.size();
+	return PF_OK;
+}
+
+int pf_model_lp_grad_batch(pf_model *m, int batch, const double *parm, double *lp, double *grad, double *parm_out,
+                           double *loglike)
+{
+	if (!m || batch < 1 || !parm || !lp) return set_error(PF_E_INVALID, "null argument or empty batch");
+	if (m->fit_entries.empty()) return set_error(PF_E_STATE, "no fit space: call pf_model_set_fit_space first");
+	if (!m->has_data) return set_error(PF_E_STATE, "no data: call pf_model_set_data first");
+	const int nrefs = (int)m->fit_refs.size();
+	std::vector<pf_param_ref> refs((size_t)nrefs);
+	for (int i = 0; i < nrefs; i++) refs[i] = pf_param_ref{m->fit_refs[i].first, m->fit_refs[i].second.c_str()};
+	FitRun fr;
+	fr.host = FitSpaceView{m->fit_entries.data(), (int)m->fit_entries.size(), m->fit_nfit, nrefs, m->fit_off};
+	fr.dev = fr.host;
+	fr.dev.e = m->d_fit_entries.as<FitEntry>();
+	fr.lp = lp;
+	fr.grad = grad;
+	fr.parm_out = parm_out;
+	fr.ll = loglike;
+	return eval_grad_batch(m, refs.data(), nrefs, batch, parm, nullptr, nullptr, &fr);
 }
 
 int pf_model_loglike_grad_fd(pf_model *m, const pf_param_ref *params, int n_params, double rel_step, double *loglike,

@@ -695,3 +695,47 @@ def test_fp32_adjoint_with_mask_and_finesampling_matches_fd64(kind, fs, conv):
         # proposal: FP32 sums in another order)
         assert ll_b[s] == pytest.approx(l1, rel=1e-6)
         np.testing.assert_allclose(g_b[s], g1, rtol=1e-5, atol=1e-6 * np.max(np.abs(g1)))
+
+
+@pytest.mark.parametrize("conv", ["brute", "brute-old", "null"])
+@pytest.mark.parametrize("crop", [True, False])
+def test_convolvers_and_crop_match_reference(conv, crop):
+    """"brute-old" (BruteForceConvolver, convolve.cpp:101-156: one running
+    sum per output pixel with edge clipping) and "brute"
+    (AssociativeBruteForceConvolver, row dot products) sum in different
+    orders; both agree with the compiled reference's own convolver of that
+    name to 1e-12, with and without a calculation mask.  crop = false
+    (model.cpp:307-322) returns the cropped image for these convolvers, since
+    they add no padding of their own; the offset stays (0, 0)."""
+    psf = W.moffat_psf(15, 3.0, 2.5)
+    mask = _mask_case("edge")
+    for use_mask in (False, True):
+        out = []
+        for M in (RefModel, Model):
+            m = M(100, 90)
+            m.set_magzero(30.0)
+            m.set_psf(psf)
+            m.set_convolver(conv)
+            m.set_crop(crop)
+            m.add_profile("sersic", xcen=52.3, ycen=44.1, re=6, nser=2.5, ang=30, axrat=0.6, convolve=True)
+            m.add_profile("moffat", xcen=20.5, ycen=70.2, fwhm=3, con=2.5, convolve=False)
+            m.add_profile("sky", bg=0.1)
+            if use_mask:
+                m.set_mask(mask)
+            out.append(m.evaluate())
+        (ref, ref_off), (got, got_off) = out
+        assert got.shape == ref.shape == (90, 100)
+        assert got_off == ref_off == (0, 0)
+        assert _rel(got, ref) <= IMG_TOL
+
+
+def test_crop_false_with_fft_is_refused():
+    m = Model(40, 30)
+    m.set_psf(W.gaussian_psf(9, 2.0))
+    m.set_convolver("fft")
+    m.set_crop(False)
+    m.add_profile("sersic", xcen=20, ycen=15, re=3, convolve=True)
+    with pytest.raises(InvalidParameter, match="crop = false"):
+        m.evaluate()
+    m.set_crop(True)
+    assert m.evaluate()[0].shape == (30, 40)
