@@ -144,6 +144,11 @@ def _late_bindings(L):
     L.pf_catalogue_gradient_offset.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.pf_catalogue_loglike_grad.argtypes = [vp, _dp, _dp]
     L.pf_catalogue_last_time.argtypes = [vp, C.POINTER(C.c_float)]
+    ip = C.POINTER(C.c_int)
+    L.pf_model_set_fit_space.argtypes = [vp, C.c_int, C.POINTER(pf_param_ref), _dp, ip, ip, _dp, _dp, _dp, _dp, _dp,
+                                         ip, ip]
+    L.pf_model_fit_size.argtypes = [vp, ip, ip]
+    L.pf_model_lp_grad_batch.argtypes = [vp, C.c_int, _dp, _dp, _dp, _dp, _dp]
     # device pointers travel as plain integers (e.g. a torch tensor's data_ptr())
     L.pf_loglike_norm_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
                                           C.c_void_p, C.c_void_p]
@@ -160,4 +165,5 @@ EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch",
                        "pf_catalogue_size", "pf_catalogue_gradient_offset", "pf_catalogue_loglike_grad",
                        "pf_catalogue_last_time", "pf_model_set_likelihood", "pf_model_set_mask",
                        "pf_model_set_adjust_mask", "pf_model_set_dimensions", "pf_model_set_dry_run",
-                       "pf_model_set_omp_threads", "pf_model_benchmark_convolvers")
+                       "pf_model_set_omp_threads", "pf_model_benchmark_convolvers", "pf_model_set_fit_space",
+                       "pf_model_fit_size", "pf_model_lp_grad_batch")

@@ -33,6 +33,8 @@ UNITS = {
     "fft.cu": [],
     "model.cu": ["--fmad=false"],
     "like_noalloc.cu": ["--fmad=false"],
+    # the fit-space kernels round like the host copy of the same code (model.cu)
+    "fitspace.cu": ["--fmad=false"],
 }
 
 

@@ -178,3 +178,15 @@ cudaError_t launch_like64(int kind, const double *model, const double *data, con
                           int nparts, double *stats, double *out, float *wseed, cudaStream_t s,
                           unsigned *tickets = nullptr);
 }  // namespace pf
+
+#include "fitspace.cuh"
+
+namespace pf {
+// fitspace.cu: ProFit's fit space for batches, one thread per proposal.
+// parm[batch][nfit] -> values[batch][nrefs] and parm_out[batch][nfit]
+cudaError_t launch_fit_remake(const FitSpaceView &fs, int batch, const double *parm, double *values, double *parm_out,
+                              cudaStream_t s);
+// out = [batch] LP, [batch][nfit] d LP / d parm, [batch] LL
+cudaError_t launch_fit_finish(const FitSpaceView &fs, int batch, const double *parm, const double *values,
+                              const double *ll, const double *grad_ll, double *out, cudaStream_t s);
+}  // namespace pf

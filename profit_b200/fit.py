@@ -1,21 +1,31 @@
 """Fit-space parameters and priors around the likelihood, as ProFit's R layer
-has them: profitRemakeModellist (R/profitRemakeModelList.R:1-167) maps the
-sampler's parameter vector to model parameters (tofit, tolog, ties, interval
-clamps), profitMakePriors (R/profitUtility.R:124-176) builds normal priors, and
-profitLikeModel returns LP = LL + priors (R/profitLikeModel.R:225-240, 338).
+has them: profitRemakeModellist (R/profitRemakeModelList.R:27-166) maps the
+sampler's parameter vector to model parameters (tofit, tolog, offsets, ties,
+interval clamps), profitMakePriors (R/profitUtility.R:124-176) builds normal
+priors, and profitLikeModel returns LP = LL + priors (R/profitLikeModel.R:
+225-240, 342).
 
 On top of ProFit this gives d LP / d parm in fit space: the device adjoint
 gradient d LL / d theta (theta the model parameters) chained through the
 transforms.
 
-    theta_i = clamp(10^parm_i if tolog_i else parm_i, interval_i)
+    value_i = 10^parm_i if tolog_i else parm_i      (fitted entries; init otherwise)
+    value_i = (value_i + offset shift) * offset size   (by parameter name)
+    theta_i = clamp(value_i, interval_i), or theta_{i-1} for a tied entry
     d theta_i / d parm_i = (0 if clamped else 1) * (theta_i ln 10 if tolog_i else 1)
+                           * (offset size for size parameters)
 
 A parameter whose tofit entry is None takes the value of the one before it
 (ProFit's NA), after the clamps, and its gradient flows to that parameter.
 Priors are normal on theta, or on log10(theta) where the prior's tolog is set,
-evaluated at the clamped values, for the fitted parameters; an infinite sigma
-means a flat prior (profitMakePriors' allowflat).
+evaluated at the clamped values, on every entry (profitMakePriors without
+tofit) or on those prior_on selects; an infinite sigma means a flat prior
+(profitMakePriors' allowflat).
+
+FitSpace is the host form of the mapping (one proposal at a time, any
+likelihood callable).  FitSpace.install(model) puts the same mapping on a
+profit_b200.Model, whose lp_grad_batch(parm) then evaluates LP and
+d LP / d parm for whole batches with the mapping on the device.
 """
 from __future__ import annotations
 
@@ -40,7 +50,8 @@ class FitSpace:
                  tofit: Sequence[Optional[bool]], tolog: Optional[Sequence[bool]] = None,
                  intervals: Optional[Sequence[Optional[Tuple[float, float]]]] = None,
                  prior_sigmas: Optional[Sequence[float]] = None, prior_means: Optional[Sequence[float]] = None,
-                 prior_tolog: Optional[Sequence[bool]] = None):
+                 prior_tolog: Optional[Sequence[bool]] = None, offset: Optional[Sequence[float]] = None,
+                 prior_on: Optional[Sequence[bool]] = None, names: Optional[Sequence[str]] = None):
         n = len(params)
         self.params = list(params)
         self.init = np.asarray(init, dtype=np.float64)
@@ -57,6 +68,23 @@ class FitSpace:
         self.prior_tolog = self.tolog.copy() if prior_tolog is None else np.asarray(prior_tolog, dtype=bool)
         if self.sigmas is not None and (len(self.sigmas) != n or np.any(self.sigmas <= 0)):
             raise ValueError("prior sigmas must be positive, one per parameter")
+        self.prior_on = np.ones(n, bool) if prior_on is None else np.asarray(prior_on, dtype=bool)
+        # R's offset: xcen/ycen/ang shifts, then size parameters scaled
+        self.offset = None if offset is None else [float(v) for v in offset]
+        names = [nm for (_, nm) in self.params] if names is None else list(names)
+        self._shift = np.zeros(n)
+        self._scale = np.ones(n)
+        if self.offset is not None:
+            ox, oy, oang, osize = self.offset
+            for i, nm in enumerate(names):
+                if nm == "xcen":
+                    self._shift[i] = ox
+                elif nm == "ycen":
+                    self._shift[i] = oy
+                elif nm == "ang" and not math.isnan(oang):
+                    self._shift[i] = oang
+                if nm in ("xcen", "ycen", "re", "fwhm", "rb", "rout", "rc", "rt") and not math.isnan(osize):
+                    self._scale[i] = osize
 
     def initial_parm(self) -> np.ndarray:
         """The sampler's starting vector (profitSetupData's init in fit space)."""
@@ -77,6 +105,8 @@ class FitSpace:
                 deriv[i] = theta[i] * LN10
             else:
                 theta[i] = parm[j]
+        theta = (theta + self._shift) * self._scale
+        deriv = deriv * self._scale
         for i, f in enumerate(self.tofit):
             if f is None:
                 theta[i] = theta[i - 1]
@@ -91,7 +121,7 @@ class FitSpace:
         for i, f in enumerate(self.tofit):  # re-inherit after the clamps
             if f is None:
                 theta[i] = theta[i - 1]
-        out = theta[self.fit_ids].copy()
+        out = (theta[self.fit_ids] - self._shift[self.fit_ids]) / self._scale[self.fit_ids]
         out = np.where(self.tolog[self.fit_ids], np.log10(out), out)
         return theta, deriv, out
 
@@ -101,7 +131,7 @@ class FitSpace:
         if self.sigmas is None:
             return 0.0, g
         lp = 0.0
-        for i in self.fit_ids:
+        for i in np.flatnonzero(self.prior_on):
             s = self.sigmas[i]
             if not math.isfinite(s):
                 continue  # flat
@@ -124,6 +154,14 @@ class FitSpace:
                 d[i - 1] += d[i]
                 d[i] = 0.0
         return np.array([d[i] * deriv[i] for i in self.fit_ids])
+
+    def install(self, model) -> None:
+        """Puts this mapping on a profit_b200.Model (pf_model_set_fit_space):
+        model.lp_grad_batch(parm) then evaluates LP, d LP / d parm, the
+        returned parm and LL for a batch of fitted vectors on the device."""
+        model.set_fit_space(self.params, self.init, self.tofit, self.tolog, self.intervals, self.offset,
+                            None if self.sigmas is None else self.sigmas, self.means, self.prior_tolog,
+                            self.prior_on)
 
     def lp_grad(self, parm: Sequence[float],
                 loglike_grad: Callable[[Sequence[Tuple[int, str]], np.ndarray], Tuple[float, np.ndarray]]

@@ -243,6 +243,56 @@ class Model:
                                                 ll.ctypes.data_as(_capi._dp), g.ctypes.data_as(_capi._dp)))
         return ll, g
 
+    def set_fit_space(self, params: Sequence[Tuple[int, str]], init: Sequence[float],
+                      tofit: Sequence[Optional[bool]], tolog: Optional[Sequence[bool]] = None,
+                      intervals: Optional[Sequence[Optional[Tuple[float, float]]]] = None,
+                      offset: Optional[Sequence[float]] = None, prior_sigmas: Optional[Sequence[float]] = None,
+                      prior_means: Optional[Sequence[float]] = None, prior_tolog: Optional[Sequence[bool]] = None,
+                      prior_on: Optional[Sequence[bool]] = None):
+        """Installs ProFit's fit space on the model (pf_model_set_fit_space):
+        entries in unlist(modellist) order; tofit True / False / None (R's NA:
+        the value of the entry before); intervals (lo, hi) or None per entry;
+        offset (x, y, ang, size) with NaN for R's NA; normal priors with an
+        infinite sigma for a flat one, on every entry unless prior_on says."""
+        n = len(params)
+        arr, keep = self._refs(params)
+        d = lambda v: np.ascontiguousarray(v, dtype=np.float64)  # noqa: E731
+        ints = lambda v: None if v is None else (C.c_int * n)(*[int(bool(x)) for x in v])  # noqa: E731
+        init_a = d(init)
+        fit_a = (C.c_int * n)(*[-1 if f is None else int(bool(f)) for f in tofit])
+        lo = hi = None
+        if intervals is not None:
+            lo = d([np.nan if iv is None else iv[0] for iv in intervals])
+            hi = d([np.nan if iv is None else iv[1] for iv in intervals])
+        off = None if offset is None else d(offset)
+        sig = None if prior_sigmas is None else d(prior_sigmas)
+        mean = None if prior_means is None else d(prior_means)
+        self._fit_keep = (keep, init_a, lo, hi, off, sig, mean)
+        p = lambda a: None if a is None else a.ctypes.data_as(_capi._dp)  # noqa: E731
+        check(lib().pf_model_set_fit_space(self._h, n, arr, p(init_a), fit_a, ints(tolog), p(lo), p(hi), p(off), p(sig),
+                                           p(mean), ints(prior_tolog), ints(prior_on)))
+
+    def fit_size(self) -> Tuple[int, int]:
+        """(number of fitted entries, number of entries) of the fit space."""
+        nf, ne = C.c_int(), C.c_int()
+        check(lib().pf_model_fit_size(self._h, C.byref(nf), C.byref(ne)))
+        return nf.value, ne.value
+
+    def lp_grad_batch(self, parm: np.ndarray) -> Tuple[np.ndarray, np.ndarray, np.ndarray, np.ndarray]:
+        """LP = LL + log prior, d LP / d parm, parm_out (limits applied, as
+        profitRemakeModellist returns it) and LL for every row of parm[b, j]."""
+        nf, _ = self.fit_size()
+        v = np.ascontiguousarray(parm, dtype=np.float64).reshape(-1, nf)
+        B = v.shape[0]
+        lp = np.zeros(B)
+        g = np.zeros((B, nf))
+        out = np.zeros((B, nf))
+        ll = np.zeros(B)
+        P = _capi._dp
+        check(lib().pf_model_lp_grad_batch(self._h, B, v.ctypes.data_as(P), lp.ctypes.data_as(P), g.ctypes.data_as(P),
+                                           out.ctypes.data_as(P), ll.ctypes.data_as(P)))
+        return lp, g, out, ll
+
     def loglike_grad_fd(self, params: Sequence[Tuple[int, str]], rel_step: float = 1e-6) -> Tuple[float, np.ndarray]:
         """logL and central finite differences of the plain FP64 form."""
         arr, keep = self._refs(params)
