@@ -2,6 +2,7 @@
 // FP64 parity kernels can be compiled without FMA contraction).
 #pragma once
 
+#include <cstddef>
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -41,11 +42,22 @@ cudaError_t launch_downsample64(const double *src, unsigned sw, unsigned sh, uns
                                 unsigned oh, cudaStream_t s);
 
 // render32.cu
-// jac: tangent planes, nt per profile (tangent_stride of the model);
+// Tangent planes of the stored-tangent adjoint, nt per profile
+// (tangent_stride of the model): FP32, or FP64 where a subsampled pixel's
+// cells must be added without FP32 cancellation (tiny, bright profiles).
+struct JacPlanes {
+	void *p = nullptr;
+	bool fp64 = false;
+	JacPlanes() = default;
+	JacPlanes(float *f) : p(f), fp64(false) {}
+	JacPlanes(double *d) : p(d), fp64(true) {}
+	JacPlanes(std::nullptr_t) {}
+};
+// jac: tangent planes (null: values only);
 // all_kinds: the model has radial profiles other than Sersic and Moffat.
 // mask: optional drawing-size calculation mask shared by the batch entries
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
-                            unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
+                            unsigned height, double sx, double sy, float *img_conv, float *img_plain, JacPlanes jac,
                             int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask = nullptr);
 // psf point-source profiles in the FP32 pipeline: the stamp (forward) and the
 // sums of the adjoint image against the stamp and its centre derivatives.
@@ -72,7 +84,7 @@ constexpr int DEEP_ONE_CTA_MAX_CUSPS = 8;
 // cusps: Sersic profiles with adjust across the launch's batch entries (those
 // that may recurse past level 2).
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
-                            float *jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s);
+                            JacPlanes jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s);
 // partials: n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN doubles;
 // tickets: n_profiles zero-initialised counters (left at zero again), one
 // more when grad is given.  grad (optional): the arguments of
@@ -93,7 +105,7 @@ struct GradStepArgs {
 	int ctrl_words = 0;
 };
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles);
-cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
+cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
                               const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
                               unsigned *tickets, double *out, cudaStream_t s, const GradStepArgs *grad = nullptr);
 // Copies `bytes` (a multiple of 16, both addresses 16-byte aligned) from

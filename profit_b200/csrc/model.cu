@@ -2687,7 +2687,7 @@ int cat_build(pf_catalogue *c)
 			while (end < mem.size()) {
 				const int g = mem[end];
 				const int gp = (int)c->gal[g].profiles.size();
-				const size_t b = npix * (8 + 12) + nout * (8 + 4) + (size_t)gp * NTAN * npix * 4;
+				const size_t b = npix * (8 + 12) + nout * (8 + 4) + (size_t)gp * NTAN * npix * sizeof(double);
 				if (end > start && (bytes + b > CAT_BUDGET_BYTES || np + gp > 60000)) break;
 				bytes += b;
 				np += gp;
@@ -2791,7 +2791,7 @@ int cat_build(pf_catalogue *c)
 		conv = std::max(conv, ch.npix() * 4 * C);
 		model = std::max(model, ch.nout() * 8 * C);
 		seed = std::max(seed, ch.nout() * 4 * C);
-		jac = std::max(jac, ch.npix() * (size_t)ch.nt * ch.nprof * 4);
+		jac = std::max(jac, ch.npix() * (size_t)ch.nt * ch.nprof * sizeof(double));
 		parts = std::max(parts, C * NPARTS * sizeof(double2));
 		qpix = std::max(qpix, ch.npix() * C);
 		jp = std::max(jp, (size_t)ch.nprof * jac_reduce_blocks((unsigned)ch.npix(), ch.nprof) * NTAN * 8);
@@ -2834,7 +2834,11 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
 	const size_t npix = ch.npix(), nout = ch.nout();
 	QueueSet q;
 	PF_TRY(prepare_queue(m, a, npix * C, q, nullptr, nullptr, false, true, ch.ak));
-	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>(), *jac = m->d_jac.as<float>();
+	// FP64 tangent planes: catalogue galaxies are often a few pixels across
+	// and bright, so most of their flux sits in subsampled pixels whose cells
+	// cancel in the position and shape tangents
+	float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>();
+	double *jac = m->d_jac.as<double>();
 	float *gconv = m->d_gconv.as<float>(), *gplain = m->d_gplain.as<float>(), *wseed = m->d_wseed.as<float>();
 	double *model64 = m->d_model64.as<double>();
 	const FProfile *fprof = c->fprof.as<FProfile>() + ch.p0;

@@ -477,8 +477,14 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 		d.dlnI_dbox = 1.0 / B + (2.0 / (B * B)) * (digamma(1.0 / B) - digamma(2.0 / B));
 	}
 	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) {
-		const double n = p.nser, h = 1e-6 * n;
-		d.dbn_dn = (qgamma(0.5, 2 * (n + h)) - qgamma(0.5, 2 * (n - h))) / (2 * h);
+		// b_n solves P(2n, b_n) = 1/2, so d b_n / d n = -2 (dP/da) / (dP/dx) at
+		// (a, x) = (2n, b_n): dP/dx is the gamma density, dP/da a central
+		// difference of P at fixed x (two P evaluations instead of two more
+		// quantile solves)
+		const double a = 2 * p.nser, bn = d.bn, h = 1e-6 * a;
+		const double dP_da = (pgamma(bn, a + h) - pgamma(bn, a - h)) / (2 * h);
+		const double dP_dx = exp((a - 1) * log(bn) - bn - lgamma(a));
+		d.dbn_dn = -2 * dP_da / dP_dx;
 	}
 	if (p.kind == PK_SERSIC) {
 		// L = re^2 2 pi n Gamma(2n) e^bn / bn^(2n)

@@ -435,10 +435,12 @@ __device__ __forceinline__ Tan<float> to_float(const Tan<T> &t)
 // pixel of the block would take the zero decision.  mask (optional, one
 // drawing-size calculation mask for every batch entry): pixels where it is 0
 // are not drawn by the radial and sky profiles (radial.cpp:306, sky.cpp:47-63).
-template <bool AK, bool J>
+// JT: element type of the tangent planes (float, or double where the cells
+// of a subsampled pixel must be summed without FP32 cancellation).
+template <bool AK, bool J, class JT>
 __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__restrict__ prof_begin,
                            unsigned width, unsigned height, double sx, double sy, float *__restrict__ img_conv,
-                           float *__restrict__ img_plain, float *__restrict__ jac, int nt, QueueSet q,
+                           float *__restrict__ img_plain, JT *__restrict__ jac, int nt, QueueSet q,
                            const uint8_t *__restrict__ mask)
 {
 	pdl_enter();
@@ -465,8 +467,8 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 		if (!drawn) {
 			if constexpr (J) {
 				if (is_radial_kind(p.kind)) {
-					float *jp = jac + (size_t)pi * nt * npix + pix;
-					for (int k = 0; k < nt; k++) jp[(size_t)k * npix] = 0.f;
+					JT *jp = jac + (size_t)pi * nt * npix + pix;
+					for (int k = 0; k < nt; k++) jp[(size_t)k * npix] = JT(0);
 				}
 			}
 			continue;
@@ -524,10 +526,10 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 			}
 		}
 		if constexpr (J) {
-			float *jp = jac + (size_t)pi * nt * npix + pix;
+			JT *jp = jac + (size_t)pi * nt * npix + pix;
 #pragma unroll
 			for (int k = 0; k < NT; k++)
-				if (k < nt) jp[(size_t)k * npix] = jl[k];
+				if (k < nt) jp[(size_t)k * npix] = (JT)jl[k];
 		}
 	}
 	img_conv[(size_t)b * npix + pix] = acc[0];
@@ -625,10 +627,10 @@ __device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem 
 // this warp's 32 doubles); FP64 sub-points from level 3 on (the Sersic cusp).
 // J: tangents are accumulated into the planes `jac` (false: values only, the
 // tangent arithmetic is compiled out).
-template <bool Deep, bool AK, bool J>
+template <bool Deep, bool AK, bool J, class JT>
 __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profiles, const SubItem &it, int level,
                                              unsigned npix, float *__restrict__ img_conv,
-                                             float *__restrict__ img_plain, float *__restrict__ jac, int nt,
+                                             float *__restrict__ img_plain, JT *__restrict__ jac, int nt,
                                              const QueueSet &q, double *s_xy, int lane, uint32_t *mask_out,
                                              unsigned base0, unsigned base1)
 {
@@ -658,20 +660,23 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 		float *img = p.target == 0 ? img_conv : img_plain;
 		atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)sums[0]));
 		if (J) {
-			float *jp = jac + (size_t)it.profile * nt * npix + pix;
+			JT *jp = jac + (size_t)it.profile * nt * npix + pix;
+			// FP32 planes: the FP32 product; FP64 planes: the cell's sums
+			// enter at full precision (a pixel's cells can cancel)
+			const JT w = sizeof(JT) == 8 ? (JT)it.weight : (JT)wgt;
 #pragma unroll
 			for (int k = 0; k < NT; k++)
-				if (k < nk) atomicAdd(&jp[(size_t)k * npix], wgt * sums[k]);
+				if (k < nk) atomicAdd(&jp[(size_t)k * npix], w * (JT)sums[k]);
 		}
 	}
 	__syncwarp();
 }
 
 // Deep: FP64 sub-points (levels >= 3, the Sersic cusp).
-template <bool AK, bool J, bool Deep>
+template <bool AK, bool J, bool Deep, class JT>
 __global__ void __launch_bounds__(256, Deep ? 2 : (AK ? 3 : 4)) k_level32(const FProfile *__restrict__ profiles, int level, unsigned npix,
                                                  float *__restrict__ img_conv, float *__restrict__ img_plain,
-                                                 float *__restrict__ jac, int nt, QueueSet q)
+                                                 JT *__restrict__ jac, int nt, QueueSet q)
 {
 	pdl_enter();
 	__shared__ double s_xy[8][32];
@@ -698,7 +703,7 @@ __global__ void __launch_bounds__(256, Deep ? 2 : (AK ? 3 : 4)) k_level32(const 
 		const SubItem it = items[item];
 		const unsigned base0 = cpi == 1 ? 0u : chunk * 32, base1 = cpi == 1 ? 256u : base0 + 32;
 		if (base0 >= (unsigned)it.res * it.res) continue;
-		level32_item<Deep, AK, J>(profiles, it, level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
+		level32_item<Deep, AK, J, JT>(profiles, it, level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
 		                    q.masks ? q.masks + ((size_t)q.off[level] + item) * MASK_WORDS : nullptr, base0,
 		                    base1);
 	}
@@ -708,10 +713,10 @@ __global__ void __launch_bounds__(256, Deep ? 2 : (AK ? 3 : 4)) k_level32(const 
 // (max_recursions = 10) reaches these levels, a few hundred cells per level
 // at most, so one block walks them in order; __syncthreads separates the
 // levels, which makes every push of level L visible before level L+1 is read.
-template <bool AK, bool J>
+template <bool AK, bool J, class JT>
 __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restrict__ profiles, int first, int levels,
                                                         unsigned npix, float *__restrict__ img_conv,
-                                                        float *__restrict__ img_plain, float *__restrict__ jac,
+                                                        float *__restrict__ img_plain, JT *__restrict__ jac,
                                                         int nt, QueueSet q)
 {
 	pdl_enter();
@@ -724,7 +729,7 @@ __global__ void __launch_bounds__(512) k_deep_levels32(const FProfile *__restric
 		const uint32_t n = min(*(volatile uint32_t *)&q.counts[level], q.cap[level]);
 		const SubItem *items = q.items + q.off[level];
 		for (uint32_t w = wib; w < n; w += nwarps)
-			level32_item<true, AK, J>(profiles, items[w], level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
+			level32_item<true, AK, J, JT>(profiles, items[w], level, npix, img_conv, img_plain, jac, nt, q, s_xy[wib], lane,
 			                   q.masks ? q.masks + ((size_t)q.off[level] + w) * MASK_WORDS : nullptr, 0, 256);
 	}
 }
@@ -910,8 +915,8 @@ __device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigne
 // its NTAN sums to `partials`; the block that finishes last (an atomic
 // ticket per profile, no waiting) adds the partials in block order and
 // resets the ticket, so the result does not depend on block scheduling.
-template <int NT>
-__global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ jac, const float *__restrict__ g_conv,
+template <int NT, class JT>
+__global__ void __launch_bounds__(256) k_jac_reduce(const JT *__restrict__ jac, const float *__restrict__ g_conv,
                                                     const float *__restrict__ g_plain,
                                                     const FProfile *__restrict__ profiles,
                                                     const int *__restrict__ prof_batch, unsigned npix, int nt,
@@ -930,26 +935,27 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const float *__restrict__ ja
 	const int nk = tangent_count(p.kind);  // <= nt <= NT
 	const int b = prof_batch[pi];
 	const float *g = (p.target == 0 ? g_conv : g_plain) + (size_t)b * npix;
-	const float *jp = jac + (size_t)pi * nt * npix;
+	const JT *jp = jac + (size_t)pi * nt * npix;
 	double acc[NT];
 #pragma unroll
 	for (int k = 0; k < NT; k++) acc[k] = 0.0;
 	const unsigned step = gridDim.x * blockDim.x * U;
 	for (unsigned t0 = blockIdx.x * blockDim.x * U + threadIdx.x; t0 < npix; t0 += step) {
-		float gv[U], jv[U][NT];
+		float gv[U];
+		JT jv[U][NT];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
 			const unsigned t = t0 + u * blockDim.x;
 			const bool in = t < npix;
 			gv[u] = in ? g[t] : 0.f;
 #pragma unroll
-			for (int k = 0; k < NT; k++) jv[u][k] = (in && k < nk) ? jp[(size_t)k * npix + t] : 0.f;
+			for (int k = 0; k < NT; k++) jv[u][k] = (in && k < nk) ? jp[(size_t)k * npix + t] : JT(0);
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++)
 			if (gv[u] != 0.f) {
 #pragma unroll
-				for (int k = 0; k < NT; k++) acc[k] += (double)(gv[u] * jv[u][k]);
+				for (int k = 0; k < NT; k++) acc[k] += (double)gv[u] * (double)jv[u][k];
 			}
 	}
 	__shared__ double s_red[NT][8];
@@ -1056,15 +1062,20 @@ cudaError_t launch_stage_in(void *dst, const void *host_src, size_t bytes, uint3
 }
 
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
-                            unsigned height, double sx, double sy, float *img_conv, float *img_plain, float *jac,
+                            unsigned height, double sx, double sy, float *img_conv, float *img_plain, JacPlanes jac,
                             int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask)
 {
 	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8), batch);
-	auto k = all_kinds ? (jac ? k_pixels32<true, true> : k_pixels32<true, false>)
-	                   : (jac ? k_pixels32<false, true> : k_pixels32<false, false>);
 	note_launches(1);
-	return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, jac, nt,
-	                  q, mask);
+	if (jac.p && jac.fp64) {
+		auto k = all_kinds ? k_pixels32<true, true, double> : k_pixels32<false, true, double>;
+		return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain,
+		                  static_cast<double *>(jac.p), nt, q, mask);
+	}
+	auto k = all_kinds ? (jac.p ? k_pixels32<true, true, float> : k_pixels32<true, false, float>)
+	                   : (jac.p ? k_pixels32<false, true, float> : k_pixels32<false, false, float>);
+	return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain,
+	                  static_cast<float *>(jac.p), nt, q, mask);
 }
 
 // Kind grouping of one wide level's items (models with profiles of every
@@ -1126,8 +1137,9 @@ __global__ void k_kind_scatter(const FProfile *__restrict__ profiles, QueueSet q
 	}
 }
 
-cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
-                            float *jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s)
+template <class JT>
+cudaError_t levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain, JT *jac,
+                     int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s)
 {
 	const int wide = n_levels < 3 ? n_levels : 3;
 	for (int l = 0; l < wide; l++) {
@@ -1139,16 +1151,16 @@ cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npi
 			note_launches(2);
 			if (e != cudaSuccess) return e;
 		}
-		auto k = all_kinds ? (jac ? k_level32<true, true, false> : k_level32<true, false, false>)
-		                   : (jac ? k_level32<false, true, false> : k_level32<false, false, false>);
+		auto k = all_kinds ? (jac ? k_level32<true, true, false, JT> : k_level32<true, false, false, JT>)
+		                   : (jac ? k_level32<false, true, false, JT> : k_level32<false, false, false, JT>);
 		cudaError_t e = launch_pdl(k, dim3(148 * 8), dim3(256), 0, s, profiles, l, npix, img_conv, img_plain, jac, nt, q);
 		if (e != cudaSuccess) return e;
 	}
 	note_launches(wide);
 	if (n_levels > wide && cusps > DEEP_ONE_CTA_MAX_CUSPS) {
 		// many cusps (a large field, a batch): one grid-wide launch per level
-		auto k = all_kinds ? (jac ? k_level32<true, true, true> : k_level32<true, false, true>)
-		                   : (jac ? k_level32<false, true, true> : k_level32<false, false, true>);
+		auto k = all_kinds ? (jac ? k_level32<true, true, true, JT> : k_level32<true, false, true, JT>)
+		                   : (jac ? k_level32<false, true, true, JT> : k_level32<false, false, true, JT>);
 		for (int l = wide; l < n_levels; l++) {
 			cudaError_t e =
 			    launch_pdl(k, dim3(148 * 8), dim3(256), 0, s, profiles, l, npix, img_conv, img_plain, jac, nt, q);
@@ -1157,14 +1169,24 @@ cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npi
 		note_launches(n_levels - wide);
 	}
 	else if (n_levels > wide) {
-		auto k = all_kinds ? (jac ? k_deep_levels32<true, true> : k_deep_levels32<true, false>)
-		                   : (jac ? k_deep_levels32<false, true> : k_deep_levels32<false, false>);
+		auto k = all_kinds ? (jac ? k_deep_levels32<true, true, JT> : k_deep_levels32<true, false, JT>)
+		                   : (jac ? k_deep_levels32<false, true, JT> : k_deep_levels32<false, false, JT>);
 		cudaError_t e = launch_pdl(k, dim3(1), dim3(512), 0, s, profiles, wide, n_levels, npix, img_conv, img_plain, jac,
 		                           nt, q);
 		note_launches(1);
 		if (e != cudaSuccess) return e;
 	}
 	return cudaGetLastError();
+}
+
+cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
+                            JacPlanes jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s)
+{
+	if (jac.p && jac.fp64)
+		return levels32<double>(profiles, n_levels, npix, img_conv, img_plain, static_cast<double *>(jac.p), nt,
+		                        all_kinds, cusps, q, s);
+	return levels32<float>(profiles, n_levels, npix, img_conv, img_plain, static_cast<float *>(jac.p), nt, all_kinds,
+	                       cusps, q, s);
 }
 
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles)
@@ -1175,16 +1197,22 @@ unsigned jac_reduce_blocks(unsigned npix, int n_profiles)
 	return bx < 1 ? 1 : bx;
 }
 
-cudaError_t launch_jac_reduce(const float *jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
+cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
                               const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
                               unsigned *tickets, double *out, cudaStream_t s, const GradStepArgs *grad)
 {
 	const unsigned bx = jac_reduce_blocks(npix, n_profiles);
-	auto k = nt <= 9 ? k_jac_reduce<9> : k_jac_reduce<NTAN>;
 	const GradStepArgs g = grad ? *grad : GradStepArgs{};
+	unsigned *gt = grad ? tickets + n_profiles : (unsigned *)nullptr;
 	note_launches(1);
-	return launch_pdl(k, dim3(bx, n_profiles), dim3(256), 0, s, jac, g_conv, g_plain, profiles, prof_batch, npix, nt,
-	                  partials, tickets, out, g, grad ? tickets + n_profiles : (unsigned *)nullptr);
+	if (jac.fp64) {
+		auto k = nt <= 9 ? k_jac_reduce<9, double> : k_jac_reduce<NTAN, double>;
+		return launch_pdl(k, dim3(bx, n_profiles), dim3(256), 0, s, static_cast<const double *>(jac.p), g_conv, g_plain,
+		                  profiles, prof_batch, npix, nt, partials, tickets, out, g, gt);
+	}
+	auto k = nt <= 9 ? k_jac_reduce<9, float> : k_jac_reduce<NTAN, float>;
+	return launch_pdl(k, dim3(bx, n_profiles), dim3(256), 0, s, static_cast<const float *>(jac.p), g_conv, g_plain,
+	                  profiles, prof_batch, npix, nt, partials, tickets, out, g, gt);
 }
 
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,

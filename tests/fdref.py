@@ -61,10 +61,14 @@ def ref_loglike(wl: Dict, profiles, image: np.ndarray, sigma: np.ndarray, thread
     return loglike_norm(image, sigma, img)
 
 
-def _decision_log(wl: Dict, profiles) -> List[Tuple]:
+def _decision_log(wl: Dict, profiles, only: int = -1) -> List[Tuple]:
     """Per radial profile: (per-pixel decisions, evaluate_at count) of the
     restatement and the PROFIT_DEBUG per-level counts of the reference.
-    Profiles are drawn unconvolved: decisions do not depend on the PSF."""
+    Profiles are drawn unconvolved: decisions do not depend on the PSF.  A
+    profile's decisions depend on its own parameters only, so `only` >= 0
+    draws just that profile."""
+    if only >= 0:
+        profiles = [profiles[only]]
     flat = [(n, {**p, "convolve": False} if n in RADIAL else p) for n, p in profiles]
     ora = OracleModel(wl["width"], wl["height"], threads=_threads())
     ora.set_magzero(wl["magzero"])
@@ -98,7 +102,7 @@ def ref_fd_gradient(wl: Dict, profiles, image: np.ndarray, sigma: np.ndarray,
              "flipped": {step: bool array}} where flipped[step][k] says that
     a decision log at theta +- h differs from the one at theta."""
     ll0 = ref_loglike(wl, profiles, image, sigma)
-    base = _decision_log(wl, profiles) if check_decisions else None
+    base = {}
     grads, flips = {}, {}
     for s in rel_steps:
         g = np.zeros(len(refs))
@@ -109,8 +113,11 @@ def ref_fd_gradient(wl: Dict, profiles, image: np.ndarray, sigma: np.ndarray,
             up = _with(profiles, {pi: {k: v + h}})
             dn = _with(profiles, {pi: {k: v - h}})
             g[j] = (ref_loglike(wl, up, image, sigma) - ref_loglike(wl, dn, image, sigma)) / (2 * h)
-            if check_decisions:
-                f[j] = not (_same_log(_decision_log(wl, up), base) and _same_log(_decision_log(wl, dn), base))
+            if check_decisions and profiles[pi][0] in RADIAL:
+                if pi not in base:
+                    base[pi] = _decision_log(wl, profiles, pi)
+                f[j] = not (_same_log(_decision_log(wl, up, pi), base[pi]) and
+                            _same_log(_decision_log(wl, dn, pi), base[pi]))
         grads[s], flips[s] = g, f
     return {"loglike": ll0, "grad": grads, "flipped": flips}
 
@@ -130,3 +137,16 @@ def closest_error(g_ad: np.ndarray, fd: Dict) -> Tuple[np.ndarray, np.ndarray, n
         best_ref[take] = fd["grad"][s][take]
     usable = np.isfinite(best_err)
     return best_err, best_ref, usable
+
+
+def gradient_errors(g_ad: np.ndarray, fd: Dict) -> Dict:
+    """The errors the FP32 bar is stated in, over the components with a
+    flip-free FD step:
+      own:  |g_ad - g_ref| / |g_ref| per component,
+      norm: ||g_ad - g_ref|| / ||g_ref|| (the vector's relative error),
+      of_norm: |g_ad - g_ref| / ||g_ref|| per component."""
+    err, ref, usable = closest_error(g_ad, fd)
+    e, r = err[usable], ref[usable]
+    nrm = float(np.linalg.norm(r))
+    return {"own": e / np.maximum(np.abs(r), 1e-300), "norm": float(np.linalg.norm(e)) / nrm, "of_norm": e / nrm,
+            "usable": usable, "ref": ref}

@@ -191,7 +191,9 @@ def test_device_fit_space_matches_host_restatement(batch):
     host.set_data(image, sigma)
     for b in range(batch):
         lp_h, g_h, out_h = fs.lp_grad(parm[b], model_loglike_grad(host))
-        assert lp[b] == pytest.approx(lp_h, rel=1e-7)
+        # two FP32 renders add their subsampled cells to the pixels in
+        # different (atomic) orders: at this brightness logL moves by ~1e-7
+        assert lp[b] == pytest.approx(lp_h, rel=1e-6)
         np.testing.assert_allclose(pout[b], out_h, rtol=1e-13, atol=1e-13)
         np.testing.assert_allclose(g[b], g_h, rtol=1e-5, atol=1e-6 * np.max(np.abs(g_h)))
     assert pout[1, ax] == pytest.approx(1.0) and g[1, ax] == 0.0

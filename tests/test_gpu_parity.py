@@ -357,15 +357,18 @@ def test_large_batch_matches_single_proposals():
 
 
 def test_adjoint_gradient_matches_fd64():
+    """The headline model against FD of the plain FP64 form (the compiled
+    reference's FD with decision checks is in test_fp32_bar.py): logL to
+    1e-5, every component to 1e-5 of its own size, the closer of two steps."""
     wl = W.bulge_disk_ps()
     m, w2 = _gradient_case(wl, 0.02)
-    ll_fd, g_fd = m.loglike_grad_fd(w2["grad"], rel_step=1e-6)
+    ll_fd, g7 = m.loglike_grad_fd(w2["grad"], rel_step=1e-7)
+    _, g8 = m.loglike_grad_fd(w2["grad"], rel_step=1e-8)
     m.set_precision(PF_FP32)
     ll_ad, g_ad = m.loglike_grad(w2["grad"])
     assert ll_ad == pytest.approx(ll_fd, rel=1e-5)
-    scale = np.max(np.abs(g_fd))
-    err = np.abs(g_ad - g_fd) / scale
-    assert np.all(err <= 1e-3), list(zip(w2["grad"], g_fd, g_ad))
+    err = np.minimum(np.abs(g_ad - g7), np.abs(g_ad - g8)) / np.abs(g7)
+    assert np.all(err <= 1e-5), list(zip(w2["grad"], g7, g8, g_ad))
 
 
 # One boxy profile of each kind without a closed-form luminosity derivative,
