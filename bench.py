@@ -302,9 +302,15 @@ def main_b200(args):
     m.set_precision(PF_FP32)
     fp64_fd_value = 1e3 / statistics.mean(fd_times)
 
+    # ctypes argument objects built once (a C caller passes plain pointers;
+    # building them per call costs the Python harness ~4 us)
+    vptrs = [v.ctypes.data_as(_capi._dp) for v in pvals]
+    llref = ctypes.byref(ll)
+    nrefs = len(refs)
+
     def step(s):
-        L.pf_model_set_parameters(m._h, arr, len(refs), pvals[s].ctypes.data_as(_capi._dp))
-        st = L.pf_model_loglike_grad(m._h, arr, len(refs), ctypes.byref(ll), gptr)
+        L.pf_model_set_parameters(m._h, arr, nrefs, vptrs[s])
+        st = L.pf_model_loglike_grad(m._h, arr, nrefs, llref, gptr)
         if st != 0:
             raise RuntimeError(L.pf_last_error().decode())
 
@@ -383,14 +389,15 @@ def main_b200(args):
             "roofline": roof,
             "gpu_launches": int(launches),
             "clocks": clk,
-            "accuracy": accuracy,
-            "plain_fp64_fd": {"value": fp64_fd_value, "unit": UNIT,
-                              "speedup_fp32_adjoint": (world * args.steps / dev_total) / fp64_fd_value},
-            "render": render,
-            "convolver_choice": conv_choice,
+            # auxiliary lines first, the headline's accuracy and render work last
             "sampler_batch": sampler,
             "catalogue_batch": catalogue,
             "large_field": large,
+            "convolver_choice": conv_choice,
+            "render": render,
+            "plain_fp64_fd": {"value": fp64_fd_value, "unit": UNIT,
+                              "speedup_fp32_adjoint": (world * args.steps / dev_total) / fp64_fd_value},
+            "accuracy": accuracy,
         }
     m.close()
     if world > 1:
@@ -401,6 +408,47 @@ def main_b200(args):
         print(json.dumps(out), flush=True)
 
 
+# Algorithmic cost of one libprofit profile evaluation (evaluate_at) in the
+# FP32 form, counted from the profile formulas with box = 0 (render32.cu:
+# sersic_tan, moffat_tan, eval_val, tan_to_j): FP32 arithmetic in FLOP (a
+# multiply or add 1, a fused multiply-add 2) and transcendental operations
+# (exp, log, sqrt, reciprocal: one XU operation each; the FMA-pipe polish
+# inside those functions is implementation, not counted).  A "tangent"
+# evaluation is the value plus every parameter tangent and its accumulation
+# into the nine tangent sums (coordinates 6 FLOP, accumulation 21 FLOP); a
+# "test" evaluation is libprofit's second point of a sub-pixel that may still
+# recurse (value only, plus the acceptance test).
+RENDER_COST = {  # kind: {"tangent": (FLOP, XU), "test": (FLOP, XU)}
+    "sersic": {"tangent": (62, 7), "test": (12, 3)},
+    "moffat": {"tangent": (59, 8), "test": (11, 3)},
+}
+
+
+def render_work(wl, counts_per_level, max_rec=2):
+    """(FLOP, XU ops) of one evaluation of the workload's radial profiles:
+    direct pixels and sub-points of the last level are tangent evaluations;
+    at a level below max_recursions (2) each sub-point is a tangent and a test
+    evaluation (libprofit counts both).  The Sersic centre cusp recurses past
+    level 2 at a handful of cells; those are counted as tangent evaluations."""
+    flop = xu = 0.0
+    for (kind, params), per in zip(wl["profiles"], counts_per_level):
+        cost = RENDER_COST.get(kind)
+        if cost is None or params.get("box", 0.0) != 0.0 or not per:
+            continue
+        tf, tx = cost["tangent"]
+        sf, sx = cost["test"]
+        flop += per[0] * tf
+        xu += per[0] * tx
+        for lvl, n in enumerate(per[1:]):
+            if lvl < max_rec:
+                flop += n / 2 * (tf + sf)
+                xu += n / 2 * (tx + sx)
+            else:
+                flop += n * tf
+                xu += n * tx
+    return flop, xu
+
+
 def render_rate(wl, image, sigma, refs, pvals, steps=20):
     """Render work of the headline evaluation, outside the timed region:
     libprofit's evaluate_at calls for the first proposal (direct pixels plus
@@ -408,8 +456,10 @@ def render_rate(wl, image, sigma, refs, pvals, steps=20):
     decisions are the reference's pixel for pixel), over the render phase of
     the FP32 LL+grad pipeline (CUDA events around the pixel and level kernels,
     median over proposals; each evaluation there also forms the profile's
-    parameter tangents).  The render is compute bound and its working set is
-    in L2 either way, so no flush here."""
+    parameter tangents).  The roofline: the FP32 FLOP and transcendental (XU)
+    operations those evaluations need (RENDER_COST) at the measured FP32 FMA
+    and XU peaks of this GPU; the slower pipe sets the time.  The render is
+    compute bound and its working set is in L2 either way, so no flush here."""
     from profit_b200 import PF_FP32, Model
     from profit_b200 import workloads as W
     try:
@@ -417,7 +467,7 @@ def render_rate(wl, image, sigma, refs, pvals, steps=20):
         m.set_parameters(refs, pvals[0])
         m.set_debug(True)
         m.evaluate()
-        counts = [m.evaluation_counts(i)[0] for i in range(len(wl["profiles"]))]
+        counts = [m.evaluation_counts(i) for i in range(len(wl["profiles"]))]
         m.set_debug(False)
         m.set_precision(PF_FP32)
         m.set_data(image, sigma)
@@ -430,13 +480,27 @@ def render_rate(wl, image, sigma, refs, pvals, steps=20):
         m.close()
     except Exception as e:  # an auxiliary figure: report, never lose the bench line
         return {"error": str(e)}
-    n_eval = int(sum(counts))
+    n_eval = int(sum(c[0] for c in counts))
     render_ms = statistics.median(ts)
-    return {"evaluations": n_eval, "per_profile": [int(c) for c in counts], "render_ms": render_ms,
-            "evaluations_per_s": n_eval / (render_ms / 1e3),
-            "definition": "evaluate_at calls of the first proposal (plain FP64 debug counters) over the "
-                          "FP32 render phase (value + parameter tangents per evaluation), median of "
-                          f"{steps} proposals; pipe utilisation in profiles/render_bulge_disk_ps.txt"}
+    flop, xu = render_work(wl, [c[1] for c in counts])
+    fp32 = measured_peak(0)   # plain FP32 FMA, TFLOP/s (the render's arithmetic is not packed)
+    xu_peak = measured_peak(3)  # Tops/s
+    t = render_ms / 1e3
+    out = {"evaluations": n_eval, "per_profile": [int(c[0]) for c in counts],
+           "per_level": [c[1] for c in counts], "render_ms": render_ms,
+           "evaluations_per_s": n_eval / t,
+           "definition": "evaluate_at calls of the first proposal (plain FP64 debug counters) over the "
+                         f"FP32 render phase (value + parameter tangents per evaluation), median of {steps} "
+                         "proposals"}
+    if fp32 and xu_peak:
+        t_fma, t_xu = flop / (fp32 * 1e12), xu / (xu_peak * 1e12)
+        out["roofline"] = {
+            "flop": flop, "xu_ops": xu, "fp32_tflops": flop / t / 1e12, "xu_tops": xu / t / 1e12,
+            "peak_fp32_tflops": fp32, "peak_xu_tops": xu_peak, "bound": "xu" if t_xu > t_fma else "fp32",
+            "frac": max(t_fma, t_xu) / t,
+            "cost": "RENDER_COST per evaluation (FLOP, XU) from the profile formulas; peaks measured on this GPU "
+                    "(libpf_peaks.so: FP32 FMA chains, fast-exponential chains)"}
+    return out
 
 
 def convolver_choice_rate(torch, flush, wl, image, sigma, refs, pvals, steps=30):
@@ -654,17 +718,32 @@ def catalogue_rate(args, torch, flush, n=10000, calls=2, fd_sample=6):
             "finite_fraction": float(np.isfinite(ll).mean())}
 
 
+_PEAKS = {}
+
+
+def measured_peak(kind):
+    """Peak of this GPU from libpf_peaks.so (best of 5): 0 FP32 FMA, 1 FP64
+    FMA, 2 packed FP32 FMA (TFLOP/s), 3 transcendental XU operations
+    (Tops/s); None if the probe is unavailable."""
+    if kind not in _PEAKS:
+        path = os.path.join(ROOT, "profit_b200", "lib", "libpf_peaks.so")
+        try:
+            lib = ctypes.CDLL(path)
+            lib.pf_peak_fma_tflops.restype = ctypes.c_double
+            lib.pf_peak_fma_tflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
+            v = lib.pf_peak_fma_tflops(kind, 4096, 5)
+            _PEAKS[kind] = v if v > 0 else None
+        except OSError:
+            _PEAKS[kind] = None
+    return _PEAKS[kind]
+
+
 def measured_fp32_peak():
-    path = os.path.join(ROOT, "profit_b200", "lib", "libpf_peaks.so")
-    try:
-        lib = ctypes.CDLL(path)
-        lib.pf_peak_fma_tflops.restype = ctypes.c_double
-        lib.pf_peak_fma_tflops.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int]
-        # the FP32 ceiling: plain FMA and packed FP32-pair FMA, whichever is higher
-        v = max(lib.pf_peak_fma_tflops(0, 4096, 5), lib.pf_peak_fma_tflops(2, 4096, 5))
-        return v if v > 0 else None
-    except OSError:
-        return None
+    """The FP32 ceiling of the convolution: plain FMA and packed FP32-pair
+    FMA, whichever is higher."""
+    a, b = measured_peak(0), measured_peak(2)
+    vals = [v for v in (a, b) if v]
+    return max(vals) if vals else None
 
 
 def recorded_traffic():

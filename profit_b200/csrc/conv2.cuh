@@ -118,16 +118,33 @@ __device__ __forceinline__ void conv3_tail(float2 (&win)[RY + 2], float2 (&acc)[
 	}
 }
 
+// All KHC taps of a kernel column with the window ring at compile-time
+// positions (tap L uses ring slots (L + r) % (RY + 2)): no loop and no tail.
+template <int RY, int L, int KHC>
+__device__ __forceinline__ void conv3_column(float2 (&win)[RY + 2], float2 (&acc)[RY], const float2 *col,
+                                             const float4 *kc)
+{
+	if constexpr (L < KHC) {
+		const float4 c2 = kc[L >> 1];
+		conv3_tap<RY, L>(win, acc, col, make_float2(c2.x, c2.y));
+		if constexpr (L + 1 < KHC) conv3_tap<RY, L + 1>(win, acc, col, make_float2(c2.z, c2.w));
+		conv3_column<RY, L + 2, KHC>(win, acc, col, kc);
+	}
+}
+
 // TOut: output type (FP32 adjoint image or FP64 model image).  `part` is the
-// FP64 scratch [batch][KSPLIT][oh][ow] used when KSPLIT > 1.
-template <class TOut, int HL, int RY, int TYT, int KS, int KSPLIT>
+// FP64 scratch [batch][KSPLIT][oh][ow] used when KSPLIT > 1.  KHC > 0: the
+// kernel height fixed at compile time (launches with another height are not
+// applicable), the taps of a column fully unrolled.
+template <class TOut, int HL, int RY, int TYT, int KS, int KSPLIT, int KHC = 0>
 __global__ void __launch_bounds__(32 * TYT * KS)
     k_conv3_tile(const float *__restrict__ src, int sw, int sh, int ox, int oy, const float *__restrict__ K, int kw,
-                 int kh, TOut *__restrict__ out, int ow, int oh, const float *__restrict__ add, int add_stride,
+                 int kh_arg, TOut *__restrict__ out, int ow, int oh, const float *__restrict__ add, int add_stride,
                  int add_ox, int add_oy, int batch_src_stride, int batch_out_stride, int batch_k_stride,
                  double *__restrict__ part)
 {
 	using S = Conv3Shape<HL, RY, TYT, KS, KSPLIT>;
+	const int kh = KHC > 0 ? KHC : kh_arg;
 	static_assert(RY % 2 == 0, "taps are consumed in pairs");
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const int khp = S::khp(kh), thp = S::thp(kh);
@@ -191,9 +208,14 @@ __global__ void __launch_bounds__(32 * TYT * KS)
 		for (int r = 0; r < RY; r++) acc[r] = make_float2(0.0f, 0.0f);
 #pragma unroll
 		for (int r = 0; r < RY + 1; r++) win[r] = col[r];
-		int l = 0;
-		for (; l + WR <= kh; l += WR) conv3_steps<RY, 0>(win, acc, col + l, kc + (l >> 1));
-		conv3_tail<RY, 0>(win, acc, col + l, kc + (l >> 1), kh - l);
+		if constexpr (KHC > 0) {
+			conv3_column<RY, 0, KHC>(win, acc, col, kc);
+		}
+		else {
+			int l = 0;
+			for (; l + WR <= kh; l += WR) conv3_steps<RY, 0>(win, acc, col + l, kc + (l >> 1));
+			conv3_tail<RY, 0>(win, acc, col + l, kc + (l >> 1), kh - l);
+		}
 #pragma unroll
 		for (int r = 0; r < RY; r++) {
 			tot[r].x += (double)acc[r].x;
@@ -271,12 +293,14 @@ __global__ void k_conv_split_sum(const double *__restrict__ part, int ksplit, TO
 	}
 }
 
-template <class TOut, int HL, int RY, int TYT, int KS, int KSPLIT>
+template <class TOut, int HL, int RY, int TYT, int KS, int KSPLIT, int KHC = 0>
 struct Conv3Variant {
 	using S = Conv3Shape<HL, RY, TYT, KS, KSPLIT>;
-	static size_t smem(int kw, int kh) { return S::smem(kw, kh); }
+	// a fixed-height variant does not apply to other kernel heights
+	static size_t smem(int kw, int kh) { return (KHC > 0 && kh != KHC) ? ~(size_t)0 >> 1 : S::smem(kw, kh); }
 	static cudaError_t run(const ConvArgs &a, cudaStream_t s)
 	{
+		if (KHC > 0 && a.kh != KHC) return cudaErrorInvalidValue;
 		if (KSPLIT > 1 && (!a.scratch || a.scratch_bytes < (size_t)a.batch * KSPLIT * a.ow * a.oh * sizeof(double)))
 			return cudaErrorInvalidValue;  // not applicable without scratch
 		if (KSPLIT > a.kw) return cudaErrorInvalidValue;
@@ -284,7 +308,7 @@ struct Conv3Variant {
 		if (smem > 227 * 1024) return cudaErrorInvalidValue;
 		static bool configured = false;
 		if (!configured) {
-			cudaError_t e = cudaFuncSetAttribute(k_conv3_tile<TOut, HL, RY, TYT, KS, KSPLIT>,
+			cudaError_t e = cudaFuncSetAttribute(k_conv3_tile<TOut, HL, RY, TYT, KS, KSPLIT, KHC>,
 			                                     cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
 			if (e != cudaSuccess) return e;
 			configured = true;
@@ -292,7 +316,7 @@ struct Conv3Variant {
 		dim3 block(32, TYT, KS);
 		dim3 grid((a.ow + S::TX - 1) / S::TX, (a.oh + S::TY - 1) / S::TY, a.batch * KSPLIT);
 		cudaError_t e = launch_pdl(
-		    k_conv3_tile<TOut, HL, RY, TYT, KS, KSPLIT>, grid, block, smem, s, static_cast<const float *>(a.src), a.sw,
+		    k_conv3_tile<TOut, HL, RY, TYT, KS, KSPLIT, KHC>, grid, block, smem, s, static_cast<const float *>(a.src), a.sw,
 		    a.sh, a.ox, a.oy, static_cast<const float *>(a.K), a.kw, a.kh, static_cast<TOut *>(a.out), a.ow, a.oh,
 		    static_cast<const float *>(a.add), a.add_stride, a.add_ox, a.add_oy, a.batch_src_stride,
 		    a.batch_out_stride, a.batch_k_stride, static_cast<double *>(a.scratch));

@@ -171,8 +171,10 @@ cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_b
 namespace pf {
 // render32.cu: catalogue batches (each entry with its own profiles)
 // pad: per profile, the drawing offset (PSF padding) of its bucket
+// lum (optional, n * LUM_SLOTS doubles of scratch): the QUADPACK
+// luminosities run first, one thread per evaluation (k_cat_lum)
 cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, int n, const ModelGeom &g,
-                                DevProfile *dev, FProfile *fprof, cudaStream_t s);
+                                double *lum, DevProfile *dev, FProfile *fprof, cudaStream_t s);
 cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,
                                 cudaStream_t s);
 }  // namespace pf

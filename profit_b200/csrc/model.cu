@@ -18,6 +18,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <tuple>
 #include <string>
 #include <vector>
@@ -56,6 +57,47 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 		if (it != choice.end()) pick = it->second;
 	}
 	if (pick < 0) {
+		// A shape close to one already tuned (same direction, kernel sides in
+		// the same 8-pixel class, the same power of two in output width and
+		// in total output pixels) takes that choice: a catalogue brings
+		// hundreds of chunk shapes that differ in canvas side, PSF size and
+		// galaxy count, and timing every candidate for each one made its
+		// first call last seconds.
+		auto lg2 = [](long long v) {
+			int r = 0;
+			while (v > 1) {
+				v >>= 1;
+				r++;
+			}
+			return r;
+		};
+		const int wc = lg2(a.ow), nc = lg2((long long)a.ow * a.oh * a.batch);
+		int near = -1;
+		{
+			std::lock_guard<std::mutex> g(mu);
+			for (const auto &kv : choice) {
+				const Key &k = kv.first;
+				if (std::get<0>(k) == type_tag && std::get<3>(k) / 8 == a.kw / 8 && std::get<4>(k) / 8 == a.kh / 8 &&
+				    lg2(std::get<5>(k)) == wc &&
+				    lg2((long long)std::get<5>(k) * std::get<6>(k) * std::get<7>(k)) == nc) {
+					near = kv.second;
+					break;
+				}
+			}
+		}
+		if (near >= 0 && cands[near].smem(a.kw, a.kh) <= 227 * 1024) {
+			cudaError_t e = cands[near].run(a, s);
+			if (e != cudaErrorInvalidValue) {
+				if (e == cudaSuccess) {
+					std::lock_guard<std::mutex> g(mu);
+					choice[key] = near;
+				}
+				return e;
+			}
+			cudaGetLastError();  // not applicable to this shape (scratch): tune it
+		}
+	}
+	if (pick < 0) {
 		cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
 		cudaStreamIsCapturing(s, &cap);
 		int first_fit = -1;
@@ -80,12 +122,15 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 				if (!cands[c].tuned || cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
 				cudaError_t e = cands[c].run(a, s);  // warm-up (and attribute setup)
 				if (e != cudaSuccess) continue;
+				// batched shapes run long enough to be timed once
+				const int reps = a.batch > 8 ? 1 : 3;
 				cudaEventRecord(e0, s);
-				for (int r = 0; r < 3; r++) cands[c].run(a, s);
+				for (int r = 0; r < reps; r++) cands[c].run(a, s);
 				cudaEventRecord(e1, s);
 				if (cudaEventSynchronize(e1) != cudaSuccess) break;
 				float ms = 0;
 				cudaEventElapsedTime(&ms, e0, e1);
+				ms *= 3.0f / reps;
 				if (log)
 					fprintf(stderr, "[profit_b200 autotune] type %d src %dx%d psf %dx%d out %dx%d batch %d: candidate %d %.4f ms\n",
 					        type_tag, a.sw, a.sh, a.kw, a.kh, a.ow, a.oh, a.batch, c, ms / 3);
@@ -2611,11 +2656,17 @@ struct pf_catalogue {
 	bool built = false;
 	std::vector<std::unique_ptr<CatChunk>> chunks;
 	DevBuf params, pad, dev, fprof;  // every profile of the catalogue, chunk after chunk
+	DevBuf lum;                       // LUM_SLOTS luminosity evaluations per profile (prologue scratch)
 	int nprof = 0;
 	std::vector<int> grad_off;
 	int grad_total = 0;
 	float last_ms = 0;
 	cudaEvent_t ev[2] = {};
+	// the whole call (prologue and every chunk) captured once and replayed
+	// while the queue capacities it was captured with hold
+	cudaGraphExec_t graph = nullptr;
+	std::vector<uint32_t> graph_caps;
+	unsigned long long graph_kernels = 0;
 };
 
 namespace {
@@ -2653,6 +2704,9 @@ Analysis cat_analysis(const CatChunk &ch)
 // Groups galaxies into chunks and uploads the static inputs.
 int cat_build(pf_catalogue *c)
 {
+	// the chunks and their buffers are rebuilt: a recorded call no longer applies
+	if (c->graph) cudaGraphExecDestroy(c->graph);
+	c->graph = nullptr;
 	// gradient layout: per galaxy, per profile (xcen, ycen, mag, ang, axrat, box, shape...)
 	c->grad_off.assign(c->gal.size(), 0);
 	int total = 0;
@@ -2703,17 +2757,14 @@ int cat_build(pf_catalogue *c)
 			c->chunks.push_back(std::move(ch));
 		}
 	}
-	// static inputs
+	// static inputs: profile records and per-chunk index tables (serial,
+	// cheap), then every chunk's images (below, in parallel)
 	std::vector<ProfileParams> params;
 	std::vector<int2> pad;
 	for (auto &chp : c->chunks) {
 		CatChunk &ch = *chp;
 		const int C = (int)ch.members.size();
-		const size_t nout = ch.nout(), nk = (size_t)ch.pw * ch.ph;
 		std::vector<int> prof_begin(C + 1, 0), prof_batch, goff;
-		std::vector<double> data(nout * C, 0.0), sigma(nout * C, 1.0);
-		std::vector<uint8_t> region(nout * C, 0);
-		std::vector<float> psf(nk * C), psfrev(nk * C);
 		ch.member_grad_off.assign(C, 0);
 		ch.p0 = (int)params.size();
 		int gtot = 0;
@@ -2737,17 +2788,6 @@ int cat_build(pf_catalogue *c)
 				if (!p.convolve) ch.plain = true;
 			}
 			prof_begin[i + 1] = (int)params.size() - ch.p0;
-			for (unsigned y = 0; y < G.h; y++)
-				for (unsigned x = 0; x < G.w; x++) {
-					const size_t o = (size_t)i * nout + x + (size_t)y * ch.W;
-					data[o] = G.data[x + (size_t)y * G.w];
-					sigma[o] = G.sigma[x + (size_t)y * G.w];
-					region[o] = 1;
-				}
-			for (size_t k = 0; k < nk; k++) {
-				psf[(size_t)i * nk + k] = (float)G.psf[k];
-				psfrev[(size_t)i * nk + k] = (float)G.psf[nk - 1 - k];
-			}
 		}
 		ch.nprof = (int)params.size() - ch.p0;
 		ch.ngrad = gtot;
@@ -2759,17 +2799,75 @@ int cat_build(pf_catalogue *c)
 		PF_TRY(up(ch.prof_begin, prof_begin.data(), prof_begin.size() * 4));
 		PF_TRY(up(ch.prof_batch, prof_batch.data(), prof_batch.size() * 4));
 		PF_TRY(up(ch.grad_off, goff.data(), goff.size() * 4));
-		PF_TRY(up(ch.data, data.data(), data.size() * 8));
-		PF_TRY(up(ch.sigma, sigma.data(), sigma.size() * 8));
-		PF_TRY(up(ch.region, region.data(), region.size()));
-		PF_TRY(up(ch.psf32, psf.data(), psf.size() * 4));
-		PF_TRY(up(ch.psfrev32, psfrev.data(), psfrev.size() * 4));
 		PF_CUDA(ensure(ch.T, (size_t)ch.nprof * NTAN * 8));
 		PF_CUDA(ensure(ch.ll, (size_t)C * 8));
 		PF_CUDA(ensure(ch.grad, (size_t)std::max(gtot, 1) * 8));
 		PF_CUDA(ensure(ch.h_ll, (size_t)C * 8));
 		PF_CUDA(ensure(ch.h_grad, (size_t)std::max(gtot, 1) * 8));
 		PF_CUDA(ensure(ch.h_ctrl, CTRL_WORDS * 4));
+	}
+	// Each chunk's data, sigma and region canvases: cleared on the device,
+	// every galaxy's rows copied straight into its slot (the canvas beyond a
+	// galaxy keeps region 0, so its sigma there is never read), PSFs and
+	// their reversals packed per chunk.  Chunks are independent: host
+	// threads take them in turn.
+	{
+		const int dev = c->engine->device;
+		std::atomic<size_t> next{0};
+		std::atomic<int> status{PF_OK};
+		std::mutex err_mu;
+		std::string err_msg;
+		auto worker = [&]() {
+			if (cudaSetDevice(dev) != cudaSuccess) {
+				status = PF_E_CUDA;
+				return;
+			}
+			for (size_t k = next++; k < c->chunks.size() && status == PF_OK; k = next++) {
+				CatChunk &ch = *c->chunks[k];
+				const int C = (int)ch.members.size();
+				const size_t nout = ch.nout(), nk = (size_t)ch.pw * ch.ph;
+				std::vector<float> psf(nk * C), psfrev(nk * C);
+				cudaError_t e = ensure(ch.data, nout * C * 8);
+				if (e == cudaSuccess) e = ensure(ch.sigma, nout * C * 8);
+				if (e == cudaSuccess) e = ensure(ch.region, nout * C);
+				if (e == cudaSuccess) e = cudaMemset(ch.data.p, 0, nout * C * 8);
+				if (e == cudaSuccess) e = cudaMemset(ch.sigma.p, 0, nout * C * 8);
+				if (e == cudaSuccess) e = cudaMemset(ch.region.p, 0, nout * C);
+				for (int i = 0; i < C && e == cudaSuccess; i++) {
+					const CatGalaxy &G = c->gal[ch.members[i]];
+					const size_t o = (size_t)i * nout;
+					e = cudaMemcpy2D(ch.data.as<double>() + o, (size_t)ch.W * 8, G.data.data(), (size_t)G.w * 8,
+					                 (size_t)G.w * 8, G.h, cudaMemcpyHostToDevice);
+					if (e == cudaSuccess)
+						e = cudaMemcpy2D(ch.sigma.as<double>() + o, (size_t)ch.W * 8, G.sigma.data(), (size_t)G.w * 8,
+						                 (size_t)G.w * 8, G.h, cudaMemcpyHostToDevice);
+					if (e == cudaSuccess) e = cudaMemset2D(ch.region.as<uint8_t>() + o, ch.W, 1, G.w, G.h);
+					for (size_t q = 0; q < nk; q++) {
+						psf[(size_t)i * nk + q] = (float)G.psf[q];
+						psfrev[(size_t)i * nk + q] = (float)G.psf[nk - 1 - q];
+					}
+				}
+				if (e == cudaSuccess) e = ensure(ch.psf32, psf.size() * 4);
+				if (e == cudaSuccess) e = cudaMemcpy(ch.psf32.p, psf.data(), psf.size() * 4, cudaMemcpyHostToDevice);
+				if (e == cudaSuccess) e = ensure(ch.psfrev32, psfrev.size() * 4);
+				if (e == cudaSuccess)
+					e = cudaMemcpy(ch.psfrev32.p, psfrev.data(), psfrev.size() * 4, cudaMemcpyHostToDevice);
+				if (e != cudaSuccess) {
+					std::lock_guard<std::mutex> g(err_mu);
+					err_msg = cudaGetErrorString(e);
+					status = PF_E_CUDA;
+				}
+			}
+		};
+		const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+		const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, 8), c->chunks.size());
+		std::vector<std::thread> pool;
+		for (size_t t = 1; t < nthreads; t++) pool.emplace_back(worker);
+		worker();
+		for (auto &t : pool) t.join();
+		if (status != PF_OK) return set_error(PF_E_CUDA, "catalogue inputs: " + err_msg);
+		// the clears and copies ran on the legacy default stream of each thread
+		PF_CUDA(cudaDeviceSynchronize());
 	}
 	c->nprof = (int)params.size();
 	PF_CUDA(ensure(c->params, params.size() * sizeof(ProfileParams)));
@@ -2778,6 +2876,7 @@ int cat_build(pf_catalogue *c)
 	PF_CUDA(cudaMemcpy(c->pad.p, pad.data(), pad.size() * sizeof(int2), cudaMemcpyHostToDevice));
 	PF_CUDA(ensure(c->dev, params.size() * sizeof(DevProfile)));
 	PF_CUDA(ensure(c->fprof, params.size() * sizeof(FProfile)));
+	PF_CUDA(ensure(c->lum, params.size() * LUM_SLOTS * sizeof(double)));
 
 	// engine scratch and queue for the largest chunk, so nothing is
 	// reallocated while chunks are queued
@@ -2890,6 +2989,7 @@ int pf_catalogue_create(pf_catalogue **out)
 int pf_catalogue_destroy(pf_catalogue *c)
 {
 	if (!c) return PF_OK;
+	if (c->graph) cudaGraphExecDestroy(c->graph);
 	c->chunks.clear();
 	for (auto &e : c->ev)
 		if (e) cudaEventDestroy(e);
@@ -2996,12 +3096,27 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 	g.sx = g.sy = g.img_sx = g.img_sy = 1;
 	g.offx = g.offy = 0;
 	g.finesampling = 1;
-	PF_CUDA(launch_cat_prologue(c->params.as<ProfileParams>(), c->pad.as<int2>(), c->nprof, g,
-	                            c->dev.as<DevProfile>(), c->fprof.as<FProfile>(), s));
+	auto enqueue_all = [&]() -> int {
+		PF_CUDA(launch_cat_prologue(c->params.as<ProfileParams>(), c->pad.as<int2>(), c->nprof, g,
+		                            c->lum.as<double>(), c->dev.as<DevProfile>(), c->fprof.as<FProfile>(), s));
+		for (auto &chp : c->chunks) PF_TRY(cat_enqueue_chunk(c, *chp));
+		return PF_OK;
+	};
 	std::vector<CatChunk *> todo;
 	for (auto &chp : c->chunks) todo.push_back(chp.get());
+	const bool replay = c->graph && c->graph_caps == m->caps;
+	bool retried = false;
 	for (int attempt = 0; attempt < 8 && !todo.empty(); attempt++) {
-		for (CatChunk *ch : todo) PF_TRY(cat_enqueue_chunk(c, *ch));
+		if (attempt == 0 && replay) {
+			PF_CUDA(cudaGraphLaunch(c->graph, s));
+			note_launches((int)c->graph_kernels);
+		}
+		else if (attempt == 0) {
+			PF_TRY(enqueue_all());
+		}
+		else {
+			for (CatChunk *ch : todo) PF_TRY(cat_enqueue_chunk(c, *ch));
+		}
 		PF_CUDA(cudaStreamSynchronize(s));
 		// every chunk is judged against the capacities it ran with; only then
 		// do the capacities grow (one chunk's growth must not hide another's
@@ -3021,9 +3136,33 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 				}
 			if (over) again.push_back(ch);
 		}
+		if (!again.empty()) retried = true;
 		todo.swap(again);
 	}
 	if (!todo.empty()) return set_error(PF_E_CAPACITY, "subsampling work queue kept overflowing");
+	if (retried && c->graph) {
+		cudaGraphExecDestroy(c->graph);  // captured with capacities that no longer hold
+		c->graph = nullptr;
+	}
+	if (!replay && !retried && m->use_graphs) {
+		// record the call that just ran (every choice it made is cached now)
+		// for the next calls; nothing runs during the capture
+		if (c->graph) cudaGraphExecDestroy(c->graph);
+		c->graph = nullptr;
+		const unsigned long long before = g_launches.load();
+		cudaGraph_t graph = nullptr;
+		PF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+		const int st = enqueue_all();
+		const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+		c->graph_kernels = g_launches.load() - before;
+		g_launches -= c->graph_kernels;
+		if (st == PF_OK && ce == cudaSuccess && graph && cudaGraphInstantiate(&c->graph, graph, 0) == cudaSuccess)
+			c->graph_caps = m->caps;
+		else
+			c->graph = nullptr;
+		if (graph) cudaGraphDestroy(graph);
+		cudaGetLastError();
+	}
 	PF_CUDA(cudaEventRecord(c->ev[1], s));
 	PF_CUDA(cudaEventSynchronize(c->ev[1]));
 	for (auto &chp : c->chunks) {

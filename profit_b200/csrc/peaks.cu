@@ -50,6 +50,56 @@ __global__ void k_fma2(float *out, int iters, float a, float b)
 	out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
+// Transcendental (XU / MUFU) throughput: 8 independent chains of the fast
+// exponential per thread (one XU operation and one multiply per step); the
+// result is XU operations per second.
+__global__ void k_xu(float *out, int iters, float a)
+{
+	float t = threadIdx.x * 1e-6f;
+	float x0 = t, x1 = t + 1e-3f, x2 = t + 2e-3f, x3 = t + 3e-3f, x4 = t + 4e-3f, x5 = t + 5e-3f, x6 = t + 6e-3f,
+	      x7 = t + 7e-3f;
+	for (int i = 0; i < iters; i++) {
+		x0 = __expf(x0 * a);
+		x1 = __expf(x1 * a);
+		x2 = __expf(x2 * a);
+		x3 = __expf(x3 * a);
+		x4 = __expf(x4 * a);
+		x5 = __expf(x5 * a);
+		x6 = __expf(x6 * a);
+		x7 = __expf(x7 * a);
+	}
+	out[blockIdx.x * blockDim.x + threadIdx.x] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
+double run_xu(int iters, int reps)
+{
+	int dev = 0, sms = 0;
+	cudaGetDevice(&dev);
+	cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+	const int threads = 256, blocks = sms * 4;
+	float *out = nullptr;
+	if (cudaMalloc(&out, sizeof(float) * threads * blocks) != cudaSuccess) return -1;
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	k_xu<<<blocks, threads>>>(out, iters, -0.5f);
+	float best = 1e30f;
+	for (int r = 0; r < reps; r++) {
+		cudaEventRecord(e0);
+		k_xu<<<blocks, threads>>>(out, iters, -0.5f);
+		cudaEventRecord(e1);
+		cudaEventSynchronize(e1);
+		float ms = 0;
+		cudaEventElapsedTime(&ms, e0, e1);
+		if (ms < best) best = ms;
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	cudaFree(out);
+	if (cudaGetLastError() != cudaSuccess) return -1;
+	return 8.0 * iters * threads * (double)blocks / (best * 1e-3) / 1e12;
+}
+
 template <class T, bool Packed = false>
 double run(int iters, int reps)
 {
@@ -92,9 +142,11 @@ double run(int iters, int reps)
 extern "C" {
 
 // TFLOP/s of dependent-chain FMA streams, best of `reps` launches.
-// kind: 0 = FP32 FMA, 1 = FP64 FMA, 2 = packed FP32 pairs (FFMA2).
+// kind: 0 = FP32 FMA, 1 = FP64 FMA, 2 = packed FP32 pairs (FFMA2),
+// 3 = transcendental (XU) operations in Tops/s (fast exponentials).
 double pf_peak_fma_tflops(int kind, int iters, int reps)
 {
+	if (kind == 3) return run_xu(iters, reps);
 	if (kind == 1) return run<double>(iters, reps);
 	if (kind == 2) return run<float, true>(iters, reps);
 	return run<float>(iters, reps);

@@ -314,7 +314,38 @@ PF_HD inline double *shape_param(ProfileParams &p, int k)
 	}
 }
 
-PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, DevProfile &d)
+// Kinds whose luminosity has no closed-form derivative here: the prologue
+// takes central differences of the luminosity (Beta function or QUADPACK) in
+// each shape parameter.
+PF_HD inline bool lum_by_difference(int kind)
+{
+	return kind == PK_FERRER || kind == PK_CORESERSIC || kind == PK_KING || kind == PK_BROKENEXP;
+}
+
+// Luminosity evaluations of such a profile: slot 0 the profile's own, slots
+// 1 + 2k and 2 + 2k the shape parameter k moved by +h and -h.
+constexpr int LUM_SLOTS = 1 + 2 * MAX_SHAPE;
+PF_HD inline int lum_slots(int kind) { return lum_by_difference(kind) ? 1 + 2 * shape_count(kind) : 0; }
+
+// Luminosity evaluation `slot` of profile p (a lum_by_difference kind); the
+// QUADPACK ones are independent, so a batch prologue can run them in
+// parallel and hand the values to derive_profile.
+PF_HD inline double lum_slot(const ProfileParams &p, int slot)
+{
+	ProfileParams q = p;
+	if (slot > 0) {
+		double *v = shape_param(q, (slot - 1) / 2);
+		const double v0 = *v, h = 1e-6 * fabs(v0) + 1e-9;
+		*v = (slot & 1) ? v0 + h : v0 - h;
+	}
+	// (the scale radius matters to the Moffat luminosity only)
+	return profile_lum(q, q.kind == PK_CORESERSIC ? qgamma(0.5, 2 * q.nser) : 0.0, 0.0);
+}
+
+// lum_pre (optional, lum_by_difference kinds): the profile's lum_slot values,
+// computed beforehand.
+PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, DevProfile &d,
+                                 const double *lum_pre = nullptr)
 {
 	d.kind = p.kind;
 	d.target = p.convolve ? 0 : 1;
@@ -384,7 +415,7 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 	d.rscale = rscale;
 
 	// lumtot (get_lumtot overrides)
-	const double lum = profile_lum(p, d.bn, rscale);
+	const double lum = (lum_pre && lum_by_difference(p.kind)) ? lum_pre[0] : profile_lum(p, d.bn, rscale);
 
 	double b2 = p.box + 2;
 	double r_box = M_PI * b2 / (2 * beta_fn(1 / b2, 1 / b2));
@@ -505,15 +536,11 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 		// Ferrer (Beta function), core-Sersic, King and broken exponential
 		// (QUADPACK): central differences of the same FP64 luminosity, so the
 		// gradient differentiates exactly the normalisation the image uses.
-		ProfileParams q = p;
 		for (int k = 0; k < shape_count(p.kind); k++) {
-			double *v = shape_param(q, k);
-			const double v0 = *v, h = 1e-6 * fabs(v0) + 1e-9;
-			*v = v0 + h;
-			const double lp = profile_lum(q, q.kind == PK_CORESERSIC ? qgamma(0.5, 2 * q.nser) : 0.0, rscale);
-			*v = v0 - h;
-			const double lm = profile_lum(q, q.kind == PK_CORESERSIC ? qgamma(0.5, 2 * q.nser) : 0.0, rscale);
-			*v = v0;
+			ProfileParams q = p;
+			const double v0 = *shape_param(q, k), h = 1e-6 * fabs(v0) + 1e-9;
+			const double lp = lum_pre ? lum_pre[1 + 2 * k] : lum_slot(p, 1 + 2 * k);
+			const double lm = lum_pre ? lum_pre[2 + 2 * k] : lum_slot(p, 2 + 2 * k);
 			d.dlnI_dp[k] = -(log(lp) - log(lm)) / (2 * h);
 		}
 	}

@@ -955,7 +955,12 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const JT *__restrict__ jac, 
 		for (int u = 0; u < U; u++)
 			if (gv[u] != 0.f) {
 #pragma unroll
-				for (int k = 0; k < NT; k++) acc[k] += (double)gv[u] * (double)jv[u][k];
+				for (int k = 0; k < NT; k++) {
+					// FP64 planes carry sums an FP32 product would round away;
+					// with FP32 planes the FP32 product is as exact as its factors
+					if constexpr (sizeof(JT) == 8) acc[k] += (double)gv[u] * jv[u][k];
+					else acc[k] += (double)(gv[u] * jv[u][k]);
+				}
 			}
 	}
 	__shared__ double s_red[NT][8];
@@ -1492,6 +1497,14 @@ static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, 
 	    // one-column-per-lane kernels
 	    {ConvVariant<float, double, TOut, 8, 1, 8>::smem, ConvVariant<float, double, TOut, 8, 1, 8>::run},
 	    {ConvVariant<float, double, TOut, 8, 2, 4>::smem, ConvVariant<float, double, TOut, 8, 2, 4>::run},
+	    // fixed kernel heights (the 51x51 and 31x31 PSFs of the benchmark
+	    // workloads): every tap of a column unrolled, no loop or tail
+	    {Conv3Variant<TOut, 32, 10, 1, 8, 1, 51>::smem, Conv3Variant<TOut, 32, 10, 1, 8, 1, 51>::run},
+	    {Conv3Variant<TOut, 16, 10, 1, 8, 1, 51>::smem, Conv3Variant<TOut, 16, 10, 1, 8, 1, 51>::run},
+	    {Conv3Variant<TOut, 16, 8, 1, 4, 1, 51>::smem, Conv3Variant<TOut, 16, 8, 1, 4, 1, 51>::run},
+	    {Conv3Variant<TOut, 16, 8, 1, 8, 1, 51>::smem, Conv3Variant<TOut, 16, 8, 1, 8, 1, 51>::run},
+	    {Conv3Variant<TOut, 32, 8, 4, 1, 1, 31>::smem, Conv3Variant<TOut, 32, 8, 4, 1, 1, 31>::run},
+	    {Conv3Variant<TOut, 32, 12, 4, 1, 1, 31>::smem, Conv3Variant<TOut, 32, 12, 4, 1, 1, 31>::run},
 	    // tensor-core kernels (tcgen05, 3xTF32): 32 output columns per tile,
 	    // kernel rows split over 1, 2 or 4 CTAs.  Never picked by the
 	    // autotuner, only when forced: on a 400x400 image with a 51x51 PSF they
@@ -1619,8 +1632,24 @@ cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, c
 // reads one parameter record per profile (validated when the galaxy was
 // added) instead of a template plus a value matrix.
 // pad[t]: the PSF padding of the bucket that draws profile t.
+// The luminosity evaluations of the catalogue's core-Sersic, King, broken
+// exponential and Ferrer profiles (lum_slot: the profile's own and +-h in each
+// shape parameter), one thread per evaluation: each is a serial QUADPACK run,
+// and one thread per profile ran up to eleven of them back to back.  A
+// profile's slots sit in consecutive lanes, so a warp integrates one kind.
+__global__ void k_cat_lum(const ProfileParams *__restrict__ params, int n, double *__restrict__ lum)
+{
+	pdl_enter();
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= (long long)n * LUM_SLOTS) return;
+	const int pi = (int)(t / LUM_SLOTS), slot = (int)(t - (long long)pi * LUM_SLOTS);
+	const ProfileParams pp = params[pi];
+	if (slot < lum_slots(pp.kind)) lum[t] = lum_slot(pp, slot);
+}
+
 __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const int2 *__restrict__ pad, int n,
-                               ModelGeom g, DevProfile *__restrict__ dev, FProfile *__restrict__ fprof)
+                               ModelGeom g, const double *__restrict__ lum, DevProfile *__restrict__ dev,
+                               FProfile *__restrict__ fprof)
 {
 	pdl_enter();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1629,7 +1658,7 @@ __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const i
 	g.offx = pad[t].x;
 	g.offy = pad[t].y;
 	DevProfile d;
-	derive_profile(pp, g, d);
+	derive_profile(pp, g, d, lum ? lum + (size_t)t * LUM_SLOTS : nullptr);
 	dev[t] = d;
 	fprof[t] = to_fprofile(d, pp);
 }
@@ -1653,10 +1682,18 @@ __global__ void k_cat_gradient(const DevProfile *__restrict__ dev, int n, const 
 }
 
 cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, int n, const ModelGeom &g,
-                                DevProfile *dev, FProfile *fprof, cudaStream_t s)
+                                double *lum, DevProfile *dev, FProfile *fprof, cudaStream_t s)
 {
+	cudaError_t e = cudaSuccess;
+	if (lum) {
+		const long long nt = (long long)n * LUM_SLOTS;
+		e = launch_pdl(k_cat_lum, dim3((unsigned)((nt + 127) / 128)), dim3(128), 0, s, params, n, lum);
+		note_launches(1);
+		if (e != cudaSuccess) return e;
+	}
 	note_launches(1);
-	return launch_pdl(k_cat_prologue, dim3((n + 63) / 64), dim3(64), 0, s, params, pad, n, g, dev, fprof);
+	return launch_pdl(k_cat_prologue, dim3((n + 63) / 64), dim3(64), 0, s, params, pad, n, g, (const double *)lum, dev,
+	                  fprof);
 }
 
 cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,

@@ -90,3 +90,28 @@ def test_catalogue_rejects_bad_input():
         cat.add_galaxy(np.zeros((10, 10)), np.ones((10, 10)), psf, [("sersic", {"fwhm": 2.0})])
     with pytest.raises(InvalidParameter):
         cat.add_galaxy(np.zeros((10, 10)), np.ones((10, 10)), psf, [("sky", {"bg": 1.0})])
+
+
+def test_catalogue_replay_matches_first_call():
+    """The second call replays the first call's recorded launch sequence (one
+    graph for the prologue and every chunk); its results equal a fresh
+    catalogue's first, eager call to FP32 rounding, and a third call gives
+    the second's."""
+    gals = _catalogue_case(n=10, seed_tag=64)
+    out = []
+    for _ in range(2):
+        cat = Catalogue(magzero=gals[0]["magzero"])
+        for g in gals:
+            cat.add_galaxy(g["data"], g["sigma"], g["psf"], g["profiles"])
+        out.append(cat)
+    ll0, g0 = out[0].loglike_grad()          # eager (recorded afterwards)
+    ll1, g1 = out[1].loglike_grad()          # eager, another catalogue
+    ll2, g2 = out[1].loglike_grad()          # replayed
+    ll3, g3 = out[1].loglike_grad()          # replayed again
+    # (FP32 cells are added to their pixels atomically, in no fixed order)
+    np.testing.assert_allclose(ll1, ll0, rtol=1e-6)
+    np.testing.assert_allclose(ll2, ll1, rtol=1e-6)
+    np.testing.assert_allclose(ll3, ll2, rtol=1e-6)
+    for a, b, c in zip(g1, g2, g3):
+        np.testing.assert_allclose(b, a, rtol=1e-5, atol=1e-6 * np.max(np.abs(a)))
+        np.testing.assert_allclose(c, b, rtol=1e-5, atol=1e-6 * np.max(np.abs(b)))
