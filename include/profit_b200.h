@@ -369,8 +369,15 @@ int pf_model_evaluation_counts(pf_model *m, int profile, int64_t *out, int max_l
 unsigned long long pf_kernel_launches(void);
 
 /* Device time (ms, CUDA events) of the last evaluation's phases:
- * [0] total, [1] render, [2] convolution, [3] likelihood/adjoint. */
+ * [0] total, [1] render, [2] convolution, [3] likelihood/adjoint.  The FP32
+ * likelihood+gradient pipeline replayed from its recorded graph times only
+ * the total (events on the stream around the launch); [1]-[3] are NaN
+ * there unless phase timing is on. */
 int pf_model_last_timings(pf_model *m, float *ms, int n);
+/* Phase timing on (nonzero): recorded FP32 pipelines carry the render /
+ * convolution / likelihood events as graph nodes, which costs each replay a
+ * few microseconds of device time.  Off by default. */
+int pf_model_set_phase_timing(pf_model *m, int on);
 
 #ifdef __cplusplus
 }

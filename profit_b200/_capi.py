@@ -34,6 +34,7 @@ EXPORTED = (
     "pf_model_set_convolver", "pf_model_set_precision", "pf_model_drawing_dims", "pf_model_evaluate",
     "pf_model_set_data", "pf_model_loglike", "pf_model_loglike_grad", "pf_model_loglike_grad_fd",
     "pf_model_set_debug", "pf_model_decisions", "pf_model_level_counts", "pf_model_evaluation_counts", "pf_model_last_timings",
+    "pf_model_set_phase_timing",
     "pf_kernel_launches",
 )
 
@@ -101,6 +102,7 @@ def lib() -> C.CDLL:
         L.pf_model_loglike_grad.argtypes = [vp, C.POINTER(pf_param_ref), C.c_int, _dp, _dp]
         L.pf_model_loglike_grad_fd.argtypes = [vp, C.POINTER(pf_param_ref), C.c_int, C.c_double, _dp, _dp]
         L.pf_model_set_debug.argtypes = [vp, C.c_int]
+        L.pf_model_set_phase_timing.argtypes = [vp, C.c_int]
         L.pf_model_decisions.argtypes = [vp, C.c_int, C.POINTER(C.c_int32), C.c_size_t]
         L.pf_model_level_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int)]
         L.pf_model_evaluation_counts.argtypes = [vp, C.c_int, C.POINTER(C.c_int64), C.c_int, C.POINTER(C.c_int64)]

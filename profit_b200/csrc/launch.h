@@ -148,9 +148,11 @@ cudaError_t launch_loglike64_seed(const double *model, const double *data, const
 
 namespace pf {
 // render32.cu: batched proposals
+// quant (optional, batch * nprof * NSER_QUANTILES doubles of scratch): the
+// gamma quantiles run first, one thread each (k_batch_quantiles)
 cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batch, const int *ref_profile,
                                   const int *ref_offset, int nrefs, const double *values, const ModelGeom &g,
-                                  DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s);
+                                  double *quant, DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s);
 cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, const int *ref_profile,
                                   const int *ref_code, int nrefs, const double *T, const double *ll,
                                   const int *invalid, double *out_ll, double *out_grad, cudaStream_t s);
@@ -161,22 +163,39 @@ cudaError_t launch_loglike64_batch(const double *model, const double *data, cons
 }  // namespace pf
 
 namespace pf {
-// render32.cu: recomputing adjoint of the render (no stored tangent planes)
-cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
-                                     unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
-                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s,
-                                     const uint8_t *mask = nullptr);
+// render32.cu: recomputing adjoint of the render (no stored tangent planes).
+// Models with at least ADJOINT_LIST_MIN_PROFILES profiles per batch entry
+// take the per-tile profile lists (k_adjoint_pixels32_listed), others one
+// block per tile and profile.
+constexpr int ADJOINT_LIST_MIN_PROFILES = 8;
+cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, const int *prof_begin,
+                                     int batch, int n_profiles, unsigned width, unsigned height, double sx, double sy,
+                                     const float *g_conv, const float *g_plain, int levels, bool all_kinds,
+                                     const QueueSet &q, double *T, cudaStream_t s, const uint8_t *mask = nullptr);
 }  // namespace pf
 
 namespace pf {
 // render32.cu: catalogue batches (each entry with its own profiles)
 // pad: per profile, the drawing offset (PSF padding) of its bucket
-// lum (optional, n * LUM_SLOTS doubles of scratch): the QUADPACK
-// luminosities run first, one thread per evaluation (k_cat_lum)
+// lum (optional, n * PRO_SLOTS doubles of scratch): the QUADPACK
+// luminosities and the gamma quantiles run first, one thread per evaluation
+// (k_cat_lum)
 cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, int n, const ModelGeom &g,
                                 double *lum, DevProfile *dev, FProfile *fprof, cudaStream_t s);
 cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,
                                 cudaStream_t s);
+
+// A block of rows of one galaxy's data and sigma, packed in a staging
+// buffer (data rows, then sigma rows), to be placed in its canvas slot.
+struct CatPiece {
+	unsigned long long dst;  // canvas element of the block's first pixel
+	unsigned long long src;  // staging element of its first data value
+	int w, rows, W;          // block width and rows; canvas row stride
+	int pad_;
+};
+// Writes every piece's data, sigma and region (= 1) into the canvases.
+cudaError_t launch_cat_scatter(const CatPiece *pieces, int n_pieces, int max_pixels, const double *stage,
+                               double *data, double *sigma, uint8_t *region, cudaStream_t s);
 }  // namespace pf
 
 namespace pf {

@@ -114,37 +114,63 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 			cudaEvent_t e0, e1;
 			cudaEventCreate(&e0);
 			cudaEventCreate(&e1);
-			float best = 1e30f;
 			// PF_AUTOTUNE_LOG=1 prints every candidate's time to stderr
 			const char *lv = getenv("PF_AUTOTUNE_LOG");
 			const bool log = lv && lv[0] == '1';
+			// Candidates are timed on the first images of a large batch only
+			// (about 2M output pixels fill every SM several times over): the
+			// ranking is per tile, and timing whole catalogue chunks made
+			// the tuning most of a catalogue's first call.  The runs write
+			// only outputs that the chosen candidate then rewrites.
+			ConvArgs t = a;
+			const long long per = std::max(1LL, (long long)a.ow * a.oh);
+			t.batch = (int)std::min<long long>(a.batch, std::max(1LL, ((1LL << 21) + per - 1) / per));
+			// scratch in proportion, so that a candidate needing it applies to
+			// the truncated batch exactly when it applies to the whole one
+			t.scratch_bytes = a.scratch_bytes / std::max(1, a.batch) * t.batch;
+			std::vector<std::pair<float, int>> ranked;
 			for (int c = 0; c < n_cands; c++) {
 				if (!cands[c].tuned || cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
-				cudaError_t e = cands[c].run(a, s);  // warm-up (and attribute setup)
-				if (e != cudaSuccess) continue;
+				cudaError_t e = cands[c].run(t, s);  // warm-up (and attribute setup)
+				if (e != cudaSuccess) {
+					cudaGetLastError();
+					continue;
+				}
 				// batched shapes run long enough to be timed once
-				const int reps = a.batch > 8 ? 1 : 3;
+				const int reps = t.batch > 8 ? 1 : 3;
 				cudaEventRecord(e0, s);
-				for (int r = 0; r < reps; r++) cands[c].run(a, s);
+				for (int r = 0; r < reps; r++) cands[c].run(t, s);
 				cudaEventRecord(e1, s);
 				if (cudaEventSynchronize(e1) != cudaSuccess) break;
 				float ms = 0;
 				cudaEventElapsedTime(&ms, e0, e1);
-				ms *= 3.0f / reps;
+				ms /= reps;
 				if (log)
-					fprintf(stderr, "[profit_b200 autotune] type %d src %dx%d psf %dx%d out %dx%d batch %d: candidate %d %.4f ms\n",
-					        type_tag, a.sw, a.sh, a.kw, a.kh, a.ow, a.oh, a.batch, c, ms / 3);
-				if (ms < best) {
-					best = ms;
-					pick = c;
-				}
+					fprintf(stderr, "[profit_b200 autotune] type %d src %dx%d psf %dx%d out %dx%d batch %d (timed on %d): "
+					        "candidate %d %.4f ms\n",
+					        type_tag, a.sw, a.sh, a.kw, a.kh, a.ow, a.oh, a.batch, t.batch, c, ms);
+				ranked.emplace_back(ms, c);
 			}
 			cudaEventDestroy(e0);
 			cudaEventDestroy(e1);
-			if (pick < 0) pick = first_fit;
-			if (log) fprintf(stderr, "[profit_b200 autotune] type %d: picked candidate %d\n", type_tag, pick);
-			std::lock_guard<std::mutex> g(mu);
-			choice[key] = pick;
+			std::stable_sort(ranked.begin(), ranked.end(),
+			                 [](const std::pair<float, int> &x, const std::pair<float, int> &y) { return x.first < y.first; });
+			ranked.emplace_back(0.0f, first_fit);
+			// the fastest that also takes the whole batch
+			for (const auto &r : ranked) {
+				cudaError_t e = cands[r.second].run(a, s);
+				if (e == cudaErrorInvalidValue) {
+					cudaGetLastError();
+					continue;
+				}
+				if (log) fprintf(stderr, "[profit_b200 autotune] type %d: picked candidate %d\n", type_tag, r.second);
+				if (e == cudaSuccess) {
+					std::lock_guard<std::mutex> g(mu);
+					choice[key] = r.second;
+				}
+				return e;
+			}
+			return cudaErrorInvalidValue;
 		}
 	}
 	return cands[pick].run(a, s);
@@ -357,6 +383,8 @@ struct ResultLayout {
 struct BatchState;
 
 struct pf_model {
+	// per profile: its gamma quantiles, kept while its nser is unchanged
+	std::vector<pf::NserQuantiles> nq;
 	unsigned width, height;
 	std::vector<ProfileParams> profiles;
 	std::vector<double> psf;  // normalised
@@ -413,6 +441,11 @@ struct pf_model {
 	std::vector<uint64_t> graph_sig;
 	unsigned long long graph_kernels = 0;
 	bool use_graphs = true;
+	// phase events (render / convolution / likelihood and adjoint) inside
+	// replayed graphs: off by default, since each event node costs the graph
+	// microseconds; the total is timed by events around the launch
+	bool phase_timing = false;
+	bool phases_recorded = false;  // the last FP32 run recorded ev[1] and ev[2]
 	int prof_begin_n = -1;
 	BatchState *batch = nullptr;
 
@@ -763,7 +796,8 @@ int derive_and_upload(pf_model *m, const Analysis &a, const std::vector<ProfileP
 	PF_CUDA(ensure(m->h_prof, n * n_slots * sizeof(DevProfile)));
 	PF_CUDA(ensure(m->d_prof, n * n_slots * sizeof(DevProfile)));
 	DevProfile *hp = m->h_prof.as<DevProfile>() + n * slot;
-	for (size_t i = 0; i < n; i++) derive_profile(params[i], g, hp[i]);
+	if (m->nq.size() < n) m->nq.resize(n);
+	for (size_t i = 0; i < n; i++) derive_profile(params[i], g, hp[i], nullptr, nser_quantiles(m->nq[i], params[i]));
 	PF_CUDA(cudaMemcpyAsync(m->d_prof.as<DevProfile>() + n * slot, hp, n * sizeof(DevProfile), cudaMemcpyHostToDevice,
 	                        m->stream));
 	if (fp32) {
@@ -1138,6 +1172,29 @@ int jac_scratch(pf_model *m, unsigned npix, int n_profiles, double **partials, u
 	return PF_OK;
 }
 
+// Events of the FP32 pipeline.  Outside a capture each is recorded on the
+// stream.  A captured graph keeps only the inner phase events ev[1] and
+// ev[2], and only with phase timing on: the caller records ev[0] and ev[3]
+// on the stream around the graph's launch.
+cudaError_t phase_event(pf_model *m, int i, cudaStream_t s)
+{
+	cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+	cudaStreamIsCapturing(s, &st);
+	if (st != cudaStreamCaptureStatusActive) return cudaEventRecord(m->ev[i], s);
+	if ((i == 1 || i == 2) && m->phase_timing) return cudaEventRecordWithFlags(m->ev[i], s, cudaEventRecordExternal);
+	return cudaSuccess;
+}
+
+// Launches a recorded FP32 pipeline between the outer timing events.
+cudaError_t launch_recorded(pf_model *m, cudaGraphExec_t g)
+{
+	cudaError_t e = cudaEventRecord(m->ev[0], m->stream);
+	if (e == cudaSuccess) e = cudaGraphLaunch(g, m->stream);
+	if (e == cudaSuccess) e = cudaEventRecord(m->ev[3], m->stream);
+	m->phases_recorded = m->phase_timing;
+	return e;
+}
+
 int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q, bool want_grad, double *d_out)
 {
 	size_t npix = (size_t)a.dw * a.dh;
@@ -1161,12 +1218,12 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(launch_psf_stamp32(m->d_prof.as<DevProfile>(), m->d_prof_begin.as<int>(), 1, m->d_psf64.as<double>(),
 		                           m->psf_w, m->psf_h, m->psf_sx, m->psf_sy, m->sx / m->fs, m->sy / m->fs, a.padx,
 		                           a.pady, a.dw, a.dh, conv, plain, m->stream));
-	PF_CUDA(record_event(m->ev[1], m->stream));
+	PF_CUDA(phase_event(m, 1, m->stream));
 	PF_CUDA(ensure(m->d_model64, (size_t)a.cw * a.ch * 8 + 8));
 	double *model64 = m->d_model64.as<double>();
 	PF_TRY(forward_conv32(m, a, conv, plain, model64, 1));
 	(void)model;
-	PF_CUDA(record_event(m->ev[2], m->stream));
+	PF_CUDA(phase_event(m, 2, m->stream));
 	if (!m->has_data) return PF_OK;
 	float *wseed = nullptr;
 	if (want_grad) {
@@ -1192,7 +1249,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 			                             m->sx / m->fs, m->sy / m->fs, a.padx, a.pady, a.dw, a.dh, gconv, gplain,
 			                             d_out + ResultLayout::T0, m->stream));
 	}
-	PF_CUDA(record_event(m->ev[3], m->stream));
+	PF_CUDA(phase_event(m, 3, m->stream));
 	return PF_OK;
 }
 
@@ -1202,7 +1259,7 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 int enqueue_fp32(pf_model *m, const Analysis &a, bool want_grad, size_t nres, QueueSet &q)
 {
 	size_t n = (size_t)a.n_profiles;
-	PF_CUDA(record_event(m->ev[0], m->stream));
+	PF_CUDA(phase_event(m, 0, m->stream));
 	PF_CUDA(cudaMemcpyAsync(m->d_fprof.p, m->h_fprof.p, n * sizeof(FProfile), cudaMemcpyHostToDevice, m->stream));
 	if (has_psf_profile(m))  // the psf stamp reads the FP64 records
 		PF_CUDA(cudaMemcpyAsync(m->d_prof.p, m->h_prof.p, n * sizeof(DevProfile), cudaMemcpyHostToDevice, m->stream));
@@ -1226,7 +1283,7 @@ std::vector<uint64_t> graph_signature(pf_model *m, const Analysis &a, bool want_
 {
 	std::vector<uint64_t> s = {a.dw, a.dh, a.ow, a.oh, (uint64_t)a.n_profiles, (uint64_t)a.levels, a.conv,
 	                           (uint64_t)m->conv_kind, (uint64_t)m->precision, m->psf_w, m->psf_h, m->has_data,
-	                           m->has_region, want_grad, (uint64_t)m->like_kind};
+	                           m->has_region, want_grad, (uint64_t)m->like_kind, (uint64_t)m->phase_timing};
 	for (int l = 0; l < a.levels; l++) s.push_back(((uint64_t)q.off[l] << 32) | q.cap[l]);
 	const DevBuf *bufs[] = {&m->d_fprof, &m->d_prof_begin, &m->d_prof_batch, &m->d_conv32, &m->d_plain32,
 	                        &m->d_model64, &m->d_conv64, &m->d_plain64, &m->d_jac, &m->d_gconv, &m->d_gplain,
@@ -1257,10 +1314,15 @@ void finish_timings32(pf_model *m) { m->timings_lazy = true; }
 void resolve_timings32(pf_model *m)
 {
 	m->timings_lazy = false;
-	cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
-	cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
+	if (m->phases_recorded) {
+		cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
+		cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
+	}
+	else {
+		m->timings[1] = m->timings[2] = m->timings[3] = NAN;
+	}
 	if (m->has_data) {
-		cudaEventElapsedTime(&m->timings[3], m->ev[2], m->ev[3]);
+		if (m->phases_recorded) cudaEventElapsedTime(&m->timings[3], m->ev[2], m->ev[3]);
 		cudaEventElapsedTime(&m->timings[0], m->ev[0], m->ev[3]);
 	}
 	else {
@@ -1287,8 +1349,9 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 		PF_CUDA(ensure(m->d_fprof, nprof * sizeof(FProfile)));
 		DevProfile *hp = m->h_prof.as<DevProfile>();
 		FProfile *hf = m->h_fprof.as<FProfile>();
+		if ((int)m->nq.size() < nprof) m->nq.resize(nprof);
 		for (int i = 0; i < nprof; i++) {
-			derive_profile(m->profiles[i], g, hp[i]);
+			derive_profile(m->profiles[i], g, hp[i], nullptr, nser_quantiles(m->nq[i], m->profiles[i]));
 			hf[i] = to_fprofile(hp[i], m->profiles[i]);
 		}
 	}
@@ -1312,12 +1375,13 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 		PF_TRY(prepare_queue(m, a, npix * nprof, q, nullptr, nullptr, false, true, all_kinds(m)));
 		bool replayed = false;
 		if (want_grad && m->graph_exec && m->graph_sig == graph_signature(m, a, want_grad, q)) {
-			PF_CUDA(cudaGraphLaunch(m->graph_exec, m->stream));
+			PF_CUDA(launch_recorded(m, m->graph_exec));
 			note_launches((int)m->graph_kernels);
 			replayed = true;
 		}
 		else {
 			PF_TRY(enqueue_fp32(m, a, want_grad, nres, q));
+			m->phases_recorded = true;
 		}
 		PF_CUDA(cudaStreamSynchronize(m->stream));
 		int retry = 0;
@@ -1393,6 +1457,7 @@ struct FitRun {
 
 struct BatchState {
 	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out, d_ll, d_T, d_stage;
+	DevBuf d_quant;  // device prologue: the gamma quantiles of every (proposal, profile)
 	HostBuf h_tmpl, h_values, h_out, h_stage;
 	// fit space: parm of the chunk, [C] LP, [C][nfit] gradient, [C] LL, [C][nfit] parm_out
 	DevBuf d_fit_parm, d_fit_out;
@@ -1441,7 +1506,7 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	                                   : bs.d_invalid.as<int>();
 	double *out_ll = bs.d_out.as<double>(), *out_grad = out_ll + C;
 
-	PF_CUDA(record_event(m->ev[0], s));
+	PF_CUDA(phase_event(m, 0, s));
 	// a small stage is read by a kernel straight from the pinned buffer, which
 	// also zeroes the queue counters (one programmatic launch instead of a
 	// memset and a copy); a large one goes by copy
@@ -1470,7 +1535,8 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		}
 		PF_CUDA(cudaMemsetAsync(bs.d_invalid.p, 0, (size_t)C * 4, s));
 		PF_CUDA(launch_batch_prologue(bs.d_tmpl.as<ProfileParams>(), nprof, C, ref_profile, ref_offset, nrefs,
-		                              bs.d_values.as<double>(), geometry(m, a), bs.d_dev.as<DevProfile>(),
+		                              bs.d_values.as<double>(), geometry(m, a), bs.d_quant.as<double>(),
+		                              bs.d_dev.as<DevProfile>(),
 		                              m->d_fprof.as<FProfile>(), bs.d_invalid.as<int>(), s));
 	}
 	const int nt = tangent_stride(m);
@@ -1483,13 +1549,14 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		PF_CUDA(launch_psf_stamp32(dev, m->d_prof_begin.as<int>(), C, m->d_psf64.as<double>(), m->psf_w, m->psf_h,
 		                           m->psf_sx, m->psf_sy, m->sx / m->fs, m->sy / m->fs, a.padx, a.pady, a.dw, a.dh,
 		                           conv, plain, s));
-	PF_CUDA(record_event(m->ev[1], s));
+	PF_CUDA(phase_event(m, 1, s));
 	PF_TRY(forward_conv32(m, a, conv, plain, model64, C));
-	PF_CUDA(record_event(m->ev[2], s));
+	PF_CUDA(phase_event(m, 2, s));
 	PF_TRY(enqueue_like(m, model64, (int)nout, C, bs.d_ll.as<double>(), wseed, s));
 	PF_TRY(adjoint_seed32(m, a, wseed, gconv, gplain, C));
 	if (recompute)
-		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh, m->sx / m->fs,
+		PF_CUDA(launch_adjoint_recompute(fprof, m->d_prof_batch.as<int>(), m->d_prof_begin.as<int>(), C, C * nprof,
+		                                 a.dw, a.dh, m->sx / m->fs,
 		                                 m->sy / m->fs, gconv, gplain, a.levels, ak, q, bs.d_T.as<double>(), s,
 		                                 fin.draw));
 	// small batches without psf profiles (nothing writes T after the
@@ -1529,7 +1596,7 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		PF_CUDA(cudaMemcpyAsync(bs.h_fit_out.p, bs.d_fit_out.p, (size_t)C * (2 + 2 * nfit) * 8, cudaMemcpyDeviceToHost,
 		                        s));
 	}
-	PF_CUDA(record_event(m->ev[3], s));
+	PF_CUDA(phase_event(m, 3, s));
 	char *ho = bs.h_out.as<char>();
 	if (!direct_out)
 		PF_CUDA(cudaMemcpyAsync(ho, bs.d_out.p, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4, cudaMemcpyDeviceToHost,
@@ -1639,6 +1706,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		PF_CUDA(ensure(bs.h_fit_out, fo));
 	}
 	PF_CUDA(ensure(bs.d_invalid, (size_t)C * 4));
+	PF_CUDA(ensure(bs.d_quant, (size_t)C * nprof * NSER_QUANTILES * 8));
 	PF_CUDA(ensure(bs.d_ll, (size_t)C * 8));
 	PF_CUDA(ensure(bs.d_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
 	PF_CUDA(ensure(bs.d_T, (size_t)C * nprof * NTAN * 8));
@@ -1716,6 +1784,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			DevProfile *hd = bs.h_stage.as<DevProfile>();
 			FProfile *hf = reinterpret_cast<FProfile *>(bs.h_stage.as<char>() + L.f);
 			int *hi = reinterpret_cast<int *>(bs.h_stage.as<char>() + L.inv);
+			if ((int)m->nq.size() < nprof) m->nq.resize(nprof);
 			for (int b = 0; b < C; b++) {
 				hi[b] = 0;
 				for (int p = 0; p < nprof; p++) {
@@ -1728,7 +1797,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 						hi[b] = 1;
 						pp.kind = PK_NULL;
 					}
-					derive_profile(pp, geom, hd[b * nprof + p]);
+					derive_profile(pp, geom, hd[b * nprof + p], nullptr, nser_quantiles(m->nq[p], pp));
 					hf[b * nprof + p] = to_fprofile(hd[b * nprof + p], pp);
 				}
 			}
@@ -1750,7 +1819,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			sig.push_back((uint64_t)(uintptr_t)m->d_masks.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_stage.p);
 			for (auto *buf : {&bs.d_tmpl, &bs.d_refs, &bs.d_values, &bs.d_dev, &bs.d_invalid, &bs.d_out, &bs.d_ll,
-			                  &bs.d_T, &bs.d_stage})
+			                  &bs.d_T, &bs.d_stage, &bs.d_quant})
 				sig.push_back((uint64_t)(uintptr_t)buf->p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_out.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_values.p);
@@ -1762,12 +1831,13 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 					sig.push_back((uint64_t)(uintptr_t)p);
 			bool replayed = false;
 			if (bs.graph && bs.sig == sig) {
-				PF_CUDA(cudaGraphLaunch(bs.graph, m->stream));
+				PF_CUDA(launch_recorded(m, bs.graph));
 				note_launches((int)bs.graph_kernels);
 				replayed = true;
 			}
 			else {
 				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute, fit));
+				m->phases_recorded = true;
 			}
 			PF_CUDA(cudaStreamSynchronize(m->stream));
 			int retry = 0;
@@ -2553,6 +2623,13 @@ int pf_model_set_adjoint_mode(pf_model *m, int mode)
 	return PF_OK;
 }
 
+int pf_model_set_phase_timing(pf_model *m, int on)
+{
+	if (!m) return set_error(PF_E_INVALID, "null model");
+	m->phase_timing = on != 0;
+	return PF_OK;
+}
+
 int pf_model_set_debug(pf_model *m, int value)
 {
 	if (!m) return set_error(PF_E_INVALID, "null model");
@@ -2630,6 +2707,16 @@ struct CatGalaxy {
 	std::vector<ProfileParams> profiles;
 };
 
+// A typed view of part of a larger buffer.
+struct Span {
+	void *p = nullptr;
+	template <class T>
+	T *as() const
+	{
+		return static_cast<T *>(p);
+	}
+};
+
 // One launch group: galaxies of one bucket, static inputs resident.
 struct CatChunk {
 	unsigned W = 0, H = 0, pw = 0, ph = 0;
@@ -2638,8 +2725,10 @@ struct CatChunk {
 	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3, cusps = 0;
 	bool ak = false;
 	bool plain = false;  // a profile drawn without convolution (reads the seed of the plain image)
-	DevBuf data, sigma, region, psf32, psfrev32, prof_begin, prof_batch, grad_off, T, ll, grad;
-	HostBuf h_ll, h_grad, h_ctrl;
+	DevBuf data, sigma, region, psf32, psfrev32;
+	// slices of the catalogue's shared device and pinned host arenas
+	Span prof_begin, prof_batch, grad_off, T, ll, grad;
+	Span h_ll, h_grad, h_ctrl;
 	size_t npix() const { return (size_t)(W + 2 * (pw / 2)) * (H + 2 * (ph / 2)); }
 	size_t nout() const { return (size_t)W * H; }
 };
@@ -2656,7 +2745,9 @@ struct pf_catalogue {
 	bool built = false;
 	std::vector<std::unique_ptr<CatChunk>> chunks;
 	DevBuf params, pad, dev, fprof;  // every profile of the catalogue, chunk after chunk
-	DevBuf lum;                       // LUM_SLOTS luminosity evaluations per profile (prologue scratch)
+	DevBuf lum;                       // PRO_SLOTS luminosities and quantiles per profile (prologue scratch)
+	DevBuf arena;                     // every chunk's index tables, tangent sums, logL and gradient
+	HostBuf h_arena;                  // every chunk's logL, gradient and queue control words
 	int nprof = 0;
 	std::vector<int> grad_off;
 	int grad_total = 0;
@@ -2757,12 +2848,30 @@ int cat_build(pf_catalogue *c)
 			c->chunks.push_back(std::move(ch));
 		}
 	}
-	// static inputs: profile records and per-chunk index tables (serial,
-	// cheap), then every chunk's images (below, in parallel)
+	// static inputs: profile records and per-chunk index tables (serial and
+	// cheap; the tables go up in one copy into a shared arena), then every
+	// chunk's images (below, in parallel)
 	std::vector<ProfileParams> params;
 	std::vector<int2> pad;
-	for (auto &chp : c->chunks) {
-		CatChunk &ch = *chp;
+	std::vector<unsigned char> tables;  // the arena's index tables, at their offsets
+	size_t dtop = 0, htop = 0;
+	auto take = [](size_t &top, size_t bytes) {
+		const size_t o = top;
+		top += (std::max<size_t>(bytes, 8) + 255) & ~(size_t)255;
+		return o;
+	};
+	auto put = [&](const std::vector<int> &v) {
+		const size_t o = take(dtop, v.size() * 4);
+		tables.resize(dtop);
+		if (!v.empty()) std::memcpy(tables.data() + o, v.data(), v.size() * 4);
+		return o;
+	};
+	struct Slots {
+		size_t prof_begin, prof_batch, grad_off, T, ll, grad, h_ll, h_grad, h_ctrl;
+	};
+	std::vector<Slots> slots(c->chunks.size());
+	for (size_t k = 0; k < c->chunks.size(); k++) {
+		CatChunk &ch = *c->chunks[k];
 		const int C = (int)ch.members.size();
 		std::vector<int> prof_begin(C + 1, 0), prof_batch, goff;
 		ch.member_grad_off.assign(C, 0);
@@ -2791,83 +2900,151 @@ int cat_build(pf_catalogue *c)
 		}
 		ch.nprof = (int)params.size() - ch.p0;
 		ch.ngrad = gtot;
-		auto up = [&](DevBuf &b, const void *src, size_t bytes) -> int {
-			PF_CUDA(ensure(b, bytes));
-			PF_CUDA(cudaMemcpy(b.p, src, bytes, cudaMemcpyHostToDevice));
-			return PF_OK;
-		};
-		PF_TRY(up(ch.prof_begin, prof_begin.data(), prof_begin.size() * 4));
-		PF_TRY(up(ch.prof_batch, prof_batch.data(), prof_batch.size() * 4));
-		PF_TRY(up(ch.grad_off, goff.data(), goff.size() * 4));
-		PF_CUDA(ensure(ch.T, (size_t)ch.nprof * NTAN * 8));
-		PF_CUDA(ensure(ch.ll, (size_t)C * 8));
-		PF_CUDA(ensure(ch.grad, (size_t)std::max(gtot, 1) * 8));
-		PF_CUDA(ensure(ch.h_ll, (size_t)C * 8));
-		PF_CUDA(ensure(ch.h_grad, (size_t)std::max(gtot, 1) * 8));
-		PF_CUDA(ensure(ch.h_ctrl, CTRL_WORDS * 4));
+		Slots &sl = slots[k];
+		sl.prof_begin = put(prof_begin);
+		sl.prof_batch = put(prof_batch);
+		sl.grad_off = put(goff);
+		sl.T = take(dtop, (size_t)ch.nprof * NTAN * 8);
+		sl.ll = take(dtop, (size_t)C * 8);
+		sl.grad = take(dtop, (size_t)std::max(gtot, 1) * 8);
+		sl.h_ll = take(htop, (size_t)C * 8);
+		sl.h_grad = take(htop, (size_t)std::max(gtot, 1) * 8);
+		sl.h_ctrl = take(htop, CTRL_WORDS * 4);
+	}
+	PF_CUDA(ensure(c->arena, dtop));
+	PF_CUDA(cudaMemcpy(c->arena.p, tables.data(), tables.size(), cudaMemcpyHostToDevice));
+	PF_CUDA(ensure(c->h_arena, htop));
+	for (size_t k = 0; k < c->chunks.size(); k++) {
+		CatChunk &ch = *c->chunks[k];
+		const Slots &sl = slots[k];
+		char *d = c->arena.as<char>(), *h = c->h_arena.as<char>();
+		ch.prof_begin.p = d + sl.prof_begin;
+		ch.prof_batch.p = d + sl.prof_batch;
+		ch.grad_off.p = d + sl.grad_off;
+		ch.T.p = d + sl.T;
+		ch.ll.p = d + sl.ll;
+		ch.grad.p = d + sl.grad;
+		ch.h_ll.p = h + sl.h_ll;
+		ch.h_grad.p = h + sl.h_grad;
+		ch.h_ctrl.p = h + sl.h_ctrl;
 	}
 	// Each chunk's data, sigma and region canvases: cleared on the device,
-	// every galaxy's rows copied straight into its slot (the canvas beyond a
-	// galaxy keeps region 0, so its sigma there is never read), PSFs and
-	// their reversals packed per chunk.  Chunks are independent: host
-	// threads take them in turn.
+	// then every galaxy's rows packed into a pinned staging buffer, copied
+	// up with one transfer per staging buffer and placed in their canvas
+	// slots by k_cat_scatter (the canvas beyond a galaxy keeps region 0, so
+	// its sigma there is never read); PSFs and their reversals packed per
+	// chunk.  Chunks are independent: host threads take them in turn, each
+	// with its own stream and two staging buffers, so packing one overlaps
+	// the transfer of the other.
 	{
 		const int dev = c->engine->device;
+		size_t maxw = 1;
+		for (const CatGalaxy &G : c->gal) maxw = std::max<size_t>(maxw, G.w);
+		constexpr int MAX_PIECES = 4096;
+		const size_t head = MAX_PIECES * sizeof(CatPiece);
+		const size_t stage = std::max<size_t>((size_t)32 << 20, head + maxw * 16);
+		const size_t cap = (stage - head) / 8;  // doubles per staging buffer
 		std::atomic<size_t> next{0};
 		std::atomic<int> status{PF_OK};
 		std::mutex err_mu;
 		std::string err_msg;
 		auto worker = [&]() {
-			if (cudaSetDevice(dev) != cudaSuccess) {
-				status = PF_E_CUDA;
-				return;
-			}
-			for (size_t k = next++; k < c->chunks.size() && status == PF_OK; k = next++) {
+			cudaError_t e = cudaSetDevice(dev);
+			cudaStream_t st = nullptr;
+			cudaEvent_t done[2] = {};
+			if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+			for (int i = 0; i < 2 && e == cudaSuccess; i++) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+			HostBuf hb;
+			DevBuf db;
+			if (e == cudaSuccess) e = ensure(hb, 2 * stage);
+			if (e == cudaSuccess) e = ensure(db, 2 * stage);
+			int half = 0, np = 0, maxpix = 0;
+			bool used[2] = {false, false};
+			size_t nv = 0;
+			auto pieces = [&]() { return reinterpret_cast<CatPiece *>(hb.as<char>() + half * stage); };
+			auto values = [&]() { return reinterpret_cast<double *>(hb.as<char>() + half * stage + head); };
+			auto flush = [&](CatChunk &ch) {
+				if (np == 0 || e != cudaSuccess) return;
+				char *hs = hb.as<char>() + half * stage, *ds = db.as<char>() + half * stage;
+				e = cudaMemcpyAsync(ds, hs, head + nv * 8, cudaMemcpyHostToDevice, st);
+				if (e == cudaSuccess)
+					e = launch_cat_scatter(reinterpret_cast<const CatPiece *>(ds), np, maxpix,
+					                       reinterpret_cast<const double *>(ds + head), ch.data.as<double>(),
+					                       ch.sigma.as<double>(), ch.region.as<uint8_t>(), st);
+				if (e == cudaSuccess) e = cudaEventRecord(done[half], st);
+				used[half] = true;
+				half ^= 1;
+				if (e == cudaSuccess && used[half]) e = cudaEventSynchronize(done[half]);
+				np = 0;
+				nv = 0;
+				maxpix = 0;
+			};
+			for (size_t k = next++; k < c->chunks.size() && status == PF_OK && e == cudaSuccess; k = next++) {
 				CatChunk &ch = *c->chunks[k];
 				const int C = (int)ch.members.size();
 				const size_t nout = ch.nout(), nk = (size_t)ch.pw * ch.ph;
 				std::vector<float> psf(nk * C), psfrev(nk * C);
-				cudaError_t e = ensure(ch.data, nout * C * 8);
+				e = ensure(ch.data, nout * C * 8);
 				if (e == cudaSuccess) e = ensure(ch.sigma, nout * C * 8);
 				if (e == cudaSuccess) e = ensure(ch.region, nout * C);
-				if (e == cudaSuccess) e = cudaMemset(ch.data.p, 0, nout * C * 8);
-				if (e == cudaSuccess) e = cudaMemset(ch.sigma.p, 0, nout * C * 8);
-				if (e == cudaSuccess) e = cudaMemset(ch.region.p, 0, nout * C);
+				if (e == cudaSuccess) e = cudaMemsetAsync(ch.data.p, 0, nout * C * 8, st);
+				if (e == cudaSuccess) e = cudaMemsetAsync(ch.sigma.p, 0, nout * C * 8, st);
+				if (e == cudaSuccess) e = cudaMemsetAsync(ch.region.p, 0, nout * C, st);
 				for (int i = 0; i < C && e == cudaSuccess; i++) {
 					const CatGalaxy &G = c->gal[ch.members[i]];
-					const size_t o = (size_t)i * nout;
-					e = cudaMemcpy2D(ch.data.as<double>() + o, (size_t)ch.W * 8, G.data.data(), (size_t)G.w * 8,
-					                 (size_t)G.w * 8, G.h, cudaMemcpyHostToDevice);
-					if (e == cudaSuccess)
-						e = cudaMemcpy2D(ch.sigma.as<double>() + o, (size_t)ch.W * 8, G.sigma.data(), (size_t)G.w * 8,
-						                 (size_t)G.w * 8, G.h, cudaMemcpyHostToDevice);
-					if (e == cudaSuccess) e = cudaMemset2D(ch.region.as<uint8_t>() + o, ch.W, 1, G.w, G.h);
+					// rows of this galaxy that fit one staging buffer (at least one: the
+					// buffer holds the widest row)
+					const unsigned rp = (unsigned)std::min<size_t>(G.h, cap / 2 / G.w);
+					for (unsigned r0 = 0; r0 < G.h && e == cudaSuccess; r0 += rp) {
+						const unsigned rows = std::min(rp, G.h - r0);
+						const size_t n = (size_t)G.w * rows;
+						if (np == MAX_PIECES || nv + 2 * n > cap) flush(ch);
+						if (e != cudaSuccess) break;
+						CatPiece &pc = pieces()[np++];
+						pc.dst = (unsigned long long)i * nout + (unsigned long long)r0 * ch.W;
+						pc.src = nv;
+						pc.w = (int)G.w;
+						pc.rows = (int)rows;
+						pc.W = (int)ch.W;
+						pc.pad_ = 0;
+						std::memcpy(values() + nv, G.data.data() + (size_t)r0 * G.w, n * 8);
+						std::memcpy(values() + nv + n, G.sigma.data() + (size_t)r0 * G.w, n * 8);
+						nv += 2 * n;
+						maxpix = std::max(maxpix, (int)std::min<size_t>(n, 1u << 30));
+					}
 					for (size_t q = 0; q < nk; q++) {
 						psf[(size_t)i * nk + q] = (float)G.psf[q];
 						psfrev[(size_t)i * nk + q] = (float)G.psf[nk - 1 - q];
 					}
 				}
+				flush(ch);
 				if (e == cudaSuccess) e = ensure(ch.psf32, psf.size() * 4);
 				if (e == cudaSuccess) e = cudaMemcpy(ch.psf32.p, psf.data(), psf.size() * 4, cudaMemcpyHostToDevice);
 				if (e == cudaSuccess) e = ensure(ch.psfrev32, psfrev.size() * 4);
 				if (e == cudaSuccess)
 					e = cudaMemcpy(ch.psfrev32.p, psfrev.data(), psfrev.size() * 4, cudaMemcpyHostToDevice);
-				if (e != cudaSuccess) {
-					std::lock_guard<std::mutex> g(err_mu);
-					err_msg = cudaGetErrorString(e);
-					status = PF_E_CUDA;
-				}
+			}
+			// the staging buffers are freed below: wait for their transfers
+			if (st) {
+				cudaError_t e2 = cudaStreamSynchronize(st);
+				if (e == cudaSuccess) e = e2;
+			}
+			for (cudaEvent_t ev : done)
+				if (ev) cudaEventDestroy(ev);
+			if (st) cudaStreamDestroy(st);
+			if (e != cudaSuccess) {
+				std::lock_guard<std::mutex> g(err_mu);
+				err_msg = cudaGetErrorString(e);
+				status = PF_E_CUDA;
 			}
 		};
 		const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-		const size_t nthreads = std::min<size_t>(std::min<size_t>(hw, 8), c->chunks.size());
+		const size_t nthreads = std::max<size_t>(1, std::min<size_t>(std::min<size_t>(hw, 8), c->chunks.size()));
 		std::vector<std::thread> pool;
 		for (size_t t = 1; t < nthreads; t++) pool.emplace_back(worker);
 		worker();
 		for (auto &t : pool) t.join();
 		if (status != PF_OK) return set_error(PF_E_CUDA, "catalogue inputs: " + err_msg);
-		// the clears and copies ran on the legacy default stream of each thread
-		PF_CUDA(cudaDeviceSynchronize());
 	}
 	c->nprof = (int)params.size();
 	PF_CUDA(ensure(c->params, params.size() * sizeof(ProfileParams)));
@@ -2876,7 +3053,7 @@ int cat_build(pf_catalogue *c)
 	PF_CUDA(cudaMemcpy(c->pad.p, pad.data(), pad.size() * sizeof(int2), cudaMemcpyHostToDevice));
 	PF_CUDA(ensure(c->dev, params.size() * sizeof(DevProfile)));
 	PF_CUDA(ensure(c->fprof, params.size() * sizeof(FProfile)));
-	PF_CUDA(ensure(c->lum, params.size() * LUM_SLOTS * sizeof(double)));
+	PF_CUDA(ensure(c->lum, params.size() * PRO_SLOTS * sizeof(double)));
 
 	// engine scratch and queue for the largest chunk, so nothing is
 	// reallocated while chunks are queued

@@ -342,10 +342,83 @@ PF_HD inline double lum_slot(const ProfileParams &p, int slot)
 	return profile_lum(q, q.kind == PK_CORESERSIC ? qgamma(0.5, 2 * q.nser) : 0.0, 0.0);
 }
 
+// The gamma quantiles of a Sersic or core-Sersic profile, which depend on
+// nser alone and are most of its scalars' cost: bn = qgamma(0.5, 2n) and,
+// for adjusted Sersic profiles, the quantiles behind rscale_switch
+// (qgamma(1 - n^2/2000, 2n)) and rscale_max (qgamma(0.9999, 2n)).  A host
+// caller keeps one per profile and reuses it while nser is unchanged; a
+// device prologue computes the three in parallel threads (nser_quantile).
+struct NserQuantiles {
+	double nser = -1;
+	double q_half = 0, q_switch = 0, q_max = 0;
+	bool has_half = false, has_switch = false, has_max = false;
+};
+
+constexpr int NSER_QUANTILES = 3;
+
+// Quantile k of p (0: bn, 1: rscale_switch's, 2: rscale_max's), or 0 where
+// derive_profile does not use it.
+PF_HD inline double nser_quantile(const ProfileParams &p, int k)
+{
+	if (p.kind != PK_SERSIC && p.kind != PK_CORESERSIC) return 0;
+	if (k == 0) return qgamma(0.5, 2 * p.nser);
+	if (p.kind != PK_SERSIC || !p.adjust) return 0;
+	if (k == 1) return qgamma(1. - p.nser * p.nser / 2e3, 2 * p.nser);
+	return p.rscale_max == 0 ? qgamma(0.9999, 2 * p.nser) : 0.0;
+}
+
+// The quantiles of p from its NSER_QUANTILES nser_quantile values.
+PF_HD inline NserQuantiles nser_quantiles_from(const ProfileParams &p, const double *q)
+{
+	NserQuantiles c;
+	c.nser = p.nser;
+	c.q_half = q[0];
+	c.q_switch = q[1];
+	c.q_max = q[2];
+	c.has_half = c.has_switch = c.has_max = true;
+	return c;
+}
+
+// Fills (or keeps, for the same nser) the quantiles p needs.
+inline const NserQuantiles *nser_quantiles(NserQuantiles &c, const ProfileParams &p)
+{
+	if (p.kind != PK_SERSIC && p.kind != PK_CORESERSIC) return nullptr;
+	if (!(c.nser == p.nser)) {
+		c = NserQuantiles();
+		c.nser = p.nser;
+	}
+	if (!c.has_half) {
+		c.q_half = nser_quantile(p, 0);
+		c.has_half = true;
+	}
+	if (p.kind == PK_SERSIC && p.adjust) {
+		if (!c.has_switch) {
+			c.q_switch = nser_quantile(p, 1);
+			c.has_switch = true;
+		}
+		if (p.rscale_max == 0 && !c.has_max) {
+			c.q_max = nser_quantile(p, 2);
+			c.has_max = true;
+		}
+	}
+	return &c;
+}
+
+// Prologue scratch per profile: its LUM_SLOTS luminosity evaluations, then
+// its NSER_QUANTILES quantiles.
+constexpr int PRO_SLOTS = LUM_SLOTS + NSER_QUANTILES;
+
+// Scratch slot `slot` of profile p (0 where p does not use it).
+PF_HD inline double pro_slot(const ProfileParams &p, int slot)
+{
+	if (slot < LUM_SLOTS) return slot < lum_slots(p.kind) ? lum_slot(p, slot) : 0.0;
+	return nser_quantile(p, slot - LUM_SLOTS);
+}
+
 // lum_pre (optional, lum_by_difference kinds): the profile's lum_slot values,
-// computed beforehand.
+// computed beforehand.  nq (optional): nser_quantiles of p.
 PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, DevProfile &d,
-                                 const double *lum_pre = nullptr)
+                                 const double *lum_pre = nullptr, const NserQuantiles *nq = nullptr)
 {
 	d.kind = p.kind;
 	d.target = p.convolve ? 0 : 1;
@@ -401,7 +474,7 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 		// the specialised forms recompute 1/invexp with the same operands
 		d.invexp = d.boxy ? p.nser * (p.box + 2) : p.nser;
 	}
-	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) d.bn = qgamma(0.5, 2 * p.nser);
+	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) d.bn = nq ? nq->q_half : qgamma(0.5, 2 * p.nser);
 
 	// rscale (get_rscale overrides)
 	double rscale;
@@ -427,7 +500,7 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 	if (p.adjust) {
 		switch (p.kind) {
 		case PK_SERSIC: {
-			double fr = p.re * pow(qgamma(1. - p.nser * p.nser / 2e3, 2 * p.nser) / d.bn, p.nser);
+			double fr = p.re * pow((nq ? nq->q_switch : qgamma(1. - p.nser * p.nser / 2e3, 2 * p.nser)) / d.bn, p.nser);
 			double rs = ceil(fr);
 			rs = pf_fmax(pf_fmin(rs, 20.), 2.);
 			rscale_switch = rs / p.re;
@@ -451,7 +524,7 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 		if (rscale_max == 0) {
 			switch (p.kind) {
 			case PK_SERSIC: {
-				double ff = p.re * pow(qgamma(0.9999, 2 * p.nser) / d.bn, p.nser);
+				double ff = p.re * pow((nq ? nq->q_max : qgamma(0.9999, 2 * p.nser)) / d.bn, p.nser);
 				rscale_max = ceil(pf_fmax(ff, 2.) / p.re);
 				break;
 			}

@@ -536,6 +536,112 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 	img_plain[(size_t)b * npix + pix] = acc[1];
 }
 
+// The render without tangent planes, for models with many profiles: each
+// block first lists, in profile order, the profiles that reach it (the sky,
+// and radial profiles not skipped by k_pixels32's block test, evaluated the
+// same way), then every pixel loops over that list only.  Profiles are
+// listed 256 at a time, one per thread, with an ordered compaction (warp
+// ballots), so each pixel adds the same terms in the same order as
+// k_pixels32 without planes: the images are the same bit for bit.
+template <bool AK>
+__global__ void __launch_bounds__(256) k_pixels32_listed(const FProfile *__restrict__ profiles,
+                                                         const int *__restrict__ prof_begin, unsigned width,
+                                                         unsigned height, double sx, double sy,
+                                                         float *__restrict__ img_conv, float *__restrict__ img_plain,
+                                                         QueueSet q, const uint8_t *__restrict__ mask)
+{
+	pdl_enter();
+	__shared__ int s_list[256];
+	__shared__ int s_count[8];
+	const int lane = threadIdx.x, wid = threadIdx.y, tid = wid * 32 + lane;
+	const unsigned i = blockIdx.x * 32 + threadIdx.x;
+	const unsigned j = blockIdx.y * 8 + threadIdx.y;
+	const int b = blockIdx.z;
+	const bool inside = i < width && j < height;
+	const size_t npix = (size_t)width * height;
+	const uint32_t pix = inside ? i + j * width : 0;
+	const int p0 = prof_begin[b], p1 = prof_begin[b + 1];
+	float acc[2] = {0.f, 0.f};
+	const double half_xbin = sx / 2., half_ybin = sy / 2.;
+	const double y = half_ybin + j * sx;
+	const double x = half_xbin + i * sy;
+	// pixel centres of this block (same expressions as x and y)
+	const unsigned tx0 = blockIdx.x * 32, ty0 = blockIdx.y * 8;
+	const unsigned tx1 = min(tx0 + 31, width - 1), ty1 = min(ty0 + 7, height - 1);
+	const double xlo = half_xbin + tx0 * sy, xhi = half_xbin + tx1 * sy;
+	const double ylo = half_ybin + ty0 * sx, yhi = half_ybin + ty1 * sx;
+	const bool drawn = inside && (!mask || mask[pix]);
+
+	for (int base = p0; base < p1; base += 256) {
+		bool keep = false;
+		if (base + tid < p1) {
+			const FProfile &p = profiles[base + tid];
+			if (p.kind == PK_SKY) {
+				keep = true;
+			}
+			else if (is_radial_kind(p.kind)) {
+				keep = true;
+				if (p.r_max > 0.f) {
+					const double nx = fmin(fmax(p.cx, xlo), xhi) - p.cx, ny = fmin(fmax(p.cy, ylo), yhi) - p.cy;
+					const double lim = (double)p.r_max + 2.0;
+					keep = !(nx * nx + ny * ny > lim * lim);
+				}
+			}
+		}
+		const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+		if (lane == 0) s_count[wid] = __popc(ballot);
+		__syncthreads();
+		int before = 0, total = 0;
+#pragma unroll
+		for (int w = 0; w < 8; w++) {
+			before += w < wid ? s_count[w] : 0;
+			total += s_count[w];
+		}
+		if (keep) s_list[before + __popc(ballot & ((1u << lane) - 1u))] = base + tid;
+		__syncthreads();
+		if (drawn) {
+			for (int k = 0; k < total; k++) {
+				const int pi = s_list[k];
+				const FProfile &p = profiles[pi];
+				if (p.kind == PK_SKY) {
+					acc[p.target] += p.flux_scale;  // sky value is kept in flux_scale
+					continue;
+				}
+				float xp, yp;
+				const int decision = pixel_decision32(p, x, y, xp, yp);
+				if (decision == PD_DIRECT) {
+					acc[p.target] += p.flux_scale * eval_val<float, AK>(p, xp, yp);
+				}
+				else if (decision == PD_SUBSAMPLE) {
+					unsigned res = p.resolution, max_rec = p.max_rec;
+					if (p.centre_override && fabs(x - p.cx) < p.img_sx && fabs(y - p.cy) < p.img_sy) {
+						res = 8;
+						max_rec = 10;
+					}
+					SubItem it;
+					const double ddx = x - p.cx, ddy = y - p.cy;
+					it.x0 = ddx - half_xbin;
+					it.x1 = ddx + half_xbin;
+					it.y0 = ddy - half_ybin;
+					it.y1 = ddy + half_ybin;
+					it.weight = 1.0 / (res * res);
+					it.pixel = pix + (uint32_t)(b * npix);
+					it.profile = (uint16_t)pi;
+					it.res = (uint8_t)res;
+					it.max_rec = (uint8_t)max_rec;
+					queue_push(q, 0, it);
+					note_max_res(q, res);
+				}
+			}
+		}
+		__syncthreads();  // the next round rewrites s_list and s_count
+	}
+	if (inside) {
+		img_conv[(size_t)b * npix + pix] = acc[0];
+		img_plain[(size_t)b * npix + pix] = acc[1];
+	}
+}
+
 // k / res == (k * div_magic(res)) >> 16 for every sub-point index k < 256
 // and resolution 1 <= res <= 16: the magic ceil(2^16 / res) exceeds 2^16 / res
 // by less than 1, so the product overshoots k / res by less than 256 / 2^16,
@@ -800,6 +906,86 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 	}
 }
 
+// The same for models with many profiles per batch entry: one block per
+// 64 x 32 tile and batch entry lists the profiles whose rscale_max (+2 px)
+// reaches the tile (the test above), then takes them one after another.  A
+// block per (tile, profile) left most blocks with nothing to do but that
+// test: on a large field the launch of the culled blocks cost more than the
+// test itself.  (T is added atomically either way, in no fixed order.)
+template <bool AK>
+__global__ void __launch_bounds__(256) k_adjoint_pixels32_listed(const FProfile *__restrict__ profiles,
+                                                                 const int *__restrict__ prof_begin, unsigned width,
+                                                                 unsigned height, double sx, double sy,
+                                                                 const float *__restrict__ g_conv,
+                                                                 const float *__restrict__ g_plain,
+                                                                 double *__restrict__ T,
+                                                                 const uint8_t *__restrict__ mask)
+{
+	pdl_enter();
+	constexpr int NT = ntk<AK>();
+	__shared__ int s_list[256];
+	__shared__ int s_count;
+	__shared__ double s_red[NT][8];
+	const int b = blockIdx.z;
+	const unsigned tx0 = blockIdx.x * 64, ty0 = blockIdx.y * 32;
+	const double half_xbin = sx / 2., half_ybin = sy / 2.;
+	const unsigned tx1 = min(tx0 + 63, width - 1), ty1 = min(ty0 + 31, height - 1);
+	const double xlo = half_xbin + tx0 * sy, xhi = half_xbin + tx1 * sy;
+	const double ylo = half_ybin + ty0 * sx, yhi = half_ybin + ty1 * sx;
+	const size_t npix = (size_t)width * height;
+	const int p0 = prof_begin[b], p1 = prof_begin[b + 1];
+	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	const unsigned i = tx0 + (threadIdx.x & 63);
+	for (int base = p0; base < p1; base += 256) {
+		if (threadIdx.x == 0) s_count = 0;
+		__syncthreads();
+		if (base + (int)threadIdx.x < p1) {
+			const int pi = base + threadIdx.x;
+			const FProfile &p = profiles[pi];
+			bool keep = is_radial_kind(p.kind);
+			if (keep && p.r_max > 0.f) {
+				const double nx = fmin(fmax(p.cx, xlo), xhi) - p.cx, ny = fmin(fmax(p.cy, ylo), yhi) - p.cy;
+				keep = !(sqrt(nx * nx + ny * ny) > (double)p.r_max + 2.0);
+			}
+			if (keep) s_list[atomicAdd(&s_count, 1)] = pi;
+		}
+		__syncthreads();
+		const int n = s_count;
+		for (int k = 0; k < n; k++) {
+			const int pi = s_list[k];
+			const FProfile &p = profiles[pi];
+			const float *g = (p.target == 0 ? g_conv : g_plain) + (size_t)b * npix;
+			float acc[NT];
+#pragma unroll
+			for (int t = 0; t < NT; t++) acc[t] = 0.f;
+			for (unsigned r = threadIdx.x >> 6; r < 32; r += 4) {
+				const unsigned j = ty0 + r;
+				if (i >= width || j >= height) continue;
+				if (mask && !mask[i + (size_t)j * width]) continue;  // not drawn by the forward pass
+				const float gv = g[i + (size_t)j * width];
+				if (gv == 0.f) continue;
+				const double y = half_ybin + j * sx, x = half_xbin + i * sy;
+				float xp, yp;
+				if (pixel_decision32(p, x, y, xp, yp) != PD_DIRECT) continue;
+				Tan<float> t = eval_tan<float, AK>(p, xp, yp);
+				tan_to_j<NT>(t, xp, yp, gv, acc);
+			}
+#pragma unroll
+			for (int t = 0; t < NT; t++) {
+				double v = warp_sum((double)acc[t]);
+				if (lane == 0) s_red[t][wid] = v;
+			}
+			__syncthreads();
+			if (threadIdx.x < NT) {
+				double v = 0;
+				for (int w = 0; w < 8; w++) v += s_red[threadIdx.x][w];
+				if (v != 0.0) atomicAdd(&T[(size_t)pi * NTAN + threadIdx.x], v);
+			}
+			__syncthreads();  // s_red is rewritten for the next profile
+		}
+	}
+}
+
 // Every queued cell of every level, one warp per cell: the tangents of the
 // accepted sub-points, times the cell weight and g(pixel).
 template <bool AK>
@@ -851,16 +1037,24 @@ __global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restr
 	}
 }
 
-cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, int n_profiles, unsigned width,
-                                     unsigned height, double sx, double sy, const float *g_conv, const float *g_plain,
-                                     int levels, bool all_kinds, const QueueSet &q, double *T, cudaStream_t s,
-                                     const uint8_t *mask)
+cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_batch, const int *prof_begin,
+                                     int batch, int n_profiles, unsigned width, unsigned height, double sx, double sy,
+                                     const float *g_conv, const float *g_plain, int levels, bool all_kinds,
+                                     const QueueSet &q, double *T, cudaStream_t s, const uint8_t *mask)
 {
-	dim3 grid((width + 63) / 64, (height + 31) / 32, n_profiles);
-	auto kp = all_kinds ? k_adjoint_pixels32<true> : k_adjoint_pixels32<false>;
+	cudaError_t e;
 	auto ki = all_kinds ? k_adjoint_items32<true> : k_adjoint_items32<false>;
-	cudaError_t e = launch_pdl(kp, grid, dim3(256), 0, s, profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T,
-	                           mask);
+	if (n_profiles >= ADJOINT_LIST_MIN_PROFILES * batch) {
+		dim3 grid((width + 63) / 64, (height + 31) / 32, batch);
+		auto kl = all_kinds ? k_adjoint_pixels32_listed<true> : k_adjoint_pixels32_listed<false>;
+		e = launch_pdl(kl, grid, dim3(256), 0, s, profiles, prof_begin, width, height, sx, sy, g_conv, g_plain, T, mask);
+	}
+	else {
+		dim3 grid((width + 63) / 64, (height + 31) / 32, n_profiles);
+		auto kp = all_kinds ? k_adjoint_pixels32<true> : k_adjoint_pixels32<false>;
+		e = launch_pdl(kp, grid, dim3(256), 0, s, profiles, prof_batch, width, height, sx, sy, g_conv, g_plain, T,
+		               mask);
+	}
 	if (e == cudaSuccess) e = launch_pdl(ki, dim3(148 * 8), dim3(256), 0, s, profiles, levels, g_conv, g_plain, q, T);
 	note_launches(2);
 	return e;
@@ -1077,8 +1271,12 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
 		return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain,
 		                  static_cast<double *>(jac.p), nt, q, mask);
 	}
-	auto k = all_kinds ? (jac.p ? k_pixels32<true, true, float> : k_pixels32<true, false, float>)
-	                   : (jac.p ? k_pixels32<false, true, float> : k_pixels32<false, false, float>);
+	if (!jac.p) {
+		auto k = all_kinds ? k_pixels32_listed<true> : k_pixels32_listed<false>;
+		return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, q,
+		                  mask);
+	}
+	auto k = all_kinds ? k_pixels32<true, true, float> : k_pixels32<false, true, float>;
 	return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain,
 	                  static_cast<float *>(jac.p), nt, q, mask);
 }
@@ -1572,25 +1770,58 @@ cudaError_t launch_crop32(const float *src, unsigned sw, unsigned ox, unsigned o
 // FP64 scalar prologue (b_n, luminosity, Ie, auto-adjusted subsampling).  A
 // proposal with an invalid profile is flagged and its profiles become null
 // profiles, so nothing is drawn for it.
+// Profile p of proposal b: the template with the proposal's values.
+__device__ __forceinline__ ProfileParams proposal_params(const ProfileParams *__restrict__ tmpl, int p, int b,
+                                                        const int *__restrict__ ref_profile,
+                                                        const int *__restrict__ ref_offset, int nrefs,
+                                                        const double *__restrict__ values)
+{
+	ProfileParams pp = tmpl[p];
+	for (int r = 0; r < nrefs; r++)
+		if (ref_profile[r] == p)
+			*reinterpret_cast<double *>(reinterpret_cast<char *>(&pp) + ref_offset[r]) = values[(size_t)b * nrefs + r];
+	return pp;
+}
+
+// One thread per (proposal, profile, quantile): the gamma quantiles of the
+// Sersic and core-Sersic profiles (nser_quantile), the serial part of their
+// scalars, three at a time instead of one after another.
+__global__ void k_batch_quantiles(const ProfileParams *__restrict__ tmpl, int nprof, int batch,
+                                  const int *__restrict__ ref_profile, const int *__restrict__ ref_offset, int nrefs,
+                                  const double *__restrict__ values, double *__restrict__ quant)
+{
+	pdl_enter();
+	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+	if (t >= (long long)batch * nprof * NSER_QUANTILES) return;
+	const int k = (int)(t % NSER_QUANTILES), bp = (int)(t / NSER_QUANTILES);
+	const int b = bp / nprof, p = bp - b * nprof;
+	const ProfileParams pp = proposal_params(tmpl, p, b, ref_profile, ref_offset, nrefs, values);
+	quant[t] = params_valid(pp) ? nser_quantile(pp, k) : 0.0;
+}
+
+// quant (optional): k_batch_quantiles' output.
 __global__ void k_batch_prologue(const ProfileParams *__restrict__ tmpl, int nprof, int batch,
                                  const int *__restrict__ ref_profile, const int *__restrict__ ref_offset, int nrefs,
-                                 const double *__restrict__ values, ModelGeom g, DevProfile *__restrict__ dev,
-                                 FProfile *__restrict__ fprof, int *__restrict__ invalid)
+                                 const double *__restrict__ values, ModelGeom g, const double *__restrict__ quant,
+                                 DevProfile *__restrict__ dev, FProfile *__restrict__ fprof, int *__restrict__ invalid)
 {
 	pdl_enter();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
 	if (t >= batch * nprof) return;
 	const int b = t / nprof, p = t - b * nprof;
-	ProfileParams pp = tmpl[p];
-	for (int r = 0; r < nrefs; r++)
-		if (ref_profile[r] == p)
-			*reinterpret_cast<double *>(reinterpret_cast<char *>(&pp) + ref_offset[r]) = values[(size_t)b * nrefs + r];
+	ProfileParams pp = proposal_params(tmpl, p, b, ref_profile, ref_offset, nrefs, values);
 	if (!params_valid(pp)) {
 		invalid[b] = 1;
 		pp.kind = PK_NULL;
 	}
 	DevProfile d;
-	derive_profile(pp, g, d);
+	if (quant) {
+		const NserQuantiles nq = nser_quantiles_from(pp, quant + (size_t)t * NSER_QUANTILES);
+		derive_profile(pp, g, d, nullptr, &nq);
+	}
+	else {
+		derive_profile(pp, g, d);
+	}
 	dev[t] = d;
 	fprof[t] = to_fprofile(d, pp);
 }
@@ -1610,12 +1841,19 @@ __global__ void k_batch_gradient(const DevProfile *__restrict__ dev, int nprof, 
 
 cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batch, const int *ref_profile,
                                   const int *ref_offset, int nrefs, const double *values, const ModelGeom &g,
-                                  DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s)
+                                  double *quant, DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s)
 {
 	int n = batch * nprof;
+	if (quant) {
+		const long long nq = (long long)n * NSER_QUANTILES;
+		cudaError_t e = launch_pdl(k_batch_quantiles, dim3((unsigned)((nq + 127) / 128)), dim3(128), 0, s, tmpl, nprof,
+		                           batch, ref_profile, ref_offset, nrefs, values, quant);
+		note_launches(1);
+		if (e != cudaSuccess) return e;
+	}
 	note_launches(1);
 	return launch_pdl(k_batch_prologue, dim3((n + 127) / 128), dim3(128), 0, s, tmpl, nprof, batch, ref_profile,
-	                  ref_offset, nrefs, values, g, dev, fprof, invalid);
+	                  ref_offset, nrefs, values, g, (const double *)quant, dev, fprof, invalid);
 }
 
 cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, const int *ref_profile,
@@ -1641,10 +1879,9 @@ __global__ void k_cat_lum(const ProfileParams *__restrict__ params, int n, doubl
 {
 	pdl_enter();
 	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= (long long)n * LUM_SLOTS) return;
-	const int pi = (int)(t / LUM_SLOTS), slot = (int)(t - (long long)pi * LUM_SLOTS);
-	const ProfileParams pp = params[pi];
-	if (slot < lum_slots(pp.kind)) lum[t] = lum_slot(pp, slot);
+	if (t >= (long long)n * PRO_SLOTS) return;
+	const int pi = (int)(t / PRO_SLOTS), slot = (int)(t - (long long)pi * PRO_SLOTS);
+	lum[t] = pro_slot(params[pi], slot);
 }
 
 __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const int2 *__restrict__ pad, int n,
@@ -1658,7 +1895,14 @@ __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const i
 	g.offx = pad[t].x;
 	g.offy = pad[t].y;
 	DevProfile d;
-	derive_profile(pp, g, d, lum ? lum + (size_t)t * LUM_SLOTS : nullptr);
+	if (lum) {
+		const double *pl = lum + (size_t)t * PRO_SLOTS;
+		const NserQuantiles nq = nser_quantiles_from(pp, pl + LUM_SLOTS);
+		derive_profile(pp, g, d, pl, &nq);
+	}
+	else {
+		derive_profile(pp, g, d);
+	}
 	dev[t] = d;
 	fprof[t] = to_fprofile(d, pp);
 }
@@ -1686,7 +1930,7 @@ cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, in
 {
 	cudaError_t e = cudaSuccess;
 	if (lum) {
-		const long long nt = (long long)n * LUM_SLOTS;
+		const long long nt = (long long)n * PRO_SLOTS;
 		e = launch_pdl(k_cat_lum, dim3((unsigned)((nt + 127) / 128)), dim3(128), 0, s, params, n, lum);
 		note_launches(1);
 		if (e != cudaSuccess) return e;
@@ -1701,6 +1945,32 @@ cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, c
 {
 	note_launches(1);
 	return launch_pdl(k_cat_gradient, dim3((n + 127) / 128), dim3(128), 0, s, dev, n, T, grad_off, grad);
+}
+
+__global__ void k_cat_scatter(const CatPiece *__restrict__ pieces, const double *__restrict__ stage,
+                              double *__restrict__ data, double *__restrict__ sigma, uint8_t *__restrict__ region)
+{
+	const CatPiece pc = pieces[blockIdx.y];
+	const long long n = (long long)pc.w * pc.rows;
+	const double *d = stage + pc.src, *sg = d + n;
+	for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+		const long long y = i / pc.w, x = i - y * pc.w;
+		const unsigned long long o = pc.dst + (unsigned long long)y * pc.W + x;
+		data[o] = d[i];
+		sigma[o] = sg[i];
+		region[o] = 1;
+	}
+}
+
+cudaError_t launch_cat_scatter(const CatPiece *pieces, int n_pieces, int max_pixels, const double *stage,
+                               double *data, double *sigma, uint8_t *region, cudaStream_t s)
+{
+	if (n_pieces <= 0) return cudaSuccess;
+	if (n_pieces > 65535) return cudaErrorInvalidValue;
+	note_launches(1);
+	const unsigned gx = (unsigned)std::min(64, std::max(1, (max_pixels + 1023) / 1024));
+	k_cat_scatter<<<dim3(gx, (unsigned)n_pieces), dim3(256), 0, s>>>(pieces, stage, data, sigma, region);
+	return cudaGetLastError();
 }
 
 cudaError_t launch_loglike64_batch(const double *model, const double *data, const double *sigma,

@@ -327,6 +327,14 @@ class Model:
         return tot.value, per
 
     def last_timings(self) -> List[float]:
+        """Device ms of the last evaluation: [total, render, convolution,
+        likelihood + adjoint]; the phases are NaN for a replayed FP32
+        pipeline unless set_phase_timing(True)."""
         out = (C.c_float * 4)()
         check(lib().pf_model_last_timings(self._h, out, 4))
         return list(out)
+
+    def set_phase_timing(self, on: bool = True) -> None:
+        """Records the phase events inside replayed FP32 pipelines (a few
+        microseconds of device time per replay)."""
+        check(lib().pf_model_set_phase_timing(self._h, int(bool(on))))

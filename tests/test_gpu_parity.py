@@ -150,6 +150,27 @@ def test_recompute_adjoint_matches_stored_tangents():
     np.testing.assert_allclose(g_r, g_s, rtol=1e-5, atol=1e-6 * np.max(np.abs(g_s)))
 
 
+def test_recompute_adjoint_tile_lists_match_stored_tangents():
+    """Models with many profiles take per-tile profile lists in the
+    recomputing adjoint (12 Sersics here): every component's gradient equals
+    the stored-plane form's."""
+    from profit_b200._capi import PF_ADJOINT_RECOMPUTE, PF_ADJOINT_STORE
+    wl = W.large_field(n_profiles=12, width=240, height=200, psf_size=31)
+    m = W.configure(Model(wl["width"], wl["height"]), wl)
+    truth, _ = m.evaluate()
+    image, sigma = W.make_data(wl, truth)
+    w2 = W.perturbed(wl, seed=11, scale=0.01)
+    mp = W.configure(Model(wl["width"], wl["height"], precision=PF_FP32), w2)
+    mp.set_data(image, sigma)
+    refs = w2["grad"]
+    mp.set_adjoint_mode(PF_ADJOINT_STORE)
+    ll_s, g_s = mp.loglike_grad(refs)
+    mp.set_adjoint_mode(PF_ADJOINT_RECOMPUTE)
+    ll_r, g_r = mp.loglike_grad(refs)
+    assert ll_r == pytest.approx(ll_s, rel=1e-6)
+    np.testing.assert_allclose(g_r, g_s, rtol=1e-5, atol=1e-6 * np.max(np.abs(g_s)))
+
+
 def test_large_field_fft_fp64_and_recompute_gradient():
     """A field of 12 Sersics (shape of the 2000x2000 / 200-component case at
     reduced size) with the FFT convolver: FP64 image against the restatement,
