@@ -309,7 +309,14 @@ def main_b200(args):
     llref = ctypes.byref(ll)
     nrefs = len(refs)
 
+    # one proposal per call: its 17 values in, logL and the gradient out
     def step(s):
+        st = L.pf_model_loglike_grad_batch(m._h, arr, nrefs, 1, vptrs[s], llref, gptr)
+        if st != 0:
+            raise RuntimeError(L.pf_last_error().decode())
+
+    # the same through libprofit's call pattern: set the parameters, evaluate
+    def step_set_parameters(s):
         L.pf_model_set_parameters(m._h, arr, nrefs, vptrs[s])
         st = L.pf_model_loglike_grad(m._h, arr, nrefs, llref, gptr)
         if st != 0:
@@ -360,6 +367,17 @@ def main_b200(args):
         conv_ms.append(tim[2])
         phase_dev_ms.append(tim[0])
     L.pf_model_set_phase_timing(m._h, 0)
+    # end to end through set_parameters + loglike_grad
+    for s in range(args.warmup):
+        step_set_parameters(s)
+    e2e_sp_ms = []
+    for s in range(args.warmup, args.warmup + args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step_set_parameters(s)
+        e2e_sp_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_sp_total = max_over_ranks([sum(e2e_sp_ms) / 1e3], dist if world > 1 else None, device="cuda")[0]
 
     dev_total, e2e_total = max_over_ranks([sum(dev_ms) / 1e3, sum(e2e_ms) / 1e3],
                                           dist if world > 1 else None, device="cuda")
@@ -403,8 +421,12 @@ def main_b200(args):
             "config": config_dict(wl, world),
             "e2e": {"value": aggregate_rate(args.steps, e2e_total, world), "unit": UNIT,
                     "h2d_bytes_per_step": 8 * len(refs), "d2h_bytes_per_step": 8 * (1 + len(refs)),
-                    "path": "pf_model_set_parameters + pf_model_loglike_grad (C ABI, host buffers)",
-                    "ms_per_step": 1e3 * e2e_total / args.steps},
+                    "path": "pf_model_loglike_grad_batch with one proposal (C ABI, host buffers: the 17 values "
+                            "in, logL and 17 gradient components out)",
+                    "ms_per_step": 1e3 * e2e_total / args.steps,
+                    "set_parameters_path": {"value": aggregate_rate(args.steps, e2e_sp_total, world), "unit": UNIT,
+                                            "path": "pf_model_set_parameters + pf_model_loglike_grad",
+                                            "ms_per_step": 1e3 * e2e_sp_total / args.steps}},
             "roofline": roof,
             "gpu_launches": int(launches),
             "clocks": clk,
@@ -548,8 +570,7 @@ def convolver_choice_rate(torch, flush, wl, image, sigma, refs, pvals, steps=30)
         flush.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        L.pf_model_set_parameters(m._h, arr, len(refs), vptrs[s % len(pvals)])
-        if L.pf_model_loglike_grad(m._h, arr, len(refs), llref, gptr) != 0:
+        if L.pf_model_loglike_grad_batch(m._h, arr, len(refs), 1, vptrs[s % len(pvals)], llref, gptr) != 0:
             raise RuntimeError(L.pf_last_error().decode())
         t1 = time.perf_counter()
         if s >= 3:

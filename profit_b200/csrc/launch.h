@@ -103,6 +103,10 @@ struct GradStepArgs {
 	const uint32_t *ctrl_in = nullptr;
 	uint32_t *ctrl_out = nullptr;
 	int ctrl_words = 0;
+	// optional: after everything above is written, *seq_in is stored to
+	// *seq_out (a word of mapped host memory the caller polls)
+	const unsigned *seq_in = nullptr;
+	unsigned *seq_out = nullptr;
 };
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles);
 cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
@@ -148,11 +152,9 @@ cudaError_t launch_loglike64_seed(const double *model, const double *data, const
 
 namespace pf {
 // render32.cu: batched proposals
-// quant (optional, batch * nprof * NSER_QUANTILES doubles of scratch): the
-// gamma quantiles run first, one thread each (k_batch_quantiles)
 cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batch, const int *ref_profile,
                                   const int *ref_offset, int nrefs, const double *values, const ModelGeom &g,
-                                  double *quant, DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s);
+                                  DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s);
 cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, const int *ref_profile,
                                   const int *ref_code, int nrefs, const double *T, const double *ll,
                                   const int *invalid, double *out_ll, double *out_grad, cudaStream_t s);
@@ -177,9 +179,8 @@ cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_b
 namespace pf {
 // render32.cu: catalogue batches (each entry with its own profiles)
 // pad: per profile, the drawing offset (PSF padding) of its bucket
-// lum (optional, n * PRO_SLOTS doubles of scratch): the QUADPACK
-// luminosities and the gamma quantiles run first, one thread per evaluation
-// (k_cat_lum)
+// lum (optional, n * LUM_SLOTS doubles of scratch): the QUADPACK
+// luminosities run first, one thread per evaluation (k_cat_lum)
 cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, int n, const ModelGeom &g,
                                 double *lum, DevProfile *dev, FProfile *fprof, cudaStream_t s);
 cudaError_t launch_cat_gradient(const DevProfile *dev, int n, const double *T, const int *grad_off, double *grad,

@@ -8,6 +8,7 @@
 // convolved with the normalised PSF, the PSF padding is cropped, the second
 // is added, and finesampled images are summed back down when requested.
 #include <algorithm>
+#include <array>
 #include <cctype>
 #include <atomic>
 #include <cmath>
@@ -117,44 +118,66 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 			// PF_AUTOTUNE_LOG=1 prints every candidate's time to stderr
 			const char *lv = getenv("PF_AUTOTUNE_LOG");
 			const bool log = lv && lv[0] == '1';
-			// Candidates are timed on the first images of a large batch only
-			// (about 2M output pixels fill every SM several times over): the
-			// ranking is per tile, and timing whole catalogue chunks made
-			// the tuning most of a catalogue's first call.  The runs write
-			// only outputs that the chosen candidate then rewrites.
-			ConvArgs t = a;
+			// Candidates are timed on the first images of a large batch only:
+			// every candidate on about 512k output pixels, then the four
+			// fastest again on about 2M (enough to fill every SM several
+			// times over).  The ranking is per tile, and timing whole
+			// catalogue chunks made the tuning most of a catalogue's first
+			// call.  The runs write only outputs that the chosen candidate
+			// then rewrites.
 			const long long per = std::max(1LL, (long long)a.ow * a.oh);
-			t.batch = (int)std::min<long long>(a.batch, std::max(1LL, ((1LL << 21) + per - 1) / per));
-			// scratch in proportion, so that a candidate needing it applies to
-			// the truncated batch exactly when it applies to the whole one
-			t.scratch_bytes = a.scratch_bytes / std::max(1, a.batch) * t.batch;
-			std::vector<std::pair<float, int>> ranked;
-			for (int c = 0; c < n_cands; c++) {
-				if (!cands[c].tuned || cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
-				cudaError_t e = cands[c].run(t, s);  // warm-up (and attribute setup)
-				if (e != cudaSuccess) {
-					cudaGetLastError();
-					continue;
+			auto truncated = [&](long long pixels) {
+				ConvArgs t = a;
+				t.batch = (int)std::min<long long>(a.batch, std::max(1LL, (pixels + per - 1) / per));
+				// scratch in proportion, so that a candidate needing it applies
+				// to the truncated batch exactly when it applies to the whole one
+				t.scratch_bytes = a.scratch_bytes / std::max(1, a.batch) * t.batch;
+				return t;
+			};
+			auto time_one = [&](const ConvArgs &t, int c, bool warm, float &ms) -> bool {
+				if (warm) {
+					cudaError_t e = cands[c].run(t, s);  // warm-up (and attribute setup)
+					if (e != cudaSuccess) {
+						cudaGetLastError();
+						return false;
+					}
 				}
 				// batched shapes run long enough to be timed once
 				const int reps = t.batch > 8 ? 1 : 3;
 				cudaEventRecord(e0, s);
 				for (int r = 0; r < reps; r++) cands[c].run(t, s);
 				cudaEventRecord(e1, s);
-				if (cudaEventSynchronize(e1) != cudaSuccess) break;
-				float ms = 0;
+				if (cudaEventSynchronize(e1) != cudaSuccess) return false;
 				cudaEventElapsedTime(&ms, e0, e1);
 				ms /= reps;
 				if (log)
 					fprintf(stderr, "[profit_b200 autotune] type %d src %dx%d psf %dx%d out %dx%d batch %d (timed on %d): "
 					        "candidate %d %.4f ms\n",
 					        type_tag, a.sw, a.sh, a.kw, a.kh, a.ow, a.oh, a.batch, t.batch, c, ms);
-				ranked.emplace_back(ms, c);
+				return true;
+			};
+			auto by_time = [](std::vector<std::pair<float, int>> &v) {
+				std::stable_sort(v.begin(), v.end(), [](const std::pair<float, int> &x, const std::pair<float, int> &y) {
+					return x.first < y.first;
+				});
+			};
+			const ConvArgs t1 = truncated(1LL << 19), t2 = truncated(1LL << 21);
+			std::vector<std::pair<float, int>> ranked;
+			for (int c = 0; c < n_cands; c++) {
+				if (!cands[c].tuned || cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
+				float ms = 0;
+				if (time_one(t1, c, true, ms)) ranked.emplace_back(ms, c);
+			}
+			by_time(ranked);
+			if (t2.batch > t1.batch) {
+				const size_t top = std::min<size_t>(4, ranked.size());
+				for (size_t r = 0; r < top; r++) time_one(t2, ranked[r].second, false, ranked[r].first);
+				std::vector<std::pair<float, int>> head(ranked.begin(), ranked.begin() + top);
+				by_time(head);
+				std::copy(head.begin(), head.end(), ranked.begin());
 			}
 			cudaEventDestroy(e0);
 			cudaEventDestroy(e1);
-			std::stable_sort(ranked.begin(), ranked.end(),
-			                 [](const std::pair<float, int> &x, const std::pair<float, int> &y) { return x.first < y.first; });
 			ranked.emplace_back(0.0f, first_fit);
 			// the fastest that also takes the whole batch
 			for (const auto &r : ranked) {
@@ -383,8 +406,8 @@ struct ResultLayout {
 struct BatchState;
 
 struct pf_model {
-	// per profile: its gamma quantiles, kept while its nser is unchanged
-	std::vector<pf::NserQuantiles> nq;
+	// per profile: its shape-only scalars, kept while nser and box are unchanged
+	std::vector<pf::ShapeMemo> nq;
 	unsigned width, height;
 	std::vector<ProfileParams> profiles;
 	std::vector<double> psf;  // normalised
@@ -797,7 +820,7 @@ int derive_and_upload(pf_model *m, const Analysis &a, const std::vector<ProfileP
 	PF_CUDA(ensure(m->d_prof, n * n_slots * sizeof(DevProfile)));
 	DevProfile *hp = m->h_prof.as<DevProfile>() + n * slot;
 	if (m->nq.size() < n) m->nq.resize(n);
-	for (size_t i = 0; i < n; i++) derive_profile(params[i], g, hp[i], nullptr, nser_quantiles(m->nq[i], params[i]));
+	for (size_t i = 0; i < n; i++) derive_profile(params[i], g, hp[i], nullptr, shape_memo(m->nq[i], params[i]));
 	PF_CUDA(cudaMemcpyAsync(m->d_prof.as<DevProfile>() + n * slot, hp, n * sizeof(DevProfile), cudaMemcpyHostToDevice,
 	                        m->stream));
 	if (fp32) {
@@ -1314,6 +1337,8 @@ void finish_timings32(pf_model *m) { m->timings_lazy = true; }
 void resolve_timings32(pf_model *m)
 {
 	m->timings_lazy = false;
+	// (a polled call returns before its closing event has been recorded)
+	cudaEventSynchronize(m->has_data ? m->ev[3] : m->ev[2]);
 	if (m->phases_recorded) {
 		cudaEventElapsedTime(&m->timings[1], m->ev[0], m->ev[1]);
 		cudaEventElapsedTime(&m->timings[2], m->ev[1], m->ev[2]);
@@ -1351,7 +1376,7 @@ int evaluate32(pf_model *m, Analysis &a, bool want_grad, std::vector<double> *re
 		FProfile *hf = m->h_fprof.as<FProfile>();
 		if ((int)m->nq.size() < nprof) m->nq.resize(nprof);
 		for (int i = 0; i < nprof; i++) {
-			derive_profile(m->profiles[i], g, hp[i], nullptr, nser_quantiles(m->nq[i], m->profiles[i]));
+			derive_profile(m->profiles[i], g, hp[i], nullptr, shape_memo(m->nq[i], m->profiles[i]));
 			hf[i] = to_fprofile(hp[i], m->profiles[i]);
 		}
 	}
@@ -1438,14 +1463,19 @@ inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t STAGE_IN_MAX_BYTES = 64 << 10;
 
 struct StageLayout {
-	size_t f = 0, inv = 0, total = 0;
+	size_t f = 0, inv = 0, seq = 0, total = 0;
 	StageLayout(int C, int nprof)
 	{
 		f = align256((size_t)C * nprof * sizeof(DevProfile));
 		inv = f + align256((size_t)C * nprof * sizeof(FProfile));
-		total = inv + align256((size_t)C * 4);
+		seq = inv + align256((size_t)C * 4);  // the call's sequence number (completion word)
+		total = seq + 256;
 	}
 };
+
+// The completion word behind the results and queue counters in the pinned
+// result buffer.
+inline size_t out_flag_offset(int C, int nrefs) { return align256((size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4); }
 
 // A batch evaluated in ProFit's fit space (pf_model_lp_grad_batch): the
 // proposals are fitted vectors parm (nfit per row) instead of model values.
@@ -1457,7 +1487,6 @@ struct FitRun {
 
 struct BatchState {
 	DevBuf d_tmpl, d_refs, d_values, d_dev, d_invalid, d_out, d_ll, d_T, d_stage;
-	DevBuf d_quant;  // device prologue: the gamma quantiles of every (proposal, profile)
 	HostBuf h_tmpl, h_values, h_out, h_stage;
 	// fit space: parm of the chunk, [C] LP, [C][nfit] gradient, [C] LL, [C][nfit] parm_out
 	DevBuf d_fit_parm, d_fit_out;
@@ -1471,6 +1500,10 @@ struct BatchState {
 	cudaGraphExec_t graph = nullptr;
 	std::vector<uint64_t> sig;
 	unsigned long long graph_kernels = 0;
+	// the pipeline ends by storing the call's sequence number into the
+	// result buffer (set by enqueue_batch_chunk); seq counts the calls
+	bool polled = false;
+	unsigned seq = 0;
 	~BatchState()
 	{
 		if (graph) cudaGraphExecDestroy(graph);
@@ -1535,8 +1568,7 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		}
 		PF_CUDA(cudaMemsetAsync(bs.d_invalid.p, 0, (size_t)C * 4, s));
 		PF_CUDA(launch_batch_prologue(bs.d_tmpl.as<ProfileParams>(), nprof, C, ref_profile, ref_offset, nrefs,
-		                              bs.d_values.as<double>(), geometry(m, a), bs.d_quant.as<double>(),
-		                              bs.d_dev.as<DevProfile>(),
+		                              bs.d_values.as<double>(), geometry(m, a), bs.d_dev.as<DevProfile>(),
 		                              m->d_fprof.as<FProfile>(), bs.d_invalid.as<int>(), s));
 	}
 	const int nt = tangent_stride(m);
@@ -1573,7 +1605,13 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 		gargs.ctrl_in = q.counts;
 		gargs.ctrl_out = reinterpret_cast<uint32_t *>(hd + (size_t)C * (1 + nrefs) * 8);
 		gargs.ctrl_words = CTRL_WORDS;
+		if (hmap) {
+			// and then the call's sequence number, which the host polls
+			gargs.seq_in = reinterpret_cast<const unsigned *>(bs.d_stage.as<char>() + L.seq);
+			gargs.seq_out = reinterpret_cast<unsigned *>(hd + out_flag_offset(C, nrefs));
+		}
 	}
+	bs.polled = direct_out && hmap;
 	if (!recompute) {
 		double *jpart;
 		unsigned *jtick;
@@ -1601,6 +1639,30 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	if (!direct_out)
 		PF_CUDA(cudaMemcpyAsync(ho, bs.d_out.p, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4, cudaMemcpyDeviceToHost,
 		                        s));
+	return PF_OK;
+}
+
+// Waits for a chunk's results.  A pipeline that ends by storing the call's
+// sequence number after its results (bs.polled) is waited for by polling
+// that word in the pinned result buffer: the host sees it a few
+// microseconds before the stream reports completion (only the end of the
+// last block, which reads nothing more, and the closing timing event
+// remain).  The stream is queried now and then, so a launch that fails
+// reports its error through the synchronisation below instead of being
+// waited for forever.
+int wait_chunk(pf_model *m, BatchState &bs, const char *flag_word)
+{
+	if (bs.polled && flag_word) {
+		const volatile unsigned *flag = reinterpret_cast<const volatile unsigned *>(flag_word);
+		for (unsigned long spin = 1;; spin++) {
+			if (*flag == bs.seq) {
+				std::atomic_thread_fence(std::memory_order_acquire);
+				return PF_OK;
+			}
+			if ((spin & 4095) == 0 && cudaStreamQuery(m->stream) != cudaErrorNotReady) break;
+		}
+	}
+	PF_CUDA(cudaStreamSynchronize(m->stream));
 	return PF_OK;
 }
 
@@ -1706,12 +1768,11 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 		PF_CUDA(ensure(bs.h_fit_out, fo));
 	}
 	PF_CUDA(ensure(bs.d_invalid, (size_t)C * 4));
-	PF_CUDA(ensure(bs.d_quant, (size_t)C * nprof * NSER_QUANTILES * 8));
 	PF_CUDA(ensure(bs.d_ll, (size_t)C * 8));
 	PF_CUDA(ensure(bs.d_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
 	PF_CUDA(ensure(bs.d_T, (size_t)C * nprof * NTAN * 8));
 	void *out_before = bs.h_out.p;
-	PF_CUDA(ensure(bs.h_out, (size_t)C * (1 + nrefs) * 8 + CTRL_WORDS * 4));
+	PF_CUDA(ensure(bs.h_out, out_flag_offset(C, nrefs) + 256));
 	if (bs.h_out.p != out_before || !bs.h_out_dev) {
 		if (cudaHostGetDevicePointer(&bs.h_out_dev, bs.h_out.p, 0) != cudaSuccess) {
 			cudaGetLastError();
@@ -1797,7 +1858,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 						hi[b] = 1;
 						pp.kind = PK_NULL;
 					}
-					derive_profile(pp, geom, hd[b * nprof + p], nullptr, nser_quantiles(m->nq[p], pp));
+					derive_profile(pp, geom, hd[b * nprof + p], nullptr, shape_memo(m->nq[p], pp));
 					hf[b * nprof + p] = to_fprofile(hd[b * nprof + p], pp);
 				}
 			}
@@ -1819,7 +1880,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			sig.push_back((uint64_t)(uintptr_t)m->d_masks.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_stage.p);
 			for (auto *buf : {&bs.d_tmpl, &bs.d_refs, &bs.d_values, &bs.d_dev, &bs.d_invalid, &bs.d_out, &bs.d_ll,
-			                  &bs.d_T, &bs.d_stage, &bs.d_quant})
+			                  &bs.d_T, &bs.d_stage})
 				sig.push_back((uint64_t)(uintptr_t)buf->p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_out.p);
 			sig.push_back((uint64_t)(uintptr_t)bs.h_values.p);
@@ -1829,6 +1890,13 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				for (const void *p : std::initializer_list<const void *>{fit->dev.e, bs.d_fit_parm.p, bs.d_fit_out.p,
 				                                                         bs.h_fit_out.p})
 					sig.push_back((uint64_t)(uintptr_t)p);
+			if (host_prologue) {
+				// a new sequence number for this launch, and its completion word
+				// cleared (pinned memory starts with whatever it held before)
+				if (++bs.seq == 0) bs.seq = 1;
+				*reinterpret_cast<unsigned *>(bs.h_stage.as<char>() + StageLayout(C, nprof).seq) = bs.seq;
+				*reinterpret_cast<volatile unsigned *>(ho + out_flag_offset(C, nrefs)) = 0;
+			}
 			bool replayed = false;
 			if (bs.graph && bs.sig == sig) {
 				PF_CUDA(launch_recorded(m, bs.graph));
@@ -1839,10 +1907,11 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 				PF_TRY(enqueue_batch_chunk(m, bs, a, C, nrefs, q, host_prologue, recompute, fit));
 				m->phases_recorded = true;
 			}
-			PF_CUDA(cudaStreamSynchronize(m->stream));
+			PF_TRY(wait_chunk(m, bs, host_prologue ? ho + out_flag_offset(C, nrefs) : nullptr));
 			int retry = 0;
 			PF_TRY(check_overflow(m, a, reinterpret_cast<uint32_t *>(ho + (size_t)C * (1 + nrefs) * 8), retry));
 			if (retry) {
+				PF_CUDA(cudaStreamSynchronize(m->stream));  // (the launch may still be finishing)
 				if (bs.graph) cudaGraphExecDestroy(bs.graph);
 				bs.graph = nullptr;
 				continue;
@@ -1850,6 +1919,7 @@ int eval_grad_batch(pf_model *m, const pf_param_ref *refs, int nrefs, int B, con
 			done = true;
 			finish_timings32(m);
 			if (!replayed && m->use_graphs) {
+				PF_CUDA(cudaStreamSynchronize(m->stream));
 				if (bs.graph) cudaGraphExecDestroy(bs.graph);
 				bs.graph = nullptr;
 				unsigned long long before = g_launches.load();
@@ -2725,8 +2795,8 @@ struct CatChunk {
 	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3, cusps = 0;
 	bool ak = false;
 	bool plain = false;  // a profile drawn without convolution (reads the seed of the plain image)
-	DevBuf data, sigma, region, psf32, psfrev32;
 	// slices of the catalogue's shared device and pinned host arenas
+	Span data, sigma, region, psf32, psfrev32;
 	Span prof_begin, prof_batch, grad_off, T, ll, grad;
 	Span h_ll, h_grad, h_ctrl;
 	size_t npix() const { return (size_t)(W + 2 * (pw / 2)) * (H + 2 * (ph / 2)); }
@@ -2745,8 +2815,9 @@ struct pf_catalogue {
 	bool built = false;
 	std::vector<std::unique_ptr<CatChunk>> chunks;
 	DevBuf params, pad, dev, fprof;  // every profile of the catalogue, chunk after chunk
-	DevBuf lum;                       // PRO_SLOTS luminosities and quantiles per profile (prologue scratch)
+	DevBuf lum;                       // LUM_SLOTS luminosity evaluations per profile (prologue scratch)
 	DevBuf arena;                     // every chunk's index tables, tangent sums, logL and gradient
+	DevBuf canvases;                  // every chunk's data, sigma, region and PSF images
 	HostBuf h_arena;                  // every chunk's logL, gradient and queue control words
 	int nprof = 0;
 	std::vector<int> grad_off;
@@ -2914,6 +2985,25 @@ int cat_build(pf_catalogue *c)
 	PF_CUDA(ensure(c->arena, dtop));
 	PF_CUDA(cudaMemcpy(c->arena.p, tables.data(), tables.size(), cudaMemcpyHostToDevice));
 	PF_CUDA(ensure(c->h_arena, htop));
+	// the images of every chunk in one allocation
+	size_t ctop = 0;
+	std::vector<std::array<size_t, 5>> coff(c->chunks.size());
+	for (size_t k = 0; k < c->chunks.size(); k++) {
+		const CatChunk &ch = *c->chunks[k];
+		const size_t C = ch.members.size(), nout = ch.nout(), nk = (size_t)ch.pw * ch.ph;
+		coff[k] = {take(ctop, nout * C * 8), take(ctop, nout * C * 8), take(ctop, nout * C), take(ctop, C * nk * 4),
+		           take(ctop, C * nk * 4)};
+	}
+	PF_CUDA(ensure(c->canvases, ctop));
+	for (size_t k = 0; k < c->chunks.size(); k++) {
+		CatChunk &ch = *c->chunks[k];
+		char *d = c->canvases.as<char>();
+		ch.data.p = d + coff[k][0];
+		ch.sigma.p = d + coff[k][1];
+		ch.region.p = d + coff[k][2];
+		ch.psf32.p = d + coff[k][3];
+		ch.psfrev32.p = d + coff[k][4];
+	}
 	for (size_t k = 0; k < c->chunks.size(); k++) {
 		CatChunk &ch = *c->chunks[k];
 		const Slots &sl = slots[k];
@@ -2942,7 +3032,7 @@ int cat_build(pf_catalogue *c)
 		for (const CatGalaxy &G : c->gal) maxw = std::max<size_t>(maxw, G.w);
 		constexpr int MAX_PIECES = 4096;
 		const size_t head = MAX_PIECES * sizeof(CatPiece);
-		const size_t stage = std::max<size_t>((size_t)32 << 20, head + maxw * 16);
+		const size_t stage = std::max<size_t>((size_t)8 << 20, head + maxw * 16);
 		const size_t cap = (stage - head) / 8;  // doubles per staging buffer
 		std::atomic<size_t> next{0};
 		std::atomic<int> status{PF_OK};
@@ -2983,11 +3073,7 @@ int cat_build(pf_catalogue *c)
 				CatChunk &ch = *c->chunks[k];
 				const int C = (int)ch.members.size();
 				const size_t nout = ch.nout(), nk = (size_t)ch.pw * ch.ph;
-				std::vector<float> psf(nk * C), psfrev(nk * C);
-				e = ensure(ch.data, nout * C * 8);
-				if (e == cudaSuccess) e = ensure(ch.sigma, nout * C * 8);
-				if (e == cudaSuccess) e = ensure(ch.region, nout * C);
-				if (e == cudaSuccess) e = cudaMemsetAsync(ch.data.p, 0, nout * C * 8, st);
+				e = cudaMemsetAsync(ch.data.p, 0, nout * C * 8, st);
 				if (e == cudaSuccess) e = cudaMemsetAsync(ch.sigma.p, 0, nout * C * 8, st);
 				if (e == cudaSuccess) e = cudaMemsetAsync(ch.region.p, 0, nout * C, st);
 				for (int i = 0; i < C && e == cudaSuccess; i++) {
@@ -3012,17 +3098,33 @@ int cat_build(pf_catalogue *c)
 						nv += 2 * n;
 						maxpix = std::max(maxpix, (int)std::min<size_t>(n, 1u << 30));
 					}
-					for (size_t q = 0; q < nk; q++) {
-						psf[(size_t)i * nk + q] = (float)G.psf[q];
-						psfrev[(size_t)i * nk + q] = (float)G.psf[nk - 1 - q];
-					}
 				}
 				flush(ch);
-				if (e == cudaSuccess) e = ensure(ch.psf32, psf.size() * 4);
-				if (e == cudaSuccess) e = cudaMemcpy(ch.psf32.p, psf.data(), psf.size() * 4, cudaMemcpyHostToDevice);
-				if (e == cudaSuccess) e = ensure(ch.psfrev32, psfrev.size() * 4);
-				if (e == cudaSuccess)
-					e = cudaMemcpy(ch.psfrev32.p, psfrev.data(), psfrev.size() * 4, cudaMemcpyHostToDevice);
+				// the chunk's PSFs and their reversals (FP32), through staging buffers
+				// too, as many galaxies per copy as fit
+				const size_t per_copy = std::max<size_t>(1, stage / (2 * nk * 4));
+				for (size_t g0 = 0; g0 < (size_t)C && e == cudaSuccess; g0 += per_copy) {
+					const size_t ng = std::min(per_copy, (size_t)C - g0);
+					if (2 * ng * nk * 4 > stage) {  // one PSF larger than a staging buffer
+						e = cudaErrorInvalidValue;
+						break;
+					}
+					float *hs = reinterpret_cast<float *>(hb.as<char>() + half * stage), *hr = hs + ng * nk;
+					for (size_t i = 0; i < ng; i++) {
+						const CatGalaxy &G = c->gal[ch.members[g0 + i]];
+						for (size_t q = 0; q < nk; q++) {
+							hs[i * nk + q] = (float)G.psf[q];
+							hr[i * nk + q] = (float)G.psf[nk - 1 - q];
+						}
+					}
+					e = cudaMemcpyAsync(ch.psf32.as<float>() + g0 * nk, hs, ng * nk * 4, cudaMemcpyHostToDevice, st);
+					if (e == cudaSuccess)
+						e = cudaMemcpyAsync(ch.psfrev32.as<float>() + g0 * nk, hr, ng * nk * 4, cudaMemcpyHostToDevice, st);
+					if (e == cudaSuccess) e = cudaEventRecord(done[half], st);
+					used[half] = true;
+					half ^= 1;
+					if (e == cudaSuccess && used[half]) e = cudaEventSynchronize(done[half]);
+				}
 			}
 			// the staging buffers are freed below: wait for their transfers
 			if (st) {
@@ -3053,7 +3155,7 @@ int cat_build(pf_catalogue *c)
 	PF_CUDA(cudaMemcpy(c->pad.p, pad.data(), pad.size() * sizeof(int2), cudaMemcpyHostToDevice));
 	PF_CUDA(ensure(c->dev, params.size() * sizeof(DevProfile)));
 	PF_CUDA(ensure(c->fprof, params.size() * sizeof(FProfile)));
-	PF_CUDA(ensure(c->lum, params.size() * PRO_SLOTS * sizeof(double)));
+	PF_CUDA(ensure(c->lum, params.size() * LUM_SLOTS * sizeof(double)));
 
 	// engine scratch and queue for the largest chunk, so nothing is
 	// reallocated while chunks are queued

@@ -342,19 +342,20 @@ PF_HD inline double lum_slot(const ProfileParams &p, int slot)
 	return profile_lum(q, q.kind == PK_CORESERSIC ? qgamma(0.5, 2 * q.nser) : 0.0, 0.0);
 }
 
-// The gamma quantiles of a Sersic or core-Sersic profile, which depend on
-// nser alone and are most of its scalars' cost: bn = qgamma(0.5, 2n) and,
-// for adjusted Sersic profiles, the quantiles behind rscale_switch
-// (qgamma(1 - n^2/2000, 2n)) and rscale_max (qgamma(0.9999, 2n)).  A host
-// caller keeps one per profile and reuses it while nser is unchanged; a
-// device prologue computes the three in parallel threads (nser_quantile).
-struct NserQuantiles {
-	double nser = -1;
-	double q_half = 0, q_switch = 0, q_max = 0;
-	bool has_half = false, has_switch = false, has_max = false;
+// Scalars of a profile that depend on its shape parameters alone, most of
+// the cost of a Sersic profile's prologue: the gamma quantiles (bn =
+// qgamma(0.5, 2n) and, for adjusted Sersic profiles, those behind
+// rscale_switch, qgamma(1 - n^2/2000, 2n), and rscale_max, qgamma(0.9999,
+// 2n)), d bn / d n and d ln L / d n (functions of nser), and the boxiness
+// factor r_box and d ln r_box / d B (functions of box).  A host caller keeps
+// one per profile and refills only what a changed nser or box invalidates;
+// every value comes from the same functions derive_profile uses without it.
+struct ShapeMemo {
+	double nser = -1, box = NAN;
+	double q_half = 0, q_switch = 0, q_max = 0, dbn_dn = 0, dlnL_dn = 0;
+	double r_box = 0, dlnI_dbox = 0;
+	bool has_half = false, has_switch = false, has_max = false, has_nser_terms = false, has_box = false;
 };
-
-constexpr int NSER_QUANTILES = 3;
 
 // Quantile k of p (0: bn, 1: rscale_switch's, 2: rscale_max's), or 0 where
 // derive_profile does not use it.
@@ -367,29 +368,59 @@ PF_HD inline double nser_quantile(const ProfileParams &p, int k)
 	return p.rscale_max == 0 ? qgamma(0.9999, 2 * p.nser) : 0.0;
 }
 
-// The quantiles of p from its NSER_QUANTILES nser_quantile values.
-PF_HD inline NserQuantiles nser_quantiles_from(const ProfileParams &p, const double *q)
+// r_box = pi B / (2 Beta(1/B, 1/B)), B = box + 2 (the boxiness factor of
+// the luminosity) and d ln r_box / d B.
+PF_HD inline double r_box_of(double b2) { return M_PI * b2 / (2 * beta_fn(1 / b2, 1 / b2)); }
+PF_HD inline double dln_rbox_dB(double B) { return 1.0 / B + (2.0 / (B * B)) * (digamma(1.0 / B) - digamma(2.0 / B)); }
+
+// b_n solves P(2n, b_n) = 1/2, so d b_n / d n = -2 (dP/da) / (dP/dx) at
+// (a, x) = (2n, b_n): dP/dx is the gamma density, dP/da a central difference
+// of P at fixed x (two P evaluations instead of two more quantile solves).
+PF_HD inline double dbn_dn_of(double nser, double bn)
 {
-	NserQuantiles c;
-	c.nser = p.nser;
-	c.q_half = q[0];
-	c.q_switch = q[1];
-	c.q_max = q[2];
-	c.has_half = c.has_switch = c.has_max = true;
-	return c;
+	const double a = 2 * nser, h = 1e-6 * a;
+	const double dP_da = (pgamma(bn, a + h) - pgamma(bn, a - h)) / (2 * h);
+	const double dP_dx = exp((a - 1) * log(bn) - bn - lgamma(a));
+	return -2 * dP_da / dP_dx;
 }
 
-// Fills (or keeps, for the same nser) the quantiles p needs.
-inline const NserQuantiles *nser_quantiles(NserQuantiles &c, const ProfileParams &p)
+// d ln L / d n of a Sersic profile, L = re^2 2 pi n Gamma(2n) e^bn / bn^(2n).
+PF_HD inline double sersic_dlnL_dn(double n, double bn, double dbn)
 {
-	if (p.kind != PK_SERSIC && p.kind != PK_CORESERSIC) return nullptr;
+	return 1.0 / n + 2.0 * digamma(2 * n) + dbn - 2.0 * log(bn) - 2.0 * n * dbn / bn;
+}
+
+// Fills (or keeps, for the same nser and box) what p needs; null for kinds
+// with nothing to keep.
+inline const ShapeMemo *shape_memo(ShapeMemo &c, const ProfileParams &p)
+{
+	if (!is_radial_kind(p.kind)) return nullptr;
 	if (!(c.nser == p.nser)) {
-		c = NserQuantiles();
+		const double box = c.box, r_box = c.r_box, dl = c.dlnI_dbox;
+		const bool hb = c.has_box;
+		c = ShapeMemo();
 		c.nser = p.nser;
+		c.box = box;
+		c.r_box = r_box;
+		c.dlnI_dbox = dl;
+		c.has_box = hb;
 	}
-	if (!c.has_half) {
-		c.q_half = nser_quantile(p, 0);
-		c.has_half = true;
+	if (!(c.box == p.box)) {
+		c.box = p.box;
+		c.r_box = r_box_of(p.box + 2);
+		c.dlnI_dbox = dln_rbox_dB(p.box + 2);
+		c.has_box = true;
+	}
+	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) {
+		if (!c.has_half) {
+			c.q_half = nser_quantile(p, 0);
+			c.has_half = true;
+		}
+		if (!c.has_nser_terms) {
+			c.dbn_dn = dbn_dn_of(p.nser, c.q_half);
+			c.dlnL_dn = sersic_dlnL_dn(p.nser, c.q_half, c.dbn_dn);
+			c.has_nser_terms = true;
+		}
 	}
 	if (p.kind == PK_SERSIC && p.adjust) {
 		if (!c.has_switch) {
@@ -404,21 +435,10 @@ inline const NserQuantiles *nser_quantiles(NserQuantiles &c, const ProfileParams
 	return &c;
 }
 
-// Prologue scratch per profile: its LUM_SLOTS luminosity evaluations, then
-// its NSER_QUANTILES quantiles.
-constexpr int PRO_SLOTS = LUM_SLOTS + NSER_QUANTILES;
-
-// Scratch slot `slot` of profile p (0 where p does not use it).
-PF_HD inline double pro_slot(const ProfileParams &p, int slot)
-{
-	if (slot < LUM_SLOTS) return slot < lum_slots(p.kind) ? lum_slot(p, slot) : 0.0;
-	return nser_quantile(p, slot - LUM_SLOTS);
-}
-
 // lum_pre (optional, lum_by_difference kinds): the profile's lum_slot values,
-// computed beforehand.  nq (optional): nser_quantiles of p.
+// computed beforehand.  nq (optional): shape_memo of p.
 PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, DevProfile &d,
-                                 const double *lum_pre = nullptr, const NserQuantiles *nq = nullptr)
+                                 const double *lum_pre = nullptr, const ShapeMemo *nq = nullptr)
 {
 	d.kind = p.kind;
 	d.target = p.convolve ? 0 : 1;
@@ -491,7 +511,7 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 	const double lum = (lum_pre && lum_by_difference(p.kind)) ? lum_pre[0] : profile_lum(p, d.bn, rscale);
 
 	double b2 = p.box + 2;
-	double r_box = M_PI * b2 / (2 * beta_fn(1 / b2, 1 / b2));
+	double r_box = nq ? nq->r_box : r_box_of(b2);
 	double lumtot = lum * p.axrat / r_box;
 	double ie = pow(10, -0.4 * (p.mag - g.magzero)) / lumtot;
 
@@ -575,27 +595,11 @@ PF_HD inline void derive_profile(const ProfileParams &p, const ModelGeom &g, Dev
 	// d log(flux_scale) / d parameter, used by the adjoint.
 	// flux_scale = sx sy 10^(-0.4(mag - mz)) r_box / (L axrat)
 	d.dlnI_dq = -1.0 / p.axrat;
-	{
-		// d ln r_box / dB with r_box = pi B / (2 Beta(1/B, 1/B))
-		double B = b2;
-		d.dlnI_dbox = 1.0 / B + (2.0 / (B * B)) * (digamma(1.0 / B) - digamma(2.0 / B));
-	}
-	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) {
-		// b_n solves P(2n, b_n) = 1/2, so d b_n / d n = -2 (dP/da) / (dP/dx) at
-		// (a, x) = (2n, b_n): dP/dx is the gamma density, dP/da a central
-		// difference of P at fixed x (two P evaluations instead of two more
-		// quantile solves)
-		const double a = 2 * p.nser, bn = d.bn, h = 1e-6 * a;
-		const double dP_da = (pgamma(bn, a + h) - pgamma(bn, a - h)) / (2 * h);
-		const double dP_dx = exp((a - 1) * log(bn) - bn - lgamma(a));
-		d.dbn_dn = -2 * dP_da / dP_dx;
-	}
+	d.dlnI_dbox = nq ? nq->dlnI_dbox : dln_rbox_dB(b2);
+	if (p.kind == PK_SERSIC || p.kind == PK_CORESERSIC) d.dbn_dn = nq ? nq->dbn_dn : dbn_dn_of(p.nser, d.bn);
 	if (p.kind == PK_SERSIC) {
-		// L = re^2 2 pi n Gamma(2n) e^bn / bn^(2n)
-		const double n = p.nser, bn = d.bn, dbn = d.dbn_dn;
 		d.dlnI_dp[0] = -2.0 / p.re;  // re
-		double dlnL_dn = 1.0 / n + 2.0 * digamma(2 * n) + dbn - 2.0 * log(bn) - 2.0 * n * dbn / bn;
-		d.dlnI_dp[1] = -dlnL_dn;     // nser
+		d.dlnI_dp[1] = -(nq ? nq->dlnL_dn : sersic_dlnL_dn(p.nser, d.bn, d.dbn_dn));  // nser
 	}
 	else if (p.kind == PK_MOFFAT) {
 		// L = rscale^2 pi / (con - 1), rscale = fwhm / (2 sqrt(2^(1/con) - 1))

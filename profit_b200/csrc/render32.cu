@@ -40,18 +40,27 @@ struct Tan {
 	T s[MAX_SHAPE + 1];
 };
 
-template <class T>
-__device__ __forceinline__ T t_exp(T x);
-template <>
-__device__ __forceinline__ float t_exp<float>(float x) { return expf(x); }
-template <>
-__device__ __forceinline__ double t_exp<double>(double x) { return exp(x); }
-template <class T>
-__device__ __forceinline__ T t_log(T x);
-template <>
-__device__ __forceinline__ float t_log<float>(float x) { return logf(x); }
-template <>
-__device__ __forceinline__ double t_log<double>(double x) { return log(x); }
+// FAST (FP32 only): the hardware approximations (ex2 / lg2 with one
+// multiply; a few ulp, growing with |x| for the exponential) instead of
+// CUDA's functions accurate to 1-2 ulp.  Used where only tangents are formed
+// (the recomputing adjoint): their per-pixel errors of ~1e-6 stay an order
+// below the gradient's accuracy bound, while the image values keep the
+// accurate functions.
+template <class T, bool FAST = false>
+__device__ __forceinline__ T t_exp(T x)
+{
+	if constexpr (sizeof(T) == 8) return exp(x);
+	else if constexpr (FAST) return __expf(x);
+	else return expf(x);
+}
+template <class T, bool FAST = false>
+__device__ __forceinline__ T t_log(T x)
+{
+	if constexpr (sizeof(T) == 8) return log(x);
+	// (subnormal arguments keep the accurate function)
+	else if constexpr (FAST) return x >= 1.17549435e-38f ? __logf(x) : logf(x);
+	else return logf(x);
+}
 template <class T>
 __device__ __forceinline__ T t_pow(T x, T y);
 template <>
@@ -82,63 +91,68 @@ __device__ __forceinline__ double qdiv<double>(double a, double b) { return a / 
 // x^y for x >= 0 given lx = ln x: exp(y lx), with pow's values at x = 0.
 // The profiles need ln x for their partials anyway, so a power costs one
 // exponential instead of pow's own logarithm and exponential.
-template <class T>
+template <class T, bool FAST = false>
 __device__ __forceinline__ T pow_ln(T x, T lx, T y)
 {
-	if (x > T(0)) return t_exp<T>(y * lx);
+	if (x > T(0)) return t_exp<T, FAST>(y * lx);
 	return y > T(0) ? T(0) : (y == T(0) ? T(1) : T(INFINITY));
 }
 
 // x^B for x >= 0 and a boxiness exponent B = 2 + box near 2, given lx = ln x:
 // x^2 exp((B - 2) lx).  The exponential's argument stays small, so the
 // rounding of lx is not amplified by |B lx| as in exp(B lx).
-template <class T>
+template <class T, bool FAST = false>
 __device__ __forceinline__ T pow_box(T x, T lx, T B)
 {
-	if (x > T(0)) return x * x * t_exp<T>((B - T(2)) * lx);
-	return pow_ln<T>(x, lx, B);
+	if (x > T(0)) return x * x * t_exp<T, FAST>((B - T(2)) * lx);
+	return pow_ln<T, FAST>(x, lx, B);
 }
 
 // ln x for x > 0, else 0 (every use multiplies it by a factor that is 0 there)
-template <class T>
+template <class T, bool FAST = false>
 __device__ __forceinline__ T ln_pos(T x)
 {
-	return x > T(0) ? t_log<T>(x) : T(0);
+	return x > T(0) ? t_log<T, FAST>(x) : T(0);
 }
 
 // Sersic: f = exp(-bn (base^(1/(n B)) - 1)), base = |x/re|^B + |y/re|^B.
 // Shape partials: s[0] = df/dre, s[1] = df/dnser (including dbn/dnser),
 // s[2] = df/dbox.
-template <class T>
+template <class T, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ Tan<T> sersic_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
 	const T B = (T)p.B, n = (T)p.nser, bn = (T)p.bn;
 	const T ire = (T)p.k[0], in = (T)p.k[1], iB = (T)p.inv_B;
 	const T u = fabs(xp) * ire, v = fabs(yp) * ire;
-	const T lu = ln_pos<T>(u), lv = ln_pos<T>(v);
-	T uB, vB;
+	T lu, lv, uB, vB;
 	if (B == T(2)) {
+		// ln u, ln v enter only the box partial here
+		lu = TAN ? ln_pos<T, FAST>(u) : T(0);
+		lv = TAN ? ln_pos<T, FAST>(v) : T(0);
 		uB = u * u;
 		vB = v * v;
 	}
 	else {
-		uB = pow_box<T>(u, lu, B);
-		vB = pow_box<T>(v, lv, B);
+		lu = ln_pos<T, FAST>(u);
+		lv = ln_pos<T, FAST>(v);
+		uB = pow_box<T, FAST>(u, lu, B);
+		vB = pow_box<T, FAST>(v, lv, B);
 	}
 	const T base = uB + vB;
 	if (!(base > T(0))) {
-		t.f = t_exp<T>(bn);
+		t.f = t_exp<T, FAST>(bn);
 		return t;
 	}
 	const T inv_nB = (T)p.inv_nB;
-	const T lnb = t_log<T>(base);
-	const T rf = t_exp<T>(lnb * inv_nB);
-	const T f = t_exp<T>(-bn * (rf - T(1)));
+	const T lnb = t_log<T, FAST>(base);
+	const T rf = t_exp<T, FAST>(lnb * inv_nB);
+	const T f = t_exp<T, FAST>(-bn * (rf - T(1)));
+	t.f = f;
+	if constexpr (!TAN) return t;
 	const T dfdrf = -bn * f;
 	const T h = dfdrf * rf * inv_nB;   // df/d ln(base)
 	const T g = qdiv<T>(h, base);      // df/dbase
-	t.f = f;
 	// dbase/dx' = B uB / x' (= 2 x' / re^2 at B = 2)
 	if (B == T(2)) {
 		t.fx = g * T(2) * xp * ire * ire;
@@ -156,27 +170,31 @@ __device__ __forceinline__ Tan<T> sersic_tan(const FProfile &p, T xp, T yp)
 
 // Boxy radius r = (|x'|^B + |y'|^B)^(1/B) (radial.h:93-102) and its partials
 // in x', y' and B.
-template <class T>
+template <class T, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ void boxy_radius(const FProfile &p, T xp, T yp, T &r, T &drdx, T &drdy, T &drdB)
 {
 	const T B = (T)p.B, ax = fabs(xp), ay = fabs(yp);
-	const T lx = ln_pos<T>(ax), ly = ln_pos<T>(ay);
+	drdx = drdy = drdB = T(0);
 	if (B == T(2)) {
 		const T S = xp * xp + yp * yp;
 		r = t_sqrt<T>(S);
+		if constexpr (!TAN) return;
+		const T lx = ln_pos<T, FAST>(ax), ly = ln_pos<T, FAST>(ay);
 		const T ir = r > T(0) ? qdiv<T>(T(1), r) : T(0);
 		drdx = xp * ir;
 		drdy = yp * ir;
 		// r ((x'^2 ln|x'| + y'^2 ln|y'|) / (2 S) - ln S / 4)
-		drdB = S > T(0) ? r * ((ax * ax * lx + ay * ay * ly) * ir * ir * T(0.5) - t_log<T>(S) * T(0.25)) : T(0);
+		drdB = S > T(0) ? r * ((ax * ax * lx + ay * ay * ly) * ir * ir * T(0.5) - t_log<T, FAST>(S) * T(0.25)) : T(0);
 	}
 	else {
-		const T xB = pow_box<T>(ax, lx, B), yB = pow_box<T>(ay, ly, B);
+		const T lx = ln_pos<T, FAST>(ax), ly = ln_pos<T, FAST>(ay);
+		const T xB = pow_box<T, FAST>(ax, lx, B), yB = pow_box<T, FAST>(ay, ly, B);
 		const T S = xB + yB;
 		const T iB = (T)p.inv_B;
-		const T lS = ln_pos<T>(S);
+		const T lS = ln_pos<T, FAST>(S);
 		// S^(1/B) = sqrt(S) S^(1/B - 1/2), the second factor's exponent small
-		r = S > T(0) ? t_sqrt<T>(S) * t_exp<T>(lS * (T)p.box_e) : T(0);
+		r = S > T(0) ? t_sqrt<T>(S) * t_exp<T, FAST>(lS * (T)p.box_e) : T(0);
+		if constexpr (!TAN) return;
 		const T iS = S > T(0) ? qdiv<T>(T(1), S) : T(0);
 		drdx = (r > T(0) && xp != T(0)) ? qdiv<T>(xB * iS * r, xp) : T(0);
 		drdy = (r > T(0) && yp != T(0)) ? qdiv<T>(yB * iS * r, yp) : T(0);
@@ -185,7 +203,7 @@ __device__ __forceinline__ void boxy_radius(const FProfile &p, T xp, T yp, T &r,
 }
 
 // Fills fx, fy and df/dbox (slot ns) from df/dr.
-template <class T>
+template <class T, bool FAST = false>
 __device__ __forceinline__ void radial_chain(Tan<T> &t, T fr, T drdx, T drdy, T drdB, int ns)
 {
 	t.fx = fr * drdx;
@@ -195,19 +213,20 @@ __device__ __forceinline__ void radial_chain(Tan<T> &t, T fr, T drdx, T drdy, T 
 
 // Moffat: f = (1 + (r/rscale)^2)^-con.  s[0] = df/dfwhm, s[1] = df/dcon,
 // s[2] = df/dbox.
-template <class T>
+template <class T, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ Tan<T> moffat_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
 	const T irs = (T)p.k[0], con = (T)p.con;
 	T r, drdx, drdy, drdB;
-	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	boxy_radius<T, FAST, TAN>(p, xp, yp, r, drdx, drdy, drdB);
 	const T rf = r * irs;
 	const T q = T(1) + rf * rf;
-	const T lq = t_log<T>(q);
-	const T f = t_exp<T>(-con * lq);
+	const T lq = t_log<T, FAST>(q);
+	const T f = t_exp<T, FAST>(-con * lq);
 	const T dfdrf = qdiv<T>(-T(2) * con * rf * f, q);
 	t.f = f;
+	if constexpr (!TAN) return t;
 	radial_chain<T>(t, dfdrf * irs, drdx, drdy, drdB, 2);
 	t.s[0] = dfdrf * (-rf) * (T)p.a;           // a holds 1/fwhm for Moffat
 	t.s[1] = -lq * f + dfdrf * (-rf) * (T)p.b;  // b holds dln(rscale)/dcon
@@ -216,21 +235,22 @@ __device__ __forceinline__ Tan<T> moffat_tan(const FProfile &p, T xp, T yp)
 
 // Ferrer: f = (1 - (r/rout)^(2-b))^a inside rout (ferrer.cpp:50-60).
 // s[0] = df/drout, s[1] = df/da, s[2] = df/db, s[3] = df/dbox.
-template <class T>
+template <class T, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ Tan<T> ferrer_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
 	T r, drdx, drdy, drdB;
-	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	boxy_radius<T, FAST, TAN>(p, xp, yp, r, drdx, drdy, drdB);
 	const T irout = (T)p.k[0], a = (T)p.a, e = T(2) - (T)p.b;
 	const T rf = r * irout;
 	if (!(rf < T(1))) return t;
-	const T lrf = ln_pos<T>(rf);
-	const T rfe = pow_ln<T>(rf, lrf, e);
+	const T lrf = ln_pos<T, FAST>(rf);
+	const T rfe = pow_ln<T, FAST>(rf, lrf, e);
 	const T g = T(1) - rfe;
-	const T lg = ln_pos<T>(g);
-	const T f = pow_ln<T>(g, lg, a);
+	const T lg = ln_pos<T, FAST>(g);
+	const T f = pow_ln<T, FAST>(g, lg, a);
 	t.f = f;
+	if constexpr (!TAN) return t;
 	if (!(g > T(0)) || !(r > T(0))) return t;
 	const T ig = qdiv<T>(T(1), g);
 	const T fr = -a * e * f * rfe * ig * qdiv<T>(T(1), r);
@@ -243,23 +263,24 @@ __device__ __forceinline__ Tan<T> ferrer_tan(const FProfile &p, T xp, T yp)
 
 // King: f = ((1 + (r/rc)^2)^(-1/a) - (1 + (rt/rc)^2)^(-1/a))^a inside rt
 // (king.cpp:51-59).  s[0] = df/drc, s[1] = df/drt, s[2] = df/da, s[3] = df/dbox.
-template <class T>
+template <class T, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ Tan<T> king_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
 	T r, drdx, drdy, drdB;
-	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	boxy_radius<T, FAST, TAN>(p, xp, yp, r, drdx, drdy, drdB);
 	const T rc = (T)p.rc, rt = (T)p.rt, a = (T)p.a, kt = (T)p.king_t;
 	if (!(r < rt)) return t;
 	const T ia = (T)p.k[0], irc = (T)p.k[1];
 	const T X = T(1) + (r * irc) * (r * irc);
-	const T lX = t_log<T>(X);
-	const T u = t_exp<T>(-lX * ia);
+	const T lX = t_log<T, FAST>(X);
+	const T u = t_exp<T, FAST>(-lX * ia);
 	const T D = u - kt;
 	// D <= 0 only by rounding at r ~ rt, where pow keeps its own sign rules
-	const T lD = ln_pos<T>(D);
-	const T f = D > T(0) ? t_exp<T>(a * lD) : t_pow<T>(D, a);
+	const T lD = ln_pos<T, FAST>(D);
+	const T f = D > T(0) ? t_exp<T, FAST>(a * lD) : t_pow<T>(D, a);
 	t.f = f;
+	if constexpr (!TAN) return t;
 	if (!(D > T(0))) return t;
 	const T iX = qdiv<T>(T(1), X), iY = (T)p.k[2];
 	const T k2 = T(2) * ia * irc * irc;
@@ -280,25 +301,26 @@ __device__ __forceinline__ Tan<T> king_tan(const FProfile &p, T xp, T yp)
 // (1/h1 - 1/h2) base), base = log(1 + exp(a (r - rb)))/a, or r - rb where
 // a (r - rb) >= 40.  s[0] = df/dh1, s[1] = df/dh2, s[2] = df/drb, s[3] = df/da,
 // s[4] = df/dbox.
-template <class T>
+template <class T, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ Tan<T> brokenexp_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
 	T r, drdx, drdy, drdB;
-	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	boxy_radius<T, FAST, TAN>(p, xp, yp, r, drdx, drdy, drdB);
 	const T a = (T)p.a, z = r - (T)p.rb;
 	const T ih1 = (T)p.k[0], ih2 = (T)p.k[1], ia = (T)p.k[2];
 	const T expo = ih1 - ih2;
 	T base = z, dbase_dr = T(1), dbase_da = T(0);
 	if (a * z < T(40)) {
-		const T ez = t_exp<T>(a * z);
-		base = t_log<T>(T(1) + ez) * ia;
+		const T ez = t_exp<T, FAST>(a * z);
+		base = t_log<T, FAST>(T(1) + ez) * ia;
 		const T sig = qdiv<T>(ez, T(1) + ez);
 		dbase_dr = sig;
 		dbase_da = (z * sig - base) * ia;
 	}
-	const T f = t_exp<T>(-r * ih1 + expo * base);
+	const T f = t_exp<T, FAST>(-r * ih1 + expo * base);
 	t.f = f;
+	if constexpr (!TAN) return t;
 	radial_chain<T>(t, f * (-ih1 + expo * dbase_dr), drdx, drdy, drdB, 4);
 	t.s[0] = f * (r - base) * ih1 * ih1;
 	t.s[1] = f * base * ih2 * ih2;
@@ -311,27 +333,28 @@ __device__ __forceinline__ Tan<T> brokenexp_tan(const FProfile &p, T xp, T yp)
 // exp(-bn ((r^a + rb^a)/re^a)^(1/(n a))).  s[0] = df/dre, s[1] = df/drb,
 // s[2] = df/dnser (including dbn/dnser), s[3] = df/da, s[4] = df/db,
 // s[5] = df/dbox.
-template <class T>
+template <class T, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ Tan<T> coresersic_tan(const FProfile &p, T xp, T yp)
 {
 	Tan<T> t = {};
 	T r, drdx, drdy, drdB;
-	boxy_radius<T>(p, xp, yp, r, drdx, drdy, drdB);
+	boxy_radius<T, FAST, TAN>(p, xp, yp, r, drdx, drdy, drdB);
 	const T a = (T)p.a, b = (T)p.b, rb = (T)p.rb, re = (T)p.re, n = (T)p.nser, bn = (T)p.bn;
 	const T ia = (T)p.k[0], in = (T)p.k[1];
-	const T lr = ln_pos<T>(r), lrb = (T)p.k[2], lre = (T)p.k[3];
-	const T ra = pow_ln<T>(r, lr, a), rba = (T)p.k[4], irea = (T)p.k[5];
+	const T lr = ln_pos<T, FAST>(r), lrb = (T)p.k[2], lre = (T)p.k[3];
+	const T ra = pow_ln<T, FAST>(r, lr, a), rba = (T)p.k[4], irea = (T)p.k[5];
 	// (r/rb)^-a, infinite at r = 0 for a > 0 as pow gives it
-	const T rho = r > T(0) ? t_exp<T>(-a * (lr - lrb)) : pow_ln<T>(T(0), T(0), -a);
+	const T rho = r > T(0) ? t_exp<T, FAST>(-a * (lr - lrb)) : pow_ln<T, FAST>(T(0), T(0), -a);
 	const T A = T(1) + rho;
 	const T Q = (ra + rba) * irea;
-	const T lnQ = t_log<T>(Q);
+	const T lnQ = t_log<T, FAST>(Q);
 	const T ina = (T)p.k[6];
-	const T W = t_exp<T>(lnQ * ina);
-	const T lnA = t_log<T>(A);
+	const T W = t_exp<T, FAST>(lnQ * ina);
+	const T lnA = t_log<T, FAST>(A);
 	const T ba = b * ia;
-	const T f = t_exp<T>(ba == T(0) ? -bn * W : ba * lnA - bn * W);
+	const T f = t_exp<T, FAST>(ba == T(0) ? -bn * W : ba * lnA - bn * W);
 	t.f = f;
+	if constexpr (!TAN) return t;
 	if (!(r > T(0)) || !(f > T(0))) return t;
 	const T ir = qdiv<T>(T(1), r), irb = qdiv<T>(T(1), rb), iA = qdiv<T>(T(1), A), iQ = qdiv<T>(T(1), Q);
 	const T dA_dr = -a * rho * ir, dA_drb = a * rho * irb, dA_da = -rho * (lr - lrb);
@@ -352,27 +375,27 @@ __device__ __forceinline__ Tan<T> coresersic_tan(const FProfile &p, T xp, T yp)
 // AK (all kinds): false compiles only the Sersic and Moffat tangents, the
 // kinds most models use, which keeps those kernels' code and registers as
 // small as before the other kinds had gradients.
-template <class T, bool AK>
+template <class T, bool AK, bool FAST = false, bool TAN = true>
 __device__ __forceinline__ Tan<T> eval_tan(const FProfile &p, T xp, T yp)
 {
-	if (p.kind == PK_SERSIC) return sersic_tan<T>(p, xp, yp);
-	if (p.kind == PK_MOFFAT) return moffat_tan<T>(p, xp, yp);
+	if (p.kind == PK_SERSIC) return sersic_tan<T, FAST, TAN>(p, xp, yp);
+	if (p.kind == PK_MOFFAT) return moffat_tan<T, FAST, TAN>(p, xp, yp);
 	if constexpr (AK) {
 		switch (p.kind) {
-		case PK_FERRER: return ferrer_tan<T>(p, xp, yp);
-		case PK_CORESERSIC: return coresersic_tan<T>(p, xp, yp);
-		case PK_KING: return king_tan<T>(p, xp, yp);
-		case PK_BROKENEXP: return brokenexp_tan<T>(p, xp, yp);
+		case PK_FERRER: return ferrer_tan<T, FAST, TAN>(p, xp, yp);
+		case PK_CORESERSIC: return coresersic_tan<T, FAST, TAN>(p, xp, yp);
+		case PK_KING: return king_tan<T, FAST, TAN>(p, xp, yp);
+		case PK_BROKENEXP: return brokenexp_tan<T, FAST, TAN>(p, xp, yp);
 		default: break;
 		}
 	}
 	return Tan<T>{};
 }
 
-template <class T, bool AK>
+template <class T, bool AK, bool FAST = false>
 __device__ __forceinline__ T eval_val(const FProfile &p, T xp, T yp)
 {
-	return eval_tan<T, AK>(p, xp, yp).f;
+	return eval_tan<T, AK, FAST, false>(p, xp, yp).f;
 }
 
 // Tangent slots the kernels of a kind set carry.
@@ -724,7 +747,7 @@ __device__ __forceinline__ void adjoint_points(const FProfile &p, const SubItem 
 		const T dx = (T)x, dy = (T)y;
 		const T xp = dx * cos_a + dy * sin_a;
 		const T yp = -dx * sin_q + dy * cos_q;
-		Tan<T> t = eval_tan<T, AK>(p, xp, yp);
+		Tan<T> t = eval_tan<T, AK, true>(p, xp, yp);  // tangents only: fast functions
 		tan_to_j<ntk<AK>()>(to_float<T>(t), (float)xp, (float)yp, 1.0f, sums);
 	}
 }
@@ -888,7 +911,7 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 		const double y = half_ybin + j * sx, x = half_xbin + i * sy;
 		float xp, yp;
 		if (pixel_decision32(p, x, y, xp, yp) != PD_DIRECT) continue;
-		Tan<float> t = eval_tan<float, AK>(p, xp, yp);
+		Tan<float> t = eval_tan<float, AK, true>(p, xp, yp);
 		tan_to_j<NT>(t, xp, yp, gv, acc);
 	}
 	__shared__ double s_red[NT][8];
@@ -967,7 +990,7 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32_listed(const FProfile 
 				const double y = half_ybin + j * sx, x = half_xbin + i * sy;
 				float xp, yp;
 				if (pixel_decision32(p, x, y, xp, yp) != PD_DIRECT) continue;
-				Tan<float> t = eval_tan<float, AK>(p, xp, yp);
+				Tan<float> t = eval_tan<float, AK, true>(p, xp, yp);
 				tan_to_j<NT>(t, xp, yp, gv, acc);
 			}
 #pragma unroll
@@ -1100,6 +1123,12 @@ __device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigne
 	if (g.ctrl_out)
 		for (int i = threadIdx.x; i < g.ctrl_words; i += blockDim.x) g.ctrl_out[i] = __ldcg(g.ctrl_in + i);
 	if (threadIdx.x == 0) *ticket = 0;
+	if (g.seq_out) {
+		// the results reach host memory before the word that announces them
+		__threadfence_system();
+		__syncthreads();
+		if (threadIdx.x == 0) *reinterpret_cast<volatile unsigned *>(g.seq_out) = __ldcg(g.seq_in);
+	}
 }
 
 // sum over pixels of g(pixel) * J_k(pixel) for each radial profile:
@@ -1783,27 +1812,10 @@ __device__ __forceinline__ ProfileParams proposal_params(const ProfileParams *__
 	return pp;
 }
 
-// One thread per (proposal, profile, quantile): the gamma quantiles of the
-// Sersic and core-Sersic profiles (nser_quantile), the serial part of their
-// scalars, three at a time instead of one after another.
-__global__ void k_batch_quantiles(const ProfileParams *__restrict__ tmpl, int nprof, int batch,
-                                  const int *__restrict__ ref_profile, const int *__restrict__ ref_offset, int nrefs,
-                                  const double *__restrict__ values, double *__restrict__ quant)
-{
-	pdl_enter();
-	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= (long long)batch * nprof * NSER_QUANTILES) return;
-	const int k = (int)(t % NSER_QUANTILES), bp = (int)(t / NSER_QUANTILES);
-	const int b = bp / nprof, p = bp - b * nprof;
-	const ProfileParams pp = proposal_params(tmpl, p, b, ref_profile, ref_offset, nrefs, values);
-	quant[t] = params_valid(pp) ? nser_quantile(pp, k) : 0.0;
-}
-
-// quant (optional): k_batch_quantiles' output.
 __global__ void k_batch_prologue(const ProfileParams *__restrict__ tmpl, int nprof, int batch,
                                  const int *__restrict__ ref_profile, const int *__restrict__ ref_offset, int nrefs,
-                                 const double *__restrict__ values, ModelGeom g, const double *__restrict__ quant,
-                                 DevProfile *__restrict__ dev, FProfile *__restrict__ fprof, int *__restrict__ invalid)
+                                 const double *__restrict__ values, ModelGeom g, DevProfile *__restrict__ dev,
+                                 FProfile *__restrict__ fprof, int *__restrict__ invalid)
 {
 	pdl_enter();
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1815,13 +1827,7 @@ __global__ void k_batch_prologue(const ProfileParams *__restrict__ tmpl, int npr
 		pp.kind = PK_NULL;
 	}
 	DevProfile d;
-	if (quant) {
-		const NserQuantiles nq = nser_quantiles_from(pp, quant + (size_t)t * NSER_QUANTILES);
-		derive_profile(pp, g, d, nullptr, &nq);
-	}
-	else {
-		derive_profile(pp, g, d);
-	}
+	derive_profile(pp, g, d);
 	dev[t] = d;
 	fprof[t] = to_fprofile(d, pp);
 }
@@ -1841,19 +1847,12 @@ __global__ void k_batch_gradient(const DevProfile *__restrict__ dev, int nprof, 
 
 cudaError_t launch_batch_prologue(const ProfileParams *tmpl, int nprof, int batch, const int *ref_profile,
                                   const int *ref_offset, int nrefs, const double *values, const ModelGeom &g,
-                                  double *quant, DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s)
+                                  DevProfile *dev, FProfile *fprof, int *invalid, cudaStream_t s)
 {
 	int n = batch * nprof;
-	if (quant) {
-		const long long nq = (long long)n * NSER_QUANTILES;
-		cudaError_t e = launch_pdl(k_batch_quantiles, dim3((unsigned)((nq + 127) / 128)), dim3(128), 0, s, tmpl, nprof,
-		                           batch, ref_profile, ref_offset, nrefs, values, quant);
-		note_launches(1);
-		if (e != cudaSuccess) return e;
-	}
 	note_launches(1);
 	return launch_pdl(k_batch_prologue, dim3((n + 127) / 128), dim3(128), 0, s, tmpl, nprof, batch, ref_profile,
-	                  ref_offset, nrefs, values, g, (const double *)quant, dev, fprof, invalid);
+	                  ref_offset, nrefs, values, g, dev, fprof, invalid);
 }
 
 cudaError_t launch_batch_gradient(const DevProfile *dev, int nprof, int batch, const int *ref_profile,
@@ -1879,9 +1878,10 @@ __global__ void k_cat_lum(const ProfileParams *__restrict__ params, int n, doubl
 {
 	pdl_enter();
 	const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-	if (t >= (long long)n * PRO_SLOTS) return;
-	const int pi = (int)(t / PRO_SLOTS), slot = (int)(t - (long long)pi * PRO_SLOTS);
-	lum[t] = pro_slot(params[pi], slot);
+	if (t >= (long long)n * LUM_SLOTS) return;
+	const int pi = (int)(t / LUM_SLOTS), slot = (int)(t - (long long)pi * LUM_SLOTS);
+	const ProfileParams pp = params[pi];
+	if (slot < lum_slots(pp.kind)) lum[t] = lum_slot(pp, slot);
 }
 
 __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const int2 *__restrict__ pad, int n,
@@ -1895,14 +1895,7 @@ __global__ void k_cat_prologue(const ProfileParams *__restrict__ params, const i
 	g.offx = pad[t].x;
 	g.offy = pad[t].y;
 	DevProfile d;
-	if (lum) {
-		const double *pl = lum + (size_t)t * PRO_SLOTS;
-		const NserQuantiles nq = nser_quantiles_from(pp, pl + LUM_SLOTS);
-		derive_profile(pp, g, d, pl, &nq);
-	}
-	else {
-		derive_profile(pp, g, d);
-	}
+	derive_profile(pp, g, d, lum ? lum + (size_t)t * LUM_SLOTS : nullptr);
 	dev[t] = d;
 	fprof[t] = to_fprofile(d, pp);
 }
@@ -1930,7 +1923,7 @@ cudaError_t launch_cat_prologue(const ProfileParams *params, const int2 *pad, in
 {
 	cudaError_t e = cudaSuccess;
 	if (lum) {
-		const long long nt = (long long)n * PRO_SLOTS;
+		const long long nt = (long long)n * LUM_SLOTS;
 		e = launch_pdl(k_cat_lum, dim3((unsigned)((nt + 127) / 128)), dim3(128), 0, s, params, n, lum);
 		note_launches(1);
 		if (e != cudaSuccess) return e;
