@@ -302,4 +302,28 @@ __device__ __forceinline__ T warp_sum(T v)
 	return v;
 }
 
+// Sums of N <= 16 values over the warp with 16 shuffles instead of 5 per
+// value: at each halving step a lane keeps one half of its values and adds
+// the partner's copy of that half.  Returns, in lanes 2m and 2m + 1, the
+// warp's sum of value m (zero for m >= N).
+template <int N, class T>
+__device__ __forceinline__ T warp_sums_spread(const T (&v)[N], int lane)
+{
+	static_assert(N <= 16, "up to 16 values");
+	T a[16];
+#pragma unroll
+	for (int i = 0; i < 16; i++) a[i] = i < N ? v[i] : T(0);
+#pragma unroll
+	for (int h = 8; h >= 1; h >>= 1) {
+		const bool upper = lane & (2 * h);  // this lane keeps values h .. 2h-1 of the current block
+#pragma unroll
+		for (int i = 0; i < h; i++) {
+			const T keep = upper ? a[i + h] : a[i];
+			const T give = upper ? a[i] : a[i + h];
+			a[i] = keep + __shfl_xor_sync(0xffffffffu, give, 2 * h);
+		}
+	}
+	return a[0] + __shfl_xor_sync(0xffffffffu, a[0], 1);
+}
+
 }  // namespace pf

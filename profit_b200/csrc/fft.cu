@@ -22,7 +22,10 @@
 //    and written only where the crop needs them (plus the unconvolved image).
 // The 1-D FFT is a self-sorting Stockham iteration (Govindaraju et al., "High
 // performance discrete Fourier transforms on graphics processors", SC 2008),
-// radices 2, 3, 4, 5, twiddles from a table built once per length.
+// radices 2, 3, 4, 5 and their pairwise products up to 16 (a composite
+// radix's butterfly is two Cooley-Tukey steps in one thread's registers, so
+// two stages cost one exchange through shared memory), twiddles from a table
+// built once per length.
 #include <cmath>
 #include <map>
 #include <mutex>
@@ -140,6 +143,81 @@ __device__ __forceinline__ void small_dft(C *v, T sign)
 	}
 }
 
+// Roots of unity exp(-2 pi i m / Q) for the composite radices (Q <= 16,
+// m < Q), filled from long double values on first use on each device.
+__constant__ double2 c_roots64[17][16];
+__constant__ float2 c_roots32[17][16];
+
+template <class C>
+__device__ __forceinline__ C root_of(int Q, int m);
+template <>
+__device__ __forceinline__ double2 root_of<double2>(int Q, int m) { return c_roots64[Q][m]; }
+template <>
+__device__ __forceinline__ float2 root_of<float2>(int Q, int m) { return c_roots32[Q][m]; }
+
+// DFT of size Q = R1 R2 on v (input index r = R2 r1 + r2) into X (output
+// index s = s1 + R1 s2): R2 transforms of size R1, the twiddles
+// exp(-+2 pi i r2 s1 / Q), then R1 transforms of size R2.
+template <int R1, int R2, class T, class C>
+__device__ __forceinline__ void fused_dft(const C (&v)[R1 * R2], C (&X)[R1 * R2], T sign)
+{
+	constexpr int Q = R1 * R2;
+	C y[R2][R1];
+#pragma unroll
+	for (int r2 = 0; r2 < R2; r2++) {
+#pragma unroll
+		for (int r1 = 0; r1 < R1; r1++) y[r2][r1] = v[R2 * r1 + r2];
+		small_dft<R1, T, C>(y[r2], sign);
+	}
+#pragma unroll
+	for (int r2 = 1; r2 < R2; r2++)
+#pragma unroll
+		for (int s1 = 1; s1 < R1; s1++) {
+			C w = root_of<C>(Q, r2 * s1);
+			w.y *= sign;
+			y[r2][s1] = cmul(y[r2][s1], w);
+		}
+#pragma unroll
+	for (int s1 = 0; s1 < R1; s1++) {
+		C t[R2];
+#pragma unroll
+		for (int r2 = 0; r2 < R2; r2++) t[r2] = y[r2][s1];
+		small_dft<R2, T, C>(t, sign);
+#pragma unroll
+		for (int s2 = 0; s2 < R2; s2++) X[s1 + R1 * s2] = t[s2];
+	}
+}
+
+// One Stockham stage of composite radix Q = R1 R2 over COLS interleaved
+// vectors, the same data movement as fft_stage with the butterfly computed
+// by fused_dft.
+template <int R1, int R2, int COLS, class T, class C>
+__device__ __forceinline__ void fft_stage_fused(const C *in, C *out, const C *stw, int nb, int ns, unsigned magic,
+                                                int tstep, bool inverse)
+{
+	constexpr int Q = R1 * R2;
+	const T sign = inverse ? T(-1) : T(1);
+	for (int t = threadIdx.x; t < nb * COLS; t += blockDim.x) {
+		const int j = t / COLS, c = t - j * COLS;
+		const int q = ns == 1 ? j : (int)__umulhi((unsigned)j, magic);
+		const int k = j - q * ns;
+		C v[Q];
+#pragma unroll
+		for (int r = 0; r < Q; r++) v[r] = in[(j + r * nb) * COLS + c];
+#pragma unroll
+		for (int r = 1; r < Q; r++) {
+			C w = stw[r * k * tstep];
+			if (inverse) w.y = -w.y;
+			v[r] = cmul(v[r], w);
+		}
+		C X[Q];
+		fused_dft<R1, R2, T, C>(v, X, sign);
+		const int idx = (j - k) * Q + k;
+#pragma unroll
+		for (int r = 0; r < Q; r++) out[(idx + r * ns) * COLS + c] = X[r];
+	}
+}
+
 // One radix-R Stockham stage over COLS interleaved vectors (element t of
 // vector c at buf[t * COLS + c]); stw: twiddles exp(-2 pi i t / n) in shared
 // memory.  Butterfly j = q ns + k reads in[j + r nb] and writes
@@ -183,7 +261,14 @@ __device__ __forceinline__ C *fft_block(C *a, C *b, const FftPlan &plan, const C
 		case 2: fft_stage<2, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
 		case 3: fft_stage<3, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
 		case 4: fft_stage<4, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
-		default: fft_stage<5, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 5: fft_stage<5, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 6: fft_stage_fused<2, 3, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 8: fft_stage_fused<2, 4, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 9: fft_stage_fused<3, 3, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 10: fft_stage_fused<2, 5, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 12: fft_stage_fused<3, 4, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		case 15: fft_stage_fused<3, 5, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
+		default: fft_stage_fused<4, 4, COLS, T, C>(in, out, stw, nb, ns, mg, ts, inverse); break;
 		}
 		__syncthreads();
 		C *tmp = in;
@@ -444,30 +529,44 @@ void fft_plan_stages(FftPlan &plan)
 	}
 }
 
-static bool factor_235(int n, FftPlan &plan)
+bool fft_factor(int n, FftPlan &plan)
 {
 	plan.n = n;
 	plan.nstages = 0;
+	int c[6] = {0, 0, 0, 0, 0, 0};  // multiplicity of the primes 2, 3, 5
 	int m = n;
-	while (m % 4 == 0 && plan.nstages < FFT_MAX_STAGES) {
-		plan.radix[plan.nstages++] = 4;
-		m /= 4;
-	}
-	const int rs[3] = {2, 3, 5};
-	for (int r : rs)
-		while (m % r == 0 && plan.nstages < FFT_MAX_STAGES) {
-			plan.radix[plan.nstages++] = r;
-			m /= r;
+	for (int p : {2, 3, 5})
+		while (m > 1 && m % p == 0) {
+			c[p]++;
+			m /= p;
 		}
+	if (m != 1 || n < 2) return false;
+	auto push = [&](int r) {
+		if (plan.nstages < FFT_MAX_STAGES) plan.radix[plan.nstages++] = r;
+	};
+	// pairs first (one register butterfly for two stages), then what is left
+	while (c[5] && c[3]) { push(15); c[5]--; c[3]--; }
+	while (c[5] && c[2]) { push(10); c[5]--; c[2]--; }
+	while (c[3] >= 2) { push(9); c[3] -= 2; }
+	while (c[3] && c[2] >= 2) { push(12); c[3]--; c[2] -= 2; }
+	while (c[3] && c[2]) { push(6); c[3]--; c[2]--; }
+	while (c[2] >= 4) { push(16); c[2] -= 4; }
+	while (c[2] >= 3) { push(8); c[2] -= 3; }
+	while (c[2] >= 2) { push(4); c[2] -= 2; }
+	while (c[5]) { push(5); c[5]--; }
+	while (c[3]) { push(3); c[3]--; }
+	while (c[2]) { push(2); c[2]--; }
 	fft_plan_stages(plan);
-	return m == 1;
+	int prod = 1;
+	for (int s = 0; s < plan.nstages; s++) prod *= plan.radix[s];
+	return prod == n;
 }
 
 int fft_good_size(int need)
 {
 	for (int n = (need + 1) & ~1;; n += 2) {
 		FftPlan p;
-		if (factor_235(n, p)) return n;
+		if (fft_factor(n, p)) return n;
 	}
 }
 
@@ -509,7 +608,7 @@ static int sm_count()
 // butterfly of the widest stage (n / smallest radix), in whole warps.
 static int fft_threads(const FftPlan &plan, int cols)
 {
-	int rmin = 5;
+	int rmin = 16;
 	for (int s = 0; s < plan.nstages; s++) rmin = plan.radix[s] < rmin ? plan.radix[s] : rmin;
 	int t = (plan.n / rmin) * cols;
 	t = (t + 31) / 32 * 32;
@@ -564,13 +663,39 @@ static cudaError_t cols_any(typename Cx<T>::type *spec, int spec_ld, int ncols, 
 	}
 }
 
+// The composite radices' roots of unity in constant memory, once per device.
+static cudaError_t ensure_roots()
+{
+	static std::mutex mu;
+	static bool done[64] = {};
+	int dev = 0;
+	cudaError_t e = cudaGetDevice(&dev);
+	if (e != cudaSuccess) return e;
+	std::lock_guard<std::mutex> g(mu);
+	if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+	static double2 r64[17][16];
+	static float2 r32[17][16];
+	for (int Q = 1; Q <= 16; Q++)
+		for (int m = 0; m < 16; m++) {
+			const long double ang = -2.0L * 3.14159265358979323846264338327950288L * (long double)(m % Q) / (long double)Q;
+			r64[Q][m] = make_double2((double)cosl(ang), (double)sinl(ang));
+			r32[Q][m] = make_float2((float)cosl(ang), (float)sinl(ang));
+		}
+	e = cudaMemcpyToSymbol(c_roots64, r64, sizeof(r64));
+	if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_roots32, r32, sizeof(r32));
+	if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+	return e;
+}
+
 template <class T>
 cudaError_t FftConv<T>::setup(int M_, int N_)
 {
+	cudaError_t re = ensure_roots();
+	if (re != cudaSuccess) return re;
 	if (M_ == M && N_ == N && tw_m && tw_n) return cudaSuccess;
 	M = M_;
 	N = N_;
-	if (!factor_235(M, plan_m) || !factor_235(N, plan_n) || (M & 1) || (N & 1)) return cudaErrorInvalidValue;
+	if (!fft_factor(M, plan_m) || !fft_factor(N, plan_n) || (M & 1) || (N & 1)) return cudaErrorInvalidValue;
 	if (N > FFT_MAX_LEN || M > FFT_MAX_LEN) return cudaErrorInvalidValue;
 	tw_m = twiddles<T>(M);
 	tw_n = twiddles<T>(N);

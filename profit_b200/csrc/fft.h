@@ -16,7 +16,10 @@ constexpr size_t FFT_SMEM_BYTES = 227 * 1024;
 // Stockham stages of a length-n transform: stage s has radix R = radix[s],
 // ns[s] = product of the earlier radices, nb[s] = n / R butterflies and
 // twiddle stride tstep[s] = n / (ns R); j / ns = umulhi(j, ns_magic) for
-// j < 2^16 (ns_magic = ceil(2^32 / ns), unused when ns = 1).
+// j < 2^16 (ns_magic = ceil(2^32 / ns), unused when ns = 1).  A stage's
+// radix is 2, 3, 4 or 5, or the product of two of them (6, 8, 9, 10, 12, 15,
+// 16), whose butterfly one thread computes in registers: two Stockham stages
+// for one round trip through shared memory.
 struct FftPlan {
 	int n;
 	int nstages;
@@ -29,6 +32,10 @@ struct FftPlan {
 
 // Fills the stage tables of plan from plan.n and plan.radix.
 void fft_plan_stages(FftPlan &plan);
+
+// The stages of a length-n transform (n 2-3-5 smooth): the prime factors
+// paired into radices of at most 16; false if n has another factor.
+bool fft_factor(int n, FftPlan &plan);
 
 // Smallest even size >= need whose prime factors are 2, 3 and 5.
 int fft_good_size(int need);

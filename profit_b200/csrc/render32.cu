@@ -779,24 +779,25 @@ __device__ __forceinline__ void level32_item(const FProfile *__restrict__ profil
 	for (int k = 0; k < NT; k++) sums[k] = 0.f;
 	if constexpr (Deep) level_points<double, AK, J>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
 	else level_points<float, AK, J>(p, it, level, s_xy, lane, q, sums, mask_out, base0, base1);
-	const int nk = J ? tangent_count(p.kind) : 1;  // warp-uniform
-#pragma unroll
-	for (int k = 0; k < NT; k++)
-		if (k < nk) sums[k] = warp_sum(sums[k]);
-	if (lane == 0) {
-		const float wgt = (float)it.weight;
-		const uint32_t b = it.pixel / npix, pix = it.pixel - b * npix;
-		float *img = p.target == 0 ? img_conv : img_plain;
-		atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)sums[0]));
-		if (J) {
+	float *img = p.target == 0 ? img_conv : img_plain;
+	if constexpr (J) {
+		// lane 2m ends with the cell's sum of tangent m (m = 0: the value) and
+		// adds it to its plane
+		const float tot = warp_sums_spread<NT>(sums, lane);
+		const int m = lane >> 1, nk = tangent_count(p.kind);
+		if (lane == 0) atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)tot));
+		if ((lane & 1) == 0 && m < nk) {
+			const uint32_t b = it.pixel / npix, pix = it.pixel - b * npix;
 			JT *jp = jac + (size_t)it.profile * nt * npix + pix;
 			// FP32 planes: the FP32 product; FP64 planes: the cell's sums
 			// enter at full precision (a pixel's cells can cancel)
-			const JT w = sizeof(JT) == 8 ? (JT)it.weight : (JT)wgt;
-#pragma unroll
-			for (int k = 0; k < NT; k++)
-				if (k < nk) atomicAdd(&jp[(size_t)k * npix], w * (JT)sums[k]);
+			const JT w = sizeof(JT) == 8 ? (JT)it.weight : (JT)(float)it.weight;
+			atomicAdd(&jp[(size_t)m * npix], w * (JT)tot);
 		}
+	}
+	else {
+		const float tot = warp_sum(sums[0]);
+		if (lane == 0) atomicAdd(&img[it.pixel], (float)(p.flux_scale64 * it.weight * (double)tot));
 	}
 	__syncwarp();
 }
