@@ -2793,6 +2793,7 @@ struct CatChunk {
 	std::vector<int> members;           // galaxy indices
 	std::vector<int> member_grad_off;   // offset of each member's gradient in the chunk's buffer
 	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3, cusps = 0;
+	int lane = 0;  // the engine (stream and scratch) its recorded pipeline runs on
 	bool ak = false;
 	bool plain = false;  // a profile drawn without convolution (reads the seed of the plain image)
 	// slices of the catalogue's shared device and pinned host arenas
@@ -2803,7 +2804,11 @@ struct CatChunk {
 	size_t nout() const { return (size_t)W * H; }
 };
 
-constexpr size_t CAT_BUDGET_BYTES = 12ull << 30;
+constexpr size_t CAT_BUDGET_BYTES = 6ull << 30;
+// Engines whose streams run chunks side by side in the recorded call: the
+// small kernels of one chunk (the cusp levels, the likelihood, the tails of
+// the waves) leave SMs idle that another chunk's kernels fill.
+constexpr int CAT_LANES = 4;
 constexpr unsigned CAT_SIDE_STEP = 64;
 
 }  // namespace
@@ -2812,6 +2817,11 @@ struct pf_catalogue {
 	std::vector<CatGalaxy> gal;
 	double magzero = 0;
 	pf_model *engine = nullptr;  // stream, scratch buffers, queue capacities
+	std::vector<pf_model *> lanes;  // lanes[0] is engine; each with its own stream and scratch
+	std::vector<size_t> lane_qpix;  // drawing pixels of each lane's largest chunk (queue sizing)
+	int max_levels = 1;
+	cudaEvent_t fork = nullptr;
+	std::vector<cudaEvent_t> joins;
 	bool built = false;
 	std::vector<std::unique_ptr<CatChunk>> chunks;
 	DevBuf params, pad, dev, fprof;  // every profile of the catalogue, chunk after chunk
@@ -3157,55 +3167,115 @@ int cat_build(pf_catalogue *c)
 	PF_CUDA(ensure(c->fprof, params.size() * sizeof(FProfile)));
 	PF_CUDA(ensure(c->lum, params.size() * LUM_SLOTS * sizeof(double)));
 
-	// engine scratch and queue for the largest chunk, so nothing is
-	// reallocated while chunks are queued
-	pf_model *m = c->engine;
-	size_t conv = 0, model = 0, seed = 0, jac = 0, parts = 0, qpix = 0, jp = 0;
-	int levels = 1, maxprof = 0, maxc = 1;
-	for (auto &chp : c->chunks) {
-		const CatChunk &ch = *chp;
-		const size_t C = ch.members.size();
-		maxc = std::max(maxc, (int)C);
-		conv = std::max(conv, ch.npix() * 4 * C);
-		model = std::max(model, ch.nout() * 8 * C);
-		seed = std::max(seed, ch.nout() * 4 * C);
-		jac = std::max(jac, ch.npix() * (size_t)ch.nt * ch.nprof * sizeof(double));
-		parts = std::max(parts, C * NPARTS * sizeof(double2));
-		qpix = std::max(qpix, ch.npix() * C);
-		jp = std::max(jp, (size_t)ch.nprof * jac_reduce_blocks((unsigned)ch.npix(), ch.nprof) * NTAN * 8);
-		levels = std::max(levels, ch.levels);
-		maxprof = std::max(maxprof, ch.nprof);
+	// lanes: engines of their own (stream, scratch, queue); chunks assigned
+	// greedily by drawing pixels to the least loaded lane
+	if (c->lanes.empty()) c->lanes.push_back(c->engine);
+	while ((int)c->lanes.size() < CAT_LANES) {
+		pf_model *e = nullptr;
+		PF_TRY(pf_model_create(1, 1, &e));
+		e->precision = PF_FP32;
+		c->lanes.push_back(e);
 	}
-	PF_CUDA(ensure(m->d_conv32, conv));
-	PF_CUDA(ensure(m->d_plain32, conv));
-	PF_CUDA(ensure(m->d_gconv, conv));
-	PF_CUDA(ensure(m->d_gplain, conv));
-	PF_CUDA(ensure(m->d_model64, model));
-	PF_CUDA(ensure(m->d_wseed, seed));
-	PF_CUDA(ensure(m->d_jac, jac));
-	PF_CUDA(ensure(m->d_partials, parts));
-	PF_CUDA(ensure(m->d_convsplit, (size_t)64 << 20));
-	PF_CUDA(ensure(m->d_jac_partials, jp));
-	void *before = m->d_jac_tickets.p;
-	PF_CUDA(ensure(m->d_jac_tickets, (size_t)maxprof * sizeof(unsigned)));
-	if (m->d_jac_tickets.p != before)
-		PF_CUDA(cudaMemsetAsync(m->d_jac_tickets.p, 0, m->d_jac_tickets.bytes, m->stream));
-	unsigned *like_tk;
-	PF_TRY(like_tickets(m, maxc, &like_tk));
-	Analysis a;
-	a.levels = levels;
-	QueueSet q;
-	PF_TRY(prepare_queue(m, a, qpix, q, nullptr, nullptr, false, true, true));  // sizes the kind-group buffer too
-	PF_CUDA(cudaStreamSynchronize(m->stream));
+	if (!c->fork) PF_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+	while ((int)c->joins.size() < CAT_LANES) {
+		cudaEvent_t e;
+		PF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+		c->joins.push_back(e);
+	}
+	{
+		std::vector<double> load(CAT_LANES, 0.0);
+		for (auto &chp : c->chunks) {
+			int best = 0;
+			for (int l = 1; l < CAT_LANES; l++)
+				if (load[l] < load[best]) best = l;
+			chp->lane = best;
+			load[best] += (double)chp->npix() * chp->members.size() * chp->levels;
+		}
+	}
+	// each lane's scratch and queue for its largest chunk, so nothing is
+	// reallocated while chunks are queued; lane 0 also runs every chunk on
+	// its own (the eager first call, re-runs after an overflow)
+	c->lane_qpix.assign(CAT_LANES, 0);
+	c->max_levels = 1;
+	for (int lane = 0; lane < CAT_LANES; lane++) {
+		pf_model *m = c->lanes[lane];
+		size_t conv = 0, model = 0, seed = 0, jac = 0, parts = 0, qpix = 0, jp = 0;
+		int levels = 1, maxprof = 0, maxc = 1;
+		for (auto &chp : c->chunks) {
+			const CatChunk &ch = *chp;
+			if (lane != 0 && ch.lane != lane) continue;
+			const size_t C = ch.members.size();
+			maxc = std::max(maxc, (int)C);
+			conv = std::max(conv, ch.npix() * 4 * C);
+			model = std::max(model, ch.nout() * 8 * C);
+			seed = std::max(seed, ch.nout() * 4 * C);
+			jac = std::max(jac, ch.npix() * (size_t)ch.nt * ch.nprof * sizeof(double));
+			parts = std::max(parts, C * NPARTS * sizeof(double2));
+			qpix = std::max(qpix, ch.npix() * C);
+			jp = std::max(jp, (size_t)ch.nprof * jac_reduce_blocks((unsigned)ch.npix(), ch.nprof) * NTAN * 8);
+			levels = std::max(levels, ch.levels);
+			maxprof = std::max(maxprof, ch.nprof);
+		}
+		PF_CUDA(ensure(m->d_conv32, conv));
+		PF_CUDA(ensure(m->d_plain32, conv));
+		PF_CUDA(ensure(m->d_gconv, conv));
+		PF_CUDA(ensure(m->d_gplain, conv));
+		PF_CUDA(ensure(m->d_model64, model));
+		PF_CUDA(ensure(m->d_wseed, seed));
+		PF_CUDA(ensure(m->d_jac, jac));
+		PF_CUDA(ensure(m->d_partials, parts));
+		PF_CUDA(ensure(m->d_convsplit, (size_t)64 << 20));
+		PF_CUDA(ensure(m->d_jac_partials, jp));
+		void *before = m->d_jac_tickets.p;
+		PF_CUDA(ensure(m->d_jac_tickets, (size_t)maxprof * sizeof(unsigned)));
+		if (m->d_jac_tickets.p != before)
+			PF_CUDA(cudaMemsetAsync(m->d_jac_tickets.p, 0, m->d_jac_tickets.bytes, m->stream));
+		unsigned *like_tk;
+		PF_TRY(like_tickets(m, maxc, &like_tk));
+		Analysis a;
+		a.levels = levels;
+		QueueSet q;
+		PF_TRY(prepare_queue(m, a, qpix, q, nullptr, nullptr, false, true, true));  // sizes the kind-group buffer too
+		PF_CUDA(cudaStreamSynchronize(m->stream));
+		c->lane_qpix[lane] = qpix;
+		c->max_levels = std::max(c->max_levels, levels);
+	}
 	c->built = true;
 	return PF_OK;
 }
 
+// Gives every lane the largest queue capacities any lane has grown to, and
+// sizes their queues for them, so that a recorded call finds them all at
+// what the eager run (on lane 0) needed.
+int cat_share_capacities(pf_catalogue *c)
+{
+	std::vector<uint32_t> mx(MAX_LEVELS, 0);
+	for (pf_model *m : c->lanes)
+		for (int l = 0; l < MAX_LEVELS && l < (int)m->caps.size(); l++) mx[l] = std::max(mx[l], m->caps[l]);
+	for (int lane = 0; lane < (int)c->lanes.size(); lane++) {
+		pf_model *m = c->lanes[lane];
+		m->caps = mx;
+		Analysis a;
+		a.levels = c->max_levels;
+		QueueSet q;
+		PF_TRY(prepare_queue(m, a, c->lane_qpix[lane], q, nullptr, nullptr, false, false, true));
+	}
+	return PF_OK;
+}
+
+// Every lane's capacities, in lane order (what a recorded call depends on).
+std::vector<uint32_t> cat_capacities(const pf_catalogue *c)
+{
+	std::vector<uint32_t> v;
+	for (const pf_model *m : c->lanes) v.insert(v.end(), m->caps.begin(), m->caps.end());
+	return v;
+}
+
 // Queues one chunk's pipeline (prologue already run); results and queue
 // counters land in the chunk's pinned buffers when the stream gets there.
-int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch)
+int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch, int lane)
 {
-	pf_model *m = c->engine;
+	pf_model *m = c->lanes[lane];
 	cudaStream_t s = m->stream;
 	const int C = (int)ch.members.size();
 	const Analysis a = cat_analysis(ch);
@@ -3272,6 +3342,9 @@ int pf_catalogue_destroy(pf_catalogue *c)
 	c->chunks.clear();
 	for (auto &e : c->ev)
 		if (e) cudaEventDestroy(e);
+	if (c->fork) cudaEventDestroy(c->fork);
+	for (cudaEvent_t e : c->joins) cudaEventDestroy(e);
+	for (size_t l = 1; l < c->lanes.size(); l++) pf_model_destroy(c->lanes[l]);
 	pf_model_destroy(c->engine);
 	delete c;
 	return PF_OK;
@@ -3375,43 +3448,64 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 	g.sx = g.sy = g.img_sx = g.img_sy = 1;
 	g.offx = g.offy = 0;
 	g.finesampling = 1;
-	auto enqueue_all = [&]() -> int {
-		PF_CUDA(launch_cat_prologue(c->params.as<ProfileParams>(), c->pad.as<int2>(), c->nprof, g,
-		                            c->lum.as<double>(), c->dev.as<DevProfile>(), c->fprof.as<FProfile>(), s));
-		for (auto &chp : c->chunks) PF_TRY(cat_enqueue_chunk(c, *chp));
+	// The prologue, then every chunk: on lane 0 alone (the eager call, whose
+	// convolution tuning then times each candidate on an otherwise idle GPU),
+	// or on the chunks' own lanes, forked from and joined back into lane 0's
+	// stream (the recorded call).
+	auto enqueue_chunks = [&](const std::vector<CatChunk *> &list, bool on_lanes) -> int {
+		if (on_lanes) {
+			PF_CUDA(cudaEventRecord(c->fork, s));
+			for (int l = 1; l < (int)c->lanes.size(); l++) PF_CUDA(cudaStreamWaitEvent(c->lanes[l]->stream, c->fork, 0));
+		}
+		for (CatChunk *ch : list) PF_TRY(cat_enqueue_chunk(c, *ch, on_lanes ? ch->lane : 0));
+		if (on_lanes)
+			for (int l = 1; l < (int)c->lanes.size(); l++) {
+				PF_CUDA(cudaEventRecord(c->joins[l], c->lanes[l]->stream));
+				PF_CUDA(cudaStreamWaitEvent(s, c->joins[l], 0));
+			}
 		return PF_OK;
 	};
-	std::vector<CatChunk *> todo;
-	for (auto &chp : c->chunks) todo.push_back(chp.get());
-	const bool replay = c->graph && c->graph_caps == m->caps;
+	std::vector<CatChunk *> all;
+	for (auto &chp : c->chunks) all.push_back(chp.get());
+	auto enqueue_all = [&](bool on_lanes) -> int {
+		PF_CUDA(launch_cat_prologue(c->params.as<ProfileParams>(), c->pad.as<int2>(), c->nprof, g,
+		                            c->lum.as<double>(), c->dev.as<DevProfile>(), c->fprof.as<FProfile>(), s));
+		return enqueue_chunks(all, on_lanes);
+	};
+	std::vector<CatChunk *> todo = all;
+	const bool replay = c->graph && c->graph_caps == cat_capacities(c);
 	bool retried = false;
 	for (int attempt = 0; attempt < 8 && !todo.empty(); attempt++) {
-		if (attempt == 0 && replay) {
+		const bool on_lanes = attempt == 0 && replay;
+		// every chunk is judged against the capacities of the lane it ran on,
+		// as they were when it ran (one chunk's growth must not hide another's
+		// overflow)
+		std::vector<std::vector<uint32_t>> used;
+		for (pf_model *e : c->lanes) used.push_back(e->caps);
+		if (on_lanes) {
 			PF_CUDA(cudaGraphLaunch(c->graph, s));
 			note_launches((int)c->graph_kernels);
 		}
 		else if (attempt == 0) {
-			PF_TRY(enqueue_all());
+			PF_TRY(enqueue_all(false));
 		}
 		else {
-			for (CatChunk *ch : todo) PF_TRY(cat_enqueue_chunk(c, *ch));
+			PF_TRY(enqueue_chunks(todo, false));
 		}
 		PF_CUDA(cudaStreamSynchronize(s));
-		// every chunk is judged against the capacities it ran with; only then
-		// do the capacities grow (one chunk's growth must not hide another's
-		// overflow)
-		const std::vector<uint32_t> used = m->caps;
 		std::vector<CatChunk *> again;
 		for (CatChunk *ch : todo) {
 			const uint32_t *ctrl = ch->h_ctrl.as<uint32_t>();
 			if (ctrl[MAX_LEVELS] & 2u) return set_error(PF_E_CAPACITY, "recursion deeper than the configured levels");
+			const int lane = on_lanes ? ch->lane : 0;
 			bool over = false;
 			for (int l = 0; l < ch->levels; l++)
-				if (ctrl[l] > used[l]) {
+				if (ctrl[l] > used[lane][l]) {
 					over = true;
 					uint64_t want = (uint64_t)ctrl[l] + ctrl[l] / 2 + 1024;
 					if (want > (1ull << 30)) return set_error(PF_E_CAPACITY, "subsampling work queue overflow");
-					m->caps[l] = std::max(m->caps[l], (uint32_t)want);
+					// the re-run goes to lane 0
+					c->lanes[0]->caps[l] = std::max(c->lanes[0]->caps[l], (uint32_t)want);
 				}
 			if (over) again.push_back(ch);
 		}
@@ -3425,18 +3519,21 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 	}
 	if (!replay && !retried && m->use_graphs) {
 		// record the call that just ran (every choice it made is cached now)
-		// for the next calls; nothing runs during the capture
+		// for the next calls, with the chunks on their lanes; nothing runs
+		// during the capture
 		if (c->graph) cudaGraphExecDestroy(c->graph);
 		c->graph = nullptr;
+		PF_TRY(cat_share_capacities(c));
+		for (pf_model *e : c->lanes) PF_CUDA(cudaStreamSynchronize(e->stream));
 		const unsigned long long before = g_launches.load();
 		cudaGraph_t graph = nullptr;
 		PF_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-		const int st = enqueue_all();
+		const int st = enqueue_all(true);
 		const cudaError_t ce = cudaStreamEndCapture(s, &graph);
 		c->graph_kernels = g_launches.load() - before;
 		g_launches -= c->graph_kernels;
 		if (st == PF_OK && ce == cudaSuccess && graph && cudaGraphInstantiate(&c->graph, graph, 0) == cudaSuccess)
-			c->graph_caps = m->caps;
+			c->graph_caps = cat_capacities(c);
 		else
 			c->graph = nullptr;
 		if (graph) cudaGraphDestroy(graph);
