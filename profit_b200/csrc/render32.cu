@@ -917,10 +917,13 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 	}
 	__shared__ double s_red[NT][8];
 	const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+	{
+		// lane 2m ends with the warp's sum of tangent m
+		double a[NT];
 #pragma unroll
-	for (int k = 0; k < NT; k++) {
-		double v = warp_sum((double)acc[k]);
-		if (lane == 0) s_red[k][wid] = v;
+		for (int k = 0; k < NT; k++) a[k] = (double)acc[k];
+		const double v = warp_sums_spread<NT>(a, lane);
+		if ((lane & 1) == 0 && (lane >> 1) < NT) s_red[lane >> 1][wid] = v;
 	}
 	__syncthreads();
 	if (threadIdx.x < NT) {
@@ -937,7 +940,7 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32(const FProfile *__rest
 // test: on a large field the launch of the culled blocks cost more than the
 // test itself.  (T is added atomically either way, in no fixed order.)
 template <bool AK>
-__global__ void __launch_bounds__(256) k_adjoint_pixels32_listed(const FProfile *__restrict__ profiles,
+__global__ void __launch_bounds__(256, AK ? 3 : 5) k_adjoint_pixels32_listed(const FProfile *__restrict__ profiles,
                                                                  const int *__restrict__ prof_begin, unsigned width,
                                                                  unsigned height, double sx, double sy,
                                                                  const float *__restrict__ g_conv,
@@ -994,10 +997,13 @@ __global__ void __launch_bounds__(256) k_adjoint_pixels32_listed(const FProfile 
 				Tan<float> t = eval_tan<float, AK, true>(p, xp, yp);
 				tan_to_j<NT>(t, xp, yp, gv, acc);
 			}
+			{
+				// lane 2m ends with the warp's sum of tangent m
+				double a[NT];
 #pragma unroll
-			for (int t = 0; t < NT; t++) {
-				double v = warp_sum((double)acc[t]);
-				if (lane == 0) s_red[t][wid] = v;
+				for (int t = 0; t < NT; t++) a[t] = (double)acc[t];
+				const double v = warp_sums_spread<NT>(a, lane);
+				if ((lane & 1) == 0 && (lane >> 1) < NT) s_red[lane >> 1][wid] = v;
 			}
 			__syncthreads();
 			if (threadIdx.x < NT) {
@@ -1133,14 +1139,16 @@ __device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigne
 }
 
 // sum over pixels of g(pixel) * J_k(pixel) for each radial profile:
-// blockIdx.y = profile, blockIdx.x strides over the pixels, four pixels per
-// thread and step with every load issued before the products (enough bytes
-// in flight to stream the tangent planes at HBM speed).  Each block writes
+// blockIdx.y = profile, blockIdx.x strides over the pixels, two pixels per
+// thread and step with every load issued before the products; about one
+// wave of four blocks per SM (at most 64 registers with FP32 planes), so the
+// last block to finish is not a second wave's.  Each
+// block writes
 // its NTAN sums to `partials`; the block that finishes last (an atomic
 // ticket per profile, no waiting) adds the partials in block order and
 // resets the ticket, so the result does not depend on block scheduling.
 template <int NT, class JT>
-__global__ void __launch_bounds__(256) k_jac_reduce(const JT *__restrict__ jac, const float *__restrict__ g_conv,
+__global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_jac_reduce(const JT *__restrict__ jac, const float *__restrict__ g_conv,
                                                     const float *__restrict__ g_plain,
                                                     const FProfile *__restrict__ profiles,
                                                     const int *__restrict__ prof_batch, unsigned npix, int nt,
@@ -1149,7 +1157,7 @@ __global__ void __launch_bounds__(256) k_jac_reduce(const JT *__restrict__ jac, 
                                                     unsigned *__restrict__ grad_ticket)
 {
 	pdl_enter();
-	constexpr int U = 4;
+	constexpr int U = 2;
 	const int pi = blockIdx.y;
 	const FProfile &p = profiles[pi];
 	if (!is_radial_kind(p.kind)) {
@@ -1424,8 +1432,8 @@ cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npi
 
 unsigned jac_reduce_blocks(unsigned npix, int n_profiles)
 {
-	unsigned bx = cdiv(npix, 256 * 4);
-	const unsigned target = cdiv(148u * 8u, (unsigned)n_profiles);  // about 8 blocks per SM in all
+	unsigned bx = cdiv(npix, 256 * 2);
+	const unsigned target = cdiv(148u * 4u, (unsigned)n_profiles);  // one wave of 4 blocks per SM in all
 	if (bx > target) bx = target;
 	return bx < 1 ? 1 : bx;
 }
