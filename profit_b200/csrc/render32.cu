@@ -1741,6 +1741,12 @@ static cudaError_t conv32_any(const float *src, int sw, int sh, int ox, int oy, 
 	    {Conv3Variant<TOut, 16, 8, 1, 8, 1, 51>::smem, Conv3Variant<TOut, 16, 8, 1, 8, 1, 51>::run},
 	    {Conv3Variant<TOut, 32, 8, 4, 1, 1, 31>::smem, Conv3Variant<TOut, 32, 8, 4, 1, 1, 31>::run},
 	    {Conv3Variant<TOut, 32, 12, 4, 1, 1, 31>::smem, Conv3Variant<TOut, 32, 12, 4, 1, 1, 31>::run},
+	    // more rows per thread (fewer window loads per packed FMA), and
+	    // 128-thread CTAs (five resident per SM instead of two)
+	    {Conv3Variant<TOut, 32, 12, 1, 8, 1, 51>::smem, Conv3Variant<TOut, 32, 12, 1, 8, 1, 51>::run},
+	    {Conv3Variant<TOut, 16, 12, 1, 8, 1, 51>::smem, Conv3Variant<TOut, 16, 12, 1, 8, 1, 51>::run},
+	    {Conv3Variant<TOut, 32, 10, 1, 4, 1, 51>::smem, Conv3Variant<TOut, 32, 10, 1, 4, 1, 51>::run},
+	    {Conv3Variant<TOut, 32, 8, 1, 8, 1, 51>::smem, Conv3Variant<TOut, 32, 8, 1, 8, 1, 51>::run},
 	    // tensor-core kernels (tcgen05, 3xTF32): 32 output columns per tile,
 	    // kernel rows split over 1, 2 or 4 CTAs.  Never picked by the
 	    // autotuner, only when forced: on a 400x400 image with a 51x51 PSF they

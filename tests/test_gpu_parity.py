@@ -226,14 +226,14 @@ def test_fp32_image_close_to_fp64(wl):
 
 
 # Number of FP32 convolution kernels the autotuner chooses from (render32.cu).
-N_FP32_CONV_CANDIDATES = 29
-# candidates 20-25 are compiled for one kernel height (51 or 31): they are
+N_FP32_CONV_CANDIDATES = 33
+# candidates 20-29 are compiled for one kernel height (51 or 31): they are
 # tested with a PSF of that size
-FIXED_HEIGHT_CANDIDATES = {20: 51, 21: 51, 22: 51, 23: 51, 24: 31, 25: 31}
+FIXED_HEIGHT_CANDIDATES = {20: 51, 21: 51, 22: 51, 23: 51, 24: 31, 25: 31, 26: 51, 27: 51, 28: 51, 29: 51}
 # candidates from this index on run on the tensor cores (3xTF32 split
 # products): their FP32-level sums differ from the FMA kernels' by a few
 # 1e-7 of logL, so logL is compared at 1e-6 there
-FIRST_TC_CONV_CANDIDATE = 26
+FIRST_TC_CONV_CANDIDATE = 30
 
 
 @pytest.mark.parametrize("cand", range(N_FP32_CONV_CANDIDATES))
