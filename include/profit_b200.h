@@ -302,6 +302,14 @@ int pf_catalogue_add_profile(pf_catalogue *c, int galaxy, const char *kind, int 
 int pf_catalogue_size(pf_catalogue *c, int *n_galaxies, int *n_grad);
 int pf_catalogue_gradient_offset(pf_catalogue *c, int galaxy, int *offset, int *count);
 int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad);
+/* The parameters of every profile in the layout of the gradient (galaxy after
+ * galaxy, profile after profile: xcen, ycen, mag, ang, axrat, box, then the
+ * kind's shape parameters).  set_values checks every profile first and
+ * changes none on error; the next pf_catalogue_loglike_grad uploads the new
+ * values and keeps the galaxies' images, batching and recorded launches (a
+ * sampler's step over the catalogue). */
+int pf_catalogue_set_values(pf_catalogue *c, const double *values);
+int pf_catalogue_get_values(pf_catalogue *c, double *values);
 /* Device time (ms, CUDA events) of the last pf_catalogue_loglike_grad. */
 int pf_catalogue_last_time(pf_catalogue *c, float *ms);
 

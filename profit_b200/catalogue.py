@@ -89,6 +89,23 @@ class Catalogue:
             off += k
         return ll, out
 
+    def values(self) -> np.ndarray:
+        """Every profile's parameters in the gradient's layout (galaxy after
+        galaxy, profile after profile, grad_names(kind) order)."""
+        _, ng = self.size()
+        v = np.zeros(max(ng, 1))
+        check(lib().pf_catalogue_get_values(self._h, v.ctypes.data_as(_capi._dp)))
+        return v[:ng]
+
+    def set_values(self, values) -> None:
+        """New parameters for every profile (the layout of values()); the
+        next loglike_grad keeps the images, batching and recorded launches."""
+        _, ng = self.size()
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        if v.shape != (ng,):
+            raise ValueError(f"expected {ng} values, got shape {v.shape}")
+        check(lib().pf_catalogue_set_values(self._h, v.ctypes.data_as(_capi._dp)))
+
     def last_time_ms(self) -> float:
         t = C.c_float()
         check(lib().pf_catalogue_last_time(self._h, C.byref(t)))

@@ -119,9 +119,9 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 			const char *lv = getenv("PF_AUTOTUNE_LOG");
 			const bool log = lv && lv[0] == '1';
 			// Candidates are timed on the first images of a large batch only:
-			// every candidate on about 512k output pixels, then the four
+			// every candidate on about 512k output pixels, then the six
 			// fastest again on about 2M (enough to fill every SM several
-			// times over).  The ranking is per tile, and timing whole
+			// times over), the best of three runs each.  The ranking is per tile, and timing whole
 			// catalogue chunks made the tuning most of a catalogue's first
 			// call.  The runs write only outputs that the chosen candidate
 			// then rewrites.
@@ -134,7 +134,7 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 				t.scratch_bytes = a.scratch_bytes / std::max(1, a.batch) * t.batch;
 				return t;
 			};
-			auto time_one = [&](const ConvArgs &t, int c, bool warm, float &ms) -> bool {
+			auto time_one = [&](const ConvArgs &t, int c, bool warm, float &ms, int min_reps) -> bool {
 				if (warm) {
 					cudaError_t e = cands[c].run(t, s);  // warm-up (and attribute setup)
 					if (e != cudaSuccess) {
@@ -142,14 +142,19 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 						return false;
 					}
 				}
-				// batched shapes run long enough to be timed once
-				const int reps = t.batch > 8 ? 1 : 3;
-				cudaEventRecord(e0, s);
-				for (int r = 0; r < reps; r++) cands[c].run(t, s);
-				cudaEventRecord(e1, s);
-				if (cudaEventSynchronize(e1) != cudaSuccess) return false;
-				cudaEventElapsedTime(&ms, e0, e1);
-				ms /= reps;
+				// batched shapes run long enough to be timed once per repetition;
+				// the fastest repetition counts
+				const int reps = std::max(min_reps, t.batch > 8 ? 1 : 3);
+				ms = 1e30f;
+				for (int r = 0; r < reps; r++) {
+					cudaEventRecord(e0, s);
+					cands[c].run(t, s);
+					cudaEventRecord(e1, s);
+					if (cudaEventSynchronize(e1) != cudaSuccess) return false;
+					float one = 0;
+					cudaEventElapsedTime(&one, e0, e1);
+					ms = std::min(ms, one);
+				}
 				if (log)
 					fprintf(stderr, "[profit_b200 autotune] type %d src %dx%d psf %dx%d out %dx%d batch %d (timed on %d): "
 					        "candidate %d %.4f ms\n",
@@ -166,12 +171,12 @@ cudaError_t conv_autotuned(const ConvCandidate *cands, int n_cands, int type_tag
 			for (int c = 0; c < n_cands; c++) {
 				if (!cands[c].tuned || cands[c].smem(a.kw, a.kh) > 227 * 1024) continue;
 				float ms = 0;
-				if (time_one(t1, c, true, ms)) ranked.emplace_back(ms, c);
+				if (time_one(t1, c, true, ms, 1)) ranked.emplace_back(ms, c);
 			}
 			by_time(ranked);
 			if (t2.batch > t1.batch) {
-				const size_t top = std::min<size_t>(4, ranked.size());
-				for (size_t r = 0; r < top; r++) time_one(t2, ranked[r].second, false, ranked[r].first);
+				const size_t top = std::min<size_t>(6, ranked.size());
+				for (size_t r = 0; r < top; r++) time_one(t2, ranked[r].second, false, ranked[r].first, 3);
 				std::vector<std::pair<float, int>> head(ranked.begin(), ranked.begin() + top);
 				by_time(head);
 				std::copy(head.begin(), head.end(), ranked.begin());
@@ -2832,6 +2837,7 @@ struct pf_catalogue {
 	int nprof = 0;
 	std::vector<int> grad_off;
 	int grad_total = 0;
+	bool params_dirty = false;  // set_values changed profiles since the last upload
 	float last_ms = 0;
 	cudaEvent_t ev[2] = {};
 	// the whole call (prologue and every chunk) captured once and replayed
@@ -2842,6 +2848,21 @@ struct pf_catalogue {
 };
 
 namespace {
+
+// Parameter k of a catalogue profile in the order of its gradient: xcen,
+// ycen, mag, ang, axrat, box, then the kind's shape parameters.
+double *cat_value_slot(ProfileParams &p, int k)
+{
+	switch (k) {
+	case 0: return &p.xcen;
+	case 1: return &p.ycen;
+	case 2: return &p.mag;
+	case 3: return &p.ang;
+	case 4: return &p.axrat;
+	case 5: return &p.box;
+	default: return shape_param(p, k - 6);
+	}
+}
 
 int cat_set_param(ProfileParams &p, const char *name, double value)
 {
@@ -2968,9 +2989,11 @@ int cat_build(pf_catalogue *c)
 				goff.push_back(gtot);
 				gtot += 6 + shape_count(p.kind);
 				unsigned mr = p.max_recursions;
-				if (p.kind == PK_SERSIC && p.adjust && p.nser > 1) {
+				// an adjusted Sersic may have its centre cusp (nser > 1) after
+				// pf_catalogue_set_values, so the levels are kept for it either way
+				if (p.kind == PK_SERSIC && p.adjust) {
 					mr = std::max(mr, 10u);
-					ch.cusps++;
+					if (p.nser > 1) ch.cusps++;
 				}
 				ch.levels = std::max(ch.levels, (int)mr + 1);
 				ch.nt = std::max(ch.nt, tangent_count(p.kind));
@@ -3407,6 +3430,46 @@ int pf_catalogue_add_profile(pf_catalogue *c, int galaxy, const char *kind, int 
 	return PF_OK;
 }
 
+int pf_catalogue_set_values(pf_catalogue *c, const double *values)
+{
+	if (!c || !values) return set_error(PF_E_INVALID, "null argument");
+	// every profile checked before any is changed
+	size_t at = 0;
+	for (size_t g = 0; g < c->gal.size(); g++)
+		for (const ProfileParams &p0 : c->gal[g].profiles) {
+			ProfileParams p = p0;
+			const int n = 6 + shape_count(p.kind);
+			for (int k = 0; k < n; k++) *cat_value_slot(p, k) = values[at + k];
+			at += n;
+			const char *err = validate_profile(p, true);
+			if (err || !params_valid(p))
+				return set_error(PF_E_INVALID, "galaxy " + std::to_string(g) + ": " +
+				                                   (err ? err : "invalid profile parameters"));
+		}
+	at = 0;
+	for (auto &G : c->gal)
+		for (ProfileParams &p : G.profiles) {
+			const int n = 6 + shape_count(p.kind);
+			for (int k = 0; k < n; k++) *cat_value_slot(p, k) = values[at + k];
+			at += n;
+		}
+	c->params_dirty = c->built;
+	return PF_OK;
+}
+
+int pf_catalogue_get_values(pf_catalogue *c, double *values)
+{
+	if (!c || !values) return set_error(PF_E_INVALID, "null argument");
+	size_t at = 0;
+	for (auto &G : c->gal)
+		for (ProfileParams &p : G.profiles) {
+			const int n = 6 + shape_count(p.kind);
+			for (int k = 0; k < n; k++) values[at + k] = *cat_value_slot(p, k);
+			at += n;
+		}
+	return PF_OK;
+}
+
 int pf_catalogue_size(pf_catalogue *c, int *n_galaxies, int *n_grad)
 {
 	if (!c) return set_error(PF_E_INVALID, "null catalogue");
@@ -3441,6 +3504,22 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 	PF_TRY(ensure_stream(c->engine));
 	if (!c->built) PF_TRY(cat_build(c));
 	pf_model *m = c->engine;
+	if (c->params_dirty) {
+		// new values (pf_catalogue_set_values): the profile records in chunk
+		// order again; the recorded call reads them from the same buffer
+		std::vector<ProfileParams> params;
+		params.reserve(c->nprof);
+		for (auto &chp : c->chunks) {
+			chp->cusps = 0;
+			for (int gi : chp->members)
+				for (const ProfileParams &p : c->gal[gi].profiles) {
+					params.push_back(p);
+					if (p.kind == PK_SERSIC && p.adjust && p.nser > 1) chp->cusps++;
+				}
+		}
+		PF_CUDA(cudaMemcpy(c->params.p, params.data(), params.size() * sizeof(ProfileParams), cudaMemcpyHostToDevice));
+		c->params_dirty = false;
+	}
 	cudaStream_t s = m->stream;
 	PF_CUDA(cudaEventRecord(c->ev[0], s));
 	ModelGeom g;

@@ -560,12 +560,52 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 }
 
 // The render without tangent planes, for models with many profiles: each
-// block first lists, in profile order, the profiles that reach it (the sky,
-// and radial profiles not skipped by k_pixels32's block test, evaluated the
-// same way), then every pixel loops over that list only.  Profiles are
-// listed 256 at a time, one per thread, with an ordered compaction (warp
-// ballots), so each pixel adds the same terms in the same order as
-// k_pixels32 without planes: the images are the same bit for bit.
+// block first lists, in profile order, the profiles that reach its tile (the
+// sky, and radial profiles not skipped by k_pixels32's block test, evaluated
+// the same way over the tile), then every pixel loops over that list only.
+// Profiles are listed 256 at a time, one per thread, with an ordered
+// compaction (warp ballots), so each pixel adds the same terms in the same
+// order as k_pixels32 without planes: the images are the same bit for bit.
+// Each thread takes two pixels, rows LISTED_ROWS apart, so one load of a
+// profile's scalars serves both.
+constexpr int LISTED_ROWS = 8;  // thread rows of a block; the tile is 32 x 2*LISTED_ROWS
+
+template <bool AK>
+__device__ __forceinline__ void listed_pixel(const FProfile &p, int pi, double x, double y, double half_xbin,
+                                             double half_ybin, uint32_t pix, int b, size_t npix, float *acc,
+                                             const QueueSet &q)
+{
+	if (p.kind == PK_SKY) {
+		acc[p.target] += p.flux_scale;  // sky value is kept in flux_scale
+		return;
+	}
+	float xp, yp;
+	const int decision = pixel_decision32(p, x, y, xp, yp);
+	if (decision == PD_DIRECT) {
+		acc[p.target] += p.flux_scale * eval_val<float, AK>(p, xp, yp);
+	}
+	else if (decision == PD_SUBSAMPLE) {
+		unsigned res = p.resolution, max_rec = p.max_rec;
+		if (p.centre_override && fabs(x - p.cx) < p.img_sx && fabs(y - p.cy) < p.img_sy) {
+			res = 8;
+			max_rec = 10;
+		}
+		SubItem it;
+		const double ddx = x - p.cx, ddy = y - p.cy;
+		it.x0 = ddx - half_xbin;
+		it.x1 = ddx + half_xbin;
+		it.y0 = ddy - half_ybin;
+		it.y1 = ddy + half_ybin;
+		it.weight = 1.0 / (res * res);
+		it.pixel = pix + (uint32_t)(b * npix);
+		it.profile = (uint16_t)pi;
+		it.res = (uint8_t)res;
+		it.max_rec = (uint8_t)max_rec;
+		queue_push(q, 0, it);
+		note_max_res(q, res);
+	}
+}
+
 template <bool AK>
 __global__ void __launch_bounds__(256) k_pixels32_listed(const FProfile *__restrict__ profiles,
                                                          const int *__restrict__ prof_begin, unsigned width,
@@ -578,22 +618,29 @@ __global__ void __launch_bounds__(256) k_pixels32_listed(const FProfile *__restr
 	__shared__ int s_count[8];
 	const int lane = threadIdx.x, wid = threadIdx.y, tid = wid * 32 + lane;
 	const unsigned i = blockIdx.x * 32 + threadIdx.x;
-	const unsigned j = blockIdx.y * 8 + threadIdx.y;
+	const unsigned ty0 = blockIdx.y * (2 * LISTED_ROWS);
+	const unsigned j[2] = {ty0 + threadIdx.y, ty0 + LISTED_ROWS + threadIdx.y};
 	const int b = blockIdx.z;
-	const bool inside = i < width && j < height;
 	const size_t npix = (size_t)width * height;
-	const uint32_t pix = inside ? i + j * width : 0;
 	const int p0 = prof_begin[b], p1 = prof_begin[b + 1];
-	float acc[2] = {0.f, 0.f};
 	const double half_xbin = sx / 2., half_ybin = sy / 2.;
-	const double y = half_ybin + j * sx;
 	const double x = half_xbin + i * sy;
-	// pixel centres of this block (same expressions as x and y)
-	const unsigned tx0 = blockIdx.x * 32, ty0 = blockIdx.y * 8;
-	const unsigned tx1 = min(tx0 + 31, width - 1), ty1 = min(ty0 + 7, height - 1);
+	bool inside[2], drawn[2];
+	uint32_t pix[2];
+	double y[2];
+	float acc[2][2] = {{0.f, 0.f}, {0.f, 0.f}};
+#pragma unroll
+	for (int r = 0; r < 2; r++) {
+		inside[r] = i < width && j[r] < height;
+		pix[r] = inside[r] ? i + j[r] * width : 0;
+		y[r] = half_ybin + j[r] * sx;
+		drawn[r] = inside[r] && (!mask || mask[pix[r]]);
+	}
+	// pixel centres of this tile (same expressions as x and y)
+	const unsigned tx0 = blockIdx.x * 32;
+	const unsigned tx1 = min(tx0 + 31, width - 1), ty1 = min(ty0 + 2 * LISTED_ROWS - 1, height - 1);
 	const double xlo = half_xbin + tx0 * sy, xhi = half_xbin + tx1 * sy;
 	const double ylo = half_ybin + ty0 * sx, yhi = half_ybin + ty1 * sx;
-	const bool drawn = inside && (!mask || mask[pix]);
 
 	for (int base = p0; base < p1; base += 256) {
 		bool keep = false;
@@ -622,47 +669,23 @@ __global__ void __launch_bounds__(256) k_pixels32_listed(const FProfile *__restr
 		}
 		if (keep) s_list[before + __popc(ballot & ((1u << lane) - 1u))] = base + tid;
 		__syncthreads();
-		if (drawn) {
+		if (drawn[0] || drawn[1]) {
 			for (int k = 0; k < total; k++) {
 				const int pi = s_list[k];
 				const FProfile &p = profiles[pi];
-				if (p.kind == PK_SKY) {
-					acc[p.target] += p.flux_scale;  // sky value is kept in flux_scale
-					continue;
-				}
-				float xp, yp;
-				const int decision = pixel_decision32(p, x, y, xp, yp);
-				if (decision == PD_DIRECT) {
-					acc[p.target] += p.flux_scale * eval_val<float, AK>(p, xp, yp);
-				}
-				else if (decision == PD_SUBSAMPLE) {
-					unsigned res = p.resolution, max_rec = p.max_rec;
-					if (p.centre_override && fabs(x - p.cx) < p.img_sx && fabs(y - p.cy) < p.img_sy) {
-						res = 8;
-						max_rec = 10;
-					}
-					SubItem it;
-					const double ddx = x - p.cx, ddy = y - p.cy;
-					it.x0 = ddx - half_xbin;
-					it.x1 = ddx + half_xbin;
-					it.y0 = ddy - half_ybin;
-					it.y1 = ddy + half_ybin;
-					it.weight = 1.0 / (res * res);
-					it.pixel = pix + (uint32_t)(b * npix);
-					it.profile = (uint16_t)pi;
-					it.res = (uint8_t)res;
-					it.max_rec = (uint8_t)max_rec;
-					queue_push(q, 0, it);
-					note_max_res(q, res);
-				}
+#pragma unroll
+				for (int r = 0; r < 2; r++)
+					if (drawn[r]) listed_pixel<AK>(p, pi, x, y[r], half_xbin, half_ybin, pix[r], b, npix, acc[r], q);
 			}
 		}
 		__syncthreads();  // the next round rewrites s_list and s_count
 	}
-	if (inside) {
-		img_conv[(size_t)b * npix + pix] = acc[0];
-		img_plain[(size_t)b * npix + pix] = acc[1];
-	}
+#pragma unroll
+	for (int r = 0; r < 2; r++)
+		if (inside[r]) {
+			img_conv[(size_t)b * npix + pix[r]] = acc[r][0];
+			img_plain[(size_t)b * npix + pix[r]] = acc[r][1];
+		}
 }
 
 // k / res == (k * div_magic(res)) >> 16 for every sub-point index k < 256
@@ -1311,8 +1334,9 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
 	}
 	if (!jac.p) {
 		auto k = all_kinds ? k_pixels32_listed<true> : k_pixels32_listed<false>;
-		return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain, q,
-		                  mask);
+		dim3 lgrid(cdiv(width, 32), cdiv(height, 2 * LISTED_ROWS), batch);
+		return launch_pdl(k, lgrid, dim3(32, LISTED_ROWS), 0, s, profiles, prof_begin, width, height, sx, sy, img_conv,
+		                  img_plain, q, mask);
 	}
 	auto k = all_kinds ? k_pixels32<true, true, float> : k_pixels32<false, true, float>;
 	return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain,

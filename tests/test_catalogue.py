@@ -115,3 +115,52 @@ def test_catalogue_replay_matches_first_call():
     for a, b, c in zip(g1, g2, g3):
         np.testing.assert_allclose(b, a, rtol=1e-5, atol=1e-6 * np.max(np.abs(a)))
         np.testing.assert_allclose(c, b, rtol=1e-5, atol=1e-6 * np.max(np.abs(b)))
+
+
+def test_catalogue_set_values_matches_a_fresh_catalogue():
+    """A sampler's step over a catalogue: new values for every profile
+    (pf_catalogue_set_values) keep the images, batching and recorded launches,
+    and give what a catalogue built with those values gives; bad values are
+    refused without changing anything."""
+    from profit_b200._capi import InvalidParameter
+    gals = _catalogue_case(n=10, seed_tag=65)
+    cat = Catalogue(magzero=gals[0]["magzero"])
+    for g in gals:
+        cat.add_galaxy(g["data"], g["sigma"], g["psf"], g["profiles"])
+    cat.loglike_grad()
+    cat.loglike_grad()  # recorded and replayed with the first values
+    v0 = cat.values()
+    r = np.random.Generator(np.random.PCG64(7))
+    moved = []
+    for g in gals:
+        profs = []
+        for kind, p in g["profiles"]:
+            q = dict(p)
+            q["xcen"] += r.uniform(-0.5, 0.5)
+            q["mag"] += r.uniform(-0.1, 0.1)
+            q["axrat"] = min(1.0, max(0.1, q["axrat"] * r.uniform(0.9, 1.1)))
+            if kind in ("sersic", "coresersic"):
+                q["nser"] *= r.uniform(0.9, 1.1)  # may cross nser = 1 (the centre cusp)
+            profs.append((kind, q))
+        moved.append(dict(g, profiles=profs))
+    fresh = Catalogue(magzero=gals[0]["magzero"])
+    for g in moved:
+        fresh.add_galaxy(g["data"], g["sigma"], g["psf"], g["profiles"])
+    v1 = fresh.values()
+    assert v1.shape == v0.shape
+    bad = v1.copy()
+    bad[4] = 1.5  # axrat > 1
+    with pytest.raises(InvalidParameter):
+        cat.set_values(bad)
+    np.testing.assert_array_equal(cat.values(), v0)
+    cat.set_values(v1)
+    np.testing.assert_array_equal(cat.values(), v1)
+    ll_f, g_f = fresh.loglike_grad()
+    for _ in range(2):  # the recorded call replayed with the new values
+        ll, gr = cat.loglike_grad()
+        # FP32 cells are added to their pixels atomically in no fixed order (and
+        # the two catalogues run their chunks on different lanes); away from
+        # the truth large residuals amplify that rounding: the FP32 bound
+        np.testing.assert_allclose(ll, ll_f, rtol=1e-5)
+        for a, b in zip(gr, g_f):
+            np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-5 * np.max(np.abs(b)))
