@@ -295,6 +295,15 @@ typedef struct pf_catalogue pf_catalogue;
 int pf_catalogue_create(pf_catalogue **out);
 int pf_catalogue_destroy(pf_catalogue *c);
 int pf_catalogue_set_magzero(pf_catalogue *c, double magzero);
+/* How the batched galaxies are convolved with their PSFs: "auto" (default;
+ * each batch times the brute-force kernels against FP64 FFTs of the same
+ * geometry, once, at the first evaluation after galaxies are added, and keeps
+ * the faster), "brute" or "fft" (batches whose FFT grid would exceed 6912
+ * points a side stay brute force).  The FFT form gives the brute-force sums
+ * to FP64 transform roundoff.  pf_catalogue_convolvers: how many of the
+ * batches convolve through FFTs, of how many (after an evaluation). */
+int pf_catalogue_set_convolver(pf_catalogue *c, const char *name);
+int pf_catalogue_convolvers(const pf_catalogue *c, int *fft_chunks, int *chunks);
 int pf_catalogue_add_galaxy(pf_catalogue *c, unsigned width, unsigned height, const double *data,
                             const double *sigma, const double *psf, unsigned psf_w, unsigned psf_h, int *index);
 int pf_catalogue_add_profile(pf_catalogue *c, int galaxy, const char *kind, int n_params,

@@ -148,6 +148,8 @@ def _late_bindings(L):
     L.pf_catalogue_last_time.argtypes = [vp, C.POINTER(C.c_float)]
     L.pf_catalogue_set_values.argtypes = [vp, _dp]
     L.pf_catalogue_get_values.argtypes = [vp, _dp]
+    L.pf_catalogue_set_convolver.argtypes = [vp, C.c_char_p]
+    L.pf_catalogue_convolvers.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     ip = C.POINTER(C.c_int)
     L.pf_model_set_fit_space.argtypes = [vp, C.c_int, C.POINTER(pf_param_ref), _dp, ip, ip, _dp, _dp, _dp, _dp, _dp,
                                          ip, ip]
@@ -168,6 +170,7 @@ EXPORTED = EXPORTED + ("pf_model_set_parameters", "pf_model_loglike_grad_batch",
                        "pf_catalogue_set_magzero", "pf_catalogue_add_galaxy", "pf_catalogue_add_profile",
                        "pf_catalogue_size", "pf_catalogue_gradient_offset", "pf_catalogue_loglike_grad",
                        "pf_catalogue_last_time", "pf_catalogue_set_values", "pf_catalogue_get_values",
+                       "pf_catalogue_set_convolver", "pf_catalogue_convolvers",
                        "pf_model_set_likelihood", "pf_model_set_mask",
                        "pf_model_set_adjust_mask", "pf_model_set_dimensions", "pf_model_set_dry_run",
                        "pf_model_set_omp_threads", "pf_model_benchmark_convolvers", "pf_model_set_fit_space",

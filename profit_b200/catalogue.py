@@ -106,6 +106,17 @@ class Catalogue:
             raise ValueError(f"expected {ng} values, got shape {v.shape}")
         check(lib().pf_catalogue_set_values(self._h, v.ctypes.data_as(_capi._dp)))
 
+    def set_convolver(self, name: str) -> None:
+        """"auto" (each batch of galaxies keeps the faster of brute force and
+        FP64 FFTs, timed once), "brute" or "fft"."""
+        check(lib().pf_catalogue_set_convolver(self._h, name.encode()))
+
+    def convolvers(self) -> Tuple[int, int]:
+        """(batches convolved through FFTs, batches), after an evaluation."""
+        f, n = C.c_int(), C.c_int()
+        check(lib().pf_catalogue_convolvers(self._h, C.byref(f), C.byref(n)))
+        return f.value, n.value
+
     def last_time_ms(self) -> float:
         t = C.c_float()
         check(lib().pf_catalogue_last_time(self._h, C.byref(t)))

@@ -378,11 +378,13 @@ __global__ void k_fft_rows_fwd(const TIn *__restrict__ src, int sw, int sh, int 
 
 // Column pass: CB columns of the half spectrum per CTA.  mode 0: forward FFT
 // only (PSF spectrum); mode 1: forward, times K, inverse; mode 2: forward,
-// times conj(K), inverse.  Shared memory: two M x CB buffers and M twiddles.
+// times conj(K), inverse.  Transform blockIdx.y of a batch reads the kernel
+// spectrum at K + blockIdx.y * k_batch (0: one kernel for the whole batch).
+// Shared memory: two M x CB buffers and M twiddles.
 template <class T, int CB, bool TWS>
 __global__ void k_fft_cols(typename Cx<T>::type *__restrict__ spec, int spec_ld, int ncols, int M, FftPlan plan,
                            const typename Cx<T>::type *__restrict__ tw, const typename Cx<T>::type *__restrict__ K,
-                           int mode, size_t spec_batch, bool k_smem)
+                           int mode, size_t spec_batch, size_t k_batch, bool k_smem)
 {
 	pdl_enter();
 	using C = typename Cx<T>::type;
@@ -390,6 +392,7 @@ __global__ void k_fft_cols(typename Cx<T>::type *__restrict__ spec, int spec_ld,
 	C *a = reinterpret_cast<C *>(smem_raw);
 	C *b = a + (size_t)M * CB;
 	spec += blockIdx.y * spec_batch;
+	if (K) K += blockIdx.y * k_batch;
 	const int c0 = blockIdx.x * CB;
 	const C *stw = load_twiddles<TWS>(b + (size_t)M * CB, tw, M);
 	// the kernel spectrum's columns, fetched with the data (k_smem: after the
@@ -632,7 +635,7 @@ static int cols_per_block(int M, int ncols, int batch)
 template <class T, int CB>
 static cudaError_t launch_cols(typename Cx<T>::type *spec, int spec_ld, int ncols, int M, const FftPlan &pm,
                                const typename Cx<T>::type *tw, const typename Cx<T>::type *K, int mode, int batch,
-                               size_t spec_batch, cudaStream_t s)
+                               size_t spec_batch, size_t k_batch, cudaStream_t s)
 {
 	const size_t e = sizeof(typename Cx<T>::type);
 	size_t smem = e * (size_t)M * 2 * CB;
@@ -647,19 +650,19 @@ static cudaError_t launch_cols(typename Cx<T>::type *spec, int spec_ld, int ncol
 	                                                               FFT_SMEM_BYTES) == cudaSuccess;
 	dim3 grid((ncols + CB - 1) / CB, batch);
 	return launch_pdl(kern, grid, dim3(fft_threads(pm, CB)), smem, s, spec, spec_ld, ncols, M, pm, tw, K, mode,
-	                  spec_batch, ks);
+	                  spec_batch, k_batch, ks);
 }
 
 template <class T>
 static cudaError_t cols_any(typename Cx<T>::type *spec, int spec_ld, int ncols, int M, const FftPlan &pm,
                             const typename Cx<T>::type *tw, const typename Cx<T>::type *K, int mode, int batch,
-                            size_t spec_batch, cudaStream_t s)
+                            size_t spec_batch, size_t k_batch, cudaStream_t s)
 {
 	switch (cols_per_block<T>(M, ncols, batch)) {
-	case 8: return launch_cols<T, 8>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, s);
-	case 4: return launch_cols<T, 4>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, s);
-	case 2: return launch_cols<T, 2>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, s);
-	default: return launch_cols<T, 1>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, s);
+	case 8: return launch_cols<T, 8>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, k_batch, s);
+	case 4: return launch_cols<T, 4>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, k_batch, s);
+	case 2: return launch_cols<T, 2>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, k_batch, s);
+	default: return launch_cols<T, 1>(spec, spec_ld, ncols, M, pm, tw, K, mode, batch, spec_batch, k_batch, s);
 	}
 }
 
@@ -726,7 +729,18 @@ cudaError_t FftConv<T>::set_kernel(const T *psf_dev, int kw, int kh, Cplx *kspec
 {
 	cudaError_t e = forward_rows<T>(psf_dev, kw, kh, 0, 0, kspec, 1, 0, s);
 	if (e != cudaSuccess) return e;
-	e = cols_any<T>(kspec, ld, ld, M, plan_m, tw_m, nullptr, 0, 1, 0, s);
+	e = cols_any<T>(kspec, ld, ld, M, plan_m, tw_m, nullptr, 0, 1, 0, 0, s);
+	have_kernel = e == cudaSuccess;
+	return e;
+}
+
+template <class T>
+cudaError_t FftConv<T>::set_kernels(const float *psf_dev, int kw, int kh, size_t psf_batch, Cplx *kspec, int batch,
+                                    cudaStream_t s)
+{
+	cudaError_t e = forward_rows<float>(psf_dev, kw, kh, 0, 0, kspec, batch, psf_batch, s);
+	if (e != cudaSuccess) return e;
+	e = cols_any<T>(kspec, ld, ld, M, plan_m, tw_m, nullptr, 0, batch, spectrum_elems(), 0, s);
 	have_kernel = e == cudaSuccess;
 	return e;
 }
@@ -736,11 +750,11 @@ template <class TIn, class TOut, class TAdd>
 cudaError_t FftConv<T>::convolve(const TIn *src, int sw, int sh, int sx0, int sy0, const Cplx *kspec, bool adjoint,
                                  Cplx *work, int dx, int dy, TOut *out, int ow, int oh, const TAdd *add,
                                  int add_stride, int add_ox, int add_oy, int batch, size_t src_batch,
-                                 size_t out_batch, size_t add_batch, cudaStream_t s)
+                                 size_t out_batch, size_t add_batch, cudaStream_t s, size_t kspec_batch)
 {
 	cudaError_t e = forward_rows<TIn>(src, sw, sh, sx0, sy0, work, batch, src_batch, s);
 	if (e != cudaSuccess) return e;
-	e = cols_any<T>(work, ld, ld, M, plan_m, tw_m, kspec, adjoint ? 2 : 1, batch, (size_t)M * ld, s);
+	e = cols_any<T>(work, ld, ld, M, plan_m, tw_m, kspec, adjoint ? 2 : 1, batch, (size_t)M * ld, kspec_batch, s);
 	if (e != cudaSuccess) return e;
 	const bool tws = sizeof(Cplx) * (3 * (size_t)N + 2) <= FFT_SMEM_BYTES;
 	size_t smem = sizeof(Cplx) * ((tws ? 3 : 2) * (size_t)N + 2);
@@ -758,18 +772,18 @@ template struct FftConv<float>;
 template cudaError_t FftConv<double>::convolve<double, double, double>(const double *, int, int, int, int,
                                                                       const Cplx *, bool, Cplx *, int, int, double *,
                                                                       int, int, const double *, int, int, int, int,
-                                                                      size_t, size_t, size_t, cudaStream_t);
+                                                                      size_t, size_t, size_t, cudaStream_t, size_t);
 template cudaError_t FftConv<double>::convolve<float, double, float>(const float *, int, int, int, int, const Cplx *,
                                                                     bool, Cplx *, int, int, double *, int, int,
                                                                     const float *, int, int, int, int, size_t,
-                                                                    size_t, size_t, cudaStream_t);
+                                                                    size_t, size_t, cudaStream_t, size_t);
 template cudaError_t FftConv<double>::convolve<float, float, float>(const float *, int, int, int, int, const Cplx *,
                                                                    bool, Cplx *, int, int, float *, int, int,
                                                                    const float *, int, int, int, int, size_t, size_t,
-                                                                   size_t, cudaStream_t);
+                                                                   size_t, cudaStream_t, size_t);
 template cudaError_t FftConv<float>::convolve<float, float, float>(const float *, int, int, int, int, const Cplx *,
                                                                   bool, Cplx *, int, int, float *, int, int,
                                                                   const float *, int, int, int, int, size_t, size_t,
-                                                                  size_t, cudaStream_t);
+                                                                  size_t, cudaStream_t, size_t);
 
 }  // namespace pf

@@ -56,16 +56,21 @@ struct FftConv {
 
 	// Spectrum of the kernel placed at (0, 0).
 	cudaError_t set_kernel(const T *psf_dev, int kw, int kh, Cplx *kspec, cudaStream_t s);
+	// Spectra of `batch` kernels of one size (kernel i at psf_dev + i *
+	// psf_batch), spectrum i at kspec + i * spectrum_elems().
+	cudaError_t set_kernels(const float *psf_dev, int kw, int kh, size_t psf_batch, Cplx *kspec, int batch,
+	                        cudaStream_t s);
 
 	// out(x, y) = c(x + dx, y + dy) [+ add(x + add_ox, y + add_oy)] for x < ow,
 	// y < oh, where c is the linear convolution of src (placed at (sx0, sy0))
 	// with the kernel (adjoint = false) or the correlation with it (adjoint =
-	// true, conjugated spectrum).  work holds batch spectra.
+	// true, conjugated spectrum).  work holds batch spectra.  Image i of the
+	// batch uses the kernel spectrum at kspec + i * kspec_batch.
 	template <class TIn, class TOut, class TAdd>
 	cudaError_t convolve(const TIn *src, int sw, int sh, int sx0, int sy0, const Cplx *kspec, bool adjoint,
 	                     Cplx *work, int dx, int dy, TOut *out, int ow, int oh, const TAdd *add, int add_stride,
 	                     int add_ox, int add_oy, int batch, size_t src_batch, size_t out_batch, size_t add_batch,
-	                     cudaStream_t s);
+	                     cudaStream_t s, size_t kspec_batch = 0);
 
 	template <class TIn>
 	cudaError_t forward_rows(const TIn *src, int sw, int sh, int sx0, int sy0, Cplx *spec, int batch,

@@ -2799,6 +2799,11 @@ struct CatChunk {
 	std::vector<int> member_grad_off;   // offset of each member's gradient in the chunk's buffer
 	int p0 = 0, nprof = 0, ngrad = 0, levels = 1, nt = NTAN_GEOM + 3, cusps = 0;
 	int lane = 0;  // the engine (stream and scratch) its recorded pipeline runs on
+	// convolutions through FP64 FFTs (each member's PSF spectrum in kspec)
+	// instead of the brute-force kernels: the faster of the two, timed at build
+	bool fft = false;
+	FftConv<double> fc;
+	DevBuf kspec;
 	bool ak = false;
 	bool plain = false;  // a profile drawn without convolution (reads the seed of the plain image)
 	// slices of the catalogue's shared device and pinned host arenas
@@ -2810,6 +2815,9 @@ struct CatChunk {
 };
 
 constexpr size_t CAT_BUDGET_BYTES = 6ull << 30;
+// PSF spectra of the chunks that convolve through FFTs, all chunks together
+constexpr size_t CAT_SPECTRA_BYTES = 16ull << 30;
+enum CatConv : int { CAT_CONV_AUTO = 0, CAT_CONV_BRUTE, CAT_CONV_FFT };
 // Engines whose streams run chunks side by side in the recorded call: the
 // small kernels of one chunk (the cusp levels, the likelihood, the tails of
 // the waves) leave SMs idle that another chunk's kernels fill.
@@ -2838,6 +2846,7 @@ struct pf_catalogue {
 	std::vector<int> grad_off;
 	int grad_total = 0;
 	bool params_dirty = false;  // set_values changed profiles since the last upload
+	int conv_mode = CAT_CONV_AUTO;  // how chunks pick their convolver (pf_catalogue_set_convolver)
 	float last_ms = 0;
 	cudaEvent_t ev[2] = {};
 	// the whole call (prologue and every chunk) captured once and replayed
@@ -2892,6 +2901,148 @@ Analysis cat_analysis(const CatChunk &ch)
 	a.levels = ch.levels;
 	a.n_profiles = ch.nprof;
 	return a;
+}
+
+// The chunk's forward convolution: the drawing (FP32, batch of C) into the
+// FP64 model image on the crop window, plus the unconvolved drawing.  Brute
+// force: out(x) = sum_i conv(x + i) psf(pw - 1 - i).  FFT: the same sum is
+// the linear convolution read at offset pw - 1; on a grid of at least the
+// drawing's size nothing it reads wraps around.
+int cat_conv_forward(pf_model *m, CatChunk &ch, const Analysis &a, bool fft, const float *conv, const float *plain,
+                     double *model64, cudaStream_t s)
+{
+	const int C = (int)ch.members.size();
+	const size_t npix = ch.npix(), nout = ch.nout();
+	if (fft) {
+		PF_CUDA(ch.fc.convolve<float, double, float>(conv, a.dw, a.dh, 0, 0, ch.kspec.as<double2>(), false,
+		                                             m->d_fftwork64.as<double2>(), (int)ch.pw - 1, (int)ch.ph - 1,
+		                                             model64, a.cw, a.ch, plain, a.dw, a.padx, a.pady, C, npix, nout,
+		                                             npix, s, ch.fc.spectrum_elems()));
+		note_launches(3);
+		return PF_OK;
+	}
+	const size_t sb = conv32_scratch_bytes(a.cw, a.ch, C);
+	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, ch.psfrev32.as<float>(), ch.pw, ch.ph, model64, a.cw, a.ch,
+	                           plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout,
+	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, (int)(ch.pw * ch.ph), s));
+	return PF_OK;
+}
+
+// Its adjoint: dlogL/dmodel (wseed, crop window) to dlogL/d(drawing pixel),
+// g(U) = sum_i w(U + 1 - pw + i) psf(i); through FFTs, the correlation with
+// the seed placed at pw - 1 (on a grid of at least the drawing's size, what
+// wraps around lands on the zeros below that offset).
+int cat_conv_adjoint(pf_model *m, CatChunk &ch, const Analysis &a, bool fft, const float *wseed, float *gconv,
+                     cudaStream_t s)
+{
+	const int C = (int)ch.members.size();
+	const size_t npix = ch.npix(), nout = ch.nout();
+	if (fft) {
+		PF_CUDA(ch.fc.convolve<float, float, float>(wseed, a.ow, a.oh, (int)ch.pw - 1, (int)ch.ph - 1,
+		                                            ch.kspec.as<double2>(), true, m->d_fftwork64.as<double2>(), 0, 0,
+		                                            gconv, a.dw, a.dh, nullptr, 0, 0, 0, C, nout, npix, 0, s,
+		                                            ch.fc.spectrum_elems()));
+		note_launches(3);
+		return PF_OK;
+	}
+	const size_t sb = conv32_scratch_bytes(a.dw, a.dh, C);
+	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)ch.pw, 1 - (int)ch.ph, ch.psf32.as<float>(), ch.pw, ch.ph, gconv,
+	                      a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix,
+	                      sb ? m->d_convsplit.as<double>() : nullptr, sb, (int)(ch.pw * ch.ph), s));
+	return PF_OK;
+}
+
+void release(DevBuf &b)
+{
+	if (b.p) cudaFree(b.p);
+	b.p = nullptr;
+	b.bytes = 0;
+}
+
+// Each chunk's convolver: brute force, or FP64 FFTs with the members' PSF
+// spectra computed here once.  Under CAT_CONV_AUTO both are timed on the
+// chunk itself (forward and adjoint, after a warm-up run, which also tunes
+// the brute-force tile) on lane 0, whose scratch takes every chunk, and the
+// faster is kept.  The timed runs read zeroed drawings and write only
+// buffers that every evaluation rewrites.
+int cat_pick_convolvers(pf_catalogue *c)
+{
+	pf_model *m = c->lanes[0];
+	cudaStream_t s = m->stream;
+	cudaEvent_t e0 = nullptr, e1 = nullptr;
+	PF_CUDA(cudaEventCreate(&e0));
+	PF_CUDA(cudaEventCreate(&e1));
+	struct Events {
+		cudaEvent_t &a, &b;
+		~Events()
+		{
+			if (a) cudaEventDestroy(a);
+			if (b) cudaEventDestroy(b);
+		}
+	} guard{e0, e1};
+	size_t spectra = 0;
+	std::vector<size_t> work(c->lanes.size(), 0);
+	for (auto &chp : c->chunks) {
+		CatChunk &ch = *chp;
+		ch.fft = false;
+		release(ch.kspec);
+		if (c->conv_mode == CAT_CONV_BRUTE) continue;
+		const Analysis a = cat_analysis(ch);
+		const int N = fft_good_size((int)a.dw), M = fft_good_size((int)a.dh);
+		if (N > FFT_MAX_LEN || M > FFT_MAX_LEN) continue;
+		if (ch.fc.setup(M, N) != cudaSuccess) {
+			cudaGetLastError();
+			continue;
+		}
+		const int C = (int)ch.members.size();
+		const size_t bytes = ch.fc.spectrum_elems() * sizeof(double2) * C;
+		if (spectra + bytes > CAT_SPECTRA_BYTES) continue;
+		PF_CUDA(ensure(ch.kspec, bytes));
+		PF_CUDA(ensure(m->d_fftwork64, bytes));
+		PF_CUDA(ch.fc.set_kernels(ch.psf32.as<float>(), (int)ch.pw, (int)ch.ph, (size_t)ch.pw * ch.ph,
+		                          ch.kspec.as<double2>(), C, s));
+		note_launches(2);
+		bool use = c->conv_mode == CAT_CONV_FFT;
+		if (!use) {
+			float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>();
+			float *wseed = m->d_wseed.as<float>(), *gconv = m->d_gconv.as<float>();
+			PF_CUDA(cudaMemsetAsync(conv, 0, ch.npix() * C * 4, s));
+			PF_CUDA(cudaMemsetAsync(plain, 0, ch.npix() * C * 4, s));
+			PF_CUDA(cudaMemsetAsync(wseed, 0, ch.nout() * C * 4, s));
+			auto run = [&](bool fft) -> int {
+				PF_TRY(cat_conv_forward(m, ch, a, fft, conv, plain, m->d_model64.as<double>(), s));
+				return cat_conv_adjoint(m, ch, a, fft, wseed, gconv, s);
+			};
+			float best[2] = {1e30f, 1e30f};
+			for (int f = 0; f < 2; f++) {
+				PF_TRY(run(f == 1));  // warm-up (brute force: tunes the tile for this shape)
+				for (int r = 0; r < 2; r++) {
+					PF_CUDA(cudaEventRecord(e0, s));
+					PF_TRY(run(f == 1));
+					PF_CUDA(cudaEventRecord(e1, s));
+					PF_CUDA(cudaEventSynchronize(e1));
+					float ms = 0;
+					PF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+					best[f] = std::min(best[f], ms);
+					if (ms > 2.0f) break;  // long enough to be timed once
+				}
+			}
+			use = best[1] < best[0];
+		}
+		if (use) {
+			ch.fft = true;
+			spectra += bytes;
+			work[0] = std::max(work[0], bytes);
+			work[ch.lane] = std::max(work[ch.lane], bytes);
+		}
+		else {
+			release(ch.kspec);
+		}
+	}
+	PF_CUDA(cudaStreamSynchronize(s));
+	for (size_t l = 0; l < c->lanes.size(); l++)
+		if (work[l]) PF_CUDA(ensure(c->lanes[l]->d_fftwork64, work[l]));
+	return PF_OK;
 }
 
 // Groups galaxies into chunks and uploads the static inputs.
@@ -3263,6 +3414,7 @@ int cat_build(pf_catalogue *c)
 		c->lane_qpix[lane] = qpix;
 		c->max_levels = std::max(c->max_levels, levels);
 	}
+	PF_TRY(cat_pick_convolvers(c));
 	c->built = true;
 	return PF_OK;
 }
@@ -3317,19 +3469,12 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch, int lane)
 	PF_CUDA(launch_pixels32(fprof, ch.prof_begin.as<int>(), C, a.dw, a.dh, 1.0, 1.0, conv, plain, jac, ch.nt, ch.ak, q,
 	                        s));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, ch.cusps, q, s));
-	const int kstride = (int)(ch.pw * ch.ph);
-	size_t sb = conv32_scratch_bytes(a.cw, a.ch, C);
-	PF_CUDA(launch_conv32_to64(conv, a.dw, a.dh, 0, 0, ch.psfrev32.as<float>(), ch.pw, ch.ph, model64, a.cw, a.ch,
-	                           plain, a.dw, a.padx, a.pady, C, (int)npix, (int)nout,
-	                           sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
+	PF_TRY(cat_conv_forward(m, ch, a, ch.fft, conv, plain, model64, s));
 	PF_CUDA(launch_loglike64_batch(model64, ch.data.as<double>(), ch.sigma.as<double>(), ch.region.as<uint8_t>(),
 	                               (int)nout, C, (int)nout, m->d_partials.as<double2>(), like_parts((int)nout, C),
 	                               ch.ll.as<double>(), wseed, s, m->d_like_tickets.as<unsigned>()));
 	if (ch.plain) PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
-	sb = conv32_scratch_bytes(a.dw, a.dh, C);
-	PF_CUDA(launch_conv32(wseed, a.ow, a.oh, 1 - (int)ch.pw, 1 - (int)ch.ph, ch.psf32.as<float>(), ch.pw, ch.ph, gconv,
-	                      a.dw, a.dh, nullptr, 0, 0, 0, C, (int)nout, (int)npix,
-	                      sb ? m->d_convsplit.as<double>() : nullptr, sb, kstride, s));
+	PF_TRY(cat_conv_adjoint(m, ch, a, ch.fft, wseed, gconv, s));
 	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, ch.prof_batch.as<int>(), ch.nprof, (unsigned)npix, ch.nt,
 	                          m->d_jac_partials.as<double>(), m->d_jac_tickets.as<unsigned>(), ch.T.as<double>(), s));
 	PF_CUDA(launch_cat_gradient(dev, ch.nprof, ch.T.as<double>(), ch.grad_off.as<int>(), ch.grad.as<double>(), s));
@@ -3377,6 +3522,30 @@ int pf_catalogue_set_magzero(pf_catalogue *c, double magzero)
 {
 	if (!c) return set_error(PF_E_INVALID, "null catalogue");
 	c->magzero = magzero;
+	return PF_OK;
+}
+
+int pf_catalogue_set_convolver(pf_catalogue *c, const char *name)
+{
+	if (!c || !name) return set_error(PF_E_INVALID, "null argument");
+	int mode;
+	if (!std::strcmp(name, "auto")) mode = CAT_CONV_AUTO;
+	else if (!std::strcmp(name, "brute")) mode = CAT_CONV_BRUTE;
+	else if (!std::strcmp(name, "fft")) mode = CAT_CONV_FFT;
+	else return set_error(PF_E_INVALID, std::string("unknown catalogue convolver: ") + name);
+	if (mode != c->conv_mode) {
+		c->conv_mode = mode;
+		c->built = false;  // chunks pick again at the next evaluation
+	}
+	return PF_OK;
+}
+
+int pf_catalogue_convolvers(const pf_catalogue *c, int *fft_chunks, int *chunks)
+{
+	if (!c || !fft_chunks || !chunks) return set_error(PF_E_INVALID, "null argument");
+	*chunks = (int)c->chunks.size();
+	*fft_chunks = 0;
+	for (const auto &ch : c->chunks) *fft_chunks += ch->fft ? 1 : 0;
 	return PF_OK;
 }
 

@@ -1075,14 +1075,14 @@ __global__ void __launch_bounds__(256) k_adjoint_items32(const FProfile *__restr
 			for (int k = 0; k < NT; k++) sums[k] = 0.f;
 			if (level >= 3) adjoint_points<double, AK>(p, it, s_xy[wib], lane, mask, sums);
 			else adjoint_points<float, AK>(p, it, s_xy[wib], lane, mask, sums);
-#pragma unroll
-			for (int k = 0; k < NT; k++) sums[k] = warp_sum(sums[k]);
-			if (lane == 0) {
-				const float gv = (p.target == 0 ? g_conv : g_plain)[it.pixel];
-				const double coef = (double)gv * it.weight;
-				if (coef != 0.0) {
-#pragma unroll
-					for (int k = 0; k < NT; k++) atomicAdd(&T[(size_t)it.profile * NTAN + k], coef * (double)sums[k]);
+			{
+				// lane 2m ends with the cell's sum of tangent m and adds it to T
+				const float tot = warp_sums_spread<NT>(sums, lane);
+				const int m = lane >> 1;
+				if ((lane & 1) == 0 && m < NT) {
+					const float gv = (p.target == 0 ? g_conv : g_plain)[it.pixel];
+					const double coef = (double)gv * it.weight;
+					if (coef != 0.0) atomicAdd(&T[(size_t)it.profile * NTAN + m], coef * (double)tot);
 				}
 			}
 			__syncwarp();
@@ -1119,28 +1119,63 @@ cudaError_t launch_adjoint_recompute(const FProfile *profiles, const int *prof_b
 // the last profile (ticket: one zero-initialised word over all profiles,
 // left at zero), which saves the launch when the batch is small.
 
-// Entry t of the gradient step (t < batch also writes logL of proposal t).
-// T is read from L2: in the fused form other SMs wrote it in the same launch.
-__device__ __forceinline__ void batch_gradient_at(const GradStepArgs &g, const double *T, int t)
+// The inputs of gradient-step entry t that do not depend on T (t < batch
+// also covers logL of proposal t; thread t < ctrl_words one control word,
+// thread 0 the completion word).  Loaded ahead of the tickets that decide
+// which block runs the step, so that the step itself waits on T and the
+// profile records only.
+struct GradPre {
+	double ll = 0;
+	int inv_t = 0, inv_b = 0, pi = 0, code = 0;
+	uint32_t ctrl = 0;
+	unsigned seq = 0;
+};
+
+__device__ __forceinline__ GradPre grad_prefetch(const GradStepArgs &g, int t)
 {
-	if (t < g.batch) g.out_ll[t] = g.invalid[t] ? -INFINITY : g.ll[t];
+	GradPre f;
+	if (t < g.batch) {
+		f.inv_t = __ldcg(g.invalid + t);
+		f.ll = __ldcg(g.ll + t);
+	}
+	if (t < g.batch * g.nrefs) {
+		const int b = t / g.nrefs, r = t - b * g.nrefs;
+		f.pi = b * g.nprof + __ldcg(g.ref_profile + r);
+		f.code = __ldcg(g.ref_code + r);
+		f.inv_b = __ldcg(g.invalid + b);
+	}
+	if (g.ctrl_out && t < g.ctrl_words) f.ctrl = __ldcg(g.ctrl_in + t);
+	if (g.seq_out && t == 0) f.seq = __ldcg(g.seq_in);
+	return f;
+}
+
+// Entry t of the gradient step from its prefetched inputs.  T is read from
+// L2: in the fused form other SMs wrote it in the same launch.
+__device__ __forceinline__ void batch_gradient_from(const GradStepArgs &g, const double *T, int t, const GradPre &f)
+{
+	if (t < g.batch) g.out_ll[t] = f.inv_t ? -INFINITY : f.ll;
 	if (t >= g.batch * g.nrefs) return;
-	const int b = t / g.nrefs, r = t - b * g.nrefs;
-	const int pi = b * g.nprof + g.ref_profile[r];
-	if (g.invalid[b]) {
+	if (f.inv_b) {
 		g.out_grad[t] = 0.0;
 		return;
 	}
 	double Tp[NTAN];
 #pragma unroll
-	for (int k = 0; k < NTAN; k++) Tp[k] = __ldcg(T + (size_t)pi * NTAN + k);
-	g.out_grad[t] = gradient_from_tangents(g.ref_code[r], g.dev[pi].axrat, g.dev[pi], Tp);
+	for (int k = 0; k < NTAN; k++) Tp[k] = __ldcg(T + (size_t)f.pi * NTAN + k);
+	g.out_grad[t] = gradient_from_tangents(f.code, g.dev[f.pi].axrat, g.dev[f.pi], Tp);
+}
+
+__device__ __forceinline__ void batch_gradient_at(const GradStepArgs &g, const double *T, int t)
+{
+	batch_gradient_from(g, T, t, grad_prefetch(g, t));
 }
 
 // Called by one block per profile once that profile's T is written (or its
 // blocks have nothing to reduce); the last of the gridDim.y calls runs the
 // gradient step with all its threads.  Writers of T fence before the call.
-__device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigned *ticket, const double *T)
+// f: grad_prefetch(g, threadIdx.x), loaded by the caller.
+__device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigned *ticket, const double *T,
+                                                  const GradPre &f)
 {
 	__shared__ bool s_all;
 	__syncthreads();
@@ -1149,15 +1184,18 @@ __device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigne
 	if (!s_all) return;
 	__threadfence();
 	const int n = g.batch * max(g.nrefs, 1);
-	for (int t = threadIdx.x; t < n; t += blockDim.x) batch_gradient_at(g, T, t);
-	if (g.ctrl_out)
-		for (int i = threadIdx.x; i < g.ctrl_words; i += blockDim.x) g.ctrl_out[i] = __ldcg(g.ctrl_in + i);
+	if ((int)threadIdx.x < n) batch_gradient_from(g, T, threadIdx.x, f);
+	for (int t = threadIdx.x + blockDim.x; t < n; t += blockDim.x) batch_gradient_at(g, T, t);
+	if (g.ctrl_out) {
+		if ((int)threadIdx.x < g.ctrl_words) g.ctrl_out[threadIdx.x] = f.ctrl;
+		for (int i = threadIdx.x + blockDim.x; i < g.ctrl_words; i += blockDim.x) g.ctrl_out[i] = __ldcg(g.ctrl_in + i);
+	}
 	if (threadIdx.x == 0) *ticket = 0;
 	if (g.seq_out) {
 		// the results reach host memory before the word that announces them
 		__threadfence_system();
 		__syncthreads();
-		if (threadIdx.x == 0) *reinterpret_cast<volatile unsigned *>(g.seq_out) = __ldcg(g.seq_in);
+		if (threadIdx.x == 0) *reinterpret_cast<volatile unsigned *>(g.seq_out) = f.seq;
 	}
 }
 
@@ -1184,7 +1222,7 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 	const int pi = blockIdx.y;
 	const FProfile &p = profiles[pi];
 	if (!is_radial_kind(p.kind)) {
-		if (grad_ticket && blockIdx.x == 0) jac_gradient_tail(grad, grad_ticket, out);
+		if (grad_ticket && blockIdx.x == 0) jac_gradient_tail(grad, grad_ticket, out, grad_prefetch(grad, threadIdx.x));
 		return;
 	}
 	const int nk = tangent_count(p.kind);  // <= nt <= NT
@@ -1239,6 +1277,9 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 	__syncthreads();
 	if (!s_last) return;
 	__threadfence();
+	// (the gradient step's own inputs travel with the partials)
+	GradPre f;
+	if (grad_ticket) f = grad_prefetch(grad, threadIdx.x);
 	// the last block merges the partials with all its threads: thread t adds
 	// blocks t, t + 256, ... in order, then warps and the block reduce in a
 	// fixed order, so the result still does not depend on scheduling
@@ -1263,7 +1304,7 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 		if (grad_ticket) __threadfence();
 	}
 	if (threadIdx.x == 0) tickets[pi] = 0;
-	if (grad_ticket) jac_gradient_tail(grad, grad_ticket, out);
+	if (grad_ticket) jac_gradient_tail(grad, grad_ticket, out, f);
 }
 
 // Scatter the residual weights w (cropped grid) into the padded grid of the
