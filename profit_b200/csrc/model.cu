@@ -2963,8 +2963,9 @@ void release(DevBuf &b)
 // spectra computed here once.  Under CAT_CONV_AUTO both are timed on the
 // chunk itself (forward and adjoint, after a warm-up run, which also tunes
 // the brute-force tile) on lane 0, whose scratch takes every chunk, and the
-// faster is kept.  The timed runs read zeroed drawings and write only
-// buffers that every evaluation rewrites.
+// faster is kept; brute force is not timed (nor tuned) where the FFTs beat
+// its FLOP count at the GPU's FP32 peak.  The timed runs read zeroed
+// drawings and write only buffers that every evaluation rewrites.
 int cat_pick_convolvers(pf_catalogue *c)
 {
 	pf_model *m = c->lanes[0];
@@ -2982,6 +2983,12 @@ int cat_pick_convolvers(pf_catalogue *c)
 	} guard{e0, e1};
 	size_t spectra = 0;
 	std::vector<size_t> work(c->lanes.size(), 0);
+	// an upper bound on the GPU's FP32 rate: 128 FMA lanes per SM at the
+	// highest SM clock, with a quarter more for safety
+	int sms = 0, khz = 0;
+	PF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device));
+	PF_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, m->device));
+	const double fp32_peak = 1.25 * 256.0 * sms * (khz * 1e3);
 	for (auto &chp : c->chunks) {
 		CatChunk &ch = *chp;
 		ch.fft = false;
@@ -3013,21 +3020,33 @@ int cat_pick_convolvers(pf_catalogue *c)
 				PF_TRY(cat_conv_forward(m, ch, a, fft, conv, plain, m->d_model64.as<double>(), s));
 				return cat_conv_adjoint(m, ch, a, fft, wseed, gconv, s);
 			};
-			float best[2] = {1e30f, 1e30f};
-			for (int f = 0; f < 2; f++) {
-				PF_TRY(run(f == 1));  // warm-up (brute force: tunes the tile for this shape)
+			auto timed = [&](bool fft, float &best) -> int {
+				PF_TRY(run(fft));  // warm-up (brute force: tunes the tile for this shape)
+				best = 1e30f;
 				for (int r = 0; r < 2; r++) {
 					PF_CUDA(cudaEventRecord(e0, s));
-					PF_TRY(run(f == 1));
+					PF_TRY(run(fft));
 					PF_CUDA(cudaEventRecord(e1, s));
 					PF_CUDA(cudaEventSynchronize(e1));
 					float ms = 0;
 					PF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-					best[f] = std::min(best[f], ms);
+					best = std::min(best, ms);
 					if (ms > 2.0f) break;  // long enough to be timed once
 				}
+				return PF_OK;
+			};
+			float t_fft = 0, t_brute = 0;
+			PF_TRY(timed(true, t_fft));
+			// brute force cannot beat its multiply-adds at the FP32 peak: an
+			// FFT faster than that wins without tuning and timing the tiles
+			const double flop = 2.0 * ch.pw * ch.ph * (double)(ch.nout() + ch.npix()) * C;
+			if (t_fft * 1e-3 < flop / fp32_peak) {
+				use = true;
 			}
-			use = best[1] < best[0];
+			else {
+				PF_TRY(timed(false, t_brute));
+				use = t_fft < t_brute;
+			}
 		}
 		if (use) {
 			ch.fft = true;
