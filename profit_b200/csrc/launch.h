@@ -85,7 +85,7 @@ constexpr int DEEP_ONE_CTA_MAX_CUSPS = 8;
 // that may recurse past level 2).
 cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npix, float *img_conv, float *img_plain,
                             JacPlanes jac, int nt, bool all_kinds, int cusps, const QueueSet &q, cudaStream_t s);
-// partials: n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN doubles;
+// partials: n_profiles * jac_reduce_blocks(width, height, n_profiles) * NTAN doubles;
 // tickets: n_profiles zero-initialised counters (left at zero again), one
 // more when grad is given.  grad (optional): the arguments of
 // launch_batch_gradient; the reduction then also runs that step (in the block
@@ -108,10 +108,13 @@ struct GradStepArgs {
 	const unsigned *seq_in = nullptr;
 	unsigned *seq_out = nullptr;
 };
-unsigned jac_reduce_blocks(unsigned npix, int n_profiles);
+unsigned jac_reduce_blocks(unsigned width, unsigned height, int n_profiles);
+// width, height, sx, sy: the drawing grid as given to launch_pixels32, whose
+// tiles skipped by a profile hold no tangent planes of that profile.
 cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
-                              const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
-                              unsigned *tickets, double *out, cudaStream_t s, const GradStepArgs *grad = nullptr);
+                              const int *prof_batch, int n_profiles, unsigned width, unsigned height, double sx,
+                              double sy, int nt, double *partials, unsigned *tickets, double *out, cudaStream_t s,
+                              const GradStepArgs *grad = nullptr);
 // Copies `bytes` (a multiple of 16, both addresses 16-byte aligned) from
 // pinned host memory mapped into the device's address space to dst, and
 // zeroes ctrl[0 .. ctrl_words); one launch in place of a copy and a memset.

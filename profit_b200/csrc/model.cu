@@ -1185,12 +1185,12 @@ bool all_kinds(const pf_model *m)
 	return false;
 }
 
-// Scratch of launch_jac_reduce for n_profiles profiles over npix pixels; the
+// Scratch of launch_jac_reduce for n_profiles profiles on a width x height drawing; the
 // tickets (one per profile and one for the folded gradient step) start at
 // zero when allocated and the kernel leaves them at zero.
-int jac_scratch(pf_model *m, unsigned npix, int n_profiles, double **partials, unsigned **tickets)
+int jac_scratch(pf_model *m, unsigned width, unsigned height, int n_profiles, double **partials, unsigned **tickets)
 {
-	const size_t pb = (size_t)n_profiles * jac_reduce_blocks(npix, n_profiles) * NTAN * sizeof(double);
+	const size_t pb = (size_t)n_profiles * jac_reduce_blocks(width, height, n_profiles) * NTAN * sizeof(double);
 	PF_CUDA(ensure(m->d_jac_partials, pb));
 	void *before = m->d_jac_tickets.p;
 	PF_CUDA(ensure(m->d_jac_tickets, (size_t)(n_profiles + 1) * sizeof(unsigned)));
@@ -1267,10 +1267,10 @@ int run_fp32(pf_model *m, const Analysis &a, const FProfile *fprof, QueueSet &q,
 		PF_CUDA(cudaMemsetAsync(d_out + ResultLayout::T0, 0, (size_t)nprof * NTAN * 8, m->stream));
 		double *jpart;
 		unsigned *jtick;
-		PF_TRY(jac_scratch(m, (unsigned)npix, nprof, &jpart, &jtick));
-		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, (unsigned)npix,
-		                          tangent_stride(m), jpart,
-		                          jtick, d_out + ResultLayout::T0, m->stream));
+		PF_TRY(jac_scratch(m, a.dw, a.dh, nprof, &jpart, &jtick));
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), nprof, a.dw, a.dh,
+		                          m->sx / m->fs, m->sy / m->fs, tangent_stride(m), jpart, jtick,
+		                          d_out + ResultLayout::T0, m->stream));
 		if (has_psf_profile(m))
 			PF_CUDA(launch_psf_adjoint32(m->d_prof.as<DevProfile>(), m->d_prof_begin.as<int>(), 1, nprof,
 			                             m->d_psf64.as<double>(), m->psf_w, m->psf_h, m->psf_sx, m->psf_sy,
@@ -1620,9 +1620,10 @@ int enqueue_batch_chunk(pf_model *m, BatchState &bs, const Analysis &a, int C, i
 	if (!recompute) {
 		double *jpart;
 		unsigned *jtick;
-		PF_TRY(jac_scratch(m, (unsigned)npix, C * nprof, &jpart, &jtick));
-		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, (unsigned)npix, nt,
-		                          jpart, jtick, bs.d_T.as<double>(), s, fold_grad ? &gargs : nullptr));
+		PF_TRY(jac_scratch(m, a.dw, a.dh, C * nprof, &jpart, &jtick));
+		PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, m->d_prof_batch.as<int>(), C * nprof, a.dw, a.dh,
+		                          m->sx / m->fs, m->sy / m->fs, nt, jpart, jtick, bs.d_T.as<double>(), s,
+		                          fold_grad ? &gargs : nullptr));
 	}
 	if (has_psf_profile(m))
 		PF_CUDA(launch_psf_adjoint32(dev, m->d_prof_begin.as<int>(), C, nprof, m->d_psf64.as<double>(), m->psf_w,
@@ -3405,7 +3406,8 @@ int cat_build(pf_catalogue *c)
 			jac = std::max(jac, ch.npix() * (size_t)ch.nt * ch.nprof * sizeof(double));
 			parts = std::max(parts, C * NPARTS * sizeof(double2));
 			qpix = std::max(qpix, ch.npix() * C);
-			jp = std::max(jp, (size_t)ch.nprof * jac_reduce_blocks((unsigned)ch.npix(), ch.nprof) * NTAN * 8);
+			jp = std::max(jp, (size_t)ch.nprof *
+			                            jac_reduce_blocks(ch.W + 2 * (ch.pw / 2), ch.H + 2 * (ch.ph / 2), ch.nprof) * NTAN * 8);
 			levels = std::max(levels, ch.levels);
 			maxprof = std::max(maxprof, ch.nprof);
 		}
@@ -3494,8 +3496,9 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch, int lane)
 	                               ch.ll.as<double>(), wseed, s, m->d_like_tickets.as<unsigned>()));
 	if (ch.plain) PF_CUDA(launch_embed_seed(wseed, a.ow, a.oh, a.padx, a.pady, a.dw, a.dh, C, gplain, s));
 	PF_TRY(cat_conv_adjoint(m, ch, a, ch.fft, wseed, gconv, s));
-	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, ch.prof_batch.as<int>(), ch.nprof, (unsigned)npix, ch.nt,
-	                          m->d_jac_partials.as<double>(), m->d_jac_tickets.as<unsigned>(), ch.T.as<double>(), s));
+	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, ch.prof_batch.as<int>(), ch.nprof, a.dw, a.dh, 1.0, 1.0,
+	                          ch.nt, m->d_jac_partials.as<double>(), m->d_jac_tickets.as<unsigned>(),
+	                          ch.T.as<double>(), s));
 	PF_CUDA(launch_cat_gradient(dev, ch.nprof, ch.T.as<double>(), ch.grad_off.as<int>(), ch.grad.as<double>(), s));
 	PF_CUDA(cudaMemcpyAsync(ch.h_ll.p, ch.ll.p, (size_t)C * 8, cudaMemcpyDeviceToHost, s));
 	PF_CUDA(cudaMemcpyAsync(ch.h_grad.p, ch.grad.p, (size_t)std::max(ch.ngrad, 1) * 8, cudaMemcpyDeviceToHost, s));

@@ -460,6 +460,44 @@ __device__ __forceinline__ Tan<float> to_float(const Tan<T> &t)
 // are not drawn by the radial and sky profiles (radial.cpp:306, sky.cpp:47-63).
 // JT: element type of the tangent planes (float, or double where the cells
 // of a subsampled pixel must be summed without FP32 cancellation).
+// Pixel tiles of k_pixels32 (its block) and of k_jac_reduce: a profile whose
+// r_max + 2 circle misses every pixel centre of a tile draws nothing there,
+// and its tangent planes are neither written nor read on that tile.  Both
+// kernels take this test, rounded alike (explicit FP32 operations, no
+// contraction), so they skip the same tiles; FP32 rounding of coordinates
+// below 2^13 px is far inside the 2 px margin, and subsampled cells lie
+// inside r_switch < r_max, never on a skipped tile.
+constexpr unsigned PIX_TILE_W = 32, PIX_TILE_H = 8;
+
+// True when tile_culled keeps every tile of the drawing: every pixel centre
+// lies within r_max + 1 of the profile centre (1 px inside the test's
+// r_max + 2, far more than its FP32 rounding), or the profile has no r_max.
+__device__ __forceinline__ bool tiles_all_reached(const FProfile &p, unsigned width, unsigned height, double sx,
+                                                  double sy)
+{
+	if (!(p.r_max > 0.f)) return true;
+	const double x0 = sx / 2., x1 = sx / 2. + (width - 1) * sy;  // x steps by sy, y by sx
+	const double y0 = sy / 2., y1 = sy / 2. + (height - 1) * sx;
+	const double fx = fmax(fabs(x0 - p.cx), fabs(x1 - p.cx)), fy = fmax(fabs(y0 - p.cy), fabs(y1 - p.cy));
+	const double lim = (double)p.r_max + 1.0;
+	return fx * fx + fy * fy <= lim * lim;
+}
+
+__device__ __forceinline__ bool tile_culled(const FProfile &p, unsigned tx0, unsigned ty0, unsigned width,
+                                            unsigned height, double sx, double sy)
+{
+	if (!(p.r_max > 0.f)) return false;
+	const float hx = __fmul_rn(__double2float_rn(sx), 0.5f), hy = __fmul_rn(__double2float_rn(sy), 0.5f);
+	const float fx = __double2float_rn(sy), fy = __double2float_rn(sx);  // x steps by sy, y by sx
+	const unsigned tx1 = min(tx0 + PIX_TILE_W - 1, width - 1), ty1 = min(ty0 + PIX_TILE_H - 1, height - 1);
+	const float xlo = __fadd_rn(hx, __fmul_rn((float)tx0, fx)), xhi = __fadd_rn(hx, __fmul_rn((float)tx1, fx));
+	const float ylo = __fadd_rn(hy, __fmul_rn((float)ty0, fy)), yhi = __fadd_rn(hy, __fmul_rn((float)ty1, fy));
+	const float cx = __double2float_rn(p.cx), cy = __double2float_rn(p.cy);
+	const float nx = __fsub_rn(fminf(fmaxf(cx, xlo), xhi), cx), ny = __fsub_rn(fminf(fmaxf(cy, ylo), yhi), cy);
+	const float lim = __fadd_rn(p.r_max, 2.0f);
+	return __fadd_rn(__fmul_rn(nx, nx), __fmul_rn(ny, ny)) > __fmul_rn(lim, lim);
+}
+
 template <bool AK, bool J, class JT>
 __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__restrict__ prof_begin,
                            unsigned width, unsigned height, double sx, double sy, float *__restrict__ img_conv,
@@ -478,40 +516,32 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 	const double half_xbin = sx / 2., half_ybin = sy / 2.;
 	const double y = half_ybin + j * sx;
 	const double x = half_xbin + i * sy;
-	// pixel centres of this block (same expressions as x and y)
-	const unsigned tx0 = blockIdx.x * blockDim.x, ty0 = blockIdx.y * blockDim.y;
-	const unsigned tx1 = min(tx0 + blockDim.x - 1, width - 1), ty1 = min(ty0 + blockDim.y - 1, height - 1);
-	const double xlo = half_xbin + tx0 * sy, xhi = half_xbin + tx1 * sy;
-	const double ylo = half_ybin + ty0 * sx, yhi = half_ybin + ty1 * sx;
+	const unsigned tx0 = blockIdx.x * PIX_TILE_W, ty0 = blockIdx.y * PIX_TILE_H;
 	const bool drawn = !mask || mask[pix];
 
 	for (int pi = p0; pi < p1; pi++) {
 		const FProfile &p = profiles[pi];
-		if (!drawn) {
-			if constexpr (J) {
-				if (is_radial_kind(p.kind)) {
-					JT *jp = jac + (size_t)pi * nt * npix + pix;
-					for (int k = 0; k < nt; k++) jp[(size_t)k * npix] = JT(0);
-				}
-			}
-			continue;
-		}
 		if (p.kind == PK_SKY) {
-			acc[p.target] += p.flux_scale;  // sky value is kept in flux_scale
+			if (drawn) acc[p.target] += p.flux_scale;  // sky value is kept in flux_scale
 			continue;
 		}
 		if (!is_radial_kind(p.kind)) continue;
+		// block-uniform: nothing drawn, no tangent planes stored
+		if (tile_culled(p, tx0, ty0, width, height, sx, sy)) continue;
+		// planes of the kind's own tangents only (the reduction reads no more)
+		const int nk = tangent_count(p.kind);
+		if (!drawn) {
+			if constexpr (J) {
+				JT *jp = jac + (size_t)pi * nt * npix + pix;
+				for (int k = 0; k < nk; k++) jp[(size_t)k * npix] = JT(0);
+			}
+			continue;
+		}
 		constexpr int NT = ntk<AK>();
 		float jl[NT];
 #pragma unroll
 		for (int k = 0; k < NT; k++) jl[k] = 0.f;
-		bool culled = false;
-		if (p.r_max > 0.f) {  // block-uniform
-			const double nx = fmin(fmax(p.cx, xlo), xhi) - p.cx, ny = fmin(fmax(p.cy, ylo), yhi) - p.cy;
-			const double lim = (double)p.r_max + 2.0;
-			culled = nx * nx + ny * ny > lim * lim;
-		}
-		if (!culled) {
+		{
 			float xp, yp;
 			const int decision = pixel_decision32(p, x, y, xp, yp);
 			if (decision == PD_ZERO) {
@@ -552,7 +582,7 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 			JT *jp = jac + (size_t)pi * nt * npix + pix;
 #pragma unroll
 			for (int k = 0; k < NT; k++)
-				if (k < nt) jp[(size_t)k * npix] = (JT)jl[k];
+				if (k < nk) jp[(size_t)k * npix] = (JT)jl[k];
 		}
 	}
 	img_conv[(size_t)b * npix + pix] = acc[0];
@@ -1200,19 +1230,21 @@ __device__ __forceinline__ void jac_gradient_tail(const GradStepArgs &g, unsigne
 }
 
 // sum over pixels of g(pixel) * J_k(pixel) for each radial profile:
-// blockIdx.y = profile, blockIdx.x strides over the pixels, two pixels per
-// thread and step with every load issued before the products; about one
-// wave of four blocks per SM (at most 64 registers with FP32 planes), so the
-// last block to finish is not a second wave's.  Each
-// block writes
-// its NTAN sums to `partials`; the block that finishes last (an atomic
-// ticket per profile, no waiting) adds the partials in block order and
+// blockIdx.y = profile, blockIdx.x strides over the pixel tiles of
+// k_pixels32 (32 x 8, one pixel per thread), two tiles per step with every
+// load issued before the products; tiles the profile does not reach
+// (tile_culled, as the render decided them) are skipped, their planes never
+// written.  About one wave of four blocks per SM (at most 64 registers with
+// FP32 planes), so the last block to finish is not a second wave's.  Each
+// block writes its NTAN sums to `partials`; the block that finishes last (an
+// atomic ticket per profile, no waiting) adds the partials in block order and
 // resets the ticket, so the result does not depend on block scheduling.
 template <int NT, class JT>
 __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_jac_reduce(const JT *__restrict__ jac, const float *__restrict__ g_conv,
                                                     const float *__restrict__ g_plain,
                                                     const FProfile *__restrict__ profiles,
-                                                    const int *__restrict__ prof_batch, unsigned npix, int nt,
+                                                    const int *__restrict__ prof_batch, unsigned width,
+                                                    unsigned height, double sx, double sy, int nt,
                                                     double *__restrict__ partials, unsigned *__restrict__ tickets,
                                                     double *__restrict__ out, GradStepArgs grad,
                                                     unsigned *__restrict__ grad_ticket)
@@ -1227,22 +1259,21 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 	}
 	const int nk = tangent_count(p.kind);  // <= nt <= NT
 	const int b = prof_batch[pi];
+	const size_t npix = (size_t)width * height;
 	const float *g = (p.target == 0 ? g_conv : g_plain) + (size_t)b * npix;
 	const JT *jp = jac + (size_t)pi * nt * npix;
 	double acc[NT];
 #pragma unroll
 	for (int k = 0; k < NT; k++) acc[k] = 0.0;
-	const unsigned step = gridDim.x * blockDim.x * U;
-	for (unsigned t0 = blockIdx.x * blockDim.x * U + threadIdx.x; t0 < npix; t0 += step) {
+	// U pixels per thread per step, every load issued before the products
+	auto step = [&](const bool (&in)[U], const size_t (&pix)[U]) {
 		float gv[U];
 		JT jv[U][NT];
 #pragma unroll
 		for (int u = 0; u < U; u++) {
-			const unsigned t = t0 + u * blockDim.x;
-			const bool in = t < npix;
-			gv[u] = in ? g[t] : 0.f;
+			gv[u] = in[u] ? g[pix[u]] : 0.f;
 #pragma unroll
-			for (int k = 0; k < NT; k++) jv[u][k] = (in && k < nk) ? jp[(size_t)k * npix + t] : JT(0);
+			for (int k = 0; k < NT; k++) jv[u][k] = (in[u] && k < nk) ? jp[(size_t)k * npix + pix[u]] : JT(0);
 		}
 #pragma unroll
 		for (int u = 0; u < U; u++)
@@ -1255,6 +1286,45 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 					else acc[k] += (double)(gv[u] * jv[u][k]);
 				}
 			}
+	};
+	if (tiles_all_reached(p, width, height, sx, sy)) {
+		// every tile holds planes: a plain stride over the pixels (no tile
+		// padding at the right edge, no per-tile test)
+		const unsigned stride = gridDim.x * blockDim.x * U;
+		for (unsigned t0 = blockIdx.x * blockDim.x * U + threadIdx.x; t0 < npix; t0 += stride) {
+			bool in[U];
+			size_t pix[U];
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				pix[u] = t0 + u * blockDim.x;
+				in[u] = pix[u] < npix;
+			}
+			step(in, pix);
+		}
+	}
+	else {
+		const unsigned tiles_x = (width + PIX_TILE_W - 1) / PIX_TILE_W;
+		const unsigned ntiles = tiles_x * ((height + PIX_TILE_H - 1) / PIX_TILE_H);
+		const unsigned lx = threadIdx.x % PIX_TILE_W, ly = threadIdx.x / PIX_TILE_W;
+		const unsigned stride = gridDim.x * U;
+		for (unsigned t0 = blockIdx.x * U; t0 < ntiles; t0 += stride) {
+			bool in[U];
+			size_t pix[U];
+#pragma unroll
+			for (int u = 0; u < U; u++) {
+				const unsigned t = t0 + u;
+				in[u] = t < ntiles;
+				pix[u] = 0;
+				if (in[u]) {
+					const unsigned ty = t / tiles_x, tx = t - ty * tiles_x;
+					const unsigned i = tx * PIX_TILE_W + lx, j = ty * PIX_TILE_H + ly;
+					in[u] = i < width && j < height &&
+					        !tile_culled(p, tx * PIX_TILE_W, ty * PIX_TILE_H, width, height, sx, sy);
+					pix[u] = (size_t)j * width + i;
+				}
+			}
+			step(in, pix);
+		}
 	}
 	__shared__ double s_red[NT][8];
 	__shared__ bool s_last;
@@ -1366,7 +1436,7 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, JacPlanes jac,
                             int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask)
 {
-	dim3 block(32, 8), grid(cdiv(width, 32), cdiv(height, 8), batch);
+	dim3 block(PIX_TILE_W, PIX_TILE_H), grid(cdiv(width, PIX_TILE_W), cdiv(height, PIX_TILE_H), batch);
 	note_launches(1);
 	if (jac.p && jac.fp64) {
 		auto k = all_kinds ? k_pixels32<true, true, double> : k_pixels32<false, true, double>;
@@ -1495,30 +1565,35 @@ cudaError_t launch_levels32(const FProfile *profiles, int n_levels, unsigned npi
 	                       cusps, q, s);
 }
 
-unsigned jac_reduce_blocks(unsigned npix, int n_profiles)
+unsigned jac_reduce_blocks(unsigned width, unsigned height, int n_profiles)
 {
-	unsigned bx = cdiv(npix, 256 * 2);
-	const unsigned target = cdiv(148u * 4u, (unsigned)n_profiles);  // one wave of 4 blocks per SM in all
-	if (bx > target) bx = target;
-	return bx < 1 ? 1 : bx;
+	// about one wave of 4 blocks per SM in all, and the same number of
+	// two-tile steps for every block (a block with one step more than the
+	// others is the launch's tail)
+	const unsigned tiles = cdiv(width, PIX_TILE_W) * cdiv(height, PIX_TILE_H);
+	const unsigned target = cdiv(148u * 4u, (unsigned)n_profiles);
+	const unsigned steps = std::max(1u, (unsigned)((double)tiles / (2.0 * target) + 0.5));
+	return std::max(1u, cdiv(tiles, 2 * steps));
 }
 
 cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
-                              const int *prof_batch, int n_profiles, unsigned npix, int nt, double *partials,
-                              unsigned *tickets, double *out, cudaStream_t s, const GradStepArgs *grad)
+                              const int *prof_batch, int n_profiles, unsigned width, unsigned height, double sx,
+                              double sy, int nt, double *partials, unsigned *tickets, double *out, cudaStream_t s,
+                              const GradStepArgs *grad)
 {
-	const unsigned bx = jac_reduce_blocks(npix, n_profiles);
+	const unsigned bx = jac_reduce_blocks(width, height, n_profiles);
 	const GradStepArgs g = grad ? *grad : GradStepArgs{};
 	unsigned *gt = grad ? tickets + n_profiles : (unsigned *)nullptr;
 	note_launches(1);
 	if (jac.fp64) {
 		auto k = nt <= 9 ? k_jac_reduce<9, double> : k_jac_reduce<NTAN, double>;
-		return launch_pdl(k, dim3(bx, n_profiles), dim3(256), 0, s, static_cast<const double *>(jac.p), g_conv, g_plain,
-		                  profiles, prof_batch, npix, nt, partials, tickets, out, g, gt);
+		return launch_pdl(k, dim3(bx, n_profiles), dim3(PIX_TILE_W * PIX_TILE_H), 0, s,
+		                  static_cast<const double *>(jac.p), g_conv, g_plain, profiles, prof_batch, width, height, sx,
+		                  sy, nt, partials, tickets, out, g, gt);
 	}
 	auto k = nt <= 9 ? k_jac_reduce<9, float> : k_jac_reduce<NTAN, float>;
-	return launch_pdl(k, dim3(bx, n_profiles), dim3(256), 0, s, static_cast<const float *>(jac.p), g_conv, g_plain,
-	                  profiles, prof_batch, npix, nt, partials, tickets, out, g, gt);
+	return launch_pdl(k, dim3(bx, n_profiles), dim3(PIX_TILE_W * PIX_TILE_H), 0, s, static_cast<const float *>(jac.p),
+	                  g_conv, g_plain, profiles, prof_batch, width, height, sx, sy, nt, partials, tickets, out, g, gt);
 }
 
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
