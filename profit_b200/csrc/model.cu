@@ -11,6 +11,7 @@
 #include <array>
 #include <cctype>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -2819,6 +2820,22 @@ constexpr size_t CAT_BUDGET_BYTES = 6ull << 30;
 // PSF spectra of the chunks that convolve through FFTs, all chunks together
 constexpr size_t CAT_SPECTRA_BYTES = 16ull << 30;
 enum CatConv : int { CAT_CONV_AUTO = 0, CAT_CONV_BRUTE, CAT_CONV_FFT };
+
+// PF_CATALOGUE_LOG=1: the host time of each step of a call that builds or
+// records, on stderr.
+bool cat_log_on()
+{
+	static const bool on = [] {
+		const char *v = getenv("PF_CATALOGUE_LOG");
+		return v && v[0] == '1';
+	}();
+	return on;
+}
+
+double cat_now()
+{
+	return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
 // Engines whose streams run chunks side by side in the recorded call: the
 // small kernels of one chunk (the cusp levels, the likelihood, the tails of
 // the waves) leave SMs idle that another chunk's kernels fill.
@@ -3068,6 +3085,7 @@ int cat_pick_convolvers(pf_catalogue *c)
 // Groups galaxies into chunks and uploads the static inputs.
 int cat_build(pf_catalogue *c)
 {
+	const double t_build = cat_now();
 	// the chunks and their buffers are rebuilt: a recorded call no longer applies
 	if (c->graph) cudaGraphExecDestroy(c->graph);
 	c->graph = nullptr;
@@ -3352,6 +3370,7 @@ int cat_build(pf_catalogue *c)
 		for (auto &t : pool) t.join();
 		if (status != PF_OK) return set_error(PF_E_CUDA, "catalogue inputs: " + err_msg);
 	}
+	if (cat_log_on()) fprintf(stderr, "[profit_b200 catalogue] inputs uploaded: %.3f s\n", cat_now() - t_build);
 	c->nprof = (int)params.size();
 	PF_CUDA(ensure(c->params, params.size() * sizeof(ProfileParams)));
 	PF_CUDA(cudaMemcpy(c->params.p, params.data(), params.size() * sizeof(ProfileParams), cudaMemcpyHostToDevice));
@@ -3435,7 +3454,15 @@ int cat_build(pf_catalogue *c)
 		c->lane_qpix[lane] = qpix;
 		c->max_levels = std::max(c->max_levels, levels);
 	}
+	const double t_conv = cat_now();
+	if (cat_log_on()) fprintf(stderr, "[profit_b200 catalogue] lanes and scratch: %.3f s\n", t_conv - t_build);
 	PF_TRY(cat_pick_convolvers(c));
+	if (cat_log_on()) {
+		int nfft = 0;
+		for (auto &ch : c->chunks) nfft += ch->fft ? 1 : 0;
+		fprintf(stderr, "[profit_b200 catalogue] convolver per batch: %.3f s (%d of %zu batches through FFTs)\n",
+		        cat_now() - t_conv, nfft, c->chunks.size());
+	}
 	c->built = true;
 	return PF_OK;
 }
@@ -3693,7 +3720,12 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 	for (auto &G : c->gal)
 		if (G.profiles.empty()) return set_error(PF_E_STATE, "a catalogue galaxy has no profiles");
 	PF_TRY(ensure_stream(c->engine));
-	if (!c->built) PF_TRY(cat_build(c));
+	const double t_call = cat_now();
+	if (!c->built) {
+		PF_TRY(cat_build(c));
+		if (cat_log_on())
+			fprintf(stderr, "[profit_b200 catalogue] build: %.3f s (%zu batches)\n", cat_now() - t_call, c->chunks.size());
+	}
 	pf_model *m = c->engine;
 	if (c->params_dirty) {
 		// new values (pf_catalogue_set_values): the profile records in chunk
@@ -3787,6 +3819,9 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 		cudaGraphExecDestroy(c->graph);  // captured with capacities that no longer hold
 		c->graph = nullptr;
 	}
+	if (cat_log_on() && !replay)
+		fprintf(stderr, "[profit_b200 catalogue] evaluation without the recorded call: %.3f s since the call began\n",
+		        cat_now() - t_call);
 	if (!replay && !retried && m->use_graphs) {
 		// record the call that just ran (every choice it made is cached now)
 		// for the next calls, with the chunks on their lanes; nothing runs
@@ -3811,6 +3846,8 @@ int pf_catalogue_loglike_grad(pf_catalogue *c, double *loglike, double *grad)
 	}
 	PF_CUDA(cudaEventRecord(c->ev[1], s));
 	PF_CUDA(cudaEventSynchronize(c->ev[1]));
+	if (cat_log_on() && !replay)
+		fprintf(stderr, "[profit_b200 catalogue] call with recording: %.3f s\n", cat_now() - t_call);
 	for (auto &chp : c->chunks) {
 		const CatChunk &ch = *chp;
 		const double *hl = ch.h_ll.as<double>(), *hg = ch.h_grad.as<double>();
