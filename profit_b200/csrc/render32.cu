@@ -1303,27 +1303,58 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 		}
 	}
 	else {
+		// the block's tiles are blockIdx.x * U + j * gridDim.x * U + u (spread
+		// over the drawing, so that the reached ones are shared out evenly);
+		// each round, one thread per tile tests it and the reached ones are
+		// listed in thread order, then the block walks the list U tiles a step
+		__shared__ uint32_t s_tile[PIX_TILE_W * PIX_TILE_H];  // (ty << 16) | tx
+		__shared__ int s_cnt[PIX_TILE_W * PIX_TILE_H / 32];
+		const int tl = threadIdx.x & 31, tw = threadIdx.x >> 5;
 		const unsigned tiles_x = (width + PIX_TILE_W - 1) / PIX_TILE_W;
 		const unsigned ntiles = tiles_x * ((height + PIX_TILE_H - 1) / PIX_TILE_H);
 		const unsigned lx = threadIdx.x % PIX_TILE_W, ly = threadIdx.x / PIX_TILE_W;
-		const unsigned stride = gridDim.x * U;
-		for (unsigned t0 = blockIdx.x * U; t0 < ntiles; t0 += stride) {
-			bool in[U];
-			size_t pix[U];
-#pragma unroll
-			for (int u = 0; u < U; u++) {
-				const unsigned t = t0 + u;
-				in[u] = t < ntiles;
-				pix[u] = 0;
-				if (in[u]) {
+		const unsigned stride = gridDim.x * U, first = blockIdx.x * U;
+		const unsigned count = first < ntiles ? ((ntiles - 1 - first) / stride + 1) * U : 0;
+		for (unsigned c0 = 0; c0 < count; c0 += blockDim.x) {
+			const unsigned c = c0 + threadIdx.x;
+			bool keep = false;
+			uint32_t code = 0;
+			if (c < count) {
+				const unsigned t = first + (c / U) * stride + (c % U);
+				if (t < ntiles) {
 					const unsigned ty = t / tiles_x, tx = t - ty * tiles_x;
-					const unsigned i = tx * PIX_TILE_W + lx, j = ty * PIX_TILE_H + ly;
-					in[u] = i < width && j < height &&
-					        !tile_culled(p, tx * PIX_TILE_W, ty * PIX_TILE_H, width, height, sx, sy);
-					pix[u] = (size_t)j * width + i;
+					keep = !tile_culled(p, tx * PIX_TILE_W, ty * PIX_TILE_H, width, height, sx, sy);
+					code = (ty << 16) | tx;
 				}
 			}
-			step(in, pix);
+			const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+			if (tl == 0) s_cnt[tw] = __popc(ballot);
+			__syncthreads();
+			int before = 0, total = 0;
+#pragma unroll
+			for (int w = 0; w < PIX_TILE_W * PIX_TILE_H / 32; w++) {
+				before += w < tw ? s_cnt[w] : 0;
+				total += s_cnt[w];
+			}
+			if (keep) s_tile[before + __popc(ballot & ((1u << tl) - 1u))] = code;
+			__syncthreads();
+			for (int k = 0; k < total; k += U) {
+				bool in[U];
+				size_t pix[U];
+#pragma unroll
+				for (int u = 0; u < U; u++) {
+					in[u] = k + u < total;
+					pix[u] = 0;
+					if (in[u]) {
+						const uint32_t tc = s_tile[k + u];
+						const unsigned i = (tc & 0xffffu) * PIX_TILE_W + lx, j = (tc >> 16) * PIX_TILE_H + ly;
+						in[u] = i < width && j < height;
+						pix[u] = (size_t)j * width + i;
+					}
+				}
+				step(in, pix);
+			}
+			__syncthreads();  // the next round rewrites s_tile and s_cnt
 		}
 	}
 	__shared__ double s_red[NT][8];
