@@ -412,16 +412,33 @@ constexpr int ntk()
 // which no contraction or reassociation can change between kernels.
 enum PixelDecision : int { PD_ZERO = 0, PD_DIRECT = 1, PD_SUBSAMPLE = 2 };
 
-__device__ __forceinline__ int pixel_decision32(const FProfile &p, double x, double y, float &xp, float &yp)
+// The terms of a pixel column (centre x) in the rotated coordinates:
+// dx cos(theta) and -dx sin(theta)/q, dx = x - xcen.  Kernels whose threads
+// walk down a column form them once per profile.
+struct ColumnTerms {
+	float c, s;
+};
+
+__device__ __forceinline__ ColumnTerms column_terms(const FProfile &p, double x)
 {
 	const float dx = __double2float_rn(__dsub_rn(x, p.cx));
+	return {__fmul_rn(dx, p.cos_ang), __fmul_rn(-dx, p.sin_q)};
+}
+
+__device__ __forceinline__ int pixel_decision32(const FProfile &p, ColumnTerms ct, double y, float &xp, float &yp)
+{
 	const float dy = __double2float_rn(__dsub_rn(y, p.cy));
-	xp = __fadd_rn(__fmul_rn(dx, p.cos_ang), __fmul_rn(dy, p.sin_ang));
-	yp = __fadd_rn(__fmul_rn(-dx, p.sin_q), __fmul_rn(dy, p.cos_q));
+	xp = __fadd_rn(ct.c, __fmul_rn(dy, p.sin_ang));
+	yp = __fadd_rn(ct.s, __fmul_rn(dy, p.cos_q));
 	const float r = __fsqrt_rn(__fadd_rn(__fmul_rn(xp, xp), __fmul_rn(yp, yp)));
 	if (p.r_max > 0.f && r > p.r_max) return PD_ZERO;
 	if (p.rough || r > p.r_switch) return PD_DIRECT;
 	return PD_SUBSAMPLE;
+}
+
+__device__ __forceinline__ int pixel_decision32(const FProfile &p, double x, double y, float &xp, float &yp)
+{
+	return pixel_decision32(p, column_terms(p, x), y, xp, yp);
 }
 
 template <int NT>
@@ -610,6 +627,8 @@ __device__ __forceinline__ void listed_pixel(const FProfile &p, int pi, double x
 		return;
 	}
 	float xp, yp;
+	// (forming the column terms once per profile for both rows took this
+	// kernel from 48 to 56 registers and one CTA per SM, a net loss)
 	const int decision = pixel_decision32(p, x, y, xp, yp);
 	if (decision == PD_DIRECT) {
 		acc[p.target] += p.flux_scale * eval_val<float, AK>(p, xp, yp);
@@ -1038,15 +1057,16 @@ __global__ void __launch_bounds__(256, AK ? 3 : 5) k_adjoint_pixels32_listed(con
 			float acc[NT];
 #pragma unroll
 			for (int t = 0; t < NT; t++) acc[t] = 0.f;
+			const ColumnTerms ct = column_terms(p, half_xbin + i * sy);  // the thread's column
 			for (unsigned r = threadIdx.x >> 6; r < 32; r += 4) {
 				const unsigned j = ty0 + r;
 				if (i >= width || j >= height) continue;
 				if (mask && !mask[i + (size_t)j * width]) continue;  // not drawn by the forward pass
 				const float gv = g[i + (size_t)j * width];
 				if (gv == 0.f) continue;
-				const double y = half_ybin + j * sx, x = half_xbin + i * sy;
+				const double y = half_ybin + j * sx;
 				float xp, yp;
-				if (pixel_decision32(p, x, y, xp, yp) != PD_DIRECT) continue;
+				if (pixel_decision32(p, ct, y, xp, yp) != PD_DIRECT) continue;
 				Tan<float> t = eval_tan<float, AK, true>(p, xp, yp);
 				tan_to_j<NT>(t, xp, yp, gv, acc);
 			}
