@@ -300,8 +300,12 @@ int pf_catalogue_set_magzero(pf_catalogue *c, double magzero);
  * geometry, once, at the first evaluation after galaxies are added, and keeps
  * the faster), "brute" or "fft" (batches whose FFT grid would exceed 6912
  * points a side stay brute force).  The FFT form gives the brute-force sums
- * to FP64 transform roundoff.  pf_catalogue_convolvers: how many of the
- * batches convolve through FFTs, of how many (after an evaluation). */
+ * to FP64 transform roundoff.  A batch that convolves through FFTs keeps each
+ * of its galaxies' PSF spectra on the device (16 bytes per point of half the
+ * FFT grid, about 8 bytes per drawing pixel); batches beyond 16 GB of spectra
+ * in all stay brute force.  pf_catalogue_convolvers: how many of the batches
+ * convolve through FFTs, of how many (after an evaluation).  No counterpart in
+ * libprofit, whose FFTConvolver serves one image (convolve.cpp:245-312). */
 int pf_catalogue_set_convolver(pf_catalogue *c, const char *name);
 int pf_catalogue_convolvers(const pf_catalogue *c, int *fft_chunks, int *chunks);
 int pf_catalogue_add_galaxy(pf_catalogue *c, unsigned width, unsigned height, const double *data,
