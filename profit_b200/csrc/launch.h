@@ -56,9 +56,13 @@ struct JacPlanes {
 // jac: tangent planes (null: values only);
 // all_kinds: the model has radial profiles other than Sersic and Moffat.
 // mask: optional drawing-size calculation mask shared by the batch entries
+// extent: optional, per batch entry the part of the drawing (x < extent.x,
+// y < extent.y) that its outputs read; beyond it the images are zero and no
+// tangent planes are written (a catalogue galaxy in a larger shared canvas)
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, JacPlanes jac,
-                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask = nullptr);
+                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask = nullptr,
+                            const int2 *extent = nullptr);
 // psf point-source profiles in the FP32 pipeline: the stamp (forward) and the
 // sums of the adjoint image against the stamp and its centre derivatives.
 cudaError_t launch_psf_stamp32(const DevProfile *dev, const int *prof_begin, int batch, const double *psf,
@@ -109,12 +113,13 @@ struct GradStepArgs {
 	unsigned *seq_out = nullptr;
 };
 unsigned jac_reduce_blocks(unsigned width, unsigned height, int n_profiles);
-// width, height, sx, sy: the drawing grid as given to launch_pixels32, whose
-// tiles skipped by a profile hold no tangent planes of that profile.
+// width, height, sx, sy, extent: the drawing grid and extents as given to
+// launch_pixels32, whose tiles skipped by a profile, and pixels beyond its
+// batch entry's extent, hold no tangent planes of that profile.
 cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
                               const int *prof_batch, int n_profiles, unsigned width, unsigned height, double sx,
                               double sy, int nt, double *partials, unsigned *tickets, double *out, cudaStream_t s,
-                              const GradStepArgs *grad = nullptr);
+                              const GradStepArgs *grad = nullptr, const int2 *extent = nullptr);
 // Copies `bytes` (a multiple of 16, both addresses 16-byte aligned) from
 // pinned host memory mapped into the device's address space to dst, and
 // zeroes ctrl[0 .. ctrl_words); one launch in place of a copy and a memset.

@@ -2811,6 +2811,7 @@ struct CatChunk {
 	// slices of the catalogue's shared device and pinned host arenas
 	Span data, sigma, region, psf32, psfrev32;
 	Span prof_begin, prof_batch, grad_off, T, ll, grad;
+	Span extent;  // per member, the drawing its outputs read (int2: own width, height + the PSF padding)
 	Span h_ll, h_grad, h_ctrl;
 	size_t npix() const { return (size_t)(W + 2 * (pw / 2)) * (H + 2 * (ph / 2)); }
 	size_t nout() const { return (size_t)W * H; }
@@ -3158,7 +3159,7 @@ int cat_build(pf_catalogue *c)
 		return o;
 	};
 	struct Slots {
-		size_t prof_begin, prof_batch, grad_off, T, ll, grad, h_ll, h_grad, h_ctrl;
+		size_t prof_begin, prof_batch, grad_off, extent, T, ll, grad, h_ll, h_grad, h_ctrl;
 	};
 	std::vector<Slots> slots(c->chunks.size());
 	for (size_t k = 0; k < c->chunks.size(); k++) {
@@ -3197,6 +3198,13 @@ int cat_build(pf_catalogue *c)
 		sl.prof_begin = put(prof_begin);
 		sl.prof_batch = put(prof_batch);
 		sl.grad_off = put(goff);
+		std::vector<int> ext(2 * (size_t)C);
+		for (int i = 0; i < C; i++) {
+			const CatGalaxy &G = c->gal[ch.members[i]];
+			ext[2 * i] = (int)(G.w + 2 * (ch.pw / 2));
+			ext[2 * i + 1] = (int)(G.h + 2 * (ch.ph / 2));
+		}
+		sl.extent = put(ext);
 		sl.T = take(dtop, (size_t)ch.nprof * NTAN * 8);
 		sl.ll = take(dtop, (size_t)C * 8);
 		sl.grad = take(dtop, (size_t)std::max(gtot, 1) * 8);
@@ -3233,6 +3241,7 @@ int cat_build(pf_catalogue *c)
 		ch.prof_begin.p = d + sl.prof_begin;
 		ch.prof_batch.p = d + sl.prof_batch;
 		ch.grad_off.p = d + sl.grad_off;
+		ch.extent.p = d + sl.extent;
 		ch.T.p = d + sl.T;
 		ch.ll.p = d + sl.ll;
 		ch.grad.p = d + sl.grad;
@@ -3515,7 +3524,7 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch, int lane)
 	const FProfile *fprof = c->fprof.as<FProfile>() + ch.p0;
 	const DevProfile *dev = c->dev.as<DevProfile>() + ch.p0;
 	PF_CUDA(launch_pixels32(fprof, ch.prof_begin.as<int>(), C, a.dw, a.dh, 1.0, 1.0, conv, plain, jac, ch.nt, ch.ak, q,
-	                        s));
+	                        s, nullptr, ch.extent.as<int2>()));
 	PF_CUDA(launch_levels32(fprof, a.levels, (unsigned)npix, conv, plain, jac, ch.nt, ch.ak, ch.cusps, q, s));
 	PF_TRY(cat_conv_forward(m, ch, a, ch.fft, conv, plain, model64, s));
 	PF_CUDA(launch_loglike64_batch(model64, ch.data.as<double>(), ch.sigma.as<double>(), ch.region.as<uint8_t>(),
@@ -3525,7 +3534,7 @@ int cat_enqueue_chunk(pf_catalogue *c, CatChunk &ch, int lane)
 	PF_TRY(cat_conv_adjoint(m, ch, a, ch.fft, wseed, gconv, s));
 	PF_CUDA(launch_jac_reduce(jac, gconv, gplain, fprof, ch.prof_batch.as<int>(), ch.nprof, a.dw, a.dh, 1.0, 1.0,
 	                          ch.nt, m->d_jac_partials.as<double>(), m->d_jac_tickets.as<unsigned>(),
-	                          ch.T.as<double>(), s));
+	                          ch.T.as<double>(), s, nullptr, ch.extent.as<int2>()));
 	PF_CUDA(launch_cat_gradient(dev, ch.nprof, ch.T.as<double>(), ch.grad_off.as<int>(), ch.grad.as<double>(), s));
 	PF_CUDA(cudaMemcpyAsync(ch.h_ll.p, ch.ll.p, (size_t)C * 8, cudaMemcpyDeviceToHost, s));
 	PF_CUDA(cudaMemcpyAsync(ch.h_grad.p, ch.grad.p, (size_t)std::max(ch.ngrad, 1) * 8, cudaMemcpyDeviceToHost, s));

@@ -519,7 +519,7 @@ template <bool AK, bool J, class JT>
 __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__restrict__ prof_begin,
                            unsigned width, unsigned height, double sx, double sy, float *__restrict__ img_conv,
                            float *__restrict__ img_plain, JT *__restrict__ jac, int nt, QueueSet q,
-                           const uint8_t *__restrict__ mask)
+                           const uint8_t *__restrict__ mask, const int2 *__restrict__ extent)
 {
 	pdl_enter();
 	const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -528,6 +528,12 @@ __global__ void k_pixels32(const FProfile *__restrict__ profiles, const int *__r
 	if (i >= width || j >= height) return;
 	const size_t npix = (size_t)width * height;
 	const uint32_t pix = i + j * width;
+	if (extent && (i >= (unsigned)extent[b].x || j >= (unsigned)extent[b].y)) {
+		// beyond what this entry's outputs read: zero images, no planes
+		img_conv[(size_t)b * npix + pix] = 0.f;
+		img_plain[(size_t)b * npix + pix] = 0.f;
+		return;
+	}
 	const int p0 = prof_begin[b], p1 = prof_begin[b + 1];
 	float acc[2] = {0.f, 0.f};
 	const double half_xbin = sx / 2., half_ybin = sy / 2.;
@@ -1267,7 +1273,8 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
                                                     unsigned height, double sx, double sy, int nt,
                                                     double *__restrict__ partials, unsigned *__restrict__ tickets,
                                                     double *__restrict__ out, GradStepArgs grad,
-                                                    unsigned *__restrict__ grad_ticket)
+                                                    unsigned *__restrict__ grad_ticket,
+                                                    const int2 *__restrict__ extent)
 {
 	pdl_enter();
 	constexpr int U = 2;
@@ -1307,7 +1314,10 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 				}
 			}
 	};
-	if (tiles_all_reached(p, width, height, sx, sy)) {
+	// the planes end at the batch entry's extent (launch_pixels32)
+	const unsigned ew = extent ? min(width, (unsigned)extent[b].x) : width;
+	const unsigned eh = extent ? min(height, (unsigned)extent[b].y) : height;
+	if (ew == width && eh == height && tiles_all_reached(p, width, height, sx, sy)) {
 		// every tile holds planes: a plain stride over the pixels (no tile
 		// padding at the right edge, no per-tile test)
 		const unsigned stride = gridDim.x * blockDim.x * U;
@@ -1343,7 +1353,8 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 				const unsigned t = first + (c / U) * stride + (c % U);
 				if (t < ntiles) {
 					const unsigned ty = t / tiles_x, tx = t - ty * tiles_x;
-					keep = !tile_culled(p, tx * PIX_TILE_W, ty * PIX_TILE_H, width, height, sx, sy);
+					keep = tx * PIX_TILE_W < ew && ty * PIX_TILE_H < eh &&
+					       !tile_culled(p, tx * PIX_TILE_W, ty * PIX_TILE_H, width, height, sx, sy);
 					code = (ty << 16) | tx;
 				}
 			}
@@ -1368,7 +1379,7 @@ __global__ void __launch_bounds__(256, (NT <= 9 && sizeof(JT) == 4) ? 4 : 2) k_j
 					if (in[u]) {
 						const uint32_t tc = s_tile[k + u];
 						const unsigned i = (tc & 0xffffu) * PIX_TILE_W + lx, j = (tc >> 16) * PIX_TILE_H + ly;
-						in[u] = i < width && j < height;
+						in[u] = i < ew && j < eh;
 						pix[u] = (size_t)j * width + i;
 					}
 				}
@@ -1485,14 +1496,15 @@ cudaError_t launch_stage_in(void *dst, const void *host_src, size_t bytes, uint3
 
 cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int batch, unsigned width,
                             unsigned height, double sx, double sy, float *img_conv, float *img_plain, JacPlanes jac,
-                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask)
+                            int nt, bool all_kinds, const QueueSet &q, cudaStream_t s, const uint8_t *mask,
+                            const int2 *extent)
 {
 	dim3 block(PIX_TILE_W, PIX_TILE_H), grid(cdiv(width, PIX_TILE_W), cdiv(height, PIX_TILE_H), batch);
 	note_launches(1);
 	if (jac.p && jac.fp64) {
 		auto k = all_kinds ? k_pixels32<true, true, double> : k_pixels32<false, true, double>;
 		return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain,
-		                  static_cast<double *>(jac.p), nt, q, mask);
+		                  static_cast<double *>(jac.p), nt, q, mask, extent);
 	}
 	if (!jac.p) {
 		auto k = all_kinds ? k_pixels32_listed<true> : k_pixels32_listed<false>;
@@ -1502,7 +1514,7 @@ cudaError_t launch_pixels32(const FProfile *profiles, const int *prof_begin, int
 	}
 	auto k = all_kinds ? k_pixels32<true, true, float> : k_pixels32<false, true, float>;
 	return launch_pdl(k, grid, block, 0, s, profiles, prof_begin, width, height, sx, sy, img_conv, img_plain,
-	                  static_cast<float *>(jac.p), nt, q, mask);
+	                  static_cast<float *>(jac.p), nt, q, mask, extent);
 }
 
 // Kind grouping of one wide level's items (models with profiles of every
@@ -1630,7 +1642,7 @@ unsigned jac_reduce_blocks(unsigned width, unsigned height, int n_profiles)
 cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g_plain, const FProfile *profiles,
                               const int *prof_batch, int n_profiles, unsigned width, unsigned height, double sx,
                               double sy, int nt, double *partials, unsigned *tickets, double *out, cudaStream_t s,
-                              const GradStepArgs *grad)
+                              const GradStepArgs *grad, const int2 *extent)
 {
 	const unsigned bx = jac_reduce_blocks(width, height, n_profiles);
 	const GradStepArgs g = grad ? *grad : GradStepArgs{};
@@ -1640,11 +1652,12 @@ cudaError_t launch_jac_reduce(JacPlanes jac, const float *g_conv, const float *g
 		auto k = nt <= 9 ? k_jac_reduce<9, double> : k_jac_reduce<NTAN, double>;
 		return launch_pdl(k, dim3(bx, n_profiles), dim3(PIX_TILE_W * PIX_TILE_H), 0, s,
 		                  static_cast<const double *>(jac.p), g_conv, g_plain, profiles, prof_batch, width, height, sx,
-		                  sy, nt, partials, tickets, out, g, gt);
+		                  sy, nt, partials, tickets, out, g, gt, extent);
 	}
 	auto k = nt <= 9 ? k_jac_reduce<9, float> : k_jac_reduce<NTAN, float>;
 	return launch_pdl(k, dim3(bx, n_profiles), dim3(PIX_TILE_W * PIX_TILE_H), 0, s, static_cast<const float *>(jac.p),
-	                  g_conv, g_plain, profiles, prof_batch, width, height, sx, sy, nt, partials, tickets, out, g, gt);
+	                  g_conv, g_plain, profiles, prof_batch, width, height, sx, sy, nt, partials, tickets, out, g, gt,
+	                  extent);
 }
 
 cudaError_t launch_embed_seed(const float *w, unsigned ow, unsigned oh, unsigned padx, unsigned pady, unsigned dw,
