@@ -2805,7 +2805,7 @@ struct CatChunk {
 	// instead of the brute-force kernels: the faster of the two, timed at build
 	bool fft = false;
 	FftConv<double> fc;
-	DevBuf kspec;
+	Span kspec;  // in pf_catalogue::spectra
 	bool ak = false;
 	bool plain = false;  // a profile drawn without convolution (reads the seed of the plain image)
 	// slices of the catalogue's shared device and pinned host arenas
@@ -2839,8 +2839,10 @@ double cat_now()
 }
 // Engines whose streams run chunks side by side in the recorded call: the
 // small kernels of one chunk (the cusp levels, the likelihood, the tails of
-// the waves) leave SMs idle that another chunk's kernels fill.
-constexpr int CAT_LANES = 4;
+// the waves) leave SMs idle that another chunk's kernels fill.  (10,000
+// galaxies on one B200: 222.5 ms per call with 4, 219.7 with 6, 218.9 with 8,
+// whose first call took longer.)
+constexpr int CAT_LANES = 6;
 constexpr unsigned CAT_SIDE_STEP = 64;
 
 }  // namespace
@@ -2860,6 +2862,7 @@ struct pf_catalogue {
 	DevBuf lum;                       // LUM_SLOTS luminosity evaluations per profile (prologue scratch)
 	DevBuf arena;                     // every chunk's index tables, tangent sums, logL and gradient
 	DevBuf canvases;                  // every chunk's data, sigma, region and PSF images
+	DevBuf spectra, spectra_trial;    // PSF spectra of the FFT chunks; one chunk's, while timing
 	HostBuf h_arena;                  // every chunk's logL, gradient and queue control words
 	int nprof = 0;
 	std::vector<int> grad_off;
@@ -2979,12 +2982,15 @@ void release(DevBuf &b)
 }
 
 // Each chunk's convolver: brute force, or FP64 FFTs with the members' PSF
-// spectra computed here once.  Under CAT_CONV_AUTO both are timed on the
-// chunk itself (forward and adjoint, after a warm-up run, which also tunes
-// the brute-force tile) on lane 0, whose scratch takes every chunk, and the
-// faster is kept; brute force is not timed (nor tuned) where the FFTs beat
-// its FLOP count at the GPU's FP32 peak.  The timed runs read zeroed
-// drawings and write only buffers that every evaluation rewrites.
+// spectra.  Under CAT_CONV_AUTO both are timed on the chunk itself (forward
+// and adjoint, after a warm-up run, which also tunes the brute-force tile) on
+// lane 0, whose scratch takes every chunk, and the faster is kept; brute
+// force is not timed (nor tuned) where the FFTs beat its FLOP count at the
+// GPU's FP32 peak.  The timed runs read zeroed drawings and write only
+// buffers that every evaluation rewrites.  The trials share one spectrum
+// buffer; the chosen chunks' spectra then go into one allocation (a device
+// allocation and release per chunk had made this step take 0.1-1 s more,
+// varying from run to run).
 int cat_pick_convolvers(pf_catalogue *c)
 {
 	pf_model *m = c->lanes[0];
@@ -3000,18 +3006,21 @@ int cat_pick_convolvers(pf_catalogue *c)
 			if (b) cudaEventDestroy(b);
 		}
 	} guard{e0, e1};
-	size_t spectra = 0;
-	std::vector<size_t> work(c->lanes.size(), 0);
 	// an upper bound on the GPU's FP32 rate: 128 FMA lanes per SM at the
 	// highest SM clock, with a quarter more for safety
 	int sms = 0, khz = 0;
 	PF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, m->device));
 	PF_CUDA(cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, m->device));
 	const double fp32_peak = 1.25 * 256.0 * sms * (khz * 1e3);
-	for (auto &chp : c->chunks) {
-		CatChunk &ch = *chp;
+	double t_alloc = 0, t_fft_trials = 0, t_brute_trials = 0;  // host time, for the timing log
+
+	// the chunks that may convolve through FFTs: their grids and spectra sizes
+	std::vector<size_t> need(c->chunks.size(), 0);
+	size_t most = 0;
+	for (size_t k = 0; k < c->chunks.size(); k++) {
+		CatChunk &ch = *c->chunks[k];
 		ch.fft = false;
-		release(ch.kspec);
+		ch.kspec.p = nullptr;
 		if (c->conv_mode == CAT_CONV_BRUTE) continue;
 		const Analysis a = cat_analysis(ch);
 		const int N = fft_good_size((int)a.dw), M = fft_good_size((int)a.dh);
@@ -3020,16 +3029,29 @@ int cat_pick_convolvers(pf_catalogue *c)
 			cudaGetLastError();
 			continue;
 		}
+		need[k] = ch.fc.spectrum_elems() * sizeof(double2) * ch.members.size();
+		most = std::max(most, need[k]);
+	}
+	if (most) {
+		const double t0 = cat_now();
+		PF_CUDA(ensure(c->spectra_trial, most));
+		PF_CUDA(ensure(m->d_fftwork64, most));
+		t_alloc += cat_now() - t0;
+	}
+
+	size_t spectra = 0;
+	std::vector<size_t> work(c->lanes.size(), 0);
+	for (size_t k = 0; k < c->chunks.size(); k++) {
+		CatChunk &ch = *c->chunks[k];
+		if (!need[k] || spectra + need[k] > CAT_SPECTRA_BYTES) continue;
 		const int C = (int)ch.members.size();
-		const size_t bytes = ch.fc.spectrum_elems() * sizeof(double2) * C;
-		if (spectra + bytes > CAT_SPECTRA_BYTES) continue;
-		PF_CUDA(ensure(ch.kspec, bytes));
-		PF_CUDA(ensure(m->d_fftwork64, bytes));
-		PF_CUDA(ch.fc.set_kernels(ch.psf32.as<float>(), (int)ch.pw, (int)ch.ph, (size_t)ch.pw * ch.ph,
-		                          ch.kspec.as<double2>(), C, s));
-		note_launches(2);
 		bool use = c->conv_mode == CAT_CONV_FFT;
 		if (!use) {
+			const Analysis a = cat_analysis(ch);
+			ch.kspec.p = c->spectra_trial.p;
+			PF_CUDA(ch.fc.set_kernels(ch.psf32.as<float>(), (int)ch.pw, (int)ch.ph, (size_t)ch.pw * ch.ph,
+			                          ch.kspec.as<double2>(), C, s));
+			note_launches(2);
 			float *conv = m->d_conv32.as<float>(), *plain = m->d_plain32.as<float>();
 			float *wseed = m->d_wseed.as<float>(), *gconv = m->d_gconv.as<float>();
 			PF_CUDA(cudaMemsetAsync(conv, 0, ch.npix() * C * 4, s));
@@ -3055,7 +3077,9 @@ int cat_pick_convolvers(pf_catalogue *c)
 				return PF_OK;
 			};
 			float t_fft = 0, t_brute = 0;
+			double t0 = cat_now();
 			PF_TRY(timed(true, t_fft));
+			t_fft_trials += cat_now() - t0;
 			// brute force cannot beat its multiply-adds at the FP32 peak: an
 			// FFT faster than that wins without tuning and timing the tiles
 			const double flop = 2.0 * ch.pw * ch.ph * (double)(ch.nout() + ch.npix()) * C;
@@ -3063,23 +3087,44 @@ int cat_pick_convolvers(pf_catalogue *c)
 				use = true;
 			}
 			else {
+				t0 = cat_now();
 				PF_TRY(timed(false, t_brute));
+				t_brute_trials += cat_now() - t0;
 				use = t_fft < t_brute;
 			}
+			ch.kspec.p = nullptr;
 		}
 		if (use) {
 			ch.fft = true;
-			spectra += bytes;
-			work[0] = std::max(work[0], bytes);
-			work[ch.lane] = std::max(work[ch.lane], bytes);
-		}
-		else {
-			release(ch.kspec);
+			spectra += need[k];
+			work[0] = std::max(work[0], need[k]);
+			work[ch.lane] = std::max(work[ch.lane], need[k]);
 		}
 	}
+
+	// the FFT chunks' spectra, one allocation for all of them
+	double t0 = cat_now();
+	if (spectra) PF_CUDA(ensure(c->spectra, spectra));
+	size_t off = 0;
+	for (size_t k = 0; k < c->chunks.size(); k++) {
+		CatChunk &ch = *c->chunks[k];
+		if (!ch.fft) continue;
+		ch.kspec.p = c->spectra.as<char>() + off;
+		off += need[k];
+		PF_CUDA(ch.fc.set_kernels(ch.psf32.as<float>(), (int)ch.pw, (int)ch.ph, (size_t)ch.pw * ch.ph,
+		                          ch.kspec.as<double2>(), (int)ch.members.size(), s));
+		note_launches(2);
+	}
 	PF_CUDA(cudaStreamSynchronize(s));
+	release(c->spectra_trial);
 	for (size_t l = 0; l < c->lanes.size(); l++)
 		if (work[l]) PF_CUDA(ensure(c->lanes[l]->d_fftwork64, work[l]));
+	t_alloc += cat_now() - t0;
+	if (cat_log_on())
+		fprintf(stderr,
+		        "[profit_b200 catalogue] convolver trials: FFT %.3f s, brute force (with tuning) %.3f s, "
+		        "spectra %.3f s\n",
+		        t_fft_trials, t_brute_trials, t_alloc);
 	return PF_OK;
 }
 
